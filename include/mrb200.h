@@ -1,0 +1,193 @@
+/*
+ * meturay_b200 -- C ABI of the B200 wavefront path-tracing core.
+ *
+ * The library (meturay_b200/libmrb200.so) replaces the MRay
+ * (yalcinerbora/meturay) TracerCUDA plugin on its hot path: the "LBVH"
+ * triangle accelerator group and the plain wavefront PathTracer.  Every
+ * object entry point names the reference interface it stands in for.
+ * Signatures use plain pointers and sizes only.
+ *
+ * Conventions
+ *   - Return value: 0 (MRB_OK) on success, a negative MRB_E* code on
+ *     failure; mrb_last_error() then describes the failure (per thread).
+ *     Nothing aborts the process (reference: TracerError values,
+ *     RayLib/TracerError.h, and TracerException on GPU OOM,
+ *     RayLib/CudaCheck.h:31-38, become status codes here).
+ *   - "d_" pointers are device pointers on the current CUDA device; "stream"
+ *     is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - HitKey layout: batch << 24 | id (RayLib/HitStructs.h:154); batches:
+ *     0 null, 1 Lambert, 2 Metal, 3 Refract, 4 primitive light.
+ */
+#ifndef MRB200_H
+#define MRB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MRB_OK 0
+#define MRB_E_ARG (-1)
+#define MRB_E_CUDA (-2)
+#define MRB_E_OOM (-3)
+#define MRB_E_STATE (-4)
+#define MRB_E_UNSUPPORTED (-5)
+#define MRB_E_DEVICE (-6) /* a device-side bounded wait or stack limit gave up */
+
+typedef struct mrb_system mrb_system;
+typedef struct mrb_scene mrb_scene;
+typedef struct mrb_tracer mrb_tracer;
+
+/* Material types of a scene description (JSON names of the reference). */
+#define MRB_MAT_LAMBERT 1 /* "Lambert"  LambertMaterialKC.cuh:12-111 */
+#define MRB_MAT_METAL 2   /* "Metal"    MetalGlassMaterialsKC.cuh:11-222 */
+#define MRB_MAT_REFRACT 3 /* "Refract"  SimpleMaterialsKC.cuh:172-302 */
+#define MRB_MAT_LIGHT 4   /* primitive-backed light, GPULightPrimitive.cuh */
+
+typedef struct mrb_material {
+    uint32_t type;
+    float albedo[3];   /* Lambert / Refract */
+    float eta[3];      /* Metal */
+    float k[3];        /* Metal */
+    float specular[3]; /* Metal */
+    float roughness;   /* Metal */
+    uint32_t medium;   /* Refract: medium index inside the surface */
+    float radiance[3]; /* Light */
+} mrb_material;
+
+typedef struct mrb_scene_desc {
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    const float* positions;      /* vertex_count * 3 */
+    const float* normals;        /* vertex_count * 3 */
+    const float* uvs;            /* vertex_count * 2, may be NULL */
+    const uint32_t* indices;     /* triangle_count * 3 */
+    const uint32_t* tri_material;/* triangle_count, index into materials */
+    const uint8_t* tri_cull;     /* triangle_count, may be NULL (two-sided) */
+    uint32_t material_count;
+    const mrb_material* materials;
+    uint32_t medium_count;       /* homogeneous media without absorption */
+    const float* medium_ior;     /* medium_count */
+    uint32_t base_medium;
+} mrb_scene_desc;
+
+/* Pinhole camera node ("Pinhole": position, gaze, up, planes, fov in
+ * radians; GPUCameraPinhole.cuh:83-106). */
+typedef struct mrb_camera {
+    float position[3];
+    float gaze[3];
+    float up[3];
+    float near_far[2];
+    float fov[2];
+} mrb_camera;
+
+/* ---- errors ---------------------------------------------------------- */
+const char* mrb_last_error(void);
+
+/* ---- tracer system: TracerSystemI (RayLib/TracerSystemI.h:34-50) ------
+ * replaces GenerateTracerSystem / DeleteTracerSystem
+ * (TracerCUDA/EntryPoint.h:12-16) plus TracerSystemI::Initialize. */
+int mrb_system_create(int device, mrb_system** out);
+void mrb_system_destroy(mrb_system* sys);
+
+/* ---- scene: TracerSystemI::GenerateScene (GPUSceneJson.cpp:163-360).
+ * Builds per-vertex tangent-space rotations as GPUPrimitiveTriangle.cpp:
+ * 160-320 does and uploads the scene to the device. */
+int mrb_scene_create(mrb_system* sys, const mrb_scene_desc* desc, mrb_scene** out);
+void mrb_scene_destroy(mrb_scene* scene);
+/* counts[0..7]: triangles, vertices, lights, lambert, metal, refract,
+ * media, id bits of the partition key. */
+int mrb_scene_counts(const mrb_scene* scene, uint32_t* counts8);
+/* Host copies of the device-side scene arrays: tbn (vertex_count*4,
+ * w,x,y,z), tri_key (triangle_count), lambert (3 each), metal (10 each:
+ * eta3 k3 spec3 roughness), refract albedo (3 each), refract medium,
+ * light radiance (3 each), light primitive.  Any pointer may be NULL. */
+int mrb_scene_export(const mrb_scene* scene, float* tbn, uint32_t* tri_key, float* lambert,
+                     float* metal, float* refract, uint32_t* refract_medium,
+                     float* light_radiance, uint32_t* light_prim);
+
+/* ---- accelerator group "LBVH": GPUAcceleratorGroupI
+ * (GPUAcceleratorI.h:46-134), drop-in for GPUAccBVHGroup
+ * (GPUAcceleratorBVH.cuh:63-203). */
+/* ConstructAccelerators: Morton codes, onesweep sort, hierarchy + AABBs. */
+int mrb_accel_construct(mrb_scene* scene, void* stream);
+/* Host copies of the build in reference numbering (LinearBVH.cuh:22-43):
+ * codes/sorted_idx (n), left/right (n-1), parent (2n-1), inner AABBs
+ * ((n-1)*6), root, triangle AABBs (n*6), extent (6).  NULL skips. */
+int mrb_accel_export(const mrb_scene* scene, uint64_t* codes, uint32_t* sorted_idx,
+                     uint32_t* left, uint32_t* right, uint32_t* parent, float* inner,
+                     uint32_t* root, float* tri_aabbs, float* extent);
+/* Hit (GPUAcceleratorI.h:95-108): closest hit of n rays.
+ * d_ray_o[i] = (origin, tMin), d_ray_d[i] = (direction, tMax) as float4.
+ * Outputs: HitKey (0 on miss), triangle index (0xFFFFFFFF on miss), t,
+ * barycentrics (1-u-v, u) as TriangleHit. */
+int mrb_accel_hit(const mrb_scene* scene, const float* d_ray_o, const float* d_ray_d, uint32_t n,
+                  uint32_t* d_key, uint32_t* d_prim, float* d_t, float* d_bary, void* stream);
+
+/* ---- tracer "PathTracer": GPUTracerI (RayLib/GPUTracerI.h:24-71) ---- */
+int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out);
+void mrb_tracer_destroy(mrb_tracer* t);
+/* SetOptions keys (PathTracer.h:17-33): "Samples", "MaxDepth",
+ * "NextEventEstimation", "RussianRouletteStart", "DirectLightMIS" (0 only),
+ * plus "Seed" (RNG key) and "Frame" (RNG iteration counter). */
+int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
+int mrb_tracer_set_resolution(mrb_tracer* t, uint32_t width, uint32_t height);
+int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* cam);
+/* The camera frame as the device sees it (14 floats: position, bottom-left,
+ * right, up, plane size, near/far); GPUCameraPinhole.cuh:135-162. */
+int mrb_camera_frame(const mrb_camera* cam, float* out14);
+/* GenerateWork / Render (1 while work remains, 0 when done) / Finalize. */
+int mrb_tracer_generate_work(mrb_tracer* t, uint32_t camera_index);
+int mrb_tracer_render(mrb_tracer* t);
+int mrb_tracer_finalize(mrb_tracer* t);
+/* GenerateWork + all Render steps + Finalize as one captured CUDA graph. */
+int mrb_tracer_render_frame(mrb_tracer* t);
+/* Per-pixel image (width*height*4: sum of per-frame means, frame count in
+ * .w) and the last frame's per-sample radiance ((w*s)*(h*s)*4). */
+int mrb_tracer_get_image(mrb_tracer* t, float* host_rgba);
+int mrb_tracer_get_samples(mrb_tracer* t, float* host_rgba);
+int mrb_tracer_reset_image(mrb_tracer* t);
+/* Rays traced (camera + path + NEE, summed over depths) since creation. */
+int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays_traced, uint32_t* frames);
+/* Stream the tracer launches on (cudaStream_t as void*). */
+void* mrb_tracer_stream(mrb_tracer* t);
+
+/* ---- kernel-level entry points (device pointers) ---------------------- */
+/* KCGenerateAABBs + extent reduce + KCGenMortonCodes
+ * (LinearBVH.hpp:102-166,444-482). */
+int mrb_morton_codes(const float* d_pos, const uint32_t* d_idx, uint32_t n, float* d_tri_aabb,
+                     float* d_extent, uint64_t* d_codes, void* stream);
+/* Stable radix sort of pairs on bits [begin_bit, end_bit), as
+ * cub::DeviceRadixSort::SortPairs(Descending) (ParallelRadixSort.cuh:60-100). */
+size_t mrb_radix_sort_temp_bytes(uint32_t n, int key_bytes, int begin_bit, int end_bit);
+int mrb_radix_sort_pairs_u64(uint64_t* d_keys, uint32_t* d_vals, uint32_t n, int begin_bit,
+                             int end_bit, int descending, void* d_temp, size_t temp_bytes,
+                             void* stream);
+int mrb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, int begin_bit,
+                             int end_bit, int descending, void* d_temp, size_t temp_bytes,
+                             void* stream);
+/* LBVH hierarchy + AABBs from sorted codes (LinearBVH.hpp:30-100,181-396).
+ * d_scratch: 3*(n-1) u32.  Outputs in reference numbering. */
+int mrb_lbvh_hierarchy(const uint64_t* d_sorted_codes, const uint32_t* d_sorted_idx,
+                       const float* d_tri_aabb, uint32_t n, uint32_t* d_left, uint32_t* d_right,
+                       uint32_t* d_parent, float* d_inner, uint32_t* d_root, uint32_t* d_scratch,
+                       void* d_nodes64, void* stream);
+/* RayMemory::SortKeys + Partition (RayMemory.cu:187-312): stable descending
+ * sort of the rays by (batch, id) key bits and per-batch [offset, end).
+ * d_portion_offset / d_portion_end: 8 entries each; d_non_null: 1. */
+size_t mrb_partition_temp_bytes(uint32_t n, uint32_t id_bits);
+int mrb_partition(const uint32_t* d_keys, uint32_t n, uint32_t id_bits, uint32_t* d_sorted_ids,
+                  uint32_t* d_sorted_dense, uint32_t* d_portion_offset, uint32_t* d_portion_end,
+                  uint32_t* d_non_null, void* d_temp, size_t temp_bytes, void* stream);
+
+/* Portable math of the device path, for the CPU/GPU bit-parity check:
+ * out[i*2+0..1] = sin, cos of x[i]; out2[i] = acos(y[i]). */
+int mrb_debug_math(const float* d_x, uint32_t n, float* d_sincos, const float* d_y,
+                   float* d_acos, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MRB200_H */

@@ -1,0 +1,13 @@
+"""meturay_b200: a B200-native (sm_100a) wavefront path-tracing core that
+drops in for MRay's (yalcinerbora/meturay) LBVH accelerator group and plain
+wavefront PathTracer.
+
+The compute path is ``libmrb200.so`` (hand-written CUDA, C ABI in
+``include/mrb200.h``); this package is the host-side mirror of the
+reference's plugin interfaces over that ABI.
+"""
+from ._lib import MrbError, lib  # noqa: F401  (fails loudly if the library is missing)
+from .tracer import GPUScene, PathTracer, TracerSystem, camera_frame  # noqa: F401
+from . import scenes  # noqa: F401
+
+__all__ = ["TracerSystem", "GPUScene", "PathTracer", "MrbError", "scenes", "camera_frame"]

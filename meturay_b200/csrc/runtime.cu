@@ -1,0 +1,1020 @@
+// Host runtime and C ABI of the meturay_b200 core.
+//
+// Objects mirror the MRay plugin surfaces on the hot path:
+//   mrb_system  <- TracerSystemI / TracerSystemCUDA (TracerSystemCUDA.cpp:19-100)
+//   mrb_scene   <- GPUSceneI with one triangle primitive group, its material
+//                  groups, primitive lights and the "LBVH" accelerator group
+//   mrb_tracer  <- GPUTracerI "PathTracer" (PathTracer.cu:144-326)
+// The wavefront loop keeps every count on the device: trace -> partition ->
+// shade per depth with no host synchronisation, and a whole frame can be
+// captured once as a CUDA graph and replayed.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/mrb200.h"
+#include "common.cuh"
+#include "lbvh.cuh"
+#include "shade.cuh"
+#include "sort.cuh"
+#include "trace.cuh"
+
+namespace mrb {
+
+static thread_local std::string g_error;
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    int alloc(size_t b) {
+        if (b <= bytes && p) return 0;
+        release();
+        if (b == 0) return 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+            p = nullptr;
+            return MRB_E_OOM;
+        }
+        bytes = b;
+        return 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+template <class T>
+int upload(DBuf& b, const std::vector<T>& v) {
+    if (v.empty()) {
+        b.release();
+        return 0;
+    }
+    int r = b.alloc(v.size() * sizeof(T));
+    if (r) return r;
+    MRB_CUDA(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side tangent space, as the triangle loader does it
+// (GPUPrimitiveTriangle.cpp:160-320, Triangle.h:73-111, Quaternion.hpp:372-480)
+// ---------------------------------------------------------------------------
+struct H3 {
+    float v[3];
+    float& operator[](int i) { return v[i]; }
+    float operator[](int i) const { return v[i]; }
+};
+inline H3 h3(float a, float b, float c) { return H3{{a, b, c}}; }
+inline H3 hsub(H3 a, H3 b) { return h3(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
+inline H3 hadd(H3 a, H3 b) { return h3(a[0] + b[0], a[1] + b[1], a[2] + b[2]); }
+inline H3 hmul(H3 a, float s) { return h3(a[0] * s, a[1] * s, a[2] * s); }
+inline float hdot(H3 a, H3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline H3 hcross(H3 a, H3 b) {
+    return h3(a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]);
+}
+inline H3 hnorm(H3 a) {
+    float inv = 1.0f / std::sqrt(hdot(a, a));
+    return hmul(a, inv);
+}
+inline bool hnan(H3 a) { return std::isnan(a[0]) || std::isnan(a[1]) || std::isnan(a[2]); }
+inline H3 orthogonal(H3 v) {  // OrthogonalVector (Vector.hpp:877-886)
+    if (std::fabs(v[0]) > std::fabs(v[1])) {
+        float s = std::sqrt(v[0] * v[0] + v[2] * v[2]);
+        return h3(-v[2] / s, 0.0f / s, v[0] / s);
+    }
+    float s = std::sqrt(v[1] * v[1] + v[2] * v[2]);
+    return h3(0.0f / s, v[2] / s, -v[1] / s);
+}
+inline H3 calc_tangent(H3 p0, H3 p1, H3 p2, const float* uv0, const float* uv1,
+                       const float* uv2) {
+    H3 vec0 = hsub(p1, p0), vec1 = hsub(p2, p0);
+    float du0x = uv1[0] - uv0[0], du0y = uv1[1] - uv0[1];
+    float du1x = uv2[0] - uv0[0], du1y = uv2[1] - uv0[1];
+    float t = (du0x * du1y - du1x * du0y);
+    if (t == 0.0f) return h3(NAN, NAN, NAN);
+    float r = 1.0f / t;
+    H3 a = hmul(vec0, du1y), b = hmul(vec1, du0y);
+    H3 tan = hmul(hsub(a, b), r);
+    if (t < 0) tan = h3(-tan[0], -tan[1], -tan[2]);
+    return tan;
+}
+inline void space_quat(H3 xIn, H3 y, H3 z, float q[4]) {
+    H3 x = xIn;
+    H3 c = hsub(hcross(x, y), z);
+    if (std::fabs(c[0]) > 0.1f && std::fabs(c[1]) > 0.1f && std::fabs(c[2]) > 0.1f)
+        x = h3(-x[0], -x[1], -x[2]);
+    float t;
+    float w, qx, qy, qz;
+    if (z[2] < 0) {
+        if (x[0] > y[1]) {
+            t = 1 + x[0] - y[1] - z[2];
+            w = y[2] - z[1]; qx = t; qy = x[1] + y[0]; qz = z[0] + x[2];
+        } else {
+            t = 1 - x[0] + y[1] - z[2];
+            w = z[0] - x[2]; qx = x[1] + y[0]; qy = t; qz = y[2] + z[1];
+        }
+    } else {
+        if (x[0] < -y[1]) {
+            t = 1 - x[0] - y[1] + z[2];
+            w = x[1] - y[0]; qx = z[0] + x[2]; qy = y[2] + z[1]; qz = t;
+        } else {
+            t = 1 + x[0] + y[1] + z[2];
+            w = t; qx = y[2] - z[1]; qy = z[0] - x[2]; qz = x[1] - y[0];
+        }
+    }
+    float s = 0.5f / std::sqrt(t);
+    w *= s; qx *= s; qy *= s; qz *= s;
+    float inv = 1.0f / std::sqrt(w * w + qx * qx + qy * qy + qz * qz);
+    q[0] = w * inv;
+    q[1] = -(qx * inv);
+    q[2] = -(qy * inv);
+    q[3] = -(qz * inv);
+}
+
+void build_tbn(const mrb_scene_desc& d, std::vector<float>& tbn) {
+    const uint32_t V = d.vertex_count, T = d.triangle_count;
+    std::vector<H3> tangents(V, h3(0, 0, 0));
+    static const float kDefUv[3][2] = {{0.f, 0.f}, {1.f, 0.f}, {0.f, 1.f}};
+    auto P = [&](uint32_t v) { return h3(d.positions[3 * v], d.positions[3 * v + 1], d.positions[3 * v + 2]); };
+    auto N = [&](uint32_t v) { return h3(d.normals[3 * v], d.normals[3 * v + 1], d.normals[3 * v + 2]); };
+    for (uint32_t t = 0; t < T; t++) {
+        uint32_t ix[3] = {d.indices[3 * t], d.indices[3 * t + 1], d.indices[3 * t + 2]};
+        const float* uv[3];
+        for (int k = 0; k < 3; k++) uv[k] = d.uvs ? d.uvs + 2 * ix[k] : kDefUv[k];
+        for (int k = 0; k < 3; k++) {
+            int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+            H3 tk = calc_tangent(P(ix[k]), P(ix[k1]), P(ix[k2]), uv[k], uv[k1], uv[k2]);
+            if (hnan(tk)) tk = orthogonal(N(ix[k]));
+            tangents[ix[k]] = hadd(tangents[ix[k]], tk);
+        }
+    }
+    tbn.resize(size_t(V) * 4);
+    for (uint32_t v = 0; v < V; v++) {
+        H3 n = N(v), t = tangents[v];
+        if (hdot(t, t) < 1.0e-5f) t = orthogonal(n);
+        t = hnorm(t);
+        H3 tn = hnorm(hsub(t, hmul(n, hdot(n, t))));
+        H3 b = hcross(n, tn);
+        space_quat(tn, b, n, &tbn[4 * size_t(v)]);
+    }
+}
+
+inline uint32_t bits_for(uint32_t maxId) {
+    uint32_t b = 1;
+    while (b < 24 && (1u << b) <= maxId) b++;
+    return b;
+}
+
+}  // namespace
+}  // namespace mrb
+
+using namespace mrb;
+
+// ===========================================================================
+// Objects
+// ===========================================================================
+struct mrb_system {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+};
+
+struct mrb_scene {
+    mrb_system* sys = nullptr;
+    uint32_t V = 0, T = 0;
+    std::vector<float> tbn;
+    std::vector<uint32_t> triKey;
+    std::vector<float> lambert, metal, refract, lightRad;
+    std::vector<uint32_t> refractMed, lightPrim;
+    std::vector<float> mediumIor;
+    uint32_t baseMedium = 0;
+    uint32_t idBits = 1;
+    DBuf dPos, dTbn, dIdx, dKey, dCull, dLambert, dMetal, dRefract, dRefractMed, dLightRad,
+        dLightPrim, dMediumIor;
+    // LBVH
+    bool built = false;
+    DBuf aTriAabb, aExtent, aCodes, aSorted, aLeft, aRight, aParent, aInner, aScratch, aRoot,
+        aNodes, aTv0, aTe0, aTe1, aSortTemp;
+    int rootInner = 0;
+    SceneDev dev() const {
+        SceneDev s{};
+        s.vertexCount = V;
+        s.triCount = T;
+        s.pos = dPos.as<float>();
+        s.tbn = dTbn.as<float4>();
+        s.idx = dIdx.as<uint32_t>();
+        s.triKey = dKey.as<uint32_t>();
+        s.triCull = dCull.as<uint8_t>();
+        s.lambertAlbedo = dLambert.as<float>();
+        s.metalParams = dMetal.as<float>();
+        s.refractAlbedo = dRefract.as<float>();
+        s.refractMedium = dRefractMed.as<uint32_t>();
+        s.lightRadiance = dLightRad.as<float>();
+        s.lightPrim = dLightPrim.as<uint32_t>();
+        s.lightCount = static_cast<uint32_t>(lightPrim.size());
+        s.mediumIor = dMediumIor.as<float>();
+        s.baseMedium = baseMedium;
+        return s;
+    }
+    AccelDev accel() const {
+        AccelDev a{};
+        a.nodes = aNodes.as<BvhNode>();
+        a.tv0 = aTv0.as<float4>();
+        a.te0 = aTe0.as<float4>();
+        a.te1 = aTe1.as<float4>();
+        a.root = rootInner;
+        a.triCount = T;
+        return a;
+    }
+};
+
+struct mrb_tracer {
+    mrb_system* sys = nullptr;
+    mrb_scene* scene = nullptr;
+    cudaStream_t stream = nullptr;
+    // options (PathTracer.h:17-33 defaults)
+    uint32_t samples = 1, maxDepth = 5, nee = 1, rrStart = 3, mis = 0;
+    uint64_t seed = 1;
+    uint32_t width = 0, height = 0;
+    CameraDev* hostCam = nullptr;  // pinned staging copy of the camera frame
+    DBuf devCam;                   // the frame the camera kernel reads
+    bool camSet = false;
+    uint32_t launchesPerFrame = 0;
+    // wavefront memory
+    uint32_t maxRays = 0;
+    DBuf rayO[2], rayD[2], aux[2], count, hitKey, hitPrim, hitT, hitBary, dense, sortedIds,
+        portion, samplesBuf, image, counters, frameWord, errorFlags, sortTemp;
+    size_t sortTempBytes = 0;
+    // stepwise GPUTracerI state
+    uint32_t depth = 0;
+    bool working = false;
+    uint32_t frames = 0;
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    bool graphDirty = true;
+    ~mrb_tracer() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (stream) cudaStreamSynchronize(stream);
+        if (hostCam) cudaFreeHost(hostCam);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int ensure_buffers(mrb_tracer* t) {
+    if (!t->width || !t->height) {
+        set_error("tracer: resolution not set");
+        return MRB_E_STATE;
+    }
+    const uint64_t paths = uint64_t(t->width) * t->samples * t->height * t->samples;
+    if (paths == 0 || paths > (1ull << 29)) {
+        set_error("tracer: %llu samples per iteration is out of range",
+                  (unsigned long long)paths);
+        return MRB_E_ARG;
+    }
+    const uint32_t maxRays = static_cast<uint32_t>(2 * paths);
+    if (maxRays == t->maxRays && t->rayO[0].p) return 0;
+    t->maxRays = maxRays;
+    int r = 0;
+    for (int i = 0; i < 2; i++) {
+        if ((r = t->rayO[i].alloc(size_t(maxRays) * 16))) return r;
+        if ((r = t->rayD[i].alloc(size_t(maxRays) * 16))) return r;
+        if ((r = t->aux[i].alloc(size_t(maxRays) * sizeof(RayAux)))) return r;
+    }
+    if ((r = t->count.alloc(2 * 4))) return r;
+    if ((r = t->hitKey.alloc(size_t(maxRays) * 4))) return r;
+    if ((r = t->hitPrim.alloc(size_t(maxRays) * 4))) return r;
+    if ((r = t->hitT.alloc(size_t(maxRays) * 4))) return r;
+    if ((r = t->hitBary.alloc(size_t(maxRays) * 8))) return r;
+    if ((r = t->dense.alloc(size_t(maxRays) * 4))) return r;
+    if ((r = t->sortedIds.alloc(size_t(maxRays) * 4))) return r;
+    if ((r = t->portion.alloc(32 * 4))) return r;
+    if ((r = t->samplesBuf.alloc(size_t(paths) * 16))) return r;
+    if ((r = t->image.alloc(size_t(t->width) * t->height * 16))) return r;
+    if ((r = t->counters.alloc(16))) return r;
+    if ((r = t->frameWord.alloc(4))) return r;
+    if ((r = t->errorFlags.alloc(16))) return r;
+    t->sortTempBytes = radix_sort_temp_bytes(maxRays, 4, 0, 3 + 24);
+    if ((r = t->sortTemp.alloc(t->sortTempBytes))) return r;
+    MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+    MRB_CUDA(cudaMemsetAsync(t->counters.p, 0, 16, t->stream));
+    MRB_CUDA(cudaMemsetAsync(t->errorFlags.p, 0, 16, t->stream));
+    MRB_CUDA(cudaMemsetAsync(t->frameWord.p, 0, 4, t->stream));
+    t->graphDirty = true;
+    return 0;
+}
+
+PathOptions path_options(const mrb_tracer* t) {
+    PathOptions o{};
+    o.width = t->width;
+    o.height = t->height;
+    o.samples = t->samples;
+    o.maxDepth = t->maxDepth;
+    o.rrStart = t->rrStart;
+    o.nee = t->nee;
+    o.seedLo = static_cast<uint32_t>(t->seed);
+    o.seedHi = static_cast<uint32_t>(t->seed >> 32);
+    o.frame = t->frameWord.as<uint32_t>();
+    return o;
+}
+
+PortionTable portion_table(const mrb_tracer* t) {
+    uint32_t* p = t->portion.as<uint32_t>();
+    return PortionTable{p, p + 8, p + 16};
+}
+
+int step_camera(mrb_tracer* t) {
+    uint32_t* cnt = t->count.as<uint32_t>();
+    return camera_generate(t->devCam.as<CameraDev>(), path_options(t), t->scene->baseMedium,
+                           t->rayO[0].as<float4>(),
+                           t->rayD[0].as<float4>(), t->aux[0].as<RayAux>(),
+                           t->samplesBuf.as<float4>(), cnt, t->stream);
+}
+
+// One Render() step: HitRays -> PartitionRaysWRTWork -> WorkRays
+// (PathTracer.cu:144-291) for the rays of buffer `cur`.
+int step_depth(mrb_tracer* t, uint32_t d) {
+    mrb_scene* sc = t->scene;
+    const int cur = d & 1, nxt = cur ^ 1;
+    uint32_t* cnt = t->count.as<uint32_t>();
+    HitOut ho{t->hitKey.as<uint32_t>(), t->hitPrim.as<uint32_t>(), t->hitT.as<float>(),
+              t->hitBary.as<float2>()};
+    int r;
+    if ((r = trace_closest(sc->accel(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+                           cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
+        return r;
+    if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
+    PortionTable pt = portion_table(t);
+    if ((r = dense_keys(ho.key, cnt + cur, t->maxRays, sc->idBits, t->dense.as<uint32_t>(), pt,
+                        t->stream)))
+        return r;
+    if ((r = radix_sort_pairs<uint32_t>(t->dense.as<uint32_t>(), t->sortedIds.as<uint32_t>(),
+                                        cnt + cur, t->maxRays, 0, 3 + int(sc->idBits), true,
+                                        t->sortTemp.p, t->sortTempBytes, t->stream, true)))
+        return r;
+    if ((r = find_portions(t->dense.as<uint32_t>(), cnt + cur, t->maxRays, sc->idBits, pt,
+                           t->stream)))
+        return r;
+    MRB_CUDA(cudaMemsetAsync(cnt + nxt, 0, 4, t->stream));
+    HitIn hi{ho.key, ho.prim, ho.t, ho.bary};
+    const bool gen = (d + 1) < t->maxDepth;
+    return shade(sc->dev(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+                 t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull,
+                 t->maxRays, t->samplesBuf.as<float4>(), path_options(t), gen,
+                 t->rayO[nxt].as<float4>(), t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(),
+                 cnt + nxt, t->stream);
+}
+
+int step_finalize(mrb_tracer* t) {
+    int r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
+                    t->image.as<float4>(), t->stream);
+    if (r) return r;
+    return frame_advance(t->frameWord.as<uint32_t>(), t->stream);
+}
+
+int record_frame(mrb_tracer* t) {
+    int r;
+    if ((r = step_camera(t))) return r;
+    for (uint32_t d = 0; d < t->maxDepth; d++)
+        if ((r = step_depth(t, d))) return r;
+    return step_finalize(t);
+}
+
+int check_device_errors(mrb_tracer* t) {
+    uint32_t e[2] = {0, 0};
+    MRB_CUDA(cudaMemcpyAsync(e, t->errorFlags.p, 4, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaMemcpyAsync(e + 1, radix_sort_error_flag(t->sortTemp.p, t->maxRays), 4,
+                             cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    if (e[0] || e[1]) {
+        set_error("device-side limit hit (trace flag %u, sort flag %u)", e[0], e[1]);
+        return MRB_E_DEVICE;
+    }
+    return 0;
+}
+
+int set_device(mrb_system* s) {
+    MRB_CUDA(cudaSetDevice(s->device));
+    return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* mrb_last_error(void) { return g_error.c_str(); }
+
+int mrb_system_create(int device, mrb_system** out) {
+    if (!out) {
+        set_error("mrb_system_create: out is NULL");
+        return MRB_E_ARG;
+    }
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available (%s)", cudaGetErrorString(e));
+        return MRB_E_CUDA;
+    }
+    if (device < 0 || device >= n) {
+        set_error("device %d out of range (%d devices)", device, n);
+        return MRB_E_ARG;
+    }
+    mrb_system* s = new mrb_system();
+    s->device = device;
+    MRB_CUDA(cudaSetDevice(device));
+    *out = s;
+    return 0;
+}
+
+void mrb_system_destroy(mrb_system* s) { delete s; }
+
+int mrb_scene_create(mrb_system* sys, const mrb_scene_desc* d, mrb_scene** out) {
+    if (!sys || !d || !out || !d->positions || !d->normals || !d->indices || !d->tri_material ||
+        (d->material_count && !d->materials)) {
+        set_error("mrb_scene_create: missing argument");
+        return MRB_E_ARG;
+    }
+    if (set_device(sys)) return MRB_E_CUDA;
+    const uint32_t T = d->triangle_count, V = d->vertex_count;
+    for (uint64_t i = 0; i < uint64_t(T) * 3; i++)
+        if (d->indices[i] >= V) {
+            set_error("triangle %llu references vertex %u >= %u",
+                      (unsigned long long)(i / 3), d->indices[i], V);
+            return MRB_E_ARG;
+        }
+    if (d->base_medium >= d->medium_count || !d->medium_ior) {
+        set_error("base medium %u not among %u media", d->base_medium, d->medium_count);
+        return MRB_E_ARG;
+    }
+    mrb_scene* s = new mrb_scene();
+    s->sys = sys;
+    s->V = V;
+    s->T = T;
+    s->baseMedium = d->base_medium;
+    s->mediumIor.assign(d->medium_ior, d->medium_ior + d->medium_count);
+    // Material groups -> batch ids and per-group ids (HitKey batch/id)
+    std::vector<uint32_t> matKey(d->material_count, 0);
+    std::vector<uint32_t> matType(d->material_count, 0);
+    for (uint32_t m = 0; m < d->material_count; m++) {
+        const mrb_material& mt = d->materials[m];
+        matType[m] = mt.type;
+        switch (mt.type) {
+            case MRB_MAT_LAMBERT:
+                matKey[m] = (kBatchLambert << kIdBits) | uint32_t(s->lambert.size() / 3);
+                s->lambert.insert(s->lambert.end(), mt.albedo, mt.albedo + 3);
+                break;
+            case MRB_MAT_METAL:
+                matKey[m] = (kBatchMetal << kIdBits) | uint32_t(s->metal.size() / 10);
+                s->metal.insert(s->metal.end(), mt.eta, mt.eta + 3);
+                s->metal.insert(s->metal.end(), mt.k, mt.k + 3);
+                s->metal.insert(s->metal.end(), mt.specular, mt.specular + 3);
+                s->metal.push_back(mt.roughness);
+                break;
+            case MRB_MAT_REFRACT:
+                if (mt.medium >= d->medium_count) {
+                    delete s;
+                    set_error("material %u: medium %u out of range", m, mt.medium);
+                    return MRB_E_ARG;
+                }
+                matKey[m] = (kBatchRefract << kIdBits) | uint32_t(s->refract.size() / 3);
+                s->refract.insert(s->refract.end(), mt.albedo, mt.albedo + 3);
+                s->refractMed.push_back(mt.medium);
+                break;
+            case MRB_MAT_LIGHT:
+                break;
+            default:
+                delete s;
+                set_error("material %u: unsupported type %u", m, mt.type);
+                return MRB_E_UNSUPPORTED;
+        }
+    }
+    s->triKey.resize(T);
+    uint32_t maxId = 0;
+    for (uint32_t t = 0; t < T; t++) {
+        uint32_t m = d->tri_material[t];
+        if (m >= d->material_count) {
+            delete s;
+            set_error("triangle %u: material %u out of range", t, m);
+            return MRB_E_ARG;
+        }
+        if (matType[m] == MRB_MAT_LIGHT) {
+            // every triangle of a light surface is one primitive light
+            uint32_t li = static_cast<uint32_t>(s->lightPrim.size());
+            s->lightPrim.push_back(t);
+            s->lightRad.insert(s->lightRad.end(), d->materials[m].radiance,
+                               d->materials[m].radiance + 3);
+            s->triKey[t] = (kBatchLight << kIdBits) | li;
+        } else {
+            s->triKey[t] = matKey[m];
+        }
+        maxId = std::max(maxId, s->triKey[t] & kIdMask);
+    }
+    if (s->lightPrim.size() > kIdMask || s->lambert.size() / 3 > kIdMask) {
+        delete s;
+        set_error("more than 2^24 entries in one batch");
+        return MRB_E_ARG;
+    }
+    s->idBits = bits_for(maxId);
+    build_tbn(*d, s->tbn);
+    std::vector<float> pos(d->positions, d->positions + size_t(V) * 3);
+    std::vector<uint32_t> idx(d->indices, d->indices + size_t(T) * 3);
+    int r = 0;
+    if ((r = upload(s->dPos, pos)) || (r = upload(s->dTbn, s->tbn)) || (r = upload(s->dIdx, idx)) ||
+        (r = upload(s->dKey, s->triKey)) || (r = upload(s->dLambert, s->lambert)) ||
+        (r = upload(s->dMetal, s->metal)) || (r = upload(s->dRefract, s->refract)) ||
+        (r = upload(s->dRefractMed, s->refractMed)) || (r = upload(s->dLightRad, s->lightRad)) ||
+        (r = upload(s->dLightPrim, s->lightPrim)) || (r = upload(s->dMediumIor, s->mediumIor))) {
+        delete s;
+        return r;
+    }
+    if (d->tri_cull) {
+        std::vector<uint8_t> cull(d->tri_cull, d->tri_cull + T);
+        if ((r = upload(s->dCull, cull))) {
+            delete s;
+            return r;
+        }
+    }
+    *out = s;
+    return 0;
+}
+
+void mrb_scene_destroy(mrb_scene* s) { delete s; }
+
+int mrb_scene_counts(const mrb_scene* s, uint32_t* c) {
+    if (!s || !c) return MRB_E_ARG;
+    c[0] = s->T;
+    c[1] = s->V;
+    c[2] = static_cast<uint32_t>(s->lightPrim.size());
+    c[3] = static_cast<uint32_t>(s->lambert.size() / 3);
+    c[4] = static_cast<uint32_t>(s->metal.size() / 10);
+    c[5] = static_cast<uint32_t>(s->refract.size() / 3);
+    c[6] = static_cast<uint32_t>(s->mediumIor.size());
+    c[7] = s->idBits;
+    return 0;
+}
+
+int mrb_scene_export(const mrb_scene* s, float* tbn, uint32_t* key, float* lambert, float* metal,
+                     float* refract, uint32_t* refractMed, float* lightRad, uint32_t* lightPrim) {
+    if (!s) return MRB_E_ARG;
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(tbn, s->tbn);
+    cp(key, s->triKey);
+    cp(lambert, s->lambert);
+    cp(metal, s->metal);
+    cp(refract, s->refract);
+    cp(refractMed, s->refractMed);
+    cp(lightRad, s->lightRad);
+    cp(lightPrim, s->lightPrim);
+    return 0;
+}
+
+int mrb_accel_construct(mrb_scene* s, void* stream) {
+    if (!s) return MRB_E_ARG;
+    if (set_device(s->sys)) return MRB_E_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t n = s->T;
+    if (n == 0) {
+        set_error("LBVH: scene has no triangles");
+        return MRB_E_ARG;
+    }
+    int r = 0;
+    const size_t ni = n > 1 ? n - 1 : 1;
+    if ((r = s->aTriAabb.alloc(size_t(n) * 24)) || (r = s->aExtent.alloc(32)) ||
+        (r = s->aCodes.alloc(size_t(n) * 8)) || (r = s->aSorted.alloc(size_t(n) * 4)) ||
+        (r = s->aLeft.alloc(ni * 4)) || (r = s->aRight.alloc(ni * 4)) ||
+        (r = s->aParent.alloc((2 * size_t(n) - 1) * 4)) || (r = s->aInner.alloc(ni * 24)) ||
+        (r = s->aScratch.alloc(ni * 12)) || (r = s->aRoot.alloc(4)) ||
+        (r = s->aNodes.alloc(ni * sizeof(BvhNode))) || (r = s->aTv0.alloc(size_t(n) * 16)) ||
+        (r = s->aTe0.alloc(size_t(n) * 16)) || (r = s->aTe1.alloc(size_t(n) * 16)))
+        return r;
+    const size_t tb = radix_sort_temp_bytes(n, 8, 0, 63);
+    if ((r = s->aSortTemp.alloc(tb))) return r;
+    if ((r = lbvh_morton(s->dPos.as<float>(), s->dIdx.as<uint32_t>(), n, s->aTriAabb.as<float>(),
+                         s->aExtent.as<float>(), s->aCodes.as<uint64_t>(), nullptr,
+                         s->aExtent.as<float>() + 6, st)))
+        return r;
+    if ((r = radix_sort_pairs<uint64_t>(s->aCodes.as<uint64_t>(), s->aSorted.as<uint32_t>(),
+                                        nullptr, n, 0, 63, false, s->aSortTemp.p, tb, st, true)))
+        return r;
+    uint32_t* scr = s->aScratch.as<uint32_t>();
+    LbvhArrays a{s->aLeft.as<uint32_t>(), s->aRight.as<uint32_t>(), s->aParent.as<uint32_t>(),
+                 s->aInner.as<float>(), scr, scr + ni, scr + 2 * ni, s->aRoot.as<uint32_t>(),
+                 s->aNodes.as<BvhNode>()};
+    if ((r = lbvh_hierarchy(s->aCodes.as<uint64_t>(), s->aSorted.as<uint32_t>(),
+                            s->aTriAabb.as<float>(), n, a, st)))
+        return r;
+    if ((r = lbvh_gather(s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>(),
+                         s->dCull.as<uint8_t>(), s->aSorted.as<uint32_t>(), n, s->aTv0.as<float4>(),
+                         s->aTe0.as<float4>(), s->aTe1.as<float4>(), st)))
+        return r;
+    uint32_t root = 0, err = 0;
+    MRB_CUDA(cudaMemcpyAsync(&root, s->aRoot.p, 4, cudaMemcpyDeviceToHost, st));
+    MRB_CUDA(cudaMemcpyAsync(&err, radix_sort_error_flag(s->aSortTemp.p, n), 4,
+                             cudaMemcpyDeviceToHost, st));
+    MRB_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        set_error("LBVH: radix sort look-back gave up");
+        return MRB_E_DEVICE;
+    }
+    s->rootInner = (n == 1) ? ~0 : static_cast<int>(root - n);
+    s->built = true;
+    return 0;
+}
+
+int mrb_accel_export(const mrb_scene* s, uint64_t* codes, uint32_t* sorted, uint32_t* left,
+                     uint32_t* right, uint32_t* parent, float* inner, uint32_t* root,
+                     float* triAabbs, float* extent) {
+    if (!s || !s->built) {
+        set_error("accelerator not constructed");
+        return MRB_E_STATE;
+    }
+    const size_t n = s->T, ni = n > 1 ? n - 1 : 0;
+    auto cp = [](void* dst, const DBuf& b, size_t bytes) -> int {
+        if (!dst || !bytes) return 0;
+        MRB_CUDA(cudaMemcpy(dst, b.p, bytes, cudaMemcpyDeviceToHost));
+        return 0;
+    };
+    if (cp(codes, s->aCodes, n * 8) || cp(sorted, s->aSorted, n * 4) || cp(left, s->aLeft, ni * 4) ||
+        cp(right, s->aRight, ni * 4) || cp(parent, s->aParent, (2 * n - 1) * 4) ||
+        cp(inner, s->aInner, ni * 24) || cp(root, s->aRoot, 4) || cp(triAabbs, s->aTriAabb, n * 24) ||
+        cp(extent, s->aExtent, 28))
+        return MRB_E_CUDA;
+    return 0;
+}
+
+int mrb_accel_hit(const mrb_scene* s, const float* rayO, const float* rayD, uint32_t n,
+                  uint32_t* key, uint32_t* prim, float* t, float* bary, void* stream) {
+    if (!s || !s->built) {
+        set_error("accelerator not constructed");
+        return MRB_E_STATE;
+    }
+    if (n == 0) return 0;
+    HitOut ho{key, prim, t, reinterpret_cast<float2*>(bary)};
+    static DBuf flag;
+    if (!flag.p) {
+        if (flag.alloc(16)) return MRB_E_OOM;
+        MRB_CUDA(cudaMemset(flag.p, 0, 16));
+    }
+    return trace_closest(s->accel(), reinterpret_cast<const float4*>(rayO),
+                         reinterpret_cast<const float4*>(rayD), nullptr, n, ho,
+                         flag.as<uint32_t>(), static_cast<cudaStream_t>(stream));
+}
+
+int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out) {
+    if (!sys || !scene || !out) return MRB_E_ARG;
+    if (!type || std::strcmp(type, "PathTracer") != 0) {
+        set_error("tracer type '%s' is not supported (PathTracer only)", type ? type : "(null)");
+        return MRB_E_UNSUPPORTED;
+    }
+    if (!scene->built) {
+        set_error("tracer: construct the accelerator first");
+        return MRB_E_STATE;
+    }
+    if (set_device(sys)) return MRB_E_CUDA;
+    mrb_tracer* t = new mrb_tracer();
+    t->sys = sys;
+    t->scene = scene;
+    cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&t->hostCam), sizeof(CameraDev));
+    if (e != cudaSuccess) {
+        delete t;
+        set_error("tracer setup: %s", cudaGetErrorString(e));
+        return MRB_E_CUDA;
+    }
+    if (t->devCam.alloc(sizeof(CameraDev))) {
+        delete t;
+        return MRB_E_OOM;
+    }
+    *out = t;
+    return 0;
+}
+
+void mrb_tracer_destroy(mrb_tracer* t) { delete t; }
+
+int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
+    if (!t || !name) return MRB_E_ARG;
+    std::string k(name);
+    if (k == "Samples") {
+        if (v == 0 || v > 64) {
+            set_error("Samples must be in [1, 64]");
+            return MRB_E_ARG;
+        }
+        t->samples = uint32_t(v);
+    } else if (k == "MaxDepth") {
+        if (v == 0 || v > 255) {
+            set_error("MaxDepth must be in [1, 255]");
+            return MRB_E_ARG;
+        }
+        t->maxDepth = uint32_t(v);
+    } else if (k == "NextEventEstimation") {
+        t->nee = v ? 1 : 0;
+    } else if (k == "RussianRouletteStart") {
+        t->rrStart = uint32_t(v);
+    } else if (k == "DirectLightMIS") {
+        if (v) {
+            set_error("DirectLightMIS=true is not supported by this core");
+            return MRB_E_UNSUPPORTED;
+        }
+        t->mis = 0;
+    } else if (k == "Seed") {
+        t->seed = v;
+    } else if (k == "Frame") {
+        if (t->frameWord.p) {
+            uint32_t f = uint32_t(v);
+            MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f, 4, cudaMemcpyHostToDevice, t->stream));
+            MRB_CUDA(cudaStreamSynchronize(t->stream));
+        } else {
+            set_error("set the resolution before the frame");
+            return MRB_E_STATE;
+        }
+        return 0;
+    } else {
+        set_error("unknown option '%s'", name);
+        return MRB_E_ARG;
+    }
+    t->graphDirty = true;
+    return 0;
+}
+
+int mrb_tracer_set_resolution(mrb_tracer* t, uint32_t w, uint32_t h) {
+    if (!t || !w || !h) return MRB_E_ARG;
+    t->width = w;
+    t->height = h;
+    t->graphDirty = true;
+    return 0;
+}
+
+int mrb_camera_frame(const mrb_camera* c, float* o) {
+    if (!c || !o) return MRB_E_ARG;
+    // GPUCameraPinhole constructor (GPUCameraPinhole.cuh:135-162)
+    H3 pos = h3(c->position[0], c->position[1], c->position[2]);
+    H3 gz = h3(c->gaze[0], c->gaze[1], c->gaze[2]);
+    H3 up = h3(c->up[0], c->up[1], c->up[2]);
+    float nearP = c->near_far[0];
+    float wh = std::tan(c->fov[0] * 0.5f) * nearP;
+    float hh = std::tan(c->fov[1] * 0.5f) * nearP;
+    H3 gd = hsub(gz, pos);
+    H3 right = hnorm(hcross(gd, up));
+    up = hnorm(hcross(right, gd));
+    gd = hnorm(hcross(up, right));
+    H3 bl = hadd(hsub(hsub(pos, hmul(right, wh)), hmul(up, hh)), hmul(gd, nearP));
+    for (int i = 0; i < 3; i++) {
+        o[i] = pos[i];
+        o[3 + i] = bl[i];
+        o[6 + i] = right[i];
+        o[9 + i] = up[i];
+    }
+    o[12] = wh * 2.0f;
+    o[13] = hh * 2.0f;
+    return 0;
+}
+
+int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* c) {
+    if (!t || !c) return MRB_E_ARG;
+    float f[14];
+    mrb_camera_frame(c, f);
+    // the previous upload may still be reading the staging copy
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    CameraDev& cam = *t->hostCam;
+    for (int i = 0; i < 3; i++) {
+        cam.position[i] = f[i];
+        cam.bottomLeft[i] = f[3 + i];
+        cam.right[i] = f[6 + i];
+        cam.up[i] = f[9 + i];
+    }
+    cam.planeSize[0] = f[12];
+    cam.planeSize[1] = f[13];
+    cam.nearFar[0] = c->near_far[0];
+    cam.nearFar[1] = c->near_far[1];
+    // host -> device copy of the frame; graphs read it from device memory
+    MRB_CUDA(cudaMemcpyAsync(t->devCam.p, t->hostCam, sizeof(CameraDev), cudaMemcpyHostToDevice,
+                             t->stream));
+    t->camSet = true;
+    return 0;
+}
+
+int mrb_tracer_generate_work(mrb_tracer* t, uint32_t) {
+    if (!t) return MRB_E_ARG;
+    if (!t->camSet) {
+        set_error("tracer: camera not set");
+        return MRB_E_STATE;
+    }
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_buffers(t);
+    if (r) return r;
+    if ((r = step_camera(t))) return r;
+    t->depth = 0;
+    t->working = true;
+    return 0;
+}
+
+int mrb_tracer_render(mrb_tracer* t) {
+    if (!t) return MRB_E_ARG;
+    if (!t->working) {
+        set_error("Render() before GenerateWork()");
+        return MRB_E_STATE;
+    }
+    if (t->depth >= t->maxDepth) return 0;
+    int r = step_depth(t, t->depth);
+    if (r) return r;
+    t->depth++;
+    return t->depth < t->maxDepth ? 1 : 0;
+}
+
+int mrb_tracer_finalize(mrb_tracer* t) {
+    if (!t || !t->working) return MRB_E_STATE;
+    int r = step_finalize(t);
+    if (r) return r;
+    t->working = false;
+    t->frames++;
+    return check_device_errors(t);
+}
+
+int mrb_tracer_render_frame(mrb_tracer* t) {
+    if (!t) return MRB_E_ARG;
+    if (!t->camSet) {
+        set_error("tracer: camera not set");
+        return MRB_E_STATE;
+    }
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_buffers(t);
+    if (r) return r;
+    if (t->graphDirty || !t->graph) {
+        if (t->graph) {
+            cudaGraphExecDestroy(t->graph);
+            t->graph = nullptr;
+        }
+        // run one frame eagerly first so that one-time setup (kernel
+        // attributes) happens outside the capture, then rewind the frame
+        uint32_t f0 = 0;
+        MRB_CUDA(cudaMemcpyAsync(&f0, t->frameWord.p, 4, cudaMemcpyDeviceToHost, t->stream));
+        MRB_CUDA(cudaStreamSynchronize(t->stream));
+        if ((r = record_frame(t))) return r;
+        MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f0, 4, cudaMemcpyHostToDevice, t->stream));
+        MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+        MRB_CUDA(cudaStreamSynchronize(t->stream));
+        cudaGraph_t g = nullptr;
+        MRB_CUDA(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));
+        r = record_frame(t);
+        cudaError_t e = cudaStreamEndCapture(t->stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) {
+            set_error("graph capture failed: %s", cudaGetErrorString(e));
+            return MRB_E_CUDA;
+        }
+        e = cudaGraphInstantiate(&t->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error("graph instantiate failed: %s", cudaGetErrorString(e));
+            return MRB_E_CUDA;
+        }
+        t->graphDirty = false;
+    }
+    MRB_CUDA(cudaGraphLaunch(t->graph, t->stream));
+    t->frames++;
+    return 0;
+}
+
+int mrb_tracer_get_image(mrb_tracer* t, float* host) {
+    if (!t || !host || !t->image.p) return MRB_E_ARG;
+    MRB_CUDA(cudaMemcpyAsync(host, t->image.p, size_t(t->width) * t->height * 16,
+                             cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    return check_device_errors(t);
+}
+
+int mrb_tracer_get_samples(mrb_tracer* t, float* host) {
+    if (!t || !host || !t->samplesBuf.p) return MRB_E_ARG;
+    const size_t n = size_t(t->width) * t->samples * t->height * t->samples;
+    MRB_CUDA(cudaMemcpyAsync(host, t->samplesBuf.p, n * 16, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    return check_device_errors(t);
+}
+
+int mrb_tracer_reset_image(mrb_tracer* t) {
+    if (!t) return MRB_E_ARG;
+    if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+    return 0;
+}
+
+int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays, uint32_t* frames) {
+    if (!t) return MRB_E_ARG;
+    unsigned long long c = 0;
+    if (t->counters.p) {
+        MRB_CUDA(cudaMemcpyAsync(&c, t->counters.p, 8, cudaMemcpyDeviceToHost, t->stream));
+        MRB_CUDA(cudaStreamSynchronize(t->stream));
+    }
+    if (rays) *rays = c;
+    if (frames) *frames = t->frames;
+    return 0;
+}
+
+void* mrb_tracer_stream(mrb_tracer* t) { return t ? static_cast<void*>(t->stream) : nullptr; }
+
+// ---- kernel-level ----------------------------------------------------------
+int mrb_morton_codes(const float* pos, const uint32_t* idx, uint32_t n, float* triAabb,
+                     float* extent, uint64_t* codes, void* stream) {
+    return lbvh_morton(pos, idx, n, triAabb, extent, codes, nullptr, extent + 6,
+                       static_cast<cudaStream_t>(stream));
+}
+
+size_t mrb_radix_sort_temp_bytes(uint32_t n, int keyBytes, int b, int e) {
+    return radix_sort_temp_bytes(n, keyBytes, b, e);
+}
+
+int mrb_radix_sort_pairs_u64(uint64_t* k, uint32_t* v, uint32_t n, int b, int e, int desc,
+                             void* tmp, size_t tb, void* stream) {
+    if (b < 0 || e > 64 || b > e) {
+        set_error("bit range [%d, %d) invalid for 64-bit keys", b, e);
+        return MRB_E_ARG;
+    }
+    return radix_sort_pairs<uint64_t>(k, v, nullptr, n, b, e, desc != 0, tmp, tb,
+                                      static_cast<cudaStream_t>(stream), false);
+}
+
+int mrb_radix_sort_pairs_u32(uint32_t* k, uint32_t* v, uint32_t n, int b, int e, int desc,
+                             void* tmp, size_t tb, void* stream) {
+    if (b < 0 || e > 32 || b > e) {
+        set_error("bit range [%d, %d) invalid for 32-bit keys", b, e);
+        return MRB_E_ARG;
+    }
+    return radix_sort_pairs<uint32_t>(k, v, nullptr, n, b, e, desc != 0, tmp, tb,
+                                      static_cast<cudaStream_t>(stream), false);
+}
+
+int mrb_lbvh_hierarchy(const uint64_t* codes, const uint32_t* sorted, const float* triAabb,
+                       uint32_t n, uint32_t* left, uint32_t* right, uint32_t* parent, float* inner,
+                       uint32_t* root, uint32_t* scratch, void* nodes, void* stream) {
+    const size_t ni = n > 1 ? n - 1 : 1;
+    LbvhArrays a{left, right, parent, inner, scratch, scratch + ni, scratch + 2 * ni, root,
+                 static_cast<BvhNode*>(nodes)};
+    return lbvh_hierarchy(codes, sorted, triAabb, n, a, static_cast<cudaStream_t>(stream));
+}
+
+size_t mrb_partition_temp_bytes(uint32_t n, uint32_t idBits) {
+    return radix_sort_temp_bytes(n, 4, 0, 3 + int(idBits)) + 256 + 16;
+}
+
+int mrb_partition(const uint32_t* keys, uint32_t n, uint32_t idBits, uint32_t* sortedIds,
+                  uint32_t* sortedDense, uint32_t* pOff, uint32_t* pEnd, uint32_t* nonNull,
+                  void* tmp, size_t tb, void* stream) {
+    if (idBits == 0 || idBits > 24) {
+        set_error("id bits %u out of [1, 24]", idBits);
+        return MRB_E_ARG;
+    }
+    if (tb < mrb_partition_temp_bytes(n, idBits)) {
+        set_error("partition scratch too small");
+        return MRB_E_ARG;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the element count is staged in the first word of the scratch
+    uint32_t* dCount = static_cast<uint32_t*>(tmp);
+    void* sortTmp = static_cast<unsigned char*>(tmp) + 256;
+    size_t sortBytes = tb - 256;
+    MRB_CUDA(cudaMemcpyAsync(dCount, &n, 4, cudaMemcpyHostToDevice, st));
+    PortionTable pt{pOff, pEnd, nonNull};
+    int r;
+    if ((r = dense_keys(keys, dCount, n, idBits, sortedDense, pt, st))) return r;
+    if ((r = radix_sort_pairs<uint32_t>(sortedDense, sortedIds, dCount, n, 0, 3 + int(idBits), true,
+                                        sortTmp, sortBytes, st, true)))
+        return r;
+    if ((r = find_portions(sortedDense, dCount, n, idBits, pt, st))) return r;
+    MRB_CUDA(cudaStreamSynchronize(st));
+    return 0;
+}
+
+}  // extern "C"

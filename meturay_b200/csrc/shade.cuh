@@ -1,0 +1,38 @@
+// Camera, partition-helper, shading and resolve entry points (see shade.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "common.cuh"
+
+namespace mrb {
+
+struct PortionTable {     // per batch: [offset, end) in the sorted order
+    uint32_t* offset;     // 8 entries
+    uint32_t* end;        // 8 entries
+    uint32_t* nonNull;    // count of rays before the NullBatch portion
+};
+
+struct HitIn {
+    const uint32_t* key;
+    const uint32_t* prim;
+    const float* t;
+    const float2* bary;
+};
+
+int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
+                    float4* rayO, float4* rayD, RayAux* aux, float4* samples, uint32_t* count,
+                    cudaStream_t stream);
+int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount, uint32_t idBits,
+               uint32_t* dense, const PortionTable& table, cudaStream_t stream);
+int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t maxCount,
+                  uint32_t idBits, const PortionTable& table, cudaStream_t stream);
+int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayAux* aux,
+          const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull, uint32_t maxCount,
+          float4* samples, const PathOptions& opt, bool gen, float4* outO, float4* outD,
+          RayAux* outAux, uint32_t* outCount, cudaStream_t stream);
+int resolve(const float4* samples, uint32_t width, uint32_t height, uint32_t sp, float4* image,
+            cudaStream_t stream);
+int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream);
+int frame_advance(uint32_t* frame, cudaStream_t stream);
+
+}  // namespace mrb

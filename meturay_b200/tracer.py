@@ -1,0 +1,265 @@
+"""Python mirror of the MRay plugin interfaces on the hot path.
+
+``TracerSystem``   <- TracerSystemI (RayLib/TracerSystemI.h:34-50):
+                      ``generate_scene``, ``generate_tracer``
+``GPUScene``       <- GPUSceneI + the "LBVH" GPUAcceleratorGroupI
+                      (GPUAcceleratorI.h:46-134): ``construct_accelerators``,
+                      ``hit``
+``PathTracer``     <- GPUTracerI "PathTracer" (RayLib/GPUTracerI.h:24-71,
+                      PathTracer.cu:120-326): ``set_options``,
+                      ``generate_work``, ``render``, ``finalize``
+
+Every call goes through the C ABI of libmrb200.so; errors raise
+``MrbError`` carrying the library's status and message, as the reference
+returns ``TracerError`` values.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import Camera, Material, MrbError, SceneDesc, check, lib
+from .scenes import Scene
+
+__all__ = ["TracerSystem", "GPUScene", "PathTracer", "MrbError"]
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def make_camera(cam: dict) -> Camera:
+    c = Camera()
+    c.position[:] = [float(v) for v in cam["position"]]
+    c.gaze[:] = [float(v) for v in cam["gaze"]]
+    c.up[:] = [float(v) for v in cam["up"]]
+    c.near_far[:] = [float(v) for v in cam["near_far"]]
+    c.fov[:] = [float(v) for v in cam["fov"]]
+    return c
+
+
+def camera_frame(cam: dict) -> np.ndarray:
+    """The 14-float pinhole frame the device uses (GPUCameraPinhole.cuh:135-162)."""
+    out = np.zeros(14, np.float32)
+    c = make_camera(cam)
+    check(lib.mrb_camera_frame(C.byref(c), _ptr(out)))
+    return out
+
+
+class TracerSystem:
+    """TracerSystemI: owns the device context and generates scenes and tracers."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.mrb_system_create(int(device), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib.mrb_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def generate_scene(self, scene: Scene) -> "GPUScene":
+        return GPUScene(self, scene)
+
+    def generate_tracer(self, scene: "GPUScene", tracer_type: str = "PathTracer",
+                        options: dict | None = None) -> "PathTracer":
+        t = PathTracer(self, scene, tracer_type)
+        if options:
+            t.set_options(options)
+        return t
+
+
+class GPUScene:
+    """A scene on the device with its "LBVH" accelerator group."""
+
+    def __init__(self, system: TracerSystem, scene: Scene):
+        self.system = system
+        self.scene = scene
+        self._keep = []
+        mats = (Material * max(1, len(scene.materials)))()
+        for i, m in enumerate(scene.materials):
+            mats[i].type = int(m["type"])
+            for key in ("albedo", "eta", "k", "specular", "radiance"):
+                if key in m:
+                    getattr(mats[i], key)[:] = [float(v) for v in m[key]]
+            mats[i].roughness = float(m.get("roughness", 0.0))
+            mats[i].medium = int(m.get("medium", 0))
+        arrs = {
+            "positions": np.ascontiguousarray(scene.positions, np.float32),
+            "normals": np.ascontiguousarray(scene.normals, np.float32),
+            "uvs": np.ascontiguousarray(scene.uvs, np.float32) if scene.uvs is not None else None,
+            "indices": np.ascontiguousarray(scene.indices, np.uint32),
+            "tri_material": np.ascontiguousarray(scene.tri_material, np.uint32),
+            "tri_cull": (np.ascontiguousarray(scene.tri_cull, np.uint8)
+                         if scene.tri_cull is not None else None),
+            "medium_ior": np.ascontiguousarray(scene.medium_ior, np.float32),
+        }
+        d = SceneDesc()
+        d.vertex_count = arrs["positions"].shape[0]
+        d.triangle_count = arrs["indices"].shape[0]
+        for k in ("positions", "normals", "uvs", "indices", "tri_material", "tri_cull",
+                  "medium_ior"):
+            setattr(d, k, _ptr(arrs[k]))
+        d.material_count = len(scene.materials)
+        d.materials = C.cast(mats, C.POINTER(Material))
+        d.medium_count = arrs["medium_ior"].shape[0]
+        d.base_medium = scene.base_medium
+        h = C.c_void_p()
+        check(lib.mrb_scene_create(system._h, C.byref(d), C.byref(h)))
+        self._h = h
+        self.counts = np.zeros(8, np.uint32)
+        check(lib.mrb_scene_counts(self._h, _ptr(self.counts)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mrb_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.counts[0])
+
+    @property
+    def id_bits(self) -> int:
+        return int(self.counts[7])
+
+    def construct_accelerators(self, stream: int | None = None):
+        """GPUAcceleratorGroupI::ConstructAccelerators for the LBVH group."""
+        check(lib.mrb_accel_construct(self._h, stream))
+
+    def export(self) -> dict:
+        """Host copies of the device scene arrays, as the hot path consumes them."""
+        c = self.counts
+        out = {
+            "tbn": np.zeros((int(c[1]), 4), np.float32),
+            "tri_key": np.zeros(int(c[0]), np.uint32),
+            "lambert": np.zeros((int(c[3]), 3), np.float32),
+            "metal": np.zeros((int(c[4]), 10), np.float32),
+            "refract": np.zeros((int(c[5]), 3), np.float32),
+            "refract_medium": np.zeros(int(c[5]), np.uint32),
+            "light_radiance": np.zeros((int(c[2]), 3), np.float32),
+            "light_prim": np.zeros(int(c[2]), np.uint32),
+        }
+        check(lib.mrb_scene_export(self._h, *[_ptr(out[k]) for k in (
+            "tbn", "tri_key", "lambert", "metal", "refract", "refract_medium",
+            "light_radiance", "light_prim")]))
+        return out
+
+    def export_accel(self) -> dict:
+        n = self.triangle_count
+        ni = max(n - 1, 0)
+        out = {"codes": np.zeros(n, np.uint64), "sorted_idx": np.zeros(n, np.uint32),
+               "left": np.zeros(ni, np.uint32), "right": np.zeros(ni, np.uint32),
+               "parent": np.zeros(2 * n - 1, np.uint32), "inner": np.zeros((ni, 6), np.float32),
+               "root": np.zeros(1, np.uint32), "tri_aabbs": np.zeros((n, 6), np.float32),
+               "extent": np.zeros(7, np.float32)}
+        check(lib.mrb_accel_export(self._h, *[_ptr(out[k]) for k in (
+            "codes", "sorted_idx", "left", "right", "parent", "inner", "root", "tri_aabbs",
+            "extent")]))
+        return out
+
+    def hit(self, ray_o_ptr: int, ray_d_ptr: int, n: int, key_ptr: int, prim_ptr: int,
+            t_ptr: int, bary_ptr: int, stream: int | None = None):
+        """GPUAcceleratorGroupI::Hit on device buffers (raw pointers)."""
+        check(lib.mrb_accel_hit(self._h, ray_o_ptr, ray_d_ptr, int(n), key_ptr, prim_ptr,
+                                t_ptr, bary_ptr, stream))
+
+
+class PathTracer:
+    """GPUTracerI "PathTracer": wavefront path tracing with NEE and Russian roulette."""
+
+    OPTION_KEYS = ("Samples", "MaxDepth", "NextEventEstimation", "RussianRouletteStart",
+                   "DirectLightMIS", "Seed", "Frame")
+
+    def __init__(self, system: TracerSystem, scene: GPUScene, tracer_type: str = "PathTracer"):
+        self.system = system
+        self.gscene = scene
+        h = C.c_void_p()
+        check(lib.mrb_tracer_create(system._h, scene._h, tracer_type.encode(), C.byref(h)))
+        self._h = h
+        self.samples = 1
+        self.width = self.height = 0
+        sc = scene.scene
+        self.set_resolution(sc.width, sc.height)
+        self.set_camera(sc.camera)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mrb_tracer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_options(self, opts: dict):
+        for k, v in opts.items():
+            if k not in self.OPTION_KEYS:
+                raise MrbError(-1, f"unknown option '{k}'")
+            if k == "Samples":
+                self.samples = int(v)
+            check(lib.mrb_tracer_set_option(self._h, k.encode(), int(v)))
+
+    def set_resolution(self, w: int, h: int):
+        check(lib.mrb_tracer_set_resolution(self._h, int(w), int(h)))
+        self.width, self.height = int(w), int(h)
+
+    def set_camera(self, cam: dict):
+        c = make_camera(cam)
+        check(lib.mrb_tracer_set_camera(self._h, C.byref(c)))
+
+    def generate_work(self, camera_index: int = 0):
+        check(lib.mrb_tracer_generate_work(self._h, int(camera_index)))
+
+    def render(self) -> bool:
+        return check(lib.mrb_tracer_render(self._h)) == 1
+
+    def finalize(self):
+        check(lib.mrb_tracer_finalize(self._h))
+
+    def render_frame(self):
+        """GenerateWork + Render* + Finalize replayed from one CUDA graph."""
+        check(lib.mrb_tracer_render_frame(self._h))
+
+    def image(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        check(lib.mrb_tracer_get_image(self._h, _ptr(out)))
+        return out
+
+    def image_into(self, host_ptr: int):
+        check(lib.mrb_tracer_get_image(self._h, host_ptr))
+
+    def sample_radiance(self) -> np.ndarray:
+        s = self.samples
+        out = np.zeros((self.height * s, self.width * s, 4), np.float32)
+        check(lib.mrb_tracer_get_samples(self._h, _ptr(out)))
+        return out
+
+    def reset_image(self):
+        check(lib.mrb_tracer_reset_image(self._h))
+
+    def stats(self) -> tuple[int, int]:
+        r = C.c_uint64()
+        f = C.c_uint32()
+        check(lib.mrb_tracer_stats(self._h, C.byref(r), C.byref(f)))
+        return int(r.value), int(f.value)
+
+    @property
+    def stream(self) -> int:
+        return lib.mrb_tracer_stream(self._h) or 0

@@ -1,0 +1,1323 @@
+// CPU oracle for the meturay_b200 wavefront path-tracing path.
+//
+// TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and
+// bench.py's cpu_baseline / reference leg as the checker; never linked into
+// or called by the product.
+//
+// Restates MRay (yalcinerbora/meturay) Source/TracerCUDA + Source/RayLib.
+// Every function names the reference file:line it follows.  Build flags:
+// -O2 -ffp-contract=off (no implicit FMA), so FP32 results follow the same
+// operation order as the CUDA kernels built with -fmad=false.
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// ------------------------------------------------------------------------
+// Portable math.  sin/cos: Cody-Waite reduction by pi/2 split in three
+// parts, then Taylor polynomials on [-pi/4, pi/4] (coefficients are the
+// float-rounded 1/n! values).  acos: asin Taylor series on [0, 1/2] with the
+// half-angle identity above 1/2.  The device copy uses the same steps.
+// ------------------------------------------------------------------------
+constexpr float kTwoOverPi = 0x1.45f306p-1f;
+constexpr float kPio2Hi = 0x1.92p+0f;
+constexpr float kPio2Mid = 0x1.fb4p-12f;
+constexpr float kPio2Lo = 0x1.4442d2p-24f;
+constexpr float kPiF = 0x1.921fb6p+1f;      // float(pi)  (Constants.h:99)
+constexpr float kPio2F = 0x1.921fb6p+0f;
+constexpr float kInvPiF = 0x1.45f306p-2f;   // float(1/pi) (Constants.h:101)
+
+inline float sin_poly(float r) {
+    float r2 = r * r;
+    float p = -0x1.ae6456p-26f;
+    p = p * r2 + 0x1.71de3ap-19f;
+    p = p * r2 + -0x1.a01a02p-13f;
+    p = p * r2 + 0x1.111112p-7f;
+    p = p * r2 + -0x1.555556p-3f;
+    return r + (r * r2) * p;
+}
+inline float cos_poly(float r) {
+    float r2 = r * r;
+    float p = 0x1.1eed8ep-29f;
+    p = p * r2 + -0x1.27e4fcp-22f;
+    p = p * r2 + 0x1.a01a02p-16f;
+    p = p * r2 + -0x1.6c16c2p-10f;
+    p = p * r2 + 0x1.555556p-5f;
+    p = p * r2 + -0.5f;
+    return 1.0f + r2 * p;
+}
+inline void pm_sincos(float x, float& s, float& c) {
+    float kf = std::rint(x * kTwoOverPi);
+    int k = static_cast<int>(kf);
+    float r = x - kf * kPio2Hi;
+    r = r - kf * kPio2Mid;
+    r = r - kf * kPio2Lo;
+    float sr = sin_poly(r), cr = cos_poly(r);
+    switch (k & 3) {
+        case 0: s = sr; c = cr; break;
+        case 1: s = cr; c = -sr; break;
+        case 2: s = -sr; c = -cr; break;
+        default: s = -cr; c = sr; break;
+    }
+}
+inline float asin_poly(float z) {  // z in [0, 0.5]
+    float z2 = z * z;
+    float p = 0x1.df3bd4p-8f;
+    p = p * z2 + 0x1.12ef3cp-7f;
+    p = p * z2 + 0x1.3fde50p-7f;
+    p = p * z2 + 0x1.7a8788p-7f;
+    p = p * z2 + 0x1.c9999ap-7f;
+    p = p * z2 + 0x1.1c4ec4p-6f;
+    p = p * z2 + 0x1.6e8ba2p-6f;
+    p = p * z2 + 0x1.f1c71cp-6f;
+    p = p * z2 + 0x1.6db6dcp-5f;
+    p = p * z2 + 0x1.333334p-4f;
+    p = p * z2 + 0x1.555556p-3f;
+    return z + (z * z2) * p;
+}
+inline float pm_acos(float x) {
+    float ax = std::fabs(x);
+    if (ax <= 0.5f) {
+        float a = asin_poly(ax);
+        a = (x < 0.0f) ? -a : a;
+        return kPio2F - a;
+    }
+    float z = std::sqrt((1.0f - ax) * 0.5f);
+    float a = 2.0f * asin_poly(z);
+    return (x > 0.0f) ? a : (kPiF - a);
+}
+
+// Math traits: FP32 uses the portable functions, FP64 the C library.
+template <class T> struct M;
+template <> struct M<float> {
+    static float sqrt(float x) { return std::sqrt(x); }
+    static void sincos(float x, float& s, float& c) { pm_sincos(x, s, c); }
+    static float sin(float x) { float s, c; pm_sincos(x, s, c); return s; }
+    static float acos(float x) { return pm_acos(x); }
+    static constexpr float Pi = kPiF;
+    static constexpr float InvPi = kInvPiF;
+    static constexpr float SmallEps = 1.0e-7f;
+    static constexpr float Eps = 1.0e-5f;
+    static constexpr float LargeEps = 1.0e-4f;
+    static constexpr float Max = 3.40282347e+38f;
+};
+template <> struct M<double> {
+    static double sqrt(double x) { return std::sqrt(x); }
+    static void sincos(double x, double& s, double& c) { s = std::sin(x); c = std::cos(x); }
+    static double sin(double x) { return std::sin(x); }
+    static double acos(double x) { return std::acos(x); }
+    static constexpr double Pi = 3.1415926535897932384626433;
+    static constexpr double InvPi = 1.0 / 3.1415926535897932384626433;
+    static constexpr double SmallEps = 1.0e-7;
+    static constexpr double Eps = 1.0e-5;
+    static constexpr double LargeEps = 1.0e-4;
+    static constexpr double Max = 3.40282347e+38;
+};
+
+// ------------------------------------------------------------------------
+// Vectors and quaternions (RayLib/Vector.hpp, RayLib/Quaternion.hpp).
+// ------------------------------------------------------------------------
+template <class T> struct V3 {
+    T x, y, z;
+    V3() : x(0), y(0), z(0) {}
+    V3(T a, T b, T c) : x(a), y(b), z(c) {}
+    T operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+template <class T> inline V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> inline V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> inline V3<T> operator-(V3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <class T> inline V3<T> operator*(V3<T> a, V3<T> b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <class T> inline V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> inline V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> inline V3<T> operator/(V3<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class T> inline bool operator!=(V3<T> a, V3<T> b) { return a.x != b.x || a.y != b.y || a.z != b.z; }
+template <class T> inline T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> inline V3<T> cross(V3<T> a, V3<T> b) {  // Vector.hpp:867-873
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T> inline V3<T> normalize(V3<T> v) {  // Vector.hpp:519-530
+    T inv = T(1) / M<T>::sqrt(dot(v, v));
+    return {v.x * inv, v.y * inv, v.z * inv};
+}
+template <class T> inline V3<T> vmax(V3<T> v, T s) { return {std::fmax(v.x, s), std::fmax(v.y, s), std::fmax(v.z, s)}; }
+template <class T> inline V3<T> vsqrt(V3<T> v) { return {M<T>::sqrt(v.x), M<T>::sqrt(v.y), M<T>::sqrt(v.z)}; }
+
+template <class T> struct Q4 { T w, x, y, z; };
+template <class T> inline Q4<T> qmul(Q4<T> a, Q4<T> b) {  // Quaternion.hpp:76-89
+    return {a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z,
+            a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+            a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+            a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w};
+}
+template <class T> inline Q4<T> qconj(Q4<T> q) { return {q.w, -q.x, -q.y, -q.z}; }
+template <class T> inline T qdot(Q4<T> a, Q4<T> b) { return a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> inline Q4<T> qnormalize(Q4<T> q) {
+    T inv = T(1) / M<T>::sqrt(qdot(q, q));
+    return {q.w * inv, q.x * inv, q.y * inv, q.z * inv};
+}
+template <class T> inline V3<T> qrotate(Q4<T> q, V3<T> v) {  // Quaternion.hpp:229-238
+    Q4<T> qi = qconj(q);
+    Q4<T> vq = {T(0), v.x, v.y, v.z};
+    Q4<T> r = qmul(q, qmul(vq, qi));
+    return {r.x, r.y, r.z};
+}
+template <class T> inline V3<T> to_space(V3<T> v, Q4<T> q) { return qrotate(qconj(q), v); }  // GPUSurface.h:45
+template <class T> inline V3<T> to_tangent(V3<T> v, Q4<T> q) { return qrotate(q, v); }      // GPUSurface.h:38
+
+template <class T> inline Q4<T> slerp(Q4<T> s, Q4<T> e, T t) {  // Quaternion.hpp:258-283
+    T cosT = qdot(s, e);
+    T cosF = (cosT >= 0) ? cosT : (-cosT);
+    T s0, s1;
+    if (cosF < (T(1) - M<T>::Eps)) {
+        T angle = M<T>::acos(cosF);
+        T sa = M<T>::sin(angle);
+        s0 = M<T>::sin(angle * (T(1) - t)) / sa;
+        s1 = M<T>::sin(angle * t) / sa;
+    } else {
+        s0 = (T(1) - t);
+        s1 = t;
+    }
+    s1 = (cosT >= 0) ? s1 : (-s1);
+    return {s.w * s0 + e.w * s1, s.x * s0 + e.x * s1, s.y * s0 + e.y * s1, s.z * s0 + e.z * s1};
+}
+template <class T> inline Q4<T> bary_slerp(Q4<T> q0, Q4<T> q1, Q4<T> q2, T a, T b) {  // Quaternion.hpp:285-318
+    T c = (T(1) - a - b);
+    if (std::fabs(a + b) < M<T>::Eps) return q2;
+    T ab = a / (a + b);
+    Q4<T> qAB = slerp(q1, q0, ab);
+    return slerp(qAB, q2, c);
+}
+
+// Ray::Nudge (RayLib/Ray.hpp:503-556), RTG-I chapter 6.
+inline V3<float> nudge(V3<float> p, V3<float> dir) {
+    const float ORIGIN = 1.0f / 32.0f, FLOAT_SCALE = 1.0f / 65536.0f, INT_SCALE = 256.0f;
+    float pc[3] = {p.x, p.y, p.z}, dc[3] = {dir.x, dir.y, dir.z}, out[3];
+    for (int i = 0; i < 3; i++) {
+        int32_t ofi = static_cast<int32_t>(INT_SCALE * dc[i]);
+        int32_t pi;
+        std::memcpy(&pi, &pc[i], 4);
+        pi += (pc[i] < 0) ? -ofi : ofi;
+        float pI;
+        std::memcpy(&pI, &pi, 4);
+        out[i] = (std::fabs(pc[i]) < ORIGIN) ? (pc[i] + FLOAT_SCALE * dc[i]) : pI;
+    }
+    return {out[0], out[1], out[2]};
+}
+inline V3<double> nudge(V3<double> p, V3<double> dir) {
+    const double ORIGIN = 1.0 / 32.0, FLOAT_SCALE = 1.0 / 65536.0, INT_SCALE = 256.0;
+    double pc[3] = {p.x, p.y, p.z}, dc[3] = {dir.x, dir.y, dir.z}, out[3];
+    for (int i = 0; i < 3; i++) {
+        int64_t ofi = static_cast<int64_t>(INT_SCALE * dc[i]);
+        int64_t pi;
+        std::memcpy(&pi, &pc[i], 8);
+        pi += (pc[i] < 0) ? -ofi : ofi;
+        double pI;
+        std::memcpy(&pI, &pi, 8);
+        out[i] = (std::fabs(pc[i]) < ORIGIN) ? (pc[i] + FLOAT_SCALE * dc[i]) : pI;
+    }
+    return {out[0], out[1], out[2]};
+}
+
+// ------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11).  Counter = {sample, frame, tag, block}.
+// ------------------------------------------------------------------------
+inline void philox(const uint32_t c_in[4], const uint32_t k_in[2], uint32_t out[4]) {
+    uint32_t c0 = c_in[0], c1 = c_in[1], c2 = c_in[2], c3 = c_in[3];
+    uint32_t k0 = k_in[0], k1 = k_in[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = uint64_t(0xD2511F53u) * c0;
+        uint64_t p1 = uint64_t(0xCD9E8D57u) * c2;
+        uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0);
+        uint32_t hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+constexpr uint32_t kTagCamera = 0x10000u;
+struct Rng4 {
+    float u[4];
+};
+inline Rng4 rng_block(uint32_t sample, uint32_t frame, uint32_t tag, uint32_t block,
+                      uint32_t seed_lo, uint32_t seed_hi) {
+    uint32_t c[4] = {sample, frame, tag, block}, k[2] = {seed_lo, seed_hi}, o[4];
+    philox(c, k, o);
+    Rng4 r;
+    for (int i = 0; i < 4; i++) r.u[i] = static_cast<float>(o[i] >> 8) * 0x1p-24f;
+    return r;
+}
+
+// ------------------------------------------------------------------------
+// Morton codes (RayLib/MortonCode.h:45-56,150-158; LinearBVH.hpp:118-166,
+// 398-414).
+// ------------------------------------------------------------------------
+inline uint64_t expand3d(uint32_t val) {
+    uint64_t x = val;
+    x &= 0x1fffff;
+    x = (x | x << 32) & 0x001f00000000ffffull;
+    x = (x | x << 16) & 0x001f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+inline uint64_t morton3d(uint32_t x, uint32_t y, uint32_t z) {
+    return (expand3d(x) << 0) | (expand3d(y) << 1) | (expand3d(z) << 2);
+}
+inline float morton_delta(const float ext[6]) {  // LinearBVH.hpp:398-414
+    const double res = 1.0f / static_cast<double>(1 << 21);
+    double dx = static_cast<double>(ext[3] - ext[0]) * res;
+    double dy = static_cast<double>(ext[4] - ext[1]) * res;
+    double dz = static_cast<double>(ext[5] - ext[2]) * res;
+    return static_cast<float>(std::max({dx, dy, dz}));
+}
+
+template <class K>
+void radix_sort(K* keys, uint32_t* vals, uint32_t n, int begin, int end, bool desc) {
+    std::vector<K> k2(n);
+    std::vector<uint32_t> v2(n);
+    K* ka = keys; K* kb = k2.data();
+    uint32_t* va = vals; uint32_t* vb = v2.data();
+    int passes = 0;
+    for (int bit = begin; bit < end; bit += 8) {
+        int nb = std::min(8, end - bit);
+        uint32_t mask = (1u << nb) - 1u;
+        uint32_t cnt[257] = {0};
+        for (uint32_t i = 0; i < n; i++) {
+            uint32_t d = uint32_t(ka[i] >> bit) & mask;
+            if (desc) d = mask - d;
+            cnt[d + 1]++;
+        }
+        for (int d = 0; d < 256; d++) cnt[d + 1] += cnt[d];
+        for (uint32_t i = 0; i < n; i++) {
+            uint32_t d = uint32_t(ka[i] >> bit) & mask;
+            if (desc) d = mask - d;
+            uint32_t p = cnt[d]++;
+            kb[p] = ka[i];
+            vb[p] = va[i];
+        }
+        std::swap(ka, kb);
+        std::swap(va, vb);
+        passes++;
+    }
+    if (passes & 1) {
+        std::memcpy(keys, ka, sizeof(K) * n);
+        std::memcpy(vals, va, sizeof(uint32_t) * n);
+    }
+}
+
+// Delta between adjacent sorted codes (LinearBVH.hpp:30-39), extended with
+// the index-augmented tie break for equal codes (Karras 2012, sec. 4): the
+// reference rejects duplicate codes, this keeps unique-code trees identical.
+inline uint32_t lbvh_delta(const uint64_t* c, uint32_t i) {
+    uint64_t d = c[i] ^ c[i + 1];
+    if (d != 0) return uint32_t(__builtin_clzll(d));
+    uint32_t di = i ^ (i + 1);
+    return 64u + uint32_t(__builtin_clz(di));
+}
+
+// ------------------------------------------------------------------------
+// Scene access helpers
+// ------------------------------------------------------------------------
+constexpr uint32_t kBatchNull = 0, kBatchLambert = 1, kBatchMetal = 2, kBatchRefract = 3,
+                   kBatchLight = 4;
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+
+template <class T> inline V3<T> vpos(const oracle_scene* s, uint32_t v) {
+    return {T(s->pos[3 * v + 0]), T(s->pos[3 * v + 1]), T(s->pos[3 * v + 2])};
+}
+template <class T> inline Q4<T> vtbn(const oracle_scene* s, uint32_t v) {
+    const float* q = s->tbn + 4 * v;
+    return {T(q[0]), T(q[1]), T(q[2]), T(q[3])};
+}
+
+// ------------------------------------------------------------------------
+// Ray/triangle (RayLib/Ray.hpp:143-184) and ray/box tests.
+// ------------------------------------------------------------------------
+template <class T>
+inline bool intersect_tri(V3<T> o, V3<T> d, V3<T> t0, V3<T> e0, V3<T> e1, bool cull,
+                          T& t, T& b0, T& b1, T* vout = nullptr) {
+    V3<T> p = cross(d, e1);
+    T det = dot(e0, p);
+    if ((cull && (det < M<T>::SmallEps)) || (std::fabs(det) < M<T>::SmallEps)) return false;
+    T invDet = T(1) / det;
+    V3<T> tv = o - t0;
+    T u = dot(tv, p) * invDet;
+    if (u < 0 || u > 1) return false;
+    V3<T> q = cross(tv, e0);
+    T v = dot(d, q) * invDet;
+    if ((v < 0) || (v + u) > 1) return false;
+    t = dot(e1, q) * invDet;
+    if (t <= M<T>::SmallEps) return false;
+    // bary reordered to (c, a, b): hit struct keeps (1-u-v, u)
+    b0 = T(1) - u - v;
+    b1 = u;
+    if (vout) *vout = v;
+    return true;
+}
+
+// Slab test with precomputed o*invD; fmaf keeps FP32 bit-identical to the
+// device kernel.  Returns entry distance via tn.
+inline bool box_hit(const float lo[3], const float hi[3], const float inv[3],
+                    const float ooi[3], float tmin, float tmax, float& tn) {
+    float tl[3], th[3];
+    for (int i = 0; i < 3; i++) {
+        float a = std::fmaf(lo[i], inv[i], -ooi[i]);
+        float b = std::fmaf(hi[i], inv[i], -ooi[i]);
+        tl[i] = std::fmin(a, b);
+        th[i] = std::fmax(a, b);
+    }
+    tn = std::fmax(std::fmax(tl[0], tl[1]), std::fmax(tl[2], tmin));
+    float tf = std::fmin(std::fmin(th[0], th[1]), std::fmin(th[2], tmax));
+    return tn <= tf;
+}
+inline bool box_hit(const float lo[3], const float hi[3], const double inv[3],
+                    const double ooi[3], double tmin, double tmax, double& tn) {
+    double tl[3], th[3];
+    for (int i = 0; i < 3; i++) {
+        double a = std::fma(double(lo[i]), inv[i], -ooi[i]);
+        double b = std::fma(double(hi[i]), inv[i], -ooi[i]);
+        tl[i] = std::fmin(a, b);
+        th[i] = std::fmax(a, b);
+    }
+    tn = std::fmax(std::fmax(tl[0], tl[1]), std::fmax(tl[2], tmin));
+    double tf = std::fmin(std::fmin(th[0], th[1]), std::fmin(th[2], tmax));
+    return tn <= tf;
+}
+inline float safe_dir(float d) { return (std::fabs(d) > 1e-20f) ? d : std::copysign(1e-20f, d); }
+inline double safe_dir(double d) { return (std::fabs(d) > 1e-20) ? d : std::copysign(1e-20, d); }
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// LBVH container
+// ------------------------------------------------------------------------
+struct oracle_bvh {
+    uint32_t n = 0;
+    uint32_t root = 0;
+    std::vector<uint64_t> codes;
+    std::vector<uint32_t> sorted_idx;
+    std::vector<float> leaf_aabbs;   // by original triangle index
+    std::vector<uint32_t> left, right, parent;
+    std::vector<float> inner;        // (n-1)*6
+    std::vector<float> e0, e1, v0;   // per original triangle (precomputed edges)
+};
+
+namespace {
+
+template <class T> struct Hit {
+    uint32_t key = 0;
+    uint32_t prim = kInvalid;
+    T t = 0;
+    T b0 = 0, b1 = 0;
+};
+
+template <class T>
+inline void tri_test(const oracle_scene* s, const oracle_bvh* b, uint32_t tri, V3<T> o, V3<T> d,
+                     T tmin, T& tmax, Hit<T>& h) {
+    V3<T> p0 = {T(b->v0[3 * tri]), T(b->v0[3 * tri + 1]), T(b->v0[3 * tri + 2])};
+    V3<T> e0 = {T(b->e0[3 * tri]), T(b->e0[3 * tri + 1]), T(b->e0[3 * tri + 2])};
+    V3<T> e1 = {T(b->e1[3 * tri]), T(b->e1[3 * tri + 1]), T(b->e1[3 * tri + 2])};
+    bool cull = s->tri_cull ? (s->tri_cull[tri] != 0) : false;
+    T t, b0, b1;
+    if (intersect_tri(o, d, p0, e0, e1, cull, t, b0, b1)) {
+        // AcceptHit (GPUAcceleratorCommonKC.cuh:35-78): t in [tMin, tMax)
+        if (t >= tmin && t < tmax) {
+            tmax = t;
+            h.t = t;
+            h.b0 = b0;
+            h.b1 = b1;
+            h.prim = tri;
+            h.key = s->tri_key[tri];
+        }
+    }
+}
+
+// Closest hit over the LBVH: both child boxes are tested at each inner node
+// and the nearer one is entered first (ties go to the left child); the
+// farther one is pushed.  The device kernel walks the same tree the same way.
+template <class T>
+Hit<T> trace_one(const oracle_scene* s, const oracle_bvh* b, V3<T> o, V3<T> d, T tmin, T tmax) {
+    Hit<T> h;
+    const uint32_t n = b->n;
+    if (n == 0) return h;
+    if (n == 1) {
+        tri_test(s, b, b->sorted_idx[0], o, d, tmin, tmax, h);
+        return h;
+    }
+    T inv[3] = {T(1) / safe_dir(d.x), T(1) / safe_dir(d.y), T(1) / safe_dir(d.z)};
+    T ooi[3] = {o.x * inv[0], o.y * inv[1], o.z * inv[2]};
+    uint32_t stack[128];
+    int sp = 0;
+    uint32_t node = b->root;  // global node index (>= n: inner)
+    for (;;) {
+        if (node >= n) {
+            uint32_t j = node - n;
+            uint32_t c[2] = {b->left[j], b->right[j]};
+            bool hit[2];
+            T tn[2];
+            for (int k = 0; k < 2; k++) {
+                const float* box = (c[k] < n) ? &b->leaf_aabbs[6 * b->sorted_idx[c[k]]]
+                                              : &b->inner[6 * (c[k] - n)];
+                hit[k] = box_hit(box, box + 3, inv, ooi, tmin, tmax, tn[k]);
+            }
+            if (hit[0] && hit[1]) {
+                bool swap = tn[1] < tn[0];
+                stack[sp++] = swap ? c[0] : c[1];
+                node = swap ? c[1] : c[0];
+                continue;
+            } else if (hit[0]) {
+                node = c[0];
+                continue;
+            } else if (hit[1]) {
+                node = c[1];
+                continue;
+            }
+        } else {
+            tri_test(s, b, b->sorted_idx[node], o, d, tmin, tmax, h);
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    return h;
+}
+
+template <class T>
+Hit<T> trace_linear_one(const oracle_scene* s, const oracle_bvh* b, V3<T> o, V3<T> d, T tmin,
+                        T tmax) {
+    Hit<T> h;
+    for (uint32_t i = 0; i < s->tri_count; i++) tri_test(s, b, i, o, d, tmin, tmax, h);
+    return h;
+}
+
+template <class F>
+void parallel_for(uint32_t n, uint32_t threads, F f) {
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    threads = std::min<uint32_t>(threads, std::max(1u, n));
+    if (threads <= 1) {
+        f(0u, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    std::atomic<uint32_t> next{0};
+    const uint32_t chunk = 256;
+    for (uint32_t t = 0; t < threads; t++) {
+        th.emplace_back([&]() {
+            for (;;) {
+                uint32_t b = next.fetch_add(chunk);
+                if (b >= n) break;
+                f(b, std::min(n, b + chunk));
+            }
+        });
+    }
+    for (auto& t : th) t.join();
+}
+
+// ------------------------------------------------------------------------
+// Path tracer (PathTracerKC.cuh:335-649, material KC files,
+// GPULightSamplerUniform.cuh:95-135, GPULightPrimitive.cuh:139-170,
+// GPUPrimitiveTriangle.h:65-115,624-700, GenerationKernels.cuh:26-108,
+// GPUCameraPinhole.cuh:209-243).
+// ------------------------------------------------------------------------
+enum RayType : uint8_t { NEE_RAY = 0, SPECULAR_PATH_RAY = 1, PATH_RAY = 2, CAMERA_RAY = 3 };
+
+template <class T> struct Aux {
+    V3<T> rf;
+    uint32_t sample;
+    uint32_t endpoint;
+    uint32_t medium;
+    uint32_t depth;
+    RayType type;
+    T prevPDF;
+};
+template <class T> struct PRay {
+    V3<T> o, d;
+    T tmin, tmax;
+    Aux<T> aux;
+};
+template <class T> struct Surface {
+    V3<T> pos;
+    Q4<T> w2t;
+    V3<T> geo;
+    bool back;
+};
+
+template <class T>
+Surface<T> gen_surface(const oracle_scene* s, uint32_t prim, T ha, T hb, V3<T> rayDir) {
+    bool twoSided = s->tri_cull ? (s->tri_cull[prim] == 0) : true;
+    T a = ha, b = hb;
+    T c = T(1) - a - b;
+    uint32_t i0 = s->idx[3 * prim], i1 = s->idx[3 * prim + 1], i2 = s->idx[3 * prim + 2];
+    Q4<T> tbn = bary_slerp(vtbn<T>(s, i0), vtbn<T>(s, i1), vtbn<T>(s, i2), a, b);
+    tbn = qnormalize(tbn);
+    V3<T> p0 = vpos<T>(s, i0), p1 = vpos<T>(s, i1), p2 = vpos<T>(s, i2);
+    Surface<T> sf;
+    sf.pos = (p0 * a + p1 * b) + p2 * c;
+    V3<T> g = normalize(cross(p1 - p0, p2 - p0));
+    g = normalize(g);
+    sf.w2t = tbn;
+    sf.back = twoSided && (dot(g, rayDir) > T(0));
+    if (sf.back) {
+        g = -g;
+        sf.w2t = qmul(Q4<T>{T(0), T(1), T(0), T(0)}, sf.w2t);
+    }
+    sf.geo = g;
+    return sf;
+}
+
+template <class T> struct Ctx {
+    const oracle_scene* s;
+    const oracle_bvh* b;
+    const oracle_options* o;
+    T* out;  // sample radiance
+};
+
+template <class T> inline void accumulate(Ctx<T>& c, uint32_t sample, V3<T> v) {
+    c.out[3 * sample + 0] += v.x;
+    c.out[3 * sample + 1] += v.y;
+    c.out[3 * sample + 2] += v.z;
+}
+
+// BxDF sample result
+template <class T> struct BSample {
+    V3<T> dir, pos;
+    V3<T> refl;
+    T pdf;
+    uint32_t medium;
+};
+
+template <class T>
+inline V3<T> hemi_cosine(T xi0, T xi1, T& pdf) {  // HemiDistribution.h:10-30
+    T coeff = T(2) * M<T>::Pi * xi1;
+    T sn, cs;
+    M<T>::sincos(coeff, sn, cs);
+    V3<T> d;
+    d.x = M<T>::sqrt(xi0) * cs;
+    d.y = M<T>::sqrt(xi0) * sn;
+    d.z = M<T>::sqrt(std::fmax(T(0), (T(1) - d.x * d.x - d.y * d.y)));
+    pdf = d.z * M<T>::InvPi;
+    return d;
+}
+
+// TracerFunctions.cuh:8-30
+template <class T> inline T fresnel_dielectric(T cosIn, T iorIn, T iorOut) {
+    T sinIn = M<T>::sqrt(std::fmax(T(0), T(1) - cosIn * cosIn));
+    T sinOut = iorIn / iorOut * sinIn;
+    if (sinOut >= T(1)) return T(1);
+    T cosOut = M<T>::sqrt(std::fmax(T(0), T(1) - sinOut * sinOut));
+    T par = ((iorOut * cosIn - iorIn * cosOut) / (iorOut * cosIn + iorIn * cosOut));
+    par = par * par;
+    T perp = ((iorIn * cosIn - iorOut * cosOut) / (iorIn * cosIn + iorOut * cosOut));
+    perp = perp * perp;
+    return (par + perp) * T(0.5);
+}
+// TracerFunctions.cuh:33-75 (per component)
+template <class T> inline V3<T> fresnel_conductor(T cosIn, V3<T> eta, V3<T> k) {
+    T cosInSqr = cosIn * cosIn;
+    T sinInSqr = std::fmax(T(0), T(1) - cosInSqr);
+    T sinInSqr2 = sinInSqr * sinInSqr;
+    T sinInSqr4 = sinInSqr2 * sinInSqr2;
+    V3<T> etaSqr = eta * eta;
+    V3<T> kSqr = k * k;
+    V3<T> diff = etaSqr - kSqr - V3<T>(sinInSqr, sinInSqr, sinInSqr);
+    V3<T> a2b2 = diff * diff;
+    a2b2 = a2b2 + T(4) * etaSqr * kSqr;
+    a2b2 = vsqrt(vmax(a2b2, T(0)));
+    V3<T> a = T(0.5) * (a2b2 + diff);
+    a = vsqrt(vmax(a, T(0)));
+    V3<T> perpT1 = a2b2 + V3<T>(cosInSqr, cosInSqr, cosInSqr);
+    V3<T> perpT2 = a * (T(2) * cosIn);
+    V3<T> perp = V3<T>((perpT1.x - perpT2.x) / (perpT1.x + perpT2.x),
+                       (perpT1.y - perpT2.y) / (perpT1.y + perpT2.y),
+                       (perpT1.z - perpT2.z) / (perpT1.z + perpT2.z));
+    V3<T> parT1 = a2b2 * cosInSqr + V3<T>(sinInSqr4, sinInSqr4, sinInSqr4);
+    V3<T> parT2 = perpT2 * sinInSqr2;
+    V3<T> num = perp * (parT1 - parT2);
+    V3<T> den = parT1 + parT2;
+    V3<T> par = V3<T>(num.x / den.x, num.y / den.y, num.z / den.z);
+    return (par + perp) * T(0.5);
+}
+template <class T> inline T dggx(T NdH, T alpha) {  // TracerFunctions.cuh:77-86
+    T a2 = alpha * alpha;
+    T den = NdH * NdH * (a2 - T(1)) + T(1);
+    den = den * den;
+    den *= M<T>::Pi;
+    return a2 / den;
+}
+template <class T> inline T lambda_smith(V3<T> v, T alpha) {  // :88-97
+    V3<T> s = v * v;
+    T a2 = alpha * alpha;
+    T inner = a2 * (s.x + s.y) / s.z;
+    T l = M<T>::sqrt(T(1) + inner) - T(1);
+    return l * T(0.5);
+}
+template <class T> inline T g_smith_single(V3<T> v, T alpha) { return T(1) / (T(1) + lambda_smith(v, alpha)); }
+template <class T> inline T g_smith_corr(V3<T> o, V3<T> i, T alpha) {
+    return T(1) / (lambda_smith(o, alpha) + lambda_smith(i, alpha) + T(1));
+}
+template <class T> inline T vndf_pdf(V3<T> V, V3<T> H, T alpha) {  // :181-190
+    T VdH = std::fmax(T(0), dot(H, V));
+    T NdH = std::fmax(T(0), H.z);
+    T NdV = std::fmax(T(0), V.z);
+    T D = dggx(NdH, alpha);
+    T G = g_smith_single(V, alpha);
+    return (NdV == T(0)) ? T(0) : (VdH * D * G / NdV);
+}
+template <class T> inline V3<T> vndf_sample(T& pdf, V3<T> V, T alpha, T xi0, T xi1) {  // :192-251
+    T a = alpha;
+    V3<T> VH = normalize(V3<T>(a * V.x, a * V.y, V.z));
+    T lensq = VH.x * VH.x + VH.y * VH.y;
+    V3<T> T1 = (lensq > 0) ? V3<T>(-VH.y, VH.x, T(0)) / M<T>::sqrt(lensq) : V3<T>(1, 0, 0);
+    V3<T> T2 = cross(VH, T1);
+    T r = M<T>::sqrt(xi0);
+    T phi = T(2) * M<T>::Pi * xi1;
+    T sn, cs;
+    M<T>::sincos(phi, sn, cs);
+    T t1 = r * cs;
+    T t2 = r * sn;
+    T s = T(0.5) * (T(1) + VH.z);
+    t2 = (T(1) - s) * M<T>::sqrt(T(1) - t1 * t1) + s * t2;
+    T val = T(1) - t1 * t1 - t2 * t2;
+    V3<T> NH = t1 * T1 + t2 * T2 + M<T>::sqrt(std::fmax(T(0), val)) * VH;
+    V3<T> NM = V3<T>(a * NH.x, a * NH.y, std::fmax(T(0), NH.z));
+    T len2 = dot(NM, NM);
+    if (len2 < M<T>::Eps) NM = V3<T>(0, 0, 1);
+    else NM = NM * (T(1) / M<T>::sqrt(len2));
+    pdf = vndf_pdf(V, NM, alpha);
+    return NM;
+}
+
+template <class T> struct MetalP {
+    V3<T> eta, k, spec;
+    T rough;
+};
+template <class T> inline MetalP<T> metal_params(const float* p) {
+    return {V3<T>(p[0], p[1], p[2]), V3<T>(p[3], p[4], p[5]), V3<T>(p[6], p[7], p[8]), T(p[9])};
+}
+
+// MetalGlassMaterialsKC.cuh:26-146
+template <class T>
+BSample<T> metal_sample(const MetalP<T>& m, V3<T> wi, const Surface<T>& sf, T xi0, T xi1,
+                        uint32_t medium) {
+    T alpha = m.rough * m.rough;
+    V3<T> V = to_tangent(wi, sf.w2t);
+    BSample<T> out;
+    T pdf;
+    V3<T> H = vndf_sample(pdf, V, alpha, xi0, xi1);
+    T VdH = std::fmax(T(0), dot(V, H));
+    V3<T> L = T(2) * VdH * H - V;
+    pdf = (VdH == T(0)) ? T(0) : pdf / (T(4) * VdH);
+    T LdH = std::fmax(T(0), dot(L, H));
+    T NdH = std::fmax(T(0), H.z);
+    T NdV = std::fmax(T(0), V.z);
+    V3<T> F = fresnel_conductor(VdH, m.eta, m.k);
+    F = F * m.spec;
+    T D = dggx(NdH, alpha);
+    T G = g_smith_corr(V, L, alpha);
+    G = (LdH == T(0)) ? T(0) : G;
+    G = (VdH == T(0)) ? T(0) : G;
+    V3<T> st = D * F * G * T(0.25) / NdV;
+    st = (NdV == T(0)) ? V3<T>() : st;
+    if (std::isinf(D) || std::isnan(D)) {
+        if (m.rough == T(0)) L = T(2) * V.z * V3<T>(0, 0, 1) - V;
+        st = G * F;
+        T gs = g_smith_single(V, alpha);
+        if (gs != T(0)) st = st / gs;
+        else st = V3<T>();
+        pdf = T(1);
+    }
+    out.dir = to_space(L, sf.w2t);
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = st;
+    out.pdf = pdf;
+    out.medium = medium;
+    return out;
+}
+// MetalGlassMaterialsKC.cuh:174-214
+template <class T>
+V3<T> metal_eval(const MetalP<T>& m, V3<T> wo, V3<T> wi, const Surface<T>& sf) {
+    T alpha = m.rough * m.rough;
+    V3<T> L = to_tangent(wo, sf.w2t);
+    V3<T> V = to_tangent(wi, sf.w2t);
+    V3<T> H = normalize(L + V);
+    T LdH = std::fmax(T(0), dot(L, H));
+    T VdH = std::fmax(T(0), dot(V, H));
+    T NdH = std::fmax(T(0), H.z);
+    T NdV = std::fmax(T(0), V.z);
+    T D = dggx(NdH, alpha);
+    D = (std::isnan(D) || std::isinf(D)) ? T(0) : D;
+    T G = g_smith_corr(V, L, alpha);
+    G = (LdH == T(0)) ? T(0) : G;
+    G = (VdH == T(0)) ? T(0) : G;
+    V3<T> F = fresnel_conductor(VdH, m.eta, m.k);
+    F = F * m.spec;
+    V3<T> st = D * F * G * T(0.25) / NdV;
+    return (NdV == T(0)) ? V3<T>() : st;
+}
+// LambertMaterialKC.cuh:14-103
+template <class T>
+BSample<T> lambert_sample(V3<T> albedo, const Surface<T>& sf, T xi0, T xi1, uint32_t medium) {
+    BSample<T> out;
+    T pdf;
+    V3<T> d = hemi_cosine(xi0, xi1, pdf);
+    d = normalize(d);
+    T nDotL = std::fmax(d.z, T(0));
+    out.dir = to_space(d, sf.w2t);
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = nDotL * albedo * M<T>::InvPi;
+    out.pdf = pdf;
+    out.medium = medium;
+    return out;
+}
+template <class T> V3<T> lambert_eval(V3<T> albedo, V3<T> wo, const Surface<T>& sf) {
+    V3<T> n = to_space(V3<T>(0, 0, 1), sf.w2t);
+    T nDotL = std::fmax(dot(n, wo), T(0));
+    return nDotL * albedo * M<T>::InvPi;
+}
+// SimpleMaterialsKC.cuh:172-286 and Ray::Reflect/Refract (Ray.hpp:302-356)
+template <class T>
+BSample<T> refract_sample(V3<T> albedo, uint32_t matMedium, const oracle_scene* s, V3<T> wi,
+                          const Surface<T>& sf, uint32_t curMedium, T xi) {
+    BSample<T> out;
+    T iIOR = T(s->medium_ior[matMedium]);
+    T dIOR = T(s->medium_ior[s->base_medium]);
+    V3<T> n = to_space(V3<T>(0, 0, 1), sf.w2t);
+    bool entering = !sf.back;
+    T from = T(s->medium_ior[curMedium]);
+    T to = entering ? iIOR : dIOR;
+    T f = fresnel_dielectric(std::fabs(dot(wi, n)), from, to);
+    if (xi < f) {
+        out.dir = T(2) * dot(wi, n) * n - wi;
+        out.pos = nudge(sf.pos, sf.geo);
+        out.pdf = f;
+        out.medium = curMedium;
+        out.refl = f * albedo;
+        return out;
+    }
+    out.medium = entering ? matMedium : s->base_medium;
+    out.pdf = T(1) - f;
+    T ratio = from / to;
+    T cosIn = dot(n, wi);
+    T sinInSqr = std::fmax(T(0), T(1) - cosIn * cosIn);
+    T sinOutSqr = ratio * ratio * sinInSqr;
+    T cosOut = M<T>::sqrt(std::fmax(T(0), T(1) - sinOutSqr));
+    if (sinOutSqr >= T(1)) {
+        out.pdf = T(0);
+        out.refl = V3<T>();
+        out.dir = wi;
+        out.pos = sf.pos;
+        return out;
+    }
+    out.dir = ratio * (-wi) + (ratio * cosIn - cosOut) * n;
+    out.pos = nudge(sf.pos, -sf.geo);
+    out.refl = albedo * T(1) * (T(1) - f);
+    return out;
+}
+
+template <class T>
+void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t batch,
+               uint32_t id, bool gen, std::vector<PRay<T>>& next) {
+    const oracle_scene* s = c.s;
+    const Aux<T>& aux = r.aux;
+    if (aux.type == NEE_RAY) return;
+    if (!gen) return;  // outputs of the last iteration are never traced
+    Surface<T> sf = gen_surface(s, prim, ha, hb, r.d);
+    V3<T> wi = -normalize(r.d);
+    V3<T> rf = aux.rf;  // vacuum / sigmaT == 0 transmittance is exactly 1
+    bool specular;
+    if (batch == kBatchLambert) specular = false;
+    else if (batch == kBatchMetal) specular = (T(1) - T(s->metal_params[10 * id + 9])) >= T(0.99f);
+    else specular = true;
+    uint32_t sampleIdx = aux.sample;
+    Rng4 ra = rng_block(sampleIdx, c.o->frame, aux.depth, 0, c.o->seed_lo, c.o->seed_hi);
+    Rng4 rb = rng_block(sampleIdx, c.o->frame, aux.depth, 1, c.o->seed_lo, c.o->seed_hi);
+
+    // ---- NEE (PathTracerKC.cuh:505-583) ----
+    if (c.o->nee && !specular && s->light_count > 0) {
+        uint32_t lc = s->light_count;
+        float r1 = ra.u[0] * static_cast<float>(lc);
+        uint32_t li = static_cast<uint32_t>(r1);
+        if (li == lc) li--;
+        uint32_t lp = s->light_prim[li];
+        // PrimSamplePos (GPUPrimitiveTriangle.h:65-115)
+        T sx = M<T>::sqrt(T(ra.u[1]));
+        T r2 = T(ra.u[2]);
+        T la = T(1) - sx;
+        T lb = (T(1) - r2) * sx;
+        T lcw = sx * r2;
+        uint32_t i0 = s->idx[3 * lp], i1 = s->idx[3 * lp + 1], i2 = s->idx[3 * lp + 2];
+        V3<T> p0 = vpos<T>(s, i0), p1 = vpos<T>(s, i1), p2 = vpos<T>(s, i2);
+        T area = M<T>::sqrt(dot(cross(p1 - p0, p2 - p0), cross(p1 - p0, p2 - p0))) * T(0.5);
+        T lpdf = T(1) / area;
+        Q4<T> q = bary_slerp(qnormalize(vtbn<T>(s, i0)), qnormalize(vtbn<T>(s, i1)),
+                             qnormalize(vtbn<T>(s, i2)), la, lb);
+        V3<T> ln = to_space(V3<T>(0, 0, 1), q);
+        V3<T> lpos = (p0 * la + p1 * lb) + p2 * lcw;
+        ln = normalize(ln);
+        V3<T> ldir = lpos - sf.pos;
+        T d2 = dot(ldir, ldir);
+        T dist = M<T>::sqrt(d2);
+        ldir = ldir * (T(1) / dist);
+        T nDotL = std::fabs(dot(ln, -ldir));
+        lpdf *= d2 / nDotL;
+        lpdf *= (T(1) / static_cast<T>(lc));
+        V3<T> refl;
+        if (batch == kBatchLambert) {
+            const float* al = s->lambert_albedo + 3 * id;
+            refl = lambert_eval(V3<T>(al[0], al[1], al[2]), ldir, sf);
+        } else {
+            refl = metal_eval(metal_params<T>(s->metal_params + 10 * id), ldir, wi, sf);
+        }
+        V3<T> nrf = rf * refl;
+        nrf = (lpdf == T(0)) ? V3<T>() : (nrf / lpdf);
+        if (nrf != V3<T>()) {
+            PRay<T> o;
+            o.o = nudge(sf.pos, sf.geo);
+            o.d = ldir;
+            o.tmin = T(0);
+            o.tmax = M<T>::Max;
+            o.aux = aux;
+            o.aux.rf = nrf;
+            o.aux.endpoint = li;
+            o.aux.type = NEE_RAY;
+            o.aux.prevPDF = std::numeric_limits<T>::quiet_NaN();
+            next.push_back(o);
+        }
+    }
+    // ---- BxDF sample (PathTracerKC.cuh:585-648) ----
+    BSample<T> bs;
+    if (batch == kBatchLambert) {
+        const float* al = s->lambert_albedo + 3 * id;
+        bs = lambert_sample(V3<T>(al[0], al[1], al[2]), sf, T(rb.u[0]), T(rb.u[1]), aux.medium);
+    } else if (batch == kBatchMetal) {
+        bs = metal_sample(metal_params<T>(s->metal_params + 10 * id), wi, sf, T(rb.u[0]),
+                          T(rb.u[1]), aux.medium);
+    } else {
+        const float* al = s->refract_albedo + 3 * id;
+        bs = refract_sample(V3<T>(al[0], al[1], al[2]), s->refract_medium[id], s, wi, sf,
+                            aux.medium, T(rb.u[0]));
+    }
+    V3<T> prf = rf * bs.refl;
+    prf = (bs.pdf == T(0)) ? V3<T>() : (prf / bs.pdf);
+    T avg = dot(prf, V3<T>(T(0.333f), T(0.333f), T(0.333f)));
+    bool term = false;
+    if (!specular && aux.depth > c.o->rr_start) {
+        // TracerFunctions.cuh:320-331
+        T prob = std::fmin(std::fmax(avg, T(0.005f)), T(1));
+        if (T(ra.u[3]) >= prob) term = true;
+        else prf = prf * (T(1) / prob);
+    }
+    if ((!term || specular) && prf != V3<T>()) {
+        PRay<T> o;
+        o.o = bs.pos;
+        o.d = bs.dir;
+        o.tmin = T(0);
+        o.tmax = M<T>::Max;
+        o.aux = aux;
+        o.aux.medium = bs.medium;
+        o.aux.rf = prf;
+        o.aux.type = specular ? SPECULAR_PATH_RAY : PATH_RAY;
+        o.aux.prevPDF = bs.pdf;
+        o.aux.depth = aux.depth + 1;
+        next.push_back(o);
+    }
+}
+
+// PathTracerKC.cuh:335-426 (MIS off)
+template <class T>
+void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx) {
+    const Aux<T>& aux = r.aux;
+    bool camera = aux.type == CAMERA_RAY;
+    bool specPath = aux.type == SPECULAR_PATH_RAY;
+    bool neeOn = c.o->nee && aux.type == NEE_RAY;
+    bool pathNeeOff = (!c.o->nee) && (aux.type == PATH_RAY || aux.type == SPECULAR_PATH_RAY);
+    bool correct = neeOn && (aux.endpoint == lightIdx);
+    if (pathNeeOff || correct || camera || specPath) {
+        const float* e = c.s->light_radiance + 3 * lightIdx;
+        V3<T> total = V3<T>(T(e[0]), T(e[1]), T(e[2])) * aux.rf;
+        accumulate(c, aux.sample, total);
+    }
+}
+
+template <class T>
+uint64_t render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera* cam,
+                const oracle_options* opt, T* out) {
+    const uint32_t sp = opt->samples;
+    const uint32_t SW = opt->width * sp, SH = opt->height * sp;
+    uint32_t rowB = opt->row_begin, rowE = opt->row_end;
+    if (rowE == 0 || rowE > SH) rowE = SH;
+    if (rowB > rowE) rowB = rowE;
+    const uint32_t first = rowB * SW;
+    const uint32_t count = (rowE - rowB) * SW;
+    std::atomic<uint64_t> rays{0};
+    const float* P = cam->position;
+    parallel_for(count, opt->threads, [&](uint32_t b0, uint32_t b1) {
+        Ctx<T> c{s, b, opt, out};
+        uint64_t local = 0;
+        std::vector<PRay<T>> cur, next;
+        for (uint32_t k = b0; k < b1; k++) {
+            uint32_t sid = first + k;
+            out[3 * sid] = out[3 * sid + 1] = out[3 * sid + 2] = T(0);
+            // Camera ray (GPUCameraPinhole.cuh:209-243; GenerationKernels.cuh:48-75)
+            uint32_t sx = sid % SW, sy = sid / SW;
+            Rng4 rc = rng_block(sid, opt->frame, kTagCamera, 0, opt->seed_lo, opt->seed_hi);
+            float dx = cam->plane_size[0] / static_cast<float>(SW);
+            float dy = cam->plane_size[1] / static_cast<float>(SH);
+            float sdx = static_cast<float>(sx) * dx;
+            float sdy = static_cast<float>(sy) * dy;
+            sdx += rc.u[0] * dx;
+            sdy += rc.u[1] * dy;
+            V3<float> sp3;
+            for (int i = 0; i < 3; i++) {
+                float v = cam->bottom_left[i] + ((sdx * cam->right[i]) + (sdy * cam->up[i]));
+                if (i == 0) sp3.x = v; else if (i == 1) sp3.y = v; else sp3.z = v;
+            }
+            V3<float> dirf = normalize(sp3 - V3<float>(P[0], P[1], P[2]));
+            PRay<T> r;
+            r.o = V3<T>(T(P[0]), T(P[1]), T(P[2]));
+            r.d = V3<T>(T(dirf.x), T(dirf.y), T(dirf.z));
+            r.tmin = T(cam->near_far[0]);
+            r.tmax = T(cam->near_far[1]);
+            r.aux = Aux<T>{V3<T>(1, 1, 1), sid, kInvalid, s->base_medium, 0, CAMERA_RAY,
+                           std::numeric_limits<T>::quiet_NaN()};
+            cur.clear();
+            cur.push_back(r);
+            for (uint32_t it = 0; it < opt->max_depth && !cur.empty(); it++) {
+                next.clear();
+                bool gen = (it + 1) < opt->max_depth;
+                for (const PRay<T>& ray : cur) {
+                    local++;
+                    Hit<T> h = trace_one<T>(s, b, ray.o, ray.d, ray.tmin, ray.tmax);
+                    if (h.prim == kInvalid) continue;
+                    uint32_t batch = h.key >> 24, id = h.key & 0xFFFFFFu;
+                    if (batch == kBatchNull) continue;
+                    if (batch == kBatchLight) boundary_work(c, ray, id);
+                    else path_work(c, ray, h.prim, h.b0, h.b1, batch, id, gen, next);
+                }
+                std::swap(cur, next);
+            }
+        }
+        rays.fetch_add(local);
+    });
+    return rays.load();
+}
+
+}  // namespace
+
+// ========================================================================
+// C ABI
+// ========================================================================
+extern "C" {
+
+void oracle_sincosf(float x, float* s, float* c) { pm_sincos(x, *s, *c); }
+float oracle_acosf(float x) { return pm_acos(x); }
+void oracle_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    philox(ctr, key, out);
+}
+uint64_t oracle_morton3d(uint32_t x, uint32_t y, uint32_t z) { return morton3d(x, y, z); }
+
+void oracle_morton_codes(const float* pos, const uint32_t* idx, uint32_t n, float* aabbs,
+                         float* extent, float* delta, uint64_t* codes) {
+    // Triangle AABBs (Triangle::BoundingBox) and the extent reduce
+    // (LinearBVH.hpp:444-457).
+    float ext[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t t = 0; t < n; t++) {
+        float* a = aabbs + 6 * t;
+        for (int i = 0; i < 3; i++) {
+            float v0 = pos[3 * idx[3 * t + 0] + i];
+            float v1 = pos[3 * idx[3 * t + 1] + i];
+            float v2 = pos[3 * idx[3 * t + 2] + i];
+            a[i] = std::fmin(std::fmin(v0, v1), v2);
+            a[3 + i] = std::fmax(std::fmax(v0, v1), v2);
+            ext[i] = std::fmin(ext[i], a[i]);
+            ext[3 + i] = std::fmax(ext[3 + i], a[3 + i]);
+        }
+    }
+    std::memcpy(extent, ext, sizeof(ext));
+    float md = morton_delta(ext);
+    *delta = md;
+    // KCGenMortonCodes (LinearBVH.hpp:118-166)
+    for (uint32_t t = 0; t < n; t++) {
+        const float* a = aabbs + 6 * t;
+        uint32_t g[3];
+        for (int i = 0; i < 3; i++) {
+            float span = a[3 + i] - a[i];
+            float center = a[i] + span * 0.5f;
+            float rel = center - ext[i];
+            g[i] = static_cast<uint32_t>(std::floor(rel / md));
+        }
+        codes[t] = morton3d(g[0], g[1], g[2]);
+    }
+}
+
+void oracle_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint32_t n, int b, int e, int desc) {
+    radix_sort<uint64_t>(keys, vals, n, b, e, desc != 0);
+}
+void oracle_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t n, int b, int e, int desc) {
+    radix_sort<uint32_t>(keys, vals, n, b, e, desc != 0);
+}
+
+int oracle_lbvh_build(const uint64_t* codes, const uint32_t* sorted_idx, const float* leaf_aabbs,
+                      uint32_t n, uint32_t* left, uint32_t* right, uint32_t* parent,
+                      float* inner, uint32_t* root) {
+    if (n == 0) return 2;
+    for (uint32_t i = 0; i < 2 * n - 1; i++) parent[i] = kInvalid;
+    if (n == 1) {
+        *root = 0;
+        return 0;
+    }
+    const uint32_t ni = n - 1;
+    std::vector<uint32_t> r0(ni, kInvalid), r1(ni, kInvalid);
+    std::vector<uint32_t> work;
+    work.reserve(n);
+    // ChooseParentAndUpdate (LinearBVH.hpp:41-100)
+    auto choose = [&](uint32_t lo, uint32_t hi, uint32_t global) {
+        bool leftEdge = (lo == 0), rightEdge = (hi == n - 1);
+        uint32_t ld = leftEdge ? 0 : lbvh_delta(codes, lo - 1);
+        uint32_t rd = rightEdge ? 0 : lbvh_delta(codes, hi);
+        uint32_t p;
+        if (rd > ld) {
+            p = hi;
+            left[p] = global;
+            r0[p] = lo;
+        } else {
+            p = lo - 1;
+            right[p] = global;
+            r1[p] = hi;
+        }
+        parent[global] = n + p;
+        if (r0[p] != kInvalid && r1[p] != kInvalid) work.push_back(p);
+    };
+    for (uint32_t i = 0; i < n; i++) choose(i, i, i);
+    *root = kInvalid;
+    for (size_t w = 0; w < work.size(); w++) {
+        uint32_t j = work[w];
+        if (r0[j] == 0 && r1[j] == n - 1) {
+            *root = n + j;
+            parent[n + j] = kInvalid;
+        } else {
+            choose(r0[j], r1[j], n + j);
+        }
+    }
+    // BottomUpAABB* (LinearBVH.hpp:290-396): post-order union.
+    std::vector<uint32_t> st;
+    std::vector<uint8_t> done(ni, 0);
+    st.push_back(*root - n);
+    auto box = [&](uint32_t g) -> const float* {
+        return g < n ? leaf_aabbs + 6 * sorted_idx[g] : inner + 6 * (g - n);
+    };
+    while (!st.empty()) {
+        uint32_t j = st.back();
+        bool ready = true;
+        uint32_t ch[2] = {left[j], right[j]};
+        for (uint32_t c : ch)
+            if (c >= n && !done[c - n]) {
+                st.push_back(c - n);
+                ready = false;
+            }
+        if (!ready) continue;
+        st.pop_back();
+        const float* a = box(ch[0]);
+        const float* b = box(ch[1]);
+        float* o = inner + 6 * j;
+        for (int i = 0; i < 3; i++) {
+            o[i] = std::fmin(a[i], b[i]);
+            o[3 + i] = std::fmax(a[3 + i], b[3 + i]);
+        }
+        done[j] = 1;
+    }
+    uint32_t dups = 0;
+    for (uint32_t i = 0; i + 1 < n; i++) dups += (codes[i] == codes[i + 1]);
+    return dups ? 1 : 0;
+}
+
+uint32_t oracle_partition(const uint32_t* keys, uint32_t n, uint32_t bb, uint32_t ib,
+                          uint32_t* skeys, uint32_t* sids, uint32_t* pb, uint32_t* po,
+                          uint32_t* pc) {
+    // SortKeys (RayMemory.cu:187-228): stable descending on id bits, then on
+    // batch bits; equivalent to one stable descending sort of the dense key.
+    std::vector<uint32_t> dk(n);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t batch = (keys[i] >> 24) & ((1u << bb) - 1u);
+        uint32_t id = keys[i] & ((ib >= 32) ? 0xFFFFFFFFu : ((1u << ib) - 1u));
+        dk[i] = (batch << ib) | id;
+        sids[i] = i;
+    }
+    radix_sort<uint32_t>(dk.data(), sids, n, 0, int(bb + ib), true);
+    for (uint32_t i = 0; i < n; i++) skeys[i] = keys[sids[i]];
+    // Partition (RayMemory.cu:230-312): batch boundaries -> portions in
+    // ascending batch order (std::set<ArrayPortion>, ArrayPortion.h:35-44).
+    std::vector<std::pair<uint32_t, std::pair<uint32_t, uint32_t>>> p;
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t batch = skeys[i] >> 24;
+        if (i == 0 || batch != (skeys[i - 1] >> 24)) p.push_back({batch, {i, 0}});
+        p.back().second.second++;
+    }
+    std::sort(p.begin(), p.end());
+    for (size_t i = 0; i < p.size(); i++) {
+        pb[i] = p[i].first;
+        po[i] = p[i].second.first;
+        pc[i] = p[i].second.second;
+    }
+    return uint32_t(p.size());
+}
+
+oracle_bvh* oracle_bvh_create(const oracle_scene* s, int* status) {
+    oracle_bvh* b = new oracle_bvh();
+    uint32_t n = s->tri_count;
+    b->n = n;
+    b->leaf_aabbs.resize(size_t(n) * 6);
+    b->codes.resize(n);
+    b->sorted_idx.resize(n);
+    b->v0.resize(size_t(n) * 3);
+    b->e0.resize(size_t(n) * 3);
+    b->e1.resize(size_t(n) * 3);
+    for (uint32_t t = 0; t < n; t++) {
+        for (int i = 0; i < 3; i++) {
+            float p0 = s->pos[3 * s->idx[3 * t] + i];
+            float p1 = s->pos[3 * s->idx[3 * t + 1] + i];
+            float p2 = s->pos[3 * s->idx[3 * t + 2] + i];
+            b->v0[3 * t + i] = p0;
+            b->e0[3 * t + i] = p1 - p0;
+            b->e1[3 * t + i] = p2 - p0;
+        }
+    }
+    float ext[6], delta;
+    std::vector<uint64_t> codes(n);
+    oracle_morton_codes(s->pos, s->idx, n, b->leaf_aabbs.data(), ext, &delta, codes.data());
+    for (uint32_t i = 0; i < n; i++) b->sorted_idx[i] = i;
+    b->codes = codes;
+    radix_sort<uint64_t>(b->codes.data(), b->sorted_idx.data(), n, 0, 64, false);
+    if (n > 0) {
+        b->left.resize(n > 1 ? n - 1 : 0);
+        b->right.resize(n > 1 ? n - 1 : 0);
+        b->parent.resize(2 * size_t(n) - 1);
+        b->inner.resize(n > 1 ? size_t(n - 1) * 6 : 0);
+        int st = oracle_lbvh_build(b->codes.data(), b->sorted_idx.data(), b->leaf_aabbs.data(), n,
+                                   b->left.data(), b->right.data(), b->parent.data(),
+                                   b->inner.data(), &b->root);
+        if (status) *status = st;
+    } else if (status) {
+        *status = 0;
+    }
+    return b;
+}
+void oracle_bvh_destroy(oracle_bvh* b) { delete b; }
+uint32_t oracle_bvh_root(const oracle_bvh* b) { return b->root; }
+
+static void write_hits(const Hit<float>& h, uint32_t i, uint32_t* k, uint32_t* p, float* t,
+                       float* bary) {
+    k[i] = h.prim == kInvalid ? 0u : h.key;
+    p[i] = h.prim;
+    t[i] = h.t;
+    bary[2 * i] = h.b0;
+    bary[2 * i + 1] = h.b1;
+}
+
+void oracle_trace(const oracle_scene* s, const oracle_bvh* b, const float* rays, uint32_t n,
+                  uint32_t* k, uint32_t* p, float* t, float* bary, uint32_t threads) {
+    parallel_for(n, threads, [&](uint32_t b0, uint32_t b1) {
+        for (uint32_t i = b0; i < b1; i++) {
+            const float* r = rays + 8 * i;
+            Hit<float> h = trace_one<float>(s, b, V3<float>(r[0], r[1], r[2]),
+                                            V3<float>(r[4], r[5], r[6]), r[3], r[7]);
+            write_hits(h, i, k, p, t, bary);
+        }
+    });
+}
+void oracle_trace_linear(const oracle_scene* s, const float* rays, uint32_t n, uint32_t* k,
+                         uint32_t* p, float* t, float* bary, uint32_t threads) {
+    int st = 0;
+    oracle_bvh* b = oracle_bvh_create(s, &st);  // only the precomputed edges are used
+    parallel_for(n, threads, [&](uint32_t b0, uint32_t b1) {
+        for (uint32_t i = b0; i < b1; i++) {
+            const float* r = rays + 8 * i;
+            Hit<float> h = trace_linear_one<float>(s, b, V3<float>(r[0], r[1], r[2]),
+                                                   V3<float>(r[4], r[5], r[6]), r[3], r[7]);
+            write_hits(h, i, k, p, t, bary);
+        }
+    });
+    delete b;
+}
+
+uint64_t oracle_render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera* cam,
+                       const oracle_options* opt, float* out) {
+    return render<float>(s, b, cam, opt, out);
+}
+uint64_t oracle_render_f64(const oracle_scene* s, const oracle_bvh* b, const oracle_camera* cam,
+                           const oracle_options* opt, double* out) {
+    return render<double>(s, b, cam, opt, out);
+}
+
+void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi, const float* w2t,
+                        const float* geo, const float* pos, uint32_t back, float from_ior,
+                        float to_ior, const float* xi, float* out_dir, float* out_pos,
+                        float* out_refl, float* out_pdf) {
+    Surface<float> sf;
+    sf.pos = V3<float>(pos[0], pos[1], pos[2]);
+    sf.w2t = Q4<float>{w2t[0], w2t[1], w2t[2], w2t[3]};
+    sf.geo = V3<float>(geo[0], geo[1], geo[2]);
+    sf.back = back != 0;
+    V3<float> w(wi[0], wi[1], wi[2]);
+    BSample<float> bs;
+    if (type == kBatchLambert) {
+        bs = lambert_sample(V3<float>(params[0], params[1], params[2]), sf, xi[0], xi[1], 0);
+    } else if (type == kBatchMetal) {
+        bs = metal_sample(metal_params<float>(params), w, sf, xi[0], xi[1], 0);
+    } else {
+        float ior[2] = {from_ior, to_ior};
+        uint32_t med[1] = {1};
+        oracle_scene tmp{};
+        tmp.medium_ior = ior;
+        tmp.medium_count = 2;
+        tmp.base_medium = 0;
+        tmp.refract_medium = med;
+        // entering: from = ior[cur=0], to = ior[1]; exiting handled by back
+        bs = refract_sample(V3<float>(params[0], params[1], params[2]), 1u, &tmp, w, sf,
+                            back ? 1u : 0u, xi[0]);
+    }
+    out_dir[0] = bs.dir.x; out_dir[1] = bs.dir.y; out_dir[2] = bs.dir.z;
+    out_pos[0] = bs.pos.x; out_pos[1] = bs.pos.y; out_pos[2] = bs.pos.z;
+    out_refl[0] = bs.refl.x; out_refl[1] = bs.refl.y; out_refl[2] = bs.refl.z;
+    *out_pdf = bs.pdf;
+}
+
+void oracle_bary_slerp(const float* q0, const float* q1, const float* q2, float a, float b,
+                       float* out) {
+    Q4<float> r = bary_slerp(Q4<float>{q0[0], q0[1], q0[2], q0[3]},
+                             Q4<float>{q1[0], q1[1], q1[2], q1[3]},
+                             Q4<float>{q2[0], q2[1], q2[2], q2[3]}, a, b);
+    out[0] = r.w; out[1] = r.x; out[2] = r.y; out[3] = r.z;
+}
+void oracle_nudge(const float* p, const float* d, float* out) {
+    V3<float> r = nudge(V3<float>(p[0], p[1], p[2]), V3<float>(d[0], d[1], d[2]));
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+int oracle_intersect_tri(const float* ro, const float* rd, const float* p0, const float* p1,
+                         const float* p2, int cull, float* t, float* bary3) {
+    V3<float> a(p0[0], p0[1], p0[2]), b(p1[0], p1[1], p1[2]), c(p2[0], p2[1], p2[2]);
+    float tt, b0, b1, v;
+    bool h = intersect_tri(V3<float>(ro[0], ro[1], ro[2]), V3<float>(rd[0], rd[1], rd[2]), a,
+                           b - a, c - a, cull != 0, tt, b0, b1, &v);
+    if (h) {
+        *t = tt;
+        bary3[0] = b0;
+        bary3[1] = b1;
+        bary3[2] = v;
+    }
+    return h ? 1 : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,145 @@
+/*
+ * CPU oracle for the meturay_b200 wavefront path-tracing path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this
+ * library: it is loaded by tests/, by __graft_entry__.smoke() and by the
+ * cpu_baseline / reference leg of bench.py, always as the checker.
+ *
+ * Every function restates the algorithm of the MRay reference
+ * (yalcinerbora/meturay, Source/...) at the cited file:line.  FP32 entry
+ * points use the same operation order as the CUDA kernels (no contraction,
+ * explicit fmaf where the kernels use one, the same portable sin/cos/acos),
+ * so that integer stages are bit-exact and radiance is bit-exact up to the
+ * order of float atomic additions.  FP64 entry points run the same
+ * algorithm in double precision and state the error of the FP32 image.
+ */
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- portable math (same algorithm as the device copy) ---- */
+void  oracle_sincosf(float x, float* s, float* c);
+float oracle_acosf(float x);
+
+/* ---- counter-based RNG: Philox4x32-10 (Salmon et al., SC'11) ---- */
+void oracle_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* ---- a1..a5: Morton codes and sort (LinearBVH.hpp:102-179,398-414) ---- */
+uint64_t oracle_morton3d(uint32_t x, uint32_t y, uint32_t z);
+/* tri_pos: tri_count*9 floats (p0,p1,p2).  Writes per-triangle AABB
+ * (tri_count*6: min xyz, max xyz), the extent (6), the Morton delta and the
+ * codes. */
+void oracle_morton_codes(const float* pos, const uint32_t* idx, uint32_t tri_count,
+                         float* aabbs, float* extent, float* delta, uint64_t* codes);
+/* Stable LSD radix sort of (key, value) pairs on bits [begin_bit, end_bit)
+ * (cub::DeviceRadixSort semantics, ascending or descending). */
+void oracle_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint32_t n,
+                           int begin_bit, int end_bit, int descending);
+void oracle_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t n,
+                           int begin_bit, int end_bit, int descending);
+
+/* ---- a6/a7: Karras/Apetrei hierarchy and bottom-up AABBs
+ *      (LinearBVH.hpp:30-100,181-396).  Node numbering as the reference:
+ *      leaves 0..n-1, internal nodes n..2n-2.  Returns 0 on success,
+ *      1 on duplicate codes (LinearBVH.hpp:505-521). ---- */
+int oracle_lbvh_build(const uint64_t* sorted_codes, const uint32_t* sorted_idx,
+                      const float* leaf_aabbs, uint32_t n,
+                      uint32_t* left, uint32_t* right, uint32_t* parent,
+                      float* inner_aabbs, uint32_t* root);
+
+/* ---- a13/a14: key sort + partition (RayMemory.cu:187-312) ---- */
+/* Sorts (key, id=0..n-1) descending on the dense key bits and returns the
+ * portions: (batch, offset, count) for each batch present, in ascending
+ * batch order like std::set<ArrayPortion>.  Returns the portion count. */
+uint32_t oracle_partition(const uint32_t* keys, uint32_t n, uint32_t batch_bits,
+                          uint32_t id_bits, uint32_t* sorted_keys, uint32_t* sorted_ids,
+                          uint32_t* portion_batch, uint32_t* portion_offset,
+                          uint32_t* portion_count);
+
+/* ---- scene, as consumed by the hot path ---- */
+typedef struct oracle_scene {
+    uint32_t vertex_count;
+    uint32_t tri_count;
+    const float*    pos;        /* vertex_count*3 */
+    const float*    tbn;        /* vertex_count*4 (w,x,y,z) */
+    const uint32_t* idx;        /* tri_count*3 */
+    const uint32_t* tri_key;    /* tri_count HitKey (batch<<24 | id) */
+    const uint8_t*  tri_cull;   /* tri_count, may be NULL (two-sided) */
+    uint32_t lambert_count;  const float* lambert_albedo;   /* 3 each */
+    uint32_t metal_count;    const float* metal_params;     /* eta3 k3 spec3 rough */
+    uint32_t refract_count;  const float* refract_albedo;   /* 3 each */
+    const uint32_t* refract_medium;
+    uint32_t light_count;    const float* light_radiance;   /* 3 each */
+    const uint32_t* light_prim;
+    uint32_t medium_count;   const float* medium_ior;
+    uint32_t base_medium;
+} oracle_scene;
+
+typedef struct oracle_camera {
+    float position[3];
+    float bottom_left[3];
+    float right[3];
+    float up[3];
+    float plane_size[2];
+    float near_far[2];
+} oracle_camera;
+
+typedef struct oracle_options {
+    uint32_t width, height;
+    uint32_t samples;        /* "Samples": s -> s*s spp per iteration */
+    uint32_t max_depth;
+    uint32_t rr_start;
+    uint32_t nee;
+    uint32_t mis;
+    uint32_t seed_lo, seed_hi;
+    uint32_t frame;
+    uint32_t threads;        /* 0 = all hardware threads */
+    uint32_t row_begin, row_end;  /* sample rows to render (0,0 = all) */
+} oracle_options;
+
+/* Build the LBVH of the scene (a1..a7) and keep it inside a handle. */
+typedef struct oracle_bvh oracle_bvh;
+oracle_bvh* oracle_bvh_create(const oracle_scene* scene, int* status);
+void        oracle_bvh_destroy(oracle_bvh*);
+uint32_t    oracle_bvh_root(const oracle_bvh*);
+
+/* a8..a11: closest hit of rays (origin3, tmin, dir3, tmax) per ray.
+ * out: key, prim (original triangle index or 0xFFFFFFFF), t, bary2. */
+void oracle_trace(const oracle_scene* scene, const oracle_bvh* bvh,
+                  const float* rays, uint32_t n,
+                  uint32_t* out_key, uint32_t* out_prim, float* out_t, float* out_bary,
+                  uint32_t threads);
+/* The reference "Linear" accelerator: brute force, triangle order, strict <. */
+void oracle_trace_linear(const oracle_scene* scene, const float* rays, uint32_t n,
+                         uint32_t* out_key, uint32_t* out_prim, float* out_t, float* out_bary,
+                         uint32_t threads);
+
+/* a16..a24: one iteration of the plain path tracer (GenerateWork, Render
+ * until done, sample radiance).  sample_rgb: (W*s)*(H*s)*3 per-sample
+ * radiance.  Returns the number of rays traced (camera+path+NEE). */
+uint64_t oracle_render(const oracle_scene* scene, const oracle_bvh* bvh,
+                       const oracle_camera* cam, const oracle_options* opt,
+                       float* sample_rgb);
+uint64_t oracle_render_f64(const oracle_scene* scene, const oracle_bvh* bvh,
+                           const oracle_camera* cam, const oracle_options* opt,
+                           double* sample_rgb);
+
+/* Single-vertex BxDF probes used by the golden-vector tests. */
+void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi,
+                        const float* w2t, const float* geo_normal, const float* pos,
+                        uint32_t backside, float from_ior, float to_ior,
+                        const float* xi, float* out_dir, float* out_pos,
+                        float* out_refl, float* out_pdf);
+void oracle_bary_slerp(const float* q0, const float* q1, const float* q2,
+                       float a, float b, float* out);
+void oracle_nudge(const float* p, const float* dir, float* out);
+int  oracle_intersect_tri(const float* ro, const float* rd, const float* p0,
+                          const float* p1, const float* p2, int cull,
+                          float* t, float* bary3);
+
+#ifdef __cplusplus
+}
+#endif

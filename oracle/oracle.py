@@ -1,0 +1,212 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference leg, always as the checker.  The C++
+restatement it loads cites the MRay reference file:line for every step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libmrayref.so"
+
+
+def build(ref_root: str | None = None) -> None:
+    """Compile the oracle (and the reference shim when the sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    root = Path(ref_root or "/root/reference")
+    if (root / "Source" / "RayLib" / "Ray.hpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
+
+
+class Scene(C.Structure):
+    _fields_ = [("vertex_count", C.c_uint32), ("tri_count", C.c_uint32),
+                ("pos", C.c_void_p), ("tbn", C.c_void_p), ("idx", C.c_void_p),
+                ("tri_key", C.c_void_p), ("tri_cull", C.c_void_p),
+                ("lambert_count", C.c_uint32), ("lambert_albedo", C.c_void_p),
+                ("metal_count", C.c_uint32), ("metal_params", C.c_void_p),
+                ("refract_count", C.c_uint32), ("refract_albedo", C.c_void_p),
+                ("refract_medium", C.c_void_p),
+                ("light_count", C.c_uint32), ("light_radiance", C.c_void_p),
+                ("light_prim", C.c_void_p),
+                ("medium_count", C.c_uint32), ("medium_ior", C.c_void_p),
+                ("base_medium", C.c_uint32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("bottom_left", C.c_float * 3),
+                ("right", C.c_float * 3), ("up", C.c_float * 3), ("plane_size", C.c_float * 2),
+                ("near_far", C.c_float * 2)]
+
+
+class Options(C.Structure):
+    _fields_ = [(k, C.c_uint32) for k in ("width", "height", "samples", "max_depth", "rr_start",
+                                          "nee", "mis", "seed_lo", "seed_hi", "frame", "threads",
+                                          "row_begin", "row_end")]
+
+
+def _load():
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    vp, u32 = C.c_void_p, C.c_uint32
+    lib.oracle_morton3d.restype = C.c_uint64
+    lib.oracle_morton3d.argtypes = [u32, u32, u32]
+    lib.oracle_acosf.restype = C.c_float
+    lib.oracle_acosf.argtypes = [C.c_float]
+    lib.oracle_bvh_create.restype = vp
+    lib.oracle_bvh_create.argtypes = [C.POINTER(Scene), C.POINTER(C.c_int)]
+    lib.oracle_bvh_destroy.argtypes = [vp]
+    lib.oracle_bvh_root.restype = u32
+    lib.oracle_bvh_root.argtypes = [vp]
+    lib.oracle_trace.argtypes = [C.POINTER(Scene), vp, vp, u32, vp, vp, vp, vp, u32]
+    lib.oracle_trace_linear.argtypes = [C.POINTER(Scene), vp, u32, vp, vp, vp, vp, u32]
+    lib.oracle_render.restype = C.c_uint64
+    lib.oracle_render.argtypes = [C.POINTER(Scene), vp, C.POINTER(Camera), C.POINTER(Options), vp]
+    lib.oracle_render_f64.restype = C.c_uint64
+    lib.oracle_render_f64.argtypes = [C.POINTER(Scene), vp, C.POINTER(Camera),
+                                      C.POINTER(Options), vp]
+    lib.oracle_partition.restype = u32
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def morton_codes(pos: np.ndarray, idx: np.ndarray):
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    n = idx.shape[0]
+    aabbs = np.zeros((n, 6), np.float32)
+    ext = np.zeros(6, np.float32)
+    delta = np.zeros(1, np.float32)
+    codes = np.zeros(n, np.uint64)
+    lib.oracle_morton_codes(_p(pos), _p(idx), C.c_uint32(n), _p(aabbs), _p(ext), _p(delta),
+                            _p(codes))
+    return aabbs, ext, float(delta[0]), codes
+
+
+def sort_pairs(keys: np.ndarray, vals: np.ndarray, begin: int, end: int, descending: bool):
+    keys = np.ascontiguousarray(keys).copy()
+    vals = np.ascontiguousarray(vals, np.uint32).copy()
+    fn = lib.oracle_sort_pairs_u64 if keys.dtype == np.uint64 else lib.oracle_sort_pairs_u32
+    fn(_p(keys), _p(vals), C.c_uint32(keys.shape[0]), C.c_int(begin), C.c_int(end),
+       C.c_int(1 if descending else 0))
+    return keys, vals
+
+
+def lbvh(sorted_codes: np.ndarray, sorted_idx: np.ndarray, leaf_aabbs: np.ndarray):
+    n = sorted_codes.shape[0]
+    ni = max(n - 1, 0)
+    out = {"left": np.zeros(ni, np.uint32), "right": np.zeros(ni, np.uint32),
+           "parent": np.zeros(2 * n - 1, np.uint32), "inner": np.zeros((ni, 6), np.float32),
+           "root": np.zeros(1, np.uint32)}
+    st = lib.oracle_lbvh_build(_p(np.ascontiguousarray(sorted_codes, np.uint64)),
+                               _p(np.ascontiguousarray(sorted_idx, np.uint32)),
+                               _p(np.ascontiguousarray(leaf_aabbs, np.float32)), C.c_uint32(n),
+                               _p(out["left"]), _p(out["right"]), _p(out["parent"]),
+                               _p(out["inner"]), _p(out["root"]))
+    out["status"] = st
+    return out
+
+
+def partition(keys: np.ndarray, batch_bits: int, id_bits: int):
+    keys = np.ascontiguousarray(keys, np.uint32)
+    n = keys.shape[0]
+    sk = np.zeros(n, np.uint32)
+    si = np.zeros(n, np.uint32)
+    pb = np.zeros(256, np.uint32)
+    po = np.zeros(256, np.uint32)
+    pc = np.zeros(256, np.uint32)
+    k = lib.oracle_partition(_p(keys), C.c_uint32(n), C.c_uint32(batch_bits), C.c_uint32(id_bits),
+                             _p(sk), _p(si), _p(pb), _p(po), _p(pc))
+    return sk, si, [(int(pb[i]), int(po[i]), int(pc[i])) for i in range(k)]
+
+
+class OracleScene:
+    """The scene as the hot path consumes it, plus the oracle's own LBVH."""
+
+    def __init__(self, scene, exported: dict):
+        self.arrays = {
+            "pos": np.ascontiguousarray(scene.positions, np.float32),
+            "tbn": np.ascontiguousarray(exported["tbn"], np.float32),
+            "idx": np.ascontiguousarray(scene.indices, np.uint32),
+            "tri_key": np.ascontiguousarray(exported["tri_key"], np.uint32),
+            "tri_cull": (np.ascontiguousarray(scene.tri_cull, np.uint8)
+                         if scene.tri_cull is not None else None),
+            "lambert": np.ascontiguousarray(exported["lambert"], np.float32),
+            "metal": np.ascontiguousarray(exported["metal"], np.float32),
+            "refract": np.ascontiguousarray(exported["refract"], np.float32),
+            "refract_medium": np.ascontiguousarray(exported["refract_medium"], np.uint32),
+            "light_radiance": np.ascontiguousarray(exported["light_radiance"], np.float32),
+            "light_prim": np.ascontiguousarray(exported["light_prim"], np.uint32),
+            "medium_ior": np.ascontiguousarray(scene.medium_ior, np.float32),
+        }
+        a = self.arrays
+        s = Scene()
+        s.vertex_count = a["pos"].shape[0]
+        s.tri_count = a["idx"].shape[0]
+        s.pos, s.tbn, s.idx, s.tri_key = _p(a["pos"]), _p(a["tbn"]), _p(a["idx"]), _p(a["tri_key"])
+        s.tri_cull = _p(a["tri_cull"])
+        s.lambert_count, s.lambert_albedo = a["lambert"].shape[0], _p(a["lambert"])
+        s.metal_count, s.metal_params = a["metal"].shape[0], _p(a["metal"])
+        s.refract_count, s.refract_albedo = a["refract"].shape[0], _p(a["refract"])
+        s.refract_medium = _p(a["refract_medium"])
+        s.light_count = a["light_prim"].shape[0]
+        s.light_radiance, s.light_prim = _p(a["light_radiance"]), _p(a["light_prim"])
+        s.medium_count, s.medium_ior = a["medium_ior"].shape[0], _p(a["medium_ior"])
+        s.base_medium = scene.base_medium
+        self.c = s
+        st = C.c_int(0)
+        self.bvh = lib.oracle_bvh_create(C.byref(s), C.byref(st))
+        self.bvh_status = st.value
+
+    def __del__(self):
+        if getattr(self, "bvh", None):
+            lib.oracle_bvh_destroy(self.bvh)
+            self.bvh = None
+
+    def trace(self, rays: np.ndarray, threads: int = 0, linear: bool = False):
+        """rays: (n, 8) float32 = origin, tMin, direction, tMax."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        key = np.zeros(n, np.uint32)
+        prim = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        bary = np.zeros((n, 2), np.float32)
+        if linear:
+            lib.oracle_trace_linear(C.byref(self.c), _p(rays), n, _p(key), _p(prim), _p(t),
+                                    _p(bary), threads)
+        else:
+            lib.oracle_trace(C.byref(self.c), self.bvh, _p(rays), n, _p(key), _p(prim), _p(t),
+                             _p(bary), threads)
+        return key, prim, t, bary
+
+    def render(self, camera_frame: np.ndarray, width: int, height: int, samples: int,
+               max_depth: int, rr_start: int, nee: bool, seed: int, frame: int = 0,
+               threads: int = 0, rows: tuple[int, int] = (0, 0), fp64: bool = False):
+        """Per-sample radiance ((h*s), (w*s), 3) and the rays traced."""
+        cam = Camera()
+        f = camera_frame
+        cam.position[:] = [float(v) for v in f[0:3]]
+        cam.bottom_left[:] = [float(v) for v in f[3:6]]
+        cam.right[:] = [float(v) for v in f[6:9]]
+        cam.up[:] = [float(v) for v in f[9:12]]
+        cam.plane_size[:] = [float(v) for v in f[12:14]]
+        cam.near_far[:] = [float(v) for v in f[14:16]]
+        o = Options(width, height, samples, max_depth, rr_start, 1 if nee else 0, 0,
+                    seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, frame, threads, rows[0], rows[1])
+        out = np.zeros((height * samples, width * samples, 3), np.float64 if fp64 else np.float32)
+        fn = lib.oracle_render_f64 if fp64 else lib.oracle_render
+        rays = fn(C.byref(self.c), self.bvh, C.byref(cam), C.byref(o), _p(out))
+        return out, int(rays)
