@@ -1,0 +1,354 @@
+"""Benchmark: Mrays/s of the plain wavefront path tracer on the 1M-triangle scene.
+
+Workload ("clusters-1M"): 1000 Gaussian clusters x 1000 triangles (seed 1),
+1920x1080, 1 sample per pixel per step ("Samples": 1), depth 8, NEE on,
+Russian roulette from depth 3.  One step = one frame: camera rays + 8
+trace/partition/shade depths + resolve, replayed from a captured CUDA graph.
+Rays traced = camera + path + NEE rays entering the traversal, summed over
+depths (the reference's "rays entering HitRays").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed (one process per GPU) as independent
+replicas: each rank renders its own frames of the same workload (weak
+scaling; the path tracer has no exchange step).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s"
+WORKLOAD = {"workload": "clusters-1M plain path tracing", "triangles": 1000004,
+            "resolution": "1920x1080", "spp_per_step": 1, "max_depth": 8,
+            "nee": True, "rr_start": 3, "scene_seed": 1,
+            "l2": "inputs larger than L2 (ray/hit buffers ~470 MB, BVH ~180 MB)"}
+OPTS = {"Samples": 1, "MaxDepth": 8, "NextEventEstimation": 1, "RussianRouletteStart": 3,
+        "DirectLightMIS": 0}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_ours(args, rank: int, world: int, dist) -> dict | None:
+    import torch
+    import meturay_b200 as m
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    scene = m.scenes.clusters(seed=1)
+    system = m.TracerSystem(dev)
+    g = m.GPUScene(system, scene)
+    g.construct_accelerators()
+    t = m.PathTracer(system, g)
+    t.set_options(dict(OPTS, Seed=1 + rank))
+    stream = torch.cuda.ExternalStream(t.stream)
+
+    for _ in range(args.warmup):
+        t.render_frame()
+    torch.cuda.synchronize()
+    rays0, _ = t.stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        t.render_frame()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    rays1, _ = t.stats()
+    rays = rays1 - rays0
+
+    # ---- end to end through the public API with host buffers ----
+    import ctypes as C
+    img_bytes = scene.width * scene.height * 16
+    host_img = torch.empty(scene.width * scene.height * 4, dtype=torch.float32).pin_memory()
+    cam_bytes = 56  # the pinhole frame uploaded by set_camera
+    for _ in range(2):
+        t.set_camera(scene.camera)
+        t.render_frame()
+        t.image_into(C.c_void_p(host_img.data_ptr()))
+    torch.cuda.synchronize()
+    r0, _ = t.stats()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        t.set_camera(scene.camera)
+        t.render_frame()
+        t.image_into(C.c_void_p(host_img.data_ptr()))
+    s1.record(stream)
+    s1.synchronize()
+    e2e_ms = s0.elapsed_time(s1)
+    r1, _ = t.stats()
+    e2e_rays = r1 - r0
+
+    # ---- roofline of the traversal kernel (one stepwise profiled frame) ----
+    prof = t.profile_frame()
+    launches = t.launches_per_frame() * args.steps
+
+    if dist:
+        tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        rr = torch.tensor([rays, e2e_rays], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
+        ms, e2e_ms = float(tt[0]), float(tt[1])
+        rays, e2e_rays = int(rr[0]), int(rr[1])
+    if rank != 0:
+        return None
+
+    peak, peak_kind = _peaks()
+    # algorithmic bytes of the traversal: per ray 32 B in (origin/tMin,
+    # direction/tMax) + 20 B out (key, prim, t, barycentrics); per inner node
+    # visited 64 B; per triangle tested 48 B (v0, e0, e1)
+    trace_bytes = 52 * prof["rays"] + 64 * prof["node_visits"] + 48 * prof["tri_tests"]
+    trace_s = prof["trace_ms"] / 1e3
+    achieved = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
+    traffic = None
+    tf = ROOT / "profiles" / "trace_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    return {
+        "metric": METRIC,
+        "value": rays / (ms / 1e3) / 1e6,
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded clusters-1M scene)",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+        "rays_per_step": rays / args.steps / world,
+        "e2e": {"value": e2e_rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+                "h2d_bytes_per_step": cam_bytes, "d2h_bytes_per_step": img_bytes},
+        "roofline": {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_frame": trace_bytes,
+                     "trace_ms_per_frame": prof["trace_ms"],
+                     "launches_per_frame": prof["trace_launches"],
+                     "stage_ms": {k: prof[k] for k in ("camera_ms", "trace_ms", "partition_ms",
+                                                       "shade_ms", "resolve_ms")},
+                     "node_visits_per_ray": prof["node_visits"] / max(prof["rays"], 1),
+                     "tri_tests_per_ray": prof["tri_tests"] / max(prof["rays"], 1)},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+
+
+def _oracle_setup(scene):
+    """Scene arrays as the hot path consumes them, built by the oracle alone."""
+    from oracle import oracle as o
+    import ctypes as C
+    tbn = np.zeros((scene.positions.shape[0], 4), np.float32)
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    nrm = np.ascontiguousarray(scene.normals, np.float32)
+    uvs = np.ascontiguousarray(scene.uvs, np.float32)
+    idx = np.ascontiguousarray(scene.indices, np.uint32)
+    o.lib.oracle_build_tbn(o._p(pos), o._p(nrm), o._p(uvs), o._p(idx),
+                           C.c_uint32(pos.shape[0]), C.c_uint32(idx.shape[0]), o._p(tbn))
+    ex = o.scene_tables(scene)
+    ex["tbn"] = tbn
+    return o.OracleScene(scene, ex)
+
+
+def _camera16(scene):
+    """Pinhole frame (GPUCameraPinhole.cuh:135-162) computed in float32."""
+    f = np.float32
+    c = scene.camera
+    pos = np.array(c["position"], f)
+    gz = np.array(c["gaze"], f)
+    up = np.array(c["up"], f)
+    near = f(c["near_far"][0])
+    wh = f(np.tan(f(c["fov"][0]) * f(0.5))) * near
+    hh = f(np.tan(f(c["fov"][1]) * f(0.5))) * near
+
+    def nrm(v):
+        return (v * (f(1) / np.sqrt(np.dot(v, v), dtype=f))).astype(f)
+
+    gd = gz - pos
+    right = nrm(np.cross(gd, up).astype(f))
+    up = nrm(np.cross(right, gd).astype(f))
+    gd = nrm(np.cross(up, right).astype(f))
+    bl = ((pos - right * wh) - up * hh) + gd * near
+    return np.concatenate([pos, bl, right, up, [wh * 2, hh * 2],
+                           np.array(c["near_far"], f)]).astype(f)
+
+
+def cpu_leg(scene, os_, rows: int, threads: int) -> dict:
+    cf = _camera16(scene)
+    t0 = time.perf_counter()
+    _, rays = os_.render(cf, scene.width, scene.height, 1, 8, 3, True, 1,
+                         threads=threads, rows=(0, rows))
+    dt = time.perf_counter() - t0
+    return {"rays": rays, "seconds": dt, "rows": rows}
+
+
+def run_reference(args) -> dict:
+    import meturay_b200.scenes as scenes
+    cores = os.cpu_count() or 1
+    scene = scenes.clusters(seed=1)
+    os_ = _oracle_setup(scene)
+    # size each step to about 1.5 s of work on this host
+    probe = cpu_leg(scene, os_, 16, cores)
+    rate = probe["rays"] / max(probe["seconds"], 1e-6)
+    rows = int(min(scene.height, max(16, 16 * 1.5 / max(probe["seconds"], 1e-3))))
+    for _ in range(args.warmup):
+        cpu_leg(scene, os_, min(rows, 64), cores)
+    total_rays, total_s = 0, 0.0
+    for _ in range(args.steps):
+        r = cpu_leg(scene, os_, rows, cores)
+        total_rays += r["rays"]
+        total_s += r["seconds"]
+    value = total_rays / total_s / 1e6
+    sample = (f"first {rows} of {scene.height} image rows (1920 px wide) of the clusters-1M frame "
+              f"per step, {cores} threads")
+    return {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded clusters-1M scene)",
+        "config": dict(WORKLOAD, parallelism="cpu"),
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "probe_rate_mrays": rate / 1e6,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    out = run_ours(args, rank, world, dist)
+    if out is not None and not args.no_cpu_baseline:
+        import meturay_b200.scenes as scenes
+        scene = scenes.clusters(seed=1)
+        os_ = _oracle_setup(scene)
+        cores = os.cpu_count() or 1
+        probe = cpu_leg(scene, os_, 16, cores)
+        rows = int(min(scene.height, max(16, 16 * 12.0 / max(probe["seconds"], 1e-3))))
+        r = cpu_leg(scene, os_, rows, cores)
+        out["cpu_baseline"] = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s",
+                               "cores": cores, "kind": "port",
+                               "sample": f"first {rows} of 1080 rows of the clusters-1M frame "
+                                         f"(1 spp, depth 8), {cores} threads, "
+                                         f"{r['seconds']:.1f} s"}
+    if out is not None:
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -153,6 +153,13 @@ int mrb_tracer_reset_image(mrb_tracer* t);
 int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays_traced, uint32_t* frames);
 /* Stream the tracer launches on (cudaStream_t as void*). */
 void* mrb_tracer_stream(mrb_tracer* t);
+/* Number of kernels one frame launches (>= 0), or a negative status. */
+int mrb_tracer_launches_per_frame(mrb_tracer* t);
+/* Render one frame stage by stage with CUDA events around each stage.
+ * stage_ms[5]: camera, traversal, partition, shading, resolve (summed over
+ * depths).  work[4]: rays traced, inner nodes visited, triangles tested,
+ * depths.  The frame counts like any other. */
+int mrb_tracer_profile_frame(mrb_tracer* t, float* stage_ms, uint64_t* work);
 
 /* ---- kernel-level entry points (device pointers) ---------------------- */
 /* KCGenerateAABBs + extent reduce + KCGenMortonCodes

@@ -356,19 +356,48 @@ int step_camera(mrb_tracer* t) {
                            t->samplesBuf.as<float4>(), cnt, t->stream);
 }
 
+struct StageTimer {
+    cudaEvent_t ev[2 * 8] = {};
+    float ms[8] = {};
+};
+
 // One Render() step: HitRays -> PartitionRaysWRTWork -> WorkRays
-// (PathTracer.cu:144-291) for the rays of buffer `cur`.
-int step_depth(mrb_tracer* t, uint32_t d) {
+// (PathTracer.cu:144-291) for the rays of buffer `cur`.  With a timer the
+// stages are bracketed by events and the traversal is repeated once in its
+// counting form (outside the timed interval) for the work figures.
+int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
+               unsigned long long* workCounters = nullptr) {
     mrb_scene* sc = t->scene;
     const int cur = d & 1, nxt = cur ^ 1;
     uint32_t* cnt = t->count.as<uint32_t>();
     HitOut ho{t->hitKey.as<uint32_t>(), t->hitPrim.as<uint32_t>(), t->hitT.as<float>(),
               t->hitBary.as<float2>()};
     int r;
+    auto mark = [&](int i) -> int {
+        if (tm) MRB_CUDA(cudaEventRecord(tm->ev[i], t->stream));
+        return 0;
+    };
+    auto lap = [&](int stage, int i0) -> int {
+        if (!tm) return 0;
+        MRB_CUDA(cudaEventSynchronize(tm->ev[i0 + 1]));
+        float ms = 0.f;
+        MRB_CUDA(cudaEventElapsedTime(&ms, tm->ev[i0], tm->ev[i0 + 1]));
+        tm->ms[stage] += ms;
+        return 0;
+    };
+    if (mark(0)) return MRB_E_CUDA;
     if ((r = trace_closest(sc->accel(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
                            cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
         return r;
+    if (mark(1) || lap(1, 0)) return MRB_E_CUDA;
+    if (workCounters) {
+        if ((r = trace_closest(sc->accel(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+                               cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream,
+                               workCounters)))
+            return r;
+    }
     if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
+    if (mark(2)) return MRB_E_CUDA;
     PortionTable pt = portion_table(t);
     if ((r = dense_keys(ho.key, cnt + cur, t->maxRays, sc->idBits, t->dense.as<uint32_t>(), pt,
                         t->stream)))
@@ -380,14 +409,18 @@ int step_depth(mrb_tracer* t, uint32_t d) {
     if ((r = find_portions(t->dense.as<uint32_t>(), cnt + cur, t->maxRays, sc->idBits, pt,
                            t->stream)))
         return r;
+    if (mark(3) || lap(2, 2)) return MRB_E_CUDA;
     MRB_CUDA(cudaMemsetAsync(cnt + nxt, 0, 4, t->stream));
     HitIn hi{ho.key, ho.prim, ho.t, ho.bary};
     const bool gen = (d + 1) < t->maxDepth;
-    return shade(sc->dev(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
-                 t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull,
-                 t->maxRays, t->samplesBuf.as<float4>(), path_options(t), gen,
-                 t->rayO[nxt].as<float4>(), t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(),
-                 cnt + nxt, t->stream);
+    if (mark(4)) return MRB_E_CUDA;
+    r = shade(sc->dev(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+              t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull, t->maxRays,
+              t->samplesBuf.as<float4>(), path_options(t), gen, t->rayO[nxt].as<float4>(),
+              t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(), cnt + nxt, t->stream);
+    if (r) return r;
+    if (mark(5) || lap(3, 4)) return MRB_E_CUDA;
+    return 0;
 }
 
 int step_finalize(mrb_tracer* t) {
@@ -403,6 +436,16 @@ int record_frame(mrb_tracer* t) {
     for (uint32_t d = 0; d < t->maxDepth; d++)
         if ((r = step_depth(t, d))) return r;
     return step_finalize(t);
+}
+
+// Kernel launches recorded per frame (camera, per depth: trace, add_count,
+// dense keys, histogram, histogram scan, onesweep passes (+copy-back),
+// portions, shade; then resolve and frame advance).
+uint32_t launches_per_frame(const mrb_tracer* t) {
+    const uint32_t bits = 3 + t->scene->idBits;
+    const uint32_t passes = (bits + 7) / 8;
+    const uint32_t sort = 2 + passes + (passes & 1);
+    return 1 + t->maxDepth * (3 + sort + 2) + 2;
 }
 
 int check_device_errors(mrb_tracer* t) {
@@ -944,6 +987,54 @@ int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays, uint32_t* frames) {
 }
 
 void* mrb_tracer_stream(mrb_tracer* t) { return t ? static_cast<void*>(t->stream) : nullptr; }
+
+int mrb_tracer_launches_per_frame(mrb_tracer* t) {
+    if (!t) return MRB_E_ARG;
+    return static_cast<int>(launches_per_frame(t));
+}
+
+int mrb_tracer_profile_frame(mrb_tracer* t, float* stageMs, uint64_t* work) {
+    if (!t || !stageMs || !work) return MRB_E_ARG;
+    if (!t->camSet) {
+        set_error("tracer: camera not set");
+        return MRB_E_STATE;
+    }
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_buffers(t);
+    if (r) return r;
+    StageTimer tm;
+    for (auto& e : tm.ev) MRB_CUDA(cudaEventCreate(&e));
+    DBuf wc;
+    if ((r = wc.alloc(16))) return r;
+    MRB_CUDA(cudaMemsetAsync(wc.p, 0, 16, t->stream));
+    unsigned long long rays0 = 0, rays1 = 0;
+    MRB_CUDA(cudaMemcpyAsync(&rays0, t->counters.p, 8, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    MRB_CUDA(cudaEventRecord(tm.ev[6], t->stream));
+    if ((r = step_camera(t))) return r;
+    MRB_CUDA(cudaEventRecord(tm.ev[7], t->stream));
+    MRB_CUDA(cudaEventSynchronize(tm.ev[7]));
+    MRB_CUDA(cudaEventElapsedTime(&tm.ms[0], tm.ev[6], tm.ev[7]));
+    for (uint32_t d = 0; d < t->maxDepth; d++)
+        if ((r = step_depth(t, d, &tm, wc.as<unsigned long long>()))) return r;
+    MRB_CUDA(cudaEventRecord(tm.ev[6], t->stream));
+    if ((r = step_finalize(t))) return r;
+    MRB_CUDA(cudaEventRecord(tm.ev[7], t->stream));
+    MRB_CUDA(cudaEventSynchronize(tm.ev[7]));
+    MRB_CUDA(cudaEventElapsedTime(&tm.ms[4], tm.ev[6], tm.ev[7]));
+    unsigned long long w[2] = {0, 0};
+    MRB_CUDA(cudaMemcpyAsync(w, wc.p, 16, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaMemcpyAsync(&rays1, t->counters.p, 8, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    for (auto& e : tm.ev) cudaEventDestroy(e);
+    for (int i = 0; i < 5; i++) stageMs[i] = tm.ms[i];
+    work[0] = rays1 - rays0;
+    work[1] = w[0];
+    work[2] = w[1];
+    work[3] = t->maxDepth;
+    t->frames++;
+    return check_device_errors(t);
+}
 
 // ---- kernel-level ----------------------------------------------------------
 int mrb_morton_codes(const float* pos, const uint32_t* idx, uint32_t n, float* triAabb,

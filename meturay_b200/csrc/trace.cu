@@ -62,11 +62,16 @@ __device__ __forceinline__ void tri_test(const AccelDev& acc, int s, V3 o, V3 d,
     }
 }
 
+// kCount: also count inner nodes visited and triangles tested (for the
+// algorithmic-bytes figure of the roofline); results are unchanged.
+template <bool kCount>
 __global__ void __launch_bounds__(128) k_trace(AccelDev acc, const float4* __restrict__ rayO,
                                                const float4* __restrict__ rayD,
                                                const uint32_t* __restrict__ dCount,
-                                               uint32_t hCount, HitOut out, uint32_t* errorFlag) {
+                                               uint32_t hCount, HitOut out, uint32_t* errorFlag,
+                                               unsigned long long* counters) {
     const uint32_t n = dCount ? *dCount : hCount;
+    uint32_t nodeVisits = 0, triTests = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 ro = rayO[i], rd = rayD[i];
         const V3 o = {ro.x, ro.y, ro.z}, d = {rd.x, rd.y, rd.z};
@@ -75,6 +80,7 @@ __global__ void __launch_bounds__(128) k_trace(AccelDev acc, const float4* __res
         int hitTri = -1;
         float hb0 = 0.0f, hb1 = 0.0f;
         if (acc.triCount == 1) {
+            if (kCount) triTests++;
             tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
         } else if (acc.triCount > 1) {
             const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
@@ -84,6 +90,7 @@ __global__ void __launch_bounds__(128) k_trace(AccelDev acc, const float4* __res
             int node = acc.root;
             for (;;) {
                 if (node >= 0) {
+                    if (kCount) nodeVisits++;
                     const float4* np = reinterpret_cast<const float4*>(acc.nodes + node);
                     const float4 na = __ldg(np), nb = __ldg(np + 1), nc = __ldg(np + 2);
                     const int4 nd = __ldg(reinterpret_cast<const int4*>(np + 3));
@@ -106,6 +113,7 @@ __global__ void __launch_bounds__(128) k_trace(AccelDev acc, const float4* __res
                         continue;
                     }
                 } else {
+                    if (kCount) triTests++;
                     tri_test(acc, ~node, o, d, tmin, closest, hitTri, hb0, hb1);
                 }
                 if (sp == 0) break;
@@ -124,17 +132,33 @@ __global__ void __launch_bounds__(128) k_trace(AccelDev acc, const float4* __res
             out.bary[i] = make_float2(0.0f, 0.0f);
         }
     }
+    if (kCount) {
+        unsigned long long a = nodeVisits, b = triTests;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+            b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 0, a);
+            atomicAdd(counters + 1, b);
+        }
+    }
 }
 
 }  // namespace
 
 int trace_closest(const AccelDev& acc, const float4* rayO, const float4* rayD,
                   const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
-                  uint32_t* errorFlag, cudaStream_t stream) {
+                  uint32_t* errorFlag, cudaStream_t stream, unsigned long long* counters) {
     if (maxCount == 0) return 0;
     uint32_t blocks = (maxCount + 127) / 128;
     blocks = blocks < 148u * 16u ? blocks : 148u * 16u;
-    k_trace<<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out, errorFlag);
+    if (counters)
+        k_trace<true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
+                                                  errorFlag, counters);
+    else
+        k_trace<false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
+                                                   errorFlag, nullptr);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

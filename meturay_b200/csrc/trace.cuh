@@ -16,6 +16,7 @@ struct HitOut {
 // rayO[i] = (origin, tMin), rayD[i] = (direction, tMax).
 int trace_closest(const AccelDev& acc, const float4* rayO, const float4* rayD,
                   const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
-                  uint32_t* errorFlag, cudaStream_t stream);
+                  uint32_t* errorFlag, cudaStream_t stream,
+                  unsigned long long* counters = nullptr);
 
 }  // namespace mrb

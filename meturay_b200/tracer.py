@@ -260,6 +260,20 @@ class PathTracer:
         check(lib.mrb_tracer_stats(self._h, C.byref(r), C.byref(f)))
         return int(r.value), int(f.value)
 
+    def launches_per_frame(self) -> int:
+        return check(lib.mrb_tracer_launches_per_frame(self._h))
+
+    def profile_frame(self) -> dict:
+        """One stepwise frame with per-stage CUDA-event timings and work counts."""
+        ms = np.zeros(5, np.float32)
+        work = np.zeros(4, np.uint64)
+        check(lib.mrb_tracer_profile_frame(self._h, _ptr(ms), _ptr(work)))
+        return {"camera_ms": float(ms[0]), "trace_ms": float(ms[1]),
+                "partition_ms": float(ms[2]), "shade_ms": float(ms[3]),
+                "resolve_ms": float(ms[4]), "rays": int(work[0]),
+                "node_visits": int(work[1]), "tri_tests": int(work[2]),
+                "trace_launches": int(work[3])}
+
     @property
     def stream(self) -> int:
         return lib.mrb_tracer_stream(self._h) or 0

@@ -448,9 +448,18 @@ inline void tri_test(const oracle_scene* s, const oracle_bvh* b, uint32_t tri, V
 // Closest hit over the LBVH: both child boxes are tested at each inner node
 // and the nearer one is entered first (ties go to the left child); the
 // farther one is pushed.  The device kernel walks the same tree the same way.
+// Traversal work counters (inner nodes entered, triangles tested), summed
+// over all threads; read with oracle_trace_counters.
+std::atomic<uint64_t> g_nodes{0}, g_tris{0};
+
 template <class T>
 Hit<T> trace_one(const oracle_scene* s, const oracle_bvh* b, V3<T> o, V3<T> d, T tmin, T tmax) {
     Hit<T> h;
+    uint64_t nodes = 0, tris = 0;
+    struct Flush {
+        uint64_t& n; uint64_t& t;
+        ~Flush() { g_nodes.fetch_add(n, std::memory_order_relaxed); g_tris.fetch_add(t, std::memory_order_relaxed); }
+    } flush{nodes, tris};
     const uint32_t n = b->n;
     if (n == 0) return h;
     if (n == 1) {
@@ -464,6 +473,7 @@ Hit<T> trace_one(const oracle_scene* s, const oracle_bvh* b, V3<T> o, V3<T> d, T
     uint32_t node = b->root;  // global node index (>= n: inner)
     for (;;) {
         if (node >= n) {
+            nodes++;
             uint32_t j = node - n;
             uint32_t c[2] = {b->left[j], b->right[j]};
             bool hit[2];
@@ -486,6 +496,7 @@ Hit<T> trace_one(const oracle_scene* s, const oracle_bvh* b, V3<T> o, V3<T> d, T
                 continue;
             }
         } else {
+            tris++;
             tri_test(s, b, b->sorted_idx[node], o, d, tmin, tmax, h);
         }
         if (sp == 0) break;
@@ -1027,6 +1038,14 @@ void oracle_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     philox(ctr, key, out);
 }
 uint64_t oracle_morton3d(uint32_t x, uint32_t y, uint32_t z) { return morton3d(x, y, z); }
+void oracle_trace_counters(uint64_t* out, int reset) {
+    out[0] = g_nodes.load();
+    out[1] = g_tris.load();
+    if (reset) {
+        g_nodes = 0;
+        g_tris = 0;
+    }
+}
 
 void oracle_morton_codes(const float* pos, const uint32_t* idx, uint32_t n, float* aabbs,
                          float* extent, float* delta, uint64_t* codes) {
@@ -1292,6 +1311,83 @@ void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi, con
     out_pos[0] = bs.pos.x; out_pos[1] = bs.pos.y; out_pos[2] = bs.pos.z;
     out_refl[0] = bs.refl.x; out_refl[1] = bs.refl.y; out_refl[2] = bs.refl.z;
     *out_pdf = bs.pdf;
+}
+
+// GPUPrimitiveTriangle.cpp:160-320 with Triangle::CalculateTangent
+// (Triangle.h:73-111), OrthogonalVector (Vector.hpp:877-886) and
+// TransformGen::Space (Quaternion.hpp:372-480).
+void oracle_build_tbn(const float* pos, const float* nrm, const float* uvs, const uint32_t* idx,
+                      uint32_t V, uint32_t T, float* out) {
+    using F3 = V3<float>;
+    auto P = [&](uint32_t v) { return F3(pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]); };
+    auto N = [&](uint32_t v) { return F3(nrm[3 * v], nrm[3 * v + 1], nrm[3 * v + 2]); };
+    auto ortho = [](F3 v) {
+        if (std::fabs(v.x) > std::fabs(v.y)) {
+            float s = std::sqrt(v.x * v.x + v.z * v.z);
+            return F3(-v.z / s, 0.0f / s, v.x / s);
+        }
+        float s = std::sqrt(v.y * v.y + v.z * v.z);
+        return F3(0.0f / s, v.z / s, -v.y / s);
+    };
+    static const float defUv[3][2] = {{0.f, 0.f}, {1.f, 0.f}, {0.f, 1.f}};
+    std::vector<F3> tan(V, F3(0, 0, 0));
+    for (uint32_t t = 0; t < T; t++) {
+        uint32_t ix[3] = {idx[3 * t], idx[3 * t + 1], idx[3 * t + 2]};
+        const float* uv[3];
+        for (int k = 0; k < 3; k++) uv[k] = uvs ? uvs + 2 * ix[k] : defUv[k];
+        for (int k = 0; k < 3; k++) {
+            int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+            F3 vec0 = P(ix[k1]) - P(ix[k]), vec1 = P(ix[k2]) - P(ix[k]);
+            float du0x = uv[k1][0] - uv[k][0], du0y = uv[k1][1] - uv[k][1];
+            float du1x = uv[k2][0] - uv[k][0], du1y = uv[k2][1] - uv[k][1];
+            float det = (du0x * du1y - du1x * du0y);
+            F3 tk;
+            if (det == 0.0f) {
+                tk = ortho(N(ix[k]));
+            } else {
+                float r = 1.0f / det;
+                tk = r * (du1y * vec0 - du0y * vec1);
+                if (det < 0) tk = -tk;
+                if (std::isnan(tk.x) || std::isnan(tk.y) || std::isnan(tk.z)) tk = ortho(N(ix[k]));
+            }
+            tan[ix[k]] = tan[ix[k]] + tk;
+        }
+    }
+    for (uint32_t v = 0; v < V; v++) {
+        F3 n = N(v), t = tan[v];
+        if (dot(t, t) < 1.0e-5f) t = ortho(n);
+        t = normalize(t);
+        F3 x = normalize(t - n * dot(n, t));
+        F3 y = cross(n, x);
+        F3 z = n;
+        F3 c = cross(x, y) - z;
+        if (std::fabs(c.x) > 0.1f && std::fabs(c.y) > 0.1f && std::fabs(c.z) > 0.1f) x = -x;
+        float tt, w, qx, qy, qz;
+        if (z.z < 0) {
+            if (x.x > y.y) {
+                tt = 1 + x.x - y.y - z.z;
+                w = y.z - z.y; qx = tt; qy = x.y + y.x; qz = z.x + x.z;
+            } else {
+                tt = 1 - x.x + y.y - z.z;
+                w = z.x - x.z; qx = x.y + y.x; qy = tt; qz = y.z + z.y;
+            }
+        } else {
+            if (x.x < -y.y) {
+                tt = 1 - x.x - y.y + z.z;
+                w = x.y - y.x; qx = z.x + x.z; qy = y.z + z.y; qz = tt;
+            } else {
+                tt = 1 + x.x + y.y + z.z;
+                w = tt; qx = y.z - z.y; qy = z.x - x.z; qz = x.y - y.x;
+            }
+        }
+        float s = 0.5f / std::sqrt(tt);
+        w *= s; qx *= s; qy *= s; qz *= s;
+        float inv = 1.0f / std::sqrt(w * w + qx * qx + qy * qy + qz * qz);
+        out[4 * v + 0] = w * inv;
+        out[4 * v + 1] = -(qx * inv);
+        out[4 * v + 2] = -(qy * inv);
+        out[4 * v + 3] = -(qz * inv);
+    }
 }
 
 void oracle_bary_slerp(const float* q0, const float* q1, const float* q2, float a, float b,

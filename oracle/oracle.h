@@ -112,6 +112,9 @@ void oracle_trace(const oracle_scene* scene, const oracle_bvh* bvh,
                   const float* rays, uint32_t n,
                   uint32_t* out_key, uint32_t* out_prim, float* out_t, float* out_bary,
                   uint32_t threads);
+/* Inner nodes entered and triangles tested by oracle_trace / oracle_render
+ * since the last reset (out[2]). */
+void oracle_trace_counters(uint64_t* out, int reset);
 /* The reference "Linear" accelerator: brute force, triangle order, strict <. */
 void oracle_trace_linear(const oracle_scene* scene, const float* rays, uint32_t n,
                          uint32_t* out_key, uint32_t* out_prim, float* out_t, float* out_bary,
@@ -126,6 +129,12 @@ uint64_t oracle_render(const oracle_scene* scene, const oracle_bvh* bvh,
 uint64_t oracle_render_f64(const oracle_scene* scene, const oracle_bvh* bvh,
                            const oracle_camera* cam, const oracle_options* opt,
                            double* sample_rgb);
+
+/* Per-vertex tangent-space rotations (w,x,y,z) of a triangle mesh, as the
+ * triangle loader builds them (GPUPrimitiveTriangle.cpp:160-320).  uvs may
+ * be NULL: each triangle then uses (0,0),(1,0),(0,1). */
+void oracle_build_tbn(const float* pos, const float* nrm, const float* uvs, const uint32_t* idx,
+                      uint32_t vertex_count, uint32_t tri_count, float* tbn_out);
 
 /* Single-vertex BxDF probes used by the golden-vector tests. */
 void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi,

@@ -210,3 +210,53 @@ class OracleScene:
         fn = lib.oracle_render_f64 if fp64 else lib.oracle_render
         rays = fn(C.byref(self.c), self.bvh, C.byref(cam), C.byref(o), _p(out))
         return out, int(rays)
+
+
+def scene_tables(scene) -> dict:
+    """HitKeys and material tables of a scene, assigned as the product's loader
+    does: batch per material type (1 Lambert, 2 Metal, 3 Refract, 4 light),
+    ids in material order, one primitive light per light triangle in triangle
+    order (GPULightPrimitive: one GPULight per primitive)."""
+    mats = scene.materials
+    key = np.zeros(len(mats), np.uint32)
+    lam, met, ref, refm = [], [], [], []
+    for i, m in enumerate(mats):
+        t = int(m["type"])
+        if t == 1:
+            key[i] = (1 << 24) | len(lam)
+            lam.append(np.asarray(m["albedo"], np.float32))
+        elif t == 2:
+            key[i] = (2 << 24) | len(met)
+            met.append(np.concatenate([m["eta"], m["k"], m["specular"], [m["roughness"]]])
+                       .astype(np.float32))
+        elif t == 3:
+            key[i] = (3 << 24) | len(ref)
+            ref.append(np.asarray(m["albedo"], np.float32))
+            refm.append(int(m["medium"]))
+    tm = np.asarray(scene.tri_material, np.uint32)
+    tri_key = key[tm].copy()
+    light_tris = np.nonzero(np.array([int(mats[i]["type"]) == 4 for i in tm]))[0] \
+        if len(tm) < 200000 else np.nonzero(np.isin(tm, [i for i, m in enumerate(mats)
+                                                         if int(m["type"]) == 4]))[0]
+    light_rad = np.array([mats[tm[t]]["radiance"] for t in light_tris], np.float32).reshape(-1, 3)
+    tri_key[light_tris] = (4 << 24) | np.arange(len(light_tris), dtype=np.uint32)
+    z3 = np.zeros((0, 3), np.float32)
+    return {"tri_key": tri_key,
+            "lambert": np.array(lam, np.float32).reshape(-1, 3) if lam else z3,
+            "metal": np.array(met, np.float32).reshape(-1, 10) if met else np.zeros((0, 10),
+                                                                                  np.float32),
+            "refract": np.array(ref, np.float32).reshape(-1, 3) if ref else z3,
+            "refract_medium": np.array(refm, np.uint32),
+            "light_radiance": light_rad,
+            "light_prim": light_tris.astype(np.uint32)}
+
+
+def build_tbn(scene) -> np.ndarray:
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    nrm = np.ascontiguousarray(scene.normals, np.float32)
+    uvs = None if scene.uvs is None else np.ascontiguousarray(scene.uvs, np.float32)
+    idx = np.ascontiguousarray(scene.indices, np.uint32)
+    out = np.zeros((pos.shape[0], 4), np.float32)
+    lib.oracle_build_tbn(_p(pos), _p(nrm), _p(uvs), _p(idx), C.c_uint32(pos.shape[0]),
+                         C.c_uint32(idx.shape[0]), _p(out))
+    return out

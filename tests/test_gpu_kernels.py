@@ -23,8 +23,9 @@ def test_portable_math_bit_identical(cuda, oracle):
     rng = np.random.default_rng(3)
     x = np.concatenate([np.linspace(0, 2 * np.pi, 50001), rng.uniform(-8, 8, 50000),
                         [0.0, np.pi / 4, np.pi / 2, np.pi, 1e-30]]).astype(np.float32)
-    y = np.concatenate([np.linspace(-1, 1, 50001), rng.uniform(-1, 1, 50004)]).astype(np.float32)
+    y = np.concatenate([np.linspace(-1, 1, 50001), rng.uniform(-1, 1, 50005)]).astype(np.float32)
     n = x.shape[0]
+    assert y.shape[0] == n
     dx, dy = _dev(torch, x), _dev(torch, y)
     sc = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
     ac = torch.zeros(n, dtype=torch.float32, device="cuda")
