@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -1388,6 +1389,63 @@ void oracle_build_tbn(const float* pos, const float* nrm, const float* uvs, cons
         out[4 * v + 2] = -(qy * inv);
         out[4 * v + 3] = -(qz * inv);
     }
+}
+
+// Single-function probes for the golden-vector tests.  in / out layouts per
+// name are documented in oracle.h.  Returns 0, or -1 for an unknown name.
+int oracle_probe(const char* name, const float* in, float* out) {
+    using F3 = V3<float>;
+    using Q = Q4<float>;
+    auto v = [&](int i) { return F3(in[i], in[i + 1], in[i + 2]); };
+    auto q = [&](int i) { return Q{in[i], in[i + 1], in[i + 2], in[i + 3]}; };
+    auto w3 = [&](int i, F3 a) { out[i] = a.x; out[i + 1] = a.y; out[i + 2] = a.z; };
+    auto w4 = [&](int i, Q a) { out[i] = a.w; out[i + 1] = a.x; out[i + 2] = a.y; out[i + 3] = a.z; };
+    std::string n(name);
+    if (n == "hemi_cosine") {  // xi0 xi1 -> dir3 pdf
+        float pdf;
+        F3 d = hemi_cosine(in[0], in[1], pdf);
+        w3(0, d);
+        out[3] = pdf;
+    } else if (n == "reflect") {  // d3 n3 -> r3 (Ray::Reflect)
+        F3 d = v(0), nn = v(3);
+        w3(0, 2.0f * dot(d, nn) * nn - d);
+    } else if (n == "refract") {  // d3 n3 from to -> ok r3 (Ray::Refract)
+        F3 d = v(0), nn = v(3);
+        float from = in[6], to = in[7];
+        float ratio = from / to;
+        float cosIn = dot(nn, d);
+        float sinInSqr = std::fmax(0.0f, 1.0f - cosIn * cosIn);
+        float sinOutSqr = ratio * ratio * sinInSqr;
+        float cosOut = std::sqrt(std::fmax(0.0f, 1.0f - sinOutSqr));
+        out[0] = (sinOutSqr >= 1.0f) ? 0.0f : 1.0f;
+        if (out[0] != 0.0f) w3(1, ratio * (-d) + (ratio * cosIn - cosOut) * nn);
+    } else if (n == "quat_rotate") {  // q4 v3 -> v3
+        w3(0, qrotate(q(0), v(4)));
+    } else if (n == "quat_mul") {  // q4 q4 -> q4
+        w4(0, qmul(q(0), q(4)));
+    } else if (n == "dggx") {  // ndh alpha -> d
+        out[0] = dggx(in[0], in[1]);
+    } else if (n == "gsmith_corr") {  // wo3 wi3 alpha -> g
+        out[0] = g_smith_corr(v(0), v(3), in[6]);
+    } else if (n == "gsmith_single") {  // v3 alpha -> g
+        out[0] = g_smith_single(v(0), in[3]);
+    } else if (n == "fresnel_conductor") {  // cos eta3 k3 -> f3
+        w3(0, fresnel_conductor(in[0], v(1), v(4)));
+    } else if (n == "fresnel_dielectric") {  // cos iorIn iorOut -> f
+        out[0] = fresnel_dielectric(in[0], in[1], in[2]);
+    } else if (n == "vndf_sample") {  // v3 alpha xi0 xi1 -> h3 pdf
+        float pdf;
+        w3(0, vndf_sample(pdf, v(0), in[3], in[4], in[5]));
+        out[3] = pdf;
+    } else if (n == "vndf_pdf") {  // v3 h3 alpha -> pdf
+        out[0] = vndf_pdf(v(0), v(3), in[6]);
+    } else if (n == "power_heuristic") {  // n0 p0 n1 p1
+        float w0 = in[0] * in[1], w1 = in[2] * in[3];
+        out[0] = (w0 * w0) / (w0 * w0 + w1 * w1);
+    } else {
+        return -1;
+    }
+    return 0;
 }
 
 void oracle_bary_slerp(const float* q0, const float* q1, const float* q2, float a, float b,

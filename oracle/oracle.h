@@ -142,6 +142,11 @@ void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi,
                         uint32_t backside, float from_ior, float to_ior,
                         const float* xi, float* out_dir, float* out_pos,
                         float* out_refl, float* out_pdf);
+/* Named single-function probes (hemi_cosine, reflect, refract, quat_rotate,
+ * quat_mul, dggx, gsmith_corr, gsmith_single, fresnel_conductor,
+ * fresnel_dielectric, vndf_sample, vndf_pdf, power_heuristic); argument
+ * layouts are listed next to each case in oracle.cpp.  0 ok, -1 unknown. */
+int oracle_probe(const char* name, const float* in, float* out);
 void oracle_bary_slerp(const float* q0, const float* q1, const float* q2,
                        float a, float b, float* out);
 void oracle_nudge(const float* p, const float* dir, float* out);

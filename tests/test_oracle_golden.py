@@ -1,0 +1,163 @@
+"""The CPU oracle against golden vectors produced by the MRay reference's own
+code (tests/golden/make_golden.py, reference routines compiled from the MRay
+sources).  This pins the oracle before it is used as the checker of the CUDA
+path.
+
+Bit-exact: Morton codes, LBVH topology and AABBs, ray/triangle intersection,
+Nudge, Reflect/Refract, quaternion products, Fresnel, GGX D/G, VNDF pdf.
+Within a stated tolerance: routines that go through sin/cos/acos, where the
+oracle (like the CUDA path) uses its own portable polynomial instead of libm.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+G = dict(np.load(Path(__file__).resolve().parent / "golden" / "reference_vectors.npz"))
+# sin/cos/acos differences of up to ~2 ulp, amplified by at most ~10x in VNDF
+TRANSCENDENTAL_ATOL = 2e-6
+VNDF_ATOL = 2e-5
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _probe(oracle, name, rows, nout):
+    out = np.zeros((rows.shape[0], nout), np.float32)
+    for i, r in enumerate(rows):
+        r = np.ascontiguousarray(r, np.float32)
+        o = np.zeros(nout, np.float32)
+        assert oracle.lib.oracle_probe(name.encode(), _p(r), _p(o)) == 0
+        out[i] = o
+    return out
+
+
+def test_morton3d(oracle):
+    got = np.array([oracle.lib.oracle_morton3d(*map(int, r)) for r in G["morton3d_in"]],
+                   np.uint64)
+    assert np.array_equal(got, G["morton3d_out"])
+
+
+def test_morton_codes_of_centroids(oracle):
+    aabb = G["morton_aabb"]
+    n = aabb.shape[0]
+    # triangles whose AABBs are exactly the stored boxes
+    pos = np.zeros((3 * n, 3), np.float32)
+    pos[0::3], pos[1::3], pos[2::3] = aabb[:, :3], aabb[:, 3:], aabb[:, :3]
+    a, ext, delta, codes = oracle.morton_codes(pos, np.arange(3 * n, dtype=np.uint32).reshape(n, 3))
+    assert np.array_equal(a, aabb)
+    assert np.array_equal(ext, G["morton_extent"])
+    assert np.float32(delta) == G["morton_delta"][0]
+    assert np.array_equal(codes, G["morton_codes"])
+
+
+@pytest.mark.parametrize("tag", ["lbvh2", "lbvh3", "lbvh257", "lbvh2000"])
+def test_lbvh_topology_and_boxes(oracle, tag):
+    r = oracle.lbvh(G[f"{tag}_codes"], G[f"{tag}_order"], G[f"{tag}_leaf_aabb"])
+    assert r["status"] == 0
+    assert r["root"][0] == G[f"{tag}_root"][0]
+    assert np.array_equal(r["left"], G[f"{tag}_left"])
+    assert np.array_equal(r["right"], G[f"{tag}_right"])
+    assert np.array_equal(r["parent"], G[f"{tag}_parent"])
+    assert np.array_equal(r["inner"], G[f"{tag}_inner"])
+
+
+def test_ray_triangle(oracle):
+    n = G["tri_hit"].shape[0]
+    for i in range(n):
+        t = np.zeros(1, np.float32)
+        b = np.zeros(3, np.float32)
+        p = [np.ascontiguousarray(G["tri_p"][i, k]) for k in range(3)]
+        h = oracle.lib.oracle_intersect_tri(_p(np.ascontiguousarray(G["tri_ro"][i])),
+                                            _p(np.ascontiguousarray(G["tri_rd"][i])), _p(p[0]),
+                                            _p(p[1]), _p(p[2]), int(G["tri_cull"][i]), _p(t), _p(b))
+        assert h == G["tri_hit"][i], i
+        if h:
+            assert t[0] == G["tri_t"][i] and np.array_equal(b, G["tri_bary"][i]), i
+    assert G["tri_hit"].sum() > n // 10
+
+
+def test_nudge(oracle):
+    for i in range(G["nudge_pos"].shape[0]):
+        o = np.zeros(3, np.float32)
+        oracle.lib.oracle_nudge(_p(np.ascontiguousarray(G["nudge_pos"][i])),
+                                _p(np.ascontiguousarray(G["nudge_dir"][i])), _p(o))
+        assert np.array_equal(o.view(np.uint32), G["nudge_out"][i].view(np.uint32)), i
+
+
+def test_reflect_refract(oracle):
+    rows = np.concatenate([G["rr_d"], G["rr_n"], G["rr_ior"]], 1)
+    refl = _probe(oracle, "reflect", rows, 3)
+    assert np.array_equal(refl, G["reflect_out"])
+    refr = _probe(oracle, "refract", rows, 4)
+    ok = G["refract_ok"] == 1
+    assert np.array_equal(refr[:, 0] == 1.0, ok)
+    assert np.array_equal(refr[ok, 1:], G["refract_out"][ok])
+
+
+def test_quaternion_product_and_rotation(oracle):
+    mul = _probe(oracle, "quat_mul", np.concatenate([G["q_q0"], G["q_q1"]], 1), 4)
+    assert np.array_equal(mul, G["q_mul"])
+    rot = _probe(oracle, "quat_rotate", np.concatenate([G["q_q0"], G["q_v"]], 1), 3)
+    assert np.array_equal(rot, G["q_rot"])
+
+
+def test_bary_slerp_within_tolerance(oracle):
+    n = G["q_ab"].shape[0]
+    out = np.zeros((n, 4), np.float32)
+    for i in range(n):
+        o = np.zeros(4, np.float32)
+        oracle.lib.oracle_bary_slerp(_p(np.ascontiguousarray(G["q_q0"][i])),
+                                     _p(np.ascontiguousarray(G["q_q1"][i])),
+                                     _p(np.ascontiguousarray(G["q_q2"][i])),
+                                     C.c_float(G["q_ab"][i, 0]), C.c_float(G["q_ab"][i, 1]), _p(o))
+        out[i] = o
+    assert np.abs(out - G["q_slerp"]).max() < TRANSCENDENTAL_ATOL
+
+
+def test_hemi_cosine_within_tolerance(oracle):
+    out = _probe(oracle, "hemi_cosine", G["hemi_xi"], 4)
+    # z = sqrt(1 - x^2 - y^2) amplifies the sin/cos ulps at grazing angles
+    assert np.abs(out[:, :2] - G["hemi_dir"][:, :2]).max() < TRANSCENDENTAL_ATOL
+    assert np.abs(out[:, 2] - G["hemi_dir"][:, 2]).max() < VNDF_ATOL
+    assert np.abs(out[:, 3] - G["hemi_pdf"]).max() < TRANSCENDENTAL_ATOL
+
+
+def test_tangent_space_of_mesh(oracle):
+    out = np.zeros_like(G["tbn_out"])
+    pos, nrm, uv, idx = (np.ascontiguousarray(G[k]) for k in ("tbn_pos", "tbn_nrm", "tbn_uv",
+                                                              "tbn_idx"))
+    oracle.lib.oracle_build_tbn(_p(pos), _p(nrm), _p(uv), _p(idx), C.c_uint32(pos.shape[0]),
+                                C.c_uint32(idx.shape[0]), _p(out))
+    assert np.array_equal(out, G["tbn_out"])
+
+
+def test_ggx_fresnel_terms(oracle):
+    d = _probe(oracle, "dggx", G["dggx_in"], 1)[:, 0]
+    assert np.array_equal(d, G["dggx_out"])
+    gc = _probe(oracle, "gsmith_corr",
+                np.concatenate([G["gs_wo"], G["gs_wi"], G["gs_alpha"][:, None]], 1), 1)[:, 0]
+    assert np.array_equal(gc, G["gs_corr"])
+    gs = _probe(oracle, "gsmith_single",
+                np.concatenate([G["gs_wo"], G["gs_alpha"][:, None]], 1), 1)[:, 0]
+    assert np.array_equal(gs, G["gs_single"])
+    fc = _probe(oracle, "fresnel_conductor",
+                np.concatenate([G["fc_cos"][:, None], G["fc_eta"], G["fc_k"]], 1), 3)
+    assert np.array_equal(fc, G["fc_out"])
+    fd = _probe(oracle, "fresnel_dielectric", G["fd_in"], 1)[:, 0]
+    assert np.array_equal(fd, G["fd_out"])
+    vp = _probe(oracle, "vndf_pdf",
+                np.concatenate([G["gs_wo"], G["gs_wi"], G["gs_alpha"][:, None]], 1), 1)[:, 0]
+    assert np.array_equal(vp, G["vndfpdf_out"])
+    ph = _probe(oracle, "power_heuristic", G["ph_in"], 1)[:, 0]
+    assert np.array_equal(ph, G["ph_out"])
+
+
+def test_vndf_sample_within_tolerance(oracle):
+    rows = np.concatenate([G["vndf_v"], G["vndf_alpha"][:, None], G["vndf_xi"]], 1)
+    out = _probe(oracle, "vndf_sample", rows, 4)
+    assert np.abs(out[:, :3] - G["vndf_h"]).max() < VNDF_ATOL
+    rel = np.abs(out[:, 3] - G["vndf_pdf"]) / np.maximum(np.abs(G["vndf_pdf"]), 1e-6)
+    assert np.median(rel) < 1e-5 and rel.max() < 1e-2
