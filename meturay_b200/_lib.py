@@ -78,6 +78,7 @@ def _load() -> C.CDLL:
         "mrb_radix_sort_temp_bytes": (sz, [u32, i32, i32, i32]),
         "mrb_radix_sort_pairs_u64": (i32, [vp, vp, u32, i32, i32, i32, vp, sz, vp]),
         "mrb_radix_sort_pairs_u32": (i32, [vp, vp, u32, i32, i32, i32, vp, sz, vp]),
+        "mrb_radix_sort_pairs_u32_noalloc": (i32, [vp, vp, u32, i32, i32, i32, vp]),
         "mrb_lbvh_hierarchy": (i32, [vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp]),
         "mrb_partition_temp_bytes": (sz, [u32, u32]),
         "mrb_partition": (i32, [vp, u32, u32, vp, vp, vp, vp, vp, vp, sz, vp]),
