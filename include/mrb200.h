@@ -126,6 +126,14 @@ int mrb_accel_export(const mrb_scene* scene, uint64_t* codes, uint32_t* sorted_i
 int mrb_accel_hit(const mrb_scene* scene, const float* d_ray_o, const float* d_ray_d, uint32_t n,
                   uint32_t* d_key, uint32_t* d_prim, float* d_t, float* d_bary, void* stream);
 
+/* Traversal layout used by Hit and by tracers of this scene: 1 (default) =
+ * 8-wide nodes with 8-bit quantised child boxes collapsed from the LBVH,
+ * 0 = the binary LBVH nodes.  Both give the same closest distance; the
+ * primitive can differ only where two triangles report the same distance. */
+int mrb_accel_set_traversal(mrb_scene* scene, int mode);
+/* info[4]: triangles, binary inner nodes, wide nodes, traversal mode. */
+int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
+
 /* ---- tracer "PathTracer": GPUTracerI (RayLib/GPUTracerI.h:24-71) ---- */
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out);
 void mrb_tracer_destroy(mrb_tracer* t);

@@ -21,6 +21,7 @@
 #include "shade.cuh"
 #include "sort.cuh"
 #include "trace.cuh"
+#include "wide.cuh"
 
 namespace mrb {
 
@@ -220,6 +221,20 @@ struct mrb_scene {
     DBuf aTriAabb, aExtent, aCodes, aSorted, aLeft, aRight, aParent, aInner, aScratch, aRoot,
         aNodes, aTv0, aTe0, aTe1, aSortTemp;
     int rootInner = 0;
+    // 8-wide quantised traversal layout derived from the LBVH
+    DBuf wNodes, wTv0, wTe0, wTe1, wScratch;
+    uint32_t wNodeCount = 0;
+    int traversal = 1;  // 0: binary LBVH nodes, 1: 8-wide nodes
+    WideAccelDev wide() const {
+        WideAccelDev a{};
+        a.nodes = wNodes.as<WideNode>();
+        a.tv0 = wTv0.as<float4>();
+        a.te0 = wTe0.as<float4>();
+        a.te1 = wTe1.as<float4>();
+        a.nodeCount = wNodeCount;
+        a.triCount = T;
+        return a;
+    }
     SceneDev dev() const {
         SceneDev s{};
         s.vertexCount = V;
@@ -348,6 +363,14 @@ PortionTable portion_table(const mrb_tracer* t) {
     return PortionTable{p, p + 8, p + 16};
 }
 
+int trace_dispatch(const mrb_scene* sc, const float4* rayO, const float4* rayD,
+                   const uint32_t* dCount, uint32_t maxCount, const HitOut& ho, uint32_t* err,
+                   cudaStream_t st, unsigned long long* counters = nullptr) {
+    if (sc->traversal == 1 && sc->T > 1)
+        return trace_closest_wide(sc->wide(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
+    return trace_closest(sc->accel(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
+}
+
 int step_camera(mrb_tracer* t) {
     uint32_t* cnt = t->count.as<uint32_t>();
     return camera_generate(t->devCam.as<CameraDev>(), path_options(t), t->scene->baseMedium,
@@ -386,14 +409,14 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
         return 0;
     };
     if (mark(0)) return MRB_E_CUDA;
-    if ((r = trace_closest(sc->accel(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
-                           cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
+    if ((r = trace_dispatch(sc, t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(), cnt + cur,
+                            t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
         return r;
     if (mark(1) || lap(1, 0)) return MRB_E_CUDA;
     if (workCounters) {
-        if ((r = trace_closest(sc->accel(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
-                               cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream,
-                               workCounters)))
+        if ((r = trace_dispatch(sc, t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+                                cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream,
+                                workCounters)))
             return r;
     }
     if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
@@ -681,6 +704,20 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
                          s->dCull.as<uint8_t>(), s->aSorted.as<uint32_t>(), n, s->aTv0.as<float4>(),
                          s->aTe0.as<float4>(), s->aTe1.as<float4>(), st)))
         return r;
+    if (n >= 2) {
+        if ((r = s->wNodes.alloc((n - 1) * sizeof(WideNode))) || (r = s->wTv0.alloc(size_t(n) * 16)) ||
+            (r = s->wTe0.alloc(size_t(n) * 16)) || (r = s->wTe1.alloc(size_t(n) * 16)) ||
+            (r = s->wScratch.alloc(wide_scratch_bytes(n))))
+            return r;
+        WideBuildIn wi{n, s->aRoot.as<uint32_t>(), s->aLeft.as<uint32_t>(), s->aRight.as<uint32_t>(),
+                       s->aInner.as<float>(), s->aTriAabb.as<float>(), s->aSorted.as<uint32_t>(),
+                       s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>(),
+                       s->dCull.as<uint8_t>()};
+        if ((r = wide_build(wi, s->wNodes.as<WideNode>(), s->wTv0.as<float4>(), s->wTe0.as<float4>(),
+                            s->wTe1.as<float4>(), s->wScratch.p, &s->wNodeCount, st)))
+            return r;
+        s->wScratch.release();
+    }
     uint32_t root = 0, err = 0;
     MRB_CUDA(cudaMemcpyAsync(&root, s->aRoot.p, 4, cudaMemcpyDeviceToHost, st));
     MRB_CUDA(cudaMemcpyAsync(&err, radix_sort_error_flag(s->aSortTemp.p, n), 4,
@@ -729,9 +766,27 @@ int mrb_accel_hit(const mrb_scene* s, const float* rayO, const float* rayD, uint
         if (flag.alloc(16)) return MRB_E_OOM;
         MRB_CUDA(cudaMemset(flag.p, 0, 16));
     }
-    return trace_closest(s->accel(), reinterpret_cast<const float4*>(rayO),
-                         reinterpret_cast<const float4*>(rayD), nullptr, n, ho,
-                         flag.as<uint32_t>(), static_cast<cudaStream_t>(stream));
+    return trace_dispatch(s, reinterpret_cast<const float4*>(rayO),
+                          reinterpret_cast<const float4*>(rayD), nullptr, n, ho,
+                          flag.as<uint32_t>(), static_cast<cudaStream_t>(stream));
+}
+
+int mrb_accel_set_traversal(mrb_scene* s, int mode) {
+    if (!s || (mode != 0 && mode != 1)) {
+        set_error("traversal mode must be 0 (binary) or 1 (8-wide)");
+        return MRB_E_ARG;
+    }
+    s->traversal = mode;
+    return 0;
+}
+
+int mrb_accel_info(const mrb_scene* s, uint32_t* info) {
+    if (!s || !info) return MRB_E_ARG;
+    info[0] = s->T;
+    info[1] = s->T > 1 ? s->T - 1 : 0;
+    info[2] = s->wNodeCount;
+    info[3] = static_cast<uint32_t>(s->traversal);
+    return 0;
 }
 
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out) {

@@ -1,0 +1,449 @@
+// 8-wide BVH with quantised child boxes, collapsed on the GPU from the LBVH,
+// and its closest-hit traversal.
+//
+// Why: the binary traversal is bound by the L1/LSU data path (64 bytes per
+// two child boxes).  A wide node carries eight child boxes quantised to 8
+// bits per plane relative to the node's own box: 80 bytes for up to eight
+// children.  Per box test that is 10 bytes instead of 32, and one node fetch
+// replaces about three binary levels.
+//
+// Collapse (top-down, one launch per level of the wide tree): a wide node is
+// formed from a binary node by repeatedly opening the internal child with
+// the largest surface area until it has eight children or only leaves.
+// Internal children get consecutive wide-node slots and leaf children
+// consecutive triangle slots; slots are handed out by atomic counters per
+// level, so the first 1 + 8 + 64 slots are the top three levels.  The
+// binary LBVH (reference numbering) is unchanged: this is a traversal layout
+// derived from it.
+//
+// Node (80 B = five 16-byte loads):
+//   n0 = (box.lo.xyz, exps): exps = ex | ey << 8 | ez << 16 | imask << 24
+//   n1 = (childBase, triBase, meta[0..3], meta[4..7])
+//   n2 = (qlo.x[0..7], qlo.y[0..7]), n3 = (qlo.z[0..7], qhi.x[0..7]),
+//   n4 = (qhi.y[0..7], qhi.z[0..7])
+// meta per slot: 0 empty, 0x80|rank internal child, 0x40|rank leaf child.
+// A child plane decodes as lo + q * 2^(e-127); quantisation rounds outward,
+// so decoded boxes contain the exact child boxes.
+#include "../../include/mrb200.h"
+#include "common.cuh"
+#include "wide.cuh"
+
+namespace mrb {
+
+namespace {
+
+struct WorkItem {
+    uint32_t bnode;  // binary node (global index, >= n inner)
+    uint32_t slot;   // wide node slot
+};
+
+__device__ __forceinline__ void child_box(uint32_t g, uint32_t n, const float* __restrict__ inner,
+                                          const float* __restrict__ triAabb,
+                                          const uint32_t* __restrict__ sortedIdx, float lo[3],
+                                          float hi[3]) {
+    const float* b = (g < n) ? triAabb + 6 * size_t(sortedIdx[g]) : inner + 6 * size_t(g - n);
+    for (int c = 0; c < 3; c++) {
+        lo[c] = b[c];
+        hi[c] = b[3 + c];
+    }
+}
+
+__device__ __forceinline__ float half_area(const float lo[3], const float hi[3]) {
+    float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Exponent byte e (scale 2^(e-127)) so that extent / scale <= 255.
+__device__ __forceinline__ uint32_t quant_exponent(float extent) {
+    if (!(extent > 0.0f)) return 1u;  // degenerate axis: planes decode to lo exactly
+    float x = extent / 255.0f;
+    uint32_t bits = __float_as_uint(x);
+    uint32_t e = (bits >> 23) & 0xFFu;
+    if (bits & 0x7FFFFFu) e += 1u;  // round up to a power of two
+    // make sure the rounded division cannot exceed 255
+    while (e < 254u && extent / __uint_as_float(e << 23) > 255.0f) e++;
+    return e < 1u ? 1u : e;
+}
+
+__global__ void __launch_bounds__(128) k_collapse(
+    const WorkItem* __restrict__ qin, const uint32_t* __restrict__ qinCount, WorkItem* qout,
+    uint32_t* qoutCount, uint32_t* nodeCounter, uint32_t* triCounter, uint32_t n,
+    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+    const float* __restrict__ inner, const float* __restrict__ triAabb,
+    const uint32_t* __restrict__ sortedIdx, const float* __restrict__ pos,
+    const uint32_t* __restrict__ idx, const uint32_t* __restrict__ key,
+    const uint8_t* __restrict__ cull, WideNode* nodes, float4* tv0, float4* te0, float4* te1) {
+    const uint32_t count = *qinCount;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
+         w += gridDim.x * blockDim.x) {
+        const WorkItem it = qin[w];
+        uint32_t ch[8];
+        float area[8];
+        int nc = 2;
+        ch[0] = left[it.bnode - n];
+        ch[1] = right[it.bnode - n];
+        for (int k = 0; k < 2; k++) {
+            float lo[3], hi[3];
+            child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
+            area[k] = (ch[k] >= n) ? half_area(lo, hi) : -1.0f;
+        }
+        // open the largest internal child until eight children
+        while (nc < 8) {
+            int best = -1;
+            for (int k = 0; k < nc; k++)
+                if (ch[k] >= n && (best < 0 || area[k] > area[best])) best = k;
+            if (best < 0) break;
+            const uint32_t b = ch[best];
+            const uint32_t c0 = left[b - n], c1 = right[b - n];
+            ch[best] = c0;
+            ch[nc] = c1;
+            float lo[3], hi[3];
+            child_box(c0, n, inner, triAabb, sortedIdx, lo, hi);
+            area[best] = (c0 >= n) ? half_area(lo, hi) : -1.0f;
+            child_box(c1, n, inner, triAabb, sortedIdx, lo, hi);
+            area[nc] = (c1 >= n) ? half_area(lo, hi) : -1.0f;
+            nc++;
+        }
+        int nInner = 0, nLeaf = 0;
+        for (int k = 0; k < nc; k++) (ch[k] >= n) ? nInner++ : nLeaf++;
+        const uint32_t childBase = nInner ? atomicAdd(nodeCounter, uint32_t(nInner)) : 0u;
+        const uint32_t triBase = nLeaf ? atomicAdd(triCounter, uint32_t(nLeaf)) : 0u;
+        const uint32_t qbase = nInner ? atomicAdd(qoutCount, uint32_t(nInner)) : 0u;
+
+        // node box = the binary node's box
+        float blo[3], bhi[3];
+        child_box(it.bnode, n, inner, triAabb, sortedIdx, blo, bhi);
+        uint32_t e[3];
+        float scale[3];
+        for (int c = 0; c < 3; c++) {
+            e[c] = quant_exponent(bhi[c] - blo[c]);
+            scale[c] = __uint_as_float(e[c] << 23);
+        }
+        uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint8_t q[6][8];
+        for (int c = 0; c < 6; c++)
+            for (int k = 0; k < 8; k++) q[c][k] = (c < 3) ? 255 : 0;  // empty slot never hits
+        uint32_t imask = 0;
+        int ri = 0, rl = 0;
+        for (int k = 0; k < nc; k++) {
+            float lo[3], hi[3];
+            child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
+            for (int c = 0; c < 3; c++) {
+                // outward rounding in double: exact for float inputs and
+                // power-of-two scales
+                double ql = floor((double(lo[c]) - double(blo[c])) / double(scale[c]));
+                double qh = ceil((double(hi[c]) - double(blo[c])) / double(scale[c]));
+                ql = ql < 0.0 ? 0.0 : (ql > 255.0 ? 255.0 : ql);
+                qh = qh < 0.0 ? 0.0 : (qh > 255.0 ? 255.0 : qh);
+                q[c][k] = static_cast<uint8_t>(ql);
+                q[3 + c][k] = static_cast<uint8_t>(qh);
+            }
+            if (ch[k] >= n) {
+                meta[k] = uint8_t(0x80u | ri);
+                imask |= 1u << k;
+                qout[qbase + ri] = WorkItem{ch[k], childBase + uint32_t(ri)};
+                ri++;
+            } else {
+                meta[k] = uint8_t(0x40u | rl);
+                // leaf: the triangle, reordered into this node's leaf block
+                const uint32_t t = sortedIdx[ch[k]];
+                const uint32_t s = triBase + uint32_t(rl);
+                const uint32_t i0 = idx[3 * size_t(t)], i1 = idx[3 * size_t(t) + 1],
+                               i2 = idx[3 * size_t(t) + 2];
+                const V3 p0 = ld3(pos + 3 * size_t(i0)), p1 = ld3(pos + 3 * size_t(i1)),
+                         p2 = ld3(pos + 3 * size_t(i2));
+                const V3 e0 = p1 - p0, e1 = p2 - p0;
+                tv0[s] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(t));
+                te0[s] = make_float4(e0.x, e0.y, e0.z, __uint_as_float(key[t]));
+                te1[s] = make_float4(e1.x, e1.y, e1.z,
+                                     __uint_as_float(cull ? uint32_t(cull[t]) : 0u));
+                rl++;
+            }
+        }
+        WideNode nd;
+        nd.n0 = make_float4(blo[0], blo[1], blo[2],
+                            __uint_as_float(e[0] | (e[1] << 8) | (e[2] << 16) | (imask << 24)));
+        uint32_t m0 = meta[0] | (meta[1] << 8) | (meta[2] << 16) | (uint32_t(meta[3]) << 24);
+        uint32_t m1 = meta[4] | (meta[5] << 8) | (meta[6] << 16) | (uint32_t(meta[7]) << 24);
+        nd.n1 = make_uint4(childBase, triBase, m0, m1);
+        auto pack = [&](int c, int k0) {
+            return q[c][k0] | (q[c][k0 + 1] << 8) | (q[c][k0 + 2] << 16) |
+                   (uint32_t(q[c][k0 + 3]) << 24);
+        };
+        nd.n2 = make_uint4(pack(0, 0), pack(0, 4), pack(1, 0), pack(1, 4));
+        nd.n3 = make_uint4(pack(2, 0), pack(2, 4), pack(3, 0), pack(3, 4));
+        nd.n4 = make_uint4(pack(4, 0), pack(4, 4), pack(5, 0), pack(5, 4));
+        nodes[it.slot] = nd;
+    }
+}
+
+__global__ void k_collapse_init(WorkItem* q0, uint32_t* counters, const uint32_t* root) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        q0[0] = WorkItem{*root, 0u};
+        counters[0] = 1;  // queue 0 count
+        counters[1] = 0;  // queue 1 count
+        counters[2] = 1;  // node counter (slot 0 = root)
+        counters[3] = 0;  // triangle counter
+    }
+}
+
+__global__ void k_reset_count(uint32_t* c) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *c = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Traversal
+// ---------------------------------------------------------------------------
+constexpr int kCachedNodes = 73;  // 1 + 8 + 64: the top three levels
+constexpr int kWideStack = 128;
+
+__device__ __forceinline__ float safe_dir(float d) {
+    return (fabsf(d) > 1e-20f) ? d : copysignf(1e-20f, d);
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
+
+__device__ __forceinline__ void cas(uint32_t& a, uint32_t& b) {
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+// Optimal 19-comparator network for eight keys (ascending).
+__device__ __forceinline__ void sort8(uint32_t k[8]) {
+    cas(k[0], k[2]); cas(k[1], k[3]); cas(k[4], k[6]); cas(k[5], k[7]);
+    cas(k[0], k[4]); cas(k[1], k[5]); cas(k[2], k[6]); cas(k[3], k[7]);
+    cas(k[0], k[1]); cas(k[2], k[3]); cas(k[4], k[5]); cas(k[6], k[7]);
+    cas(k[2], k[4]); cas(k[3], k[5]);
+    cas(k[1], k[4]); cas(k[3], k[6]);
+    cas(k[1], k[2]); cas(k[3], k[4]); cas(k[5], k[6]);
+}
+
+__device__ __forceinline__ void tri_test(const WideAccelDev& acc, uint32_t s, V3 o, V3 d,
+                                         float tmin, float& closest, int& hitTri, float& hb0,
+                                         float& hb1) {
+    float4 a = __ldg(acc.tv0 + s), b = __ldg(acc.te0 + s), c = __ldg(acc.te1 + s);
+    V3 v0 = {a.x, a.y, a.z}, e0 = {b.x, b.y, b.z}, e1 = {c.x, c.y, c.z};
+    bool cull = __float_as_uint(c.w) != 0u;
+    V3 p = cross(d, e1);
+    float det = dot(e0, p);
+    if ((cull && (det < 1.0e-7f)) || (fabsf(det) < 1.0e-7f)) return;
+    float invDet = 1.0f / det;
+    V3 tv = o - v0;
+    float u = dot(tv, p) * invDet;
+    if (u < 0.0f || u > 1.0f) return;
+    V3 q = cross(tv, e0);
+    float v = dot(d, q) * invDet;
+    if ((v < 0.0f) || (v + u) > 1.0f) return;
+    float t = dot(e1, q) * invDet;
+    if (t <= 1.0e-7f) return;
+    if (t >= tmin && t < closest) {
+        closest = t;
+        hitTri = static_cast<int>(s);
+        hb0 = 1.0f - u - v;
+        hb1 = u;
+    }
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(128) k_trace_wide(WideAccelDev acc,
+                                                    const float4* __restrict__ rayO,
+                                                    const float4* __restrict__ rayD,
+                                                    const uint32_t* __restrict__ dCount,
+                                                    uint32_t hCount, HitOut out,
+                                                    uint32_t* errorFlag,
+                                                    unsigned long long* counters) {
+    __shared__ WideNode sNodes[kCachedNodes];
+    const int cached = acc.nodeCount < uint32_t(kCachedNodes) ? int(acc.nodeCount) : kCachedNodes;
+    for (int i = threadIdx.x; i < cached * 5; i += blockDim.x)
+        reinterpret_cast<uint4*>(sNodes)[i] = __ldg(reinterpret_cast<const uint4*>(acc.nodes) + i);
+    __syncthreads();
+    const uint32_t n = dCount ? *dCount : hCount;
+    uint32_t nodeVisits = 0, triTests = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 ro = rayO[i], rd = rayD[i];
+        const V3 o = {ro.x, ro.y, ro.z}, d = {rd.x, rd.y, rd.z};
+        const float tmin = ro.w;
+        float closest = rd.w;
+        int hitTri = -1;
+        float hb0 = 0.0f, hb1 = 0.0f;
+        if (acc.triCount == 1) {
+            if (kCount) triTests++;
+            tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
+        } else if (acc.triCount > 1) {
+            const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
+            uint2 stack[kWideStack];  // (node, entry distance bits)
+            int sp = 0;
+            int node = 0;
+            while (node >= 0) {
+                if (kCount) nodeVisits++;
+                uint4 w0, w1, w2, w3, w4;
+                if (node < cached) {
+                    const uint4* s = reinterpret_cast<const uint4*>(sNodes + node);
+                    w0 = s[0]; w1 = s[1]; w2 = s[2]; w3 = s[3]; w4 = s[4];
+                } else {
+                    const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
+                    w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
+                    w4 = __ldg(g + 4);
+                }
+                const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
+                            lz = __uint_as_float(w0.z);
+                const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+                const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+                const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+                // t = (lo + q*s - o) * inv = q * (s*inv) + (lo - o) * inv
+                const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
+                const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
+                            bz = (lz - o.z) * inv.z;
+                const uint32_t childBase = w1.x, triBase = w1.y;
+                // near/far plane choice per axis from the ray direction
+                const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
+                const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
+                const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
+                const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
+                const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
+                const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
+                // internal children that are hit, keyed by entry distance:
+                // (distance bits with the low three cleared) | slot
+                uint32_t key[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    key[k] = 0xFFFFFFFFu;
+                    const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
+                    if (meta == 0u) continue;
+                    const int kk = k & 3;
+                    const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
+                    const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
+                    const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
+                    const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
+                    const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
+                    const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
+                    const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+                    const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
+                    if (!(tn <= tf)) continue;
+                    if (meta & 0x40u) {  // leaf: test the triangle right away
+                        if (kCount) triTests++;
+                        tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
+                                 hb0, hb1);
+                    } else {
+                        key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
+                    }
+                }
+                sort8(key);
+                // push the farther hits (farthest first), enter the nearest
+                node = -1;
+#pragma unroll
+                for (int j = 7; j >= 0; j--) {
+                    if (key[j] == 0xFFFFFFFFu) continue;
+                    const float tn = __uint_as_float(key[j] & ~7u);
+                    if (tn > closest) continue;
+                    const uint32_t slot = key[j] & 7u;
+                    const uint32_t meta = byte_of(slot < 4 ? w1.z : w1.w, int(slot & 3u));
+                    const uint32_t child = childBase + (meta & 0x3Fu);
+                    if (j == 0) {
+                        node = int(child);
+                    } else if (sp < kWideStack) {
+                        stack[sp++] = make_uint2(child, key[j] & ~7u);
+                    } else {
+                        atomicExch(errorFlag, 3u);
+                    }
+                }
+                if (node < 0) {
+                    // the nearest hit was beyond the closest triangle: fall
+                    // through to the stack
+                }
+                while (node < 0 && sp > 0) {
+                    const uint2 e = stack[--sp];
+                    if (__uint_as_float(e.y) <= closest) node = int(e.x);
+                }
+            }
+        }
+        if (hitTri >= 0) {
+            out.key[i] = __float_as_uint(__ldg(&acc.te0[hitTri].w));
+            out.prim[i] = __float_as_uint(__ldg(&acc.tv0[hitTri].w));
+            out.t[i] = closest;
+            out.bary[i] = make_float2(hb0, hb1);
+        } else {
+            out.key[i] = kBatchNull;
+            out.prim[i] = kInvalid;
+            out.t[i] = closest;
+            out.bary[i] = make_float2(0.0f, 0.0f);
+        }
+    }
+    if (kCount) {
+        unsigned long long a = nodeVisits, b = triTests;
+        for (int s = 16; s > 0; s >>= 1) {
+            a += __shfl_xor_sync(0xFFFFFFFFu, a, s);
+            b += __shfl_xor_sync(0xFFFFFFFFu, b, s);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 0, a);
+            atomicAdd(counters + 1, b);
+        }
+    }
+}
+
+}  // namespace
+
+size_t wide_scratch_bytes(uint32_t n) {
+    // two work queues of n items + 4 counters
+    return size_t(n + 1) * sizeof(WorkItem) * 2 + 64;
+}
+
+int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0, float4* te1,
+               void* scratch, uint32_t* nodeCountOut, cudaStream_t stream) {
+    const uint32_t n = in.n;
+    if (n < 2) {
+        set_error("wide BVH: needs at least two triangles");
+        return MRB_E_ARG;
+    }
+    WorkItem* q[2];
+    q[0] = static_cast<WorkItem*>(scratch);
+    q[1] = q[0] + (n + 1);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(q[1] + (n + 1));
+    k_collapse_init<<<1, 32, 0, stream>>>(q[0], counters, in.root);
+    MRB_CUDA(cudaGetLastError());
+    // one launch per level; the host checks for an empty queue every 8 levels
+    const uint32_t grid = std::min<uint32_t>((n + 127) / 128, 148u * 8u);
+    for (int level = 0; level < 4 * 96; level++) {
+        const int cur = level & 1;
+        k_reset_count<<<1, 32, 0, stream>>>(counters + (cur ^ 1));
+        k_collapse<<<grid, 128, 0, stream>>>(q[cur], counters + cur, q[cur ^ 1], counters + (cur ^ 1),
+                                             counters + 2, counters + 3, n, in.left, in.right,
+                                             in.inner, in.triAabb, in.sortedIdx, in.pos, in.idx,
+                                             in.key, in.cull, nodes, tv0, te0, te1);
+        MRB_CUDA(cudaGetLastError());
+        if ((level & 7) == 7) {
+            uint32_t h[4];
+            MRB_CUDA(cudaMemcpyAsync(h, counters, 16, cudaMemcpyDeviceToHost, stream));
+            MRB_CUDA(cudaStreamSynchronize(stream));
+            if (h[0] == 0 && h[1] == 0) {
+                if (h[3] != n) {
+                    set_error("wide BVH: %u of %u triangles placed", h[3], n);
+                    return MRB_E_DEVICE;
+                }
+                *nodeCountOut = h[2];
+                return 0;
+            }
+        }
+    }
+    set_error("wide BVH: collapse did not finish");
+    return MRB_E_DEVICE;
+}
+
+int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
+                       const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
+                       uint32_t* errorFlag, cudaStream_t stream, unsigned long long* counters) {
+    if (maxCount == 0) return 0;
+    uint32_t blocks = (maxCount + 127) / 128;
+    blocks = blocks < 148u * 16u ? blocks : 148u * 16u;
+    if (counters)
+        k_trace_wide<true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
+                                                       errorFlag, counters);
+    else
+        k_trace_wide<false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
+                                                        errorFlag, nullptr);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mrb

@@ -1,0 +1,49 @@
+// 8-wide quantised BVH: build from the LBVH and closest-hit traversal (see wide.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <algorithm>
+#include "common.cuh"
+#include "trace.cuh"
+
+namespace mrb {
+
+struct alignas(16) WideNode {
+    float4 n0;
+    uint4 n1, n2, n3, n4;
+};
+
+struct WideAccelDev {
+    const WideNode* nodes;
+    const float4* tv0;  // triangles in wide-leaf order: v0 | original index
+    const float4* te0;  // e0 | HitKey
+    const float4* te1;  // e1 | cull flag
+    uint32_t nodeCount;
+    uint32_t triCount;
+};
+
+struct WideBuildIn {
+    uint32_t n;                  // triangles (>= 2)
+    const uint32_t* root;        // device: global index of the LBVH root
+    const uint32_t* left;
+    const uint32_t* right;
+    const float* inner;
+    const float* triAabb;
+    const uint32_t* sortedIdx;
+    const float* pos;
+    const uint32_t* idx;
+    const uint32_t* key;
+    const uint8_t* cull;
+};
+
+size_t wide_scratch_bytes(uint32_t n);
+// Collapses the LBVH into wide nodes (at most n-1) and reorders triangles
+// into tv0/te0/te1 (n each).  Synchronises the stream every 8 levels.
+int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0, float4* te1,
+               void* scratch, uint32_t* nodeCountOut, cudaStream_t stream);
+int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
+                       const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
+                       uint32_t* errorFlag, cudaStream_t stream,
+                       unsigned long long* counters = nullptr);
+
+}  // namespace mrb

@@ -141,6 +141,16 @@ class GPUScene:
         """GPUAcceleratorGroupI::ConstructAccelerators for the LBVH group."""
         check(lib.mrb_accel_construct(self._h, stream))
 
+    def set_traversal(self, mode: int):
+        """1: 8-wide quantised nodes (default), 0: binary LBVH nodes."""
+        check(lib.mrb_accel_set_traversal(self._h, int(mode)))
+
+    def accel_info(self) -> dict:
+        info = np.zeros(4, np.uint32)
+        check(lib.mrb_accel_info(self._h, _ptr(info)))
+        return {"triangles": int(info[0]), "binary_nodes": int(info[1]),
+                "wide_nodes": int(info[2]), "traversal": int(info[3])}
+
     def export(self) -> dict:
         """Host copies of the device scene arrays, as the hot path consumes them."""
         c = self.counts
