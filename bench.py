@@ -124,6 +124,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     system = m.TracerSystem(dev)
     g = m.GPUScene(system, scene)
     g.construct_accelerators()
+    g.set_traversal(args.traversal)
     t = m.PathTracer(system, g)
     t.set_options(dict(OPTS, Seed=1 + rank))
     stream = torch.cuda.ExternalStream(t.stream)
@@ -190,9 +191,12 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
     peak, peak_kind = _peaks()
     # algorithmic bytes of the traversal: per ray 32 B in (origin/tMin,
-    # direction/tMax) + 20 B out (key, prim, t, barycentrics); per inner node
-    # visited 64 B; per triangle tested 48 B (v0, e0, e1)
-    trace_bytes = 52 * prof["rays"] + 64 * prof["node_visits"] + 48 * prof["tri_tests"]
+    # direction/tMax) + 20 B out (key, prim, t, barycentrics); per node
+    # visited 80 B (8-wide quantised) or 64 B (binary); per triangle tested
+    # 48 B (v0, e0, e1)
+    node_bytes = 80 if args.traversal == 1 else 64
+    trace_bytes = (52 * prof["rays"] + node_bytes * prof["node_visits"]
+                   + 48 * prof["tri_tests"])
     trace_s = prof["trace_ms"] / 1e3
     achieved = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
     traffic = _traffic_per_launch()
@@ -209,11 +213,14 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded clusters-1M scene)",
-        "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}",
+                       traversal="8-wide quantised BVH" if args.traversal else "binary LBVH"),
         "rays_per_step": rays / args.steps / world,
         "e2e": {"value": e2e_rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
                 "h2d_bytes_per_step": cam_bytes, "d2h_bytes_per_step": img_bytes},
-        "roofline": {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_trace_wide" if args.traversal == 1 else "k_trace",
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
                      "algorithmic_bytes_per_frame": trace_bytes,
@@ -316,6 +323,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traversal", type=int, default=1, choices=[0, 1],
+                    help="1: 8-wide quantised BVH (default), 0: binary LBVH nodes")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
