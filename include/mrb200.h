@@ -134,6 +134,25 @@ int mrb_accel_set_traversal(mrb_scene* scene, int mode);
 /* info[4]: triangles, binary inner nodes, wide nodes, traversal mode. */
 int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
 
+/* ---- sparse voxel octree of the scene (the WFPG radiance cache):
+ * AnisoSVOctreeCPU::Constrcut (AnisoSVO.cu:657-1188) with the accelerator
+ * group's EachPrimVoxelCount / VoxelizeSurfaces (GPUAcceleratorI.h:118-134,
+ * TriFunctions::Voxelize, GPUPrimitiveTriangle.h:385-620).  resolution: leaf
+ * voxels per axis, a power of two in [2, 1024] (leaf depth = log2).
+ * Needs mrb_accel_construct first (its extent bounds the octree). */
+int mrb_svo_build(mrb_scene* scene, uint32_t resolution, void* stream);
+/* info[6]: voxels before de-duplication, leaves, nodes, leaf depth,
+ * resolution, level-offset count; params[7]: cube min xyz, max xyz, leaf
+ * voxel size.  Either pointer may be NULL. */
+int mrb_svo_info(const mrb_scene* scene, uint32_t* info6, float* params7);
+/* Host copies: packed nodes (child 0-26 | parent 27-54 | child mask 55-62
+ * | children-are-leaves 63; AnisoSVO.cuh:125-151), leaf parents, sorted
+ * unique leaf Morton codes, packed leaf normals, leaf light HitKeys, level
+ * offsets (depth + 2).  NULL skips. */
+int mrb_svo_export(const mrb_scene* scene, uint64_t* nodes, uint32_t* leaf_parents,
+                   uint64_t* leaf_codes, uint32_t* leaf_normals, uint32_t* leaf_lights,
+                   uint32_t* level_offsets);
+
 /* ---- tracer "PathTracer": GPUTracerI (RayLib/GPUTracerI.h:24-71) ---- */
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out);
 void mrb_tracer_destroy(mrb_tracer* t);

@@ -59,6 +59,9 @@ def _load() -> C.CDLL:
         "mrb_accel_hit": (i32, [vp, vp, vp, u32, vp, vp, vp, vp, vp]),
         "mrb_accel_set_traversal": (i32, [vp, i32]),
         "mrb_accel_info": (i32, [vp, vp]),
+        "mrb_svo_build": (i32, [vp, u32, vp]),
+        "mrb_svo_info": (i32, [vp, vp, vp]),
+        "mrb_svo_export": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "mrb_tracer_create": (i32, [vp, vp, C.c_char_p, C.POINTER(vp)]),
         "mrb_tracer_destroy": (None, [vp]),
         "mrb_tracer_set_option": (i32, [vp, C.c_char_p, u64]),

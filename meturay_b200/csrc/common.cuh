@@ -225,6 +225,23 @@ __device__ __forceinline__ float pm_acos(float x) {
     return (x > 0.0f) ? a : (kPiF - a);
 }
 
+// asin on [0, 1] from the same series (half-angle identity above 1/2)
+__device__ __forceinline__ float pm_asin01(float z) {
+    if (z <= 0.5f) return pm_asin_poly(z);
+    return kPio2F - 2.0f * pm_asin_poly(sqrtf((1.0f - z) * 0.5f));
+}
+// atan2 from atan(a) = asin(a / sqrt(1 + a^2)) on a = min/max in [0, 1]
+__device__ __forceinline__ float pm_atan2(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    if (mx == 0.0f) return 0.0f;
+    const float a = mn / mx;
+    float r = pm_asin01(a / sqrtf(1.0f + a * a));
+    if (ay > ax) r = kPio2F - r;
+    if (x < 0.0f) r = kPiF - r;
+    return (y < 0.0f) ? -r : r;
+}
+
 // Quat::SLerp / Quat::BarySLerp (Quaternion.hpp:258-318)
 __device__ __forceinline__ Q4 slerp(Q4 s, Q4 e, float t) {
     float cosT = qdot(s, e);

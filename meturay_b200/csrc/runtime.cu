@@ -22,6 +22,7 @@
 #include "sort.cuh"
 #include "trace.cuh"
 #include "wide.cuh"
+#include "svo.cuh"
 
 namespace mrb {
 
@@ -221,6 +222,13 @@ struct mrb_scene {
     DBuf aTriAabb, aExtent, aCodes, aSorted, aLeft, aRight, aParent, aInner, aScratch, aRoot,
         aNodes, aTv0, aTe0, aTe1, aSortTemp;
     int rootInner = 0;
+    // sparse voxel octree (path-guiding radiance cache)
+    bool svoBuilt = false;
+    SvoParams svoP{};
+    SvoResult svo;
+    ~mrb_scene() {
+        if (svoBuilt) svo_free(svo);
+    }
     // 8-wide quantised traversal layout derived from the LBVH
     DBuf wNodes, wTv0, wTe0, wTe1, wScratch;
     uint32_t wNodeCount = 0;
@@ -769,6 +777,81 @@ int mrb_accel_hit(const mrb_scene* s, const float* rayO, const float* rayD, uint
     return trace_dispatch(s, reinterpret_cast<const float4*>(rayO),
                           reinterpret_cast<const float4*>(rayD), nullptr, n, ho,
                           flag.as<uint32_t>(), static_cast<cudaStream_t>(stream));
+}
+
+int mrb_svo_build(mrb_scene* s, uint32_t resolution, void* stream) {
+    if (!s || !s->built) {
+        set_error("SVO: construct the accelerator first (the scene extent comes from it)");
+        return MRB_E_STATE;
+    }
+    if (resolution < 2 || resolution > 1024 || (resolution & (resolution - 1))) {
+        set_error("SVO: resolution %u must be a power of two in [2, 1024]", resolution);
+        return MRB_E_ARG;
+    }
+    if (set_device(s->sys)) return MRB_E_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    float ext[8];
+    MRB_CUDA(cudaMemcpyAsync(ext, s->aExtent.p, 24, cudaMemcpyDeviceToHost, st));
+    MRB_CUDA(cudaStreamSynchronize(st));
+    if (s->svoBuilt) {
+        svo_free(s->svo);
+        s->svoBuilt = false;
+    }
+    s->svoP = svo_params(ext, resolution);
+    SvoBuildIn in{s->T, s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>()};
+    int r = svo_build(in, s->svoP, s->svo, st);
+    if (r) {
+        svo_free(s->svo);
+        return r;
+    }
+    s->svoBuilt = true;
+    return 0;
+}
+
+int mrb_svo_info(const mrb_scene* s, uint32_t* info, float* params) {
+    if (!s || !s->svoBuilt) {
+        set_error("SVO not built");
+        return MRB_E_STATE;
+    }
+    if (info) {
+        info[0] = s->svo.voxelCount;
+        info[1] = s->svo.leafCount;
+        info[2] = s->svo.nodeCount;
+        info[3] = s->svoP.depth;
+        info[4] = s->svoP.res;
+        info[5] = static_cast<uint32_t>(s->svo.levelOffsets.size());
+    }
+    if (params) {
+        for (int c = 0; c < 3; c++) {
+            params[c] = s->svoP.lo[c];
+            params[3 + c] = s->svoP.hi[c];
+        }
+        params[6] = s->svoP.leafVoxelSize;
+    }
+    return 0;
+}
+
+int mrb_svo_export(const mrb_scene* s, uint64_t* nodes, uint32_t* leafParents,
+                   uint64_t* leafCodes, uint32_t* leafNormal, uint32_t* leafLight,
+                   uint32_t* levelOffsets) {
+    if (!s || !s->svoBuilt) {
+        set_error("SVO not built");
+        return MRB_E_STATE;
+    }
+    const SvoResult& v = s->svo;
+    auto cp = [](void* dst, const void* src, size_t bytes) -> int {
+        if (!dst || !bytes) return 0;
+        MRB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return 0;
+    };
+    if (cp(nodes, v.nodes, size_t(v.nodeCount) * 8) || cp(leafParents, v.leafParents, size_t(v.leafCount) * 4) ||
+        cp(leafCodes, v.leafCodes, size_t(v.leafCount) * 8) ||
+        cp(leafNormal, v.leafNormal, size_t(v.leafCount) * 4) ||
+        cp(leafLight, v.leafLight, size_t(v.leafCount) * 4))
+        return MRB_E_CUDA;
+    if (levelOffsets)
+        std::memcpy(levelOffsets, v.levelOffsets.data(), v.levelOffsets.size() * 4);
+    return 0;
 }
 
 int mrb_accel_set_traversal(mrb_scene* s, int mode) {

@@ -151,6 +151,27 @@ class GPUScene:
         return {"triangles": int(info[0]), "binary_nodes": int(info[1]),
                 "wide_nodes": int(info[2]), "traversal": int(info[3])}
 
+    def build_svo(self, resolution: int):
+        """Sparse voxel octree of the scene at `resolution` leaf voxels per axis."""
+        check(lib.mrb_svo_build(self._h, int(resolution), None))
+
+    def export_svo(self) -> dict:
+        info = np.zeros(6, np.uint32)
+        params = np.zeros(7, np.float32)
+        check(lib.mrb_svo_info(self._h, _ptr(info), _ptr(params)))
+        U, N = int(info[1]), int(info[2])
+        out = {"voxels": int(info[0]), "leaves": U, "nodes_count": N, "depth": int(info[3]),
+               "resolution": int(info[4]), "lo": params[0:3].copy(), "hi": params[3:6].copy(),
+               "leaf_size": float(params[6]),
+               "nodes": np.zeros(N, np.uint64), "leaf_parents": np.zeros(U, np.uint32),
+               "leaf_codes": np.zeros(U, np.uint64), "leaf_normals": np.zeros(U, np.uint32),
+               "leaf_lights": np.zeros(U, np.uint32),
+               "level_offsets": np.zeros(int(info[5]), np.uint32)}
+        check(lib.mrb_svo_export(self._h, *[_ptr(out[k]) for k in (
+            "nodes", "leaf_parents", "leaf_codes", "leaf_normals", "leaf_lights",
+            "level_offsets")]))
+        return out
+
     def export(self) -> dict:
         """Host copies of the device scene arrays, as the hot path consumes them."""
         c = self.counts

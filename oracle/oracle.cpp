@@ -95,6 +95,21 @@ inline float pm_acos(float x) {
     return (x > 0.0f) ? a : (kPiF - a);
 }
 
+inline float pm_asin01(float z) {
+    if (z <= 0.5f) return asin_poly(z);
+    return kPio2F - 2.0f * asin_poly(std::sqrt((1.0f - z) * 0.5f));
+}
+inline float pm_atan2(float y, float x) {
+    const float ax = std::fabs(x), ay = std::fabs(y);
+    const float mx = std::fmax(ax, ay), mn = std::fmin(ax, ay);
+    if (mx == 0.0f) return 0.0f;
+    const float a = mn / mx;
+    float r = pm_asin01(a / std::sqrt(1.0f + a * a));
+    if (ay > ax) r = kPio2F - r;
+    if (x < 0.0f) r = kPiF - r;
+    return (y < 0.0f) ? -r : r;
+}
+
 // Math traits: FP32 uses the portable functions, FP64 the C library.
 template <class T> struct M;
 template <> struct M<float> {
@@ -1026,6 +1041,328 @@ uint64_t render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera*
     return rays.load();
 }
 
+
+// ------------------------------------------------------------------------
+// Sparse voxel octree: TriFunctions::Voxelize (GPUPrimitiveTriangle.h:
+// 385-620) and AnisoSVOctreeCPU::Constrcut (AnisoSVO.cu:657-1188) with its
+// level kernels KCMarkMortonChanges / KCMarkChild / KCExtractChildrenCounts
+// / KCSetChildrenPtrs / KCSetParentOf(Leaf)Children (AnisoSVO.cu:58-222),
+// restated in the reference's own order (the device build derives the same
+// canonical layout from prefix ranks instead).
+// ------------------------------------------------------------------------
+struct SvoP {
+    float lo[3], hi[3];
+    uint32_t res, depth;
+    float leaf;
+};
+inline SvoP svo_params_of(const float ext[6], uint32_t res) {
+    SvoP P{};
+    float span[3] = {ext[3] - ext[0], ext[4] - ext[1], ext[5] - ext[2]};
+    int md = 0;  // Vector::Max: first index of the largest component
+    if (span[1] > span[md]) md = 1;
+    if (span[2] > span[md]) md = 2;
+    const float world = span[md];
+    const float pad = world / static_cast<float>(res);
+    for (int c = 0; c < 3; c++) {
+        P.lo[c] = ext[c] - pad;
+        P.hi[c] = ext[c] + (pad + world);
+    }
+    P.res = res;
+    uint32_t d = 0;
+    while ((1u << (d + 1)) <= res) d++;
+    P.depth = d;
+    P.leaf = (world + 2.0f * pad) / static_cast<float>(res);
+    return P;
+}
+
+// returns the voxel count; writes codes/normals when out != nullptr
+uint32_t voxelize_tri(const SvoP& P, V3<float> p0, V3<float> p1, V3<float> p2,
+                      std::vector<uint64_t>* codes, std::vector<uint32_t>* normals) {
+    using F3 = V3<float>;
+    const F3 pos[3] = {p0, p1, p2};
+    const F3 n = normalize(cross(p1 - p0, p2 - p0));
+    const float an[3] = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
+    int dom = 0;
+    float mx = an[0];
+    if (an[1] > mx) { mx = an[1]; dom = 1; }
+    if (an[2] > mx) { mx = an[2]; dom = 2; }
+    const float nd = dom == 0 ? n.x : (dom == 1 ? n.y : n.z);
+    const bool neg = std::signbit(nd);
+    const float domSign = neg ? -1.0f : 1.0f;
+    // Utility::CartesianToSphericalUnit (CoordinateConversion.h:97-108)
+    const float az = pm_atan2(n.y, n.x);
+    const float incl = pm_acos(std::fmin(std::fmax(n.z, -1.0f), 1.0f));
+    const float s0 = (az + kPiF) * kInvPiF * 0.5f;
+    const float s1 = incl * kInvPiF;
+    int u = static_cast<int>(s0 * 65535.0f), v = static_cast<int>(s1 * 65535.0f);
+    u = std::min(std::max(u, 0), 65535);
+    v = std::min(std::max(v, 0), 65535);
+    const uint32_t packed = uint32_t(u) | (uint32_t(v) << 16);
+    // Quaternion(angle, axis) (Quaternion.hpp:15-24)
+    Q4<float> rot{1.0f, 0.0f, 0.0f, 0.0f};
+    if (dom != 2 || neg) {
+        const float angle = ((dom == 2) ? kPiF : (kPiF * 0.5f)) * 0.5f;
+        float sn, cs;
+        pm_sincos(angle, sn, cs);
+        F3 axis = (dom == 0) ? F3(-domSign * 0.0f, -domSign * 1.0f, -domSign * 0.0f)
+                 : (dom == 1) ? F3(domSign * 1.0f, domSign * 0.0f, domSign * 0.0f)
+                              : F3(0.0f, 1.0f, 0.0f);
+        rot = Q4<float>{cs, axis.x * sn, axis.y * sn, axis.z * sn};
+    }
+    // TransformGen::Ortogonal (Matrix.hpp:1021-1039), column-major product
+    const float l = P.lo[0], r = P.hi[0], t = P.hi[1], b = P.lo[1], nn = P.lo[2], f = P.hi[2];
+    const float xt = -((r + l) / (r - l)), yt = -((t + b) / (t - b)), zt = -((f + nn) / (f - nn));
+    const float xs = 2.0f / (r - l), ys = 2.0f / (t - b), zs = 2.0f / (f - nn);
+    float q2[3][2];
+    float amn[2] = {M<float>::Max, M<float>::Max}, amx[2] = {-M<float>::Max, -M<float>::Max};
+    for (int i = 0; i < 3; i++) {
+        F3 pt(xs * pos[i].x + xt, ys * pos[i].y + yt, zs * pos[i].z + zt);
+        pt = qrotate(rot, pt);
+        q2[i][0] = pt.x;
+        q2[i][1] = pt.y;
+        for (int c = 0; c < 2; c++) {
+            amn[c] = std::fmin(amn[c], q2[i][c]);
+            amx[c] = std::fmax(amx[c], q2[i][c]);
+        }
+    }
+    const float res = static_cast<float>(P.res);
+    const int ri = static_cast<int>(P.res);
+    auto clampi = [&](int x) { return std::min(std::max(x, 0), ri); };
+    const int x0 = clampi(static_cast<int>(std::floor((0.5f + 0.5f * amn[0]) * res)));
+    const int x1 = clampi(static_cast<int>(std::ceil((0.5f + 0.5f * amx[0]) * res)));
+    const int y0 = clampi(static_cast<int>(std::floor((0.5f + 0.5f * amn[1]) * res)));
+    const int y1 = clampi(static_cast<int>(std::ceil((0.5f + 0.5f * amx[1]) * res)));
+    const float half = 1.0f / res;
+    const float deltaPix = 2.0f * half;
+    F3 pl[3];
+    for (int i = 0; i < 3; i++) {
+        const float* a = q2[i];
+        const float* c = q2[(i + 1) % 3];
+        pl[i] = cross(F3(c[0] - a[0], c[1] - a[1], 0.0f), F3(a[0], a[1], 1.0f));
+        pl[i].z -= half * std::fabs(pl[i].x) + half * std::fabs(pl[i].y);
+    }
+    const F3 pc[3] = {cross(pl[0], pl[2]), cross(pl[0], pl[1]), cross(pl[1], pl[2])};
+    float c2[3][2];
+    for (int i = 0; i < 3; i++) {
+        c2[i][0] = pc[i].x / pc[i].z;
+        c2[i][1] = pc[i].y / pc[i].z;
+    }
+    const float ec0[2] = {c2[1][0] - c2[0][0], c2[1][1] - c2[0][1]};
+    const float ec1[2] = {c2[2][0] - c2[0][0], c2[2][1] - c2[0][1]};
+    const float denomC = 1.0f / (ec0[0] * ec1[1] - ec1[0] * ec0[1]);
+    const float e0[2] = {q2[1][0] - q2[0][0], q2[1][1] - q2[0][1]};
+    const float e1[2] = {q2[2][0] - q2[0][0], q2[2][1] - q2[0][1]};
+    const float denom = 1.0f / (e0[0] * e1[1] - e1[0] * e0[1]);
+    uint32_t w = 0;
+    for (int y = y0; y < y1; y++)
+        for (int x = x0; x < x1; x++) {
+            const float px = (static_cast<float>(x) + 0.5f) * deltaPix - 1.0f;
+            const float py = (static_cast<float>(y) + 0.5f) * deltaPix - 1.0f;
+            const float ec2[2] = {px - c2[0][0], py - c2[0][1]};
+            const float bb = (ec2[0] * ec1[1] - ec1[0] * ec2[1]) * denomC;
+            const float cc = (ec0[0] * ec2[1] - ec2[0] * ec0[1]) * denomC;
+            const float aa = 1.0f - bb - cc;
+            if (!(bb >= 0.0f && bb <= 1.0f && cc >= 0.0f && cc <= 1.0f && aa >= 0.0f && aa <= 1.0f))
+                continue;
+            if (codes) {
+                const float e2[2] = {px - q2[0][0], py - q2[0][1]};
+                const float ab = (e2[0] * e1[1] - e1[0] * e2[1]) * denom;
+                const float ac = (e0[0] * e2[1] - e2[0] * e0[1]) * denom;
+                const float aA = 1.0f - ab - ac;
+                const F3 vp = (p0 * aA + p1 * ab) + p2 * ac;
+                const float vpc[3] = {vp.x, vp.y, vp.z};
+                uint32_t vi[3];
+                for (int k = 0; k < 3; k++) {
+                    float fi = (vpc[k] - P.lo[k]) / (P.hi[k] - P.lo[k]);
+                    fi *= res;
+                    // the device conversion saturates below zero; ClampSelf(0, res-1)
+                    uint32_t q = fi > 0.0f ? static_cast<uint32_t>(fi) : 0u;
+                    vi[k] = std::min(q, P.res - 1);
+                }
+                codes->push_back(morton3d(vi[0], vi[1], vi[2]));
+                normals->push_back(packed);
+            }
+            w++;
+        }
+    return w;
+}
+
+}  // namespace
+
+struct oracle_svo {
+    SvoP P{};
+    std::vector<uint32_t> triVoxelCounts;
+    std::vector<uint64_t> leafCodes;
+    std::vector<uint32_t> levelOffsets;
+    std::vector<uint64_t> nodes;
+    std::vector<uint32_t> leafParents;
+    std::vector<uint32_t> leafLight;
+    uint32_t voxelCount = 0;
+};
+
+namespace {
+// __brevll on the host
+inline uint64_t brev64(uint64_t x) {
+    x = ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
+    x = ((x >> 2) & 0x3333333333333333ull) | ((x & 0x3333333333333333ull) << 2);
+    x = ((x >> 4) & 0x0F0F0F0F0F0F0F0Full) | ((x & 0x0F0F0F0F0F0F0F0Full) << 4);
+    x = ((x >> 8) & 0x00FF00FF00FF00FFull) | ((x & 0x00FF00FF00FF00FFull) << 8);
+    x = ((x >> 16) & 0x0000FFFF0000FFFFull) | ((x & 0x0000FFFF0000FFFFull) << 16);
+    return (x >> 32) | (x << 32);
+}
+// AnisoSVOctreeGPU packing (AnisoSVO.cuh:125-151)
+inline uint32_t svo_child_mask(uint64_t n) { return uint32_t(n >> 55) & 0xFFu; }
+inline uint32_t svo_children_index(uint64_t n) { return uint32_t(n) & 0x7FFFFFFu; }
+inline uint32_t svo_child_offset(uint64_t n, uint32_t childId) {
+    return uint32_t(__builtin_popcount(svo_child_mask(n) & ((1u << childId) - 1u)));
+}
+inline void svo_set_children_index(uint64_t& n, uint32_t c) {
+    n = (n & ~uint64_t(0x7FFFFFFu)) | (uint64_t(c) & 0x7FFFFFFu);
+}
+inline void svo_set_parent(uint64_t& n, uint32_t p) {
+    n = (n & ~(uint64_t(0xFFFFFFFu) << 27)) | ((uint64_t(p) & 0xFFFFFFFu) << 27);
+}
+}  // namespace
+
+extern "C" oracle_svo* oracle_svo_build(const float* pos, const uint32_t* idx, const uint32_t* key,
+                                        uint32_t T, const float* extent, uint32_t res,
+                                        int* status) {
+    oracle_svo* o = new oracle_svo();
+    o->P = svo_params_of(extent, res);
+    const SvoP& P = o->P;
+    std::vector<uint64_t> codes;
+    std::vector<uint32_t> normals, lights;
+    o->triVoxelCounts.resize(T);
+    for (uint32_t t = 0; t < T; t++) {
+        V3<float> a(pos[3 * idx[3 * t]], pos[3 * idx[3 * t] + 1], pos[3 * idx[3 * t] + 2]);
+        V3<float> b(pos[3 * idx[3 * t + 1]], pos[3 * idx[3 * t + 1] + 1], pos[3 * idx[3 * t + 1] + 2]);
+        V3<float> c(pos[3 * idx[3 * t + 2]], pos[3 * idx[3 * t + 2] + 1], pos[3 * idx[3 * t + 2] + 2]);
+        const size_t before = codes.size();
+        o->triVoxelCounts[t] = voxelize_tri(P, a, b, c, &codes, &normals);
+        const uint32_t lk = ((key[t] >> 24) == kBatchLight) ? key[t] : 0u;
+        lights.resize(codes.size(), 0u);
+        for (size_t i = before; i < codes.size(); i++) lights[i] = lk;
+    }
+    const uint32_t total = uint32_t(codes.size());
+    o->voxelCount = total;
+    // cub::DeviceRadixSort::SortPairs on bits [0, 3*depth + 1), then RLE
+    std::vector<uint32_t> order(total);
+    for (uint32_t i = 0; i < total; i++) order[i] = i;
+    std::vector<uint64_t> sorted = codes;
+    radix_sort<uint64_t>(sorted.data(), order.data(), total, 0, int(3 * P.depth + 1), false);
+    for (uint32_t i = 0; i < total; i++)
+        if (i == 0 || sorted[i] != sorted[i - 1]) {
+            o->leafCodes.push_back(sorted[i]);
+            o->leafLight.push_back(0u);
+        }
+    {  // first light voxel of each run
+        size_t u = 0;
+        for (uint32_t i = 0; i < total; i++) {
+            if (i > 0 && sorted[i] != sorted[i - 1]) u++;
+            if (!o->leafLight[u]) o->leafLight[u] = lights[order[i]];
+        }
+    }
+    const uint32_t U = uint32_t(o->leafCodes.size());
+    const uint32_t D = P.depth;
+    // level node counts: KCMarkMortonChanges + reduce, per level
+    std::vector<uint32_t> levelCounts(D + 1, 0);
+    levelCounts[0] = 1;
+    for (uint32_t L = 1; L <= D; L++) {
+        uint32_t changes = 0;
+        const uint32_t msbStart = 64 - D * 3;
+        for (uint32_t j = 0; j + 1 < U; j++) {
+            uint64_t a = brev64(o->leafCodes[j]) >> msbStart;
+            uint64_t b = brev64(o->leafCodes[j + 1]) >> msbStart;
+            a &= (1ull << (L * 3)) - 1;
+            b &= (1ull << (L * 3)) - 1;
+            changes += (a != b) ? 1u : 0u;
+        }
+        levelCounts[L] = changes + 1;
+    }
+    o->levelOffsets.assign(D + 2, 0);
+    for (uint32_t L = 0; L <= D; L++) o->levelOffsets[L + 1] = o->levelOffsets[L] + levelCounts[L];
+    const uint32_t N = o->levelOffsets[D];
+    o->nodes.assign(N, 0x007FFFFFFFFFFFFFull);
+    o->leafParents.assign(U, 0xFFFFFFFFu);
+    for (uint32_t L = 0; L < D; L++) {
+        // KCMarkChild: walk from the root, then set the child bit
+        for (uint32_t j = 0; j < U; j++) {
+            const uint64_t code = o->leafCodes[j];
+            uint32_t shift = (D - 1) * 3;
+            uint32_t cur = 0;
+            for (uint32_t i = 0; i < L; i++) {
+                const uint64_t nd = o->nodes[cur];
+                const uint32_t cid = uint32_t(code >> shift) & 7u;
+                cur = svo_children_index(nd) + svo_child_offset(nd, cid);
+                shift -= 3;
+            }
+            const uint32_t cid = uint32_t(code >> shift) & 7u;
+            o->nodes[cur] |= (uint64_t(1u << cid) << 55);
+        }
+        // KCExtractChildrenCounts + ExclusiveSum + KCSetChildrenPtrs
+        const bool last = (L == D - 1);
+        const uint32_t nextOffset = last ? 0 : o->levelOffsets[L + 1];
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < levelCounts[L]; k++) {
+            uint64_t& nd = o->nodes[o->levelOffsets[L] + k];
+            const uint32_t cnt = uint32_t(__builtin_popcount(svo_child_mask(nd)));
+            svo_set_children_index(nd, nextOffset + run);
+            if (last) nd |= (1ull << 63);
+            run += cnt;
+        }
+        if (run != levelCounts[L + 1]) {
+            if (status) *status = 2;
+            return o;
+        }
+        // KCSetParentOfChildren / KCSetParentOfLeafChildren
+        for (uint32_t k = 0; k < levelCounts[L]; k++) {
+            const uint32_t g = o->levelOffsets[L] + k;
+            const uint64_t nd = o->nodes[g];
+            const uint32_t cnt = uint32_t(__builtin_popcount(svo_child_mask(nd)));
+            const uint32_t ci = svo_children_index(nd);
+            for (uint32_t i = 0; i < cnt; i++) {
+                if (last) o->leafParents[ci + i] = g;
+                else svo_set_parent(o->nodes[ci + i], g);
+            }
+        }
+    }
+    if (status) *status = 0;
+    return o;
+}
+
+extern "C" void oracle_svo_destroy(oracle_svo* o) { delete o; }
+
+extern "C" void oracle_svo_sizes(const oracle_svo* o, uint32_t* s) {
+    s[0] = o->voxelCount;
+    s[1] = uint32_t(o->leafCodes.size());
+    s[2] = uint32_t(o->nodes.size());
+    s[3] = o->P.depth;
+    s[4] = uint32_t(o->levelOffsets.size());
+    s[5] = uint32_t(o->triVoxelCounts.size());
+}
+
+extern "C" void oracle_svo_get(const oracle_svo* o, uint64_t* nodes, uint32_t* leafParents,
+                               uint64_t* leafCodes, uint32_t* leafLights, uint32_t* levelOffsets,
+                               uint32_t* triVoxelCounts, float* params) {
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(nodes, o->nodes);
+    cp(leafParents, o->leafParents);
+    cp(leafCodes, o->leafCodes);
+    cp(leafLights, o->leafLight);
+    cp(levelOffsets, o->levelOffsets);
+    cp(triVoxelCounts, o->triVoxelCounts);
+    if (params) {
+        for (int c = 0; c < 3; c++) {
+            params[c] = o->P.lo[c];
+            params[3 + c] = o->P.hi[c];
+        }
+        params[6] = o->P.leaf;
+    }
+}
+
+namespace {
 }  // namespace
 
 // ========================================================================

@@ -136,6 +136,21 @@ uint64_t oracle_render_f64(const oracle_scene* scene, const oracle_bvh* bvh,
 void oracle_build_tbn(const float* pos, const float* nrm, const float* uvs, const uint32_t* idx,
                       uint32_t vertex_count, uint32_t tri_count, float* tbn_out);
 
+/* Sparse voxel octree (AnisoSVO.cu:657-1188 with TriFunctions::Voxelize,
+ * GPUPrimitiveTriangle.h:385-620), built in the reference's own order:
+ * voxelise, sort + RLE, then per level mark children from the root, scan
+ * child counts, set child and parent pointers. */
+typedef struct oracle_svo oracle_svo;
+oracle_svo* oracle_svo_build(const float* pos, const uint32_t* idx, const uint32_t* key,
+                             uint32_t tri_count, const float* extent6, uint32_t resolution,
+                             int* status);
+void oracle_svo_destroy(oracle_svo*);
+/* sizes[6]: voxels, leaves, nodes, depth, level-offset count, triangles */
+void oracle_svo_sizes(const oracle_svo*, uint32_t* sizes);
+void oracle_svo_get(const oracle_svo*, uint64_t* nodes, uint32_t* leaf_parents,
+                    uint64_t* leaf_codes, uint32_t* leaf_lights, uint32_t* level_offsets,
+                    uint32_t* tri_voxel_counts, float* params7);
+
 /* Single-vertex BxDF probes used by the golden-vector tests. */
 void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi,
                         const float* w2t, const float* geo_normal, const float* pos,

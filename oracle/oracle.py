@@ -260,3 +260,27 @@ def build_tbn(scene) -> np.ndarray:
     lib.oracle_build_tbn(_p(pos), _p(nrm), _p(uvs), _p(idx), C.c_uint32(pos.shape[0]),
                          C.c_uint32(idx.shape[0]), _p(out))
     return out
+
+
+def svo_build(scene, tri_key: np.ndarray, extent: np.ndarray, resolution: int) -> dict:
+    """The oracle's sparse voxel octree of a scene (reference build order)."""
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    idx = np.ascontiguousarray(scene.indices, np.uint32)
+    key = np.ascontiguousarray(tri_key, np.uint32)
+    ext = np.ascontiguousarray(extent[:6], np.float32)
+    lib.oracle_svo_build.restype = C.c_void_p
+    st = C.c_int(0)
+    h = lib.oracle_svo_build(_p(pos), _p(idx), _p(key), C.c_uint32(idx.shape[0]), _p(ext),
+                             C.c_uint32(resolution), C.byref(st))
+    sz = np.zeros(6, np.uint32)
+    lib.oracle_svo_sizes(C.c_void_p(h), _p(sz))
+    out = {"status": st.value, "voxels": int(sz[0]), "depth": int(sz[3]),
+           "nodes": np.zeros(int(sz[2]), np.uint64), "leaf_parents": np.zeros(int(sz[1]), np.uint32),
+           "leaf_codes": np.zeros(int(sz[1]), np.uint64), "leaf_lights": np.zeros(int(sz[1]), np.uint32),
+           "level_offsets": np.zeros(int(sz[4]), np.uint32),
+           "tri_voxels": np.zeros(int(sz[5]), np.uint32), "params": np.zeros(7, np.float32)}
+    lib.oracle_svo_get(C.c_void_p(h), _p(out["nodes"]), _p(out["leaf_parents"]),
+                       _p(out["leaf_codes"]), _p(out["leaf_lights"]), _p(out["level_offsets"]),
+                       _p(out["tri_voxels"]), _p(out["params"]))
+    lib.oracle_svo_destroy(C.c_void_p(h))
+    return out
