@@ -16,7 +16,8 @@
  *   - "d_" pointers are device pointers on the current CUDA device; "stream"
  *     is a cudaStream_t passed as void* (NULL = legacy default stream).
  *   - HitKey layout: batch << 24 | id (RayLib/HitStructs.h:154); batches:
- *     0 null, 1 Lambert, 2 Metal, 3 Refract, 4 primitive light.
+ *     0 null, 1 Lambert, 2 Metal, 3 Refract, 4 primitive light, 5 LambertC,
+ *     6 Unreal.
  */
 #ifndef MRB200_H
 #define MRB200_H
@@ -45,14 +46,17 @@ typedef struct mrb_tracer mrb_tracer;
 #define MRB_MAT_METAL 2   /* "Metal"    MetalGlassMaterialsKC.cuh:11-222 */
 #define MRB_MAT_REFRACT 3 /* "Refract"  SimpleMaterialsKC.cuh:172-302 */
 #define MRB_MAT_LIGHT 4   /* primitive-backed light, GPULightPrimitive.cuh */
+#define MRB_MAT_LAMBERTC 5 /* "LambertC" SimpleMaterialsKC.cuh:16-103 */
+#define MRB_MAT_UNREAL 6  /* "Unreal"   UnrealMaterialKC.cuh:19-359 */
 
 typedef struct mrb_material {
     uint32_t type;
     float albedo[3];   /* Lambert / Refract */
     float eta[3];      /* Metal */
     float k[3];        /* Metal */
-    float specular[3]; /* Metal */
-    float roughness;   /* Metal */
+    float specular[3]; /* Metal (Unreal uses specular[0]) */
+    float roughness;   /* Metal, Unreal */
+    float metallic;    /* Unreal */
     uint32_t medium;   /* Refract: medium index inside the surface */
     float radiance[3]; /* Light */
 } mrb_material;
@@ -108,6 +112,11 @@ int mrb_scene_export(const mrb_scene* scene, float* tbn, uint32_t* tri_key, floa
                      float* metal, float* refract, uint32_t* refract_medium,
                      float* light_radiance, uint32_t* light_prim);
 
+/* LambertC albedo (3 each) and Unreal parameters (6 each: albedo3,
+ * roughness, metallic, specular); counts2 = their counts.  NULL skips. */
+int mrb_scene_export_ext(const mrb_scene* scene, float* lambertc, float* unreal,
+                         uint32_t* counts2);
+
 /* ---- accelerator group "LBVH": GPUAcceleratorGroupI
  * (GPUAcceleratorI.h:46-134), drop-in for GPUAccBVHGroup
  * (GPUAcceleratorBVH.cuh:63-203). */
@@ -157,7 +166,7 @@ int mrb_svo_export(const mrb_scene* scene, uint64_t* nodes, uint32_t* leaf_paren
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out);
 void mrb_tracer_destroy(mrb_tracer* t);
 /* SetOptions keys (PathTracer.h:17-33): "Samples", "MaxDepth",
- * "NextEventEstimation", "RussianRouletteStart", "DirectLightMIS" (0 only),
+ * "NextEventEstimation", "RussianRouletteStart", "DirectLightMIS",
  * plus "Seed" (RNG key) and "Frame" (RNG iteration counter). */
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
 int mrb_tracer_set_resolution(mrb_tracer* t, uint32_t width, uint32_t height);

@@ -22,7 +22,7 @@ class MrbError(RuntimeError):
 class Material(C.Structure):
     _fields_ = [("type", C.c_uint32), ("albedo", C.c_float * 3), ("eta", C.c_float * 3),
                 ("k", C.c_float * 3), ("specular", C.c_float * 3), ("roughness", C.c_float),
-                ("medium", C.c_uint32), ("radiance", C.c_float * 3)]
+                ("metallic", C.c_float), ("medium", C.c_uint32), ("radiance", C.c_float * 3)]
 
 
 class SceneDesc(C.Structure):
@@ -54,6 +54,7 @@ def _load() -> C.CDLL:
         "mrb_scene_destroy": (None, [vp]),
         "mrb_scene_counts": (i32, [vp, vp]),
         "mrb_scene_export": (i32, [vp] + [vp] * 8),
+        "mrb_scene_export_ext": (i32, [vp, vp, vp, vp]),
         "mrb_accel_construct": (i32, [vp, vp]),
         "mrb_accel_export": (i32, [vp] + [vp] * 9),
         "mrb_accel_hit": (i32, [vp, vp, vp, u32, vp, vp, vp, vp, vp]),

@@ -21,7 +21,9 @@ constexpr uint32_t kBatchLambert = 1;
 constexpr uint32_t kBatchMetal = 2;
 constexpr uint32_t kBatchRefract = 3;
 constexpr uint32_t kBatchLight = 4;
-constexpr uint32_t kBatchCount = 5;
+constexpr uint32_t kBatchLambertC = 5;
+constexpr uint32_t kBatchUnreal = 6;
+constexpr uint32_t kBatchCount = 7;
 constexpr uint32_t kIdBits = 24;
 constexpr uint32_t kIdMask = 0xFFFFFFu;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
@@ -66,6 +68,8 @@ struct SceneDev {
     const float* metalParams;    // eta3 k3 spec3 roughness
     const float* refractAlbedo;  // 3 per Refract material
     const uint32_t* refractMedium;
+    const float* lambertCAlbedo; // 3 per LambertC material
+    const float* unrealParams;   // albedo3 roughness metallic specular
     const float* lightRadiance;  // 3 per primitive light
     const uint32_t* lightPrim;
     uint32_t lightCount;
@@ -93,7 +97,7 @@ struct CameraDev {         // GPUCameraPinhole frame (GPUCameraPinhole.cuh:135-1
 
 struct PathOptions {
     uint32_t width, height, samples;   // samples: s -> s*s per pixel
-    uint32_t maxDepth, rrStart, nee;
+    uint32_t maxDepth, rrStart, nee, mis;
     uint32_t seedLo, seedHi;
     const uint32_t* frame;             // device word: iteration index (RNG counter)
 };

@@ -210,13 +210,13 @@ struct mrb_scene {
     uint32_t V = 0, T = 0;
     std::vector<float> tbn;
     std::vector<uint32_t> triKey;
-    std::vector<float> lambert, metal, refract, lightRad;
+    std::vector<float> lambert, metal, refract, lightRad, lambertC, unreal;
     std::vector<uint32_t> refractMed, lightPrim;
     std::vector<float> mediumIor;
     uint32_t baseMedium = 0;
     uint32_t idBits = 1;
     DBuf dPos, dTbn, dIdx, dKey, dCull, dLambert, dMetal, dRefract, dRefractMed, dLightRad,
-        dLightPrim, dMediumIor;
+        dLightPrim, dMediumIor, dLambertC, dUnreal;
     // LBVH
     bool built = false;
     DBuf aTriAabb, aExtent, aCodes, aSorted, aLeft, aRight, aParent, aInner, aScratch, aRoot,
@@ -256,6 +256,8 @@ struct mrb_scene {
         s.metalParams = dMetal.as<float>();
         s.refractAlbedo = dRefract.as<float>();
         s.refractMedium = dRefractMed.as<uint32_t>();
+        s.lambertCAlbedo = dLambertC.as<float>();
+        s.unrealParams = dUnreal.as<float>();
         s.lightRadiance = dLightRad.as<float>();
         s.lightPrim = dLightPrim.as<uint32_t>();
         s.lightCount = static_cast<uint32_t>(lightPrim.size());
@@ -360,6 +362,7 @@ PathOptions path_options(const mrb_tracer* t) {
     o.maxDepth = t->maxDepth;
     o.rrStart = t->rrStart;
     o.nee = t->nee;
+    o.mis = t->mis;
     o.seedLo = static_cast<uint32_t>(t->seed);
     o.seedHi = static_cast<uint32_t>(t->seed >> 32);
     o.frame = t->frameWord.as<uint32_t>();
@@ -583,6 +586,17 @@ int mrb_scene_create(mrb_system* sys, const mrb_scene_desc* d, mrb_scene** out) 
                 s->refract.insert(s->refract.end(), mt.albedo, mt.albedo + 3);
                 s->refractMed.push_back(mt.medium);
                 break;
+            case MRB_MAT_LAMBERTC:
+                matKey[m] = (kBatchLambertC << kIdBits) | uint32_t(s->lambertC.size() / 3);
+                s->lambertC.insert(s->lambertC.end(), mt.albedo, mt.albedo + 3);
+                break;
+            case MRB_MAT_UNREAL:
+                matKey[m] = (kBatchUnreal << kIdBits) | uint32_t(s->unreal.size() / 6);
+                s->unreal.insert(s->unreal.end(), mt.albedo, mt.albedo + 3);
+                s->unreal.push_back(mt.roughness);
+                s->unreal.push_back(mt.metallic);
+                s->unreal.push_back(mt.specular[0]);
+                break;
             case MRB_MAT_LIGHT:
                 break;
             default:
@@ -626,7 +640,8 @@ int mrb_scene_create(mrb_system* sys, const mrb_scene_desc* d, mrb_scene** out) 
         (r = upload(s->dKey, s->triKey)) || (r = upload(s->dLambert, s->lambert)) ||
         (r = upload(s->dMetal, s->metal)) || (r = upload(s->dRefract, s->refract)) ||
         (r = upload(s->dRefractMed, s->refractMed)) || (r = upload(s->dLightRad, s->lightRad)) ||
-        (r = upload(s->dLightPrim, s->lightPrim)) || (r = upload(s->dMediumIor, s->mediumIor))) {
+        (r = upload(s->dLightPrim, s->lightPrim)) || (r = upload(s->dMediumIor, s->mediumIor)) ||
+        (r = upload(s->dLambertC, s->lambertC)) || (r = upload(s->dUnreal, s->unreal))) {
         delete s;
         return r;
     }
@@ -670,6 +685,18 @@ int mrb_scene_export(const mrb_scene* s, float* tbn, uint32_t* key, float* lambe
     cp(refractMed, s->refractMed);
     cp(lightRad, s->lightRad);
     cp(lightPrim, s->lightPrim);
+    return 0;
+}
+
+int mrb_scene_export_ext(const mrb_scene* s, float* lambertC, float* unreal, uint32_t* counts2) {
+    if (!s) return MRB_E_ARG;
+    if (counts2) {
+        counts2[0] = static_cast<uint32_t>(s->lambertC.size() / 3);
+        counts2[1] = static_cast<uint32_t>(s->unreal.size() / 6);
+    }
+    if (lambertC && !s->lambertC.empty())
+        std::memcpy(lambertC, s->lambertC.data(), s->lambertC.size() * 4);
+    if (unreal && !s->unreal.empty()) std::memcpy(unreal, s->unreal.data(), s->unreal.size() * 4);
     return 0;
 }
 
@@ -923,11 +950,7 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
     } else if (k == "RussianRouletteStart") {
         t->rrStart = uint32_t(v);
     } else if (k == "DirectLightMIS") {
-        if (v) {
-            set_error("DirectLightMIS=true is not supported by this core");
-            return MRB_E_UNSUPPORTED;
-        }
-        t->mis = 0;
+        t->mis = v ? 1 : 0;
     } else if (k == "Seed") {
         t->seed = v;
     } else if (k == "Frame") {

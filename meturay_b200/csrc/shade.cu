@@ -284,6 +284,179 @@ __device__ BSample refract_sample(V3 albedo, uint32_t matMedium, const SceneDev&
     return out;
 }
 
+// Quat::RotationBetweenZAxis (Quaternion.hpp:333-358)
+__device__ __forceinline__ Q4 rotation_between_z(V3 b) {
+    V3 zc = v3(-b.y, b.x, 0.0f);
+    const float zd = b.z;
+    const float sn = sqrtf((1.0f - zd) * 0.5f);
+    const float cs = sqrtf((zd + 1.0f) * 0.5f);
+    zc = normalize(zc);
+    if (fabsf(zd + 1.0f) < 1.0e-4f) return Q4{0.0f, 0.0f, 1.0f, 0.0f};
+    if (fabsf(zd - 1.0f) < 1.0e-4f) return Q4{1.0f, 0.0f, 0.0f, 0.0f};
+    return Q4{cs, zc.x * sn, zc.y * sn, zc.z * sn};
+}
+
+// LambertConstFuncs, "LambertC" (SimpleMaterialsKC.cuh:16-103): uniform
+// hemisphere sampling around the shading normal
+__device__ __forceinline__ BSample lambertc_sample(V3 albedo, const Surface& sf, float xi0, float xi1,
+                                                   uint32_t medium) {
+    BSample out;
+    const V3 n = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+    // HemiDistribution::HemiUniformCDF (HemiDistribution.h:34-51)
+    const float c0 = sqrtf(fmaxf(0.0f, 1.0f - xi0 * xi0));
+    const float c1 = 2.0f * kPiF * xi1;
+    float sn, cs;
+    pm_sincos(c1, sn, cs);
+    V3 d = v3(c0 * cs, c0 * sn, xi0);
+    out.pdf = kInvPiF * 0.5f;
+    d = normalize(d);
+    d = qrotate(rotation_between_z(n), d);
+    const float nDotL = fabsf(dot(n, d));
+    out.dir = d;
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = nDotL * albedo * kInvPiF;
+    out.medium = medium;
+    return out;
+}
+__device__ __forceinline__ V3 lambertc_eval(V3 albedo, V3 wo, const Surface& sf) {
+    const V3 n = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+    return fmaxf(dot(n, wo), 0.0f) * albedo * kInvPiF;
+}
+__device__ __forceinline__ float lambert_pdf(V3 wo, const Surface& sf) {
+    const V3 n = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+    return fmaxf(dot(wo, n), 0.0f) * kInvPiF;
+}
+// MetalMatFuncs::Pdf (MetalGlassMaterialsKC.cuh:148-172)
+__device__ float metal_pdf(const MetalP& m, V3 wo, V3 wi, const Surface& sf) {
+    const float alpha = m.rough * m.rough;
+    const V3 L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3 H = normalize(L + V);
+    const float NdH = fmaxf(0.0f, H.z), VdH = fmaxf(0.0f, dot(V, H));
+    float p = vndf_pdf(V, H, alpha);
+    const float D = dggx(NdH, alpha);
+    p = (isnan(D) || isinf(D)) ? 0.0f : p;
+    return (VdH == 0.0f) ? 0.0f : p / (4.0f * VdH);
+}
+
+// UnrealDeviceFuncs (UnrealMaterialKC.cuh:19-359): Lambert + GGX with
+// Schlick Fresnel, lobes chosen by a luminance-based ratio
+struct UnrealP {
+    V3 albedo;
+    float rough, metallic, specular;
+};
+__device__ __forceinline__ UnrealP unreal_params(const float* p) {
+    return {ld3(p), p[3], p[4], p[5]};
+}
+__device__ __forceinline__ float luminance(V3 c) {  // ColorConversion.h:15-21
+    return 0.2120f * c.x + 0.7150f * c.y + 0.0722f * c.z;
+}
+__device__ __forceinline__ float unreal_mis_ratio(float metallic, float specular, float lum) {
+    float diffuse = 2.0f * kPiF * lum;
+    diffuse *= (1.0f - metallic);
+    const float specRatio = (1.0f - metallic) * specular + metallic * lum;
+    const float total = specRatio + diffuse;
+    return diffuse / total;
+}
+__device__ __forceinline__ V3 unreal_f0(V3 albedo, float metallic, float specular) {
+    specular *= 0.08f;
+    // Vector3::Lerp(a, b, t) = a * (1 - t) + b * t
+    const V3 a = v3(specular, specular, specular);
+    return a * (1.0f - metallic) + albedo * metallic;
+}
+__device__ __forceinline__ V3 f_schlick(float VdH, V3 f0) {  // TracerFunctions.cuh:160-179
+    const float pt = 1.0f - VdH;
+    float p5 = pt * pt;
+    p5 *= p5;
+    p5 *= pt;
+    V3 r = (v3(1.0f, 1.0f, 1.0f) - f0) * p5;
+    return r + f0;
+}
+__device__ BSample unreal_sample(const UnrealP& m, V3 wi, const Surface& sf, float xiSel,
+                                 float xi0, float xi1, uint32_t medium) {
+    BSample out;
+    const float alpha = m.rough * m.rough;
+    const V3 V = to_tangent(wi, sf.w2t);
+    float misRatio = unreal_mis_ratio(m.metallic, m.specular, luminance(m.albedo));
+    const bool diffuse = xiSel < misRatio;
+    float VdH, pdfSel, pdfOther;
+    V3 H, L;
+    if (diffuse) {
+        L = hemi_cosine(xi0, xi1, pdfSel);
+        H = normalize(V + L);
+        VdH = fmaxf(0.0f, dot(V, H));
+        pdfOther = vndf_pdf(V, H, alpha);
+        pdfOther = (VdH == 0.0f) ? 0.0f : pdfOther / (4.0f * VdH);
+    } else {
+        H = vndf_sample(pdfSel, V, alpha, xi0, xi1);
+        VdH = fmaxf(0.0f, dot(V, H));
+        L = 2.0f * VdH * H - V;
+        pdfOther = fmaxf(0.0f, L.z) * kInvPiF;
+        pdfSel = (VdH == 0.0f) ? 0.0f : pdfSel / (4.0f * VdH);
+        misRatio = 1.0f - misRatio;
+    }
+    float& pdfSpec = diffuse ? pdfOther : pdfSel;
+    pdfSpec = (VdH == 0.0f) ? 0.0f : pdfSpec;
+    const float LdH = fmaxf(0.0f, dot(L, H)), NdH = fmaxf(0.0f, H.z), NdV = fmaxf(0.0f, V.z);
+    const float D = dggx(NdH, alpha);
+    float G = g_smith_corr(V, L, alpha);
+    G = (LdH == 0.0f) ? 0.0f : G;
+    G = (VdH == 0.0f) ? 0.0f : G;
+    const V3 F = f_schlick(VdH, unreal_f0(m.albedo, m.metallic, m.specular));
+    V3 spec = D * F * G * 0.25f / NdV;
+    spec = (NdV == 0.0f) ? v3(0.0f, 0.0f, 0.0f) : spec;
+    if (isinf(D) || isnan(D)) {
+        spec = G * F / g_smith_single(V, alpha);
+        pdfSpec = diffuse ? 0.0f : 1.0f;
+    }
+    const float NdL = fmaxf(0.0f, L.z);
+    const V3 diffAlbedo = (1.0f - m.metallic) * m.albedo;
+    const V3 diffTerm = NdL * diffAlbedo * kInvPiF;
+    // TracerFunctions::BalanceHeuristic
+    const float w0 = misRatio * pdfSel, w1 = (1.0f - misRatio) * pdfOther;
+    const float misWeight = w0 / (w0 + w1);
+    out.pdf = (pdfSel == 0.0f) ? 0.0f : (misRatio * pdfSel / misWeight);
+    out.dir = to_space(L, sf.w2t);
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = diffTerm + spec;
+    out.medium = medium;
+    return out;
+}
+__device__ V3 unreal_eval(const UnrealP& m, V3 wo, V3 wi, const Surface& sf) {
+    const float alpha = m.rough * m.rough;
+    const V3 L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3 H = normalize(L + V);
+    const float LdH = fmaxf(0.0f, dot(L, H)), VdH = fmaxf(0.0f, dot(V, H));
+    const float NdH = fmaxf(0.0f, H.z), NdV = fmaxf(0.0f, V.z);
+    float D = dggx(NdH, alpha);
+    D = (isnan(D) || isinf(D)) ? 0.0f : D;
+    float G = g_smith_corr(V, L, alpha);
+    G = (LdH == 0.0f) ? 0.0f : G;
+    G = (VdH == 0.0f) ? 0.0f : G;
+    const V3 F = f_schlick(VdH, unreal_f0(m.albedo, m.metallic, m.specular));
+    V3 spec = D * F * G * 0.25f / NdV;
+    spec = (NdV == 0.0f) ? v3(0.0f, 0.0f, 0.0f) : spec;
+    const float NdL = fmaxf(0.0f, L.z);
+    const V3 diffTerm = NdL * ((1.0f - m.metallic) * m.albedo) * kInvPiF;
+    return diffTerm + spec;
+}
+__device__ float unreal_pdf(const UnrealP& m, V3 wo, V3 wi, const Surface& sf) {
+    const float alpha = m.rough * m.rough;
+    const V3 L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3 H = normalize(L + V);
+    const float NdH = fmaxf(0.0f, H.z), VdH = fmaxf(0.0f, dot(V, H));
+    float ps = vndf_pdf(V, H, alpha);
+    const float D = dggx(NdH, alpha);
+    ps = (isnan(D) || isinf(D)) ? 0.0f : ps;
+    ps = (VdH == 0.0f) ? 0.0f : ps / (4.0f * VdH);
+    const float pd = fmaxf(0.0f, L.z) * kInvPiF;
+    const float r = unreal_mis_ratio(m.metallic, m.specular, luminance(m.albedo));
+    return r * pd + (1.0f - r) * ps;
+}
+__device__ __forceinline__ float power_heuristic(float p0, float p1) {  // n0 = n1 = 1
+    const float w0 = 1.0f * p0, w1 = 1.0f * p1;
+    return (w0 * w0) / (w0 * w0 + w1 * w1);
+}
+
 __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ camPtr,
                                                 PathOptions opt, uint32_t baseMedium,
                                                 float4* __restrict__ rayO,
@@ -409,15 +582,42 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
             const float4 rd = A.rayD[rid];
             const RayAux aux = A.aux[rid];
             if (batch == kBatchLight) {
-                // PathTracerBoundaryWork, MIS off (PathTracerKC.cuh:335-426)
+                // PathTracerBoundaryWork (PathTracerKC.cuh:335-426)
+                const bool pathAsMis = A.opt.mis && aux.type == kPathRay;
                 const bool camera = aux.type == kCameraRay;
                 const bool specPath = aux.type == kSpecPathRay;
                 const bool neeOn = A.opt.nee && aux.type == kNeeRay;
                 const bool pathNeeOff =
                     (!A.opt.nee) && (aux.type == kPathRay || aux.type == kSpecPathRay);
                 const bool correct = neeOn && (aux.endpoint == id);
-                if (pathNeeOff || correct || camera || specPath) {
+                float misWeight = 1.0f;
+                if (pathAsMis) {
+                    // light pdf of this hit: GPULightSamplerUniform::Pdf and
+                    // GPULight::Pdf(distance, position, direction, tbn)
+                    const uint32_t prim = A.hit.prim[rid];
+                    const float2 hb = A.hit.bary[rid];
+                    const V3 d = {rd.x, rd.y, rd.z};
+                    const Surface sf = gen_surface(s, prim, hb.x, hb.y, d);
+                    const V3 dir = normalize(d);
+                    float pdfM = 0.0f, pdfC = 0.0f;
+                    if (id < s.lightCount) {
+                        pdfM = 1.0f / static_cast<float>(s.lightCount);
+                        const uint32_t i0 = s.idx[3 * prim], i1 = s.idx[3 * prim + 1],
+                                       i2 = s.idx[3 * prim + 2];
+                        const V3 p0 = ld3(s.pos + 3 * size_t(i0)), p1 = ld3(s.pos + 3 * size_t(i1)),
+                                 p2 = ld3(s.pos + 3 * size_t(i2));
+                        const V3 cr = cross(p1 - p0, p2 - p0);
+                        const float area = sqrtf(dot(cr, cr)) * 0.5f;
+                        const V3 ln = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+                        const float nDotL = fabsf(dot(ln, -dir));
+                        const float dist = A.hit.t[rid];
+                        pdfC = (1.0f / area) * dist * dist / nDotL;
+                    }
+                    misWeight = power_heuristic(aux.prevPDF, pdfC * pdfM);
+                }
+                if (pathNeeOff || pathAsMis || correct || camera || specPath) {
                     V3 total = ld3(s.lightRadiance + 3 * id) * v3(aux.rf[0], aux.rf[1], aux.rf[2]);
+                    total = total * misWeight;
                     accumulate(A.samples, aux.sample, total);
                 }
             } else if (aux.type != kNeeRay && A.gen) {
@@ -429,8 +629,9 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                 const V3 wi = -normalize(d);
                 const V3 rf = {aux.rf[0], aux.rf[1], aux.rf[2]};
                 bool specular;
-                if (batch == kBatchLambert) specular = false;
+                if (batch == kBatchLambert || batch == kBatchLambertC) specular = false;
                 else if (batch == kBatchMetal) specular = (1.0f - s.metalParams[10 * id + 9]) >= 0.99f;
+                else if (batch == kBatchUnreal) specular = (1.0f - s.unrealParams[6 * id + 3]) >= 0.99f;
                 else specular = true;
                 const Rand4 ra = philox_uniform4(aux.sample, frame, aux.depth, 0u,
                                                  A.opt.seedLo, A.opt.seedHi);
@@ -469,13 +670,29 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                     lpdf *= d2 / nDotL;
                     lpdf *= (1.0f / static_cast<float>(lc));
                     V3 refl;
+                    float pdfBxdf;
                     if (batch == kBatchLambert) {
                         refl = lambert_eval(ld3(s.lambertAlbedo + 3 * id), ldir, sf);
+                        pdfBxdf = A.opt.mis ? lambert_pdf(ldir, sf) : 0.0f;
+                    } else if (batch == kBatchLambertC) {
+                        refl = lambertc_eval(ld3(s.lambertCAlbedo + 3 * id), ldir, sf);
+                        pdfBxdf = A.opt.mis ? lambert_pdf(ldir, sf) : 0.0f;
+                    } else if (batch == kBatchUnreal) {
+                        const UnrealP up = unreal_params(s.unrealParams + 6 * id);
+                        refl = unreal_eval(up, ldir, wi, sf);
+                        pdfBxdf = A.opt.mis ? unreal_pdf(up, ldir, wi, sf) : 0.0f;
                     } else {
-                        refl = metal_eval(metal_params(s.metalParams + 10 * id), ldir, wi, sf);
+                        const MetalP mp = metal_params(s.metalParams + 10 * id);
+                        refl = metal_eval(mp, ldir, wi, sf);
+                        pdfBxdf = A.opt.mis ? metal_pdf(mp, ldir, wi, sf) : 0.0f;
+                    }
+                    float pdfNee = lpdf;
+                    if (A.opt.mis) {
+                        pdfNee /= power_heuristic(lpdf, pdfBxdf);
+                        if (isnan(pdfNee)) pdfNee = 0.0f;
                     }
                     V3 nrf = rf * refl;
-                    nrf = (lpdf == 0.0f) ? v3(0.0f, 0.0f, 0.0f) : (nrf / lpdf);
+                    nrf = (pdfNee == 0.0f) ? v3(0.0f, 0.0f, 0.0f) : (nrf / pdfNee);
                     if (nonzero(nrf)) {
                         const V3 o = nudge(sf.pos, sf.geo);
                         emitNee = true;
@@ -495,6 +712,12 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                 if (batch == kBatchLambert) {
                     bs = lambert_sample(ld3(s.lambertAlbedo + 3 * id), sf, rb.u[0], rb.u[1],
                                         aux.medium);
+                } else if (batch == kBatchLambertC) {
+                    bs = lambertc_sample(ld3(s.lambertCAlbedo + 3 * id), sf, rb.u[0], rb.u[1],
+                                         aux.medium);
+                } else if (batch == kBatchUnreal) {
+                    bs = unreal_sample(unreal_params(s.unrealParams + 6 * id), wi, sf, rb.u[2],
+                                       rb.u[0], rb.u[1], aux.medium);
                 } else if (batch == kBatchMetal) {
                     bs = metal_sample(metal_params(s.metalParams + 10 * id), wi, sf, rb.u[0],
                                       rb.u[1], aux.medium);

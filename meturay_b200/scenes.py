@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-LAMBERT, METAL, REFRACT, LIGHT = 1, 2, 3, 4
+LAMBERT, METAL, REFRACT, LIGHT, LAMBERTC, UNREAL = 1, 2, 3, 4, 5, 6
 
 
 @dataclass
@@ -99,7 +99,9 @@ class _Builder:
                 np.concatenate(self.mat).astype(np.uint32))
 
 
-def cornell(seed: int = 1, width: int = 128, height: int = 128) -> Scene:
+def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = False) -> Scene:
+    """mixed=True gives the spheres, in turn, Lambert, LambertC, Metal (GGX
+    conductor), Unreal and Refract materials (a test input for every BxDF)."""
     rng = np.random.default_rng(seed)
     b = _Builder()
     mats = []
@@ -121,16 +123,34 @@ def cornell(seed: int = 1, width: int = 128, height: int = 128) -> Scene:
     light = len(mats) - 1
     y = 0.999
     b.add(*_quad((0, y, 0), (0, y, 1), (1, y, 1), (1, y, 0), (0, -1, 0)), light)
-    for _ in range(8):
+    kinds = [LAMBERT, LAMBERTC, METAL, UNREAL, REFRACT]
+    for k in range(8):
         r = float(rng.uniform(0.1, 0.25))
         c = rng.uniform(r, 1.0 - r, 3)
-        b.add(*uv_sphere(c, r), lambert())
+        if not mixed or kinds[k % 5] == LAMBERT:
+            b.add(*uv_sphere(c, r), lambert())
+            continue
+        kind = kinds[k % 5]
+        if kind == LAMBERTC:
+            mats.append({"type": LAMBERTC, "albedo": rng.uniform(0.2, 0.8, 3).astype(np.float32)})
+        elif kind == METAL:
+            f0 = rng.uniform(0.5, 0.95, 3)
+            mats.append({"type": METAL, "eta": ((1 + np.sqrt(f0)) / (1 - np.sqrt(f0))).astype(
+                np.float32), "k": np.zeros(3, np.float32), "specular": np.ones(3, np.float32),
+                "roughness": float(rng.uniform(0.1, 0.6))})
+        elif kind == UNREAL:
+            mats.append({"type": UNREAL, "albedo": rng.uniform(0.2, 0.8, 3).astype(np.float32),
+                         "roughness": float(rng.uniform(0.2, 0.8)),
+                         "metallic": float(rng.uniform(0.0, 1.0)), "specular_scalar": 0.5})
+        else:
+            mats.append({"type": REFRACT, "albedo": np.ones(3, np.float32), "medium": 1})
+        b.add(*uv_sphere(c, r), len(mats) - 1)
     pos, nrm, uv, idx, mat = b.arrays()
     fov = math.radians(40.0)
     cam = {"position": [0.5, 0.5, -1.0], "gaze": [0.5, 0.5, 0.5], "up": [0.0, 1.0, 0.0],
            "near_far": [0.1, 100.0], "fov": [fov, fov]}
-    return Scene("cornell", pos, nrm, uv, idx, mat, mats, np.array([1.0], np.float32), 0, cam,
-                 width, height, meta={"seed": seed})
+    return Scene("cornell", pos, nrm, uv, idx, mat, mats, np.array([1.0, 1.5], np.float32), 0,
+                 cam, width, height, meta={"seed": seed, "mixed": mixed})
 
 
 def clusters(seed: int = 1, width: int = 1920, height: int = 1080, n_clusters: int = 1000,

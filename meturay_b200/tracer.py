@@ -91,6 +91,9 @@ class GPUScene:
                 if key in m:
                     getattr(mats[i], key)[:] = [float(v) for v in m[key]]
             mats[i].roughness = float(m.get("roughness", 0.0))
+            mats[i].metallic = float(m.get("metallic", 0.0))
+            if "specular_scalar" in m:
+                mats[i].specular[0] = float(m["specular_scalar"])
             mats[i].medium = int(m.get("medium", 0))
         arrs = {
             "positions": np.ascontiguousarray(scene.positions, np.float32),
@@ -188,6 +191,11 @@ class GPUScene:
         check(lib.mrb_scene_export(self._h, *[_ptr(out[k]) for k in (
             "tbn", "tri_key", "lambert", "metal", "refract", "refract_medium",
             "light_radiance", "light_prim")]))
+        n2 = np.zeros(2, np.uint32)
+        check(lib.mrb_scene_export_ext(self._h, None, None, _ptr(n2)))
+        out["lambertc"] = np.zeros((int(n2[0]), 3), np.float32)
+        out["unreal"] = np.zeros((int(n2[1]), 6), np.float32)
+        check(lib.mrb_scene_export_ext(self._h, _ptr(out["lambertc"]), _ptr(out["unreal"]), None))
         return out
 
     def export_accel(self) -> dict:

@@ -348,7 +348,7 @@ inline uint32_t lbvh_delta(const uint64_t* c, uint32_t i) {
 // Scene access helpers
 // ------------------------------------------------------------------------
 constexpr uint32_t kBatchNull = 0, kBatchLambert = 1, kBatchMetal = 2, kBatchRefract = 3,
-                   kBatchLight = 4;
+                   kBatchLight = 4, kBatchLambertC = 5, kBatchUnreal = 6;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 
 template <class T> inline V3<T> vpos(const oracle_scene* s, uint32_t v) {
@@ -853,6 +853,175 @@ BSample<T> refract_sample(V3<T> albedo, uint32_t matMedium, const oracle_scene* 
     return out;
 }
 
+// Quat::RotationBetweenZAxis (Quaternion.hpp:333-358)
+template <class T> inline Q4<T> rotation_between_z(V3<T> b) {
+    V3<T> zc(-b.y, b.x, T(0));
+    const T zd = b.z;
+    const T sn = M<T>::sqrt((T(1) - zd) * T(0.5));
+    const T cs = M<T>::sqrt((zd + T(1)) * T(0.5));
+    zc = normalize(zc);
+    if (std::fabs(zd + T(1)) < M<T>::LargeEps) return Q4<T>{T(0), T(0), T(1), T(0)};
+    if (std::fabs(zd - T(1)) < M<T>::LargeEps) return Q4<T>{T(1), T(0), T(0), T(0)};
+    return Q4<T>{cs, zc.x * sn, zc.y * sn, zc.z * sn};
+}
+// LambertConstFuncs (SimpleMaterialsKC.cuh:16-103), HemiUniformCDF
+// (HemiDistribution.h:34-51)
+template <class T>
+BSample<T> lambertc_sample(V3<T> albedo, const Surface<T>& sf, T xi0, T xi1, uint32_t medium) {
+    BSample<T> out;
+    const V3<T> n = to_space(V3<T>(0, 0, 1), sf.w2t);
+    const T c0 = M<T>::sqrt(std::fmax(T(0), T(1) - xi0 * xi0));
+    const T c1 = T(2) * M<T>::Pi * xi1;
+    T sn, cs;
+    M<T>::sincos(c1, sn, cs);
+    V3<T> d(c0 * cs, c0 * sn, xi0);
+    out.pdf = M<T>::InvPi * T(0.5f);
+    d = normalize(d);
+    d = qrotate(rotation_between_z(n), d);
+    const T nDotL = std::fabs(dot(n, d));
+    out.dir = d;
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = nDotL * albedo * M<T>::InvPi;
+    out.medium = medium;
+    return out;
+}
+template <class T> V3<T> lambertc_eval(V3<T> albedo, V3<T> wo, const Surface<T>& sf) {
+    const V3<T> n = to_space(V3<T>(0, 0, 1), sf.w2t);
+    return std::fmax(dot(n, wo), T(0)) * albedo * M<T>::InvPi;
+}
+template <class T> T lambert_pdf(V3<T> wo, const Surface<T>& sf) {
+    const V3<T> n = to_space(V3<T>(0, 0, 1), sf.w2t);
+    return std::fmax(dot(wo, n), T(0)) * M<T>::InvPi;
+}
+// MetalMatFuncs::Pdf (MetalGlassMaterialsKC.cuh:148-172)
+template <class T> T metal_pdf(const MetalP<T>& m, V3<T> wo, V3<T> wi, const Surface<T>& sf) {
+    const T alpha = m.rough * m.rough;
+    const V3<T> L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3<T> H = normalize(L + V);
+    const T NdH = std::fmax(T(0), H.z), VdH = std::fmax(T(0), dot(V, H));
+    T p = vndf_pdf(V, H, alpha);
+    const T D = dggx(NdH, alpha);
+    p = (std::isnan(D) || std::isinf(D)) ? T(0) : p;
+    return (VdH == T(0)) ? T(0) : p / (T(4) * VdH);
+}
+// UnrealDeviceFuncs (UnrealMaterialKC.cuh:19-359)
+template <class T> struct UnrealP {
+    V3<T> albedo;
+    T rough, metallic, specular;
+};
+template <class T> inline UnrealP<T> unreal_params(const float* p) {
+    return {V3<T>(p[0], p[1], p[2]), T(p[3]), T(p[4]), T(p[5])};
+}
+template <class T> inline T luminance(V3<T> c) {  // ColorConversion.h:15-21
+    return T(0.2120f) * c.x + T(0.7150f) * c.y + T(0.0722f) * c.z;
+}
+template <class T> inline T unreal_mis_ratio(T metallic, T specular, T lum) {
+    T diffuse = T(2) * M<T>::Pi * lum;
+    diffuse *= (T(1) - metallic);
+    const T specRatio = (T(1) - metallic) * specular + metallic * lum;
+    const T total = specRatio + diffuse;
+    return diffuse / total;
+}
+template <class T> inline V3<T> unreal_f0(V3<T> albedo, T metallic, T specular) {
+    specular *= T(0.08f);
+    return V3<T>(specular, specular, specular) * (T(1) - metallic) + albedo * metallic;
+}
+template <class T> inline V3<T> f_schlick(T VdH, V3<T> f0) {  // TracerFunctions.cuh:160-179
+    const T pt = T(1) - VdH;
+    T p5 = pt * pt;
+    p5 *= p5;
+    p5 *= pt;
+    V3<T> r = (V3<T>(1, 1, 1) - f0) * p5;
+    return r + f0;
+}
+template <class T>
+BSample<T> unreal_sample(const UnrealP<T>& m, V3<T> wi, const Surface<T>& sf, T xiSel, T xi0,
+                         T xi1, uint32_t medium) {
+    BSample<T> out;
+    const T alpha = m.rough * m.rough;
+    const V3<T> V = to_tangent(wi, sf.w2t);
+    T misRatio = unreal_mis_ratio(m.metallic, m.specular, luminance(m.albedo));
+    const bool diffuse = xiSel < misRatio;
+    T VdH, pdfSel, pdfOther;
+    V3<T> H, L;
+    if (diffuse) {
+        L = hemi_cosine(xi0, xi1, pdfSel);
+        H = normalize(V + L);
+        VdH = std::fmax(T(0), dot(V, H));
+        pdfOther = vndf_pdf(V, H, alpha);
+        pdfOther = (VdH == T(0)) ? T(0) : pdfOther / (T(4) * VdH);
+    } else {
+        H = vndf_sample(pdfSel, V, alpha, xi0, xi1);
+        VdH = std::fmax(T(0), dot(V, H));
+        L = T(2) * VdH * H - V;
+        pdfOther = std::fmax(T(0), L.z) * M<T>::InvPi;
+        pdfSel = (VdH == T(0)) ? T(0) : pdfSel / (T(4) * VdH);
+        misRatio = T(1) - misRatio;
+    }
+    T& pdfSpec = diffuse ? pdfOther : pdfSel;
+    pdfSpec = (VdH == T(0)) ? T(0) : pdfSpec;
+    const T LdH = std::fmax(T(0), dot(L, H)), NdH = std::fmax(T(0), H.z),
+            NdV = std::fmax(T(0), V.z);
+    const T D = dggx(NdH, alpha);
+    T G = g_smith_corr(V, L, alpha);
+    G = (LdH == T(0)) ? T(0) : G;
+    G = (VdH == T(0)) ? T(0) : G;
+    const V3<T> F = f_schlick(VdH, unreal_f0(m.albedo, m.metallic, m.specular));
+    V3<T> spec = D * F * G * T(0.25) / NdV;
+    spec = (NdV == T(0)) ? V3<T>() : spec;
+    if (std::isinf(D) || std::isnan(D)) {
+        spec = G * F / g_smith_single(V, alpha);
+        pdfSpec = diffuse ? T(0) : T(1);
+    }
+    const T NdL = std::fmax(T(0), L.z);
+    const V3<T> diffAlbedo = (T(1) - m.metallic) * m.albedo;
+    const V3<T> diffTerm = NdL * diffAlbedo * M<T>::InvPi;
+    const T w0 = misRatio * pdfSel, w1 = (T(1) - misRatio) * pdfOther;
+    const T misWeight = w0 / (w0 + w1);
+    out.pdf = (pdfSel == T(0)) ? T(0) : (misRatio * pdfSel / misWeight);
+    out.dir = to_space(L, sf.w2t);
+    out.pos = nudge(sf.pos, sf.geo);
+    out.refl = diffTerm + spec;
+    out.medium = medium;
+    return out;
+}
+template <class T>
+V3<T> unreal_eval(const UnrealP<T>& m, V3<T> wo, V3<T> wi, const Surface<T>& sf) {
+    const T alpha = m.rough * m.rough;
+    const V3<T> L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3<T> H = normalize(L + V);
+    const T LdH = std::fmax(T(0), dot(L, H)), VdH = std::fmax(T(0), dot(V, H));
+    const T NdH = std::fmax(T(0), H.z), NdV = std::fmax(T(0), V.z);
+    T D = dggx(NdH, alpha);
+    D = (std::isnan(D) || std::isinf(D)) ? T(0) : D;
+    T G = g_smith_corr(V, L, alpha);
+    G = (LdH == T(0)) ? T(0) : G;
+    G = (VdH == T(0)) ? T(0) : G;
+    const V3<T> F = f_schlick(VdH, unreal_f0(m.albedo, m.metallic, m.specular));
+    V3<T> spec = D * F * G * T(0.25) / NdV;
+    spec = (NdV == T(0)) ? V3<T>() : spec;
+    const T NdL = std::fmax(T(0), L.z);
+    const V3<T> diffTerm = NdL * ((T(1) - m.metallic) * m.albedo) * M<T>::InvPi;
+    return diffTerm + spec;
+}
+template <class T> T unreal_pdf(const UnrealP<T>& m, V3<T> wo, V3<T> wi, const Surface<T>& sf) {
+    const T alpha = m.rough * m.rough;
+    const V3<T> L = to_tangent(wo, sf.w2t), V = to_tangent(wi, sf.w2t);
+    const V3<T> H = normalize(L + V);
+    const T NdH = std::fmax(T(0), H.z), VdH = std::fmax(T(0), dot(V, H));
+    T ps = vndf_pdf(V, H, alpha);
+    const T D = dggx(NdH, alpha);
+    ps = (std::isnan(D) || std::isinf(D)) ? T(0) : ps;
+    ps = (VdH == T(0)) ? T(0) : ps / (T(4) * VdH);
+    const T pd = std::fmax(T(0), L.z) * M<T>::InvPi;
+    const T r = unreal_mis_ratio(m.metallic, m.specular, luminance(m.albedo));
+    return r * pd + (T(1) - r) * ps;
+}
+template <class T> inline T power_heuristic(T p0, T p1) {  // TracerFunctions.cuh:300-308
+    const T w0 = T(1) * p0, w1 = T(1) * p1;
+    return (w0 * w0) / (w0 * w0 + w1 * w1);
+}
+
 template <class T>
 void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t batch,
                uint32_t id, bool gen, std::vector<PRay<T>>& next) {
@@ -864,8 +1033,9 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
     V3<T> wi = -normalize(r.d);
     V3<T> rf = aux.rf;  // vacuum / sigmaT == 0 transmittance is exactly 1
     bool specular;
-    if (batch == kBatchLambert) specular = false;
+    if (batch == kBatchLambert || batch == kBatchLambertC) specular = false;
     else if (batch == kBatchMetal) specular = (T(1) - T(s->metal_params[10 * id + 9])) >= T(0.99f);
+    else if (batch == kBatchUnreal) specular = (T(1) - T(s->unreal_params[6 * id + 3])) >= T(0.99f);
     else specular = true;
     uint32_t sampleIdx = aux.sample;
     Rng4 ra = rng_block(sampleIdx, c.o->frame, aux.depth, 0, c.o->seed_lo, c.o->seed_hi);
@@ -901,14 +1071,32 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
         lpdf *= d2 / nDotL;
         lpdf *= (T(1) / static_cast<T>(lc));
         V3<T> refl;
+        T pdfBxdf = T(0);
+        const bool mis = c.o->mis != 0;
         if (batch == kBatchLambert) {
             const float* al = s->lambert_albedo + 3 * id;
             refl = lambert_eval(V3<T>(al[0], al[1], al[2]), ldir, sf);
+            if (mis) pdfBxdf = lambert_pdf(ldir, sf);
+        } else if (batch == kBatchLambertC) {
+            const float* al = s->lambertc_albedo + 3 * id;
+            refl = lambertc_eval(V3<T>(al[0], al[1], al[2]), ldir, sf);
+            if (mis) pdfBxdf = lambert_pdf(ldir, sf);
+        } else if (batch == kBatchUnreal) {
+            const UnrealP<T> up = unreal_params<T>(s->unreal_params + 6 * id);
+            refl = unreal_eval(up, ldir, wi, sf);
+            if (mis) pdfBxdf = unreal_pdf(up, ldir, wi, sf);
         } else {
-            refl = metal_eval(metal_params<T>(s->metal_params + 10 * id), ldir, wi, sf);
+            const MetalP<T> mp = metal_params<T>(s->metal_params + 10 * id);
+            refl = metal_eval(mp, ldir, wi, sf);
+            if (mis) pdfBxdf = metal_pdf(mp, ldir, wi, sf);
+        }
+        T pdfNee = lpdf;
+        if (mis) {
+            pdfNee /= power_heuristic(lpdf, pdfBxdf);
+            if (std::isnan(pdfNee)) pdfNee = T(0);
         }
         V3<T> nrf = rf * refl;
-        nrf = (lpdf == T(0)) ? V3<T>() : (nrf / lpdf);
+        nrf = (pdfNee == T(0)) ? V3<T>() : (nrf / pdfNee);
         if (nrf != V3<T>()) {
             PRay<T> o;
             o.o = nudge(sf.pos, sf.geo);
@@ -928,6 +1116,12 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
     if (batch == kBatchLambert) {
         const float* al = s->lambert_albedo + 3 * id;
         bs = lambert_sample(V3<T>(al[0], al[1], al[2]), sf, T(rb.u[0]), T(rb.u[1]), aux.medium);
+    } else if (batch == kBatchLambertC) {
+        const float* al = s->lambertc_albedo + 3 * id;
+        bs = lambertc_sample(V3<T>(al[0], al[1], al[2]), sf, T(rb.u[0]), T(rb.u[1]), aux.medium);
+    } else if (batch == kBatchUnreal) {
+        bs = unreal_sample(unreal_params<T>(s->unreal_params + 6 * id), wi, sf, T(rb.u[2]),
+                           T(rb.u[0]), T(rb.u[1]), aux.medium);
     } else if (batch == kBatchMetal) {
         bs = metal_sample(metal_params<T>(s->metal_params + 10 * id), wi, sf, T(rb.u[0]),
                           T(rb.u[1]), aux.medium);
@@ -962,18 +1156,39 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
     }
 }
 
-// PathTracerKC.cuh:335-426 (MIS off)
+// PathTracerKC.cuh:335-426
 template <class T>
-void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx) {
+void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx, uint32_t prim, T ha, T hb,
+                   T hitT) {
     const Aux<T>& aux = r.aux;
+    const oracle_scene* s = c.s;
+    const bool pathAsMis = c.o->mis && aux.type == PATH_RAY;
+    T misWeight = T(1);
+    if (pathAsMis) {
+        const Surface<T> sf = gen_surface(s, prim, ha, hb, r.d);
+        const V3<T> dir = normalize(r.d);
+        T pdfM = T(0), pdfC = T(0);
+        if (lightIdx < s->light_count) {
+            pdfM = T(1) / static_cast<T>(s->light_count);
+            uint32_t i0 = s->idx[3 * prim], i1 = s->idx[3 * prim + 1], i2 = s->idx[3 * prim + 2];
+            V3<T> p0 = vpos<T>(s, i0), p1 = vpos<T>(s, i1), p2 = vpos<T>(s, i2);
+            V3<T> cr = cross(p1 - p0, p2 - p0);
+            T area = M<T>::sqrt(dot(cr, cr)) * T(0.5);
+            V3<T> ln = to_space(V3<T>(0, 0, 1), sf.w2t);
+            T nDotL = std::fabs(dot(ln, -dir));
+            pdfC = (T(1) / area) * hitT * hitT / nDotL;
+        }
+        misWeight = power_heuristic(aux.prevPDF, pdfC * pdfM);
+    }
     bool camera = aux.type == CAMERA_RAY;
     bool specPath = aux.type == SPECULAR_PATH_RAY;
     bool neeOn = c.o->nee && aux.type == NEE_RAY;
     bool pathNeeOff = (!c.o->nee) && (aux.type == PATH_RAY || aux.type == SPECULAR_PATH_RAY);
     bool correct = neeOn && (aux.endpoint == lightIdx);
-    if (pathNeeOff || correct || camera || specPath) {
+    if (pathNeeOff || pathAsMis || correct || camera || specPath) {
         const float* e = c.s->light_radiance + 3 * lightIdx;
         V3<T> total = V3<T>(T(e[0]), T(e[1]), T(e[2])) * aux.rf;
+        total = total * misWeight;
         accumulate(c, aux.sample, total);
     }
 }
@@ -1030,7 +1245,7 @@ uint64_t render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera*
                     if (h.prim == kInvalid) continue;
                     uint32_t batch = h.key >> 24, id = h.key & 0xFFFFFFu;
                     if (batch == kBatchNull) continue;
-                    if (batch == kBatchLight) boundary_work(c, ray, id);
+                    if (batch == kBatchLight) boundary_work(c, ray, id, h.prim, h.b0, h.b1, h.t);
                     else path_work(c, ray, h.prim, h.b0, h.b1, batch, id, gen, next);
                 }
                 std::swap(cur, next);

@@ -76,6 +76,8 @@ typedef struct oracle_scene {
     const uint32_t* light_prim;
     uint32_t medium_count;   const float* medium_ior;
     uint32_t base_medium;
+    uint32_t lambertc_count; const float* lambertc_albedo;  /* 3 each */
+    uint32_t unreal_count;   const float* unreal_params;    /* albedo3 rough metal spec */
 } oracle_scene;
 
 typedef struct oracle_camera {

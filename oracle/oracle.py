@@ -36,7 +36,9 @@ class Scene(C.Structure):
                 ("light_count", C.c_uint32), ("light_radiance", C.c_void_p),
                 ("light_prim", C.c_void_p),
                 ("medium_count", C.c_uint32), ("medium_ior", C.c_void_p),
-                ("base_medium", C.c_uint32)]
+                ("base_medium", C.c_uint32),
+                ("lambertc_count", C.c_uint32), ("lambertc_albedo", C.c_void_p),
+                ("unreal_count", C.c_uint32), ("unreal_params", C.c_void_p)]
 
 
 class Camera(C.Structure):
@@ -151,6 +153,9 @@ class OracleScene:
             "light_radiance": np.ascontiguousarray(exported["light_radiance"], np.float32),
             "light_prim": np.ascontiguousarray(exported["light_prim"], np.uint32),
             "medium_ior": np.ascontiguousarray(scene.medium_ior, np.float32),
+            "lambertc": np.ascontiguousarray(exported.get("lambertc", np.zeros((0, 3))),
+                                             np.float32),
+            "unreal": np.ascontiguousarray(exported.get("unreal", np.zeros((0, 6))), np.float32),
         }
         a = self.arrays
         s = Scene()
@@ -166,6 +171,8 @@ class OracleScene:
         s.light_radiance, s.light_prim = _p(a["light_radiance"]), _p(a["light_prim"])
         s.medium_count, s.medium_ior = a["medium_ior"].shape[0], _p(a["medium_ior"])
         s.base_medium = scene.base_medium
+        s.lambertc_count, s.lambertc_albedo = a["lambertc"].shape[0], _p(a["lambertc"])
+        s.unreal_count, s.unreal_params = a["unreal"].shape[0], _p(a["unreal"])
         self.c = s
         st = C.c_int(0)
         self.bvh = lib.oracle_bvh_create(C.byref(s), C.byref(st))
@@ -194,7 +201,8 @@ class OracleScene:
 
     def render(self, camera_frame: np.ndarray, width: int, height: int, samples: int,
                max_depth: int, rr_start: int, nee: bool, seed: int, frame: int = 0,
-               threads: int = 0, rows: tuple[int, int] = (0, 0), fp64: bool = False):
+               threads: int = 0, rows: tuple[int, int] = (0, 0), fp64: bool = False,
+               mis: bool = False):
         """Per-sample radiance ((h*s), (w*s), 3) and the rays traced."""
         cam = Camera()
         f = camera_frame
@@ -204,7 +212,7 @@ class OracleScene:
         cam.up[:] = [float(v) for v in f[9:12]]
         cam.plane_size[:] = [float(v) for v in f[12:14]]
         cam.near_far[:] = [float(v) for v in f[14:16]]
-        o = Options(width, height, samples, max_depth, rr_start, 1 if nee else 0, 0,
+        o = Options(width, height, samples, max_depth, rr_start, 1 if nee else 0, 1 if mis else 0,
                     seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, frame, threads, rows[0], rows[1])
         out = np.zeros((height * samples, width * samples, 3), np.float64 if fp64 else np.float32)
         fn = lib.oracle_render_f64 if fp64 else lib.oracle_render
@@ -219,9 +227,16 @@ def scene_tables(scene) -> dict:
     order (GPULightPrimitive: one GPULight per primitive)."""
     mats = scene.materials
     key = np.zeros(len(mats), np.uint32)
-    lam, met, ref, refm = [], [], [], []
+    lam, met, ref, refm, lamc, unr = [], [], [], [], [], []
     for i, m in enumerate(mats):
         t = int(m["type"])
+        if t == 5:
+            key[i] = (5 << 24) | len(lamc)
+            lamc.append(np.asarray(m["albedo"], np.float32))
+        elif t == 6:
+            key[i] = (6 << 24) | len(unr)
+            unr.append(np.array(list(m["albedo"]) + [m["roughness"], m.get("metallic", 0.0),
+                                                     m.get("specular_scalar", 0.0)], np.float32))
         if t == 1:
             key[i] = (1 << 24) | len(lam)
             lam.append(np.asarray(m["albedo"], np.float32))
@@ -248,7 +263,10 @@ def scene_tables(scene) -> dict:
             "refract": np.array(ref, np.float32).reshape(-1, 3) if ref else z3,
             "refract_medium": np.array(refm, np.uint32),
             "light_radiance": light_rad,
-            "light_prim": light_tris.astype(np.uint32)}
+            "light_prim": light_tris.astype(np.uint32),
+            "lambertc": np.array(lamc, np.float32).reshape(-1, 3) if lamc else z3,
+            "unreal": np.array(unr, np.float32).reshape(-1, 6) if unr else np.zeros((0, 6),
+                                                                                  np.float32)}
 
 
 def build_tbn(scene) -> np.ndarray:

@@ -110,3 +110,26 @@ def test_cornell_fp64_error_is_stated(system, oracle):
     err = _rel_mean_err(gpu, ref64)
     print(f"FP32 image vs FP64 oracle: relative mean error {err:.3e}")
     assert np.isfinite(err)
+
+
+@pytest.mark.parametrize("mis", [0, 1])
+def test_every_bxdf_with_and_without_mis(system, oracle, mis):
+    """Lambert, LambertC, Metal, Unreal and Refract spheres; NEE with and
+    without direct-light MIS (PathTracerKC.cuh:358-380,520-540)."""
+    from meturay_b200 import camera_frame, scenes
+    scene = scenes.cornell(seed=6, width=64, height=64, mixed=True)
+    opts = dict(CORNELL_OPTS, DirectLightMIS=mis, Seed=3)
+    g, t = _setup(system, scene, opts)
+    t.generate_work()
+    while t.render():
+        pass
+    t.finalize()
+    gpu = t.sample_radiance()[..., :3]
+    os_ = oracle.OracleScene(scene, g.export())
+    cf = np.concatenate([camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
+    ref, ref_rays = os_.render(cf, scene.width, scene.height, opts["Samples"], opts["MaxDepth"],
+                               opts["RussianRouletteStart"], True, opts["Seed"], mis=bool(mis))
+    rays, _ = t.stats()
+    assert rays == ref_rays
+    assert gpu.sum() > 0
+    assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
