@@ -36,15 +36,16 @@ WORKLOAD = {"workload": "clusters-1M plain path tracing", "triangles": 1000004,
             "resolution": "1920x1080", "spp_per_step": 1, "max_depth": 8,
             "nee": True, "rr_start": 3, "scene_seed": 1,
             "l2": "inputs larger than L2 (ray/hit buffers ~470 MB, BVH ~180 MB)"}
-TRACE_PROFILE = "k_trace_clusters1M_bvh2.md"
+# committed ncu summaries of the traversal kernel, per traversal mode
+TRACE_PROFILE = {0: "k_trace_clusters1M_bvh2.md", 1: "k_trace_wide_clusters1M.md"}
 OPTS = {"Samples": 1, "MaxDepth": 8, "NextEventEstimation": 1, "RussianRouletteStart": 3,
         "DirectLightMIS": 0}
 
 
-def _traffic_per_launch():
+def _traffic_per_launch(traversal):
     """DRAM bytes per traversal launch from the committed ncu summary."""
     import re
-    f = ROOT / "profiles" / TRACE_PROFILE
+    f = ROOT / "profiles" / TRACE_PROFILE[traversal]
     if not f.exists():
         return None
     m = re.search(r"dram_bytes_per_launch \(mean of \d+\): (\d+)", f.read_text())
@@ -199,7 +200,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                    + 48 * prof["tri_tests"])
     trace_s = prof["trace_ms"] / 1e3
     achieved = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
-    traffic = _traffic_per_launch()
+    traffic = _traffic_per_launch(args.traversal)
     return {
         "metric": METRIC,
         "value": rays / (ms / 1e3) / 1e6,

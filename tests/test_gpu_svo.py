@@ -59,7 +59,13 @@ def test_svo_leaf_normals_are_unit_directions(system):
     az = (pn & 0xFFFF) / 65535.0 * 2 * np.pi - np.pi
     inc = (pn >> 16) / 65535.0 * np.pi
     n = np.stack([np.cos(az) * np.sin(inc), np.sin(az) * np.sin(inc), np.cos(inc)], 1)
-    # floor voxels (lowest y layer, away from walls) carry the floor normal +y
+    # floor voxels (lowest y layer, away from walls) carry the floor's
+    # geometric normal, cross(p1 - p0, p2 - p0) as the reference voxeliser
+    # takes it (GPUPrimitiveTriangle.h:434-435); the floor's winding gives -y
+    p = scene.positions[scene.indices[0]].astype(np.float64)
+    gn = np.cross(p[1] - p[0], p[2] - p[0])
+    gn /= np.linalg.norm(gn)
+    assert abs(abs(gn[1]) - 1.0) < 1e-12
     codes = s["leaf_codes"]
     def decode(c, shift):
         v = np.zeros_like(c)
@@ -71,4 +77,4 @@ def test_svo_leaf_normals_are_unit_directions(system):
     z = decode(codes, 2)
     floor = (y == y.min()) & (x > 20) & (x < 100) & (z > 20) & (z < 100)
     assert floor.sum() > 100
-    assert np.median(n[floor][:, 1]) > 0.99
+    assert np.median(n[floor][:, 1] * gn[1]) > 0.99
