@@ -156,19 +156,49 @@ int mrb_svo_build(mrb_scene* scene, uint32_t resolution, void* stream);
 int mrb_svo_info(const mrb_scene* scene, uint32_t* info6, float* params7);
 /* Host copies: packed nodes (child 0-26 | parent 27-54 | child mask 55-62
  * | children-are-leaves 63; AnisoSVO.cuh:125-151), leaf parents, sorted
- * unique leaf Morton codes, packed leaf normals, leaf light HitKeys, level
- * offsets (depth + 2).  NULL skips. */
+ * unique leaf Morton codes, leaf normal words (VoxelPayload packing, see
+ * mrb_svo_export_payload), leaf light HitKeys, level offsets (depth + 2).
+ * NULL skips. */
 int mrb_svo_export(const mrb_scene* scene, uint64_t* nodes, uint32_t* leaf_parents,
                    uint64_t* leaf_codes, uint32_t* leaf_normals, uint32_t* leaf_lights,
                    uint32_t* level_offsets);
 
-/* ---- tracer "PathTracer": GPUTracerI (RayLib/GPUTracerI.h:24-71) ---- */
+/* Radiance-cache payload of the scene-level octree (VoxelPayload,
+ * AnisoSVO.cuh:22-114): node normal words (normal x,y 9+9 bits | length 7 |
+ * specular 6 | z sign 1; the leaf words come from mrb_svo_export), leaf
+ * radiance sums (2 per leaf, 2^24 fixed point), leaf sample counts (2 per
+ * leaf), leaf and node averages (half2, front | back << 16).  NULL skips. */
+int mrb_svo_export_payload(const mrb_scene* scene, uint32_t* node_norm_spec, uint64_t* leaf_irr,
+                           uint32_t* leaf_cnt, uint32_t* leaf_avg, uint32_t* node_avg);
+
+/* ---- tracers: GPUTracerI (RayLib/GPUTracerI.h:24-71) ----
+ * type "PathTracer" (PathTracer.cu) or "WFPGTracer" (WFPGTracer.cu, product
+ * path guiding over the tracer's own voxel octree). */
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out);
 void mrb_tracer_destroy(mrb_tracer* t);
 /* SetOptions keys (PathTracer.h:17-33): "Samples", "MaxDepth",
  * "NextEventEstimation", "RussianRouletteStart", "DirectLightMIS",
- * plus "Seed" (RNG key) and "Frame" (RNG iteration counter). */
+ * plus "Seed" (RNG key) and "Frame" (RNG iteration counter).  WFPGTracer
+ * also takes (WFPGTracer.h:25-56) "OctreeLevel", "MinRayBinLevel",
+ * "BinRayCount", "DoProductPathGuiding" (true only), "PurePG", "SkipPG",
+ * "GuideBounceAmount", "OmitDirectRadiance". */
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
+/* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha". */
+int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double value);
+/* The WFPG tracer's octree (built at first use): info/params as
+ * mrb_svo_info, and its structure plus payload as mrb_svo_export and
+ * mrb_svo_export_payload.  NULL skips. */
+int mrb_tracer_svo_info(mrb_tracer* t, uint32_t* info6, float* params7);
+int mrb_tracer_svo_export(mrb_tracer* t, uint64_t* nodes, uint32_t* leaf_parents,
+                          uint64_t* leaf_codes, uint32_t* leaf_norm_spec, uint32_t* leaf_lights,
+                          uint32_t* level_offsets, uint32_t* node_norm_spec, uint64_t* leaf_irr,
+                          uint32_t* leaf_cnt, uint32_t* leaf_avg, uint32_t* node_avg);
+/* Guide state of the wavefront shaded by the last Render() step of a WFPG
+ * frame: ray count, per ray its path (sample) index and guide words (uv
+ * half2 | pdf half + flags bit16 BxDF-selected, bit17 valid), and the
+ * bin-sorted keys with their ray indices.  NULL skips. */
+int mrb_tracer_guide_export(mrb_tracer* t, uint32_t* count, uint32_t* samples, uint32_t* guide2,
+                            uint32_t* sorted_bin_key, uint32_t* sorted_rid);
 int mrb_tracer_set_resolution(mrb_tracer* t, uint32_t width, uint32_t height);
 int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* cam);
 /* The camera frame as the device sees it (14 floats: position, bottom-left,

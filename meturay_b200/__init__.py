@@ -7,7 +7,8 @@ The compute path is ``libmrb200.so`` (hand-written CUDA, C ABI in
 reference's plugin interfaces over that ABI.
 """
 from ._lib import MrbError, lib  # noqa: F401  (fails loudly if the library is missing)
-from .tracer import GPUScene, PathTracer, TracerSystem, camera_frame  # noqa: F401
+from .tracer import GPUScene, PathTracer, TracerSystem, WFPGTracer, camera_frame  # noqa: F401
 from . import scenes  # noqa: F401
 
-__all__ = ["TracerSystem", "GPUScene", "PathTracer", "MrbError", "scenes", "camera_frame"]
+__all__ = ["TracerSystem", "GPUScene", "PathTracer", "WFPGTracer", "MrbError", "scenes",
+           "camera_frame"]

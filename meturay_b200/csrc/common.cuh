@@ -100,6 +100,7 @@ struct PathOptions {
     uint32_t maxDepth, rrStart, nee, mis;
     uint32_t seedLo, seedHi;
     const uint32_t* frame;             // device word: iteration index (RNG counter)
+    uint32_t wfpg;                     // WFPG tracer: camera rays at depth 1, path chain kept
 };
 
 // ---------------------------------------------------------------------------

@@ -4,7 +4,10 @@
 //   mrb_system  <- TracerSystemI / TracerSystemCUDA (TracerSystemCUDA.cpp:19-100)
 //   mrb_scene   <- GPUSceneI with one triangle primitive group, its material
 //                  groups, primitive lights and the "LBVH" accelerator group
-//   mrb_tracer  <- GPUTracerI "PathTracer" (PathTracer.cu:144-326)
+//   mrb_tracer  <- GPUTracerI "PathTracer" (PathTracer.cu:144-326) and
+//                  "WFPGTracer" (WFPGTracer.cu:435-1833): the same wavefront
+//                  with a per-depth guiding step and a per-frame radiance
+//                  deposit into the tracer's own voxel octree
 // The wavefront loop keeps every count on the device: trace -> partition ->
 // shade per depth with no host synchronisation, and a whole frame can be
 // captured once as a CUDA graph and replayed.
@@ -23,6 +26,7 @@
 #include "trace.cuh"
 #include "wide.cuh"
 #include "svo.cuh"
+#include "guide.cuh"
 
 namespace mrb {
 
@@ -298,10 +302,23 @@ struct mrb_tracer {
     uint32_t depth = 0;
     bool working = false;
     uint32_t frames = 0;
+    // WFPG tracer (WFPGTracer.h:58-96 defaults)
+    bool wfpg = false;
+    uint32_t octreeLevel = 10, minRayBinLevel = 5, binRayCount = 512, productPG = 1, purePG = 0,
+             skipPG = 0, guideBounce = 512, omitDirect = 0;
+    float misRatio = 0.5f, filterAlpha = 1.0f;
+    bool svoReady = false;
+    SvoParams svoP{};
+    SvoResult svo;
+    DBuf chainA, chainB, chainNee, chainPath, binKey, binRid, heads, headScan, binBegin, binEnd,
+        guideSort, guideScan, guideBuf, payloadBackup;
+    size_t guideSortBytes = 0;
+    uint32_t chainPaths = 0, chainLevels = 0;
     // graph
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
     ~mrb_tracer() {
+        if (svoReady) svo_free(svo);
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
         if (hostCam) cudaFreeHost(hostCam);
@@ -346,6 +363,25 @@ int ensure_buffers(mrb_tracer* t) {
     if ((r = t->errorFlags.alloc(16))) return r;
     t->sortTempBytes = radix_sort_temp_bytes(maxRays, 4, 0, 3 + 24);
     if ((r = t->sortTemp.alloc(t->sortTempBytes))) return r;
+    if (t->wfpg) {
+        const size_t levels = size_t(t->maxDepth) + 1;
+        const size_t chain = levels * paths * 16;
+        if ((r = t->chainA.alloc(chain)) || (r = t->chainB.alloc(chain)) ||
+            (r = t->chainNee.alloc(chain)) || (r = t->chainPath.alloc(chain)) ||
+            (r = t->binKey.alloc(size_t(maxRays) * 4)) || (r = t->binRid.alloc(size_t(maxRays) * 4)) ||
+            (r = t->heads.alloc((size_t(maxRays) + 1) * 4)) ||
+            (r = t->headScan.alloc((size_t(maxRays) + 1) * 4)) ||
+            (r = t->binBegin.alloc(size_t(maxRays) * 4)) || (r = t->binEnd.alloc(size_t(maxRays) * 4)) ||
+            (r = t->guideScan.alloc(guide_scan_temp_bytes(maxRays))) ||
+            (r = t->guideBuf.alloc(size_t(maxRays) * 8)))
+            return r;
+        t->guideSortBytes = guide_sort_temp_bytes(maxRays);
+        if ((r = t->guideSort.alloc(t->guideSortBytes))) return r;
+        // frame stamps start out matching no frame
+        MRB_CUDA(cudaMemsetAsync(t->chainA.p, 0xFF, chain, t->stream));
+        t->chainPaths = static_cast<uint32_t>(paths);
+        t->chainLevels = static_cast<uint32_t>(levels);
+    }
     MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->counters.p, 0, 16, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->errorFlags.p, 0, 16, t->stream));
@@ -366,7 +402,61 @@ PathOptions path_options(const mrb_tracer* t) {
     o.seedLo = static_cast<uint32_t>(t->seed);
     o.seedHi = static_cast<uint32_t>(t->seed >> 32);
     o.frame = t->frameWord.as<uint32_t>();
+    o.wfpg = t->wfpg ? 1 : 0;
     return o;
+}
+
+PathChain path_chain(const mrb_tracer* t) {
+    PathChain c{};
+    if (!t->wfpg) return c;
+    c.nodeA = t->chainA.as<float4>();
+    c.nodeB = t->chainB.as<float4>();
+    c.contribNee = t->chainNee.as<float4>();
+    c.contribPath = t->chainPath.as<float4>();
+    c.paths = t->chainPaths;
+    c.levels = t->chainLevels;
+    return c;
+}
+
+GuideOptions guide_options(const mrb_tracer* t) {
+    GuideOptions g{};
+    g.minBinLevel = std::min(t->octreeLevel, t->minRayBinLevel);
+    g.binRayCount = t->binRayCount;
+    g.purePG = t->purePG;
+    g.misRatio = t->misRatio;
+    // StaticGaussianFilter1D<11> (BlockTextureFilter.cuh:72-110): taps
+    // exp(-t^2 / (2 alpha)) normalised to sum 1, evaluated in double
+    double w[11], tot = 0.0;
+    for (int i = 0; i < 11; i++) {
+        const double x = double(i - 5);
+        w[i] = std::exp(-(x * x) * 0.5 / double(t->filterAlpha));
+        tot += w[i];
+    }
+    for (int i = 0; i < 11; i++) g.filter[i] = static_cast<float>(w[i] / tot);
+    return g;
+}
+
+// The tracer's own octree: AnisoSVOctreeCPU::Constrcut at
+// WFPGTracer::Initialize, resolution 2^OctreeLevel.
+int ensure_svo(mrb_tracer* t) {
+    if (!t->wfpg || t->svoReady) return 0;
+    mrb_scene* sc = t->scene;
+    float ext[8];
+    MRB_CUDA(cudaMemcpyAsync(ext, sc->aExtent.p, 24, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    t->svoP = svo_params(ext, 1u << t->octreeLevel);
+    SvoBuildIn in{sc->T, sc->dPos.as<float>(), sc->dIdx.as<uint32_t>(), sc->dKey.as<uint32_t>(),
+                  sc->dLightRad.as<float>(), t->omitDirect};
+    int r = svo_build(in, t->svoP, t->svo, t->stream);
+    if (!r) r = svo_payload_finish(guide_dev(t->svo, t->svoP), t->svo, t->stream);
+    if (r) {
+        svo_free(t->svo);
+        return r;
+    }
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    t->svoReady = true;
+    t->graphDirty = true;
+    return 0;
 }
 
 PortionTable portion_table(const mrb_tracer* t) {
@@ -387,7 +477,7 @@ int step_camera(mrb_tracer* t) {
     return camera_generate(t->devCam.as<CameraDev>(), path_options(t), t->scene->baseMedium,
                            t->rayO[0].as<float4>(),
                            t->rayD[0].as<float4>(), t->aux[0].as<RayAux>(),
-                           t->samplesBuf.as<float4>(), cnt, t->stream);
+                           t->samplesBuf.as<float4>(), cnt, path_chain(t), t->stream);
 }
 
 struct StageTimer {
@@ -431,6 +521,18 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
             return r;
     }
     if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
+    const bool guideNow = t->wfpg && !t->skipPG && d < t->guideBounce;
+    if (guideNow) {
+        GuideWave gw{t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(), t->aux[cur].as<RayAux>(),
+                     HitIn{ho.key, ho.prim, ho.t, ho.bary}, cnt + cur, t->maxRays};
+        GuideScratch gs{t->binKey.as<uint32_t>(), t->binRid.as<uint32_t>(), t->heads.as<uint32_t>(),
+                        t->headScan.as<uint32_t>(), t->binBegin.as<uint32_t>(),
+                        t->binEnd.as<uint32_t>(), t->guideSort.p, t->guideSortBytes,
+                        t->guideScan.p, t->guideBuf.as<uint2>()};
+        if ((r = guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), t->svo, gw, gs,
+                                 guide_options(t), path_options(t), d, d, t->stream)))
+            return r;
+    }
     if (mark(2)) return MRB_E_CUDA;
     PortionTable pt = portion_table(t);
     if ((r = dense_keys(ho.key, cnt + cur, t->maxRays, sc->idBits, t->dense.as<uint32_t>(), pt,
@@ -451,14 +553,22 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
     r = shade(sc->dev(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
               t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull, t->maxRays,
               t->samplesBuf.as<float4>(), path_options(t), gen, t->rayO[nxt].as<float4>(),
-              t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(), cnt + nxt, t->stream);
+              t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(), cnt + nxt, path_chain(t),
+              guideNow ? t->guideBuf.as<uint2>() : nullptr, t->stream);
     if (r) return r;
     if (mark(5) || lap(3, 4)) return MRB_E_CUDA;
     return 0;
 }
 
 int step_finalize(mrb_tracer* t) {
-    int r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
+    int r;
+    if (t->wfpg) {
+        // WFPGTracer::Finalize: AccumulateRaidances + NormalizeAndFilterRadiance
+        const GuideDev g = guide_dev(t->svo, t->svoP);
+        if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream))) return r;
+        if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
+    }
+    r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
                     t->image.as<float4>(), t->stream);
     if (r) return r;
     return frame_advance(t->frameWord.as<uint32_t>(), t->stream);
@@ -479,20 +589,77 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
     const uint32_t bits = 3 + t->scene->idBits;
     const uint32_t passes = (bits + 7) / 8;
     const uint32_t sort = 2 + passes + (passes & 1);
-    return 1 + t->maxDepth * (3 + sort + 2) + 2;
+    uint32_t n = 1 + t->maxDepth * (3 + sort + 2) + 2;
+    if (t->wfpg && t->svoReady) {
+        // guiding per guided depth; deposit, leaf averages and the two
+        // level filters per frame
+        const uint32_t guided = t->skipPG ? 0u : std::min(t->maxDepth, t->guideBounce);
+        n += guided * guide_launches(t->svo, guide_options(t), t->maxRays) + 2 + 2 * t->svoP.depth;
+    }
+    return n;
 }
 
 int check_device_errors(mrb_tracer* t) {
-    uint32_t e[2] = {0, 0};
+    uint32_t e[3] = {0, 0, 0};
     MRB_CUDA(cudaMemcpyAsync(e, t->errorFlags.p, 4, cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaMemcpyAsync(e + 1, radix_sort_error_flag(t->sortTemp.p, t->maxRays), 4,
                              cudaMemcpyDeviceToHost, t->stream));
+    if (t->wfpg && t->guideSort.p)
+        MRB_CUDA(cudaMemcpyAsync(e + 2, radix_sort_error_flag(t->guideSort.p, t->maxRays), 4,
+                                 cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaStreamSynchronize(t->stream));
-    if (e[0] || e[1]) {
-        set_error("device-side limit hit (trace flag %u, sort flag %u)", e[0], e[1]);
+    if (e[0] || e[1] || e[2]) {
+        set_error("device-side limit hit (trace flag %u, sort flags %u %u)", e[0], e[1], e[2]);
         return MRB_E_DEVICE;
     }
     return 0;
+}
+
+int svo_copy(void* dst, const void* src, size_t bytes) {
+    if (!dst || !bytes) return 0;
+    MRB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int export_svo(const SvoResult& v, uint64_t* nodes, uint32_t* leafParents, uint64_t* leafCodes,
+               uint32_t* leafNormSpec, uint32_t* leafLight, uint32_t* levelOffsets) {
+    if (svo_copy(nodes, v.nodes, size_t(v.nodeCount) * 8) ||
+        svo_copy(leafParents, v.leafParents, size_t(v.leafCount) * 4) ||
+        svo_copy(leafCodes, v.leafCodes, size_t(v.leafCount) * 8) ||
+        svo_copy(leafNormSpec, v.leafNormSpec, size_t(v.leafCount) * 4) ||
+        svo_copy(leafLight, v.leafLight, size_t(v.leafCount) * 4))
+        return MRB_E_CUDA;
+    if (levelOffsets)
+        std::memcpy(levelOffsets, v.levelOffsets.data(), v.levelOffsets.size() * 4);
+    return 0;
+}
+
+int export_payload(const SvoResult& v, uint32_t* nodeNormSpec, uint64_t* leafIrr,
+                   uint32_t* leafCnt, uint32_t* leafAvg, uint32_t* nodeAvg) {
+    const size_t U = v.leafCount, N = v.nodeCount;
+    if (svo_copy(nodeNormSpec, v.nodeNormSpec, N * 4) || svo_copy(leafIrr, v.leafIrr, U * 16) ||
+        svo_copy(leafCnt, v.leafCnt, U * 8) || svo_copy(leafAvg, v.leafAvg, U * 4) ||
+        svo_copy(nodeAvg, v.nodeAvg, N * 4))
+        return MRB_E_CUDA;
+    return 0;
+}
+
+void svo_info(const SvoResult& v, const SvoParams& p, uint32_t* info, float* params) {
+    if (info) {
+        info[0] = v.voxelCount;
+        info[1] = v.leafCount;
+        info[2] = v.nodeCount;
+        info[3] = p.depth;
+        info[4] = p.res;
+        info[5] = static_cast<uint32_t>(v.levelOffsets.size());
+    }
+    if (params) {
+        for (int c = 0; c < 3; c++) {
+            params[c] = p.lo[c];
+            params[3 + c] = p.hi[c];
+        }
+        params[6] = p.leafVoxelSize;
+    }
 }
 
 int set_device(mrb_system* s) {
@@ -825,8 +992,11 @@ int mrb_svo_build(mrb_scene* s, uint32_t resolution, void* stream) {
         s->svoBuilt = false;
     }
     s->svoP = svo_params(ext, resolution);
-    SvoBuildIn in{s->T, s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>()};
+    SvoBuildIn in{s->T, s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>(),
+                  s->dLightRad.as<float>(), 0u};
     int r = svo_build(in, s->svoP, s->svo, st);
+    if (!r) r = svo_payload_finish(guide_dev(s->svo, s->svoP), s->svo, st);
+    if (!r) MRB_CUDA(cudaStreamSynchronize(st));
     if (r) {
         svo_free(s->svo);
         return r;
@@ -840,21 +1010,7 @@ int mrb_svo_info(const mrb_scene* s, uint32_t* info, float* params) {
         set_error("SVO not built");
         return MRB_E_STATE;
     }
-    if (info) {
-        info[0] = s->svo.voxelCount;
-        info[1] = s->svo.leafCount;
-        info[2] = s->svo.nodeCount;
-        info[3] = s->svoP.depth;
-        info[4] = s->svoP.res;
-        info[5] = static_cast<uint32_t>(s->svo.levelOffsets.size());
-    }
-    if (params) {
-        for (int c = 0; c < 3; c++) {
-            params[c] = s->svoP.lo[c];
-            params[3 + c] = s->svoP.hi[c];
-        }
-        params[6] = s->svoP.leafVoxelSize;
-    }
+    svo_info(s->svo, s->svoP, info, params);
     return 0;
 }
 
@@ -865,20 +1021,16 @@ int mrb_svo_export(const mrb_scene* s, uint64_t* nodes, uint32_t* leafParents,
         set_error("SVO not built");
         return MRB_E_STATE;
     }
-    const SvoResult& v = s->svo;
-    auto cp = [](void* dst, const void* src, size_t bytes) -> int {
-        if (!dst || !bytes) return 0;
-        MRB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
-        return 0;
-    };
-    if (cp(nodes, v.nodes, size_t(v.nodeCount) * 8) || cp(leafParents, v.leafParents, size_t(v.leafCount) * 4) ||
-        cp(leafCodes, v.leafCodes, size_t(v.leafCount) * 8) ||
-        cp(leafNormal, v.leafNormal, size_t(v.leafCount) * 4) ||
-        cp(leafLight, v.leafLight, size_t(v.leafCount) * 4))
-        return MRB_E_CUDA;
-    if (levelOffsets)
-        std::memcpy(levelOffsets, v.levelOffsets.data(), v.levelOffsets.size() * 4);
-    return 0;
+    return export_svo(s->svo, nodes, leafParents, leafCodes, leafNormal, leafLight, levelOffsets);
+}
+
+int mrb_svo_export_payload(const mrb_scene* s, uint32_t* nodeNormSpec, uint64_t* leafIrr,
+                           uint32_t* leafCnt, uint32_t* leafAvg, uint32_t* nodeAvg) {
+    if (!s || !s->svoBuilt) {
+        set_error("SVO not built");
+        return MRB_E_STATE;
+    }
+    return export_payload(s->svo, nodeNormSpec, leafIrr, leafCnt, leafAvg, nodeAvg);
 }
 
 int mrb_accel_set_traversal(mrb_scene* s, int mode) {
@@ -901,8 +1053,10 @@ int mrb_accel_info(const mrb_scene* s, uint32_t* info) {
 
 int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_tracer** out) {
     if (!sys || !scene || !out) return MRB_E_ARG;
-    if (!type || std::strcmp(type, "PathTracer") != 0) {
-        set_error("tracer type '%s' is not supported (PathTracer only)", type ? type : "(null)");
+    const bool wfpg = type && std::strcmp(type, "WFPGTracer") == 0;
+    if (!type || (!wfpg && std::strcmp(type, "PathTracer") != 0)) {
+        set_error("tracer type '%s' is not supported (PathTracer, WFPGTracer)",
+                  type ? type : "(null)");
         return MRB_E_UNSUPPORTED;
     }
     if (!scene->built) {
@@ -913,6 +1067,8 @@ int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_t
     mrb_tracer* t = new mrb_tracer();
     t->sys = sys;
     t->scene = scene;
+    t->wfpg = wfpg;
+    if (wfpg) t->maxDepth = 10;  // WFPGTracer::Options::maximumDepth
     cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&t->hostCam), sizeof(CameraDev));
     if (e != cudaSuccess) {
@@ -929,6 +1085,29 @@ int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_t
 }
 
 void mrb_tracer_destroy(mrb_tracer* t) { delete t; }
+
+int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double v) {
+    if (!t || !name) return MRB_E_ARG;
+    std::string k(name);
+    if (t->wfpg && k == "BXDF-GuideMISRatio") {
+        if (!(v >= 0.0 && v <= 1.0)) {
+            set_error("BXDF-GuideMISRatio must be in [0, 1]");
+            return MRB_E_ARG;
+        }
+        t->misRatio = static_cast<float>(v);
+    } else if (t->wfpg && k == "RFieldFilterAlpha") {
+        if (!(v > 0.0)) {
+            set_error("RFieldFilterAlpha must be > 0");
+            return MRB_E_ARG;
+        }
+        t->filterAlpha = static_cast<float>(v);
+    } else {
+        set_error("unknown float option '%s'", name);
+        return MRB_E_ARG;
+    }
+    t->graphDirty = true;
+    return 0;
+}
 
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
     if (!t || !name) return MRB_E_ARG;
@@ -953,6 +1132,38 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
         t->mis = v ? 1 : 0;
     } else if (k == "Seed") {
         t->seed = v;
+    } else if (t->wfpg && (k == "OctreeLevel" || k == "OmitDirectRadiance")) {
+        if (k == "OctreeLevel" && (v < 1 || v > 10)) {
+            set_error("OctreeLevel must be in [1, 10]");
+            return MRB_E_ARG;
+        }
+        if (k == "OctreeLevel") t->octreeLevel = uint32_t(v);
+        else t->omitDirect = v ? 1 : 0;
+        if (t->svoReady) {
+            MRB_CUDA(cudaStreamSynchronize(t->stream));
+            svo_free(t->svo);
+            t->svoReady = false;
+        }
+    } else if (t->wfpg && k == "MinRayBinLevel") {
+        t->minRayBinLevel = uint32_t(v);
+    } else if (t->wfpg && k == "BinRayCount") {
+        if (v == 0 || v > 0x7FFFFFFF) {
+            set_error("BinRayCount must be in [1, 2^31)");
+            return MRB_E_ARG;
+        }
+        t->binRayCount = uint32_t(v);
+    } else if (t->wfpg && k == "DoProductPathGuiding") {
+        if (!v) {
+            set_error("DoProductPathGuiding=false (non-product 2D PWC guiding) is not built");
+            return MRB_E_UNSUPPORTED;
+        }
+        t->productPG = 1;
+    } else if (t->wfpg && k == "PurePG") {
+        t->purePG = v ? 1 : 0;
+    } else if (t->wfpg && k == "SkipPG") {
+        t->skipPG = v ? 1 : 0;
+    } else if (t->wfpg && k == "GuideBounceAmount") {
+        t->guideBounce = uint32_t(v);
     } else if (k == "Frame") {
         if (t->frameWord.p) {
             uint32_t f = uint32_t(v);
@@ -1037,6 +1248,7 @@ int mrb_tracer_generate_work(mrb_tracer* t, uint32_t) {
     if (set_device(t->sys)) return MRB_E_CUDA;
     int r = ensure_buffers(t);
     if (r) return r;
+    if ((r = ensure_svo(t))) return r;
     if ((r = step_camera(t))) return r;
     t->depth = 0;
     t->working = true;
@@ -1074,6 +1286,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
     if (set_device(t->sys)) return MRB_E_CUDA;
     int r = ensure_buffers(t);
     if (r) return r;
+    if ((r = ensure_svo(t))) return r;
     if (t->graphDirty || !t->graph) {
         if (t->graph) {
             cudaGraphExecDestroy(t->graph);
@@ -1084,8 +1297,26 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         uint32_t f0 = 0;
         MRB_CUDA(cudaMemcpyAsync(&f0, t->frameWord.p, 4, cudaMemcpyDeviceToHost, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
+        // the octree's radiance state of a WFPG tracer is put back too
+        const size_t U = t->svo.leafCount, N = t->svo.nodeCount;
+        const size_t pb = t->wfpg ? U * 16 + U * 8 + U * 4 + N * 4 : 0;
+        if (pb) {
+            if ((r = t->payloadBackup.alloc(pb))) return r;
+            char* b = t->payloadBackup.as<char>();
+            MRB_CUDA(cudaMemcpyAsync(b, t->svo.leafIrr, U * 16, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(b + U * 16, t->svo.leafCnt, U * 8, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(b + U * 24, t->svo.leafAvg, U * 4, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(b + U * 28, t->svo.nodeAvg, N * 4, cudaMemcpyDeviceToDevice, t->stream));
+        }
         if ((r = record_frame(t))) return r;
         MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f0, 4, cudaMemcpyHostToDevice, t->stream));
+        if (pb) {
+            const char* b = t->payloadBackup.as<char>();
+            MRB_CUDA(cudaMemcpyAsync(t->svo.leafIrr, b, U * 16, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->svo.leafCnt, b + U * 16, U * 8, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->svo.leafAvg, b + U * 24, U * 4, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->svo.nodeAvg, b + U * 28, N * 4, cudaMemcpyDeviceToDevice, t->stream));
+        }
         MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
         cudaGraph_t g = nullptr;
@@ -1132,6 +1363,54 @@ int mrb_tracer_get_samples(mrb_tracer* t, float* host) {
 int mrb_tracer_reset_image(mrb_tracer* t) {
     if (!t) return MRB_E_ARG;
     if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+    return 0;
+}
+
+int mrb_tracer_svo_info(mrb_tracer* t, uint32_t* info, float* params) {
+    if (!t || !t->wfpg) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_svo(t);
+    if (r) return r;
+    svo_info(t->svo, t->svoP, info, params);
+    return 0;
+}
+
+int mrb_tracer_svo_export(mrb_tracer* t, uint64_t* nodes, uint32_t* leafParents,
+                          uint64_t* leafCodes, uint32_t* leafNormSpec, uint32_t* leafLight,
+                          uint32_t* levelOffsets, uint32_t* nodeNormSpec, uint64_t* leafIrr,
+                          uint32_t* leafCnt, uint32_t* leafAvg, uint32_t* nodeAvg) {
+    if (!t || !t->wfpg) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_svo(t);
+    if (r) return r;
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    if ((r = export_svo(t->svo, nodes, leafParents, leafCodes, leafNormSpec, leafLight,
+                        levelOffsets)))
+        return r;
+    return export_payload(t->svo, nodeNormSpec, leafIrr, leafCnt, leafAvg, nodeAvg);
+}
+
+int mrb_tracer_guide_export(mrb_tracer* t, uint32_t* count, uint32_t* samples, uint32_t* guide2,
+                            uint32_t* sortedBinKey, uint32_t* sortedRid) {
+    if (!t || !t->wfpg || !t->working || t->depth == 0) {
+        set_error("guide export: render at least one step of a WFPG frame first");
+        return MRB_E_STATE;
+    }
+    const int cur = (t->depth - 1) & 1;
+    uint32_t n = 0;
+    MRB_CUDA(cudaMemcpyAsync(&n, t->count.as<uint32_t>() + cur, 4, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    if (count) *count = n;
+    if (samples && n) {
+        std::vector<RayAux> aux(n);
+        MRB_CUDA(cudaMemcpy(aux.data(), t->aux[cur].p, size_t(n) * sizeof(RayAux),
+                            cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; i++) samples[i] = aux[i].sample;
+    }
+    if (svo_copy(guide2, t->guideBuf.p, size_t(n) * 8) ||
+        svo_copy(sortedBinKey, t->binKey.p, size_t(n) * 4) ||
+        svo_copy(sortedRid, t->binRid.p, size_t(n) * 4))
+        return MRB_E_CUDA;
     return 0;
 }
 

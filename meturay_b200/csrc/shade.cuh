@@ -19,9 +19,24 @@ struct HitIn {
     const float2* bary;
 };
 
+// Path chain of one WFPG frame, depth-major arrays of `paths` entries per
+// depth (WFPGPathNode, PathNode.cuh:28-149):
+//   nodeA = (vertex position, frame stamp bits); depth 0 is the camera
+//   nodeB = (path throughput arriving at the vertex, -)
+//   contribNee / contribPath = endpoint radiance reaching the chain from
+//   the NEE / path ray of that depth (AccumRadianceDownChain input)
+struct PathChain {
+    float4* nodeA;
+    float4* nodeB;
+    float4* contribNee;
+    float4* contribPath;
+    uint32_t paths;
+    uint32_t levels;        // maxDepth + 1
+};
+
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
                     float4* rayO, float4* rayD, RayAux* aux, float4* samples, uint32_t* count,
-                    cudaStream_t stream);
+                    const PathChain& chain, cudaStream_t stream);
 int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount, uint32_t idBits,
                uint32_t* dense, const PortionTable& table, cudaStream_t stream);
 int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t maxCount,
@@ -29,7 +44,8 @@ int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t 
 int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayAux* aux,
           const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull, uint32_t maxCount,
           float4* samples, const PathOptions& opt, bool gen, float4* outO, float4* outD,
-          RayAux* outAux, uint32_t* outCount, cudaStream_t stream);
+          RayAux* outAux, uint32_t* outCount, const PathChain& chain, const uint2* guide,
+          cudaStream_t stream);
 int resolve(const float4* samples, uint32_t width, uint32_t height, uint32_t sp, float4* image,
             cudaStream_t stream);
 int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream);

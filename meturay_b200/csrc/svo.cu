@@ -19,6 +19,7 @@
 #include "scan.cuh"
 #include "sort.cuh"
 #include "svo.cuh"
+#include "svo_dev.cuh"
 
 namespace mrb {
 namespace {
@@ -256,36 +257,79 @@ __global__ void k_leaf_parents(const uint32_t* __restrict__ rankLast, uint32_t U
         leafParents[j] = lastOffset + anc(rankLast, j);
 }
 
-// Leaf payload: mean of the voxel normals of the run (re-packed) and the
-// light key of the run's first light voxel.
+// Leaf payload, KCReduceVoxelPayload (AnisoSVOKC.cuh:8-320) with one thread
+// per unique voxel: 2-means clustering of the voxel normals (4 passes;
+// initial means n0 and -n0; the means are normalised at the start of each
+// pass; a normal joins mean 0 when its angular distance to mean 0 is >= the
+// distance to mean 1, as the reference compares), the larger cluster's mean
+// becomes the leaf normal, and light voxels start with luminance x 10000
+// samples on both sides (AnisoSVO.cuh SetLeafRadiance / SetLeafNormal).
+// Sums run over the voxel's duplicates in sorted order; the reference's
+// warp reductions add the same terms in a tree order.
 __global__ void k_leaf_payload(const uint32_t* __restrict__ runStart,
                                const uint32_t* __restrict__ sortedIdx,
                                const uint32_t* __restrict__ normals,
-                               const uint32_t* __restrict__ lightKeys, uint32_t U,
-                               uint32_t* leafNormal, uint32_t* leafLight) {
+                               const uint32_t* __restrict__ lightKeys,
+                               const float* __restrict__ lightRad, uint32_t omitDirect,
+                               uint32_t U, uint32_t* leafNormSpec, unsigned long long* leafIrr,
+                               uint32_t* leafCnt, uint32_t* leafLight) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < U; j += gridDim.x * blockDim.x) {
-        V3 acc = {0.0f, 0.0f, 0.0f};
-        uint32_t lk = 0;
-        for (uint32_t i = runStart[j]; i < runStart[j + 1]; i++) {
-            const uint32_t vi = sortedIdx[i];
-            const uint32_t pn = normals[vi];
-            const float az = static_cast<float>(pn & 0xFFFFu) / 65535.0f * (kPiF * 2.0f) - kPiF;
-            const float in = static_cast<float>(pn >> 16) / 65535.0f * kPiF;
-            float sa, ca, si, ci;
-            pm_sincos(az, sa, ca);
-            pm_sincos(in, si, ci);
-            acc = acc + v3(ca * si, sa * si, ci);
-            if (!lk) lk = lightKeys[vi];
+        const uint32_t b = runStart[j], e = runStart[j + 1], dup = e - b;
+        const V3 n0 = unpack_normal16(normals[sortedIdx[b]]);
+        V3 m0 = n0, m1 = -n0;
+        uint32_t c0 = 0, c1 = 0;
+        for (int it = 0; it < 4; it++) {
+            m0 = normalize(m0);
+            m1 = normalize(m1);
+            V3 a0 = v3(0.0f, 0.0f, 0.0f), a1 = v3(0.0f, 0.0f, 0.0f);
+            uint32_t k0 = 0, k1 = 0;
+            for (uint32_t i = b; i < e; i++) {
+                const V3 n = unpack_normal16(normals[sortedIdx[i]]);
+                if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) continue;
+                const float d0 = 1.0f - dot(m0, n), d1 = 1.0f - dot(m1, n);
+                if (d0 >= d1) {
+                    a0 = a0 + n;
+                    k0++;
+                } else {
+                    a1 = a1 + n;
+                    k1++;
+                }
+            }
+            m0 = a0;
+            m1 = a1;
+            c0 = k0;
+            c1 = k1;
         }
-        const float len2 = dot(acc, acc);
-        const V3 nrm = len2 > 0.0f ? acc * (1.0f / sqrtf(len2)) : v3(0.0f, 0.0f, 1.0f);
-        const float az = pm_atan2(nrm.y, nrm.x);
-        const float incl = pm_acos(fminf(fmaxf(nrm.z, -1.0f), 1.0f));
-        int u = static_cast<int>((az + kPiF) * kInvPiF * 0.5f * 65535.0f);
-        int v = static_cast<int>(incl * kInvPiF * 65535.0f);
-        u = u < 0 ? 0 : (u > 65535 ? 65535 : u);
-        v = v < 0 ? 0 : (v > 65535 ? 65535 : v);
-        leafNormal[j] = uint32_t(u) | (uint32_t(v) << 16);
+        V3 mean = (c0 >= c1) ? m0 * (1.0f / static_cast<float>(c0)) : m1 * (1.0f / static_cast<float>(c1));
+        float lum = 0.0f;
+        uint32_t lk = 0;
+        const uint32_t passes = (dup + 63u) / 64u;
+        for (uint32_t pass = 0; pass < passes; pass++) {
+            mean = normalize(mean);
+            const uint32_t pe = min(e, b + (pass + 1) * 64u);
+            for (uint32_t i = b + pass * 64u; i < pe; i++) {
+                const uint32_t key = lightKeys[sortedIdx[i]];
+                if (!key) continue;
+                if (!lk) lk = key;
+                const uint32_t li = key & kIdMask;
+                const V3 r = ld3(lightRad + 3 * li);
+                lum = lum + (0.2120f * r.x + 0.7150f * r.y + 0.0722f * r.z);
+            }
+        }
+        unsigned long long fx = 0;
+        uint32_t cnt = 0;
+        if (lum != 0.0f) {
+            lum /= static_cast<float>(dup);
+            lum *= 10000.0f;
+            if (omitDirect) lum = 0.0f;
+            fx = (lum > 0.0f) ? __double2ull_rn(static_cast<double>(lum) * kFixScale) : 0ull;
+            cnt = 10000u;
+        }
+        leafIrr[2 * j] = fx;
+        leafIrr[2 * j + 1] = fx;
+        leafCnt[2 * j] = cnt;
+        leafCnt[2 * j + 1] = cnt;
+        leafNormSpec[j] = write_normal_spec(mean, 0.0f);
         leafLight[j] = lk;
     }
 }
@@ -411,8 +455,16 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
     out.nodeCount = out.levelOffsets[D];
     if ((r = alloc(reinterpret_cast<void**>(&out.nodes), size_t(out.nodeCount) * 8)) ||
         (r = alloc(reinterpret_cast<void**>(&out.leafParents), size_t(U) * 4)) ||
-        (r = alloc(reinterpret_cast<void**>(&out.leafNormal), size_t(U) * 4)) ||
-        (r = alloc(reinterpret_cast<void**>(&out.leafLight), size_t(U) * 4))) {
+        (r = alloc(reinterpret_cast<void**>(&out.leafNormSpec), size_t(U) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafLight), size_t(U) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.nodeNormSpec), size_t(out.nodeCount) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafIrr), size_t(U) * 16)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafCnt), size_t(U) * 8)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafAvg), size_t(U) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.nodeAvg), size_t(out.nodeCount) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafBin), size_t(U) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.nodeBin), size_t(out.nodeCount) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.dLevelOffsets), out.levelOffsets.size() * 4))) {
         cleanup();
         return r;
     }
@@ -433,8 +485,11 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
     }
     k_leaf_parents<<<grid_of(U), 256, 0, st>>>(lr[D - 1], U, out.levelOffsets[D - 1],
                                               out.leafParents);
-    k_leaf_payload<<<grid_of(U), 256, 0, st>>>(out.leafRunStart, vidx, vnorm, vlight, U,
-                                              out.leafNormal, out.leafLight);
+    k_leaf_payload<<<grid_of(U), 256, 0, st>>>(out.leafRunStart, vidx, vnorm, vlight, in.lightRad,
+                                              in.omitDirect, U, out.leafNormSpec, out.leafIrr,
+                                              out.leafCnt, out.leafLight);
+    MRB_CUDA(cudaMemcpyAsync(out.dLevelOffsets, out.levelOffsets.data(),
+                             out.levelOffsets.size() * 4, cudaMemcpyHostToDevice, st));
     MRB_CUDA(cudaGetLastError());
     MRB_CUDA(cudaStreamSynchronize(st));
     cleanup();
@@ -446,8 +501,16 @@ void svo_free(SvoResult& r) {
     cudaFree(r.leafParents);
     cudaFree(r.leafCodes);
     cudaFree(r.leafRunStart);
-    cudaFree(r.leafNormal);
     cudaFree(r.leafLight);
+    cudaFree(r.leafNormSpec);
+    cudaFree(r.nodeNormSpec);
+    cudaFree(r.leafIrr);
+    cudaFree(r.leafCnt);
+    cudaFree(r.leafAvg);
+    cudaFree(r.nodeAvg);
+    cudaFree(r.leafBin);
+    cudaFree(r.nodeBin);
+    cudaFree(r.dLevelOffsets);
     r = SvoResult{};
 }
 

@@ -19,6 +19,8 @@ struct SvoBuildIn {
     const float* pos;
     const uint32_t* idx;
     const uint32_t* key;
+    const float* lightRad;    // 3 per primitive light (radiance)
+    uint32_t omitDirect;      // "OmitDirectRadiance": light voxels start at zero
 };
 
 struct SvoResult {
@@ -30,8 +32,17 @@ struct SvoResult {
     uint32_t* leafParents = nullptr;
     uint64_t* leafCodes = nullptr;   // sorted unique voxel Morton codes
     uint32_t* leafRunStart = nullptr;
-    uint32_t* leafNormal = nullptr;  // packed spherical normal (2 x 16 bit)
     uint32_t* leafLight = nullptr;   // HitKey of a light voxel, 0 otherwise
+    // radiance-cache payload (VoxelPayload, AnisoSVO.cuh:22-114)
+    uint32_t* leafNormSpec = nullptr;      // normal x,y 9+9 | length 7 | specular 6 | z sign 1
+    uint32_t* nodeNormSpec = nullptr;
+    unsigned long long* leafIrr = nullptr; // 2 per leaf, radiance sums in 2^24 fixed point
+    uint32_t* leafCnt = nullptr;           // 2 per leaf, sample counts
+    uint32_t* leafAvg = nullptr;           // half2 averages (front | back << 16)
+    uint32_t* nodeAvg = nullptr;
+    uint32_t* leafBin = nullptr;           // ray bins: mark bit 31 | ray count
+    uint32_t* nodeBin = nullptr;
+    uint32_t* dLevelOffsets = nullptr;     // device copy of levelOffsets
 };
 
 SvoParams svo_params(const float extent[6], uint32_t res);

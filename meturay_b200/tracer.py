@@ -22,7 +22,7 @@ import numpy as np
 from ._lib import Camera, Material, MrbError, SceneDesc, check, lib
 from .scenes import Scene
 
-__all__ = ["TracerSystem", "GPUScene", "PathTracer", "MrbError"]
+__all__ = ["TracerSystem", "GPUScene", "PathTracer", "WFPGTracer", "MrbError"]
 
 
 def _ptr(a: np.ndarray | None):
@@ -159,20 +159,13 @@ class GPUScene:
         check(lib.mrb_svo_build(self._h, int(resolution), None))
 
     def export_svo(self) -> dict:
+        """Octree structure and radiance-cache payload (host copies)."""
         info = np.zeros(6, np.uint32)
         params = np.zeros(7, np.float32)
         check(lib.mrb_svo_info(self._h, _ptr(info), _ptr(params)))
-        U, N = int(info[1]), int(info[2])
-        out = {"voxels": int(info[0]), "leaves": U, "nodes_count": N, "depth": int(info[3]),
-               "resolution": int(info[4]), "lo": params[0:3].copy(), "hi": params[3:6].copy(),
-               "leaf_size": float(params[6]),
-               "nodes": np.zeros(N, np.uint64), "leaf_parents": np.zeros(U, np.uint32),
-               "leaf_codes": np.zeros(U, np.uint64), "leaf_normals": np.zeros(U, np.uint32),
-               "leaf_lights": np.zeros(U, np.uint32),
-               "level_offsets": np.zeros(int(info[5]), np.uint32)}
-        check(lib.mrb_svo_export(self._h, *[_ptr(out[k]) for k in (
-            "nodes", "leaf_parents", "leaf_codes", "leaf_normals", "leaf_lights",
-            "level_offsets")]))
+        out = _svo_arrays(info, params)
+        check(lib.mrb_svo_export(self._h, *[_ptr(out[k]) for k in _SVO_KEYS]))
+        check(lib.mrb_svo_export_payload(self._h, *[_ptr(out[k]) for k in _PAYLOAD_KEYS]))
         return out
 
     def export(self) -> dict:
@@ -216,6 +209,25 @@ class GPUScene:
         """GPUAcceleratorGroupI::Hit on device buffers (raw pointers)."""
         check(lib.mrb_accel_hit(self._h, ray_o_ptr, ray_d_ptr, int(n), key_ptr, prim_ptr,
                                 t_ptr, bary_ptr, stream))
+
+
+_SVO_KEYS = ("nodes", "leaf_parents", "leaf_codes", "leaf_normals", "leaf_lights",
+             "level_offsets")
+_PAYLOAD_KEYS = ("node_normals", "leaf_irr", "leaf_cnt", "leaf_avg", "node_avg")
+
+
+def _svo_arrays(info, params) -> dict:
+    U, N = int(info[1]), int(info[2])
+    return {"voxels": int(info[0]), "leaves": U, "nodes_count": N, "depth": int(info[3]),
+            "resolution": int(info[4]), "lo": params[0:3].copy(), "hi": params[3:6].copy(),
+            "leaf_size": float(params[6]),
+            "nodes": np.zeros(N, np.uint64), "leaf_parents": np.zeros(U, np.uint32),
+            "leaf_codes": np.zeros(U, np.uint64), "leaf_normals": np.zeros(U, np.uint32),
+            "leaf_lights": np.zeros(U, np.uint32),
+            "level_offsets": np.zeros(int(info[5]), np.uint32),
+            "node_normals": np.zeros(N, np.uint32), "leaf_irr": np.zeros((U, 2), np.uint64),
+            "leaf_cnt": np.zeros((U, 2), np.uint32), "leaf_avg": np.zeros(U, np.uint32),
+            "node_avg": np.zeros(N, np.uint32)}
 
 
 class PathTracer:
@@ -316,3 +328,44 @@ class PathTracer:
     @property
     def stream(self) -> int:
         return lib.mrb_tracer_stream(self._h) or 0
+
+
+class WFPGTracer(PathTracer):
+    """GPUTracerI "WFPGTracer": the wavefront path tracer with product path
+    guiding from the tracer's sparse voxel octree radiance cache."""
+
+    OPTION_KEYS = PathTracer.OPTION_KEYS + (
+        "OctreeLevel", "MinRayBinLevel", "BinRayCount", "DoProductPathGuiding", "PurePG",
+        "SkipPG", "GuideBounceAmount", "OmitDirectRadiance")
+    FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha")
+
+    def __init__(self, system: TracerSystem, scene: GPUScene):
+        super().__init__(system, scene, "WFPGTracer")
+
+    def set_options(self, opts: dict):
+        ints = {k: v for k, v in opts.items() if k not in self.FLOAT_KEYS}
+        super().set_options(ints)
+        for k, v in opts.items():
+            if k in self.FLOAT_KEYS:
+                check(lib.mrb_tracer_set_option_float(self._h, k.encode(), float(v)))
+
+    def export_svo(self) -> dict:
+        """The tracer's octree with its current radiance state."""
+        info = np.zeros(6, np.uint32)
+        params = np.zeros(7, np.float32)
+        check(lib.mrb_tracer_svo_info(self._h, _ptr(info), _ptr(params)))
+        out = _svo_arrays(info, params)
+        check(lib.mrb_tracer_svo_export(self._h, *[_ptr(out[k]) for k in _SVO_KEYS + _PAYLOAD_KEYS]))
+        return out
+
+    def guide_state(self) -> dict:
+        """Per-ray guide words of the wavefront the last Render() step shaded."""
+        n = C.c_uint32()
+        check(lib.mrb_tracer_guide_export(self._h, C.byref(n), None, None, None, None))
+        k = int(n.value)
+        out = {"samples": np.zeros(k, np.uint32), "guide": np.zeros((k, 2), np.uint32),
+               "sorted_bin": np.zeros(k, np.uint32), "sorted_rid": np.zeros(k, np.uint32)}
+        check(lib.mrb_tracer_guide_export(self._h, C.byref(n), _ptr(out["samples"]),
+                                          _ptr(out["guide"]), _ptr(out["sorted_bin"]),
+                                          _ptr(out["sorted_rid"])))
+        return out

@@ -18,6 +18,8 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <map>
+#include <type_traits>
 
 namespace {
 
@@ -1022,13 +1024,236 @@ template <class T> inline T power_heuristic(T p0, T p1) {  // TracerFunctions.cu
     return (w0 * w0) / (w0 * w0 + w1 * w1);
 }
 
+
+// ========================================================================
+// Wavefront path guiding (WFPGTracer.cu, WFPGTracerKC.cuh, AnisoSVO.cu/.cuh,
+// ProductSampler.cuh, BlockTextureFilter.cuh, PathNode.cuh), FP32,
+// processed depth by depth over every path of the frame.  The bin counts
+// and the fixed-point radiance sums are order independent, the per-bin and
+// per-ray random numbers are keyed by bin / path, so the octree state and
+// every guided direction are reproducible exactly.
+// ========================================================================
+constexpr uint32_t kSvoInvalidParent = 0xFFFFFFFu;
+constexpr uint32_t kBinMark = 0x80000000u;
+constexpr uint32_t kBinLeaf = 0x80000000u;
+constexpr uint32_t kBinInvalid = 0xFFFFFFFFu;
+constexpr uint16_t kHalfMax = 0x7BFFu;
+constexpr double kFixScale = 16777216.0;
+constexpr uint32_t kTagGuide = 0x20000u;
+constexpr uint32_t kTagGuideBin = 0x30000u;
+constexpr uint32_t kGuideValid = 1u << 17;
+constexpr uint32_t kGuideBxdf = 1u << 16;
+
+inline uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float bitsf(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline uint32_t f2u_sat(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967040.0f) return 0xFFFFFFFFu;
+    return static_cast<uint32_t>(x);
+}
+inline int32_t f2i_sat(float x) {
+    if (x != x) return 0;
+    if (x >= 2147483520.0f) return 0x7FFFFFFF;
+    if (x <= -2147483648.0f) return static_cast<int32_t>(0x80000000u);
+    return static_cast<int32_t>(x);
+}
+// IEEE binary32 -> binary16, round to nearest even
+inline uint16_t f2h(float f) {
+    const uint32_t x = fbits(f);
+    const uint32_t sign = (x >> 16) & 0x8000u;
+    const uint32_t ax = x & 0x7FFFFFFFu;
+    if (ax > 0x7F800000u) return uint16_t(sign | 0x7E00u);
+    if (ax >= 0x47800000u) return uint16_t(sign | 0x7C00u);
+    if (ax < 0x38800000u) {
+        const uint32_t e = ax >> 23;
+        if (e == 0) return uint16_t(sign);
+        const uint32_t m = (ax & 0x7FFFFFu) | 0x800000u;
+        const uint32_t sh = 126u - e;
+        if (sh > 24u) return uint16_t(sign);
+        uint32_t q = m >> sh;
+        const uint32_t rem = m & ((1u << sh) - 1u), halfway = 1u << (sh - 1u);
+        if (rem > halfway || (rem == halfway && (q & 1u))) q++;
+        return uint16_t(sign | q);
+    }
+    uint32_t h = (((ax >> 23) - 112u) << 10) | ((ax & 0x7FFFFFu) >> 13);
+    const uint32_t rem = ax & 0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) h++;
+    return uint16_t(sign | h);
+}
+inline float h2f(uint16_t h) {
+    const uint32_t sign = (uint32_t(h) & 0x8000u) << 16;
+    const uint32_t e = (h >> 10) & 0x1Fu, m = h & 0x3FFu;
+    if (e == 0) {
+        if (m == 0) return bitsf(sign);
+        const float v = static_cast<float>(m) * 0x1p-24f;
+        return sign ? -v : v;
+    }
+    if (e == 31) return bitsf(sign | 0x7F800000u | (m << 13));
+    return bitsf(sign | ((e + 112u) << 23) | (m << 13));
+}
+inline float next_up(float x) {
+    if (x != x || x == bitsf(0x7F800000u)) return x;
+    if (x == 0.0f) return bitsf(1u);
+    const uint32_t b = fbits(x);
+    return bitsf(x > 0.0f ? b + 1u : b - 1u);
+}
+// "lowbias32" integer hash (C. Wellons, hash-prospector)
+inline uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+using F3 = V3<float>;
+using FQ = Q4<float>;
+
+// RayLib/CoordinateConversion.h:112-233
+constexpr float kTwoOvrPiF = 0x1.45f306p-1f;
+constexpr float kPiOvr4F = 0x1.921fb6p-1f;
+inline void dir_to_octa(F3 d, float& s, float& t) {
+    if (d.x == 0.0f && d.y == 0.0f) { s = 0.0f; t = 0.0f; return; }
+    const float xAbs = std::fabs(d.x), yAbs = std::fabs(d.y);
+    const float phiPrime = pm_atan2(yAbs, xAbs);
+    const float radius = std::sqrt(1.0f - std::fabs(d.z));
+    float v = radius * kTwoOvrPiF * phiPrime;
+    float u = radius - v;
+    if (d.z < 0.0f) {
+        const float up = 1.0f - v, vp = 1.0f - u;
+        u = up;
+        v = vp;
+    }
+    u *= std::signbit(d.x) ? -1.0f : 1.0f;
+    v *= std::signbit(d.y) ? -1.0f : 1.0f;
+    s = (u + 1.0f) * 0.5f;
+    t = (v + 1.0f) * 0.5f;
+}
+inline F3 octa_to_dir(float s, float t) {
+    const float u = s * 2.0f - 1.0f, v = t * 2.0f - 1.0f;
+    const float ua = std::fabs(u), va = std::fabs(v);
+    const float d = 1.0f - (ua + va);
+    const float radius = 1.0f - std::fabs(d);
+    float phiPrime = 0.0f;
+    if (radius != 0.0f) phiPrime = ((va - ua) / radius + 1.0f) * kPiOvr4F;
+    float sp, cp;
+    pm_sincos(phiPrime, sp, cp);
+    const float cosPhi = (std::signbit(u) ? -1.0f : 1.0f) * cp;
+    const float sinPhi = (std::signbit(v) ? -1.0f : 1.0f) * sp;
+    const float z = (std::signbit(d) ? -1.0f : 1.0f) * (1.0f - radius * radius);
+    const float xyFactor = radius * std::sqrt(2.0f - radius * radius);
+    return F3(cosPhi * xyFactor, sinPhi * xyFactor, z);
+}
+inline F3 octa_to_dir_yup(float s, float t) {
+    const F3 r = octa_to_dir(s, t);
+    return F3(r.y, r.z, r.x);
+}
+inline void dir_yup_to_octa(F3 d, float& s, float& t) { dir_to_octa(F3(d.z, d.x, d.y), s, t); }
+inline void octa_wrap(float& s, float& t) {
+    float a = s, b = t;
+    if (s < 0.0f) a = -2.0f - s;
+    if (t < 0.0f) b = -2.0f - t;
+    const float ia = std::trunc(a), ib = std::trunc(b);
+    float fa = std::fabs(a - ia), fb = std::fabs(b - ib);
+    const int32_t ii = f2i_sat(ia), ij = f2i_sat(ib);
+    if ((ii & 1) ^ (ij & 1)) {
+        fa = 1.0f - fa;
+        fb = 1.0f - fb;
+    }
+    s = fa;
+    t = fb;
+}
+inline void octa_wrap_int(int32_t& x, int32_t& y, int32_t dimX, int32_t dimY) {
+    int32_t a = x, b = y;
+    if (x < 0) a = -2 * dimX - x;
+    if (y < 0) b = -2 * dimY - y;
+    const int32_t ia = a / dimX, ib = b / dimY;
+    int32_t fa = a % dimX, fb = b % dimY;
+    fa = fa < 0 ? -fa : fa;
+    fb = fb < 0 ? -fb : fb;
+    if ((ia & 1) ^ (ib & 1)) {
+        fa = (dimX - 1) - fa;
+        fb = (dimY - 1) - fb;
+    }
+    x = fa;
+    y = fb;
+}
+// Utility::SphericalToCartesianUnit of the 2 x 16-bit voxel normal
+inline F3 unpack_normal16(uint32_t pn) {
+    const float az = static_cast<float>(pn & 0xFFFFu) / 65535.0f * (kPiF * 2.0f) - kPiF;
+    const float in = static_cast<float>(pn >> 16) / 65535.0f * kPiF;
+    float sa, ca, si, ci;
+    pm_sincos(az, sa, ca);
+    pm_sincos(in, si, ci);
+    return normalize(F3(ca * si, sa * si, ci));
+}
+// VoxelPayload::ReadNormalAndSpecular / WriteNormalAndSpecular
+inline F3 read_normal_spec(uint32_t packed, float& stdDev, float& spec) {
+    const float kx = (1.0f / 511.0f) * 2.0f;
+    float nx = static_cast<float>(packed & 511u) * kx;
+    float ny = static_cast<float>((packed >> 9) & 511u) * kx;
+    nx -= 1.0f;
+    ny -= 1.0f;
+    const float nz = std::sqrt(std::fmax(0.0f, 1.0f - nx * nx - ny * ny));
+    F3 n = normalize(F3(nx, ny, nz));
+    if ((packed >> 31) & 1u) n.z *= -1.0f;
+    const float len = static_cast<float>((packed >> 18) & 127u) * (1.0f / 127.0f);
+    spec = static_cast<float>((packed >> 25) & 63u) * (1.0f / 6.0f);
+    stdDev = (1.0f - len) / len;
+    return n;
+}
+inline uint32_t write_normal_spec(F3 n, float spec) {
+    const float length = std::sqrt(dot(n, n));
+    const float il = 1.0f / length;
+    float x = n.x * il, y = n.y * il;
+    x += 1.0f;
+    y += 1.0f;
+    x *= 0.5f;
+    y *= 0.5f;
+    x *= 511.0f;
+    y *= 511.0f;
+    const uint32_t px = f2u_sat(x), py = f2u_sat(y);
+    const uint32_t pl = f2u_sat(length * 127.0f);
+    const uint32_t ps = f2u_sat(spec * 63.0f);
+    const uint32_t sz = std::signbit(n.z) ? 1u : 0u;
+    return (px & 511u) | ((py & 511u) << 9) | ((pl & 127u) << 18) | ((ps & 63u) << 25) | (sz << 31);
+}
+inline uint64_t to_fixed(float x) {
+    return (x > 0.0f) ? static_cast<uint64_t>(std::nearbyint(static_cast<double>(x) * kFixScale)) : 0ull;
+}
+inline float lum3(F3 c) { return 0.2120f * c.x + 0.7150f * c.y + 0.0722f * c.z; }
+
+inline uint32_t node_child_index(uint64_t n) { return uint32_t(n & 0x7FFFFFFull); }
+inline uint32_t node_parent(uint64_t n) { return uint32_t((n >> 27) & 0xFFFFFFFull); }
+inline uint32_t node_mask(uint64_t n) { return uint32_t((n >> 55) & 0xFFull); }
+inline bool node_children_leaf(uint64_t n) { return (n >> 63) != 0; }
+inline uint32_t node_child_offset(uint64_t n, uint32_t c) {
+    return uint32_t(__builtin_popcount(((1u << c) - 1u) & node_mask(n)));
+}
+
+struct Chain {
+    uint32_t levels, paths;
+    std::vector<float> pos;      // levels * paths * 3
+    std::vector<float> rf;       // levels * paths * 3
+    std::vector<uint8_t> valid;  // levels * paths
+    std::vector<float> nee, path;
+    Chain(uint32_t L, uint32_t P)
+        : levels(L), paths(P), pos(size_t(L) * P * 3, 0.0f), rf(size_t(L) * P * 3, 0.0f),
+          valid(size_t(L) * P, 0), nee(size_t(L) * P * 3, 0.0f), path(size_t(L) * P * 3, 0.0f) {}
+    size_t at(uint32_t d, uint32_t p) const { return size_t(d) * paths + p; }
+};
+
+
+// PathTracerPathWork (PathTracerKC.cuh:428-649); with a chain and guide
+// words it is WFPGTracerPathWork (WFPGTracerKC.cuh:212-519), FP32 only.
 template <class T>
 void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t batch,
-               uint32_t id, bool gen, std::vector<PRay<T>>& next) {
+               uint32_t id, bool gen, std::vector<PRay<T>>& next,
+               const uint32_t* guide = nullptr, Chain* chain = nullptr) {
     const oracle_scene* s = c.s;
     const Aux<T>& aux = r.aux;
     if (aux.type == NEE_RAY) return;
-    if (!gen) return;  // outputs of the last iteration are never traced
+    if (!gen && !chain) return;  // outputs of the last iteration are never traced
     Surface<T> sf = gen_surface(s, prim, ha, hb, r.d);
     V3<T> wi = -normalize(r.d);
     V3<T> rf = aux.rf;  // vacuum / sigmaT == 0 transmittance is exactly 1
@@ -1037,6 +1262,24 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
     else if (batch == kBatchMetal) specular = (T(1) - T(s->metal_params[10 * id + 9])) >= T(0.99f);
     else if (batch == kBatchUnreal) specular = (T(1) - T(s->unreal_params[6 * id + 3])) >= T(0.99f);
     else specular = true;
+    if constexpr (std::is_same_v<T, float>) {
+        if (chain) {
+            // WFPGPathNode of this vertex; the rays it launches start empty
+            const size_t at = chain->at(aux.depth, aux.sample);
+            chain->pos[3 * at] = sf.pos.x;
+            chain->pos[3 * at + 1] = sf.pos.y;
+            chain->pos[3 * at + 2] = sf.pos.z;
+            chain->rf[3 * at] = rf.x;
+            chain->rf[3 * at + 1] = rf.y;
+            chain->rf[3 * at + 2] = rf.z;
+            chain->valid[at] = 1;
+            if (aux.depth + 1 < chain->levels) {
+                const size_t nx = chain->at(aux.depth + 1, aux.sample);
+                for (int k = 0; k < 3; k++) chain->nee[3 * nx + k] = chain->path[3 * nx + k] = 0.0f;
+            }
+        }
+    }
+    if (!gen) return;
     uint32_t sampleIdx = aux.sample;
     Rng4 ra = rng_block(sampleIdx, c.o->frame, aux.depth, 0, c.o->seed_lo, c.o->seed_hi);
     Rng4 rb = rng_block(sampleIdx, c.o->frame, aux.depth, 1, c.o->seed_lo, c.o->seed_hi);
@@ -1111,9 +1354,35 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
             next.push_back(o);
         }
     }
-    // ---- BxDF sample (PathTracerKC.cuh:585-648) ----
+    // ---- BxDF sample (PathTracerKC.cuh:585-648), or the guided direction
     BSample<T> bs;
-    if (batch == kBatchLambert) {
+    bool guided = false;
+    if constexpr (std::is_same_v<T, float>) {
+        if (guide && !specular) {
+            const float gp = h2f(uint16_t(guide[1] & 0xFFFFu));
+            if ((guide[1] & kGuideValid) && gp == gp) {
+                const F3 dir = octa_to_dir_yup(h2f(uint16_t(guide[0] & 0xFFFFu)), h2f(uint16_t(guide[0] >> 16)));
+                bs.dir = dir;
+                bs.pdf = gp;
+                bs.pos = nudge(sf.pos, sf.geo);
+                bs.medium = aux.medium;
+                if (batch == kBatchLambert) {
+                    const float* al = s->lambert_albedo + 3 * id;
+                    bs.refl = lambert_eval(F3(al[0], al[1], al[2]), dir, sf);
+                } else if (batch == kBatchLambertC) {
+                    const float* al = s->lambertc_albedo + 3 * id;
+                    bs.refl = lambertc_eval(F3(al[0], al[1], al[2]), dir, sf);
+                } else if (batch == kBatchUnreal) {
+                    bs.refl = unreal_eval(unreal_params<float>(s->unreal_params + 6 * id), dir, wi, sf);
+                } else {
+                    bs.refl = metal_eval(metal_params<float>(s->metal_params + 10 * id), dir, wi, sf);
+                }
+                guided = true;
+            }
+        }
+    }
+    if (guided) {
+    } else if (batch == kBatchLambert) {
         const float* al = s->lambert_albedo + 3 * id;
         bs = lambert_sample(V3<T>(al[0], al[1], al[2]), sf, T(rb.u[0]), T(rb.u[1]), aux.medium);
     } else if (batch == kBatchLambertC) {
@@ -1159,7 +1428,7 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
 // PathTracerKC.cuh:335-426
 template <class T>
 void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx, uint32_t prim, T ha, T hb,
-                   T hitT) {
+                   T hitT, Chain* chain = nullptr) {
     const Aux<T>& aux = r.aux;
     const oracle_scene* s = c.s;
     const bool pathAsMis = c.o->mis && aux.type == PATH_RAY;
@@ -1190,6 +1459,16 @@ void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx, uint32_t prim
         V3<T> total = V3<T>(T(e[0]), T(e[1]), T(e[2])) * aux.rf;
         total = total * misWeight;
         accumulate(c, aux.sample, total);
+        if constexpr (std::is_same_v<T, float>) {
+            // WFPGTracerBoundaryWork: AccumRadianceDownChain input
+            if (chain && !camera) {
+                const size_t at = chain->at(aux.depth, aux.sample);
+                float* dst = (aux.type == NEE_RAY) ? &chain->nee[3 * at] : &chain->path[3 * at];
+                dst[0] = total.x;
+                dst[1] = total.y;
+                dst[2] = total.z;
+            }
+        }
     }
 }
 
@@ -1413,6 +1692,11 @@ struct oracle_svo {
     std::vector<uint32_t> leafParents;
     std::vector<uint32_t> leafLight;
     uint32_t voxelCount = 0;
+    // voxel records behind each leaf, in sorted order (payload input)
+    std::vector<uint32_t> runStart, runVoxel, voxNormal, voxLightKey;
+    // radiance-cache payload (VoxelPayload, AnisoSVO.cuh:22-114)
+    std::vector<uint32_t> leafNormSpec, nodeNormSpec, leafAvg, nodeAvg, leafBin, nodeBin, leafCnt;
+    std::vector<uint64_t> leafIrr;
 };
 
 namespace {
@@ -1479,6 +1763,12 @@ extern "C" oracle_svo* oracle_svo_build(const float* pos, const uint32_t* idx, c
     }
     const uint32_t U = uint32_t(o->leafCodes.size());
     const uint32_t D = P.depth;
+    o->runVoxel = order;
+    o->voxNormal = normals;
+    o->voxLightKey = lights;
+    for (uint32_t i = 0; i < total; i++)
+        if (i == 0 || sorted[i] != sorted[i - 1]) o->runStart.push_back(i);
+    o->runStart.push_back(total);
     // level node counts: KCMarkMortonChanges + reduce, per level
     std::vector<uint32_t> levelCounts(D + 1, 0);
     levelCounts[0] = 1;
@@ -1575,6 +1865,845 @@ extern "C" void oracle_svo_get(const oracle_svo* o, uint64_t* nodes, uint32_t* l
         }
         params[6] = o->P.leaf;
     }
+}
+
+namespace {
+
+struct Tree {
+    const oracle_svo* o;
+    float level_voxel_size(uint32_t level) const {
+        return o->P.leaf * static_cast<float>(1u << (o->P.depth - level));
+    }
+    // AnisoSVOctreeGPU::Descend (AnisoSVO.cuh:1128-1155)
+    bool descend(uint32_t& index, uint64_t code, uint32_t depth) const {
+        uint32_t shift = (o->P.depth - 1) * 3;
+        uint32_t cur = 0;
+        for (uint32_t i = 0; i < depth; i++) {
+            const uint64_t node = o->nodes[cur];
+            const uint32_t childId = uint32_t(code >> shift) & 7u;
+            if (!((node_mask(node) >> childId) & 1u)) return false;
+            cur = node_child_index(node) + node_child_offset(node, childId);
+            shift -= 3;
+        }
+        index = cur;
+        return true;
+    }
+    // AnisoSVOctreeGPU::NearestNodeIndex (AnisoSVO.cuh:1171-1242)
+    bool nearest(uint32_t& index, F3 p, uint32_t depth) const {
+        index = kInvalid;
+        const SvoP& P = o->P;
+        if (!(p.x >= P.lo[0] && p.x <= P.hi[0] && p.y >= P.lo[1] && p.y <= P.hi[1] &&
+              p.z >= P.lo[2] && p.z <= P.hi[2]))
+            return false;
+        const float vs = level_voxel_size(depth);
+        const float li[3] = {(p.x - P.lo[0]) / vs, (p.y - P.lo[1]) / vs, (p.z - P.lo[2]) / vs};
+        float fr[3], fl[3];
+        uint32_t inc[3];
+        for (int c = 0; c < 3; c++) {
+            const float ip = std::trunc(li[c]);
+            fr[c] = li[c] - ip;
+            fl[c] = std::floor(li[c]);
+            inc[c] = (fr[c] < 0.5f) ? 0xFFFFFFFFu : 1u;
+            fr[c] = 0.5f - std::fabs(fr[c] - 0.5f);
+        }
+        int m0 = 0;
+        if (fr[1] < fr[m0]) m0 = 1;
+        if (fr[2] < fr[m0]) m0 = 2;
+        const float a = fr[(m0 + 1) % 3], b = fr[(m0 + 2) % 3];
+        int m1 = (b < a) ? 1 : 0;
+        m1 = (m0 + m1 + 1) % 3;
+        const int m2 = 3 - m0 - m1;
+        const uint32_t dense[3] = {f2u_sat(fl[0]), f2u_sat(fl[1]), f2u_sat(fl[2])};
+        for (uint32_t i = 0; i < 8; i++) {
+            uint32_t sh[3];
+            sh[m0] = i & 1u;
+            sh[m1] = (i >> 1) & 1u;
+            sh[m2] = (i >> 2) & 1u;
+            const uint64_t code = morton3d(dense[0] + sh[0] * inc[0], dense[1] + sh[1] * inc[1],
+                                           dense[2] + sh[2] * inc[2]);
+            if (descend(index, code, depth)) return true;
+        }
+        return false;
+    }
+    float read_radiance(F3 coneDir, uint32_t id, bool isLeaf) const {
+        if (id == kInvalid) return 0.0f;
+        float sd, sp;
+        const F3 n = read_normal_spec(isLeaf ? o->leafNormSpec[id] : o->nodeNormSpec[id], sd, sp);
+        const bool towards = dot(n, -coneDir) >= 0.0f;
+        const uint32_t w = isLeaf ? o->leafAvg[id] : o->nodeAvg[id];
+        return h2f(uint16_t(towards ? (w & 0xFFFFu) : (w >> 16)));
+    }
+    // AnisoSVOctreeGPU::ConeTraceRay (AnisoSVO.cuh:767-1000), bounded loop
+    float cone_trace(F3 pos, F3 dir, float tMin, float aperture, uint32_t maxQueryLevelOffset,
+                     bool& isLeaf, uint32_t& leafId) const {
+        const SvoP& P = o->P;
+        const float EPS = 1.0e-5f;
+        leafId = kInvalid;
+        isLeaf = false;
+        if (std::fabs(dir.x) < EPS) dir.x = std::copysign(EPS, dir.x);
+        if (std::fabs(dir.y) < EPS) dir.y = std::copysign(EPS, dir.y);
+        if (std::fabs(dir.z) < EPS) dir.z = std::copysign(EPS, dir.z);
+        const F3 sc(1.0f / (P.hi[0] - P.lo[0]), 1.0f / (P.hi[1] - P.lo[1]), 1.0f / (P.hi[2] - P.lo[2]));
+        F3 d = dir * sc;
+        F3 p = (pos + F3(-P.lo[0], -P.lo[1], -P.lo[2])) * sc;
+        if (!(d.x == d.x && d.y == d.y && d.z == d.z && p.x == p.x && p.y == p.y && p.z == p.z))
+            return tMin;
+        p.x = (d.x < 0.0f) ? (1.0f - p.x) : p.x;
+        p.y = (d.y < 0.0f) ? (1.0f - p.y) : p.y;
+        p.z = (d.z < 0.0f) ? (1.0f - p.z) : p.z;
+        uint32_t mirror = 0;
+        if (d.x < 0.0f) mirror |= 1u;
+        if (d.y < 0.0f) mirror |= 2u;
+        if (d.z < 0.0f) mirror |= 4u;
+        const F3 dc(1.0f / std::fabs(d.x), 1.0f / std::fabs(d.y), 1.0f / std::fabs(d.z));
+        const F3 pb = p * dc;
+        {
+            const F3 t0 = -pb;
+            const float tSvo = std::fmax(std::fmax(t0.x, t0.y), t0.z);
+            if (!(t0.x < tMin && t0.y < tMin && t0.z < tMin)) tMin = next_up(tSvo);
+        }
+        auto neg_exp2i = [](uint32_t q) { return (q == 0) ? 1.0f : bitsf((127u - q) << 23); };
+        uint64_t stack = 0;
+        uint32_t depthBits = 0, nodeId = 0;
+        F3 corner(0.0f, 0.0f, 0.0f);
+        bool emptyNode = false;
+        for (uint32_t step = 0; nodeId != kSvoInvalidParent; step++) {
+            if (step == (1u << 16)) {
+                leafId = kInvalid;
+                isLeaf = false;
+                break;
+            }
+            const float childSpan = neg_exp2i(depthBits + 1), curSpan = neg_exp2i(depthBits);
+            const F3 center = corner + F3(childSpan, childSpan, childSpan);
+            const F3 topRight = corner + F3(curSpan, curSpan, curSpan);
+            const F3 tm = topRight * dc - pb;
+            const float tMax = std::fmin(std::fmin(tm.x, tm.y), tm.z);
+            if (emptyNode) {
+                tMin = next_up(tMax);
+                const uint32_t b = uint32_t(stack & 7u);
+                corner = corner - F3((b & 1u) ? curSpan : 0.0f, (b & 2u) ? curSpan : 0.0f,
+                                     (b & 4u) ? curSpan : 0.0f);
+                stack >>= 3;
+                depthBits -= 1;
+                emptyNode = false;
+                continue;
+            }
+            const uint64_t node = o->nodes[nodeId];
+            if (tMax < tMin) {
+                const uint32_t b = uint32_t(stack & 7u);
+                corner = corner - F3((b & 1u) ? curSpan : 0.0f, (b & 2u) ? curSpan : 0.0f,
+                                     (b & 4u) ? curSpan : 0.0f);
+                stack >>= 3;
+                depthBits -= 1;
+                nodeId = node_parent(node);
+                emptyNode = false;
+            } else {
+                const F3 tc = center * dc - pb;
+                uint32_t childId = 0;
+                if (tc.x < tMin) childId |= 1u;
+                if (tc.y < tMin) childId |= 2u;
+                if (tc.z < tMin) childId |= 4u;
+                const uint32_t mir = childId ^ mirror;
+                const bool has = (node_mask(node) >> mir) & 1u;
+                if (has) {
+                    nodeId = node_child_index(node) + node_child_offset(node, mir);
+                    const uint32_t level = depthBits + 1;
+                    const float area = tMin * tMin * aperture;
+                    const float diam2 = 4.0f * (area * kInvPiF);
+                    const float vs = level_voxel_size(level);
+                    bool term = diam2 > vs * vs;
+                    const bool childLeaf = node_children_leaf(node);
+                    term |= (P.depth - level) <= maxQueryLevelOffset;
+                    if (childLeaf || term) {
+                        isLeaf = childLeaf;
+                        leafId = nodeId;
+                        break;
+                    }
+                }
+                emptyNode = !has;
+                corner = corner + F3((childId & 1u) ? childSpan : 0.0f, (childId & 2u) ? childSpan : 0.0f,
+                                     (childId & 4u) ? childSpan : 0.0f);
+                stack = (stack << 3) | childId;
+                depthBits += 1;
+            }
+        }
+        return tMin;
+    }
+    uint32_t marked_bin(uint32_t leaf, bool& isLeaf) const {
+        isLeaf = true;
+        uint32_t bin = o->leafBin[leaf];
+        uint32_t parent = o->leafParents[leaf];
+        uint32_t node = leaf;
+        while (parent != kSvoInvalidParent && !(bin & kBinMark)) {
+            node = parent;
+            bin = o->nodeBin[parent];
+            parent = node_parent(o->nodes[parent]);
+            isLeaf = false;
+        }
+        return node;
+    }
+};
+
+// KCReduceVoxelPayload (AnisoSVOKC.cuh:8-320), one voxel at a time with
+// sequential sums, then KCAverageNormals bottom-up (AnisoSVO.cu:428-528)
+void payload_init(oracle_svo* o, const float* lightRad, uint32_t omit) {
+    const uint32_t U = uint32_t(o->leafCodes.size()), N = uint32_t(o->nodes.size());
+    const uint32_t D = o->P.depth;
+    o->leafNormSpec.assign(U, 0);
+    o->leafIrr.assign(2 * size_t(U), 0);
+    o->leafCnt.assign(2 * size_t(U), 0);
+    o->leafAvg.assign(U, 0);
+    o->nodeAvg.assign(N, 0);
+    o->nodeNormSpec.assign(N, 0);
+    o->leafBin.assign(U, 0);
+    o->nodeBin.assign(N, 0);
+    for (uint32_t j = 0; j < U; j++) {
+        const uint32_t b = o->runStart[j], e = o->runStart[j + 1], dup = e - b;
+        const F3 n0 = unpack_normal16(o->voxNormal[o->runVoxel[b]]);
+        F3 m0 = n0, m1 = -n0;
+        uint32_t c0 = 0, c1 = 0;
+        for (int it = 0; it < 4; it++) {
+            m0 = normalize(m0);
+            m1 = normalize(m1);
+            F3 a0(0.0f, 0.0f, 0.0f), a1(0.0f, 0.0f, 0.0f);
+            uint32_t k0 = 0, k1 = 0;
+            for (uint32_t i = b; i < e; i++) {
+                const F3 n = unpack_normal16(o->voxNormal[o->runVoxel[i]]);
+                if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) continue;
+                const float d0 = 1.0f - dot(m0, n), d1 = 1.0f - dot(m1, n);
+                if (d0 >= d1) { a0 = a0 + n; k0++; } else { a1 = a1 + n; k1++; }
+            }
+            m0 = a0;
+            m1 = a1;
+            c0 = k0;
+            c1 = k1;
+        }
+        F3 mean = (c0 >= c1) ? m0 * (1.0f / static_cast<float>(c0)) : m1 * (1.0f / static_cast<float>(c1));
+        float lum = 0.0f;
+        const uint32_t passes = (dup + 63u) / 64u;
+        for (uint32_t pass = 0; pass < passes; pass++) {
+            mean = normalize(mean);
+            const uint32_t pe = std::min(e, b + (pass + 1) * 64u);
+            for (uint32_t i = b + pass * 64u; i < pe; i++) {
+                const uint32_t key = o->voxLightKey[o->runVoxel[i]];
+                if (!key) continue;
+                const float* r = lightRad + 3 * (key & 0xFFFFFFu);
+                lum = lum + (0.2120f * r[0] + 0.7150f * r[1] + 0.0722f * r[2]);
+            }
+        }
+        if (lum != 0.0f) {
+            lum /= static_cast<float>(dup);
+            lum *= 10000.0f;
+            if (omit) lum = 0.0f;
+            o->leafIrr[2 * j] = o->leafIrr[2 * j + 1] = to_fixed(lum);
+            o->leafCnt[2 * j] = o->leafCnt[2 * j + 1] = 10000u;
+        }
+        o->leafNormSpec[j] = write_normal_spec(mean, 0.0f);
+    }
+    for (int L = int(D) - 1; L >= 0; L--) {
+        const bool childLeaf = (L == int(D) - 1);
+        for (uint32_t k = o->levelOffsets[L]; k < o->levelOffsets[L + 1]; k++) {
+            const uint64_t node = o->nodes[k];
+            const uint32_t cnt = uint32_t(__builtin_popcount(node_mask(node)));
+            const uint32_t ci = node_child_index(node);
+            F3 nb[8];
+            float avgSpec = 0.0f;
+            for (uint32_t i = 0; i < cnt; i++) {
+                float sd, sp;
+                const F3 n = read_normal_spec(childLeaf ? o->leafNormSpec[ci + i] : o->nodeNormSpec[ci + i],
+                                              sd, sp);
+                const float len = 1.0f / (1.0f + sd);
+                nb[i] = n * len;
+                avgSpec += sp;
+            }
+            avgSpec *= 1.0f / static_cast<float>(cnt);
+            F3 mean[2][2];
+            uint32_t counts[2][2] = {{0, 0}, {0, 0}};
+            mean[0][0] = nb[0];
+            mean[0][1] = -nb[0];
+            mean[1][0] = mean[1][1] = F3(0.0f, 0.0f, 0.0f);
+            for (int pass = 0; pass < 4; pass++) {
+                const int rd = pass % 2, wr = rd ? 0 : 1;
+                for (uint32_t i = 0; i < cnt; i++) {
+                    const F3 n = nb[i];
+                    if (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) continue;
+                    const float d0 = 1.0f - dot(mean[rd][0], n), d1 = 1.0f - dot(mean[rd][1], n);
+                    const int up = (d0 >= d1) ? 0 : 1;
+                    mean[wr][up] = mean[wr][up] + n;
+                    counts[wr][up] += 1;
+                }
+                mean[rd][0] = mean[rd][1] = F3(0.0f, 0.0f, 0.0f);
+                counts[rd][0] = counts[rd][1] = 0;
+            }
+            const int idx = (counts[0][0] >= counts[0][1]) ? 0 : 1;
+            const F3 m = mean[0][idx] * (1.0f / static_cast<float>(counts[0][idx]));
+            o->nodeNormSpec[k] = write_normal_spec(m, avgSpec);
+        }
+    }
+}
+
+// NormalizeAndFilterRadiance (AnisoSVO.cu:352-428,1415-1484)
+void normalize_filter(oracle_svo* o) {
+    const uint32_t U = uint32_t(o->leafCodes.size());
+    const uint32_t D = o->P.depth;
+    for (uint32_t l = 0; l < U; l++) {
+        uint32_t w = 0;
+        for (int s = 0; s < 2; s++) {
+            const uint32_t c = o->leafCnt[2 * l + s];
+            float avg = 0.0f;
+            if (c) avg = static_cast<float>(static_cast<double>(o->leafIrr[2 * l + s]) / kFixScale /
+                                            static_cast<double>(c));
+            avg = std::fmin(avg, 65504.0f);
+            w |= uint32_t(f2h(avg)) << (16 * s);
+        }
+        o->leafAvg[l] = w;
+    }
+    for (int L = int(D) - 1; L >= 0; L--) {
+        const bool childLeaf = (L == int(D) - 1);
+        for (uint32_t k = o->levelOffsets[L]; k < o->levelOffsets[L + 1]; k++) {
+            const uint64_t node = o->nodes[k];
+            const uint32_t cnt = uint32_t(__builtin_popcount(node_mask(node))), ci = node_child_index(node);
+            float sd, sp;
+            const F3 n = read_normal_spec(o->nodeNormSpec[k], sd, sp);
+            float sum[2] = {0.0f, 0.0f};
+            uint32_t valid[2] = {0, 0};
+            for (uint32_t i = 0; i < cnt; i++) {
+                const uint32_t c = ci + i;
+                const uint32_t irr = childLeaf ? o->leafAvg[c] : o->nodeAvg[c];
+                const F3 cn = read_normal_spec(childLeaf ? o->leafNormSpec[c] : o->nodeNormSpec[c], sd, sp);
+                const bool swap = dot(cn, n) < 0.0f;
+                for (int j = 0; j < 2; j++) {
+                    const int rdx = swap ? ((j + 1) % 2) : j;
+                    const uint16_t h = uint16_t(irr >> (16 * rdx));
+                    if (h != kHalfMax) {
+                        valid[j]++;
+                        sum[j] += h2f(h);
+                    }
+                }
+            }
+            uint32_t w = 0;
+            for (int j = 0; j < 2; j++) {
+                const uint16_t h = valid[j] ? f2h(std::fmin(sum[j] / static_cast<float>(valid[j]), 65504.0f))
+                                            : kHalfMax;
+                w |= uint32_t(h) << (16 * j);
+            }
+            o->nodeAvg[k] = w;
+        }
+    }
+    for (uint32_t L = 1; L <= D; L++) {
+        const bool leaf = (L == D);
+        const uint32_t b = leaf ? 0u : o->levelOffsets[L];
+        const uint32_t e = leaf ? U : o->levelOffsets[L + 1];
+        for (uint32_t k = b; k < e; k++) {
+            const uint32_t parent = leaf ? o->leafParents[k] : node_parent(o->nodes[k]);
+            uint32_t& w = leaf ? o->leafAvg[k] : o->nodeAvg[k];
+            const uint32_t pw = o->nodeAvg[parent];
+            uint32_t lo = w & 0xFFFFu, hi = w >> 16;
+            if (lo == kHalfMax) lo = pw & 0xFFFFu;
+            if (hi == kHalfMax) hi = pw >> 16;
+            w = lo | (hi << 16);
+        }
+    }
+}
+
+// ---- BxDF dispatch by batch -------------------------------------------
+bool mat_specular(const oracle_scene* s, uint32_t batch, uint32_t id) {
+    if (batch == kBatchLambert || batch == kBatchLambertC) return false;
+    if (batch == kBatchMetal) return (1.0f - s->metal_params[10 * id + 9]) >= 0.99f;
+    if (batch == kBatchUnreal) return (1.0f - s->unreal_params[6 * id + 3]) >= 0.99f;
+    return true;
+}
+F3 mat_eval(const oracle_scene* s, uint32_t batch, uint32_t id, F3 wo, F3 wi, const Surface<float>& sf) {
+    if (batch == kBatchLambert) {
+        const float* a = s->lambert_albedo + 3 * id;
+        return lambert_eval(F3(a[0], a[1], a[2]), wo, sf);
+    }
+    if (batch == kBatchLambertC) {
+        const float* a = s->lambertc_albedo + 3 * id;
+        return lambertc_eval(F3(a[0], a[1], a[2]), wo, sf);
+    }
+    if (batch == kBatchUnreal) return unreal_eval(unreal_params<float>(s->unreal_params + 6 * id), wo, wi, sf);
+    if (batch == kBatchMetal) return metal_eval(metal_params<float>(s->metal_params + 10 * id), wo, wi, sf);
+    return F3(0.0f, 0.0f, 0.0f);
+}
+float mat_pdf(const oracle_scene* s, uint32_t batch, uint32_t id, F3 wo, F3 wi, const Surface<float>& sf) {
+    if (batch == kBatchLambert || batch == kBatchLambertC) return lambert_pdf(wo, sf);
+    if (batch == kBatchUnreal) return unreal_pdf(unreal_params<float>(s->unreal_params + 6 * id), wo, wi, sf);
+    if (batch == kBatchMetal) return metal_pdf(metal_params<float>(s->metal_params + 10 * id), wo, wi, sf);
+    return 0.0f;
+}
+BSample<float> mat_sample(const oracle_scene* s, uint32_t batch, uint32_t id, F3 wi,
+                          const Surface<float>& sf, uint32_t medium, float u0, float u1, float u2) {
+    if (batch == kBatchLambert) {
+        const float* a = s->lambert_albedo + 3 * id;
+        return lambert_sample(F3(a[0], a[1], a[2]), sf, u0, u1, medium);
+    }
+    if (batch == kBatchLambertC) {
+        const float* a = s->lambertc_albedo + 3 * id;
+        return lambertc_sample(F3(a[0], a[1], a[2]), sf, u0, u1, medium);
+    }
+    if (batch == kBatchUnreal)
+        return unreal_sample(unreal_params<float>(s->unreal_params + 6 * id), wi, sf, u2, u0, u1, medium);
+    if (batch == kBatchMetal)
+        return metal_sample(metal_params<float>(s->metal_params + 10 * id), wi, sf, u0, u1, medium);
+    const float* a = s->refract_albedo + 3 * id;
+    return refract_sample(F3(a[0], a[1], a[2]), s->refract_medium[id], s, wi, sf, medium, u0);
+}
+
+// BxDFProjFunc of KCGenAndSampleDistributionProduct
+F3 bxdf_proj(int cx, int cy, F3 nrm) {
+    const float rc = 1.0f / 8.0f;
+    const float s = (static_cast<float>(cx) + 0.5f) * rc, t = (static_cast<float>(cy) + 0.5f) * rc;
+    F3 dir = octa_to_dir_yup(s, t);
+    const F3 right = normalize(cross(dir, nrm));
+    float angle = 4.0f * kPiF / 64.0f;
+    angle *= 0.5f;
+    float sn, cs;
+    pm_sincos(angle, sn, cs);
+    const FQ q{cs, right.x * sn, right.y * sn, right.z * sn};
+    return qrotate(q, dir);
+}
+// inclusive Kogge-Stone scan over 8 lanes (as the warp computes it)
+void scan8(const float in[8], float out[8]) {
+    float x[8];
+    for (int i = 0; i < 8; i++) x[i] = in[i];
+    for (int off = 1; off < 8; off <<= 1) {
+        float y[8];
+        for (int i = 0; i < 8; i++) y[i] = x[i];
+        for (int i = 0; i < 8; i++)
+            if (i >= off) x[i] = y[i - off] + y[i];
+    }
+    for (int i = 0; i < 8; i++) out[i] = x[i];
+}
+
+}  // namespace
+
+extern "C" void oracle_svo_payload_init(oracle_svo* o, const float* light_rad, uint32_t omit) {
+    payload_init(o, light_rad, omit);
+    normalize_filter(o);
+}
+
+extern "C" void oracle_svo_payload_get(const oracle_svo* o, uint32_t* leafNormSpec,
+                                       uint32_t* nodeNormSpec, uint64_t* leafIrr, uint32_t* leafCnt,
+                                       uint32_t* leafAvg, uint32_t* nodeAvg) {
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(leafNormSpec, o->leafNormSpec);
+    cp(nodeNormSpec, o->nodeNormSpec);
+    cp(leafIrr, o->leafIrr);
+    cp(leafCnt, o->leafCnt);
+    cp(leafAvg, o->leafAvg);
+    cp(nodeAvg, o->nodeAvg);
+}
+
+namespace {
+
+struct WRay {
+    PRay<float> r;
+    uint32_t g0 = 0, g1 = 0x7E00u;  // guide words of this step (invalid by default)
+    bool guided = false;
+    // hit record
+    uint32_t key = 0, prim = kInvalid;
+    float t = 0.0f, b0 = 0.0f, b1 = 0.0f;
+};
+
+// One bin of KCGenAndSampleDistributionProduct, X x X field
+template <int X>
+void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* opt,
+               const oracle_wfpg_options* w, uint32_t depthTag, uint32_t key,
+               const std::vector<uint32_t>& rays, std::vector<WRay>& wave) {
+    constexpr int DPP = X / 8;
+    const float dppF = static_cast<float>(DPP);
+    const uint32_t frame = opt->frame;
+    const float aperture = (4.0f * kPiF) / (static_cast<float>(X) * static_cast<float>(X));
+    const uint32_t mix = hash32(frame ^ hash32(depthTag ^ 0xA511E9B3u ^ opt->seed_lo));
+    uint64_t best = ~0ull;
+    uint32_t rep = 0;
+    for (uint32_t i : rays) {
+        const uint32_t smp = wave[i].r.aux.sample;
+        const uint64_t k = (uint64_t(hash32(smp ^ mix)) << 32) | smp;
+        if (k < best) {
+            best = k;
+            rep = i;
+        }
+    }
+    const WRay& rr = wave[rep];
+    const Surface<float> sf0 = gen_surface(s, rr.prim, rr.b0, rr.b1, rr.r.d);
+    F3 org = nudge(sf0.pos, sf0.geo);
+    org = org + sf0.geo * (tree.o->P.leaf * 0.01f);
+    float tMin = tree.o->P.leaf * 0.15f;
+    tMin += 1.0e-5f;
+    const Rng4 rj = rng_block(key, frame, kTagGuideBin | depthTag, 0u, opt->seed_lo, opt->seed_hi);
+    std::vector<float> field(X * X), tmp(X * X);
+    for (int p = 0; p < X * X; p++) {
+        const int x = p % X, y = p / X;
+        float ss = (static_cast<float>(x) + rj.u[0]) / static_cast<float>(X);
+        float tt = (static_cast<float>(y) + rj.u[1]) / static_cast<float>(X);
+        octa_wrap(ss, tt);
+        const F3 dir = octa_to_dir_yup(ss, tt);
+        bool isLeaf;
+        uint32_t id;
+        tree.cone_trace(org, dir, tMin, aperture, 0u, isLeaf, id);
+        float r = tree.read_radiance(dir, id, isLeaf);
+        if (r == 0.0f) r = 1.0e-4f;
+        field[p] = r;
+    }
+    for (int p = 0; p < X * X; p++) {
+        const int x = p % X, y = p / X;
+        float acc = 0.0f;
+        for (int j = -5; j <= 5; j++) {
+            int nx = x + j, ny = y;
+            if (nx >= X || nx < 0) octa_wrap_int(nx, ny, X, X);
+            acc += field[ny * X + nx] * w->filter[j + 5];
+        }
+        tmp[p] = acc;
+    }
+    for (int p = 0; p < X * X; p++) {
+        const int x = p % X, y = p / X;
+        float acc = 0.0f;
+        for (int j = -5; j <= 5; j++) {
+            int nx = x, ny = y + j;
+            if (ny >= X || ny < 0) octa_wrap_int(nx, ny, X, X);
+            acc += tmp[ny * X + nx] * w->filter[j + 5];
+        }
+        field[p] = acc;
+    }
+    float small[64], normc[64];
+    for (int c = 0; c < 64; c++) {
+        const int cx = c & 7, cy = c >> 3;
+        float sum = 0.0f, mx = 0.0f;
+        for (int iy = 0; iy < DPP; iy++)
+            for (int ix = 0; ix < DPP; ix++) {
+                const float v = field[(cy * DPP + iy) * X + cx * DPP + ix];
+                sum += v;
+                mx = std::fmax(mx, v);
+            }
+        small[c] = sum / static_cast<float>(DPP * DPP);
+        normc[c] = mx;
+    }
+    const float kInv4Pi = 0.25f * kInvPiF;
+    for (uint32_t i : rays) {
+        WRay& wr = wave[i];
+        const uint32_t batch = wr.key >> 24, id = wr.key & 0xFFFFFFu;
+        const bool isLight = batch == kBatchLight;
+        const bool spec = !isLight && mat_specular(s, batch, id);
+        const Surface<float> sf = gen_surface(s, wr.prim, wr.b0, wr.b1, wr.r.d);
+        const F3 wi = -wr.r.d;
+        const F3 nrm = to_space(F3(0.0f, 0.0f, 1.0f), sf.w2t);
+        float pdfX[64], cdfX[64], rowTot[8], pdfY[8], cdfY[8];
+        for (int row = 0; row < 8; row++) {
+            float prod[8], incl[8];
+            for (int cx = 0; cx < 8; cx++) {
+                const int c = row * 8 + cx;
+                float gray = 1.0f;
+                if (!isLight && !spec) gray = lum3(mat_eval(s, batch, id, bxdf_proj(cx, row, nrm), wi, sf));
+                prod[cx] = std::fmax(1.0e-3f, gray * small[c]);
+            }
+            scan8(prod, incl);
+            const float rowTotal = incl[7];
+            const float rcp = 1.0f / rowTotal;
+            for (int cx = 0; cx < 8; cx++) {
+                cdfX[row * 8 + cx] = incl[cx] * rcp;
+                pdfX[row * 8 + cx] = prod[cx] * 8.0f * rcp;
+            }
+            rowTot[row] = rowTotal;
+        }
+        {
+            float incl[8];
+            scan8(rowTot, incl);
+            const float rcp = 1.0f / incl[7];
+            for (int l = 0; l < 8; l++) {
+                cdfY[l] = incl[l] * rcp;
+                pdfY[l] = rowTot[l] * (8.0f * rcp);
+            }
+        }
+        const uint32_t smp = wr.r.aux.sample;
+        const Rng4 r0 = rng_block(smp, frame, kTagGuide | depthTag, 0u, opt->seed_lo, opt->seed_hi);
+        const bool purePG = w->pure_pg != 0;
+        float ss = 0.0f, tt = 0.0f, pdf = 1.0f;
+        bool bxdfSel = true;
+        auto product_pdf = [&](float u, float v) {
+            const float ex = u * 8.0f, ey = v * 8.0f;
+            const float ox = std::floor(ex), oy = std::floor(ey);
+            const float ix = (ex - ox) * dppF, iy = (ey - oy) * dppF;
+            int ocx = std::min(std::max(f2i_sat(ox), 0), 7), ocy = std::min(std::max(f2i_sat(oy), 0), 7);
+            int gx = ocx * DPP + f2i_sat(std::floor(ix)), gy = ocy * DPP + f2i_sat(std::floor(iy));
+            gx = std::min(std::max(gx, 0), X - 1);
+            gy = std::min(std::max(gy, 0), X - 1);
+            const int cell = ocy * 8 + ocx;
+            const float inner = field[gy * X + gx] / small[cell];
+            return pdfX[cell] * pdfY[ocy] * inner;
+        };
+        if (!purePG && (isLight || spec)) {
+        } else if (!purePG && r0.u[0] >= w->mis_ratio) {
+            const Rng4 r1 = rng_block(smp, frame, kTagGuide | depthTag, 1u, opt->seed_lo, opt->seed_hi);
+            const BSample<float> bs = mat_sample(s, batch, id, wi, sf, wr.r.aux.medium, r1.u[0], r1.u[1], r1.u[2]);
+            dir_yup_to_octa(bs.dir, ss, tt);
+            const float pdfSampled = bs.pdf;
+            const float pdfOther = product_pdf(ss, tt) * kInv4Pi;
+            const float ratio = 1.0f - w->mis_ratio;
+            const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+            pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+            pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            bxdfSel = true;
+        } else {
+            const float xi0 = r0.u[1], xi1 = r0.u[2];
+            int rowId = 8;
+            for (int l = 0; l < 8; l++)
+                if (!(xi0 > cdfY[l])) { rowId = l; break; }
+            rowId = std::min(rowId, 7);
+            int colId = 8;
+            for (int l = 0; l < 8; l++)
+                if (!(xi1 > cdfX[rowId * 8 + l])) { colId = l; break; }
+            colId = std::min(colId, 7);
+            const int cell = rowId * 8 + colId;
+            float u = 0.0f, v = 0.0f, tex = 0.0f;
+            bool lucky = false;
+            float u0 = 0.0f, v0 = 0.0f, tex0 = 0.0f;
+            for (int round = 0; round < 24 && !lucky; round++) {
+                for (uint32_t lane = 0; lane < 32; lane++) {
+                    const Rng4 rl = rng_block(smp, frame, kTagGuide | depthTag, 2u + uint32_t(round) * 32u + lane,
+                                              opt->seed_lo, opt->seed_hi);
+                    const int ix = f2i_sat(rl.u[0] * dppF), iy = f2i_sat(rl.u[1] * dppF);
+                    const float tx = field[(rowId * DPP + iy) * X + colId * DPP + ix];
+                    if (lane == 0) {
+                        u0 = rl.u[0];
+                        v0 = rl.u[1];
+                        tex0 = tx;
+                    }
+                    if (rl.u[2] <= tx / normc[cell]) {
+                        u = rl.u[0];
+                        v = rl.u[1];
+                        tex = tx;
+                        lucky = true;
+                        break;
+                    }
+                }
+            }
+            if (!lucky) {
+                u = u0;
+                v = v0;
+                tex = tex0;
+            }
+            const float pdfInner = lucky ? tex / small[cell] : 1.0f;
+            const float pdfS = pdfY[rowId] * pdfX[cell] * pdfInner;
+            const float rcpX = 1.0f / static_cast<float>(X);
+            ss = (static_cast<float>(colId) * dppF + u * dppF) * rcpX;
+            tt = (static_cast<float>(rowId) * dppF + v * dppF) * rcpX;
+            if (purePG) {
+                pdf = pdfS * kInv4Pi;
+            } else {
+                const float pdfSampled = pdfS * kInv4Pi;
+                const F3 wo = octa_to_dir_yup(ss, tt);
+                const float pdfOther = mat_pdf(s, batch, id, wo, wi, sf);
+                const float ratio = w->mis_ratio;
+                const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+                pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+                pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            }
+            bxdfSel = false;
+        }
+        if (pdf != pdf || ss != ss || tt != tt) {
+            ss = 0.5f;
+            tt = 0.5f;
+            pdf = 1.0f;
+        }
+        wr.g0 = uint32_t(f2h(ss)) | (uint32_t(f2h(tt)) << 16);
+        wr.g1 = uint32_t(f2h(pdf)) | (bxdfSel ? kGuideBxdf : 0u) | kGuideValid;
+    }
+}
+
+}  // namespace
+
+extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* b,
+                                       const oracle_camera* cam, const oracle_options* opt,
+                                       const oracle_wfpg_options* w, oracle_svo* svo, float* out,
+                                       uint32_t* dumpGuide, uint32_t* dumpBin) {
+    const uint32_t sp = opt->samples;
+    const uint32_t SW = opt->width * sp, SH = opt->height * sp;
+    const uint32_t P = SW * SH;
+    const uint32_t levels = opt->max_depth + 1;
+    Chain chain(levels, P);
+    Tree tree{svo};
+    const uint32_t D = svo->P.depth;
+    const uint32_t minLevel = std::min(w->min_bin_level, D);
+    Ctx<float> c{s, b, opt, out};
+    for (uint32_t i = 0; i < 3 * P; i++) out[i] = 0.0f;
+    std::vector<WRay> cur, next;
+    cur.reserve(P);
+    const float* Pc = cam->position;
+    for (uint32_t sid = 0; sid < P; sid++) {
+        // camera ray as in render(); WFPG numbers it depth 1 (RayAuxInitWFPG)
+        const uint32_t sx = sid % SW, sy = sid / SW;
+        const Rng4 rc = rng_block(sid, opt->frame, kTagCamera, 0, opt->seed_lo, opt->seed_hi);
+        float dx = cam->plane_size[0] / static_cast<float>(SW);
+        float dy = cam->plane_size[1] / static_cast<float>(SH);
+        float sdx = static_cast<float>(sx) * dx;
+        float sdy = static_cast<float>(sy) * dy;
+        sdx += rc.u[0] * dx;
+        sdy += rc.u[1] * dy;
+        float v[3];
+        for (int i = 0; i < 3; i++) v[i] = cam->bottom_left[i] + ((sdx * cam->right[i]) + (sdy * cam->up[i]));
+        const F3 dirf = normalize(F3(v[0], v[1], v[2]) - F3(Pc[0], Pc[1], Pc[2]));
+        WRay wr;
+        wr.r.o = F3(Pc[0], Pc[1], Pc[2]);
+        wr.r.d = dirf;
+        wr.r.tmin = cam->near_far[0];
+        wr.r.tmax = cam->near_far[1];
+        wr.r.aux = Aux<float>{F3(1, 1, 1), sid, kInvalid, s->base_medium, 1, CAMERA_RAY,
+                              std::numeric_limits<float>::quiet_NaN()};
+        cur.push_back(wr);
+        const size_t at = chain.at(0, sid);
+        chain.pos[3 * at] = Pc[0];
+        chain.pos[3 * at + 1] = Pc[1];
+        chain.pos[3 * at + 2] = Pc[2];
+        chain.rf[3 * at] = chain.rf[3 * at + 1] = chain.rf[3 * at + 2] = 1.0f;
+        chain.valid[at] = 1;
+    }
+    uint64_t rays = 0;
+    for (uint32_t it = 0; it < opt->max_depth && !cur.empty(); it++) {
+        parallel_for(uint32_t(cur.size()), opt->threads, [&](uint32_t b0, uint32_t b1) {
+            for (uint32_t i = b0; i < b1; i++) {
+                WRay& wr = cur[i];
+                const Hit<float> h = trace_one<float>(s, b, wr.r.o, wr.r.d, wr.r.tmin, wr.r.tmax);
+                wr.prim = h.prim;
+                wr.key = (h.prim == kInvalid) ? 0u : h.key;
+                wr.t = h.t;
+                wr.b0 = h.b0;
+                wr.b1 = h.b1;
+                wr.guided = false;
+                wr.g0 = 0u;
+                wr.g1 = 0x7E00u;
+            }
+        });
+        rays += cur.size();
+        const bool guideNow = !w->skip_pg && it < w->guide_bounce;
+        if (guideNow) {
+            std::fill(svo->leafBin.begin(), svo->leafBin.end(), 0u);
+            std::fill(svo->nodeBin.begin(), svo->nodeBin.end(), 0u);
+            std::vector<uint32_t> binKey(cur.size(), kBinInvalid);
+            for (size_t i = 0; i < cur.size(); i++) {
+                const WRay& wr = cur[i];
+                if (wr.r.aux.type == NEE_RAY || (wr.key >> 24) == kBatchNull) continue;
+                const F3 p(wr.r.o.x + wr.t * wr.r.d.x, wr.r.o.y + wr.t * wr.r.d.y, wr.r.o.z + wr.t * wr.r.d.z);
+                uint32_t leaf;
+                if (tree.nearest(leaf, p, D)) {
+                    binKey[i] = leaf | kBinLeaf;
+                    svo->leafBin[leaf] += 1u;
+                }
+            }
+            // KCCollapseRayCountsLeaf / KCCollapseRayCounts
+            for (size_t l = 0; l < svo->leafBin.size(); l++) {
+                if (D == minLevel) { svo->leafBin[l] |= kBinMark; continue; }
+                const uint32_t cnt = svo->leafBin[l] & ~kBinMark;
+                if (cnt == 0) continue;
+                if (cnt < w->bin_ray_count) svo->nodeBin[svo->leafParents[l]] += cnt;
+                else svo->leafBin[l] |= kBinMark;
+            }
+            for (int L = int(D) - 1; L >= int(minLevel); L--) {
+                for (uint32_t k = svo->levelOffsets[L]; k < svo->levelOffsets[L + 1]; k++) {
+                    if (uint32_t(L) == minLevel) { svo->nodeBin[k] |= kBinMark; continue; }
+                    const uint32_t cnt = svo->nodeBin[k] & ~kBinMark;
+                    if (cnt < w->bin_ray_count) svo->nodeBin[node_parent(svo->nodes[k])] += cnt;
+                    else svo->nodeBin[k] |= kBinMark;
+                }
+            }
+            std::map<uint32_t, std::vector<uint32_t>> bins;
+            for (size_t i = 0; i < cur.size(); i++) {
+                if (binKey[i] == kBinInvalid) continue;
+                bool isLeaf;
+                const uint32_t node = tree.marked_bin(binKey[i] & ~kBinLeaf, isLeaf);
+                if (!isLeaf) binKey[i] = node;
+                bins[binKey[i]].push_back(uint32_t(i));
+            }
+            std::vector<std::pair<uint32_t, const std::vector<uint32_t>*>> list;
+            for (auto& kv : bins) list.push_back({kv.first, &kv.second});
+            const uint32_t ki = it < 4 ? it : 4;
+            parallel_for(uint32_t(list.size()), opt->threads, [&](uint32_t b0, uint32_t b1) {
+                for (uint32_t q = b0; q < b1; q++) {
+                    const uint32_t key = list[q].first;
+                    const std::vector<uint32_t>& rs = *list[q].second;
+                    if (ki <= 1) guide_bin<64>(s, tree, opt, w, it, key, rs, cur);
+                    else if (ki == 2) guide_bin<32>(s, tree, opt, w, it, key, rs, cur);
+                    else if (ki == 3) guide_bin<16>(s, tree, opt, w, it, key, rs, cur);
+                    else guide_bin<8>(s, tree, opt, w, it, key, rs, cur);
+                }
+            });
+            for (size_t i = 0; i < cur.size(); i++) cur[i].guided = binKey[i] != kBinInvalid;
+            if (it == w->dump_iteration) {
+                for (size_t i = 0; i < cur.size(); i++) {
+                    if (binKey[i] == kBinInvalid) continue;
+                    const uint32_t smp = cur[i].r.aux.sample;
+                    if (dumpGuide) {
+                        dumpGuide[2 * smp] = cur[i].g0;
+                        dumpGuide[2 * smp + 1] = cur[i].g1;
+                    }
+                    if (dumpBin) dumpBin[smp] = binKey[i];
+                }
+            }
+        }
+        next.clear();
+        const bool gen = (it + 1) < opt->max_depth;
+        std::vector<PRay<float>> outs;
+        for (WRay& wr : cur) {
+            if (wr.prim == kInvalid) continue;
+            const uint32_t batch = wr.key >> 24, id = wr.key & 0xFFFFFFu;
+            if (batch == kBatchNull) continue;
+            if (batch == kBatchLight) {
+                boundary_work(c, wr.r, id, wr.prim, wr.b0, wr.b1, wr.t, &chain);
+            } else {
+                outs.clear();
+                const uint32_t gw[2] = {wr.g0, wr.g1};
+                path_work(c, wr.r, wr.prim, wr.b0, wr.b1, batch, id, gen, outs,
+                          (guideNow && wr.guided) ? gw : nullptr, &chain);
+                for (const PRay<float>& o : outs) {
+                    WRay n;
+                    n.r = o;
+                    next.push_back(n);
+                }
+            }
+        }
+        std::swap(cur, next);
+    }
+    // WFPGTracer::Finalize: chain sums, deposit, normalise and filter
+    for (uint32_t p = 0; p < P; p++) {
+        uint32_t L = 0;
+        while (L + 1 < levels && chain.valid[chain.at(L + 1, p)]) L++;
+        const uint32_t lastD = (L + 1 < levels) ? L + 1 : levels - 1;
+        for (uint32_t d = 1; d <= L; d++) {
+            const size_t at = chain.at(d, p);
+            const float bx = chain.rf[3 * at], by = chain.rf[3 * at + 1], bz = chain.rf[3 * at + 2];
+            F3 tot(0.0f, 0.0f, 0.0f);
+            for (uint32_t Dd = d + 1; Dd <= lastD; Dd++) {
+                const size_t q = chain.at(Dd, p);
+                const float* cn = &chain.nee[3 * q];
+                const float* cp = &chain.path[3 * q];
+                tot.x += (bx == 0.0f) ? 0.0f : cn[0] / bx;
+                tot.y += (by == 0.0f) ? 0.0f : cn[1] / by;
+                tot.z += (bz == 0.0f) ? 0.0f : cn[2] / bz;
+                tot.x += (bx == 0.0f) ? 0.0f : cp[0] / bx;
+                tot.y += (by == 0.0f) ? 0.0f : cp[1] / by;
+                tot.z += (bz == 0.0f) ? 0.0f : cp[2] / bz;
+            }
+            const F3 pos(chain.pos[3 * at], chain.pos[3 * at + 1], chain.pos[3 * at + 2]);
+            const size_t pa = chain.at(d - 1, p);
+            const F3 wo = normalize(F3(chain.pos[3 * pa], chain.pos[3 * pa + 1], chain.pos[3 * pa + 2]) - pos);
+            uint32_t leaf;
+            if (!tree.nearest(leaf, pos, D)) continue;
+            float sd, spc;
+            const F3 n = read_normal_spec(svo->leafNormSpec[leaf], sd, spc);
+            const float NdL = dot(n, wo);
+            int side;
+            if (NdL >= 0.0f) side = 0;
+            else if (NdL < 0.0f) side = 1;
+            else continue;
+            svo->leafIrr[2 * leaf + side] += to_fixed(lum3(tot));
+            svo->leafCnt[2 * leaf + side] += 1u;
+        }
+    }
+    normalize_filter(svo);
+    return rays;
 }
 
 namespace {
@@ -1953,7 +3082,22 @@ int oracle_probe(const char* name, const float* in, float* out) {
     auto w3 = [&](int i, F3 a) { out[i] = a.x; out[i + 1] = a.y; out[i + 2] = a.z; };
     auto w4 = [&](int i, Q a) { out[i] = a.w; out[i + 1] = a.x; out[i + 2] = a.y; out[i + 3] = a.z; };
     std::string n(name);
-    if (n == "hemi_cosine") {  // xi0 xi1 -> dir3 pdf
+    if (n == "half") {  // x -> h2f(f2h(x)), f2h bits
+        const uint16_t h = f2h(in[0]);
+        out[0] = h2f(h);
+        out[1] = static_cast<float>(h);
+    } else if (n == "octa") {  // dir3 (y-up) -> s t, dir3 back
+        float ss, tt;
+        dir_yup_to_octa(v(0), ss, tt);
+        out[0] = ss;
+        out[1] = tt;
+        w3(2, octa_to_dir_yup(ss, tt));
+    } else if (n == "octa_wrap_int") {  // x y dim -> x y
+        int32_t x = int32_t(in[0]), y = int32_t(in[1]);
+        octa_wrap_int(x, y, int32_t(in[2]), int32_t(in[2]));
+        out[0] = float(x);
+        out[1] = float(y);
+    } else if (n == "hemi_cosine") {  // xi0 xi1 -> dir3 pdf
         float pdf;
         F3 d = hemi_cosine(in[0], in[1], pdf);
         w3(0, d);

@@ -153,6 +153,36 @@ void oracle_svo_get(const oracle_svo*, uint64_t* nodes, uint32_t* leaf_parents,
                     uint64_t* leaf_codes, uint32_t* leaf_lights, uint32_t* level_offsets,
                     uint32_t* tri_voxel_counts, float* params7);
 
+/* Radiance-cache payload of the octree (KCReduceVoxelPayload,
+ * KCAverageNormals, NormalizeAndFilterRadiance): light radiance per light
+ * (3 floats), omit = OmitDirectRadiance.  Get: leaf / node normal words,
+ * leaf radiance sums (2 per leaf, 2^24 fixed point), leaf counts (2 per
+ * leaf), leaf / node half2 averages. */
+void oracle_svo_payload_init(oracle_svo*, const float* light_rad, uint32_t omit);
+void oracle_svo_payload_get(const oracle_svo*, uint32_t* leaf_norm_spec, uint32_t* node_norm_spec,
+                            uint64_t* leaf_irr, uint32_t* leaf_cnt, uint32_t* leaf_avg,
+                            uint32_t* node_avg);
+
+/* One WFPG frame (WFPGTracer.cu:1480-1833) over the octree, which it
+ * updates (deposit + normalise/filter).  Per-sample radiance to out (3 per
+ * sample); guide words and bin ids of step dump_iteration per path to
+ * dump_guide (2 per path) / dump_bin (1 per path), either may be NULL.
+ * Returns the rays traced. */
+typedef struct oracle_wfpg_options {
+    uint32_t min_bin_level;
+    uint32_t bin_ray_count;
+    uint32_t pure_pg;
+    uint32_t skip_pg;
+    uint32_t guide_bounce;
+    float mis_ratio;
+    float filter[11];
+    uint32_t dump_iteration;
+} oracle_wfpg_options;
+uint64_t oracle_render_wfpg(const oracle_scene* scene, const oracle_bvh* bvh,
+                            const oracle_camera* cam, const oracle_options* opt,
+                            const oracle_wfpg_options* wopt, oracle_svo* svo, float* out_rgb,
+                            uint32_t* dump_guide, uint32_t* dump_bin);
+
 /* Single-vertex BxDF probes used by the golden-vector tests. */
 void oracle_bxdf_sample(uint32_t type, const float* params, const float* wi,
                         const float* w2t, const float* geo_normal, const float* pos,

@@ -7,6 +7,7 @@ restatement it loads cites the MRay reference file:line for every step.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import subprocess
 from pathlib import Path
 
@@ -219,6 +220,43 @@ class OracleScene:
         rays = fn(C.byref(self.c), self.bvh, C.byref(cam), C.byref(o), _p(out))
         return out, int(rays)
 
+    def render_wfpg(self, camera_frame: np.ndarray, width: int, height: int, samples: int,
+                    max_depth: int, rr_start: int, nee: bool, seed: int, svo: "OracleSvo",
+                    frame: int = 0, mis: bool = False, min_bin_level: int = 5,
+                    bin_ray_count: int = 512, pure_pg: bool = False, skip_pg: bool = False,
+                    guide_bounce: int = 512, mis_ratio: float = 0.5, filter_alpha: float = 1.0,
+                    dump_iteration: int | None = None, threads: int = 0):
+        """One WFPG frame; returns per-sample radiance, rays traced and the
+        guide words / bin ids (per path) of step dump_iteration."""
+        cam = Camera()
+        f = camera_frame
+        cam.position[:] = [float(v) for v in f[0:3]]
+        cam.bottom_left[:] = [float(v) for v in f[3:6]]
+        cam.right[:] = [float(v) for v in f[6:9]]
+        cam.up[:] = [float(v) for v in f[9:12]]
+        cam.plane_size[:] = [float(v) for v in f[12:14]]
+        cam.near_far[:] = [float(v) for v in f[14:16]]
+        o = Options(width, height, samples, max_depth, rr_start, 1 if nee else 0, 1 if mis else 0,
+                    seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, frame, threads, 0, 0)
+        w = WfpgOptions()
+        w.min_bin_level = min_bin_level
+        w.bin_ray_count = bin_ray_count
+        w.pure_pg = 1 if pure_pg else 0
+        w.skip_pg = 1 if skip_pg else 0
+        w.guide_bounce = guide_bounce
+        w.mis_ratio = float(mis_ratio)
+        w.filter[:] = [float(v) for v in gauss_taps(filter_alpha)]
+        w.dump_iteration = 0xFFFFFFFF if dump_iteration is None else int(dump_iteration)
+        paths = width * samples * height * samples
+        out = np.zeros((height * samples, width * samples, 3), np.float32)
+        dg = np.zeros((paths, 2), np.uint32)
+        dg[:, 1] = 0x7E00
+        db = np.full(paths, 0xFFFFFFFF, np.uint32)
+        lib.oracle_render_wfpg.restype = C.c_uint64
+        rays = lib.oracle_render_wfpg(C.byref(self.c), self.bvh, C.byref(cam), C.byref(o),
+                                      C.byref(w), svo.h, _p(out), _p(dg), _p(db))
+        return out, int(rays), dg, db
+
 
 def scene_tables(scene) -> dict:
     """HitKeys and material tables of a scene, assigned as the product's loader
@@ -278,6 +316,71 @@ def build_tbn(scene) -> np.ndarray:
     lib.oracle_build_tbn(_p(pos), _p(nrm), _p(uvs), _p(idx), C.c_uint32(pos.shape[0]),
                          C.c_uint32(idx.shape[0]), _p(out))
     return out
+
+
+class WfpgOptions(C.Structure):
+    _fields_ = [("min_bin_level", C.c_uint32), ("bin_ray_count", C.c_uint32),
+                ("pure_pg", C.c_uint32), ("skip_pg", C.c_uint32), ("guide_bounce", C.c_uint32),
+                ("mis_ratio", C.c_float), ("filter", C.c_float * 11),
+                ("dump_iteration", C.c_uint32)]
+
+
+def gauss_taps(alpha: float) -> np.ndarray:
+    """StaticGaussianFilter1D<11> taps, exp(-t^2 / (2 alpha)) normalised,
+    evaluated in double from the float option value and rounded once."""
+    a = float(np.float32(alpha))
+    w = [math.exp(-(float(i - 5) * float(i - 5)) * 0.5 / a) for i in range(11)]
+    tot = 0.0
+    for v in w:
+        tot += v
+    return np.array([v / tot for v in w], np.float32)
+
+
+class OracleSvo:
+    """The oracle's octree with its radiance-cache payload; a WFPG frame
+    rendered by OracleScene.render_wfpg updates it."""
+
+    def __init__(self, scene, tri_key: np.ndarray, extent: np.ndarray, resolution: int,
+                 light_radiance: np.ndarray, omit_direct: bool = False):
+        self._pos = np.ascontiguousarray(scene.positions, np.float32)
+        self._idx = np.ascontiguousarray(scene.indices, np.uint32)
+        self._key = np.ascontiguousarray(tri_key, np.uint32)
+        ext = np.ascontiguousarray(extent[:6], np.float32)
+        lib.oracle_svo_build.restype = C.c_void_p
+        st = C.c_int(0)
+        self.h = C.c_void_p(lib.oracle_svo_build(_p(self._pos), _p(self._idx), _p(self._key),
+                                                 C.c_uint32(self._idx.shape[0]), _p(ext),
+                                                 C.c_uint32(resolution), C.byref(st)))
+        self.status = st.value
+        self._rad = np.ascontiguousarray(np.asarray(light_radiance, np.float32).reshape(-1, 3))
+        if self.status == 0:
+            lib.oracle_svo_payload_init(self.h, _p(self._rad), C.c_uint32(1 if omit_direct else 0))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.oracle_svo_destroy(self.h)
+            self.h = None
+
+    def export(self) -> dict:
+        sz = np.zeros(6, np.uint32)
+        lib.oracle_svo_sizes(self.h, _p(sz))
+        U, N = int(sz[1]), int(sz[2])
+        out = {"status": self.status, "voxels": int(sz[0]), "depth": int(sz[3]),
+               "nodes": np.zeros(N, np.uint64), "leaf_parents": np.zeros(U, np.uint32),
+               "leaf_codes": np.zeros(U, np.uint64), "leaf_lights": np.zeros(U, np.uint32),
+               "level_offsets": np.zeros(int(sz[4]), np.uint32),
+               "tri_voxels": np.zeros(int(sz[5]), np.uint32), "params": np.zeros(7, np.float32),
+               "leaf_normals": np.zeros(U, np.uint32), "node_normals": np.zeros(N, np.uint32),
+               "leaf_irr": np.zeros((U, 2), np.uint64), "leaf_cnt": np.zeros((U, 2), np.uint32),
+               "leaf_avg": np.zeros(U, np.uint32), "node_avg": np.zeros(N, np.uint32)}
+        lib.oracle_svo_get(self.h, _p(out["nodes"]), _p(out["leaf_parents"]),
+                           _p(out["leaf_codes"]), _p(out["leaf_lights"]), _p(out["level_offsets"]),
+                           _p(out["tri_voxels"]), _p(out["params"]))
+        if self.status == 0:
+            lib.oracle_svo_payload_get(self.h, _p(out["leaf_normals"]), _p(out["node_normals"]),
+                                       _p(out["leaf_irr"]), _p(out["leaf_cnt"]),
+                                       _p(out["leaf_avg"]), _p(out["node_avg"]))
+        return out
 
 
 def svo_build(scene, tri_key: np.ndarray, extent: np.ndarray, resolution: int) -> dict:

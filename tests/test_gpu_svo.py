@@ -55,10 +55,14 @@ def test_svo_leaf_normals_are_unit_directions(system):
     g.construct_accelerators()
     g.build_svo(128)
     s = g.export_svo()
-    pn = s["leaf_normals"]
-    az = (pn & 0xFFFF) / 65535.0 * 2 * np.pi - np.pi
-    inc = (pn >> 16) / 65535.0 * np.pi
-    n = np.stack([np.cos(az) * np.sin(inc), np.sin(az) * np.sin(inc), np.cos(inc)], 1)
+    # VoxelPayload normal word: x, y 9-bit UNORM, length 7 bits, z sign bit 31
+    w = s["leaf_normals"].astype(np.int64)
+    nx = (w & 511) * (2.0 / 511.0) - 1.0
+    ny = ((w >> 9) & 511) * (2.0 / 511.0) - 1.0
+    nz = np.sqrt(np.maximum(0.0, 1.0 - nx * nx - ny * ny)) * np.where((w >> 31) & 1, -1.0, 1.0)
+    n = np.stack([nx, ny, nz], 1)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    assert np.all(((w >> 18) & 127) >= 126)  # leaf normals are unit means (length ~1)
     # floor voxels (lowest y layer, away from walls) carry the floor's
     # geometric normal, cross(p1 - p0, p2 - p0) as the reference voxeliser
     # takes it (GPUPrimitiveTriangle.h:434-435); the floor's winding gives -y

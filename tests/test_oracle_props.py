@@ -134,3 +134,81 @@ def test_cpu_render_is_deterministic_and_fp64_close(oracle):
     assert a.sum() > 0 and np.isfinite(d).all()
     # same RNG stream; paths only part after precision-sensitive events
     assert abs(a.sum() - d.sum()) / d.sum() < 0.2
+
+
+def _probe(oracle, name, vals, nout):
+    import ctypes as C
+    a = np.ascontiguousarray(vals, np.float32)
+    o = np.zeros(nout, np.float32)
+    assert oracle.lib.oracle_probe(name.encode(), a.ctypes.data_as(C.c_void_p),
+                                   o.ctypes.data_as(C.c_void_p)) == 0
+    return o
+
+
+def test_half_conversion_is_ieee_round_to_nearest_even(oracle):
+    """The guide words and radiance averages use a portable binary16
+    conversion; it must equal IEEE round-to-nearest-even (numpy float16)."""
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([
+        rng.standard_normal(2000).astype(np.float32) * 10.0,
+        (rng.random(2000) * 7e4).astype(np.float32),
+        (rng.random(500) * 1e-4).astype(np.float32),            # subnormal halves
+        np.array([0.0, -0.0, 65504.0, 65519.0, 65520.0, 1e9, 6e-8, 3e-8, 2.0 ** -25,
+                  2.0 ** -24, 1.0 + 2.0 ** -11, 1.0 + 3 * 2.0 ** -11], np.float32)])
+    for x in xs:
+        o = _probe(oracle, "half", [x], 2)
+        with np.errstate(over="ignore"):
+            ref = np.float32(np.float16(x))
+        assert o[0] == ref or (np.isinf(ref) and np.isinf(o[0])), (x, o[0], ref)
+
+
+def test_octahedral_map_round_trip(oracle):
+    """Co-centric octahedral map (CoordinateConversion.h:112-183): direction
+    -> (s, t) in [0,1]^2 -> the same direction."""
+    rng = np.random.default_rng(6)
+    d = rng.standard_normal((500, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    for v in d.astype(np.float32):
+        o = _probe(oracle, "octa", v, 5)
+        assert 0.0 <= o[0] <= 1.0 and 0.0 <= o[1] <= 1.0
+        assert np.abs(o[2:5] - v).max() < 2e-6, (v, o)
+
+
+def test_octahedral_int_wrap_mirrors_edges(oracle):
+    """CocentricOctohedralWrapInt: stepping over an edge mirrors the other
+    coordinate, a corner step goes to the opposite corner; in-range texels
+    are unchanged."""
+    X = 64
+    for x, y, ex, ey in [(-1, 10, 0, 53), (64, 10, 63, 53), (10, -1, 53, 0), (10, 64, 53, 63),
+                         (5, 7, 5, 7), (-3, -2, 61, 62)]:
+        o = _probe(oracle, "octa_wrap_int", [x, y, X], 2)
+        assert (int(o[0]), int(o[1])) == (ex, ey), (x, y, o)
+
+
+def test_oracle_wfpg_is_deterministic_and_deposits(oracle):
+    """Two oracle WFPG frames from identical caches agree bit for bit; the
+    frame deposits one sample per path vertex into the cache."""
+    from meturay_b200 import camera_frame, scenes
+    sc = scenes.cornell(seed=6, width=16, height=16, mixed=True)
+    ex = oracle.scene_tables(sc)
+    ex["tbn"] = oracle.build_tbn(sc)
+    os_ = oracle.OracleScene(sc, ex)
+    ext = np.concatenate([sc.positions.min(0), sc.positions.max(0)]).astype(np.float32)
+    cf = np.concatenate([camera_frame(sc.camera), np.float32(sc.camera["near_far"])])
+    outs = []
+    for _ in range(2):
+        svo = oracle.OracleSvo(sc, ex["tri_key"], ext, 32, ex["light_radiance"])
+        before = svo.export()
+        img, rays, dg, db = os_.render_wfpg(cf, 16, 16, 1, 4, 3, True, 9, svo, min_bin_level=2,
+                                            bin_ray_count=16, dump_iteration=0)
+        after = svo.export()
+        outs.append((img, rays, dg, db, after))
+    a, b = outs
+    assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+    assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+    for k in ("leaf_irr", "leaf_cnt", "leaf_avg", "node_avg"):
+        assert np.array_equal(a[4][k], b[4][k])
+    deposits = int(a[4]["leaf_cnt"].sum() - before["leaf_cnt"].sum())
+    assert 0 < deposits <= 16 * 16 * 4
+    guided = (a[2][:, 1] >> 17) & 1
+    assert guided.sum() > 0 and np.all(a[3][guided == 1] != 0xFFFFFFFF)
