@@ -1,4 +1,6 @@
-"""Benchmark: Mrays/s of the plain wavefront path tracer on the 1M-triangle scene.
+"""Benchmark: Mrays/s of the plain wavefront path tracer on the 1M-triangle scene,
+plus the same frame with SVO path guiding (WFPGTracer) and the equal-time MSE
+of both against a converged plain render (the "guided" object of the line).
 
 Workload ("clusters-1M"): 1000 Gaussian clusters x 1000 triangles (seed 1),
 1920x1080, 1 sample per pixel per step ("Samples": 1), depth 8, NEE on,
@@ -179,6 +181,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     # ---- roofline of the traversal kernel (one stepwise profiled frame) ----
     prof = t.profile_frame()
     launches = t.launches_per_frame() * args.steps
+    guided = run_guided(args, g, m, torch, dev) if (args.guided and rank == 0 and world == 1) \
+        else None
 
     if dist:
         tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
@@ -233,7 +237,95 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                      "tri_tests_per_ray": prof["tri_tests"] / max(prof["rays"], 1)},
         "gpu_launches": launches,
         "clocks": clk,
+        "guided": guided,
     }
+
+
+# WFPG options of the guided run (WFPGTracer.h:25-96; tConf_veach_product.json
+# values for the ones the config does not fix): leaf depth 10, field
+# 64^2 for the first two depths then 32^2, 16^2, 8^2 (WFPGTracer.cu:224-230)
+GUIDED_OPTS = dict(OPTS, OctreeLevel=10, MinRayBinLevel=5, BinRayCount=512,
+                   DoProductPathGuiding=1, GuideBounceAmount=512)
+GUIDED_FLOATS = {"BXDF-GuideMISRatio": 0.5, "RFieldFilterAlpha": 0.6}
+
+
+def _frames_image(t, frames: int) -> np.ndarray:
+    t.reset_image()
+    for _ in range(frames):
+        t.render_frame()
+    img = t.image()
+    return img[..., :3].astype(np.float64) / max(float(img[0, 0, 3]), 1.0)
+
+
+def run_guided(args, g, m, torch, dev: int) -> dict:
+    """The same frame with SVO path guiding, and the equal-time MSE of the
+    guided and plain tracers against a converged plain render
+    (Python/mse_hdr.py:36-44: mean over pixels and RGB of the squared
+    difference)."""
+    t = m.WFPGTracer(g.system, g)
+    t.set_options(dict(GUIDED_OPTS, Seed=101))
+    t.set_options(GUIDED_FLOATS)
+    stream = torch.cuda.ExternalStream(t.stream)
+    for _ in range(args.warmup):
+        t.render_frame()
+    torch.cuda.synchronize()
+    steps = max(10, args.steps // 5)
+    r0, _ = t.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        t.render_frame()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    r1, _ = t.stats()
+    guided_ms = ms / steps
+    out = {"metric": METRIC, "value": (r1 - r0) / (ms / 1e3) / 1e6, "unit": "Mrays/s",
+           "steps": steps, "ms_per_step": guided_ms,
+           "rays_per_step": (r1 - r0) / steps,
+           "launches_per_frame": t.launches_per_frame(),
+           "config": {"tracer": "WFPGTracer", **{k: v for k, v in GUIDED_OPTS.items()},
+                      **GUIDED_FLOATS,
+                      "field": "64x64 at depths 0-1, then 32x32, 16x16, 8x8",
+                      "leaf_radiance": "64-bit fixed-point sums (2^-24), FP16 averages"}}
+    if args.mse_budget_ms <= 0:
+        return out
+    # ---- equal-time MSE ----
+    p = m.PathTracer(g.system, g)
+    p.set_options(dict(OPTS, Seed=7))
+    for _ in range(2):
+        p.render_frame()
+    torch.cuda.synchronize()
+    pstream = torch.cuda.ExternalStream(p.stream)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(pstream)
+    for _ in range(20):
+        p.render_frame()
+    q1.record(pstream)
+    q1.synchronize()
+    plain_ms = q0.elapsed_time(q1) / 20
+    ref = m.PathTracer(g.system, g)
+    ref.set_options(dict(OPTS, Seed=99))
+    ref_img = _frames_image(ref, args.mse_reference_spp)
+    ref.close()
+    budget = float(args.mse_budget_ms)
+    plain_frames = max(1, int(budget / plain_ms))
+    guided_frames = max(1, int(budget / guided_ms))
+    plain_img = _frames_image(p, plain_frames)
+    gt = m.WFPGTracer(g.system, g)   # a cold cache: learning is part of the budget
+    gt.set_options(dict(GUIDED_OPTS, Seed=202))
+    gt.set_options(GUIDED_FLOATS)
+    guided_img = _frames_image(gt, guided_frames)
+    mse_p = float(np.mean((plain_img - ref_img) ** 2))
+    mse_g = float(np.mean((guided_img - ref_img) ** 2))
+    out["equal_time_mse"] = {
+        "budget_ms": budget, "reference_spp": args.mse_reference_spp,
+        "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "mse": mse_p},
+        "guided": {"frames": guided_frames, "ms_per_frame": guided_ms, "mse": mse_g},
+        "guided_over_plain": mse_g / mse_p if mse_p > 0 else None,
+        "note": "1 spp per frame at 1920x1080; the reference is a separate plain render "
+                "(different seed); the guided tracer starts with a cold octree"}
+    return out
 
 
 def _oracle_setup(scene):
@@ -326,6 +418,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traversal", type=int, default=1, choices=[0, 1],
                     help="1: 8-wide quantised BVH (default), 0: binary LBVH nodes")
+    ap.add_argument("--no-guided", dest="guided", action="store_false",
+                    help="skip the WFPG (SVO path guiding) run")
+    ap.add_argument("--mse-budget-ms", type=float, default=2000.0,
+                    help="equal-time MSE budget per tracer (0 skips the comparison)")
+    ap.add_argument("--mse-reference-spp", type=int, default=1024)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

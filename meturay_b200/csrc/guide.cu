@@ -202,6 +202,7 @@ struct GuideSmem {
     float origin[4];
     float jitter[2];
     uint32_t begin, end, key;
+    int nextTile;
 };
 
 // BxDFProjFunc of KCGenAndSampleDistributionProduct: cell centre of the
@@ -249,7 +250,7 @@ __device__ __forceinline__ float product_pdf(const GuideSmem<X>& S, int warp, fl
 }
 
 template <int X>
-__global__ void __launch_bounds__(kGuideTPB) k_guide(GuideArgs A) {
+__global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
     __shared__ GuideSmem<X> S;
     constexpr int DPP = X / 8;
     const float dppF = static_cast<float>(DPP);
@@ -318,15 +319,25 @@ __global__ void __launch_bounds__(kGuideTPB) k_guide(GuideArgs A) {
                                              A.opt.seedLo, A.opt.seedHi);
             S.jitter[0] = rj.u[0];
             S.jitter[1] = rj.u[1];
+            S.nextTile = 0;
         }
         __syncthreads();
-        // GenerateRadianceField: one cone per texel of the X*X map
+        // GenerateRadianceField: one cone per texel of the X*X map.  Warps
+        // take 8x4 texel tiles from a shared counter (neighbouring cones
+        // traverse similar nodes; fast warps take more tiles).
         {
             const V3 org = v3(S.origin[0], S.origin[1], S.origin[2]);
             const float tMin = S.origin[3];
             const float jx = S.jitter[0], jy = S.jitter[1];
-            for (int p = static_cast<int>(tid); p < X * X; p += kGuideTPB) {
-                const int x = p % X, y = p / X;
+            constexpr int kTiles = (X / 8) * (X / 4);
+            for (;;) {
+                int tile = 0;
+                if (lane == 0) tile = atomicAdd(&S.nextTile, 1);
+                tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+                if (tile >= kTiles) break;
+                const int x = (tile % (X / 8)) * 8 + static_cast<int>(lane & 7u);
+                const int y = (tile / (X / 8)) * 4 + static_cast<int>(lane >> 3);
+                const int p = y * X + x;
                 float s = (static_cast<float>(x) + jx) / static_cast<float>(X);
                 float t = (static_cast<float>(y) + jy) / static_cast<float>(X);
                 octa_wrap(s, t);
@@ -774,7 +785,7 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
     const uint32_t kernelIndex = iteration < 4 ? iteration : 4;
     switch (kernelIndex) {
         case 0:
-        case 1: k_guide<64><<<148 * 2, kGuideTPB, 0, st>>>(ga); break;
+        case 1: k_guide<64><<<148 * 3, kGuideTPB, 0, st>>>(ga); break;
         case 2: k_guide<32><<<148 * 4, kGuideTPB, 0, st>>>(ga); break;
         case 3: k_guide<16><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;
         default: k_guide<8><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;

@@ -377,6 +377,13 @@ __device__ __forceinline__ float neg_exp2i(uint32_t p) {  // 2^-p for p <= 126
     return (p == 0) ? 1.0f : bitsf((127u - p) << 23);
 }
 
+// The reference steps into an empty child, then on the next iteration
+// computes that child's exit, moves tMin past it and pops.  Here that pair
+// of iterations is one: the empty child's exit is computed in place.  The
+// corner moves by powers of two and stays exactly representable, so the
+// add/subtract pair of the reference changes nothing and the operations
+// that reach tMin are the same.  The voxel size test uses a per-level
+// table of the same products.
 __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, float tMin,
                                             float aperture, uint32_t maxQueryLevelOffset,
                                             bool& isLeaf, uint32_t& leafId) {
@@ -406,11 +413,18 @@ __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, f
         const float tSvo = fmaxf(fmaxf(t0.x, t0.y), t0.z);
         if (!(t0.x < tMin && t0.y < tMin && t0.z < tMin)) tMin = next_up(tSvo);
     }
+    // squared voxel size of each level (ConeDiameterSqr's comparand)
+    float vs2[11];
+#pragma unroll
+    for (int L = 0; L <= 10; L++) {
+        const uint32_t sh = (static_cast<uint32_t>(L) <= g.leafDepth) ? g.leafDepth - L : 0u;
+        const float vs = g.leafVoxelSize * static_cast<float>(1u << sh);
+        vs2[L] = vs * vs;
+    }
     uint64_t stack = 0;
     uint32_t depthBits = 0;
     uint32_t nodeId = 0;
     V3 corner = v3(0.0f, 0.0f, 0.0f);
-    bool emptyNode = false;
     for (uint32_t step = 0; nodeId != kSvoInvalidParent; step++) {
         if (step == kConeTraceMaxSteps) {
             leafId = kInvalid;
@@ -419,20 +433,9 @@ __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, f
         }
         const float childSpan = neg_exp2i(depthBits + 1);
         const float curSpan = neg_exp2i(depthBits);
-        const V3 center = corner + v3(childSpan, childSpan, childSpan);
         const V3 topRight = corner + v3(curSpan, curSpan, curSpan);
         const V3 tm = topRight * dc - pb;
         const float tMax = fminf(fminf(tm.x, tm.y), tm.z);
-        if (emptyNode) {
-            tMin = next_up(tMax);
-            const uint32_t b = uint32_t(stack & 7u);
-            corner = corner - v3((b & 1u) ? curSpan : 0.0f, (b & 2u) ? curSpan : 0.0f,
-                                 (b & 4u) ? curSpan : 0.0f);
-            stack >>= 3;
-            depthBits -= 1;
-            emptyNode = false;
-            continue;
-        }
         const uint64_t node = g.nodes[nodeId];
         if (tMax < tMin) {
             const uint32_t b = uint32_t(stack & 7u);
@@ -441,37 +444,40 @@ __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, f
             stack >>= 3;
             depthBits -= 1;
             nodeId = svo_parent(node);
-            emptyNode = false;
-        } else {
-            const V3 tc = center * dc - pb;
-            uint32_t childId = 0;
-            if (tc.x < tMin) childId |= 1u;
-            if (tc.y < tMin) childId |= 2u;
-            if (tc.z < tMin) childId |= 4u;
-            const uint32_t mir = childId ^ mirror;
-            const bool has = (svo_mask(node) >> mir) & 1u;
-            if (has) {
-                nodeId = svo_child_index(node) + svo_child_offset(node, mir);
-                const uint32_t level = depthBits + 1;
-                // ConeDiameterSqr (AnisoSVO.cuh:755-765) against the level's voxel size
-                const float area = tMin * tMin * aperture;
-                const float diam2 = 4.0f * (area * kInvPiF);
-                const float vs = level_voxel_size(g, level);
-                bool term = diam2 > vs * vs;
-                const bool childLeaf = svo_children_leaf(node);
-                term |= (g.leafDepth - level) <= maxQueryLevelOffset;
-                if (childLeaf || term) {
-                    isLeaf = childLeaf;
-                    leafId = nodeId;
-                    break;
-                }
-            }
-            emptyNode = !has;
-            corner = corner + v3((childId & 1u) ? childSpan : 0.0f, (childId & 2u) ? childSpan : 0.0f,
-                                 (childId & 4u) ? childSpan : 0.0f);
-            stack = (stack << 3) | childId;
-            depthBits += 1;
+            continue;
         }
+        const V3 center = corner + v3(childSpan, childSpan, childSpan);
+        const V3 tc = center * dc - pb;
+        uint32_t childId = 0;
+        if (tc.x < tMin) childId |= 1u;
+        if (tc.y < tMin) childId |= 2u;
+        if (tc.z < tMin) childId |= 4u;
+        const uint32_t mir = childId ^ mirror;
+        const V3 childCorner = corner + v3((childId & 1u) ? childSpan : 0.0f,
+                                           (childId & 2u) ? childSpan : 0.0f,
+                                           (childId & 4u) ? childSpan : 0.0f);
+        if (!((svo_mask(node) >> mir) & 1u)) {
+            // empty child: leave it at once
+            const V3 ctr = childCorner + v3(childSpan, childSpan, childSpan);
+            const V3 ct = ctr * dc - pb;
+            tMin = next_up(fminf(fminf(ct.x, ct.y), ct.z));
+            continue;
+        }
+        nodeId = svo_child_index(node) + svo_child_offset(node, mir);
+        const uint32_t level = depthBits + 1;
+        const float area = tMin * tMin * aperture;
+        const float diam2 = 4.0f * (area * kInvPiF);
+        bool term = diam2 > vs2[level];
+        const bool childLeaf = svo_children_leaf(node);
+        term |= (g.leafDepth - level) <= maxQueryLevelOffset;
+        if (childLeaf || term) {
+            isLeaf = childLeaf;
+            leafId = nodeId;
+            break;
+        }
+        corner = childCorner;
+        stack = (stack << 3) | childId;
+        depthBits += 1;
     }
     return tMin;
 }

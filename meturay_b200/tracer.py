@@ -71,7 +71,9 @@ class TracerSystem:
 
     def generate_tracer(self, scene: "GPUScene", tracer_type: str = "PathTracer",
                         options: dict | None = None) -> "PathTracer":
-        t = PathTracer(self, scene, tracer_type)
+        """GenerateTracer (TracerSystemI): "PathTracer" or "WFPGTracer"."""
+        t = WFPGTracer(self, scene) if tracer_type == "WFPGTracer" else \
+            PathTracer(self, scene, tracer_type)
         if options:
             t.set_options(options)
         return t
