@@ -171,6 +171,25 @@ int mrb_svo_export(const mrb_scene* scene, uint64_t* nodes, uint32_t* leaf_paren
 int mrb_svo_export_payload(const mrb_scene* scene, uint32_t* node_norm_spec, uint64_t* leaf_irr,
                            uint32_t* leaf_cnt, uint32_t* leaf_avg, uint32_t* node_avg);
 
+/* ---- scene JSON: TracerSystemI::GenerateScene's parse of an MRay scene
+ * file (GPUSceneJson.cpp:150-560, RayLib/SceneIO.cpp:78-226) for the hot
+ * path's subset: Pinhole cameras; Null and Primitive lights; Vacuum and
+ * IOR-only Homogeneous media; Identity and Single (matrix4x4 / trs)
+ * transforms, applied at load; Lambert, LambertC, Metal, Unreal, Refract
+ * materials with constant parameters; in-node triangles (".nodeTriangle",
+ * ".nodeTriangleIndexed") with "cullFace"; Surfaces, LightSurfaces,
+ * CameraSurfaces, BaseMedium, a Null BaseBoundaryLight.  // and block
+ * comments and trailing commas are accepted.  Anything else returns
+ * MRB_E_UNSUPPORTED naming it.  The description's arrays stay valid until
+ * mrb_json_scene_destroy; pass it to mrb_scene_create. */
+typedef struct mrb_json_scene mrb_json_scene;
+int mrb_json_scene_load(const char* json_text, size_t length, mrb_json_scene** out);
+int mrb_json_scene_load_file(const char* path, mrb_json_scene** out);
+void mrb_json_scene_destroy(mrb_json_scene* js);
+int mrb_json_scene_get(const mrb_json_scene* js, mrb_scene_desc* desc, uint32_t* camera_count);
+/* CameraSurfaces entry `index` as a pinhole camera (fov in radians). */
+int mrb_json_scene_camera(const mrb_json_scene* js, uint32_t index, mrb_camera* cam);
+
 /* ---- tracers: GPUTracerI (RayLib/GPUTracerI.h:24-71) ----
  * type "PathTracer" (PathTracer.cu) or "WFPGTracer" (WFPGTracer.cu, product
  * path guiding over the tracer's own voxel octree). */

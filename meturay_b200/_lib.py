@@ -64,6 +64,11 @@ def _load() -> C.CDLL:
         "mrb_svo_info": (i32, [vp, vp, vp]),
         "mrb_svo_export": (i32, [vp, vp, vp, vp, vp, vp, vp]),
         "mrb_svo_export_payload": (i32, [vp, vp, vp, vp, vp, vp]),
+        "mrb_json_scene_load": (i32, [C.c_char_p, sz, C.POINTER(vp)]),
+        "mrb_json_scene_load_file": (i32, [C.c_char_p, C.POINTER(vp)]),
+        "mrb_json_scene_destroy": (None, [vp]),
+        "mrb_json_scene_get": (i32, [vp, C.POINTER(SceneDesc), C.POINTER(u32)]),
+        "mrb_json_scene_camera": (i32, [vp, u32, C.POINTER(Camera)]),
         "mrb_tracer_set_option_float": (i32, [vp, C.c_char_p, C.c_double]),
         "mrb_tracer_svo_info": (i32, [vp, vp, vp]),
         "mrb_tracer_svo_export": (i32, [vp] + [vp] * 11),

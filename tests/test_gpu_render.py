@@ -133,3 +133,27 @@ def test_every_bxdf_with_and_without_mis(system, oracle, mis):
     assert rays == ref_rays
     assert gpu.sum() > 0
     assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
+
+
+def test_scene_file_renders_like_the_oracle(system, oracle):
+    """An MRay scene file (tests/scenes/box_mixed.json) through the loader,
+    the LBVH and the path tracer with MIS, against the oracle on the same
+    description."""
+    from pathlib import Path
+    import meturay_b200 as m
+    scene = m.load_scene(Path(__file__).resolve().parent / "scenes" / "box_mixed.json", 48, 36)
+    opts = dict(CORNELL_OPTS, DirectLightMIS=1, Seed=5)
+    g, t = _setup(system, scene, opts)
+    t.generate_work()
+    while t.render():
+        pass
+    t.finalize()
+    gpu = t.sample_radiance()[..., :3]
+    os_ = oracle.OracleScene(scene, g.export())
+    cf = np.concatenate([m.camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
+    ref, ref_rays = os_.render(cf, scene.width, scene.height, opts["Samples"], opts["MaxDepth"],
+                               opts["RussianRouletteStart"], True, opts["Seed"], mis=True)
+    rays, _ = t.stats()
+    assert rays == ref_rays
+    assert gpu.sum() > 0
+    assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL

@@ -179,3 +179,27 @@ def test_wfpg_skip_pg_is_unguided(system, oracle):
                                  **_oracle_kwargs(opts))
     assert _rel_mean_err(t.sample_radiance()[..., :3], ref) < REL_MEAN_TOL
     _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
+
+
+def test_wfpg_on_a_scene_file(system, oracle):
+    """WFPG frames of an MRay scene file (transformed light, Unreal, Metal,
+    Refract) match the oracle, image and octree."""
+    from pathlib import Path
+    import meturay_b200 as m
+    scene = m.load_scene(Path(__file__).resolve().parent / "scenes" / "box_mixed.json", 32, 24)
+    opts = dict(WFPG_OPTS, OctreeLevel=5, MinRayBinLevel=2, BinRayCount=32)
+    g, t = _wfpg(system, scene, opts)
+    o = oracle.OracleScene(scene, g.export())
+    svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
+    for frame in range(2):
+        t.generate_work()
+        while t.render():
+            pass
+        t.finalize()
+        ref, _, _, _ = o.render_wfpg(_cam(scene), scene.width, scene.height, 1, opts["MaxDepth"],
+                                     opts["RussianRouletteStart"], True, opts["Seed"], svo,
+                                     frame=frame, **_oracle_kwargs(opts))
+        gpu = t.sample_radiance()[..., :3]
+        assert gpu.sum() > 0
+        assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
+        _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
