@@ -190,6 +190,56 @@ int mrb_json_scene_get(const mrb_json_scene* js, mrb_scene_desc* desc, uint32_t*
 /* CameraSurfaces entry `index` as a pinhole camera (fov in radians). */
 int mrb_json_scene_camera(const mrb_json_scene* js, uint32_t index, mrb_camera* cam);
 
+/* ---- reconstruction filters: GPUReconFilterI (GPUReconFilterI.h:6-33) --
+ * replaces TracerSystemI::GenerateReconFilter (TracerSystemCUDA.cpp:109-137)
+ * and the "Box" / "Tent" / "Gaussian" / "Mitchell" filters
+ * (GPUReconFilterBox.h, ...Tent.h, ...Gaussian.h, ...Mitchell.h).
+ * Options as name/value pairs: Gaussian needs "alpha", Mitchell "b" and "c";
+ * a missing one returns MRB_E_ARG naming it.  radius in [0, 64] pixels;
+ * radius 0 is the Box filter's no-filter mode (one pixel, weight 1) and is
+ * rejected for the other types. */
+typedef struct mrb_recon_filter mrb_recon_filter;
+typedef struct mrb_image mrb_image;
+int mrb_recon_filter_create(const char* type, float radius, uint32_t option_count,
+                            const char* const* option_names, const float* option_values,
+                            mrb_recon_filter** out);
+void mrb_recon_filter_destroy(mrb_recon_filter* f);
+const char* mrb_recon_filter_type(const mrb_recon_filter* f);
+/* Device scratch the filter holds (GPUReconFilter::UsedGPUMemory). */
+size_t mrb_recon_filter_used_bytes(const mrb_recon_filter* f);
+/* FilterRadiusToPixelWH (GPUReconFilterKC.cuh:10-31). */
+uint32_t mrb_recon_filter_pixel_wh(float radius);
+/* The filter functor evaluated on the host (pixel centre, sample). */
+float mrb_recon_filter_weight(const mrb_recon_filter* f, float pixel_x, float pixel_y,
+                              float sample_x, float sample_y);
+/* FilterToImg (GPUReconFilter.h:59-260): splat sample_count samples
+ * (d_values: channels floats each, channels = the image's 1 or 4; d_img_coords:
+ * 2 floats each, image-space pixel units) into the image's pixels and sample
+ * counts, every weight times scalar_multiplier.  Each pixel adds its samples
+ * in ascending sample order.  Pixels outside the image's portion are not
+ * written.  Allocates scratch on first use or growth. */
+int mrb_recon_filter_to_img(mrb_recon_filter* f, mrb_image* img, const float* d_values,
+                            uint32_t channels, const float* d_img_coords, uint32_t sample_count,
+                            float scalar_multiplier, void* stream);
+
+/* ---- image memory: ImageMemory (ImageMemory.h:14-78) ----------------------
+ * Pixels (channels floats each, 1 = R_FLOAT, 4 = RGBA_FLOAT) and per-pixel
+ * sample counts (weight sums) of the image portion, zeroed at creation. */
+int mrb_image_create(int32_t width, int32_t height, uint32_t channels, mrb_image** out);
+void mrb_image_destroy(mrb_image* img);
+/* Reportion(start, end): end clamped to the resolution; reallocates, zeroed. */
+int mrb_image_reportion(mrb_image* img, int32_t start_x, int32_t start_y, int32_t end_x,
+                        int32_t end_y);
+/* Resize(resolution): the portion must still fit. */
+int mrb_image_resize(mrb_image* img, int32_t width, int32_t height);
+int mrb_image_reset(mrb_image* img, void* stream);
+/* info7: portion offset x, y, portion size w, h, resolution w, h, channels. */
+int mrb_image_info(const mrb_image* img, int32_t* info7);
+int mrb_image_device(const mrb_image* img, float** d_pixels, float** d_sample_counts);
+/* GetImageToCPU (ImageMemory.cu:150-190): NaN pixels set to 1e30 magenta,
+ * pixels and counts copied out, then the image reset.  Synchronises. */
+int mrb_image_get(mrb_image* img, float* host_pixels, float* host_counts, void* stream);
+
 /* ---- tracers: GPUTracerI (RayLib/GPUTracerI.h:24-71) ----
  * type "PathTracer" (PathTracer.cu) or "WFPGTracer" (WFPGTracer.cu, product
  * path guiding over the tracer's own voxel octree). */
@@ -229,8 +279,14 @@ int mrb_tracer_render(mrb_tracer* t);
 int mrb_tracer_finalize(mrb_tracer* t);
 /* GenerateWork + all Render steps + Finalize as one captured CUDA graph. */
 int mrb_tracer_render_frame(mrb_tracer* t);
-/* Per-pixel image (width*height*4: sum of per-frame means, frame count in
- * .w) and the last frame's per-sample radiance ((w*s)*(h*s)*4). */
+/* AttachReconFilter (RayTracer.cu:71-74): Finalize splats each frame's
+ * samples through a copy of the filter's functor (NULL detaches). */
+int mrb_tracer_set_filter(mrb_tracer* t, const mrb_recon_filter* f);
+/* Per-pixel image (width*height*4) and the last frame's per-sample radiance
+ * ((w*s)*(h*s)*4).  With a filter attached the image holds the filtered sums
+ * (rgb = sum of weight * radiance, .w = sum of weights); without one, the
+ * sum of per-frame per-pixel means with the frame count in .w.  Either way
+ * rgb / w is the pixel's estimate. */
 int mrb_tracer_get_image(mrb_tracer* t, float* host_rgba);
 int mrb_tracer_get_samples(mrb_tracer* t, float* host_rgba);
 int mrb_tracer_reset_image(mrb_tracer* t);

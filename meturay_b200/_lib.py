@@ -99,6 +99,23 @@ def _load() -> C.CDLL:
         "mrb_partition_temp_bytes": (sz, [u32, u32]),
         "mrb_partition": (i32, [vp, u32, u32, vp, vp, vp, vp, vp, vp, sz, vp]),
         "mrb_debug_math": (i32, [vp, u32, vp, vp, vp, vp]),
+        "mrb_recon_filter_create": (i32, [C.c_char_p, C.c_float, u32, C.POINTER(C.c_char_p),
+                                          C.POINTER(C.c_float), C.POINTER(vp)]),
+        "mrb_recon_filter_destroy": (None, [vp]),
+        "mrb_recon_filter_type": (C.c_char_p, [vp]),
+        "mrb_recon_filter_used_bytes": (sz, [vp]),
+        "mrb_recon_filter_pixel_wh": (u32, [C.c_float]),
+        "mrb_recon_filter_weight": (C.c_float, [vp] + [C.c_float] * 4),
+        "mrb_recon_filter_to_img": (i32, [vp, vp, vp, u32, vp, u32, C.c_float, vp]),
+        "mrb_image_create": (i32, [C.c_int32, C.c_int32, u32, C.POINTER(vp)]),
+        "mrb_image_destroy": (None, [vp]),
+        "mrb_image_reportion": (i32, [vp] + [C.c_int32] * 4),
+        "mrb_image_resize": (i32, [vp, C.c_int32, C.c_int32]),
+        "mrb_image_reset": (i32, [vp, vp]),
+        "mrb_image_info": (i32, [vp, vp]),
+        "mrb_image_device": (i32, [vp, C.POINTER(vp), C.POINTER(vp)]),
+        "mrb_image_get": (i32, [vp, vp, vp, vp]),
+        "mrb_tracer_set_filter": (i32, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

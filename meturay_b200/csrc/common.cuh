@@ -8,6 +8,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace mrb {
 
@@ -245,6 +246,43 @@ __device__ __forceinline__ float pm_atan2(float y, float x) {
     if (ay > ax) r = kPio2F - r;
     if (x < 0.0f) r = kPiF - r;
     return (y < 0.0f) ? -r : r;
+}
+
+// exp(x): Cody-Waite reduction x = k ln2 + r with ln2 split into a 16-bit
+// head (45426 / 2^16, so k * head is exact for |k| < 369) and the float
+// nearest the remainder; e^r from its Taylor series through r^8 / 8!
+// (|r| <= ln2 / 2, truncation below 2^-26); 2^k applied in two exact
+// power-of-two steps so results down to the subnormal range round once.
+__host__ __device__ __forceinline__ float pm_bits_float(int b) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(b);
+#else
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+__host__ __device__ __forceinline__ float pm_exp(float x) {
+    if (x != x) return x;
+    if (x > 88.72283f) return pm_bits_float(0x7F800000);
+    if (x < -103.97208f) return 0.0f;
+    const float kf = rintf(x * 0x1.715476p+0f);
+    const int k = static_cast<int>(kf);
+    float r = x - kf * 0x1.62e4p-1f;
+    r = r - kf * 0x1.7f7d1cp-20f;
+    float p = 0x1.a01a02p-16f;
+    p = p * r + 0x1.a01a02p-13f;
+    p = p * r + 0x1.6c16c2p-10f;
+    p = p * r + 0x1.111112p-7f;
+    p = p * r + 0x1.555556p-5f;
+    p = p * r + 0x1.555556p-3f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    // k in [-150, 128]: 2^k = 2^k1 * 2^k2 with both factors normal
+    const int k1 = k / 2, k2 = k - k1;
+    p = p * pm_bits_float((k1 + 127) << 23);
+    return p * pm_bits_float((k2 + 127) << 23);
 }
 
 // Quat::SLerp / Quat::BarySLerp (Quaternion.hpp:258-318)

@@ -27,6 +27,7 @@
 #include "wide.cuh"
 #include "svo.cuh"
 #include "guide.cuh"
+#include "recon.cuh"
 
 namespace mrb {
 
@@ -314,6 +315,10 @@ struct mrb_tracer {
         guideSort, guideScan, guideBuf, payloadBackup;
     size_t guideSortBytes = 0;
     uint32_t chainPaths = 0, chainLevels = 0;
+    // reconstruction filter (AttachReconFilter); image coordinates per sample
+    bool hasFilter = false;
+    ReconFilterDev filter{};
+    DBuf imgCoords;
     // graph
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
@@ -357,6 +362,7 @@ int ensure_buffers(mrb_tracer* t) {
     if ((r = t->sortedIds.alloc(size_t(maxRays) * 4))) return r;
     if ((r = t->portion.alloc(32 * 4))) return r;
     if ((r = t->samplesBuf.alloc(size_t(paths) * 16))) return r;
+    if (t->hasFilter && (r = t->imgCoords.alloc(size_t(paths) * 8))) return r;
     if ((r = t->image.alloc(size_t(t->width) * t->height * 16))) return r;
     if ((r = t->counters.alloc(16))) return r;
     if ((r = t->frameWord.alloc(4))) return r;
@@ -477,7 +483,8 @@ int step_camera(mrb_tracer* t) {
     return camera_generate(t->devCam.as<CameraDev>(), path_options(t), t->scene->baseMedium,
                            t->rayO[0].as<float4>(),
                            t->rayD[0].as<float4>(), t->aux[0].as<RayAux>(),
-                           t->samplesBuf.as<float4>(), cnt, path_chain(t), t->stream);
+                           t->samplesBuf.as<float4>(), cnt, path_chain(t),
+                           t->hasFilter ? t->imgCoords.as<float2>() : nullptr, t->stream);
 }
 
 struct StageTimer {
@@ -568,7 +575,12 @@ int step_finalize(mrb_tracer* t) {
         if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream))) return r;
         if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
     }
-    r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
+    if (t->hasFilter)
+        r = recon_filter_grid(t->filter, t->samplesBuf.as<float4>(), t->imgCoords.as<float2>(),
+                              t->width, t->height, t->samples, 1.0f, t->image.as<float4>(),
+                              t->stream);
+    else
+        r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
                     t->image.as<float4>(), t->stream);
     if (r) return r;
     return frame_advance(t->frameWord.as<uint32_t>(), t->stream);
@@ -1363,6 +1375,23 @@ int mrb_tracer_get_samples(mrb_tracer* t, float* host) {
 int mrb_tracer_reset_image(mrb_tracer* t) {
     if (!t) return MRB_E_ARG;
     if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+    return 0;
+}
+
+int mrb_tracer_set_filter(mrb_tracer* t, const mrb_recon_filter* f) {
+    if (!t) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    t->hasFilter = f != nullptr;
+    if (f) t->filter = *recon_filter_dev(f);
+    // the camera kernel writes one coordinate pair per sample from now on
+    if (t->hasFilter && t->maxRays) {
+        int r = t->imgCoords.alloc(size_t(t->maxRays / 2) * 8);
+        if (r) return r;
+    }
+    // the image's .w changes meaning (weight sum vs frame count): start over
+    if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+    t->graphDirty = true;
     return 0;
 }
 

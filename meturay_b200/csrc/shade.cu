@@ -14,6 +14,8 @@
 //                  Refract BxDFs; outputs are compacted with warp-aggregated
 //                  atomics into the next wavefront
 //   k_resolve      per-pixel mean of its s*s samples, accumulated per frame
+//                  (with no reconstruction filter attached; recon.cu splats
+//                  through the filter otherwise)
 #include "common.cuh"
 #include "bxdf.cuh"
 #include "shade.cuh"
@@ -30,7 +32,8 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
                                                 RayAux* __restrict__ aux,
                                                 float4* __restrict__ samples,
                                                 uint32_t* __restrict__ count, uint32_t total,
-                                                PathChain chain) {
+                                                PathChain chain,
+                                                float2* __restrict__ imgCoords) {
     const uint32_t SW = opt.width * opt.samples, SH = opt.height * opt.samples;
     const uint32_t frame = *opt.frame;
     const CameraDev cam = *camPtr;
@@ -64,6 +67,15 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
         a.pad = 0;
         aux[sid] = a;
         samples[sid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // image-space coordinates for the reconstruction filter
+        // (GPUCameraPinhole::GenerateRay localCoords * resolution,
+        // GenerationKernels.cuh:62-88)
+        if (imgCoords) {
+            const float lx = (static_cast<float>(sx) + rc.u[0]) / static_cast<float>(SW);
+            const float ly = (static_cast<float>(sy) + rc.u[1]) / static_cast<float>(SH);
+            imgCoords[sid] = make_float2(lx * static_cast<float>(opt.width),
+                                         ly * static_cast<float>(opt.height));
+        }
         if (opt.wfpg) {
             chain.nodeA[sid] = make_float4(cam.position[0], cam.position[1], cam.position[2],
                                            __uint_as_float(frame));
@@ -427,10 +439,11 @@ inline uint32_t grid_for(uint32_t n, uint32_t block, uint32_t cap) {
 
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
                     float4* rayO, float4* rayD, RayAux* aux, float4* samples, uint32_t* count,
-                    const PathChain& chain, cudaStream_t stream) {
+                    const PathChain& chain, float2* imgCoords, cudaStream_t stream) {
     const uint32_t total = opt.width * opt.samples * opt.height * opt.samples;
     k_camera<<<grid_for(total, 256, 148 * 16), 256, 0, stream>>>(cam, opt, baseMedium, rayO, rayD,
-                                                                aux, samples, count, total, chain);
+                                                                aux, samples, count, total, chain,
+                                                                imgCoords);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

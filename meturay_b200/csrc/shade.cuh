@@ -36,7 +36,7 @@ struct PathChain {
 
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
                     float4* rayO, float4* rayD, RayAux* aux, float4* samples, uint32_t* count,
-                    const PathChain& chain, cudaStream_t stream);
+                    const PathChain& chain, float2* imgCoords, cudaStream_t stream);
 int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount, uint32_t idBits,
                uint32_t* dense, const PortionTable& table, cudaStream_t stream);
 int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t maxCount,

@@ -69,6 +69,11 @@ class TracerSystem:
     def generate_scene(self, scene: Scene) -> "GPUScene":
         return GPUScene(self, scene)
 
+    def generate_recon_filter(self, filter_options: dict):
+        """GenerateReconFilter (TracerSystemCUDA.cpp:109-137): {"type", "radius", ...}."""
+        from .recon import ReconFilter
+        return ReconFilter.from_options(filter_options)
+
     def generate_tracer(self, scene: "GPUScene", tracer_type: str = "PathTracer",
                         options: dict | None = None) -> "PathTracer":
         """GenerateTracer (TracerSystemI): "PathTracer" or "WFPGTracer"."""
@@ -276,6 +281,12 @@ class PathTracer:
     def set_camera(self, cam: dict):
         c = make_camera(cam)
         check(lib.mrb_tracer_set_camera(self._h, C.byref(c)))
+
+    def attach_recon_filter(self, recon_filter):
+        """AttachReconFilter: Finalize splats through the filter (None detaches).
+        The image restarts; afterwards .w holds the weight sums."""
+        check(lib.mrb_tracer_set_filter(self._h, recon_filter._h if recon_filter else None))
+        self.recon_filter = recon_filter
 
     def generate_work(self, camera_index: int = 0):
         check(lib.mrb_tracer_generate_work(self._h, int(camera_index)))

@@ -2957,6 +2957,23 @@ uint64_t oracle_render(const oracle_scene* s, const oracle_bvh* b, const oracle_
                        const oracle_options* opt, float* out) {
     return render<float>(s, b, cam, opt, out);
 }
+
+// Image-space sample coordinates: GPUCameraPinhole::GenerateRay's
+// localCoords = (sampleId + offset) / sampleMax (GPUCameraPinhole.cuh:236),
+// times the resolution (GenerationKernels.cuh:72), with the camera ray's
+// own jitter.
+void oracle_camera_img_coords(const oracle_options* opt, float* out) {
+    const uint32_t SW = opt->width * opt->samples, SH = opt->height * opt->samples;
+    const uint32_t total = SW * SH;
+    for (uint32_t sid = 0; sid < total; sid++) {
+        const uint32_t sx = sid % SW, sy = sid / SW;
+        const Rng4 rc = rng_block(sid, opt->frame, kTagCamera, 0, opt->seed_lo, opt->seed_hi);
+        const float lx = (static_cast<float>(sx) + rc.u[0]) / static_cast<float>(SW);
+        const float ly = (static_cast<float>(sy) + rc.u[1]) / static_cast<float>(SH);
+        out[2 * sid] = lx * static_cast<float>(opt->width);
+        out[2 * sid + 1] = ly * static_cast<float>(opt->height);
+    }
+}
 uint64_t oracle_render_f64(const oracle_scene* s, const oracle_bvh* b, const oracle_camera* cam,
                            const oracle_options* opt, double* out) {
     return render<double>(s, b, cam, opt, out);

@@ -201,6 +201,30 @@ int  oracle_intersect_tri(const float* ro, const float* rd, const float* p0,
                           const float* p1, const float* p2, int cull,
                           float* t, float* bary3);
 
+/* ---- reconstruction filters (oracle/recon.cpp) ----
+ * type 0 Box, 1 Tent, 2 Gaussian (alpha), 3 Mitchell (b, c). */
+typedef struct oracle_filter {
+    uint32_t type;
+    float radius, alpha, b, c;
+} oracle_filter;
+uint32_t oracle_filter_pixel_wh(float radius);
+void oracle_exp(const float* x, uint32_t n, float* out);
+float oracle_filter_weight(const oracle_filter* f, float px, float py, float sx, float sy);
+/* FilterToImg: values (channels 1 or 4 per sample), coords (2 per sample);
+ * pixels (segW*segH*channels) and counts (segW*segH) are added to. */
+void oracle_filter_to_img(const oracle_filter* f, const float* values, uint32_t channels,
+                          const float* coords, uint32_t n, int32_t resW, int32_t resH,
+                          int32_t offX, int32_t offY, int32_t segW, int32_t segH,
+                          float multiplier, float* pixels, float* counts);
+/* The reference test's direct CPU expectation (RGBA, whole image). */
+void oracle_filter_direct(const oracle_filter* f, const float* values, const float* coords,
+                          uint32_t n, int32_t resW, int32_t resH, float* pixels, float* counts);
+/* The reference test's mt19937 sample coordinates (2 floats per sample). */
+void oracle_mt19937_coords(uint32_t n, int32_t width, int32_t height, uint32_t seed, float* out);
+/* Image coordinates of the camera samples of one iteration (2 per sample):
+ * ((s + jitter) / samples across) * resolution per axis. */
+void oracle_camera_img_coords(const oracle_options* opt, float* out);
+
 #ifdef __cplusplus
 }
 #endif

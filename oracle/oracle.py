@@ -405,3 +405,96 @@ def svo_build(scene, tri_key: np.ndarray, extent: np.ndarray, resolution: int) -
                        _p(out["tri_voxels"]), _p(out["params"]))
     lib.oracle_svo_destroy(C.c_void_p(h))
     return out
+
+
+# ---- reconstruction filters (oracle/recon.cpp) ----------------------------
+FILTER_TYPES = {"Box": 0, "Tent": 1, "Gaussian": 2, "Mitchell": 3}
+
+
+class Filter(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("radius", C.c_float), ("alpha", C.c_float),
+                ("b", C.c_float), ("c", C.c_float)]
+
+
+def _filter(ftype: str, radius: float, alpha: float = 0.0, b: float = 0.0, c: float = 0.0):
+    return Filter(FILTER_TYPES[ftype], radius, alpha, b, c)
+
+
+lib.oracle_filter_pixel_wh.restype = C.c_uint32
+lib.oracle_filter_pixel_wh.argtypes = [C.c_float]
+lib.oracle_filter_weight.restype = C.c_float
+lib.oracle_filter_weight.argtypes = [C.POINTER(Filter)] + [C.c_float] * 4
+lib.oracle_filter_to_img.argtypes = [C.POINTER(Filter), C.c_void_p, C.c_uint32, C.c_void_p,
+                                     C.c_uint32] + [C.c_int32] * 6 + [C.c_float, C.c_void_p,
+                                                                      C.c_void_p]
+lib.oracle_filter_direct.argtypes = [C.POINTER(Filter), C.c_void_p, C.c_void_p, C.c_uint32,
+                                     C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+lib.oracle_mt19937_coords.argtypes = [C.c_uint32, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p]
+lib.oracle_camera_img_coords.argtypes = [C.POINTER(Options), C.c_void_p]
+lib.oracle_exp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+
+
+def pexp(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros_like(x)
+    lib.oracle_exp(_p(x), x.size, _p(out))
+    return out
+
+
+def filter_pixel_wh(radius: float) -> int:
+    return int(lib.oracle_filter_pixel_wh(radius))
+
+
+def filter_weight(ftype: str, radius: float, px, py, sx, sy, **params) -> float:
+    f = _filter(ftype, radius, **params)
+    return float(lib.oracle_filter_weight(C.byref(f), px, py, sx, sy))
+
+
+def filter_to_img(ftype: str, radius: float, values: np.ndarray, coords: np.ndarray,
+                  resolution, segment=None, multiplier: float = 1.0, pixels=None, counts=None,
+                  **params):
+    """FilterToImg on the CPU.  values: (n,) or (n, 4); coords: (n, 2).
+    segment: (offX, offY, w, h), default the whole image.  Returns the
+    image portion's (pixels, counts), added onto the given arrays if any."""
+    f = _filter(ftype, radius, **params)
+    values = np.ascontiguousarray(values, np.float32)
+    coords = np.ascontiguousarray(coords, np.float32)
+    ch = 1 if values.ndim == 1 else values.shape[1]
+    W, H = resolution
+    ox, oy, sw, sh = segment if segment is not None else (0, 0, W, H)
+    if pixels is None:
+        pixels = np.zeros((sh, sw, ch) if ch > 1 else (sh, sw), np.float32)
+    if counts is None:
+        counts = np.zeros((sh, sw), np.float32)
+    lib.oracle_filter_to_img(C.byref(f), _p(values), ch, _p(coords), coords.shape[0], W, H, ox, oy,
+                             sw, sh, multiplier, _p(pixels), _p(counts))
+    return pixels, counts
+
+
+def filter_direct(ftype: str, radius: float, values: np.ndarray, coords: np.ndarray, resolution,
+                  **params):
+    """The reference test's own direct CPU splat (RGBA, whole image)."""
+    f = _filter(ftype, radius, **params)
+    values = np.ascontiguousarray(values, np.float32)
+    coords = np.ascontiguousarray(coords, np.float32)
+    W, H = resolution
+    pixels = np.zeros((H, W, 4), np.float32)
+    counts = np.zeros((H, W), np.float32)
+    lib.oracle_filter_direct(C.byref(f), _p(values), _p(coords), coords.shape[0], W, H,
+                             _p(pixels), _p(counts))
+    return pixels, counts
+
+
+def mt19937_coords(n: int, width: int, height: int, seed: int = 0) -> np.ndarray:
+    out = np.zeros((n, 2), np.float32)
+    lib.oracle_mt19937_coords(n, width, height, seed, _p(out))
+    return out
+
+
+def camera_img_coords(width: int, height: int, samples: int, seed: int, frame: int) -> np.ndarray:
+    o = Options()
+    o.width, o.height, o.samples = width, height, samples
+    o.seed_lo, o.seed_hi, o.frame = seed & 0xFFFFFFFF, seed >> 32, frame
+    out = np.zeros((width * samples * height * samples, 2), np.float32)
+    lib.oracle_camera_img_coords(C.byref(o), _p(out))
+    return out
