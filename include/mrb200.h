@@ -239,6 +239,25 @@ int mrb_image_device(const mrb_image* img, float** d_pixels, float** d_sample_co
 /* GetImageToCPU (ImageMemory.cu:150-190): NaN pixels set to 1e30 magenta,
  * pixels and counts copied out, then the image reset.  Synchronises. */
 int mrb_image_get(mrb_image* img, float* host_pixels, float* host_counts, void* stream);
+/* Pixels divided by their sample counts, to a .exr (FLOAT) or .pfm file. */
+int mrb_image_write(mrb_image* img, const char* path);
+
+/* ---- image files (the headless stand-in for ImageIO's EXR writer,
+ * ImageIO/ImageIO.cpp:290-360) ----------------------------------------------
+ * pixels: width*height*channels floats, rows bottom to top as the tracers
+ * produce them (EXR files store the top row first, so rows are flipped on
+ * write and read).  channels 1, 3 or 4.  OpenEXR: single-part scanline,
+ * uncompressed, FLOAT or HALF (half != 0) channels R,G,B(,A) or Y.  PFM:
+ * "PF" RGB (the alpha of 4-channel input dropped) or "Pf" grey, little
+ * endian. */
+int mrb_write_exr(const char* path, const float* pixels, uint32_t width, uint32_t height,
+                  uint32_t channels, int half);
+int mrb_write_pfm(const char* path, const float* pixels, uint32_t width, uint32_t height,
+                  uint32_t channels);
+/* Read a .exr (uncompressed scanline) or .pfm file.  pixels == NULL returns
+ * the size only; otherwise capacity must hold width*height*channels floats. */
+int mrb_read_image(const char* path, float* pixels, size_t capacity, uint32_t* width,
+                   uint32_t* height, uint32_t* channels);
 
 /* ---- tracers: GPUTracerI (RayLib/GPUTracerI.h:24-71) ----
  * type "PathTracer" (PathTracer.cu) or "WFPGTracer" (WFPGTracer.cu, product
@@ -254,6 +273,22 @@ void mrb_tracer_destroy(mrb_tracer* t);
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
 /* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha". */
 int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double value);
+/* String WFPG options (WFPGTracer.h:39,54): "InitialSVO" -- path of an
+ * octree dump that the next GenerateWork loads instead of building the
+ * octree (empty: build); "PGDataStructDumpName" -- file name of the periodic
+ * dumps (default "wfpg_svo").  The integer options "PGDumpDataStruct" (0/1)
+ * and "PGDataStructDumpIntervalExp" (default 2) switch the dumps on: after
+ * the frames numbered interval^0, interval^1, ... the octree is written to
+ * "<frame>_<name>" (WFPGTracer.cu:1733-1745). */
+int mrb_tracer_set_option_string(mrb_tracer* t, const char* name, const char* value);
+/* The WFPG octree in DumpSVOAsBinary's byte layout (AnisoSVO.cu:1555-1697).
+ * out == NULL returns the size only.  Builds the octree if it does not
+ * exist yet. */
+int mrb_tracer_svo_dump(mrb_tracer* t, void* out, size_t capacity, size_t* size);
+/* Replace the WFPG octree with a dump (Constrcut(data), AnisoSVO.cu:
+ * 1190-1413).  Structure indices are range-checked before upload; a dump
+ * that fails a check returns MRB_E_ARG naming it. */
+int mrb_tracer_svo_load(mrb_tracer* t, const void* data, size_t size);
 /* The WFPG tracer's octree (built at first use): info/params as
  * mrb_svo_info, and its structure plus payload as mrb_svo_export and
  * mrb_svo_export_payload.  NULL skips. */
@@ -290,6 +325,8 @@ int mrb_tracer_set_filter(mrb_tracer* t, const mrb_recon_filter* f);
 int mrb_tracer_get_image(mrb_tracer* t, float* host_rgba);
 int mrb_tracer_get_samples(mrb_tracer* t, float* host_rgba);
 int mrb_tracer_reset_image(mrb_tracer* t);
+/* The image's per-pixel estimate (rgb / w) as a .exr (FLOAT RGB) or .pfm file. */
+int mrb_tracer_write_image(mrb_tracer* t, const char* path);
 /* Rays traced (camera + path + NEE, summed over depths) since creation. */
 int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays_traced, uint32_t* frames);
 /* Stream the tracer launches on (cudaStream_t as void*). */

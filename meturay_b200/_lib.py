@@ -116,6 +116,15 @@ def _load() -> C.CDLL:
         "mrb_image_device": (i32, [vp, C.POINTER(vp), C.POINTER(vp)]),
         "mrb_image_get": (i32, [vp, vp, vp, vp]),
         "mrb_tracer_set_filter": (i32, [vp, vp]),
+        "mrb_tracer_set_option_string": (i32, [vp, C.c_char_p, C.c_char_p]),
+        "mrb_tracer_svo_dump": (i32, [vp, vp, sz, C.POINTER(sz)]),
+        "mrb_tracer_svo_load": (i32, [vp, vp, sz]),
+        "mrb_tracer_write_image": (i32, [vp, C.c_char_p]),
+        "mrb_image_write": (i32, [vp, C.c_char_p]),
+        "mrb_write_exr": (i32, [C.c_char_p, vp, u32, u32, u32, i32]),
+        "mrb_write_pfm": (i32, [C.c_char_p, vp, u32, u32, u32]),
+        "mrb_read_image": (i32, [C.c_char_p, vp, sz, C.POINTER(u32), C.POINTER(u32),
+                                 C.POINTER(u32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -18,6 +18,7 @@
 // own CPU expectation (Test_TracerCUDA/T_ReconFilter.cu:96-140).
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "../../include/mrb200.h"
 #include "recon.cuh"
@@ -653,3 +654,16 @@ int mrb_image_get(mrb_image* img, float* host_pixels, float* host_counts, void* 
 }
 
 }  // extern "C"
+
+#include "io.cuh"
+
+extern "C" int mrb_image_write(mrb_image* img, const char* path) {
+    if (!img || !path) return MRB_E_ARG;
+    const size_t pix = img->pixel_count();
+    if (pix == 0) return MRB_E_ARG;
+    std::vector<float> px(pix * img->channels), cnt(pix);
+    MRB_CUDA(cudaMemcpy(px.data(), img->pixels, px.size() * 4, cudaMemcpyDeviceToHost));
+    MRB_CUDA(cudaMemcpy(cnt.data(), img->counts, cnt.size() * 4, cudaMemcpyDeviceToHost));
+    return mrb::write_averaged(path, px.data(), cnt.data(), 1, static_cast<uint32_t>(img->w),
+                               static_cast<uint32_t>(img->h), img->channels, img->channels);
+}

@@ -28,6 +28,7 @@
 #include "svo.cuh"
 #include "guide.cuh"
 #include "recon.cuh"
+#include "io.cuh"
 
 namespace mrb {
 
@@ -303,11 +304,18 @@ struct mrb_tracer {
     uint32_t depth = 0;
     bool working = false;
     uint32_t frames = 0;
+    uint32_t frameStart = 0;  // "Frame": RNG iteration of the next frame
     // WFPG tracer (WFPGTracer.h:58-96 defaults)
     bool wfpg = false;
     uint32_t octreeLevel = 10, minRayBinLevel = 5, binRayCount = 512, productPG = 1, purePG = 0,
              skipPG = 0, guideBounce = 512, omitDirect = 0;
     float misRatio = 0.5f, filterAlpha = 1.0f;
+    // octree files: "InitialSVO" replaces the build with a dump; with
+    // "PGDumpDataStruct" the octree is dumped after the frames numbered
+    // interval^0, interval^1, ... ("PGDataStructDumpIntervalExp") to
+    // "<frame>_<PGDataStructDumpName>" (WFPGTracer.cu:1289-1309,1733-1745)
+    std::string initialSvo, dumpName = "wfpg_svo";
+    uint32_t dumpEnabled = 0, dumpInterval = 2, iterationCount = 0, treeDumpCount = 0;
     bool svoReady = false;
     SvoParams svoP{};
     SvoResult svo;
@@ -391,7 +399,9 @@ int ensure_buffers(mrb_tracer* t) {
     MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->counters.p, 0, 16, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->errorFlags.p, 0, 16, t->stream));
-    MRB_CUDA(cudaMemsetAsync(t->frameWord.p, 0, 4, t->stream));
+    MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &t->frameStart, 4, cudaMemcpyHostToDevice,
+                             t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
     t->graphDirty = true;
     return 0;
 }
@@ -450,6 +460,24 @@ int ensure_svo(mrb_tracer* t) {
     float ext[8];
     MRB_CUDA(cudaMemcpyAsync(ext, sc->aExtent.p, 24, cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaStreamSynchronize(t->stream));
+    if (!t->initialSvo.empty()) {
+        // Constrcut(data) (AnisoSVO.cu:1190-1413): the dump replaces the build
+        FILE* f = std::fopen(t->initialSvo.c_str(), "rb");
+        if (!f) {
+            set_error("InitialSVO: cannot open %s", t->initialSvo.c_str());
+            return MRB_E_ARG;
+        }
+        std::vector<uint8_t> data;
+        uint8_t buf[1 << 16];
+        size_t got;
+        while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0) data.insert(data.end(), buf, buf + got);
+        std::fclose(f);
+        int r = svo_load(data.data(), data.size(), t->svoP, t->svo, t->stream);
+        if (r) return r;
+        t->svoReady = true;
+        t->graphDirty = true;
+        return 0;
+    }
     t->svoP = svo_params(ext, 1u << t->octreeLevel);
     SvoBuildIn in{sc->T, sc->dPos.as<float>(), sc->dIdx.as<uint32_t>(), sc->dKey.as<uint32_t>(),
                   sc->dLightRad.as<float>(), t->omitDirect};
@@ -611,6 +639,34 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
     return n;
 }
 
+// WFPGTracer::Finalize's frame count and periodic octree dump
+// (WFPGTracer.cu:1703,1733-1745): dumps after frames interval^k, k = 0, 1, ...
+int wfpg_after_frame(mrb_tracer* t) {
+    if (!t->wfpg) return 0;
+    t->iterationCount++;
+    if (!t->dumpEnabled) return 0;
+    uint64_t due = 1;
+    for (uint32_t k = 0; k < t->treeDumpCount && due <= 0xFFFFFFFFull; k++) due *= t->dumpInterval;
+    if (due != t->iterationCount) return 0;
+    std::vector<uint8_t> data;
+    int r = svo_dump(t->svo, t->svoP, data, t->stream);
+    if (r) return r;
+    // "<frame>_<name>", the frame number in front of the file name itself
+    const size_t slash = t->dumpName.find_last_of('/');
+    const std::string dir = slash == std::string::npos ? "" : t->dumpName.substr(0, slash + 1);
+    const std::string base = slash == std::string::npos ? t->dumpName : t->dumpName.substr(slash + 1);
+    const std::string path = dir + std::to_string(t->iterationCount) + "_" + base;
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f || std::fwrite(data.data(), 1, data.size(), f) != data.size()) {
+        if (f) std::fclose(f);
+        set_error("octree dump: cannot write %s", path.c_str());
+        return MRB_E_ARG;
+    }
+    std::fclose(f);
+    t->treeDumpCount++;
+    return 0;
+}
+
 int check_device_errors(mrb_tracer* t) {
     uint32_t e[3] = {0, 0, 0};
     MRB_CUDA(cudaMemcpyAsync(e, t->errorFlags.p, 4, cudaMemcpyDeviceToHost, t->stream));
@@ -629,6 +685,10 @@ int check_device_errors(mrb_tracer* t) {
 
 int svo_copy(void* dst, const void* src, size_t bytes) {
     if (!dst || !bytes) return 0;
+    if (!src) {  // arrays a loaded dump does not carry (leaf codes, light keys)
+        std::memset(dst, 0, bytes);
+        return 0;
+    }
     MRB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
     return 0;
 }
@@ -1176,14 +1236,19 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
         t->skipPG = v ? 1 : 0;
     } else if (t->wfpg && k == "GuideBounceAmount") {
         t->guideBounce = uint32_t(v);
+    } else if (t->wfpg && k == "PGDumpDataStruct") {
+        t->dumpEnabled = v ? 1 : 0;
+        return 0;
+    } else if (t->wfpg && k == "PGDataStructDumpIntervalExp") {
+        t->dumpInterval = uint32_t(v);
+        return 0;
     } else if (k == "Frame") {
+        // applied now, or when the buffers are first allocated
+        t->frameStart = uint32_t(v);
         if (t->frameWord.p) {
-            uint32_t f = uint32_t(v);
-            MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f, 4, cudaMemcpyHostToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &t->frameStart, 4, cudaMemcpyHostToDevice,
+                                     t->stream));
             MRB_CUDA(cudaStreamSynchronize(t->stream));
-        } else {
-            set_error("set the resolution before the frame");
-            return MRB_E_STATE;
         }
         return 0;
     } else {
@@ -1286,7 +1351,8 @@ int mrb_tracer_finalize(mrb_tracer* t) {
     if (r) return r;
     t->working = false;
     t->frames++;
-    return check_device_errors(t);
+    if ((r = check_device_errors(t))) return r;
+    return wfpg_after_frame(t);
 }
 
 int mrb_tracer_render_frame(mrb_tracer* t) {
@@ -1353,7 +1419,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
     }
     MRB_CUDA(cudaGraphLaunch(t->graph, t->stream));
     t->frames++;
-    return 0;
+    return wfpg_after_frame(t);
 }
 
 int mrb_tracer_get_image(mrb_tracer* t, float* host) {
@@ -1376,6 +1442,76 @@ int mrb_tracer_reset_image(mrb_tracer* t) {
     if (!t) return MRB_E_ARG;
     if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
     return 0;
+}
+
+int mrb_tracer_set_option_string(mrb_tracer* t, const char* name, const char* value) {
+    if (!t || !name || !value) return MRB_E_ARG;
+    const std::string k(name);
+    if (t->wfpg && k == "InitialSVO") {
+        t->initialSvo = value;
+        // the next GenerateWork builds (empty path) or loads the octree
+        if (t->svoReady) {
+            if (set_device(t->sys)) return MRB_E_CUDA;
+            MRB_CUDA(cudaStreamSynchronize(t->stream));
+            svo_free(t->svo);
+            t->svoReady = false;
+        }
+        t->graphDirty = true;
+        return 0;
+    }
+    if (t->wfpg && k == "PGDataStructDumpName") {
+        if (!*value) {
+            set_error("PGDataStructDumpName must not be empty");
+            return MRB_E_ARG;
+        }
+        t->dumpName = value;
+        return 0;
+    }
+    set_error("unknown string option '%s'", name);
+    return MRB_E_ARG;
+}
+
+int mrb_tracer_svo_dump(mrb_tracer* t, void* out, size_t capacity, size_t* size) {
+    if (!t || !t->wfpg || !size) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_svo(t);
+    if (r) return r;
+    *size = svo_dump_size(t->svo.nodeCount, t->svo.leafCount,
+                          static_cast<uint32_t>(t->svo.levelOffsets.size()));
+    if (!out) return 0;
+    if (capacity < *size) {
+        set_error("octree dump: %zu bytes needed, %zu given", *size, capacity);
+        return MRB_E_ARG;
+    }
+    std::vector<uint8_t> data;
+    if ((r = svo_dump(t->svo, t->svoP, data, t->stream))) return r;
+    std::memcpy(out, data.data(), data.size());
+    return 0;
+}
+
+int mrb_tracer_svo_load(mrb_tracer* t, const void* data, size_t size) {
+    if (!t || !t->wfpg || !data) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    SvoParams P{};
+    SvoResult v{};
+    int r = svo_load(static_cast<const uint8_t*>(data), size, P, v, t->stream);
+    if (r) return r;
+    if (t->svoReady) svo_free(t->svo);
+    t->svo = v;
+    t->svoP = P;
+    t->svoReady = true;
+    t->graphDirty = true;
+    return 0;
+}
+
+int mrb_tracer_write_image(mrb_tracer* t, const char* path) {
+    if (!t || !path || !t->image.p) return MRB_E_ARG;
+    std::vector<float> img(size_t(t->width) * t->height * 4);
+    int r = mrb_tracer_get_image(t, img.data());
+    if (r) return r;
+    // rgb / w: the per-pixel estimate whether w counts frames or weights
+    return write_averaged(path, img.data(), img.data() + 3, 4, t->width, t->height, 4, 3);
 }
 
 int mrb_tracer_set_filter(mrb_tracer* t, const mrb_recon_filter* f) {

@@ -138,6 +138,10 @@ class ImageMemory:
         check(lib.mrb_image_device(self._h, C.byref(p), C.byref(c)))
         return int(p.value or 0), int(c.value or 0)
 
+    def write(self, path):
+        """Pixels / sample counts as .exr (FLOAT) or .pfm."""
+        check(lib.mrb_image_write(self._h, str(path).encode()))
+
     def get_image(self, stream: int | None = None) -> tuple[np.ndarray, np.ndarray]:
         """GetImageToCPU: (pixels (h, w[, 4]), counts (h, w)); resets the image."""
         i = self.info()

@@ -282,6 +282,10 @@ class PathTracer:
         c = make_camera(cam)
         check(lib.mrb_tracer_set_camera(self._h, C.byref(c)))
 
+    def write_image(self, path):
+        """The image's estimate (rgb / w) as .exr or .pfm."""
+        check(lib.mrb_tracer_write_image(self._h, str(path).encode()))
+
     def attach_recon_filter(self, recon_filter):
         """AttachReconFilter: Finalize splats through the filter (None detaches).
         The image restarts; afterwards .w holds the weight sums."""
@@ -349,18 +353,35 @@ class WFPGTracer(PathTracer):
 
     OPTION_KEYS = PathTracer.OPTION_KEYS + (
         "OctreeLevel", "MinRayBinLevel", "BinRayCount", "DoProductPathGuiding", "PurePG",
-        "SkipPG", "GuideBounceAmount", "OmitDirectRadiance")
+        "SkipPG", "GuideBounceAmount", "OmitDirectRadiance", "PGDumpDataStruct",
+        "PGDataStructDumpIntervalExp")
     FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha")
+    STRING_KEYS = ("InitialSVO", "PGDataStructDumpName")
 
     def __init__(self, system: TracerSystem, scene: GPUScene):
         super().__init__(system, scene, "WFPGTracer")
 
     def set_options(self, opts: dict):
-        ints = {k: v for k, v in opts.items() if k not in self.FLOAT_KEYS}
+        ints = {k: v for k, v in opts.items()
+                if k not in self.FLOAT_KEYS and k not in self.STRING_KEYS}
         super().set_options(ints)
         for k, v in opts.items():
             if k in self.FLOAT_KEYS:
                 check(lib.mrb_tracer_set_option_float(self._h, k.encode(), float(v)))
+            elif k in self.STRING_KEYS:
+                check(lib.mrb_tracer_set_option_string(self._h, k.encode(), str(v).encode()))
+
+    def dump_svo(self) -> bytes:
+        """DumpSVOAsBinary: the octree and its radiance state as bytes."""
+        n = C.c_size_t()
+        check(lib.mrb_tracer_svo_dump(self._h, None, 0, C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        check(lib.mrb_tracer_svo_dump(self._h, buf, n.value, C.byref(n)))
+        return bytes(buf)
+
+    def load_svo(self, data: bytes):
+        """Constrcut(data): replace the octree with a dump."""
+        check(lib.mrb_tracer_svo_load(self._h, data, len(data)))
 
     def export_svo(self) -> dict:
         """The tracer's octree with its current radiance state."""

@@ -498,3 +498,43 @@ def camera_img_coords(width: int, height: int, samples: int, seed: int, frame: i
     out = np.zeros((width * samples * height * samples, 2), np.float32)
     lib.oracle_camera_img_coords(C.byref(o), _p(out))
     return out
+
+
+# ---- octree dump layout (DumpSVOAsBinary, AnisoSVO.cu:1555-1697) ----------
+def _u64_to_f32_rne(v: int) -> np.float32:
+    """uint64 -> float32 with one round-to-nearest-even step."""
+    if v < (1 << 24):
+        return np.float32(v)
+    shift = v.bit_length() - 24
+    m, rem = v >> shift, v & ((1 << shift) - 1)
+    half = 1 << (shift - 1)
+    if rem > half or (rem == half and (m & 1)):
+        m += 1
+    return np.float32(np.ldexp(np.float64(m), shift))
+
+
+def svo_dump_bytes(ex: dict, node_bin16=None, leaf_bin16=None) -> bytes:
+    """The dump of an exported octree (tracer.export_svo()), restated from
+    the reference's layout: 48-byte header, tree arrays, then the payload
+    with FP32 sums (2^-24 fixed point here), FP32 averages (half pairs here)
+    and zero guiding factors."""
+    N, U = ex["nodes_count"], ex["leaves"]
+    lv = ex["level_offsets"].astype(np.uint32)
+    nb = np.zeros(N, np.uint16) if node_bin16 is None else np.asarray(node_bin16, np.uint16)
+    lb = np.zeros(U, np.uint16) if leaf_bin16 is None else np.asarray(leaf_bin16, np.uint16)
+
+    def halves(words):
+        w = np.asarray(words, np.uint32)
+        pairs = np.stack([w & 0xFFFF, w >> 16], 1).astype(np.uint16)
+        return pairs.view(np.float16).astype(np.float32)
+
+    irr = np.array([_u64_to_f32_rne(int(v)) for v in ex["leaf_irr"].ravel()],
+                   np.float32) * np.float32(2.0 ** -24)
+    parts = [np.asarray(ex["lo"], np.float32), np.asarray(ex["hi"], np.float32),
+             np.array([ex["resolution"], ex["depth"], N, U], np.uint32),
+             np.array([ex["leaf_size"]], np.float32), np.array([lv.size], np.uint32),
+             ex["nodes"].astype(np.uint64), nb, ex["leaf_parents"].astype(np.uint32), lb, lv,
+             halves(ex["node_avg"]), ex["node_normals"].astype(np.uint32), np.zeros(N, np.uint8),
+             irr.astype(np.float32), ex["leaf_cnt"].astype(np.uint32), halves(ex["leaf_avg"]),
+             ex["leaf_normals"].astype(np.uint32), np.zeros(U, np.uint8)]
+    return b"".join(np.ascontiguousarray(p).tobytes() for p in parts)
