@@ -4,8 +4,10 @@ of both against a converged plain render (the "guided" object of the line).
 
 Workload ("clusters-1M"): 1000 Gaussian clusters x 1000 triangles (seed 1),
 1920x1080, 1 sample per pixel per step ("Samples": 1), depth 8, NEE on,
-Russian roulette from depth 3.  One step = one frame: camera rays + 8
-trace/partition/shade depths + resolve, replayed from a captured CUDA graph.
+Russian roulette from depth 3, samples splatted through a Tent filter of
+radius 1 pixel (the reference's tracer configurations).  One step = one
+frame: camera rays + 8 trace/partition/shade depths + the filter splat,
+replayed from a captured CUDA graph.
 Rays traced = camera + path + NEE rays entering the traversal, summed over
 depths (the reference's "rays entering HitRays").
 
@@ -37,11 +39,18 @@ METRIC = "Mrays/s"
 WORKLOAD = {"workload": "clusters-1M plain path tracing", "triangles": 1000004,
             "resolution": "1920x1080", "spp_per_step": 1, "max_depth": 8,
             "nee": True, "rr_start": 3, "scene_seed": 1,
+            "recon_filter": "Tent, radius 1 pixel (the reference's tConf filter)",
             "l2": "inputs larger than L2 (ray/hit buffers ~470 MB, BVH ~180 MB)"}
 # committed ncu summaries of the traversal kernel, per traversal mode
 TRACE_PROFILE = {0: "k_trace_clusters1M_bvh2.md", 1: "k_trace_wide_clusters1M.md"}
 OPTS = {"Samples": 1, "MaxDepth": 8, "NextEventEstimation": 1, "RussianRouletteStart": 3,
         "DirectLightMIS": 0}
+# FilterOptions of the reference's tracer configurations (tConf_veach_*.json)
+RECON = {"type": "Tent", "radius": 1.0}
+
+
+def _attach_filter(system, t):
+    t.attach_recon_filter(system.generate_recon_filter(RECON))
 
 
 def _traffic_per_launch(traversal):
@@ -123,13 +132,16 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    scene = m.scenes.clusters(seed=1)
+    scene = m.scenes.clusters(seed=1, width=args.res[0], height=args.res[1])
     system = m.TracerSystem(dev)
     g = m.GPUScene(system, scene)
     g.construct_accelerators()
     g.set_traversal(args.traversal)
+    if args.only == "guided":
+        return run_guided(args, g, m, torch, dev)
     t = m.PathTracer(system, g)
     t.set_options(dict(OPTS, Seed=1 + rank))
+    _attach_filter(system, t)
     stream = torch.cuda.ExternalStream(t.stream)
 
     for _ in range(args.warmup):
@@ -181,8 +193,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     # ---- roofline of the traversal kernel (one stepwise profiled frame) ----
     prof = t.profile_frame()
     launches = t.launches_per_frame() * args.steps
-    guided = run_guided(args, g, m, torch, dev) if (args.guided and rank == 0 and world == 1) \
-        else None
+    guided = run_guided(args, g, m, torch, dev) \
+        if (args.guided and args.only == "all" and rank == 0 and world == 1) else None
 
     if dist:
         tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
@@ -221,6 +233,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "config": dict(WORKLOAD, parallelism=f"replicas{world}",
                        traversal="8-wide quantised BVH" if args.traversal else "binary LBVH"),
         "rays_per_step": rays / args.steps / world,
+        "mpaths_per_s": scene.width * scene.height * world * args.steps / ms / 1e3,
         "e2e": {"value": e2e_rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
                 "h2d_bytes_per_step": cam_bytes, "d2h_bytes_per_step": img_bytes},
         "roofline": {"bound": "hbm",
@@ -250,11 +263,13 @@ GUIDED_FLOATS = {"BXDF-GuideMISRatio": 0.5, "RFieldFilterAlpha": 0.6}
 
 
 def _frames_image(t, frames: int) -> np.ndarray:
+    """rgb / w after `frames` frames (w: the filter's weight sum per pixel)."""
     t.reset_image()
     for _ in range(frames):
         t.render_frame()
-    img = t.image()
-    return img[..., :3].astype(np.float64) / max(float(img[0, 0, 3]), 1.0)
+    img = t.image().astype(np.float64)
+    w = img[..., 3:]
+    return np.where(w > 0, img[..., :3] / np.where(w > 0, w, 1.0), 0.0)
 
 
 def run_guided(args, g, m, torch, dev: int) -> dict:
@@ -265,6 +280,7 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     t = m.WFPGTracer(g.system, g)
     t.set_options(dict(GUIDED_OPTS, Seed=101))
     t.set_options(GUIDED_FLOATS)
+    _attach_filter(g.system, t)
     stream = torch.cuda.ExternalStream(t.stream)
     for _ in range(args.warmup):
         t.render_frame()
@@ -293,6 +309,7 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     # ---- equal-time MSE ----
     p = m.PathTracer(g.system, g)
     p.set_options(dict(OPTS, Seed=7))
+    _attach_filter(g.system, p)
     for _ in range(2):
         p.render_frame()
     torch.cuda.synchronize()
@@ -306,6 +323,7 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     plain_ms = q0.elapsed_time(q1) / 20
     ref = m.PathTracer(g.system, g)
     ref.set_options(dict(OPTS, Seed=99))
+    _attach_filter(g.system, ref)
     ref_img = _frames_image(ref, args.mse_reference_spp)
     ref.close()
     budget = float(args.mse_budget_ms)
@@ -315,6 +333,7 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     gt = m.WFPGTracer(g.system, g)   # a cold cache: learning is part of the budget
     gt.set_options(dict(GUIDED_OPTS, Seed=202))
     gt.set_options(GUIDED_FLOATS)
+    _attach_filter(g.system, gt)
     guided_img = _frames_image(gt, guided_frames)
     mse_p = float(np.mean((plain_img - ref_img) ** 2))
     mse_g = float(np.mean((guided_img - ref_img) ** 2))
@@ -423,7 +442,12 @@ def main():
     ap.add_argument("--mse-budget-ms", type=float, default=2000.0,
                     help="equal-time MSE budget per tracer (0 skips the comparison)")
     ap.add_argument("--mse-reference-spp", type=int, default=1024)
+    ap.add_argument("--only", choices=["all", "guided"], default="all",
+                    help="guided: only the WFPG timing (for profiling a small case)")
+    ap.add_argument("--res", default="1920x1080",
+                    help="image size WxH (the workload is 1920x1080; smaller for profiling)")
     args = ap.parse_args()
+    args.res = tuple(int(v) for v in args.res.lower().split("x"))
     if args.warmup < 3:
         args.warmup = 3
 
@@ -442,7 +466,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     out = run_ours(args, rank, world, dist)
-    if out is not None and not args.no_cpu_baseline:
+    if out is not None and not args.no_cpu_baseline and args.only == "all":
         import meturay_b200.scenes as scenes
         scene = scenes.clusters(seed=1)
         os_ = _oracle_setup(scene)
