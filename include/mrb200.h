@@ -339,6 +339,52 @@ int mrb_tracer_launches_per_frame(mrb_tracer* t);
  * depths.  The frame counts like any other. */
 int mrb_tracer_profile_frame(mrb_tracer* t, float* stage_ms, uint64_t* work);
 
+/* ---- wavefront pool: continuous batching of render jobs ----------------
+ * (no counterpart in the reference: MRay renders one scene per tracer.)
+ * Jobs of different scenes, resolutions and sample counts share one
+ * device-resident wavefront: every iteration generates one frame of each
+ * admitted job (as many as `capacity` camera samples hold, round robin),
+ * traces all their rays in one traversal launch per depth, shades them in
+ * one launch and resolves each job's frame into its own image.  Jobs are
+ * admitted first come first served while their images fit the HBM budget
+ * (hbm_budget 0: the free memory at creation minus the pool's buffers and a
+ * 10 % reserve).  A job renders the same samples alone and in any mix: its
+ * random numbers are keyed by its own sample index, frame and seed.  The
+ * pool's iteration is one captured CUDA graph. */
+typedef struct mrb_pool mrb_pool;
+typedef struct mrb_pool_job {
+    mrb_camera camera;
+    uint32_t width, height;
+    uint32_t samples;        /* "Samples": s -> s*s per pixel per frame */
+    uint32_t frames;         /* frames to render (spp = frames * s*s) */
+    uint32_t max_depth, rr_start, nee, mis;
+    uint64_t seed;
+} mrb_pool_job;
+#define MRB_JOB_QUEUED 0
+#define MRB_JOB_ACTIVE 1
+#define MRB_JOB_DONE 2
+/* capacity: camera samples per iteration (the wavefront holds 2 rays per
+ * sample); max_depth: depths per iteration, the bound of every job's. */
+int mrb_pool_create(mrb_system* sys, uint32_t capacity, uint32_t max_depth, size_t hbm_budget,
+                    mrb_pool** out);
+void mrb_pool_destroy(mrb_pool* pool);
+/* Traversal launch shape: block 64/128/256 threads, stack 64/128 entries. */
+int mrb_pool_set_launch(mrb_pool* pool, int trace_block, int trace_stack);
+/* Queue a job (the scene's accelerator must be built; the scene must stay
+ * alive until the job is done).  One frame must fit the capacity. */
+int mrb_pool_submit(mrb_pool* pool, mrb_scene* scene, const mrb_pool_job* job, uint64_t* job_id);
+/* Admit what fits, run one iteration (synchronous).  Outputs: jobs that
+ * finished in this iteration, jobs active and queued afterwards. */
+int mrb_pool_step(mrb_pool* pool, uint32_t* finished, uint32_t* active, uint32_t* queued);
+int mrb_pool_job_status(mrb_pool* pool, uint64_t job_id, uint32_t* state, uint32_t* frames_done);
+/* A done job's image (width*height*4: sum of per-frame means, frame count
+ * in .w); release != 0 frees it and forgets the job. */
+int mrb_pool_job_image(mrb_pool* pool, uint64_t job_id, float* host_rgba, int release);
+/* Rays traced, iterations run, HBM held by admitted jobs and the budget. */
+int mrb_pool_stats(mrb_pool* pool, uint64_t* rays, uint64_t* iterations, size_t* hbm_used,
+                   size_t* hbm_budget);
+void* mrb_pool_stream(mrb_pool* pool);
+
 /* ---- kernel-level entry points (device pointers) ---------------------- */
 /* KCGenerateAABBs + extent reduce + KCGenMortonCodes
  * (LinearBVH.hpp:102-166,444-482). */

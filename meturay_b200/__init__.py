@@ -13,7 +13,9 @@ from . import scenes  # noqa: F401
 from .scene_json import load_scene, load_scene_text, load_tracer_config  # noqa: F401
 from .recon import ImageMemory, ReconFilter, filter_pixel_wh  # noqa: F401
 from . import imageio  # noqa: F401
+from .pool import Job, WavefrontPool  # noqa: F401
 
 __all__ = ["TracerSystem", "GPUScene", "PathTracer", "WFPGTracer", "MrbError", "scenes",
            "camera_frame", "load_scene", "load_scene_text", "load_tracer_config",
-           "ReconFilter", "ImageMemory", "filter_pixel_wh", "imageio"]
+           "ReconFilter", "ImageMemory", "filter_pixel_wh", "imageio",
+           "WavefrontPool", "Job"]

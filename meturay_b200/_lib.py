@@ -39,6 +39,13 @@ class Camera(C.Structure):
                 ("near_far", C.c_float * 2), ("fov", C.c_float * 2)]
 
 
+class PoolJob(C.Structure):
+    _fields_ = [("camera", Camera), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("samples", C.c_uint32), ("frames", C.c_uint32), ("max_depth", C.c_uint32),
+                ("rr_start", C.c_uint32), ("nee", C.c_uint32), ("mis", C.c_uint32),
+                ("seed", C.c_uint64)]
+
+
 def _load() -> C.CDLL:
     if not _LIB_PATH.exists():
         raise ImportError(
@@ -117,6 +124,16 @@ def _load() -> C.CDLL:
         "mrb_image_get": (i32, [vp, vp, vp, vp]),
         "mrb_tracer_set_filter": (i32, [vp, vp]),
         "mrb_tracer_set_option_string": (i32, [vp, C.c_char_p, C.c_char_p]),
+        "mrb_pool_create": (i32, [vp, u32, u32, sz, C.POINTER(vp)]),
+        "mrb_pool_destroy": (None, [vp]),
+        "mrb_pool_set_launch": (i32, [vp, i32, i32]),
+        "mrb_pool_submit": (i32, [vp, vp, C.POINTER(PoolJob), C.POINTER(u64)]),
+        "mrb_pool_step": (i32, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]),
+        "mrb_pool_job_status": (i32, [vp, u64, C.POINTER(u32), C.POINTER(u32)]),
+        "mrb_pool_job_image": (i32, [vp, u64, vp, i32]),
+        "mrb_pool_stats": (i32, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(sz),
+                                 C.POINTER(sz)]),
+        "mrb_pool_stream": (vp, [vp]),
         "mrb_tracer_svo_dump": (i32, [vp, vp, sz, C.POINTER(sz)]),
         "mrb_tracer_svo_load": (i32, [vp, vp, sz]),
         "mrb_tracer_write_image": (i32, [vp, C.c_char_p]),

@@ -20,10 +20,30 @@
 #include "bxdf.cuh"
 #include "shade.cuh"
 #include "svo_dev.cuh"
+#include "pool.cuh"
 
 namespace mrb {
 
 namespace {
+
+// GPUCameraPinhole::GenerateRay for sample (sx, sy) of an SW x SH sample grid
+// (GPUCameraPinhole.cuh:209-243); the tracer and the pool share it.
+__device__ __forceinline__ void camera_ray(const CameraDev& cam, uint32_t sx, uint32_t sy,
+                                           uint32_t SW, uint32_t SH, const Rand4& rc,
+                                           float4& o, float4& d) {
+    float dx = cam.planeSize[0] / static_cast<float>(SW);
+    float dy = cam.planeSize[1] / static_cast<float>(SH);
+    float sdx = static_cast<float>(sx) * dx;
+    float sdy = static_cast<float>(sy) * dy;
+    sdx += rc.u[0] * dx;
+    sdy += rc.u[1] * dy;
+    V3 sp = {cam.bottomLeft[0] + ((sdx * cam.right[0]) + (sdy * cam.up[0])),
+             cam.bottomLeft[1] + ((sdx * cam.right[1]) + (sdy * cam.up[1])),
+             cam.bottomLeft[2] + ((sdx * cam.right[2]) + (sdy * cam.up[2]))};
+    V3 dir = normalize(sp - ld3(cam.position));
+    o = make_float4(cam.position[0], cam.position[1], cam.position[2], cam.nearFar[0]);
+    d = make_float4(dir.x, dir.y, dir.z, cam.nearFar[1]);
+}
 
 __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ camPtr,
                                                 PathOptions opt, uint32_t baseMedium,
@@ -42,18 +62,7 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
          sid += gridDim.x * blockDim.x) {
         const uint32_t sx = sid % SW, sy = sid / SW;
         Rand4 rc = philox_uniform4(sid, frame, kTagCamera, 0u, opt.seedLo, opt.seedHi);
-        float dx = cam.planeSize[0] / static_cast<float>(SW);
-        float dy = cam.planeSize[1] / static_cast<float>(SH);
-        float sdx = static_cast<float>(sx) * dx;
-        float sdy = static_cast<float>(sy) * dy;
-        sdx += rc.u[0] * dx;
-        sdy += rc.u[1] * dy;
-        V3 sp = {cam.bottomLeft[0] + ((sdx * cam.right[0]) + (sdy * cam.up[0])),
-                 cam.bottomLeft[1] + ((sdx * cam.right[1]) + (sdy * cam.up[1])),
-                 cam.bottomLeft[2] + ((sdx * cam.right[2]) + (sdy * cam.up[2]))};
-        V3 dir = normalize(sp - ld3(cam.position));
-        rayO[sid] = make_float4(cam.position[0], cam.position[1], cam.position[2], cam.nearFar[0]);
-        rayD[sid] = make_float4(dir.x, dir.y, dir.z, cam.nearFar[1]);
+        camera_ray(cam, sx, sy, SW, SH, rc, rayO[sid], rayD[sid]);
         RayAux a;
         a.rf[0] = a.rf[1] = a.rf[2] = 1.0f;
         a.sample = sid;
@@ -143,6 +152,7 @@ struct ShadeArgs {
     uint32_t* outCount;
     PathChain chain;     // WFPG only
     const uint2* guide;  // WFPG guided directions of this wavefront, or null
+    const JobDev* jobs;  // wavefront pool: the job table (null for one tracer)
 };
 
 __device__ __forceinline__ void accumulate(float4* samples, uint32_t s, V3 v) {
@@ -152,10 +162,12 @@ __device__ __forceinline__ void accumulate(float4* samples, uint32_t s, V3 v) {
     atomicAdd(p + 2, v.z);
 }
 
+// kMulti: rays of a wavefront pool; scene, options, frame and the RNG
+// sample index come from each ray's job (pool.cuh).
+template <bool kMulti>
 __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
     const uint32_t n = *A.nonNull;
-    const uint32_t frame = *A.opt.frame;
-    const SceneDev& s = A.sc;
+    const uint32_t tracerFrame = kMulti ? 0u : *A.opt.frame;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t ltMask = (1u << lane) - 1u;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -169,14 +181,24 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
             const uint32_t batch = key >> kIdBits, id = key & kIdMask;
             const float4 rd = A.rayD[rid];
             const RayAux aux = A.aux[rid];
+            const JobDev* job = kMulti ? A.jobs + aux.pad : nullptr;
+            const SceneDev& s = kMulti ? job->sc : A.sc;
+            const uint32_t frame = kMulti ? job->frame : tracerFrame;
+            const uint32_t oNee = kMulti ? job->nee : A.opt.nee;
+            const uint32_t oMis = kMulti ? job->mis : A.opt.mis;
+            const uint32_t oRr = kMulti ? job->rrStart : A.opt.rrStart;
+            const uint32_t oSeedLo = kMulti ? job->seedLo : A.opt.seedLo;
+            const uint32_t oSeedHi = kMulti ? job->seedHi : A.opt.seedHi;
+            const uint32_t rngSample = kMulti ? aux.sample - job->sampleBase : aux.sample;
+            const bool gen = kMulti ? (uint32_t(aux.depth) + 1u < job->maxDepth) : (A.gen != 0);
             if (batch == kBatchLight) {
                 // PathTracerBoundaryWork (PathTracerKC.cuh:335-426)
-                const bool pathAsMis = A.opt.mis && aux.type == kPathRay;
+                const bool pathAsMis = oMis && aux.type == kPathRay;
                 const bool camera = aux.type == kCameraRay;
                 const bool specPath = aux.type == kSpecPathRay;
-                const bool neeOn = A.opt.nee && aux.type == kNeeRay;
+                const bool neeOn = oNee && aux.type == kNeeRay;
                 const bool pathNeeOff =
-                    (!A.opt.nee) && (aux.type == kPathRay || aux.type == kSpecPathRay);
+                    (!oNee) && (aux.type == kPathRay || aux.type == kSpecPathRay);
                 const bool correct = neeOn && (aux.endpoint == id);
                 float misWeight = 1.0f;
                 if (pathAsMis) {
@@ -215,7 +237,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                             make_float4(total.x, total.y, total.z, 0.0f);
                     }
                 }
-            } else if (aux.type != kNeeRay && (A.gen || A.opt.wfpg)) {
+            } else if (aux.type != kNeeRay && (gen || A.opt.wfpg)) {
                 // PathTracerPathWork (PathTracerKC.cuh:428-649)
                 const uint32_t prim = A.hit.prim[rid];
                 const float2 hb = A.hit.bary[rid];
@@ -243,13 +265,13 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                 }
                 // the last step's outputs are never traced; WFPG still keeps its
                 // chain vertex (WorkRays runs at every depth, WFPGTracer.cu:1590-1697)
-                if (A.gen) {
-                const Rand4 ra = philox_uniform4(aux.sample, frame, aux.depth, 0u,
-                                                 A.opt.seedLo, A.opt.seedHi);
-                const Rand4 rb = philox_uniform4(aux.sample, frame, aux.depth, 1u,
-                                                 A.opt.seedLo, A.opt.seedHi);
+                if (gen) {
+                const Rand4 ra = philox_uniform4(rngSample, frame, aux.depth, 0u,
+                                                 oSeedLo, oSeedHi);
+                const Rand4 rb = philox_uniform4(rngSample, frame, aux.depth, 1u,
+                                                 oSeedLo, oSeedHi);
                 // ---- NEE: GPULightSamplerUniform::SampleLight + primitive light
-                if (A.opt.nee && !specular && s.lightCount > 0) {
+                if (oNee && !specular && s.lightCount > 0) {
                     const uint32_t lc = s.lightCount;
                     float r1 = ra.u[0] * static_cast<float>(lc);
                     uint32_t li = static_cast<uint32_t>(r1);
@@ -284,21 +306,21 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                     float pdfBxdf;
                     if (batch == kBatchLambert) {
                         refl = lambert_eval(ld3(s.lambertAlbedo + 3 * id), ldir, sf);
-                        pdfBxdf = A.opt.mis ? lambert_pdf(ldir, sf) : 0.0f;
+                        pdfBxdf = oMis ? lambert_pdf(ldir, sf) : 0.0f;
                     } else if (batch == kBatchLambertC) {
                         refl = lambertc_eval(ld3(s.lambertCAlbedo + 3 * id), ldir, sf);
-                        pdfBxdf = A.opt.mis ? lambert_pdf(ldir, sf) : 0.0f;
+                        pdfBxdf = oMis ? lambert_pdf(ldir, sf) : 0.0f;
                     } else if (batch == kBatchUnreal) {
                         const UnrealP up = unreal_params(s.unrealParams + 6 * id);
                         refl = unreal_eval(up, ldir, wi, sf);
-                        pdfBxdf = A.opt.mis ? unreal_pdf(up, ldir, wi, sf) : 0.0f;
+                        pdfBxdf = oMis ? unreal_pdf(up, ldir, wi, sf) : 0.0f;
                     } else {
                         const MetalP mp = metal_params(s.metalParams + 10 * id);
                         refl = metal_eval(mp, ldir, wi, sf);
-                        pdfBxdf = A.opt.mis ? metal_pdf(mp, ldir, wi, sf) : 0.0f;
+                        pdfBxdf = oMis ? metal_pdf(mp, ldir, wi, sf) : 0.0f;
                     }
                     float pdfNee = lpdf;
-                    if (A.opt.mis) {
+                    if (oMis) {
                         pdfNee /= power_heuristic(lpdf, pdfBxdf);
                         if (isnan(pdfNee)) pdfNee = 0.0f;
                     }
@@ -357,7 +379,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                 prf = (bs.pdf == 0.0f) ? v3(0.0f, 0.0f, 0.0f) : (prf / bs.pdf);
                 const float avg = dot(prf, v3(0.333f, 0.333f, 0.333f));
                 bool term = false;
-                if (!specular && aux.depth > A.opt.rrStart) {
+                if (!specular && aux.depth > oRr) {
                     // TracerFunctions::RussianRoulette (TracerFunctions.cuh:320-331)
                     const float prob = fminf(fmaxf(avg, 0.005f), 1.0f);
                     if (ra.u[3] >= prob) term = true;
@@ -376,7 +398,7 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                     pathAux.prevPDF = bs.pdf;
                     pathAux.depth = static_cast<uint8_t>(aux.depth + 1);
                 }
-                }  // A.gen
+                }  // gen
             }
         }
         // warp-aggregated compaction of the outputs into the next wavefront
@@ -435,6 +457,85 @@ inline uint32_t grid_for(uint32_t n, uint32_t block, uint32_t cap) {
     return g < cap ? (g ? g : 1) : cap;
 }
 
+
+// Largest j < n with base[j] <= g (base ascending, base[0] = 0).
+__device__ __forceinline__ uint32_t job_of(const uint32_t* base, uint32_t n, uint32_t g) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (base[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Camera rays of every job of a pool iteration: slot g belongs to the job
+// whose sample range holds it, and is that job's sample g - sampleBase.
+__global__ void __launch_bounds__(256) k_pool_camera(const PoolHeader* __restrict__ hdr,
+                                                     const JobDev* __restrict__ jobs,
+                                                     float4* __restrict__ rayO,
+                                                     float4* __restrict__ rayD,
+                                                     RayAux* __restrict__ aux,
+                                                     float4* __restrict__ samples,
+                                                     uint32_t* __restrict__ count) {
+    __shared__ uint32_t sBase[kPoolMaxJobs];
+    const uint32_t nj = hdr->jobs, total = hdr->samples;
+    for (uint32_t j = threadIdx.x; j < nj; j += blockDim.x) sBase[j] = jobs[j].sampleBase;
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = total;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+         g += gridDim.x * blockDim.x) {
+        const uint32_t j = job_of(sBase, nj, g);
+        const JobDev& J = jobs[j];
+        const uint32_t sid = g - J.sampleBase;
+        const uint32_t SW = J.width * J.samples, SH = J.height * J.samples;
+        const uint32_t sx = sid % SW, sy = sid / SW;
+        const Rand4 rc = philox_uniform4(sid, J.frame, kTagCamera, 0u, J.seedLo, J.seedHi);
+        camera_ray(J.cam, sx, sy, SW, SH, rc, rayO[g], rayD[g]);
+        RayAux a;
+        a.rf[0] = a.rf[1] = a.rf[2] = 1.0f;
+        a.sample = g;
+        a.endpoint = kInvalid;
+        a.medium = static_cast<uint16_t>(J.sc.baseMedium);
+        a.depth = 0;
+        a.type = kCameraRay;
+        a.prevPDF = __int_as_float(0x7fc00000);
+        a.pad = j;
+        aux[g] = a;
+        samples[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// k_resolve over every job's image: per pixel the mean of its s*s samples
+// is added to the job's image, the frame counted in .w.
+__global__ void __launch_bounds__(256) k_pool_resolve(const PoolHeader* __restrict__ hdr,
+                                                      const JobDev* __restrict__ jobs,
+                                                      const float4* __restrict__ samples) {
+    __shared__ uint32_t sBase[kPoolMaxJobs];
+    const uint32_t nj = hdr->jobs, total = hdr->pixels;
+    for (uint32_t j = threadIdx.x; j < nj; j += blockDim.x) sBase[j] = jobs[j].pixelBase;
+    __syncthreads();
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+         g += gridDim.x * blockDim.x) {
+        const JobDev& J = jobs[job_of(sBase, nj, g)];
+        const uint32_t p = g - J.pixelBase;
+        const uint32_t sp = J.samples, SW = J.width * sp;
+        const uint32_t px = p % J.width, py = p / J.width;
+        const float inv = 1.0f / static_cast<float>(sp * sp);
+        const float4* base = samples + J.sampleBase;
+        float r = 0.0f, gg = 0.0f, b = 0.0f;
+        for (uint32_t j = 0; j < sp; j++)
+            for (uint32_t i = 0; i < sp; i++) {
+                const float4 v = base[(py * sp + j) * SW + (px * sp + i)];
+                r += v.x;
+                gg += v.y;
+                b += v.z;
+            }
+        const float4 acc = J.image[p];
+        J.image[p] = make_float4(acc.x + r * inv, acc.y + gg * inv, acc.z + b * inv, acc.w + 1.0f);
+    }
+}
+
 }  // namespace
 
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
@@ -470,8 +571,8 @@ int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayA
           RayAux* outAux, uint32_t* outCount, const PathChain& chain, const uint2* guide,
           cudaStream_t stream) {
     ShadeArgs a{sc,   rayO,    rayD, aux,  hit,  sortedIds, nonNull, samples,
-                opt,  gen ? 1 : 0, outO, outD, outAux, outCount, chain, guide};
-    k_shade<<<grid_for(maxCount, 128, 148 * 16), 128, 0, stream>>>(a);
+                opt,  gen ? 1 : 0, outO, outD, outAux, outCount, chain, guide, nullptr};
+    k_shade<false><<<grid_for(maxCount, 128, 148 * 16), 128, 0, stream>>>(a);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -492,6 +593,33 @@ int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream) {
 
 int frame_advance(uint32_t* frame, cudaStream_t stream) {
     k_frame_advance<<<1, 32, 0, stream>>>(frame);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int pool_camera(const PoolHeader* hdr, const JobDev* jobs, uint32_t maxSamples, float4* rayO,
+                float4* rayD, RayAux* aux, float4* samples, uint32_t* count, cudaStream_t stream) {
+    k_pool_camera<<<grid_for(maxSamples, 256, 148 * 16), 256, 0, stream>>>(hdr, jobs, rayO, rayD,
+                                                                          aux, samples, count);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int pool_resolve(const PoolHeader* hdr, const JobDev* jobs, uint32_t maxPixels,
+                 const float4* samples, cudaStream_t stream) {
+    k_pool_resolve<<<grid_for(maxPixels, 256, 148 * 8), 256, 0, stream>>>(hdr, jobs, samples);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int shade_jobs(const JobDev* jobs, const float4* rayO, const float4* rayD, const RayAux* aux,
+               const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull,
+               uint32_t maxCount, float4* samples, float4* outO, float4* outD, RayAux* outAux,
+               uint32_t* outCount, cudaStream_t stream) {
+    PathOptions opt{};
+    ShadeArgs a{SceneDev{}, rayO, rayD, aux, hit, sortedIds, nonNull, samples, opt, 1,
+                outO, outD, outAux, outCount, PathChain{}, nullptr, jobs};
+    k_shade<true><<<grid_for(maxCount, 128, 148 * 16), 128, 0, stream>>>(a);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

@@ -27,6 +27,7 @@
 #include "../../include/mrb200.h"
 #include "common.cuh"
 #include "wide.cuh"
+#include "pool.cuh"
 
 namespace mrb {
 
@@ -244,6 +245,122 @@ __device__ __forceinline__ void tri_test(const WideAccelDev& acc, uint32_t s, V3
     }
 }
 
+// Closest hit of one ray in one 8-wide tree.  The top `cached` nodes are
+// read from shared memory (sNodes), the rest through the read-only cache.
+template <bool kCount, int kStack>
+__device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const WideNode* sNodes,
+                                               int cached, V3 o, V3 d, float tmin,
+                                               float& closest, int& hitTri, float& hb0,
+                                               float& hb1, uint32_t& nodeVisits,
+                                               uint32_t& triTests, uint32_t* errorFlag) {
+    if (acc.triCount == 1) {
+        if (kCount) triTests++;
+        tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
+    } else if (acc.triCount > 1) {
+        const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
+        uint2 stack[kStack];  // (node, entry distance bits)
+        int sp = 0;
+        int node = 0;
+        while (node >= 0) {
+            if (kCount) nodeVisits++;
+            uint4 w0, w1, w2, w3, w4;
+            if (node < cached) {
+                const uint4* s = reinterpret_cast<const uint4*>(sNodes + node);
+                w0 = s[0]; w1 = s[1]; w2 = s[2]; w3 = s[3]; w4 = s[4];
+            } else {
+                const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
+                w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
+                w4 = __ldg(g + 4);
+            }
+            const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
+                        lz = __uint_as_float(w0.z);
+            const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+            const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+            const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+            // t = (lo + q*s - o) * inv = q * (s*inv) + (lo - o) * inv
+            const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
+            const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
+                        bz = (lz - o.z) * inv.z;
+            const uint32_t childBase = w1.x, triBase = w1.y;
+            // near/far plane choice per axis from the ray direction
+            const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
+            const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
+            const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
+            const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
+            const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
+            const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
+            // internal children that are hit, keyed by entry distance:
+            // (distance bits with the low three cleared) | slot
+            uint32_t key[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                key[k] = 0xFFFFFFFFu;
+                const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
+                if (meta == 0u) continue;
+                const int kk = k & 3;
+                const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
+                const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
+                const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
+                const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
+                const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
+                const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
+                if (!(tn <= tf)) continue;
+                if (meta & 0x40u) {  // leaf: test the triangle right away
+                    if (kCount) triTests++;
+                    tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
+                             hb0, hb1);
+                } else {
+                    key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
+                }
+            }
+            sort8(key);
+            // push the farther hits (farthest first), enter the nearest
+            node = -1;
+#pragma unroll
+            for (int j = 7; j >= 0; j--) {
+                if (key[j] == 0xFFFFFFFFu) continue;
+                const float tn = __uint_as_float(key[j] & ~7u);
+                if (tn > closest) continue;
+                const uint32_t slot = key[j] & 7u;
+                const uint32_t meta = byte_of(slot < 4 ? w1.z : w1.w, int(slot & 3u));
+                const uint32_t child = childBase + (meta & 0x3Fu);
+                if (j == 0) {
+                    node = int(child);
+                } else if (sp < kStack) {
+                    stack[sp++] = make_uint2(child, key[j] & ~7u);
+                } else {
+                    atomicExch(errorFlag, 3u);
+                }
+            }
+            if (node < 0) {
+                // the nearest hit was beyond the closest triangle: fall
+                // through to the stack
+            }
+            while (node < 0 && sp > 0) {
+                const uint2 e = stack[--sp];
+                if (__uint_as_float(e.y) <= closest) node = int(e.x);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut& out, uint32_t i,
+                                          int hitTri, float closest, float hb0, float hb1) {
+    if (hitTri >= 0) {
+        out.key[i] = __float_as_uint(__ldg(&acc.te0[hitTri].w));
+        out.prim[i] = __float_as_uint(__ldg(&acc.tv0[hitTri].w));
+        out.t[i] = closest;
+        out.bary[i] = make_float2(hb0, hb1);
+    } else {
+        out.key[i] = kBatchNull;
+        out.prim[i] = kInvalid;
+        out.t[i] = closest;
+        out.bary[i] = make_float2(0.0f, 0.0f);
+    }
+}
+
 template <bool kCount>
 __global__ void __launch_bounds__(128) k_trace_wide(WideAccelDev acc,
                                                     const float4* __restrict__ rayO,
@@ -261,113 +378,13 @@ __global__ void __launch_bounds__(128) k_trace_wide(WideAccelDev acc,
     uint32_t nodeVisits = 0, triTests = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 ro = rayO[i], rd = rayD[i];
-        const V3 o = {ro.x, ro.y, ro.z}, d = {rd.x, rd.y, rd.z};
-        const float tmin = ro.w;
         float closest = rd.w;
         int hitTri = -1;
         float hb0 = 0.0f, hb1 = 0.0f;
-        if (acc.triCount == 1) {
-            if (kCount) triTests++;
-            tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
-        } else if (acc.triCount > 1) {
-            const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
-            uint2 stack[kWideStack];  // (node, entry distance bits)
-            int sp = 0;
-            int node = 0;
-            while (node >= 0) {
-                if (kCount) nodeVisits++;
-                uint4 w0, w1, w2, w3, w4;
-                if (node < cached) {
-                    const uint4* s = reinterpret_cast<const uint4*>(sNodes + node);
-                    w0 = s[0]; w1 = s[1]; w2 = s[2]; w3 = s[3]; w4 = s[4];
-                } else {
-                    const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
-                    w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
-                    w4 = __ldg(g + 4);
-                }
-                const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
-                            lz = __uint_as_float(w0.z);
-                const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
-                const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
-                const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-                // t = (lo + q*s - o) * inv = q * (s*inv) + (lo - o) * inv
-                const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
-                const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
-                            bz = (lz - o.z) * inv.z;
-                const uint32_t childBase = w1.x, triBase = w1.y;
-                // near/far plane choice per axis from the ray direction
-                const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
-                const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
-                const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
-                const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
-                const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
-                const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
-                // internal children that are hit, keyed by entry distance:
-                // (distance bits with the low three cleared) | slot
-                uint32_t key[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    key[k] = 0xFFFFFFFFu;
-                    const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
-                    if (meta == 0u) continue;
-                    const int kk = k & 3;
-                    const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
-                    const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
-                    const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
-                    const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
-                    const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
-                    const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
-                    const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-                    const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
-                    if (!(tn <= tf)) continue;
-                    if (meta & 0x40u) {  // leaf: test the triangle right away
-                        if (kCount) triTests++;
-                        tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
-                                 hb0, hb1);
-                    } else {
-                        key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
-                    }
-                }
-                sort8(key);
-                // push the farther hits (farthest first), enter the nearest
-                node = -1;
-#pragma unroll
-                for (int j = 7; j >= 0; j--) {
-                    if (key[j] == 0xFFFFFFFFu) continue;
-                    const float tn = __uint_as_float(key[j] & ~7u);
-                    if (tn > closest) continue;
-                    const uint32_t slot = key[j] & 7u;
-                    const uint32_t meta = byte_of(slot < 4 ? w1.z : w1.w, int(slot & 3u));
-                    const uint32_t child = childBase + (meta & 0x3Fu);
-                    if (j == 0) {
-                        node = int(child);
-                    } else if (sp < kWideStack) {
-                        stack[sp++] = make_uint2(child, key[j] & ~7u);
-                    } else {
-                        atomicExch(errorFlag, 3u);
-                    }
-                }
-                if (node < 0) {
-                    // the nearest hit was beyond the closest triangle: fall
-                    // through to the stack
-                }
-                while (node < 0 && sp > 0) {
-                    const uint2 e = stack[--sp];
-                    if (__uint_as_float(e.y) <= closest) node = int(e.x);
-                }
-            }
-        }
-        if (hitTri >= 0) {
-            out.key[i] = __float_as_uint(__ldg(&acc.te0[hitTri].w));
-            out.prim[i] = __float_as_uint(__ldg(&acc.tv0[hitTri].w));
-            out.t[i] = closest;
-            out.bary[i] = make_float2(hb0, hb1);
-        } else {
-            out.key[i] = kBatchNull;
-            out.prim[i] = kInvalid;
-            out.t[i] = closest;
-            out.bary[i] = make_float2(0.0f, 0.0f);
-        }
+        trace_wide_ray<kCount, kWideStack>(acc, sNodes, cached, V3{ro.x, ro.y, ro.z},
+                                           V3{rd.x, rd.y, rd.z}, ro.w, closest, hitTri, hb0, hb1,
+                                           nodeVisits, triTests, errorFlag);
+        write_hit(acc, out, i, hitTri, closest, hb0, hb1);
     }
     if (kCount) {
         unsigned long long a = nodeVisits, b = triTests;
@@ -379,6 +396,32 @@ __global__ void __launch_bounds__(128) k_trace_wide(WideAccelDev acc,
             atomicAdd(counters + 0, a);
             atomicAdd(counters + 1, b);
         }
+    }
+}
+
+// Rays of many scenes: each ray's tree is its job's (RayAux::pad is the job
+// slot).  No shared-memory top levels: neighbouring rays may use different
+// trees.
+template <int kBlock, int kStack>
+__global__ void __launch_bounds__(kBlock) k_trace_wide_jobs(const JobDev* __restrict__ jobs,
+                                                            const RayAux* __restrict__ aux,
+                                                            const float4* __restrict__ rayO,
+                                                            const float4* __restrict__ rayD,
+                                                            const uint32_t* __restrict__ dCount,
+                                                            uint32_t hCount, HitOut out,
+                                                            uint32_t* errorFlag) {
+    const uint32_t n = dCount ? *dCount : hCount;
+    uint32_t nodeVisits = 0, triTests = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const WideAccelDev acc = jobs[aux[i].pad].wide;
+        const float4 ro = rayO[i], rd = rayD[i];
+        float closest = rd.w;
+        int hitTri = -1;
+        float hb0 = 0.0f, hb1 = 0.0f;
+        trace_wide_ray<false, kStack>(acc, nullptr, 0, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z},
+                                      ro.w, closest, hitTri, hb0, hb1, nodeVisits, triTests,
+                                      errorFlag);
+        write_hit(acc, out, i, hitTri, closest, hb0, hb1);
     }
 }
 
@@ -444,6 +487,44 @@ int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4
                                                         errorFlag, nullptr);
     MRB_CUDA(cudaGetLastError());
     return 0;
+}
+
+template <int kBlock, int kStack>
+static int launch_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
+                       const float4* rayD, const uint32_t* dCount, uint32_t maxCount,
+                       const HitOut& out, uint32_t* errorFlag, cudaStream_t stream) {
+    uint32_t blocks = (maxCount + kBlock - 1) / kBlock;
+    const uint32_t cap = 148u * (2048u / kBlock);
+    blocks = blocks < cap ? blocks : cap;
+    k_trace_wide_jobs<kBlock, kStack><<<blocks, kBlock, 0, stream>>>(jobs, aux, rayO, rayD, dCount,
+                                                                     maxCount, out, errorFlag);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int trace_closest_wide_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
+                            const float4* rayD, const uint32_t* dCount, uint32_t maxCount,
+                            const HitOut& out, uint32_t* errorFlag, int block, int stack,
+                            cudaStream_t stream) {
+    if (maxCount == 0) return 0;
+    const bool big = stack > 64;
+    switch (block) {
+        case 64:
+            return big ? launch_jobs<64, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                              errorFlag, stream)
+                       : launch_jobs<64, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                             errorFlag, stream);
+        case 256:
+            return big ? launch_jobs<256, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                               errorFlag, stream)
+                       : launch_jobs<256, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                              errorFlag, stream);
+        default:
+            return big ? launch_jobs<128, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                               errorFlag, stream)
+                       : launch_jobs<128, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                              errorFlag, stream);
+    }
 }
 
 }  // namespace mrb

@@ -64,18 +64,19 @@ def uv_sphere(center, radius, segments=32, rings=16):
     n = np.stack([np.sin(tt) * np.cos(pp), np.cos(tt), np.sin(tt) * np.sin(pp)], -1).reshape(-1, 3)
     uv = np.stack([pp / (2 * math.pi), tt / math.pi], -1).reshape(-1, 2)
     pos = np.asarray(center, np.float64) + radius * n
-    tris = []
+    # per quad (ring r, segment s), in r-major then s order: (a, d, b) unless
+    # r is the top ring, then (d, c, b) unless r is the bottom ring
     w = segments + 1
-    for r in range(rings):
-        for s in range(segments):
-            a, b = r * w + s, (r + 1) * w + s
-            c, d = (r + 1) * w + s + 1, r * w + s + 1
-            if r != 0:
-                tris.append((a, d, b))
-            if r != rings - 1:
-                tris.append((d, c, b))
+    rr, ss = np.meshgrid(np.arange(rings), np.arange(segments), indexing="ij")
+    a, b = rr * w + ss, (rr + 1) * w + ss
+    c, d = (rr + 1) * w + ss + 1, rr * w + ss + 1
+    t1 = np.stack([a, d, b], -1)
+    t2 = np.stack([d, c, b], -1)
+    both = np.stack([t1, t2], 2)                     # rings x segments x 2 x 3
+    keep = np.stack([rr != 0, rr != rings - 1], -1)  # rings x segments x 2
+    tris = both[keep]
     return (pos.astype(np.float32), n.astype(np.float32), uv.astype(np.float32),
-            np.array(tris, np.uint32))
+            tris.astype(np.uint32))
 
 
 class _Builder:
@@ -99,10 +100,19 @@ class _Builder:
                 np.concatenate(self.mat).astype(np.uint32))
 
 
-def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = False) -> Scene:
+def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = False,
+            triangles: int | None = None) -> Scene:
     """mixed=True gives the spheres, in turn, Lambert, LambertC, Metal (GGX
-    conductor), Unreal and Refract materials (a test input for every BxDF)."""
+    conductor), Unreal and Refract materials (a test input for every BxDF).
+    triangles: scale the spheres' tessellation (segments = 2 x rings) so the
+    scene has about that many triangles (default 32 x 16 per sphere)."""
     rng = np.random.default_rng(seed)
+    segments, rings = 32, 16
+    if triangles is not None:
+        # a sphere of S segments and S/2 rings has S^2 - 2S triangles
+        per = max(8.0, (triangles - 12) / 8.0)
+        segments = max(4, 2 * int(round((1.0 + math.sqrt(1.0 + per)) / 2.0)))
+        rings = segments // 2
     b = _Builder()
     mats = []
 
@@ -128,7 +138,7 @@ def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = Fa
         r = float(rng.uniform(0.1, 0.25))
         c = rng.uniform(r, 1.0 - r, 3)
         if not mixed or kinds[k % 5] == LAMBERT:
-            b.add(*uv_sphere(c, r), lambert())
+            b.add(*uv_sphere(c, r, segments, rings), lambert())
             continue
         kind = kinds[k % 5]
         if kind == LAMBERTC:
@@ -144,13 +154,14 @@ def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = Fa
                          "metallic": float(rng.uniform(0.0, 1.0)), "specular_scalar": 0.5})
         else:
             mats.append({"type": REFRACT, "albedo": np.ones(3, np.float32), "medium": 1})
-        b.add(*uv_sphere(c, r), len(mats) - 1)
+        b.add(*uv_sphere(c, r, segments, rings), len(mats) - 1)
     pos, nrm, uv, idx, mat = b.arrays()
     fov = math.radians(40.0)
     cam = {"position": [0.5, 0.5, -1.0], "gaze": [0.5, 0.5, 0.5], "up": [0.0, 1.0, 0.0],
            "near_far": [0.1, 100.0], "fov": [fov, fov]}
     return Scene("cornell", pos, nrm, uv, idx, mat, mats, np.array([1.0, 1.5], np.float32), 0,
-                 cam, width, height, meta={"seed": seed, "mixed": mixed})
+                 cam, width, height, meta={"seed": seed, "mixed": mixed,
+                                           "sphere_tessellation": (segments, rings)})
 
 
 def clusters(seed: int = 1, width: int = 1920, height: int = 1080, n_clusters: int = 1000,
