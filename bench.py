@@ -20,7 +20,9 @@ scaling; the path tracer has no exchange step).  Rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import datetime
+import math
 import json
 import os
 import statistics
@@ -195,6 +197,13 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     launches = t.launches_per_frame() * args.steps
     guided = run_guided(args, g, m, torch, dev) \
         if (args.guided and args.only == "all" and rank == 0 and world == 1) else None
+    batching = serving = None
+    if args.pool and args.only == "all" and rank == 0 and world == 1:
+        batching = run_batching(args, m, system, torch)
+        if not args.pool_block:
+            args.pool_block = batching["autotune"]["chosen"]["block"]
+            args.pool_stack = batching["autotune"]["chosen"]["stack"]
+        serving = run_serving(args, m, system)
 
     if dist:
         tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
@@ -251,6 +260,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "gpu_launches": launches,
         "clocks": clk,
         "guided": guided,
+        "batching": batching,
+        "serving": serving,
     }
 
 
@@ -345,6 +356,139 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
         "note": "1 spp per frame at 1920x1080; the reference is a separate plain render "
                 "(different seed); the guided tracer starts with a cold octree"}
     return out
+
+
+# ---- wavefront pool: batching (many small scenes) and serving ----------
+BATCH = {"scenes": 256, "tris": (1000, 64000), "res": (64, 128, 256, 512), "spp": 16,
+         "max_depth": 6, "seed": 3}
+SERVE = {"scenes": 32, "tris": (10000, 2000000), "res": (256, 512, 1024),
+         "spp": (1, 16, 64), "rate_per_s": 200.0, "max_depth": 5, "seed": 4}
+
+
+def _log_uniform(rng, lo, hi):
+    return int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+
+
+def _pool_scenes(m, system, rng, n, tris):
+    """n seeded Cornell-style scenes (config-1 generator), triangle counts
+    log-uniform in `tris` through the spheres' tessellation."""
+    out = []
+    for i in range(n):
+        t = _log_uniform(rng, *tris)
+        sc = m.scenes.cornell(seed=10_000 + i, triangles=t, width=64, height=64)
+        g = m.GPUScene(system, sc)
+        g.construct_accelerators()
+        out.append(g)
+    return out
+
+
+def run_batching(args, m, system, torch) -> dict:
+    """C3: one frame of 16 spp for each of 256 seeded scenes, all jobs in one
+    wavefront pool (every traversal launch covers every scene in flight);
+    wavefront size and traversal launch shape picked by the autotuner."""
+    from meturay_b200.pool import autotune
+    rng = np.random.default_rng(BATCH["seed"])
+    scenes = _pool_scenes(m, system, rng, BATCH["scenes"], BATCH["tris"])
+    jobs = []
+    for i, g in enumerate(scenes):
+        r = int(rng.choice(BATCH["res"]))
+        jobs.append(m.Job(g, r, r, samples=1, frames=BATCH["spp"], max_depth=BATCH["max_depth"],
+                          seed=100 + i))
+    largest = max(j.width * j.height for j in jobs)
+    # the autotuner's sample: one frame of every fourth job; wavefront sizes
+    # of 2^16 .. 2^22 rays (two rays per camera sample)
+    caps = [1 << k for k in (15, 17, 19, 21)]
+    tune = autotune(system, [dataclasses.replace(j, frames=1) for j in jobs[::4]],
+                    capacities=caps, blocks=(64, 128, 256), stacks=(64, 128),
+                    max_depth=BATCH["max_depth"], iterations=3)
+    feasible = [r for r in tune["table"] if r["capacity"] >= largest]
+    best = max(feasible, key=lambda r: r["mrays_s"])
+    pool = m.WavefrontPool(system, capacity=best["capacity"], max_depth=BATCH["max_depth"])
+    pool.set_launch(best["block"], best["stack"])
+    pool.run([dataclasses.replace(j, frames=1) for j in jobs[:8]])  # graph capture, warm-up
+    stream = torch.cuda.ExternalStream(lib_stream(pool))
+    r0 = pool.stats()["rays"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    pool.run(jobs)
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    st = pool.stats()
+    rays = st["rays"] - r0
+    samples = sum(j.width * j.height * j.frames for j in jobs)
+    pool.close()
+    return {"metric": METRIC, "value": rays / (ms / 1e3) / 1e6, "unit": "Mrays/s",
+            "seconds": ms / 1e3, "wall_seconds": wall, "rays": rays, "samples": samples,
+            "jobs": len(jobs), "triangles_total": int(sum(g.scene.triangle_count for g in scenes)),
+            "config": {**BATCH, "wavefront": "one pool; every traversal launch covers all "
+                                             "scenes in flight; iterations replay one graph"},
+            "autotune": {"chosen": best, "table": tune["table"],
+                         "note": "capacity = camera samples per iteration (2 rays each); "
+                                 "measured on every fourth job, 3 iterations each"}}
+
+
+def lib_stream(pool):
+    from meturay_b200._lib import lib
+    return lib.mrb_pool_stream(pool._h)
+
+
+def _sphere_camera(rng, center, radius):
+    u = rng.normal(size=3)
+    u /= np.linalg.norm(u)
+    pos = np.asarray(center) + radius * u
+    up = [0.0, 1.0, 0.0] if abs(u[1]) < 0.95 else [1.0, 0.0, 0.0]
+    fov = math.radians(40.0)
+    return {"position": pos.tolist(), "gaze": list(center), "up": up,
+            "near_far": [0.01, 100.0], "fov": [fov, fov]}
+
+
+def run_serving(args, m, system) -> dict:
+    """C4: Poisson arrivals of render jobs against one wavefront pool with
+    32 resident scenes; jobs are admitted by free HBM and join the running
+    iterations as they arrive.  Latency = arrival to the end of the
+    iteration that finished the job (host clock)."""
+    from meturay_b200.pool import serve
+    rng = np.random.default_rng(SERVE["seed"])
+    scenes = _pool_scenes(m, system, rng, SERVE["scenes"], SERVE["tris"])
+    n = int(args.serve_jobs)
+    t, arrivals = 0.0, []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / SERVE["rate_per_s"]))
+        g = scenes[int(rng.integers(len(scenes)))]
+        r = int(rng.choice(SERVE["res"]))
+        spp = int(rng.choice(SERVE["spp"]))
+        job = m.Job(g, r, r, samples=1, frames=spp, max_depth=SERVE["max_depth"],
+                    seed=1000 + i, camera=_sphere_camera(rng, (0.5, 0.5, 0.5), 2.0),
+                    meta={"spp": spp})
+        arrivals.append((t, job))
+    pool = m.WavefrontPool(system, capacity=1 << 21, max_depth=SERVE["max_depth"])
+    if args.pool_block:
+        pool.set_launch(args.pool_block, args.pool_stack)
+    pool.run([dataclasses.replace(arrivals[0][1], frames=1)])  # graph capture, warm-up
+    r0 = pool.stats()["rays"]
+    t0 = time.perf_counter()
+    recs = serve(pool, arrivals)
+    wall = time.perf_counter() - t0
+    rays = pool.stats()["rays"] - r0
+    lat = np.array([r["latency"] for r in recs])
+    samples = sum(j.width * j.height * j.frames for _, j in arrivals)
+    pool.close()
+    return {"metric": METRIC, "value": rays / wall / 1e6, "unit": "Mrays/s",
+            "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean()), "jobs": len(recs),
+            "arrival_span_s": arrivals[-1][0], "wall_seconds": wall, "rays": rays,
+            "samples": samples,
+            "offered_samples_per_s": samples / max(arrivals[-1][0], 1e-9),
+            "config": {**SERVE, "jobs": n, "capacity_samples": 1 << 21,
+                       "camera": "uniform on a sphere of radius 2 around the box centre",
+                       "admission": "first come first served by free HBM"},
+            "note": "latency on the host clock (arrival -> end of the finishing iteration); "
+                    "Mrays/s = rays traced / wall time of the serving window; the offered "
+                    "load exceeds the device's throughput, so latency includes queueing"}
 
 
 def _oracle_setup(scene):
@@ -442,6 +586,12 @@ def main():
     ap.add_argument("--mse-budget-ms", type=float, default=2000.0,
                     help="equal-time MSE budget per tracer (0 skips the comparison)")
     ap.add_argument("--mse-reference-spp", type=int, default=1024)
+    ap.add_argument("--no-pool", dest="pool", action="store_false",
+                    help="skip the wavefront-pool batching and serving runs")
+    ap.add_argument("--serve-jobs", type=int, default=64,
+                    help="jobs in the serving run (Poisson arrivals at 200/s)")
+    ap.add_argument("--pool-block", type=int, default=0)
+    ap.add_argument("--pool-stack", type=int, default=128)
     ap.add_argument("--only", choices=["all", "guided"], default="all",
                     help="guided: only the WFPG timing (for profiling a small case)")
     ap.add_argument("--res", default="1920x1080",
