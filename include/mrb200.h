@@ -385,6 +385,40 @@ int mrb_pool_stats(mrb_pool* pool, uint64_t* rays, uint64_t* iterations, size_t*
                    size_t* hbm_budget);
 void* mrb_pool_stream(mrb_pool* pool);
 
+/* ---- learned guiding network (no counterpart in the reference) ---------
+ * An MLP from a path vertex to a mixture of 8 von Mises-Fisher lobes over
+ * incident directions: 80 input features (sin/cos of 2^j pi p for j < 12 on
+ * each axis of the position normalised to the scene box, the normal, the
+ * outgoing direction, two zeros) -> 64 -> 64 -> 64 (ReLU) -> 40 raw lobe
+ * parameters (per lobe: direction xyz, log concentration, weight logit).
+ * BF16 weights and activations, FP32 accumulation, on the tcgen05 tensor
+ * cores; Adam (0.9, 0.999, 1e-8) on FP32 master parameters.  Parameters:
+ * per layer W[in][64] (out contiguous) then 64 biases; the output layer's
+ * columns 40..63 and the first layer's inputs 78..79 are held at zero. */
+typedef struct mrb_mlp mrb_mlp;
+uint32_t mrb_mlp_param_count(void);
+int mrb_mlp_create(mrb_system* sys, mrb_mlp** out);
+void mrb_mlp_destroy(mrb_mlp* mlp);
+/* Host parameters in; resets the optimiser state. */
+int mrb_mlp_set_params(mrb_mlp* mlp, const float* host_params);
+int mrb_mlp_get_params(const mrb_mlp* mlp, float* host_params);
+/* Device arrays: pos (normalised to [0,1]^3), normal, outgoing direction,
+ * 3 floats each -> n x 80 features. */
+int mrb_mlp_encode(const float* d_pos, const float* d_nrm, const float* d_wo, uint32_t n,
+                   float* d_features, void* stream);
+/* n x 80 features -> n x 40 raw outputs (16-byte aligned arrays). */
+int mrb_mlp_forward(mrb_mlp* mlp, const float* d_features, uint32_t n, float* d_out,
+                    void* stream);
+/* Adds the gradient of sum_s w_s * -log q(dir_s | x_s) into d_grad
+ * (param_count floats) and (sum w_s * -log q, sum w_s) into d_loss[2];
+ * targets n x 4: incident direction xyz (unit), weight w_s >= 0. */
+int mrb_mlp_gradients(mrb_mlp* mlp, const float* d_features, const float* d_targets, uint32_t n,
+                      float* d_grad, float* d_loss, void* stream);
+/* One optimiser step on the loss normalised by sum w_s; host_loss2 (may be
+ * NULL) receives (weighted loss sum, weight sum) of the batch. */
+int mrb_mlp_train_step(mrb_mlp* mlp, const float* d_features, const float* d_targets, uint32_t n,
+                       float lr, float* host_loss2, void* stream);
+
 /* ---- kernel-level entry points (device pointers) ---------------------- */
 /* KCGenerateAABBs + extent reduce + KCGenMortonCodes
  * (LinearBVH.hpp:102-166,444-482). */

@@ -134,6 +134,15 @@ def _load() -> C.CDLL:
         "mrb_pool_stats": (i32, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(sz),
                                  C.POINTER(sz)]),
         "mrb_pool_stream": (vp, [vp]),
+        "mrb_mlp_param_count": (u32, []),
+        "mrb_mlp_create": (i32, [vp, C.POINTER(vp)]),
+        "mrb_mlp_destroy": (None, [vp]),
+        "mrb_mlp_set_params": (i32, [vp, vp]),
+        "mrb_mlp_get_params": (i32, [vp, vp]),
+        "mrb_mlp_encode": (i32, [vp, vp, vp, u32, vp, vp]),
+        "mrb_mlp_forward": (i32, [vp, vp, u32, vp, vp]),
+        "mrb_mlp_gradients": (i32, [vp, vp, vp, u32, vp, vp, vp]),
+        "mrb_mlp_train_step": (i32, [vp, vp, vp, u32, C.c_float, vp, vp]),
         "mrb_tracer_svo_dump": (i32, [vp, vp, sz, C.POINTER(sz)]),
         "mrb_tracer_svo_load": (i32, [vp, vp, sz]),
         "mrb_tracer_write_image": (i32, [vp, C.c_char_p]),
