@@ -271,8 +271,23 @@ void mrb_tracer_destroy(mrb_tracer* t);
  * "BinRayCount", "DoProductPathGuiding" (true only), "PurePG", "SkipPG",
  * "GuideBounceAmount", "OmitDirectRadiance". */
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
-/* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha". */
+/* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha",
+ * "LearnedRate" (Adam step size of the learned guide, default 1e-2),
+ * "LearnedWeightMax" (cap on a training sample's weight, 0 = none).
+ * Learned guiding (no counterpart in the reference), integer options of the
+ * WFPG tracer: "LearnedGuiding" (0/1): a guiding network (mrb_mlp_*) trains
+ * every frame from the path chains and, after "LearnedWarmupFrames" frames
+ * (default 16) of octree guiding, its vMF mixture replaces the octree product
+ * sampler (one-sample MIS with the BxDF, ratio BXDF-GuideMISRatio);
+ * "LearnedTrainSteps" (Adam steps per frame, default 4), "LearnedSamples"
+ * (training samples per frame, default 65,536), "LearnedSeed" (weights'
+ * initial draw). */
 int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double value);
+/* The learned guiding network's parameters (mrb_mlp_param_count floats). */
+int mrb_tracer_learned_params(mrb_tracer* t, float* host_params);
+/* The last frame's training: (sum of w * -log q over its batches, sum of w),
+ * each batch scored before the step that learns from it. */
+int mrb_tracer_learned_loss(mrb_tracer* t, float* host_loss2);
 /* String WFPG options (WFPGTracer.h:39,54): "InitialSVO" -- path of an
  * octree dump that the next GenerateWork loads instead of building the
  * octree (empty: build); "PGDataStructDumpName" -- file name of the periodic

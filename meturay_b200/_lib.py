@@ -135,6 +135,8 @@ def _load() -> C.CDLL:
                                  C.POINTER(sz)]),
         "mrb_pool_stream": (vp, [vp]),
         "mrb_mlp_param_count": (u32, []),
+        "mrb_tracer_learned_params": (i32, [vp, vp]),
+        "mrb_tracer_learned_loss": (i32, [vp, vp]),
         "mrb_mlp_create": (i32, [vp, C.POINTER(vp)]),
         "mrb_mlp_destroy": (None, [vp]),
         "mrb_mlp_set_params": (i32, [vp, vp]),

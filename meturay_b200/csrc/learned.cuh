@@ -1,0 +1,49 @@
+// Learned guiding in the wavefront tracer: the MLP's mixture replaces the
+// octree product sampler once it has trained (learned.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "guide.cuh"
+#include "mlp.cuh"
+#include "shade.cuh"
+#include "svo_dev.cuh"
+
+namespace mrb {
+
+struct LearnedScratch {
+    float* features;      // maxRays x 80 (per wavefront); reused for training samples
+    float* outputs;       // maxRays x 40
+    float* trainX;        // capacity x 80
+    float* trainT;        // capacity x 4
+    uint32_t* pathCount;  // paths + 1
+    uint32_t* pathOffset; // paths + 1
+    void* scanTemp;
+    uint32_t* stepCount;  // steps
+    uint32_t capacity;    // training samples per frame
+    uint32_t steps;       // optimiser steps per frame
+    float* frameLoss;     // 2: weighted loss and weight sums of the frame's batches
+    float weightMax;      // training weights capped at this (0: no cap)
+};
+
+// Guide words for one wavefront from the network: features of every ray's
+// hit, a forward pass, then per ray a draw from the vMF mixture (with
+// probability misRatio) or from the BxDF, the one-sample MIS pdf of the
+// drawn direction, and its octahedral coordinates (half precision, as the
+// octree sampler writes them).  Rays at specular surfaces, lights or none
+// get no guide word.
+int learned_guide_wavefront(const SceneDev& sc, const GuideDev& g, const GuideWave& w,
+                            mrb_mlp* net, const LearnedScratch& s, float misRatio,
+                            const PathOptions& opt, uint32_t depthTag, uint2* guide,
+                            cudaStream_t st);
+
+// Training samples of the frame from the path chain (every non-specular
+// vertex whose path ray carried radiance: features, the ray's direction and
+// weight lum(L_in) / pdf, L_in the radiance that arrived along it), then
+// `steps` Adam steps, step k on the samples j = k mod steps.
+int learned_train_frame(const GuideDev& g, const PathChain& pc, const uint32_t* frame,
+                        mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st);
+size_t learned_scan_temp_bytes(uint32_t paths);
+uint32_t learned_launches(uint32_t steps);
+
+}  // namespace mrb

@@ -189,53 +189,6 @@ __device__ __forceinline__ void load_row(const unsigned char* buf, uint32_t row,
     }
 }
 
-// ---- the von Mises-Fisher mixture ---------------------------------------------
-// Lobe k of the raw outputs r: direction r[5k..5k+2] (normalised), log
-// concentration r[5k+3] clamped to [-10, kMlpLogKappaMax], weight logit
-// r[5k+4] (softmax over the lobes).  vMF(w; mu, kappa) =
-// kappa / (2 pi (1 - exp(-2 kappa))) * exp(kappa (mu.w - 1)).
-__device__ __forceinline__ void mixture_from_raw(const float* r, VmfMixture& mx, float* rawLen) {
-    float lse = -INFINITY;
-    float logit[kMlpLobes];
-#pragma unroll
-    for (int k = 0; k < kMlpLobes; k++) {
-        const float x = r[5 * k], y = r[5 * k + 1], z = r[5 * k + 2];
-        const float nn = sqrtf(x * x + y * y + z * z + 1e-12f);
-        rawLen[k] = nn;
-        mx.mu[k][0] = x / nn;
-        mx.mu[k][1] = y / nn;
-        mx.mu[k][2] = z / nn;
-        const float lk = fminf(fmaxf(r[5 * k + 3], -10.0f), kMlpLogKappaMax);
-        const float kap = expf(lk);
-        mx.kappa[k] = kap;
-        mx.logNorm[k] = lk - logf(2.0f * kPiF) - logf(-expm1f(-2.0f * kap));
-        logit[k] = r[5 * k + 4];
-        lse = fmaxf(lse, logit[k]);
-    }
-    float s = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kMlpLobes; k++) s += expf(logit[k] - lse);
-    lse += logf(s);
-#pragma unroll
-    for (int k = 0; k < kMlpLobes; k++) mx.logPi[k] = logit[k] - lse;
-}
-
-// log q(w) and each lobe's log(pi_k vMF_k(w)).
-__device__ __forceinline__ float mixture_logpdf(const VmfMixture& mx, float wx, float wy, float wz,
-                                                float* lobeLog) {
-    float m = -INFINITY;
-#pragma unroll
-    for (int k = 0; k < kMlpLobes; k++) {
-        const float c = mx.mu[k][0] * wx + mx.mu[k][1] * wy + mx.mu[k][2] * wz;
-        lobeLog[k] = mx.logPi[k] + mx.logNorm[k] + mx.kappa[k] * (c - 1.0f);
-        m = fmaxf(m, lobeLog[k]);
-    }
-    float s = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kMlpLobes; k++) s += expf(lobeLog[k] - m);
-    return m + logf(s);
-}
-
 // d(-w log q(dir))/d raw into g[0..39]; returns -log q.
 __device__ __forceinline__ float mixture_grad(const float* r, float wx, float wy, float wz,
                                               float weight, float* g) {
@@ -406,9 +359,12 @@ __device__ __forceinline__ bool forward_tile(MlpSmem& S, uint32_t tmem, uint32_t
 }
 
 __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_forward(MlpDev m, const float* __restrict__ in,
-                                                            uint32_t n, float* __restrict__ out) {
+                                                            uint32_t maxN,
+                                                            const uint32_t* __restrict__ dCount,
+                                                            float* __restrict__ out) {
     extern __shared__ __align__(1024) unsigned char smemRaw[];
     MlpSmem& S = *reinterpret_cast<MlpSmem*>(smemRaw);
+    const uint32_t n = dCount ? min(*dCount, maxN) : maxN;
     const uint32_t tmem = mlp_prologue(S, m, 64);
     uint32_t phase = 0;
     const uint32_t tiles = (n + kMlpTile - 1) / kMlpTile;
@@ -447,10 +403,13 @@ __device__ __forceinline__ void round_bf16(float* v, int n) {
 
 __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_train(MlpDev m, const float* __restrict__ in,
                                                           const float* __restrict__ targets,
-                                                          uint32_t n, float* __restrict__ grad,
+                                                          uint32_t maxN,
+                                                          const uint32_t* __restrict__ dCount,
+                                                          float* __restrict__ grad,
                                                           float* __restrict__ loss) {
     extern __shared__ __align__(1024) unsigned char smemRaw[];
     MlpSmem& S = *reinterpret_cast<MlpSmem*>(smemRaw);
+    const uint32_t n = dCount ? min(*dCount, maxN) : maxN;
     const uint32_t tmem = mlp_prologue(S, m, 512);
     const uint32_t row = threadIdx.x;
     const uint32_t lane = (threadIdx.x & ~31u) << 16;
@@ -604,6 +563,7 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ params, fl
                                                   float* __restrict__ grad,
                                                   const float* __restrict__ loss, float lr,
                                                   uint16_t* __restrict__ image) {
+    const bool empty = !(loss[1] > 0.0f);  // a batch without weight: no step
     const uint32_t t = *step + 1u;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f - powf(b1, float(t)), c2 = 1.0f - powf(b2, float(t));
@@ -611,7 +571,7 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ params, fl
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < uint32_t(kMlpParams);
          i += gridDim.x * blockDim.x) {
         float p = params[i];
-        if (!param_frozen(i)) {
+        if (!empty && !param_frozen(i)) {
             const float g = grad[i] * inv;
             const float a = b1 * m1[i] + (1.0f - b1) * g;
             const float b = b2 * m2[i] + (1.0f - b2) * g * g;
@@ -628,8 +588,8 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ params, fl
     }
 }
 
-__global__ void k_mlp_step(uint32_t* step) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1u;
+__global__ void k_mlp_step(uint32_t* step, const float* loss) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && loss[1] > 0.0f) *step += 1u;
 }
 
 __global__ void __launch_bounds__(256) k_mlp_image(const float* __restrict__ params,
@@ -641,34 +601,6 @@ __global__ void __launch_bounds__(256) k_mlp_image(const float* __restrict__ par
         if (param_weight(i, l, in, out))
             image[(image_layer_offset(l) + w_offset(in, out)) / 2] = bf16_bits(params[i]);
     }
-}
-
-// Features of a vertex: per axis c and frequency j, sin and cos of
-// 2^j pi p_c at 24c + 2j and 24c + 2j + 1; then the normal and the
-// outgoing direction; then two zeros.
-__device__ __forceinline__ void encode_vertex(float px, float py, float pz, float nx, float ny,
-                                              float nz, float ox, float oy, float oz, float* f) {
-    const float p[3] = {px, py, pz};
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        float x = p[c];
-#pragma unroll
-        for (int j = 0; j < 12; j++) {
-            float sv, cv;
-            sincospif(x, &sv, &cv);
-            f[24 * c + 2 * j] = sv;
-            f[24 * c + 2 * j + 1] = cv;
-            x *= 2.0f;
-        }
-    }
-    f[72] = nx;
-    f[73] = ny;
-    f[74] = nz;
-    f[75] = ox;
-    f[76] = oy;
-    f[77] = oz;
-    f[78] = 0.0f;
-    f[79] = 0.0f;
 }
 
 __global__ void __launch_bounds__(256) k_mlp_encode(const float* __restrict__ pos,
@@ -707,19 +639,21 @@ uint32_t mlp_grid(uint32_t n) {
 
 }  // namespace
 
-int mlp_forward(const MlpDev& m, const float* in, uint32_t n, float* out, cudaStream_t st) {
+int mlp_forward(const MlpDev& m, const float* in, uint32_t n, float* out, cudaStream_t st,
+                const uint32_t* dCount) {
     if (n == 0) return 0;
     if (mlp_smem_setup()) return MRB_E_CUDA;
-    k_mlp_forward<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, n, out);
+    k_mlp_forward<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, n, dCount, out);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
 
 int mlp_gradients(const MlpDev& m, const float* in, const float* targets, uint32_t n, float* grad,
-                  float* loss, cudaStream_t st) {
+                  float* loss, cudaStream_t st, const uint32_t* dCount) {
     if (n == 0) return 0;
     if (mlp_smem_setup()) return MRB_E_CUDA;
-    k_mlp_train<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, targets, n, grad, loss);
+    k_mlp_train<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, targets, n, dCount, grad,
+                                                               loss);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -728,7 +662,7 @@ int mlp_adam(float* params, float* m1, float* m2, uint32_t* step, float* grad, c
              float lr, uint16_t* wImage, cudaStream_t st) {
     k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(params, m1, m2, step, grad, loss, lr,
                                                         wImage);
-    k_mlp_step<<<1, 32, 0, st>>>(step);
+    k_mlp_step<<<1, 32, 0, st>>>(step, loss);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -779,6 +713,32 @@ int mlp_check(mrb_mlp* m, cudaStream_t st) {
 namespace mrb {
 MlpDev mlp_dev(const mrb_mlp* m) { return m->dev(); }
 float* mlp_params(mrb_mlp* m) { return m->params.as<float>(); }
+int mlp_train_step_dev(mrb_mlp* m, const float* in, const float* targets, uint32_t maxN,
+                       const uint32_t* dCount, float lr, cudaStream_t st) {
+    MRB_CUDA(cudaMemsetAsync(m->loss.p, 0, 8, st));
+    int r = mlp_gradients(m->dev(), in, targets, maxN, m->grad.as<float>(), m->loss.as<float>(),
+                          st, dCount);
+    if (r) return r;
+    return mlp_adam(m->params.as<float>(), m->m1.as<float>(), m->m2.as<float>(),
+                    m->step.as<uint32_t>(), m->grad.as<float>(), m->loss.as<float>(), lr,
+                    m->image.as<uint16_t>(), st);
+}
+uint32_t* mlp_error_flag(mrb_mlp* m) { return m->err.as<uint32_t>(); }
+float* mlp_loss(mrb_mlp* m) { return m->loss.as<float>(); }
+size_t mlp_state_bytes() { return size_t(kMlpParams) * 4 * 3 + 16 + kMlpImageBytes; }
+// Parameters, optimiser state and weight image to / from a device buffer.
+int mlp_state_copy(mrb_mlp* m, void* buf, bool save, cudaStream_t st) {
+    const size_t P = size_t(kMlpParams) * 4;
+    unsigned char* b = static_cast<unsigned char*>(buf);
+    DBuf* parts[5] = {&m->params, &m->m1, &m->m2, &m->step, &m->image};
+    const size_t sizes[5] = {P, P, P, 16, kMlpImageBytes};
+    for (int i = 0; i < 5; i++) {
+        if (save) MRB_CUDA(cudaMemcpyAsync(b, parts[i]->p, sizes[i], cudaMemcpyDeviceToDevice, st));
+        else MRB_CUDA(cudaMemcpyAsync(parts[i]->p, b, sizes[i], cudaMemcpyDeviceToDevice, st));
+        b += sizes[i];
+    }
+    return 0;
+}
 }  // namespace mrb
 
 extern "C" {

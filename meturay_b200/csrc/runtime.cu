@@ -29,6 +29,7 @@
 #include "guide.cuh"
 #include "recon.cuh"
 #include "io.cuh"
+#include "learned.cuh"
 #include "objects.cuh"
 
 namespace mrb {
@@ -194,6 +195,14 @@ struct mrb_tracer {
     // interval^0, interval^1, ... ("PGDataStructDumpIntervalExp") to
     // "<frame>_<PGDataStructDumpName>" (WFPGTracer.cu:1289-1309,1733-1745)
     std::string initialSvo, dumpName = "wfpg_svo";
+    // learned guiding: the network's mixture replaces the octree sampler
+    // after learnedWarmup frames; it trains every frame from the path chains
+    uint32_t learned = 0, learnedWarmup = 16, learnedSteps = 4, learnedSamples = 1u << 16;
+    uint64_t learnedSeed = 1;
+    float learnedRate = 1.0e-2f, learnedWeightMax = 0.0f;
+    mrb_mlp* net = nullptr;
+    DBuf chainN, chainD, chainT, lFeat, lOut, lTrainX, lTrainT, lCount, lOffset, lScan, lSteps,
+        lLoss, netBackup;
     uint32_t dumpEnabled = 0, dumpInterval = 2, iterationCount = 0, treeDumpCount = 0;
     bool svoReady = false;
     SvoParams svoP{};
@@ -210,6 +219,7 @@ struct mrb_tracer {
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
     ~mrb_tracer() {
+        if (net) mrb_mlp_destroy(net);
         if (svoReady) svo_free(svo);
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
@@ -310,7 +320,85 @@ PathChain path_chain(const mrb_tracer* t) {
     c.contribPath = t->chainPath.as<float4>();
     c.paths = t->chainPaths;
     c.levels = t->chainLevels;
+    if (t->learned) {
+        c.nodeN = t->chainN.as<float4>();
+        c.nodeD = t->chainD.as<float4>();
+        c.nodeT = t->chainT.as<float4>();
+    }
     return c;
+}
+
+// He-uniform initial weights from a seed (splitmix64 stream), zero biases;
+// the padded entries stay zero.
+std::vector<float> learned_init(uint64_t seed) {
+    std::vector<float> p(kMlpParams, 0.0f);
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    auto next = [&x]() {
+        uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return static_cast<float>(z >> 40) * 0x1p-24f;
+    };
+    for (int l = 0; l < kMlpLayers; l++) {
+        const int K = l == 0 ? kMlpIn : 64;
+        const float lim = std::sqrt((l < kMlpLayers - 1 ? 6.0f : 3.0f) / float(K));
+        float* w = p.data() + mlp_layer_offset(l);
+        for (int i = 0; i < K; i++)
+            for (int o = 0; o < 64; o++) {
+                const float u = next();
+                const bool frozen = (l == 0 && i >= kMlpFeatures) ||
+                                    (l == kMlpLayers - 1 && o >= kMlpOut);
+                w[i * 64 + o] = frozen ? 0.0f : (2.0f * u - 1.0f) * lim;
+            }
+    }
+    return p;
+}
+
+LearnedScratch learned_scratch(const mrb_tracer* t) {
+    LearnedScratch s{};
+    s.features = t->lFeat.as<float>();
+    s.outputs = t->lOut.as<float>();
+    s.trainX = t->lTrainX.as<float>();
+    s.trainT = t->lTrainT.as<float>();
+    s.pathCount = t->lCount.as<uint32_t>();
+    s.pathOffset = t->lOffset.as<uint32_t>();
+    s.scanTemp = t->lScan.p;
+    s.stepCount = t->lSteps.as<uint32_t>();
+    s.frameLoss = t->lLoss.as<float>();
+    s.weightMax = t->learnedWeightMax;
+    s.steps = t->learnedSteps;
+    s.capacity = t->learnedSamples / t->learnedSteps * t->learnedSteps;
+    return s;
+}
+
+// Buffers and network of learned guiding (after ensure_buffers).
+int ensure_learned(mrb_tracer* t) {
+    if (!t->wfpg || !t->learned) return 0;
+    const size_t chain = size_t(t->chainLevels) * t->chainPaths * 16;
+    const uint32_t cap = t->learnedSamples / t->learnedSteps * t->learnedSteps;
+    int r;
+    if ((r = t->chainN.alloc(chain)) || (r = t->chainD.alloc(chain)) ||
+        (r = t->chainT.alloc(chain)) || (r = t->lFeat.alloc(size_t(t->maxRays) * kMlpIn * 4)) ||
+        (r = t->lOut.alloc(size_t(t->maxRays) * kMlpOut * 4)) ||
+        (r = t->lTrainX.alloc(size_t(cap) * kMlpIn * 4)) ||
+        (r = t->lTrainT.alloc(size_t(cap) * 16)) ||
+        (r = t->lCount.alloc((size_t(t->chainPaths) + 1) * 4)) ||
+        (r = t->lOffset.alloc((size_t(t->chainPaths) + 1) * 4)) ||
+        (r = t->lScan.alloc(learned_scan_temp_bytes(t->chainPaths))) ||
+        (r = t->lSteps.alloc(size_t(t->learnedSteps) * 4)) || (r = t->lLoss.alloc(16)) ||
+        (r = t->netBackup.alloc(mlp_state_bytes())))
+        return r;
+    if (!t->net) {
+        if ((r = mrb_mlp_create(t->sys, &t->net))) return r;
+        const std::vector<float> p = learned_init(t->learnedSeed);
+        if ((r = mrb_mlp_set_params(t->net, p.data()))) return r;
+    }
+    return 0;
+}
+
+bool learned_active(const mrb_tracer* t) {
+    return t->wfpg && t->learned && t->net && t->frames >= t->learnedWarmup;
 }
 
 GuideOptions guide_options(const mrb_tracer* t) {
@@ -443,9 +531,14 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
                         t->headScan.as<uint32_t>(), t->binBegin.as<uint32_t>(),
                         t->binEnd.as<uint32_t>(), t->guideSort.p, t->guideSortBytes,
                         t->guideScan.p, t->guideBuf.as<uint2>()};
-        if ((r = guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), t->svo, gw, gs,
-                                 guide_options(t), path_options(t), d, d, t->stream)))
-            return r;
+        if (learned_active(t))
+            r = learned_guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), gw, t->net,
+                                        learned_scratch(t), t->misRatio, path_options(t), d,
+                                        t->guideBuf.as<uint2>(), t->stream);
+        else
+            r = guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), t->svo, gw, gs,
+                                guide_options(t), path_options(t), d, d, t->stream);
+        if (r) return r;
     }
     if (mark(2)) return MRB_E_CUDA;
     PortionTable pt = portion_table(t);
@@ -481,6 +574,10 @@ int step_finalize(mrb_tracer* t) {
         const GuideDev g = guide_dev(t->svo, t->svoP);
         if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream))) return r;
         if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
+        if (t->learned && t->net &&
+            (r = learned_train_frame(g, path_chain(t), t->frameWord.as<uint32_t>(), t->net,
+                                     learned_scratch(t), t->learnedRate, t->stream)))
+            return r;
     }
     if (t->hasFilter)
         r = recon_filter_grid(t->filter, t->samplesBuf.as<float4>(), t->imgCoords.as<float2>(),
@@ -513,7 +610,12 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
         // guiding per guided depth; deposit, leaf averages and the two
         // level filters per frame
         const uint32_t guided = t->skipPG ? 0u : std::min(t->maxDepth, t->guideBounce);
-        n += guided * guide_launches(t->svo, guide_options(t), t->maxRays) + 2 + 2 * t->svoP.depth;
+        // learned guiding: features, forward pass and sampler per guided
+        // depth, and the frame's training
+        const uint32_t perDepth = learned_active(t) ? 3u
+                                                    : guide_launches(t->svo, guide_options(t), t->maxRays);
+        n += guided * perDepth + 2 + 2 * t->svoP.depth;
+        if (t->learned && t->net) n += learned_launches(t->learnedSteps);
     }
     return n;
 }
@@ -1052,6 +1154,18 @@ int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double v) {
             return MRB_E_ARG;
         }
         t->filterAlpha = static_cast<float>(v);
+    } else if (t->wfpg && k == "LearnedRate") {
+        if (!(v > 0.0 && v < 1.0)) {
+            set_error("LearnedRate must be in (0, 1)");
+            return MRB_E_ARG;
+        }
+        t->learnedRate = static_cast<float>(v);
+    } else if (t->wfpg && k == "LearnedWeightMax") {
+        if (!(v >= 0.0)) {
+            set_error("LearnedWeightMax must be >= 0");
+            return MRB_E_ARG;
+        }
+        t->learnedWeightMax = static_cast<float>(v);
     } else {
         set_error("unknown float option '%s'", name);
         return MRB_E_ARG;
@@ -1115,6 +1229,27 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
         t->skipPG = v ? 1 : 0;
     } else if (t->wfpg && k == "GuideBounceAmount") {
         t->guideBounce = uint32_t(v);
+    } else if (t->wfpg && k == "LearnedGuiding") {
+        t->learned = v ? 1 : 0;
+    } else if (t->wfpg && k == "LearnedWarmupFrames") {
+        t->learnedWarmup = uint32_t(v);
+    } else if (t->wfpg && (k == "LearnedTrainSteps" || k == "LearnedSamples")) {
+        if (k == "LearnedTrainSteps" && (v == 0 || v > 32)) {
+            set_error("LearnedTrainSteps must be in [1, 32]");
+            return MRB_E_ARG;
+        }
+        if (k == "LearnedSamples" && (v < 128 || v > (1u << 24))) {
+            set_error("LearnedSamples must be in [128, 2^24]");
+            return MRB_E_ARG;
+        }
+        if (k == "LearnedTrainSteps") t->learnedSteps = uint32_t(v);
+        else t->learnedSamples = uint32_t(v);
+    } else if (t->wfpg && k == "LearnedSeed") {
+        t->learnedSeed = v;
+        if (t->net) {
+            const std::vector<float> p = learned_init(v);
+            if (mrb_mlp_set_params(t->net, p.data())) return MRB_E_CUDA;
+        }
     } else if (t->wfpg && k == "PGDumpDataStruct") {
         t->dumpEnabled = v ? 1 : 0;
         return 0;
@@ -1205,6 +1340,7 @@ int mrb_tracer_generate_work(mrb_tracer* t, uint32_t) {
     int r = ensure_buffers(t);
     if (r) return r;
     if ((r = ensure_svo(t))) return r;
+    if ((r = ensure_learned(t))) return r;
     if ((r = step_camera(t))) return r;
     t->depth = 0;
     t->working = true;
@@ -1244,6 +1380,10 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
     int r = ensure_buffers(t);
     if (r) return r;
     if ((r = ensure_svo(t))) return r;
+    if ((r = ensure_learned(t))) return r;
+    // the captured frame bakes in which sampler guides: capture again when
+    // the network takes over
+    if (t->wfpg && t->learned && t->frames == t->learnedWarmup) t->graphDirty = true;
     if (t->graphDirty || !t->graph) {
         if (t->graph) {
             cudaGraphExecDestroy(t->graph);
@@ -1265,7 +1405,9 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             MRB_CUDA(cudaMemcpyAsync(b + U * 24, t->svo.leafAvg, U * 4, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(b + U * 28, t->svo.nodeAvg, N * 4, cudaMemcpyDeviceToDevice, t->stream));
         }
+        if (t->net && mlp_state_copy(t->net, t->netBackup.p, true, t->stream)) return MRB_E_CUDA;
         if ((r = record_frame(t))) return r;
+        if (t->net && mlp_state_copy(t->net, t->netBackup.p, false, t->stream)) return MRB_E_CUDA;
         MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f0, 4, cudaMemcpyHostToDevice, t->stream));
         if (pb) {
             const char* b = t->payloadBackup.as<char>();
@@ -1321,6 +1463,27 @@ int mrb_tracer_reset_image(mrb_tracer* t) {
     if (!t) return MRB_E_ARG;
     if (t->image.p) MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
     return 0;
+}
+
+int mrb_tracer_learned_loss(mrb_tracer* t, float* host_loss2) {
+    if (!t || !host_loss2 || !t->net) {
+        set_error("tracer: no learned guiding network (option LearnedGuiding, then a frame)");
+        return MRB_E_STATE;
+    }
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    MRB_CUDA(cudaMemcpyAsync(host_loss2, t->lLoss.p, 8, cudaMemcpyDeviceToHost, t->stream));
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    return 0;
+}
+
+int mrb_tracer_learned_params(mrb_tracer* t, float* host_params) {
+    if (!t || !host_params || !t->net) {
+        set_error("tracer: no learned guiding network (option LearnedGuiding, then a frame)");
+        return MRB_E_STATE;
+    }
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    return mrb_mlp_get_params(t->net, host_params);
 }
 
 int mrb_tracer_set_option_string(mrb_tracer* t, const char* name, const char* value) {

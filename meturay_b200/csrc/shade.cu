@@ -257,6 +257,11 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                     const size_t at = size_t(aux.depth) * P + aux.sample;
                     A.chain.nodeA[at] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, __uint_as_float(frame));
                     A.chain.nodeB[at] = make_float4(rf.x, rf.y, rf.z, 0.0f);
+                    if (A.chain.nodeN) {
+                        const V3 nrm = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+                        A.chain.nodeN[at] = make_float4(nrm.x, nrm.y, nrm.z, specular ? 1.0f : 0.0f);
+                        A.chain.nodeT[at] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0xFFFFFFFFu));
+                    }
                     if (uint32_t(aux.depth) + 1 < A.chain.levels) {
                         const size_t nx = at + P;
                         A.chain.contribNee[nx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -397,6 +402,11 @@ __global__ void __launch_bounds__(128) k_shade(ShadeArgs A) {
                     pathAux.type = specular ? kSpecPathRay : kPathRay;
                     pathAux.prevPDF = bs.pdf;
                     pathAux.depth = static_cast<uint8_t>(aux.depth + 1);
+                    if (A.opt.wfpg && A.chain.nodeN) {
+                        const size_t at = size_t(aux.depth) * A.chain.paths + aux.sample;
+                        A.chain.nodeD[at] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.pdf);
+                        A.chain.nodeT[at] = make_float4(prf.x, prf.y, prf.z, __uint_as_float(frame));
+                    }
                 }
                 }  // gen
             }

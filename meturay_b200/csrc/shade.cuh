@@ -32,6 +32,12 @@ struct PathChain {
     float4* contribPath;
     uint32_t paths;
     uint32_t levels;        // maxDepth + 1
+    // learned guiding only (null otherwise): per vertex the shading normal
+    // and 1 for a specular surface; the path ray it emitted (direction, pdf)
+    // and that ray's throughput with the frame stamp in .w
+    float4* nodeN;
+    float4* nodeD;
+    float4* nodeT;
 };
 
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,

@@ -354,8 +354,9 @@ class WFPGTracer(PathTracer):
     OPTION_KEYS = PathTracer.OPTION_KEYS + (
         "OctreeLevel", "MinRayBinLevel", "BinRayCount", "DoProductPathGuiding", "PurePG",
         "SkipPG", "GuideBounceAmount", "OmitDirectRadiance", "PGDumpDataStruct",
-        "PGDataStructDumpIntervalExp")
-    FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha")
+        "PGDataStructDumpIntervalExp", "LearnedGuiding", "LearnedWarmupFrames",
+        "LearnedTrainSteps", "LearnedSamples", "LearnedSeed")
+    FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha", "LearnedRate", "LearnedWeightMax")
     STRING_KEYS = ("InitialSVO", "PGDataStructDumpName")
 
     def __init__(self, system: TracerSystem, scene: GPUScene):
@@ -370,6 +371,18 @@ class WFPGTracer(PathTracer):
                 check(lib.mrb_tracer_set_option_float(self._h, k.encode(), float(v)))
             elif k in self.STRING_KEYS:
                 check(lib.mrb_tracer_set_option_string(self._h, k.encode(), str(v).encode()))
+
+    def learned_params(self) -> np.ndarray:
+        """The learned guiding network's parameters (LearnedGuiding)."""
+        p = np.zeros(int(lib.mrb_mlp_param_count()), np.float32)
+        check(lib.mrb_tracer_learned_params(self._h, _ptr(p)))
+        return p
+
+    def learned_loss(self) -> float:
+        """Weighted mean -log q of the last frame's training batches."""
+        out = np.zeros(2, np.float32)
+        check(lib.mrb_tracer_learned_loss(self._h, _ptr(out)))
+        return float(out[0] / out[1]) if out[1] > 0 else float("nan")
 
     def dump_svo(self) -> bytes:
         """DumpSVOAsBinary: the octree and its radiance state as bytes."""

@@ -1,0 +1,84 @@
+"""Learned guiding inside the WFPG tracer.
+
+The network trains every frame from the path chains; each frame's batch is
+scored before the step that learns from it, so the per-frame loss is a
+held-out estimate of how well the mixture predicts where radiance arrives.
+After the warm-up frames the network's sampler writes the guide words, and
+the estimator stays unbiased (image mean against the plain tracer's).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+OPTS = {"Samples": 1, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
+        "DirectLightMIS": 0, "Seed": 5, "OctreeLevel": 6, "MinRayBinLevel": 3,
+        "BinRayCount": 64, "LearnedGuiding": 1, "LearnedWarmupFrames": 4,
+        "LearnedTrainSteps": 4, "LearnedSamples": 8192}
+
+
+def _scene(system, w=64, h=48):
+    from meturay_b200 import GPUScene, scenes
+    g = GPUScene(system, scenes.cornell(seed=2, width=w, height=h))
+    g.construct_accelerators()
+    return g
+
+
+def _mean(img):
+    return img[..., :3].sum() / max(float(img[0, 0, 3]), 1.0) / (img.shape[0] * img.shape[1])
+
+
+def test_learned_guiding_trains_and_guides(system):
+    from meturay_b200 import PathTracer, WFPGTracer
+    g = _scene(system)
+    t = WFPGTracer(system, g)
+    t.set_options(dict(OPTS, LearnedTrainSteps=4, LearnedWarmupFrames=40))
+    t.set_options({"LearnedRate": 3e-3, "LearnedWeightMax": 5.0})
+    t.render_frame()
+    p0 = t.learned_params()
+    losses = [t.learned_loss()]
+    for _ in range(119):
+        t.render_frame()
+        losses.append(t.learned_loss())
+    p1 = t.learned_params()
+    assert np.all(np.isfinite(p1)) and not np.array_equal(p0, p1)
+    assert all(np.isfinite(losses))
+    # the held-out loss falls as the network learns the incident radiance
+    assert np.mean(losses[-10:]) < np.mean(losses[:3]) - 0.3, (losses[:3], losses[-10:])
+    # after the warm-up the network's sampler writes the guide words
+    t.generate_work()
+    assert t.render()
+    gs = t.guide_state()
+    valid = (gs["guide"][:, 1] >> 17) & 1
+    assert valid.sum() > 0.5 * len(valid)
+    while t.render():
+        pass
+    t.finalize()
+    # unbiased: the image mean matches the plain tracer's within the noise
+    guided = t.image()
+    p = PathTracer(system, g)
+    p.set_options({k: OPTS[k] for k in ("Samples", "MaxDepth", "NextEventEstimation",
+                                         "RussianRouletteStart", "DirectLightMIS")})
+    p.set_options({"Seed": 77})
+    for _ in range(121):
+        p.render_frame()
+    a, b = _mean(guided), _mean(p.image())
+    assert abs(a - b) < 0.05 * b, (a, b)
+
+
+def test_learned_options_and_errors(system):
+    import meturay_b200 as m
+    from meturay_b200 import WFPGTracer
+    g = _scene(system, 16, 16)
+    t = WFPGTracer(system, g)
+    with pytest.raises(m.MrbError):
+        t.learned_params()                   # no network before the option and a frame
+    for bad in ({"LearnedTrainSteps": 0}, {"LearnedSamples": 10}):
+        with pytest.raises(m.MrbError):
+            t.set_options(bad)
+    with pytest.raises(m.MrbError):
+        t.set_options({"LearnedRate": 2.0})
+    t.set_options(dict(OPTS, LearnedWarmupFrames=1, LearnedSeed=9))
+    for _ in range(3):
+        t.render_frame()
+    assert np.all(np.isfinite(t.learned_params()))
