@@ -204,6 +204,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             args.pool_block = batching["autotune"]["chosen"]["block"]
             args.pool_stack = batching["autotune"]["chosen"]["stack"]
         serving = run_serving(args, m, system)
+    learned = run_learned(args, m, system, torch) \
+        if (args.learned and args.only == "all" and rank == 0 and world == 1) else None
 
     if dist:
         tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
@@ -262,6 +264,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "guided": guided,
         "batching": batching,
         "serving": serving,
+        "learned": learned,
     }
 
 
@@ -491,6 +494,86 @@ def run_serving(args, m, system) -> dict:
                     "load exceeds the device's throughput, so latency includes queueing"}
 
 
+# ---- learned guiding (C5) ------------------------------------------------
+C1 = {"Samples": 2, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
+      "DirectLightMIS": 0}
+LEARNED = {"LearnedGuiding": 1, "LearnedWarmupFrames": 16, "LearnedTrainSteps": 4,
+           "LearnedSamples": 65536, "OctreeLevel": 10, "MinRayBinLevel": 5, "BinRayCount": 512}
+LEARNED_FLOATS = {"LearnedRate": 1e-2, "LearnedWeightMax": 5.0, "BXDF-GuideMISRatio": 0.5,
+                  "RFieldFilterAlpha": 0.6}
+
+
+def _frame_ms(t, torch, frames=20):
+    stream = torch.cuda.ExternalStream(t.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(frames):
+        t.render_frame()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / frames
+
+
+def run_learned(args, m, system, torch) -> dict:
+    """C5: the config-1 Cornell scene (128x128, 4 spp per frame, depth 5);
+    plain path tracing, SVO path guiding and learned guiding (MLP vMF
+    mixture trained online on the tensor cores, the SVO guider for the first
+    16 frames) get the same time budget from a cold start and are scored by
+    mean squared error against a 4096-spp plain render."""
+    scene = m.scenes.cornell(seed=1)
+    g = m.GPUScene(system, scene)
+    g.construct_accelerators()
+
+    def make(kind, seed):
+        t = m.PathTracer(system, g) if kind == "plain" else m.WFPGTracer(system, g)
+        opts = dict(C1, Seed=seed)
+        learned = kind.startswith("learned")
+        if kind != "plain":
+            opts.update({k: v for k, v in LEARNED.items()
+                         if learned or not k.startswith("Learned")})
+            if learned:
+                opts["LearnedTrainSteps"] = int(kind.split("_")[1])
+        t.set_options(opts)
+        if kind != "plain":
+            t.set_options({k: v for k, v in LEARNED_FLOATS.items()
+                           if learned or not k.startswith("Learned")})
+        return t
+
+    ref = make("plain", 4242)
+    ref_img = _frames_image(ref, args.learned_reference_spp // 4)
+    ref.close()
+    out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp}
+    for kind, seed in (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14)):
+        probe = make(kind, seed + 100)
+        for _ in range(24):           # past the warm-up: the frame time the budget meets
+            probe.render_frame()
+        ms = _frame_ms(probe, torch)
+        probe.close()
+        frames = max(1, int(args.learned_budget_ms / ms))
+        t = make(kind, seed)
+        img = _frames_image(t, frames)
+        entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames,
+                 "mse": float(np.mean((img - ref_img) ** 2))}
+        if kind.startswith("learned"):
+            entry["held_out_loss_last_frame"] = t.learned_loss()
+            entry["train_steps_per_frame"] = int(kind.split("_")[1])
+        t.close()
+        out[kind] = entry
+    best = min(("learned_1", "learned_4"), key=lambda k: out[k]["mse"])
+    out["learned"] = dict(out[best], variant=best)
+    out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
+    out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
+    # per-sample efficiency (MSE x spp; lower is better), which the frame
+    # cost then trades against
+    out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
+                        for k in ("plain", "svo", "learned_1", "learned_4")}
+    out["config"] = {"scene": "config-1 Cornell box (seed 1), 128x128, 4 spp per frame, depth 5",
+                     **LEARNED, **LEARNED_FLOATS,
+                     "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
+                                "activations, FP32 accumulation on tcgen05 tensor cores"}
+    return out
+
+
 def _oracle_setup(scene):
     """Scene arrays as the hot path consumes them, built by the oracle alone."""
     from oracle import oracle as o
@@ -592,6 +675,10 @@ def main():
                     help="jobs in the serving run (Poisson arrivals at 200/s)")
     ap.add_argument("--pool-block", type=int, default=0)
     ap.add_argument("--pool-stack", type=int, default=128)
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the learned-guiding equal-time MSE comparison")
+    ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
+    ap.add_argument("--learned-reference-spp", type=int, default=4096)
     ap.add_argument("--only", choices=["all", "guided"], default="all",
                     help="guided: only the WFPG timing (for profiling a small case)")
     ap.add_argument("--res", default="1920x1080",

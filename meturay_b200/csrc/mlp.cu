@@ -228,6 +228,20 @@ struct alignas(1024) MlpSmem {
     uint64_t mbar;
     uint32_t tmem;
     uint32_t fail;
+    __device__ unsigned char* hidden(int l) { return h[l]; }
+};
+// Inference keeps no activations for a backward pass: two hidden buffers in
+// turn (about 89 KB, two CTAs per SM).
+struct alignas(1024) MlpFwdSmem {
+    unsigned char w[kMlpImageBytes];
+    unsigned char x[kMlpTile * kMlpIn * 2];
+    unsigned char h[2][kMlpTile * 64 * 2];
+    float bias[kMlpLayers][64];
+    float dbias[kMlpLayers][64];
+    uint64_t mbar;
+    uint32_t tmem;
+    uint32_t fail;
+    __device__ unsigned char* hidden(int l) { return h[l & 1]; }
 };
 
 // TMEM columns: the 128 x 64 accumulator, then dW^T of each layer (64 rows
@@ -239,7 +253,8 @@ __host__ __device__ constexpr uint32_t col_dw(int l) {
 
 // Weights (bf16 image) and biases into shared memory, barrier init, TMEM
 // allocation by warp 0.  Returns the TMEM base address.
-__device__ __forceinline__ uint32_t mlp_prologue(MlpSmem& S, const MlpDev& m, uint32_t cols) {
+template <class SM>
+__device__ __forceinline__ uint32_t mlp_prologue(SM& S, const MlpDev& m, uint32_t cols) {
     const uint4* src = reinterpret_cast<const uint4*>(m.wImage);
     uint4* dst = reinterpret_cast<uint4*>(S.w);
     for (uint32_t i = threadIdx.x; i < kMlpImageBytes / 16; i += blockDim.x) dst[i] = src[i];
@@ -264,7 +279,8 @@ __device__ __forceinline__ uint32_t mlp_prologue(MlpSmem& S, const MlpDev& m, ui
     return S.tmem;
 }
 
-__device__ __forceinline__ void mlp_epilogue(MlpSmem& S, uint32_t tmem, uint32_t cols) {
+template <class SM>
+__device__ __forceinline__ void mlp_epilogue(SM& S, uint32_t tmem, uint32_t cols) {
     tc_fence_before();
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -274,7 +290,8 @@ __device__ __forceinline__ void mlp_epilogue(MlpSmem& S, uint32_t tmem, uint32_t
 }
 
 // One sample row of the input features into the X buffer (zeros past n).
-__device__ __forceinline__ void load_input(MlpSmem& S, const float* in, uint32_t n, uint32_t s,
+template <class SM>
+__device__ __forceinline__ void load_input(SM& S, const float* in, uint32_t n, uint32_t s,
                                            uint32_t row) {
     float v[kMlpIn];
     if (s < n) {
@@ -297,7 +314,8 @@ __device__ __forceinline__ void load_input(MlpSmem& S, const float* in, uint32_t
 // Wait for the MMAs committed to S.mbar; on expiry mark the CTA failed.
 // Every thread of the CTA calls it at the same point; the outcome is made
 // common with a block-wide vote so that no thread leaves a barrier behind.
-__device__ __forceinline__ bool mlp_wait(MlpSmem& S, uint32_t& phase, uint32_t* errorFlag) {
+template <class SM>
+__device__ __forceinline__ bool mlp_wait(SM& S, uint32_t& phase, uint32_t* errorFlag) {
     bool ok = mbar_wait(&S.mbar, phase);
     phase ^= 1u;
     ok = __syncthreads_and(ok) != 0;
@@ -319,12 +337,13 @@ __device__ __forceinline__ void read_acc(uint32_t tmem, float* v) {
 
 // Forward pass of the tile in S.x: hidden activations into S.h[0..2], the
 // output layer (bias added) into out[64].  Returns false after a failed wait.
-__device__ __forceinline__ bool forward_tile(MlpSmem& S, uint32_t tmem, uint32_t& phase,
+template <class SM>
+__device__ __forceinline__ bool forward_tile(SM& S, uint32_t tmem, uint32_t& phase,
                                              uint32_t* errorFlag, float* out) {
     const uint32_t row = threadIdx.x;
 #pragma unroll 1
     for (int l = 0; l < kMlpLayers; l++) {
-        const unsigned char* A = (l == 0) ? S.x : S.h[l - 1];
+        const unsigned char* A = (l == 0) ? S.x : S.hidden(l - 1);
         const uint32_t K = (l == 0) ? kMlpIn : 64;
         if (threadIdx.x == 0) {
             const uint32_t a0 = smem_u32(A), b0 = smem_u32(S.w + image_layer_offset(l));
@@ -345,7 +364,7 @@ __device__ __forceinline__ bool forward_tile(MlpSmem& S, uint32_t tmem, uint32_t
         if (l < kMlpLayers - 1) {
 #pragma unroll
             for (int o = 0; o < 64; o++) v[o] = fmaxf(v[o], 0.0f);
-            store_row<64>(S.h[l], row, v);
+            store_row<64>(S.hidden(l), row, v);
         } else {
 #pragma unroll
             for (int o = 0; o < 64; o++) out[o] = v[o];
@@ -358,12 +377,12 @@ __device__ __forceinline__ bool forward_tile(MlpSmem& S, uint32_t tmem, uint32_t
     return true;
 }
 
-__global__ void __launch_bounds__(kMlpTile, 1) k_mlp_forward(MlpDev m, const float* __restrict__ in,
+__global__ void __launch_bounds__(kMlpTile, 2) k_mlp_forward(MlpDev m, const float* __restrict__ in,
                                                             uint32_t maxN,
                                                             const uint32_t* __restrict__ dCount,
                                                             float* __restrict__ out) {
     extern __shared__ __align__(1024) unsigned char smemRaw[];
-    MlpSmem& S = *reinterpret_cast<MlpSmem*>(smemRaw);
+    MlpFwdSmem& S = *reinterpret_cast<MlpFwdSmem*>(smemRaw);
     const uint32_t n = dCount ? min(*dCount, maxN) : maxN;
     const uint32_t tmem = mlp_prologue(S, m, 64);
     uint32_t phase = 0;
@@ -624,7 +643,7 @@ int mlp_smem_setup() {
     MRB_CUDA(cudaGetDevice(&dev));
     if (!done[dev & 63]) {
         MRB_CUDA(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(sizeof(MlpSmem))));
+                                      int(sizeof(MlpFwdSmem))));
         MRB_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(sizeof(MlpSmem))));
         done[dev & 63] = true;
@@ -632,9 +651,10 @@ int mlp_smem_setup() {
     return 0;
 }
 
-uint32_t mlp_grid(uint32_t n) {
+uint32_t mlp_grid(uint32_t n, uint32_t perSm = 1) {
     const uint32_t tiles = (n + kMlpTile - 1) / kMlpTile;
-    return tiles < 148u ? (tiles ? tiles : 1u) : 148u;
+    const uint32_t cap = 148u * perSm;
+    return tiles < cap ? (tiles ? tiles : 1u) : cap;
 }
 
 }  // namespace
@@ -643,7 +663,7 @@ int mlp_forward(const MlpDev& m, const float* in, uint32_t n, float* out, cudaSt
                 const uint32_t* dCount) {
     if (n == 0) return 0;
     if (mlp_smem_setup()) return MRB_E_CUDA;
-    k_mlp_forward<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, n, dCount, out);
+    k_mlp_forward<<<mlp_grid(n, 2), kMlpTile, sizeof(MlpFwdSmem), st>>>(m, in, n, dCount, out);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

@@ -572,8 +572,13 @@ int step_finalize(mrb_tracer* t) {
     if (t->wfpg) {
         // WFPGTracer::Finalize: AccumulateRaidances + NormalizeAndFilterRadiance
         const GuideDev g = guide_dev(t->svo, t->svoP);
-        if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream))) return r;
-        if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
+        // the octree learns while it guides; once the network guides, the
+        // octree keeps its state as the fallback and skips the update
+        if (!learned_active(t)) {
+            if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream)))
+                return r;
+            if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
+        }
         if (t->learned && t->net &&
             (r = learned_train_frame(g, path_chain(t), t->frameWord.as<uint32_t>(), t->net,
                                      learned_scratch(t), t->learnedRate, t->stream)))
@@ -614,7 +619,7 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
         // depth, and the frame's training
         const uint32_t perDepth = learned_active(t) ? 3u
                                                     : guide_launches(t->svo, guide_options(t), t->maxRays);
-        n += guided * perDepth + 2 + 2 * t->svoP.depth;
+        n += guided * perDepth + (learned_active(t) ? 0u : 2 + 2 * t->svoP.depth);
         if (t->learned && t->net) n += learned_launches(t->learnedSteps);
     }
     return n;
