@@ -141,6 +141,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     g.set_traversal(args.traversal)
     if args.only == "guided":
         return run_guided(args, g, m, torch, dev)
+    if args.only == "learned":
+        return {"learned": run_learned(args, m, system, torch)}
     t = m.PathTracer(system, g)
     t.set_options(dict(OPTS, Seed=1 + rank))
     _attach_filter(system, t)
@@ -286,6 +288,31 @@ def _frames_image(t, frames: int) -> np.ndarray:
     return np.where(w > 0, img[..., :3] / np.where(w > 0, w, 1.0), 0.0)
 
 
+def _budget_image(t, budget_ms: float, est_ms: float, torch):
+    """rgb / w after as many frames as fit in `budget_ms` of device time on
+    the tracer's stream, cold start (octree build, warm-up frames) included;
+    frames run in chunks bracketed by CUDA events.  Returns (image, frames,
+    device ms used)."""
+    t.reset_image()
+    stream = torch.cuda.ExternalStream(t.stream)
+    used, frames, est = 0.0, 0, max(est_ms, 1e-3)
+    while budget_ms - used > 0.5 * est:
+        k = max(1, int(0.5 * (budget_ms - used) / est))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            t.render_frame()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        used += ms
+        frames += k
+        est = max(ms / k, 1e-3)
+    img = t.image().astype(np.float64)
+    w = img[..., 3:]
+    return np.where(w > 0, img[..., :3] / np.where(w > 0, w, 1.0), 0.0), frames, used
+
+
 def run_guided(args, g, m, torch, dev: int) -> dict:
     """The same frame with SVO path guiding, and the equal-time MSE of the
     guided and plain tracers against a converged plain render
@@ -341,23 +368,25 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     ref_img = _frames_image(ref, args.mse_reference_spp)
     ref.close()
     budget = float(args.mse_budget_ms)
-    plain_frames = max(1, int(budget / plain_ms))
-    guided_frames = max(1, int(budget / guided_ms))
-    plain_img = _frames_image(p, plain_frames)
+    plain_img, plain_frames, plain_used = _budget_image(p, budget, plain_ms, torch)
     gt = m.WFPGTracer(g.system, g)   # a cold cache: learning is part of the budget
     gt.set_options(dict(GUIDED_OPTS, Seed=202))
     gt.set_options(GUIDED_FLOATS)
     _attach_filter(g.system, gt)
-    guided_img = _frames_image(gt, guided_frames)
+    guided_img, guided_frames, guided_used = _budget_image(gt, budget, guided_ms, torch)
     mse_p = float(np.mean((plain_img - ref_img) ** 2))
     mse_g = float(np.mean((guided_img - ref_img) ** 2))
     out["equal_time_mse"] = {
         "budget_ms": budget, "reference_spp": args.mse_reference_spp,
-        "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "mse": mse_p},
-        "guided": {"frames": guided_frames, "ms_per_frame": guided_ms, "mse": mse_g},
+        "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "device_ms": plain_used,
+                  "mse": mse_p},
+        "guided": {"frames": guided_frames, "ms_per_frame": guided_ms,
+                   "device_ms": guided_used, "mse": mse_g},
         "guided_over_plain": mse_g / mse_p if mse_p > 0 else None,
+        "mse_x_frames": {"plain": mse_p * plain_frames, "guided": mse_g * guided_frames},
         "note": "1 spp per frame at 1920x1080; the reference is a separate plain render "
-                "(different seed); the guided tracer starts with a cold octree"}
+                "(different seed); the guided tracer starts with a cold octree, and its "
+                "build and every frame count against the budget (device time)"}
     return out
 
 
@@ -543,30 +572,33 @@ def run_learned(args, m, system, torch) -> dict:
     ref_img = _frames_image(ref, args.learned_reference_spp // 4)
     ref.close()
     out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp}
-    for kind, seed in (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14)):
+    kinds = (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14))
+    if args.learned_kinds:
+        kinds = tuple(k for k in kinds if k[0] in args.learned_kinds.split(","))
+    for kind, seed in kinds:
         probe = make(kind, seed + 100)
         for _ in range(24):           # past the warm-up: the frame time the budget meets
             probe.render_frame()
         ms = _frame_ms(probe, torch)
         probe.close()
-        frames = max(1, int(args.learned_budget_ms / ms))
         t = make(kind, seed)
-        img = _frames_image(t, frames)
-        entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames,
+        img, frames, used = _budget_image(t, args.learned_budget_ms, ms, torch)
+        entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames, "device_ms": used,
                  "mse": float(np.mean((img - ref_img) ** 2))}
         if kind.startswith("learned"):
             entry["held_out_loss_last_frame"] = t.learned_loss()
             entry["train_steps_per_frame"] = int(kind.split("_")[1])
         t.close()
         out[kind] = entry
-    best = min(("learned_1", "learned_4"), key=lambda k: out[k]["mse"])
-    out["learned"] = dict(out[best], variant=best)
-    out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
-    out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
-    # per-sample efficiency (MSE x spp; lower is better), which the frame
-    # cost then trades against
-    out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
-                        for k in ("plain", "svo", "learned_1", "learned_4")}
+    if len(kinds) == 4:
+        best = min(("learned_1", "learned_4"), key=lambda k: out[k]["mse"])
+        out["learned"] = dict(out[best], variant=best)
+        out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
+        out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
+        # per-sample efficiency (MSE x spp; lower is better), which the frame
+        # cost then trades against
+        out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
+                            for k in ("plain", "svo", "learned_1", "learned_4")}
     out["config"] = {"scene": "config-1 Cornell box (seed 1), 128x128, 4 spp per frame, depth 5",
                      **LEARNED, **LEARNED_FLOATS,
                      "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
@@ -679,8 +711,11 @@ def main():
                     help="skip the learned-guiding equal-time MSE comparison")
     ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
     ap.add_argument("--learned-reference-spp", type=int, default=4096)
-    ap.add_argument("--only", choices=["all", "guided"], default="all",
-                    help="guided: only the WFPG timing (for profiling a small case)")
+    ap.add_argument("--learned-kinds", default="",
+                    help="comma list of plain,svo,learned_1,learned_4 (default all)")
+    ap.add_argument("--only", choices=["all", "guided", "learned"], default="all",
+                    help="guided: only the WFPG timing (for profiling a small case); "
+                         "learned: only the learned-guiding comparison")
     ap.add_argument("--res", default="1920x1080",
                     help="image size WxH (the workload is 1920x1080; smaller for profiling)")
     args = ap.parse_args()

@@ -177,6 +177,7 @@ struct GuideArgs {
     const uint32_t* binBegin;
     const uint32_t* binEnd;
     const uint32_t* binCount; // headScan[maxRays]
+    uint32_t* binNext;        // bins are taken in turn from this counter (zeroed)
     uint2* guide;
     GuideOptions go;
     PathOptions opt;
@@ -201,7 +202,8 @@ struct GuideSmem {
     uint32_t repRid[kGuideWarps];
     float origin[4];
     float jitter[2];
-    uint32_t begin, end, key;
+    ConePrefix prefix;  // the descent every cone of the bin shares
+    uint32_t begin, end, key, bin;
     int nextTile;
 };
 
@@ -261,13 +263,20 @@ __global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
     const SceneDev& sc = A.sc;
     const float aperture = (4.0f * kPiF) / (static_cast<float>(X) * static_cast<float>(X));
     const uint32_t mix = hash32(frame ^ hash32(A.depthTag ^ 0xA511E9B3u ^ A.opt.seedLo));
-    for (uint32_t bin = blockIdx.x; bin < nBins; bin += gridDim.x) {
+    // bins differ widely in cost (rays, cone lengths): blocks take them in
+    // turn from a counter rather than in a fixed stride
+    for (;;) {
         if (tid == 0) {
-            S.begin = A.binBegin[bin];
-            S.end = A.binEnd[bin];
-            S.key = A.binKey[S.begin];
+            const uint32_t b = atomicAdd(A.binNext, 1u);
+            S.bin = b;
+            if (b < nBins) {
+                S.begin = A.binBegin[b];
+                S.end = A.binEnd[b];
+                S.key = A.binKey[S.begin];
+            }
         }
         __syncthreads();
+        if (S.bin >= nBins) break;
         const uint32_t begin = S.begin, end = S.end;
         // representative ray: smallest (hash(path), path) of the bin
         unsigned long long best = ~0ull;
@@ -315,6 +324,7 @@ __global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
             S.origin[1] = pos.y;
             S.origin[2] = pos.z;
             S.origin[3] = tMin;
+            S.prefix = cone_prefix(A.g, pos, tMin, aperture, 0u);
             const Rand4 rj = philox_uniform4(S.key, frame, kTagGuideBin | A.depthTag, 0u,
                                              A.opt.seedLo, A.opt.seedHi);
             S.jitter[0] = rj.u[0];
@@ -324,7 +334,8 @@ __global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
         __syncthreads();
         // GenerateRadianceField: one cone per texel of the X*X map.  Warps
         // take 8x4 texel tiles from a shared counter (neighbouring cones
-        // traverse similar nodes; fast warps take more tiles).
+        // traverse similar nodes; fast warps take more tiles); every cone
+        // starts below the bin's shared descent.
         {
             const V3 org = v3(S.origin[0], S.origin[1], S.origin[2]);
             const float tMin = S.origin[3];
@@ -344,7 +355,7 @@ __global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
                 const V3 dir = octa_to_dir_yup(s, t);
                 bool isLeaf;
                 uint32_t id;
-                cone_trace(A.g, org, dir, tMin, aperture, 0u, isLeaf, id);
+                cone_trace(A.g, org, dir, tMin, aperture, 0u, isLeaf, id, &S.prefix);
                 float r = read_radiance(A.g, dir, id, isLeaf);
                 if (r == 0.0f) r = kLargeEpsilon;
                 S.field[p] = r;
@@ -780,8 +791,9 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
     if ((r = exclusive_scan_u32(s.heads, s.headScan, w.maxRays, s.scanTemp, st))) return r;
     k_bin_ranges<<<grid, 256, 0, st>>>(s.binKey, w.count, s.heads, s.headScan, s.binBegin,
                                        s.binEnd);
+    MRB_CUDA(cudaMemsetAsync(s.binNext, 0, 4, st));
     GuideArgs ga{sc, g, w, s.binKey, s.binRid, s.binBegin, s.binEnd, s.headScan + w.maxRays,
-                 s.guide, go, opt, depthTag};
+                 s.binNext, s.guide, go, opt, depthTag};
     const uint32_t kernelIndex = iteration < 4 ? iteration : 4;
     switch (kernelIndex) {
         case 0:

@@ -39,6 +39,7 @@ struct GuideScratch {
     size_t sortTempBytes;
     void* scanTemp;
     uint2* guide;         // per ray: uv half2 | pdf half + flags
+    uint32_t* binNext;    // 1: the next bin a block of the guide kernel takes
 };
 size_t guide_sort_temp_bytes(uint32_t maxRays);
 size_t guide_scan_temp_bytes(uint32_t maxRays);

@@ -159,6 +159,7 @@ struct ChainView {
     PathChain pc;
     const uint32_t* frame;
     float weightMax;
+    uint32_t product;
 };
 
 __device__ __forceinline__ uint32_t chain_length(const PathChain& pc, uint32_t p, uint32_t frame) {
@@ -187,6 +188,9 @@ __device__ __forceinline__ bool chain_sample(const ChainView& v, uint32_t p, uin
     const V3 li = v3(tt.x > 0.0f ? sum.x / tt.x : 0.0f, tt.y > 0.0f ? sum.y / tt.y : 0.0f,
                      tt.z > 0.0f ? sum.z / tt.z : 0.0f);
     float wgt = lum3(li) / dd.w;
+    // the integrand's cosine: the mixture then learns L_in |cos| (for a
+    // diffuse vertex the ideal sampling density up to a constant)
+    if (v.product) wgt *= fabsf(nn.x * dd.x + nn.y * dd.y + nn.z * dd.z);
     if (!(wgt > 0.0f) || !(wgt < 3.0e38f)) return false;
     if (v.weightMax > 0.0f) wgt = fminf(wgt, v.weightMax);
     const float4 a = pc.nodeA[at], pa = pc.nodeA[at - P];
@@ -251,7 +255,6 @@ __global__ void k_learned_loss(const float* __restrict__ stepLoss, float* __rest
 }
 
 __global__ void k_learned_steps(const uint32_t* __restrict__ total, LearnedScratch s) {
-    if (threadIdx.x == 0) s.frameLoss[0] = s.frameLoss[1] = 0.0f;
     const uint32_t k = threadIdx.x;
     if (k >= s.steps) return;
     const uint32_t n = *total, perStep = s.capacity / s.steps;
@@ -262,13 +265,13 @@ __global__ void k_learned_steps(const uint32_t* __restrict__ total, LearnedScrat
 }  // namespace
 
 int learned_guide_wavefront(const SceneDev& sc, const GuideDev& g, const GuideWave& w,
-                            mrb_mlp* net, const LearnedScratch& s, float misRatio,
+                            const MlpDev& net, const LearnedScratch& s, float misRatio,
                             const PathOptions& opt, uint32_t depthTag, uint2* guide,
                             cudaStream_t st) {
     const uint32_t grid = grid_for(w.maxRays, 256, 148 * 8);
     k_learned_features<<<grid, 256, 0, st>>>(sc, g, w, s.features);
     MRB_CUDA(cudaGetLastError());
-    int r = mlp_forward(mlp_dev(net), s.features, w.maxRays, s.outputs, st, w.count);
+    int r = mlp_forward(net, s.features, w.maxRays, s.outputs, st, w.count);
     if (r) return r;
     k_learned_sample<<<grid, 256, 0, st>>>(sc, w, s.outputs, misRatio, opt, depthTag, guide);
     MRB_CUDA(cudaGetLastError());
@@ -282,9 +285,9 @@ uint32_t learned_launches(uint32_t steps) {
     return 6 + 4 * steps;
 }
 
-int learned_train_frame(const GuideDev& g, const PathChain& pc, const uint32_t* frame,
-                        mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st) {
-    const ChainView v{g, pc, frame, s.weightMax};
+int learned_collect(const GuideDev& g, const PathChain& pc, const uint32_t* frame,
+                    const LearnedScratch& s, cudaStream_t st) {
+    const ChainView v{g, pc, frame, s.weightMax, s.product};
     const uint32_t grid = grid_for(pc.paths, 256, 148 * 8);
     k_learned_count<<<grid, 256, 0, st>>>(v, s.pathCount);
     MRB_CUDA(cudaGetLastError());
@@ -292,6 +295,11 @@ int learned_train_frame(const GuideDev& g, const PathChain& pc, const uint32_t* 
     k_learned_write<<<grid, 256, 0, st>>>(v, s.pathOffset, s);
     k_learned_steps<<<1, 32, 0, st>>>(s.pathOffset + pc.paths, s);
     MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int learned_train(mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st) {
+    MRB_CUDA(cudaMemsetAsync(s.frameLoss, 0, 8, st));
     const uint32_t perStep = s.capacity / s.steps;
     for (uint32_t k = 0; k < s.steps; k++) {
         int r = mlp_train_step_dev(net, s.trainX + size_t(k) * perStep * kMlpIn,
@@ -300,6 +308,7 @@ int learned_train_frame(const GuideDev& g, const PathChain& pc, const uint32_t* 
         if (r) return r;
         k_learned_loss<<<1, 32, 0, st>>>(mlp_loss(net), s.frameLoss);
     }
+    MRB_CUDA(cudaGetLastError());
     return 0;
 }
 

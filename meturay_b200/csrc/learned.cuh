@@ -24,6 +24,7 @@ struct LearnedScratch {
     uint32_t steps;       // optimiser steps per frame
     float* frameLoss;     // 2: weighted loss and weight sums of the frame's batches
     float weightMax;      // training weights capped at this (0: no cap)
+    uint32_t product;     // 1: weights carry |cos| at the vertex (target L_in |cos|)
 };
 
 // Guide words for one wavefront from the network: features of every ray's
@@ -33,16 +34,20 @@ struct LearnedScratch {
 // octree sampler writes them).  Rays at specular surfaces, lights or none
 // get no guide word.
 int learned_guide_wavefront(const SceneDev& sc, const GuideDev& g, const GuideWave& w,
-                            mrb_mlp* net, const LearnedScratch& s, float misRatio,
+                            const MlpDev& net, const LearnedScratch& s, float misRatio,
                             const PathOptions& opt, uint32_t depthTag, uint2* guide,
                             cudaStream_t st);
 
-// Training samples of the frame from the path chain (every non-specular
-// vertex whose path ray carried radiance: features, the ray's direction and
-// weight lum(L_in) / pdf, L_in the radiance that arrived along it), then
-// `steps` Adam steps, step k on the samples j = k mod steps.
-int learned_train_frame(const GuideDev& g, const PathChain& pc, const uint32_t* frame,
-                        mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st);
+// Training samples of the frame from the path chain: every non-specular
+// vertex whose path ray carried radiance gives its features, the ray's
+// direction and the weight lum(L_in) / pdf (times |cos| at the vertex with
+// s.product), L_in the radiance that arrived along it.  Sample j goes to
+// step j mod steps; the per-step counts are written for learned_train.
+int learned_collect(const GuideDev& g, const PathChain& pc, const uint32_t* frame,
+                    const LearnedScratch& s, cudaStream_t st);
+// `steps` Adam steps on the collected samples, step k on its share; the
+// frame loss sums the batches' losses, each scored before its step.
+int learned_train(mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st);
 size_t learned_scan_temp_bytes(uint32_t paths);
 uint32_t learned_launches(uint32_t steps);
 

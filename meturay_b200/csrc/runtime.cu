@@ -198,11 +198,22 @@ struct mrb_tracer {
     // learned guiding: the network's mixture replaces the octree sampler
     // after learnedWarmup frames; it trains every frame from the path chains
     uint32_t learned = 0, learnedWarmup = 16, learnedSteps = 4, learnedSamples = 1u << 16;
+    uint32_t learnedProduct = 1;
+    uint32_t learnedWarmupOctree = 1;  // 0: the BxDF alone samples the warm-up frames
     uint64_t learnedSeed = 1;
     float learnedRate = 1.0e-2f, learnedWeightMax = 0.0f;
     mrb_mlp* net = nullptr;
     DBuf chainN, chainD, chainT, lFeat, lOut, lTrainX, lTrainT, lCount, lOffset, lScan, lSteps,
         lLoss, netBackup;
+    // The network trains on a side stream while the frame renders: frame f
+    // trains on frame f-1's samples and renders with the weights as they
+    // were at the start of frame f (lFwd: fp32 parameters, then the bf16
+    // weight image; refreshed after the join).
+    DBuf lFwd;
+    cudaStream_t trainStream = nullptr;
+    cudaEvent_t trainFork = nullptr, trainJoin = nullptr;
+    bool trainPending = false;  // forked in the current frame, not yet joined
+    bool learnedReset = true;   // step counts and forward image to (re)initialise
     uint32_t dumpEnabled = 0, dumpInterval = 2, iterationCount = 0, treeDumpCount = 0;
     bool svoReady = false;
     SvoParams svoP{};
@@ -219,11 +230,15 @@ struct mrb_tracer {
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
     ~mrb_tracer() {
+        if (trainStream) cudaStreamSynchronize(trainStream);
         if (net) mrb_mlp_destroy(net);
         if (svoReady) svo_free(svo);
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
         if (hostCam) cudaFreeHost(hostCam);
+        if (trainFork) cudaEventDestroy(trainFork);
+        if (trainJoin) cudaEventDestroy(trainJoin);
+        if (trainStream) cudaStreamDestroy(trainStream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -274,7 +289,7 @@ int ensure_buffers(mrb_tracer* t) {
             (r = t->binKey.alloc(size_t(maxRays) * 4)) || (r = t->binRid.alloc(size_t(maxRays) * 4)) ||
             (r = t->heads.alloc((size_t(maxRays) + 1) * 4)) ||
             (r = t->headScan.alloc((size_t(maxRays) + 1) * 4)) ||
-            (r = t->binBegin.alloc(size_t(maxRays) * 4)) || (r = t->binEnd.alloc(size_t(maxRays) * 4)) ||
+            (r = t->binBegin.alloc(size_t(maxRays) * 4)) || (r = t->binEnd.alloc((size_t(maxRays) + 1) * 4)) ||
             (r = t->guideScan.alloc(guide_scan_temp_bytes(maxRays))) ||
             (r = t->guideBuf.alloc(size_t(maxRays) * 8)))
             return r;
@@ -367,9 +382,21 @@ LearnedScratch learned_scratch(const mrb_tracer* t) {
     s.stepCount = t->lSteps.as<uint32_t>();
     s.frameLoss = t->lLoss.as<float>();
     s.weightMax = t->learnedWeightMax;
+    s.product = t->learnedProduct;
     s.steps = t->learnedSteps;
     s.capacity = t->learnedSamples / t->learnedSteps * t->learnedSteps;
     return s;
+}
+
+// The forward passes' copy of the network (parameters and weight image).
+int learned_refresh_forward(mrb_tracer* t) {
+    const MlpDev m = mlp_dev(t->net);
+    char* f = t->lFwd.as<char>();
+    MRB_CUDA(cudaMemcpyAsync(f, m.params, size_t(kMlpParams) * 4, cudaMemcpyDeviceToDevice,
+                             t->stream));
+    MRB_CUDA(cudaMemcpyAsync(f + size_t(kMlpParams) * 4, m.wImage, kMlpImageBytes,
+                             cudaMemcpyDeviceToDevice, t->stream));
+    return 0;
 }
 
 // Buffers and network of learned guiding (after ensure_buffers).
@@ -387,18 +414,67 @@ int ensure_learned(mrb_tracer* t) {
         (r = t->lOffset.alloc((size_t(t->chainPaths) + 1) * 4)) ||
         (r = t->lScan.alloc(learned_scan_temp_bytes(t->chainPaths))) ||
         (r = t->lSteps.alloc(size_t(t->learnedSteps) * 4)) || (r = t->lLoss.alloc(16)) ||
-        (r = t->netBackup.alloc(mlp_state_bytes())))
+        (r = t->netBackup.alloc(mlp_state_bytes())) || (r = t->lFwd.alloc(size_t(kMlpParams) * 4 + kMlpImageBytes)))
         return r;
+    if (!t->trainStream) {
+        MRB_CUDA(cudaStreamCreateWithFlags(&t->trainStream, cudaStreamNonBlocking));
+        MRB_CUDA(cudaEventCreateWithFlags(&t->trainFork, cudaEventDisableTiming));
+        MRB_CUDA(cudaEventCreateWithFlags(&t->trainJoin, cudaEventDisableTiming));
+    }
     if (!t->net) {
         if ((r = mrb_mlp_create(t->sys, &t->net))) return r;
         const std::vector<float> p = learned_init(t->learnedSeed);
         if ((r = mrb_mlp_set_params(t->net, p.data()))) return r;
+        t->learnedReset = true;
+    }
+    if (t->learnedReset) {
+        // no samples collected yet: the first frame's steps train on nothing
+        MRB_CUDA(cudaMemsetAsync(t->lSteps.p, 0, t->lSteps.bytes, t->stream));
+        MRB_CUDA(cudaMemsetAsync(t->lLoss.p, 0, t->lLoss.bytes, t->stream));
+        if ((r = learned_refresh_forward(t))) return r;
+        t->learnedReset = false;
     }
     return 0;
 }
 
+// The network's weights as the frame's forward passes read them.
+MlpDev learned_forward_net(const mrb_tracer* t) {
+    MlpDev m = mlp_dev(t->net);
+    m.params = t->lFwd.as<float>();
+    m.wImage = reinterpret_cast<const uint16_t*>(t->lFwd.as<char>() + size_t(kMlpParams) * 4);
+    return m;
+}
+
+// Fork the frame's training onto the side stream (once per frame).
+int learned_fork(mrb_tracer* t) {
+    if (!t->wfpg || !t->learned || !t->net || t->trainPending) return 0;
+    MRB_CUDA(cudaEventRecord(t->trainFork, t->stream));
+    MRB_CUDA(cudaStreamWaitEvent(t->trainStream, t->trainFork, 0));
+    int r = learned_train(t->net, learned_scratch(t), t->learnedRate, t->trainStream);
+    if (r) return r;
+    MRB_CUDA(cudaEventRecord(t->trainJoin, t->trainStream));
+    t->trainPending = true;
+    return 0;
+}
+
+// Join the training branch; the forward image takes the trained weights.
+int learned_join(mrb_tracer* t) {
+    if (!t->trainPending) return 0;
+    MRB_CUDA(cudaStreamWaitEvent(t->stream, t->trainJoin, 0));
+    t->trainPending = false;
+    return learned_refresh_forward(t);
+}
+
 bool learned_active(const mrb_tracer* t) {
     return t->wfpg && t->learned && t->net && t->frames >= t->learnedWarmup;
+}
+
+// The octree guides (and learns) this frame: always without learned
+// guiding; with it, during the warm-up if LearnedWarmupOctree is set.
+bool octree_guides(const mrb_tracer* t) {
+    if (!t->wfpg) return false;
+    if (!t->learned || !t->net) return true;
+    return !learned_active(t) && t->learnedWarmupOctree;
 }
 
 GuideOptions guide_options(const mrb_tracer* t) {
@@ -475,6 +551,8 @@ int trace_dispatch(const mrb_scene* sc, const float4* rayO, const float4* rayD,
 
 int step_camera(mrb_tracer* t) {
     uint32_t* cnt = t->count.as<uint32_t>();
+    int r = learned_fork(t);
+    if (r) return r;
     return camera_generate(t->devCam.as<CameraDev>(), path_options(t), t->scene->baseMedium,
                            t->rayO[0].as<float4>(),
                            t->rayD[0].as<float4>(), t->aux[0].as<RayAux>(),
@@ -523,16 +601,20 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
             return r;
     }
     if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
-    const bool guideNow = t->wfpg && !t->skipPG && d < t->guideBounce;
+    // the learned sampler skips the last depth, whose guide words no ray
+    // reads (the octree guider keeps the reference's schedule)
+    const bool guideNow = t->wfpg && !t->skipPG && d < t->guideBounce &&
+                          (learned_active(t) ? d + 1 < t->maxDepth : octree_guides(t));
     if (guideNow) {
         GuideWave gw{t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(), t->aux[cur].as<RayAux>(),
                      HitIn{ho.key, ho.prim, ho.t, ho.bary}, cnt + cur, t->maxRays};
         GuideScratch gs{t->binKey.as<uint32_t>(), t->binRid.as<uint32_t>(), t->heads.as<uint32_t>(),
                         t->headScan.as<uint32_t>(), t->binBegin.as<uint32_t>(),
                         t->binEnd.as<uint32_t>(), t->guideSort.p, t->guideSortBytes,
-                        t->guideScan.p, t->guideBuf.as<uint2>()};
+                        t->guideScan.p, t->guideBuf.as<uint2>(), t->binEnd.as<uint32_t>() + t->maxRays};
         if (learned_active(t))
-            r = learned_guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), gw, t->net,
+            r = learned_guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), gw,
+                                        learned_forward_net(t),
                                         learned_scratch(t), t->misRatio, path_options(t), d,
                                         t->guideBuf.as<uint2>(), t->stream);
         else
@@ -574,14 +656,15 @@ int step_finalize(mrb_tracer* t) {
         const GuideDev g = guide_dev(t->svo, t->svoP);
         // the octree learns while it guides; once the network guides, the
         // octree keeps its state as the fallback and skips the update
-        if (!learned_active(t)) {
+        if (octree_guides(t)) {
             if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream)))
                 return r;
             if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
         }
+        if ((r = learned_join(t))) return r;
         if (t->learned && t->net &&
-            (r = learned_train_frame(g, path_chain(t), t->frameWord.as<uint32_t>(), t->net,
-                                     learned_scratch(t), t->learnedRate, t->stream)))
+            (r = learned_collect(g, path_chain(t), t->frameWord.as<uint32_t>(),
+                                 learned_scratch(t), t->stream)))
             return r;
     }
     if (t->hasFilter)
@@ -614,12 +697,14 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
     if (t->wfpg && t->svoReady) {
         // guiding per guided depth; deposit, leaf averages and the two
         // level filters per frame
-        const uint32_t guided = t->skipPG ? 0u : std::min(t->maxDepth, t->guideBounce);
+        uint32_t guided = t->skipPG ? 0u : std::min(t->maxDepth, t->guideBounce);
+        if (learned_active(t) && guided == t->maxDepth) guided--;
+        if (!learned_active(t) && !octree_guides(t)) guided = 0;
         // learned guiding: features, forward pass and sampler per guided
         // depth, and the frame's training
         const uint32_t perDepth = learned_active(t) ? 3u
                                                     : guide_launches(t->svo, guide_options(t), t->maxRays);
-        n += guided * perDepth + (learned_active(t) ? 0u : 2 + 2 * t->svoP.depth);
+        n += guided * perDepth + (octree_guides(t) ? 2 + 2 * t->svoP.depth : 0u);
         if (t->learned && t->net) n += learned_launches(t->learnedSteps);
     }
     return n;
@@ -1249,11 +1334,17 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
         }
         if (k == "LearnedTrainSteps") t->learnedSteps = uint32_t(v);
         else t->learnedSamples = uint32_t(v);
+        t->learnedReset = true;
+    } else if (t->wfpg && k == "LearnedWarmupOctree") {
+        t->learnedWarmupOctree = v ? 1 : 0;
+    } else if (t->wfpg && k == "LearnedProductTarget") {
+        t->learnedProduct = v ? 1 : 0;
     } else if (t->wfpg && k == "LearnedSeed") {
         t->learnedSeed = v;
         if (t->net) {
             const std::vector<float> p = learned_init(v);
             if (mrb_mlp_set_params(t->net, p.data())) return MRB_E_CUDA;
+            t->learnedReset = true;
         }
     } else if (t->wfpg && k == "PGDumpDataStruct") {
         t->dumpEnabled = v ? 1 : 0;
@@ -1386,6 +1477,8 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
     if (r) return r;
     if ((r = ensure_svo(t))) return r;
     if ((r = ensure_learned(t))) return r;
+    // a training branch left open by the step-wise calls ends first
+    if ((r = learned_join(t))) return r;
     // the captured frame bakes in which sampler guides: capture again when
     // the network takes over
     if (t->wfpg && t->learned && t->frames == t->learnedWarmup) t->graphDirty = true;
@@ -1413,6 +1506,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, true, t->stream)) return MRB_E_CUDA;
         if ((r = record_frame(t))) return r;
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, false, t->stream)) return MRB_E_CUDA;
+        if (t->net && (r = learned_refresh_forward(t))) return r;
         MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f0, 4, cudaMemcpyHostToDevice, t->stream));
         if (pb) {
             const char* b = t->payloadBackup.as<char>();

@@ -384,9 +384,103 @@ __device__ __forceinline__ float neg_exp2i(uint32_t p) {  // 2^-p for p <= 126
 // add/subtract pair of the reference changes nothing and the operations
 // that reach tMin are the same.  The voxel size test uses a per-level
 // table of the same products.
-__device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, float tMin,
-                                            float aperture, uint32_t maxQueryLevelOffset,
-                                            bool& isLeaf, uint32_t& leafId) {
+// The descent that every cone from one origin shares.  At the start of a
+// trace, tMin moves only when a cone skips an empty child, so while the
+// point origin + dir * tMin lies on the same side of each centre plane for
+// every direction, each cone takes the same children as a descent by the
+// origin alone.  "Same side for every direction" means the origin is
+// farther than |dir| * tMin from each plane in the normalised frame (|dir|
+// at most the largest axis scale), plus a slack far above the rounding of
+// the cone's own plane crossings (a few ulps of values in [0, 1]).  The
+// prefix stops before the first level where that fails, where the child is
+// empty, or where the descent would terminate.  A termination that every
+// cone reaches on the shared path (leaf child, or a voxel smaller than the
+// cone's footprint at the common tMin) is recorded as the result of every
+// cone.  The cone then starts at the prefix's node with the corner and
+// Morton stack its own descent would have built (mirrored per direction:
+// the corner 1 - c - span, the stack bits xor the mirror mask), both exact
+// in binary32 since they are dyadic with at most leafDepth bits.
+struct ConePrefix {
+    uint32_t nodeId;     // node reached (0: no shared descent)
+    uint32_t depth;      // its level
+    uint32_t stack;      // child ids on the way down, unmirrored, 3 bits each
+    float corner[3];     // its minimum corner in the normalised frame
+    uint32_t termId;     // with `term`: the node every cone stops at
+    uint32_t term;       // 1: every cone stops at termId
+    uint32_t termLeaf;   // ... which is a leaf
+};
+
+__device__ __forceinline__ float level_voxel_size_sqr(const GuideDev& g, uint32_t level) {
+    const uint32_t sh = (level <= g.leafDepth) ? g.leafDepth - level : 0u;
+    const float vs = g.leafVoxelSize * static_cast<float>(1u << sh);
+    return vs * vs;
+}
+
+__device__ __forceinline__ ConePrefix cone_prefix(const GuideDev& g, V3 pos, float tMin,
+                                                  float aperture, uint32_t maxQueryLevelOffset) {
+    ConePrefix P{};
+    const V3 sc = v3(1.0f / (g.hi[0] - g.lo[0]), 1.0f / (g.hi[1] - g.lo[1]),
+                     1.0f / (g.hi[2] - g.lo[2]));
+    const V3 p = (pos + v3(-g.lo[0], -g.lo[1], -g.lo[2])) * sc;
+    const float pa[3] = {p.x, p.y, p.z};
+    const float scMax = fmaxf(fmaxf(sc.x, sc.y), sc.z);
+    const float margin = tMin * scMax * 1.0001f + 4.0e-6f;
+    if (!(margin < 0.25f)) return P;
+    for (int a = 0; a < 3; a++)
+        if (!(pa[a] > margin && pa[a] < 1.0f - margin)) return P;
+    float corner[3] = {0.0f, 0.0f, 0.0f};
+    uint32_t nodeId = 0, stack = 0;
+    const float area = tMin * tMin * aperture;
+    const float diam2 = 4.0f * (area * kInvPiF);
+    for (uint32_t level = 0; level < g.leafDepth; level++) {
+        const float half = neg_exp2i(level + 1);
+        uint32_t c = 0;
+        for (int a = 0; a < 3; a++) {
+            const float ctr = corner[a] + half;
+            if (!(fabsf(pa[a] - ctr) > margin)) return P;
+            if (pa[a] > ctr) c |= 1u << a;
+        }
+        const uint64_t node = g.nodes[nodeId];
+        if (!((svo_mask(node) >> c) & 1u)) return P;
+        const uint32_t child = svo_child_index(node) + svo_child_offset(node, c);
+        const uint32_t lvl = level + 1;
+        const bool childLeaf = svo_children_leaf(node);
+        const bool term = diam2 > level_voxel_size_sqr(g, lvl) ||
+                          (g.leafDepth - lvl) <= maxQueryLevelOffset;
+        if (childLeaf || term) {
+            P.term = 1;
+            P.termLeaf = childLeaf ? 1u : 0u;
+            P.termId = child;
+            return P;
+        }
+        for (int a = 0; a < 3; a++)
+            if ((c >> a) & 1u) corner[a] += half;
+        stack = (stack << 3) | c;
+        nodeId = child;
+        P.nodeId = nodeId;
+        P.depth = lvl;
+        P.stack = stack;
+        P.corner[0] = corner[0];
+        P.corner[1] = corner[1];
+        P.corner[2] = corner[2];
+    }
+    return P;
+}
+
+// The trace in two parts: cone_begin is the setup before the loop,
+// cone_step one iteration of it.  The Morton stack holds at
+// most leafDepth <= 10 levels of 3 bits.
+struct ConeState {
+    V3 dc, pb, corner;
+    float tMin;
+    uint32_t mirror, stack, depth, nodeId, step;
+};
+
+// True when the trace has already ended (NaN input, or a termination that
+// the prefix shares); isLeaf / leafId then hold the result.
+__device__ __forceinline__ bool cone_begin(const GuideDev& g, V3 pos, V3 dir, float tMin,
+                                           const ConePrefix* pre, ConeState& s, bool& isLeaf,
+                                           uint32_t& leafId) {
     const float EPS = 1.0e-5f;
     leafId = kInvalid;
     isLeaf = false;
@@ -397,8 +491,9 @@ __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, f
                      1.0f / (g.hi[2] - g.lo[2]));
     V3 d = dir * sc;
     V3 p = (pos + v3(-g.lo[0], -g.lo[1], -g.lo[2])) * sc;
+    s.tMin = tMin;
     if (!(d.x == d.x && d.y == d.y && d.z == d.z && p.x == p.x && p.y == p.y && p.z == p.z))
-        return tMin;
+        return true;
     p.x = (d.x < 0.0f) ? (1.0f - p.x) : p.x;
     p.y = (d.y < 0.0f) ? (1.0f - p.y) : p.y;
     p.z = (d.z < 0.0f) ? (1.0f - p.z) : p.z;
@@ -406,80 +501,115 @@ __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, f
     if (d.x < 0.0f) mirror |= 1u;
     if (d.y < 0.0f) mirror |= 2u;
     if (d.z < 0.0f) mirror |= 4u;
-    const V3 dc = v3(1.0f / fabsf(d.x), 1.0f / fabsf(d.y), 1.0f / fabsf(d.z));
-    const V3 pb = p * dc;
+    s.mirror = mirror;
+    s.dc = v3(1.0f / fabsf(d.x), 1.0f / fabsf(d.y), 1.0f / fabsf(d.z));
+    s.pb = p * s.dc;
     {
-        const V3 t0 = -pb;
+        const V3 t0 = -s.pb;
         const float tSvo = fmaxf(fmaxf(t0.x, t0.y), t0.z);
-        if (!(t0.x < tMin && t0.y < tMin && t0.z < tMin)) tMin = next_up(tSvo);
+        if (!(t0.x < s.tMin && t0.y < s.tMin && t0.z < s.tMin)) s.tMin = next_up(tSvo);
     }
-    // squared voxel size of each level (ConeDiameterSqr's comparand)
-    float vs2[11];
-#pragma unroll
-    for (int L = 0; L <= 10; L++) {
-        const uint32_t sh = (static_cast<uint32_t>(L) <= g.leafDepth) ? g.leafDepth - L : 0u;
-        const float vs = g.leafVoxelSize * static_cast<float>(1u << sh);
-        vs2[L] = vs * vs;
-    }
-    uint64_t stack = 0;
-    uint32_t depthBits = 0;
-    uint32_t nodeId = 0;
-    V3 corner = v3(0.0f, 0.0f, 0.0f);
-    for (uint32_t step = 0; nodeId != kSvoInvalidParent; step++) {
-        if (step == kConeTraceMaxSteps) {
-            leafId = kInvalid;
-            isLeaf = false;
-            break;
+    s.stack = 0;
+    s.depth = 0;
+    s.nodeId = 0;
+    s.step = 0;
+    s.corner = v3(0.0f, 0.0f, 0.0f);
+    if (pre) {
+        if (pre->term) {
+            isLeaf = pre->termLeaf != 0;
+            leafId = pre->termId;
+            return true;
         }
-        const float childSpan = neg_exp2i(depthBits + 1);
-        const float curSpan = neg_exp2i(depthBits);
-        const V3 topRight = corner + v3(curSpan, curSpan, curSpan);
-        const V3 tm = topRight * dc - pb;
-        const float tMax = fminf(fminf(tm.x, tm.y), tm.z);
-        const uint64_t node = g.nodes[nodeId];
-        if (tMax < tMin) {
-            const uint32_t b = uint32_t(stack & 7u);
-            corner = corner - v3((b & 1u) ? curSpan : 0.0f, (b & 2u) ? curSpan : 0.0f,
+        if (pre->depth) {
+            const float span = neg_exp2i(pre->depth);
+            s.corner = v3((mirror & 1u) ? 1.0f - pre->corner[0] - span : pre->corner[0],
+                          (mirror & 2u) ? 1.0f - pre->corner[1] - span : pre->corner[1],
+                          (mirror & 4u) ? 1.0f - pre->corner[2] - span : pre->corner[2]);
+            uint32_t pattern = 0;
+            for (uint32_t j = 0; j < pre->depth; j++) pattern = (pattern << 3) | mirror;
+            s.stack = pre->stack ^ pattern;
+            s.depth = pre->depth;
+            s.nodeId = pre->nodeId;
+            s.step = pre->depth;
+        }
+    }
+    return false;
+}
+
+// One iteration of the reference's loop.  The empty-child skip takes the
+// child's exit crossings from values the iteration already has: per axis
+// the child's far plane is the node's far plane (child bit set: corner +
+// span/2 + span/2 = corner + span, exact for these dyadic corners) or its
+// centre plane, so the crossings are tm or tc, value for value.  True when
+// the trace has ended.
+__device__ __forceinline__ bool cone_step(const GuideDev& g, float aperture,
+                                          uint32_t maxQueryLevelOffset, ConeState& s,
+                                          bool& isLeaf, uint32_t& leafId) {
+    if (s.step == kConeTraceMaxSteps) {
+        leafId = kInvalid;
+        isLeaf = false;
+        return true;
+    }
+    s.step++;
+    const float childSpan = neg_exp2i(s.depth + 1);
+    const float curSpan = neg_exp2i(s.depth);
+    const V3 topRight = s.corner + v3(curSpan, curSpan, curSpan);
+    const V3 tm = topRight * s.dc - s.pb;
+    const float tMax = fminf(fminf(tm.x, tm.y), tm.z);
+    const uint64_t node = g.nodes[s.nodeId];
+    if (tMax < s.tMin) {
+        const uint32_t b = s.stack & 7u;
+        s.corner = s.corner - v3((b & 1u) ? curSpan : 0.0f, (b & 2u) ? curSpan : 0.0f,
                                  (b & 4u) ? curSpan : 0.0f);
-            stack >>= 3;
-            depthBits -= 1;
-            nodeId = svo_parent(node);
-            continue;
-        }
-        const V3 center = corner + v3(childSpan, childSpan, childSpan);
-        const V3 tc = center * dc - pb;
-        uint32_t childId = 0;
-        if (tc.x < tMin) childId |= 1u;
-        if (tc.y < tMin) childId |= 2u;
-        if (tc.z < tMin) childId |= 4u;
-        const uint32_t mir = childId ^ mirror;
-        const V3 childCorner = corner + v3((childId & 1u) ? childSpan : 0.0f,
-                                           (childId & 2u) ? childSpan : 0.0f,
-                                           (childId & 4u) ? childSpan : 0.0f);
-        if (!((svo_mask(node) >> mir) & 1u)) {
-            // empty child: leave it at once
-            const V3 ctr = childCorner + v3(childSpan, childSpan, childSpan);
-            const V3 ct = ctr * dc - pb;
-            tMin = next_up(fminf(fminf(ct.x, ct.y), ct.z));
-            continue;
-        }
-        nodeId = svo_child_index(node) + svo_child_offset(node, mir);
-        const uint32_t level = depthBits + 1;
-        const float area = tMin * tMin * aperture;
-        const float diam2 = 4.0f * (area * kInvPiF);
-        bool term = diam2 > vs2[level];
-        const bool childLeaf = svo_children_leaf(node);
-        term |= (g.leafDepth - level) <= maxQueryLevelOffset;
-        if (childLeaf || term) {
-            isLeaf = childLeaf;
-            leafId = nodeId;
-            break;
-        }
-        corner = childCorner;
-        stack = (stack << 3) | childId;
-        depthBits += 1;
+        s.stack >>= 3;
+        s.depth -= 1;
+        s.nodeId = svo_parent(node);
+        return s.nodeId == kSvoInvalidParent;  // left the tree: a miss
     }
-    return tMin;
+    const V3 center = s.corner + v3(childSpan, childSpan, childSpan);
+    const V3 tc = center * s.dc - s.pb;
+    uint32_t childId = 0;
+    if (tc.x < s.tMin) childId |= 1u;
+    if (tc.y < s.tMin) childId |= 2u;
+    if (tc.z < s.tMin) childId |= 4u;
+    const uint32_t mir = childId ^ s.mirror;
+    if (!((svo_mask(node) >> mir) & 1u)) {
+        // empty child: leave it at once
+        const float ex = (childId & 1u) ? tm.x : tc.x;
+        const float ey = (childId & 2u) ? tm.y : tc.y;
+        const float ez = (childId & 4u) ? tm.z : tc.z;
+        s.tMin = next_up(fminf(fminf(ex, ey), ez));
+        return false;
+    }
+    const uint32_t child = svo_child_index(node) + svo_child_offset(node, mir);
+    const uint32_t level = s.depth + 1;
+    const float area = s.tMin * s.tMin * aperture;
+    const float diam2 = 4.0f * (area * kInvPiF);
+    bool term = diam2 > level_voxel_size_sqr(g, level);
+    const bool childLeaf = svo_children_leaf(node);
+    term |= (g.leafDepth - level) <= maxQueryLevelOffset;
+    if (childLeaf || term) {
+        isLeaf = childLeaf;
+        leafId = child;
+        return true;
+    }
+    s.nodeId = child;
+    s.corner = s.corner + v3((childId & 1u) ? childSpan : 0.0f, (childId & 2u) ? childSpan : 0.0f,
+                             (childId & 4u) ? childSpan : 0.0f);
+    s.stack = (s.stack << 3) | childId;
+    s.depth = level;
+    return false;
+}
+
+__device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, float tMin,
+                                            float aperture, uint32_t maxQueryLevelOffset,
+                                            bool& isLeaf, uint32_t& leafId,
+                                            const ConePrefix* pre = nullptr) {
+    ConeState s;
+    if (cone_begin(g, pos, dir, tMin, pre, s, isLeaf, leafId)) return s.tMin;
+    while (!cone_step(g, aperture, maxQueryLevelOffset, s, isLeaf, leafId)) {
+    }
+    return s.tMin;
 }
 
 // AnisoSVOctreeGPU::FindMarkedBin (AnisoSVO.cuh:1244-1262): walk up from

@@ -355,7 +355,8 @@ class WFPGTracer(PathTracer):
         "OctreeLevel", "MinRayBinLevel", "BinRayCount", "DoProductPathGuiding", "PurePG",
         "SkipPG", "GuideBounceAmount", "OmitDirectRadiance", "PGDumpDataStruct",
         "PGDataStructDumpIntervalExp", "LearnedGuiding", "LearnedWarmupFrames",
-        "LearnedTrainSteps", "LearnedSamples", "LearnedSeed")
+        "LearnedTrainSteps", "LearnedSamples", "LearnedSeed", "LearnedProductTarget",
+        "LearnedWarmupOctree")
     FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha", "LearnedRate", "LearnedWeightMax")
     STRING_KEYS = ("InitialSVO", "PGDataStructDumpName")
 
