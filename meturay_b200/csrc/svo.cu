@@ -42,10 +42,20 @@ struct V2 {
 };
 __device__ __forceinline__ V3 cross3(V3 a, V3 b) { return cross(a, b); }
 
-// TriFunctions::Voxelize (GPUPrimitiveTriangle.h:385-620), one triangle.
-// Writes up to `maxOut` voxels when codes != nullptr; returns the count.
-__device__ uint32_t voxelize_tri(const SvoParams& P, V3 p0, V3 p1, V3 p2, uint64_t* codes,
-                                 uint32_t* normals, uint32_t maxOut) {
+// TriFunctions::Voxelize (GPUPrimitiveTriangle.h:385-620), split into the
+// per-triangle setup and one raster row, so that the rows of a large
+// triangle run on separate threads.  Voxels of a triangle come out in the
+// reference's order, rows bottom-up and pixels left to right; the row
+// offsets of the build keep that order in the voxel array.
+struct TriRaster {
+    V2 q2[3], c0, ec0, ec1, e0, e1;
+    V3 p0, p1, p2;
+    float denomC, denom, deltaPix, res;
+    uint32_t packedNormal;
+    int x0, x1, y0, y1;
+};
+
+__device__ TriRaster tri_setup(const SvoParams& P, V3 p0, V3 p1, V3 p2) {
     const V3 pos[3] = {p0, p1, p2};
     const V3 normal = normalize(cross(p1 - p0, p2 - p0));
     const float an[3] = {fabsf(normal.x), fabsf(normal.y), fabsf(normal.z)};
@@ -118,36 +128,68 @@ __device__ uint32_t voxelize_tri(const SvoParams& P, V3 p0, V3 p1, V3 p2, uint64
     const float denomC = 1.0f / (ec0.x * ec1.y - ec1.x * ec0.y);
     const V2 e0 = {q2[1].x - q2[0].x, q2[1].y - q2[0].y}, e1 = {q2[2].x - q2[0].x, q2[2].y - q2[0].y};
     const float denom = 1.0f / (e0.x * e1.y - e1.x * e0.y);
+    TriRaster R;
+    for (int i = 0; i < 3; i++) R.q2[i] = q2[i];
+    R.c0 = c0;
+    R.ec0 = ec0;
+    R.ec1 = ec1;
+    R.e0 = e0;
+    R.e1 = e1;
+    R.p0 = p0;
+    R.p1 = p1;
+    R.p2 = p2;
+    R.denomC = denomC;
+    R.denom = denom;
+    R.deltaPix = deltaPix;
+    R.res = res;
+    R.packedNormal = packedNormal;
+    R.x0 = x0;
+    R.x1 = x1;
+    R.y0 = y0;
+    R.y1 = y1;
+    return R;
+}
+
+// Rows of the triangle's pixel rectangle (0 when it has no columns).
+__device__ __forceinline__ uint32_t tri_rows(const TriRaster& R) {
+    return (R.x1 > R.x0 && R.y1 > R.y0) ? uint32_t(R.y1 - R.y0) : 0u;
+}
+
+// Row y of the triangle: writes up to `maxOut` voxels when codes !=
+// nullptr; returns the row's count.
+__device__ uint32_t tri_row(const SvoParams& P, const TriRaster& R, int y, uint64_t* codes,
+                            uint32_t* normals, uint32_t maxOut) {
+    const V2 c0 = R.c0, ec0 = R.ec0, ec1 = R.ec1, e0 = R.e0, e1 = R.e1;
+    const float denomC = R.denomC, denom = R.denom, deltaPix = R.deltaPix, res = R.res;
     uint32_t w = 0;
-    for (int y = y0; y < y1; y++)
-        for (int x = x0; x < x1; x++) {
-            const V2 p = {(static_cast<float>(x) + 0.5f) * deltaPix - 1.0f,
-                          (static_cast<float>(y) + 0.5f) * deltaPix - 1.0f};
-            const V2 ec2 = {p.x - c0.x, p.y - c0.y};
-            const float bb = (ec2.x * ec1.y - ec1.x * ec2.y) * denomC;
-            const float cc = (ec0.x * ec2.y - ec2.x * ec0.y) * denomC;
-            const float aa = 1.0f - bb - cc;
-            if (!(bb >= 0.0f && bb <= 1.0f && cc >= 0.0f && cc <= 1.0f && aa >= 0.0f && aa <= 1.0f))
-                continue;
-            if (codes && w < maxOut) {
-                const V2 e2 = {p.x - q2[0].x, p.y - q2[0].y};
-                const float ab = (e2.x * e1.y - e1.x * e2.y) * denom;
-                const float ac = (e0.x * e2.y - e2.x * e0.y) * denom;
-                const float aA = 1.0f - ab - ac;
-                const V3 vp = (p0 * aA + p1 * ab) + p2 * ac;
-                uint32_t vi[3];
-                const float vpc[3] = {vp.x, vp.y, vp.z};
-                for (int k = 0; k < 3; k++) {
-                    float fi = (vpc[k] - P.lo[k]) / (P.hi[k] - P.lo[k]);
-                    fi *= res;
-                    uint32_t q = fi > 0.0f ? static_cast<uint32_t>(fi) : 0u;
-                    vi[k] = q > P.res - 1 ? P.res - 1 : q;
-                }
-                codes[w] = expand3d(vi[0]) | (expand3d(vi[1]) << 1) | (expand3d(vi[2]) << 2);
-                normals[w] = packedNormal;
+    for (int x = R.x0; x < R.x1; x++) {
+        const V2 p = {(static_cast<float>(x) + 0.5f) * deltaPix - 1.0f,
+                      (static_cast<float>(y) + 0.5f) * deltaPix - 1.0f};
+        const V2 ec2 = {p.x - c0.x, p.y - c0.y};
+        const float bb = (ec2.x * ec1.y - ec1.x * ec2.y) * denomC;
+        const float cc = (ec0.x * ec2.y - ec2.x * ec0.y) * denomC;
+        const float aa = 1.0f - bb - cc;
+        if (!(bb >= 0.0f && bb <= 1.0f && cc >= 0.0f && cc <= 1.0f && aa >= 0.0f && aa <= 1.0f))
+            continue;
+        if (codes && w < maxOut) {
+            const V2 e2 = {p.x - R.q2[0].x, p.y - R.q2[0].y};
+            const float ab = (e2.x * e1.y - e1.x * e2.y) * denom;
+            const float ac = (e0.x * e2.y - e2.x * e0.y) * denom;
+            const float aA = 1.0f - ab - ac;
+            const V3 vp = (R.p0 * aA + R.p1 * ab) + R.p2 * ac;
+            uint32_t vi[3];
+            const float vpc[3] = {vp.x, vp.y, vp.z};
+            for (int k = 0; k < 3; k++) {
+                float fi = (vpc[k] - P.lo[k]) / (P.hi[k] - P.lo[k]);
+                fi *= res;
+                uint32_t q = fi > 0.0f ? static_cast<uint32_t>(fi) : 0u;
+                vi[k] = q > P.res - 1 ? P.res - 1 : q;
             }
-            w++;
+            codes[w] = expand3d(vi[0]) | (expand3d(vi[1]) << 1) | (expand3d(vi[2]) << 2);
+            normals[w] = R.packedNormal;
         }
+        w++;
+    }
     return w;
 }
 
@@ -159,25 +201,52 @@ __device__ __forceinline__ void tri_pos(const SvoBuildIn& in, uint32_t t, V3& a,
     c = ld3(in.pos + 3 * size_t(i2));
 }
 
-__global__ void __launch_bounds__(128) k_voxel_count(SvoBuildIn in, SvoParams P, uint32_t* counts) {
+__global__ void __launch_bounds__(128) k_tri_rows(SvoBuildIn in, SvoParams P, uint32_t* rows) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < in.triCount;
          t += gridDim.x * blockDim.x) {
         V3 a, b, c;
         tri_pos(in, t, a, b, c);
-        counts[t] = voxelize_tri(P, a, b, c, nullptr, nullptr, 0);
+        rows[t] = tri_rows(tri_setup(P, a, b, c));
     }
 }
 
-__global__ void __launch_bounds__(128) k_voxelize(SvoBuildIn in, SvoParams P,
-                                                  const uint32_t* __restrict__ offsets,
-                                                  uint64_t* codes, uint32_t* normals,
-                                                  uint32_t* lightKeys) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < in.triCount;
-         t += gridDim.x * blockDim.x) {
+// The triangle of every row: row r of the flat list belongs to triangle t
+// for rowStart[t] <= r < rowStart[t + 1].
+__global__ void __launch_bounds__(256) k_row_tri(const uint32_t* __restrict__ rowStart, uint32_t T,
+                                                 uint32_t* __restrict__ rowTri) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
+        for (uint32_t r = rowStart[t]; r < rowStart[t + 1]; r++) rowTri[r] = t;
+}
+
+__global__ void __launch_bounds__(128) k_row_count(SvoBuildIn in, SvoParams P,
+                                                   const uint32_t* __restrict__ rowStart,
+                                                   const uint32_t* __restrict__ rowTri,
+                                                   uint32_t rowsTotal, uint32_t* counts) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rowsTotal;
+         r += gridDim.x * blockDim.x) {
+        const uint32_t t = rowTri[r];
         V3 a, b, c;
         tri_pos(in, t, a, b, c);
-        const uint32_t o = offsets[t], cnt = offsets[t + 1] - o;
-        voxelize_tri(P, a, b, c, codes + o, normals + o, cnt);
+        const TriRaster R = tri_setup(P, a, b, c);
+        counts[r] = tri_row(P, R, R.y0 + int(r - rowStart[t]), nullptr, nullptr, 0);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_row_voxelize(SvoBuildIn in, SvoParams P,
+                                                      const uint32_t* __restrict__ rowStart,
+                                                      const uint32_t* __restrict__ rowTri,
+                                                      uint32_t rowsTotal,
+                                                      const uint32_t* __restrict__ offsets,
+                                                      uint64_t* codes, uint32_t* normals,
+                                                      uint32_t* lightKeys) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rowsTotal;
+         r += gridDim.x * blockDim.x) {
+        const uint32_t t = rowTri[r];
+        V3 a, b, c;
+        tri_pos(in, t, a, b, c);
+        const TriRaster R = tri_setup(P, a, b, c);
+        const uint32_t o = offsets[r], cnt = offsets[r + 1] - o;
+        tri_row(P, R, R.y0 + int(r - rowStart[t]), codes + o, normals + o, cnt);
         const uint32_t key = in.key[t];
         const uint32_t lk = ((key >> kIdBits) == kBatchLight) ? key : 0u;
         for (uint32_t i = 0; i < cnt; i++) lightKeys[o + i] = lk;
@@ -389,15 +458,29 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
         temps.clear();
     };
     int r = 0;
-    // 1. voxel counts, offsets, voxelisation
-    uint32_t* counts = static_cast<uint32_t*>(tmp(size_t(T) * 4));
-    uint32_t* offsets = static_cast<uint32_t*>(tmp((size_t(T) + 1) * 4));
-    void* scanTmp = tmp(exclusive_scan_temp_bytes(T + 1) + exclusive_scan_temp_bytes(1u << 26));
-    if (!counts || !offsets || !scanTmp) { cleanup(); return MRB_E_OOM; }
-    k_voxel_count<<<grid_of(T), 128, 0, st>>>(in, P, counts);
-    if ((r = exclusive_scan_u32(counts, offsets, T, scanTmp, st))) { cleanup(); return r; }
+    // 1. raster rows of every triangle, voxel counts per row, voxelisation
+    // (rows in triangle order, so the voxel array keeps the per-triangle
+    // order of the reference)
+    uint32_t* rows = static_cast<uint32_t*>(tmp(size_t(T) * 4));
+    uint32_t* rowStart = static_cast<uint32_t*>(tmp((size_t(T) + 1) * 4));
+    void* scanTmp = tmp(exclusive_scan_temp_bytes(T + 1));
+    if (!rows || !rowStart || !scanTmp) { cleanup(); return MRB_E_OOM; }
+    k_tri_rows<<<grid_of(T), 128, 0, st>>>(in, P, rows);
+    if ((r = exclusive_scan_u32(rows, rowStart, T, scanTmp, st))) { cleanup(); return r; }
+    uint32_t rowsTotal = 0;
+    MRB_CUDA(cudaMemcpyAsync(&rowsTotal, rowStart + T, 4, cudaMemcpyDeviceToHost, st));
+    MRB_CUDA(cudaStreamSynchronize(st));
+    if (rowsTotal == 0) { cleanup(); set_error("SVO: no voxels"); return MRB_E_ARG; }
+    uint32_t* rowTri = static_cast<uint32_t*>(tmp(size_t(rowsTotal) * 4));
+    uint32_t* counts = static_cast<uint32_t*>(tmp(size_t(rowsTotal) * 4));
+    uint32_t* offsets = static_cast<uint32_t*>(tmp((size_t(rowsTotal) + 1) * 4));
+    void* scanRows = tmp(exclusive_scan_temp_bytes(rowsTotal + 1));
+    if (!rowTri || !counts || !offsets || !scanRows) { cleanup(); return MRB_E_OOM; }
+    k_row_tri<<<grid_of(T), 256, 0, st>>>(rowStart, T, rowTri);
+    k_row_count<<<grid_of(rowsTotal), 128, 0, st>>>(in, P, rowStart, rowTri, rowsTotal, counts);
+    if ((r = exclusive_scan_u32(counts, offsets, rowsTotal, scanRows, st))) { cleanup(); return r; }
     uint32_t total = 0;
-    MRB_CUDA(cudaMemcpyAsync(&total, offsets + T, 4, cudaMemcpyDeviceToHost, st));
+    MRB_CUDA(cudaMemcpyAsync(&total, offsets + rowsTotal, 4, cudaMemcpyDeviceToHost, st));
     MRB_CUDA(cudaStreamSynchronize(st));
     if (total == 0) { cleanup(); set_error("SVO: no voxels"); return MRB_E_ARG; }
     if (total > (1u << 27)) { cleanup(); set_error("SVO: %u voxels exceed 2^27", total); return MRB_E_ARG; }
@@ -414,7 +497,8 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
         cleanup();
         return MRB_E_OOM;
     }
-    k_voxelize<<<grid_of(T), 128, 0, st>>>(in, P, offsets, codes, vnorm, vlight);
+    k_row_voxelize<<<grid_of(rowsTotal), 128, 0, st>>>(in, P, rowStart, rowTri, rowsTotal, offsets,
+                                                       codes, vnorm, vlight);
     k_iota<<<grid_of(total), 256, 0, st>>>(vidx, total);
     // 2. sort on bits [0, 3*depth + 1) and run-length encode
     if ((r = radix_sort_pairs<uint64_t>(codes, vidx, nullptr, total, 0, int(3 * P.depth + 1), false,
