@@ -220,6 +220,7 @@ struct mrb_tracer {
     SvoResult svo;
     DBuf chainA, chainB, chainNee, chainPath, binKey, binRid, heads, headScan, binBegin, binEnd,
         guideSort, guideScan, guideBuf, payloadBackup;
+    DBuf imageBackup;  // image and ray counters around the eager frame of a capture
     size_t guideSortBytes = 0;
     uint32_t chainPaths = 0, chainLevels = 0;
     // reconstruction filter (AttachReconFilter); image coordinates per sample
@@ -1488,8 +1489,15 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             t->graph = nullptr;
         }
         // run one frame eagerly first so that one-time setup (kernel
-        // attributes) happens outside the capture, then rewind the frame
+        // attributes) happens outside the capture, then rewind the frame:
+        // frame word, octree radiance, network state, the accumulated image
+        // and the ray counters are put back
         uint32_t f0 = 0;
+        if ((r = t->imageBackup.alloc(t->image.bytes + 16))) return r;
+        MRB_CUDA(cudaMemcpyAsync(t->imageBackup.p, t->image.p, t->image.bytes,
+                                 cudaMemcpyDeviceToDevice, t->stream));
+        MRB_CUDA(cudaMemcpyAsync(t->imageBackup.as<char>() + t->image.bytes, t->counters.p, 16,
+                                 cudaMemcpyDeviceToDevice, t->stream));
         MRB_CUDA(cudaMemcpyAsync(&f0, t->frameWord.p, 4, cudaMemcpyDeviceToHost, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
         // the octree's radiance state of a WFPG tracer is put back too
@@ -1515,7 +1523,10 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             MRB_CUDA(cudaMemcpyAsync(t->svo.leafAvg, b + U * 24, U * 4, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(t->svo.nodeAvg, b + U * 28, N * 4, cudaMemcpyDeviceToDevice, t->stream));
         }
-        MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
+        MRB_CUDA(cudaMemcpyAsync(t->image.p, t->imageBackup.p, t->image.bytes,
+                                 cudaMemcpyDeviceToDevice, t->stream));
+        MRB_CUDA(cudaMemcpyAsync(t->counters.p, t->imageBackup.as<char>() + t->image.bytes, 16,
+                                 cudaMemcpyDeviceToDevice, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
         cudaGraph_t g = nullptr;
         MRB_CUDA(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));

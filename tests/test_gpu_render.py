@@ -157,3 +157,24 @@ def test_scene_file_renders_like_the_oracle(system, oracle):
     assert rays == ref_rays
     assert gpu.sum() > 0
     assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
+
+
+def test_recapture_keeps_the_accumulated_image(system):
+    """Changing an option re-captures the frame graph; the eager frame that
+    precedes the capture is rewound, and the image and ray counters keep the
+    frames rendered before it."""
+    from meturay_b200 import scenes
+    scene = scenes.cornell(seed=1, width=32, height=32)
+    opts = dict(CORNELL_OPTS, Seed=3)
+    _, t = _setup(system, scene, opts)
+    _, u = _setup(system, scene, opts)
+    for _ in range(3):
+        t.render_frame()
+        u.render_frame()
+    t.set_options({"Seed": 3})          # same value: only the graph is rebuilt
+    t.render_frame()
+    u.render_frame()
+    a, b = t.image(), u.image()
+    assert float(a[..., 3].mean()) == float(b[..., 3].mean()) == 4.0
+    assert t.stats() == u.stats()
+    assert _rel_mean_err(a[..., :3], b[..., :3]) < 1e-6
