@@ -526,8 +526,9 @@ def run_serving(args, m, system) -> dict:
 # ---- learned guiding (C5) ------------------------------------------------
 C1 = {"Samples": 2, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
       "DirectLightMIS": 0}
-LEARNED = {"LearnedGuiding": 1, "LearnedWarmupFrames": 16, "LearnedTrainSteps": 4,
-           "LearnedSamples": 65536, "OctreeLevel": 10, "MinRayBinLevel": 5, "BinRayCount": 512}
+LEARNED = {"LearnedGuiding": 1, "LearnedWarmupFrames": 16, "LearnedTrainSteps": 1,
+           "LearnedSamples": 65536, "LearnedWarmupOctree": 0, "OctreeLevel": 10,
+           "MinRayBinLevel": 5, "BinRayCount": 512}
 LEARNED_FLOATS = {"LearnedRate": 1e-2, "LearnedWeightMax": 5.0, "BXDF-GuideMISRatio": 0.5,
                   "RFieldFilterAlpha": 0.6}
 
@@ -544,11 +545,12 @@ def _frame_ms(t, torch, frames=20):
 
 
 def run_learned(args, m, system, torch) -> dict:
-    """C5: the config-1 Cornell scene (128x128, 4 spp per frame, depth 5);
-    plain path tracing, SVO path guiding and learned guiding (MLP vMF
-    mixture trained online on the tensor cores, the SVO guider for the first
-    16 frames) get the same time budget from a cold start and are scored by
-    mean squared error against a 4096-spp plain render."""
+    """Learned guiding on the 8k-triangle Cornell scene (128x128, 4 spp per
+    frame, depth 5): plain path tracing, SVO path guiding and learned guiding
+    (MLP vMF mixture trained online on the tensor cores; its first 16 frames
+    sampled by the BxDF alone, or by the octree guider for "_octree") get
+    the same device-time budget from a cold start and are scored by mean
+    squared error against a 4096-spp plain render."""
     scene = m.scenes.cornell(seed=1)
     g = m.GPUScene(system, scene)
     g.construct_accelerators()
@@ -562,6 +564,7 @@ def run_learned(args, m, system, torch) -> dict:
                          if learned or not k.startswith("Learned")})
             if learned:
                 opts["LearnedTrainSteps"] = int(kind.split("_")[1])
+                opts["LearnedWarmupOctree"] = 1 if kind.endswith("_octree") else 0
         t.set_options(opts)
         if kind != "plain":
             t.set_options({k: v for k, v in LEARNED_FLOATS.items()
@@ -572,7 +575,8 @@ def run_learned(args, m, system, torch) -> dict:
     ref_img = _frames_image(ref, args.learned_reference_spp // 4)
     ref.close()
     out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp}
-    kinds = (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14))
+    kinds = (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
+             ("learned_1_octree", 15))
     if args.learned_kinds:
         kinds = tuple(k for k in kinds if k[0] in args.learned_kinds.split(","))
     for kind, seed in kinds:
@@ -588,17 +592,19 @@ def run_learned(args, m, system, torch) -> dict:
         if kind.startswith("learned"):
             entry["held_out_loss_last_frame"] = t.learned_loss()
             entry["train_steps_per_frame"] = int(kind.split("_")[1])
+            entry["warm_up_sampler"] = "octree" if kind.endswith("_octree") else "BxDF"
         t.close()
         out[kind] = entry
-    if len(kinds) == 4:
-        best = min(("learned_1", "learned_4"), key=lambda k: out[k]["mse"])
+    if len(kinds) == 5:
+        best = min(("learned_1", "learned_4", "learned_1_octree"), key=lambda k: out[k]["mse"])
         out["learned"] = dict(out[best], variant=best)
         out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
         out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
         # per-sample efficiency (MSE x spp; lower is better), which the frame
         # cost then trades against
         out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
-                            for k in ("plain", "svo", "learned_1", "learned_4")}
+                            for k in ("plain", "svo", "learned_1", "learned_4",
+                                      "learned_1_octree")}
     out["config"] = {"scene": "config-1 Cornell box (seed 1), 128x128, 4 spp per frame, depth 5",
                      **LEARNED, **LEARNED_FLOATS,
                      "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
@@ -712,7 +718,8 @@ def main():
     ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
     ap.add_argument("--learned-reference-spp", type=int, default=4096)
     ap.add_argument("--learned-kinds", default="",
-                    help="comma list of plain,svo,learned_1,learned_4 (default all)")
+                    help="comma list of plain,svo,learned_1,learned_4,learned_1_octree "
+                         "(default all)")
     ap.add_argument("--only", choices=["all", "guided", "learned"], default="all",
                     help="guided: only the WFPG timing (for profiling a small case); "
                          "learned: only the learned-guiding comparison")

@@ -3,6 +3,7 @@
 #include "../../include/mrb200.h"
 #include "bxdf.cuh"
 #include "learned.cuh"
+#include "mlp_tile.cuh"
 #include "scan.cuh"
 
 namespace mrb {
@@ -39,32 +40,6 @@ __device__ __forceinline__ bool guided_hit(const SceneDev& sc, const GuideWave& 
     return !mat_specular(sc, batch, id);
 }
 
-__global__ void __launch_bounds__(256) k_learned_features(SceneDev sc, GuideDev g, GuideWave w,
-                                                          float* __restrict__ features) {
-    const uint32_t n = *w.count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float f[kMlpIn];
-        uint32_t batch, id;
-        if (guided_hit(sc, w, i, batch, id)) {
-            const float4 rd = w.rayD[i];
-            const float2 hb = w.hit.bary[i];
-            const V3 d = v3(rd.x, rd.y, rd.z);
-            const Surface sf = gen_surface(sc, w.hit.prim[i], hb.x, hb.y, d);
-            const V3 nrm = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
-            const V3 wo = -normalize(d);
-            const V3 p = box_coords(g, sf.pos);
-            encode_vertex(p.x, p.y, p.z, nrm.x, nrm.y, nrm.z, wo.x, wo.y, wo.z, f);
-        } else {
-#pragma unroll
-            for (int k = 0; k < kMlpIn; k++) f[k] = 0.0f;
-        }
-        float4* dst = reinterpret_cast<float4*>(features + size_t(i) * kMlpIn);
-#pragma unroll
-        for (int c = 0; c < kMlpIn / 4; c++)
-            dst[c] = make_float4(f[4 * c], f[4 * c + 1], f[4 * c + 2], f[4 * c + 3]);
-    }
-}
-
 // Orthonormal basis around a unit vector (Duff et al., "Building an
 // Orthonormal Basis, Revisited", JCGT 2017).
 __device__ __forceinline__ void onb(V3 n, V3& t1, V3& t2) {
@@ -88,26 +63,47 @@ __device__ __forceinline__ V3 vmf_sample(V3 mu, float kappa, float u0, float u1)
     return normalize(t1 * (s * cp) + t2 * (s * sp) + mu * c);
 }
 
-__global__ void __launch_bounds__(256) k_learned_sample(SceneDev sc, GuideWave w,
-                                                        const float* __restrict__ outputs,
-                                                        float misRatio, PathOptions opt,
-                                                        uint32_t depthTag, uint2* __restrict__ guide) {
-    const uint32_t n = *w.count;
-    const uint32_t frame = *opt.frame;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// The guide of one wavefront in one kernel: each thread of a 128-row tile
+// encodes its ray's hit as the network's input, the tile goes through the
+// tensor-core forward pass, and each thread draws its ray's direction from
+// the vMF mixture (probability misRatio) or the BxDF, with the one-sample
+// MIS pdf of the drawn direction at its half-precision octahedral
+// coordinates (the form the shading kernel decodes).  Rays at specular
+// surfaces, lights or none get no guide word.
+struct GuideIO {
+    SceneDev sc;
+    GuideDev g;
+    GuideWave w;
+    float misRatio;
+    PathOptions opt;
+    uint32_t depthTag;
+    uint2* guide;
+
+    __device__ uint32_t rows() const {
+        const uint32_t n = *w.count;
+        return n < w.maxRays ? n : w.maxRays;
+    }
+    __device__ void input(uint32_t i, uint32_t n, float* f) const {
+        uint32_t batch, id;
+        if (i < n && guided_hit(sc, w, i, batch, id)) {
+            const float4 rd = w.rayD[i];
+            const float2 hb = w.hit.bary[i];
+            const V3 d = v3(rd.x, rd.y, rd.z);
+            const Surface sf = gen_surface(sc, w.hit.prim[i], hb.x, hb.y, d);
+            const V3 nrm = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+            const V3 wo = -normalize(d);
+            const V3 p = box_coords(g, sf.pos);
+            encode_vertex(p.x, p.y, p.z, nrm.x, nrm.y, nrm.z, wo.x, wo.y, wo.z, f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kMlpIn; k++) f[k] = 0.0f;
+        }
+    }
+    __device__ void output(uint32_t i, const float* r) const {
         uint32_t batch, id;
         uint2 word = make_uint2(0u, 0x7E00u);  // no guide: the BxDF samples the ray
         if (guided_hit(sc, w, i, batch, id)) {
-            float r[kMlpOut];
-            const float4* src = reinterpret_cast<const float4*>(outputs + size_t(i) * kMlpOut);
-#pragma unroll
-            for (int c = 0; c < kMlpOut / 4; c++) {
-                const float4 q = src[c];
-                r[4 * c] = q.x;
-                r[4 * c + 1] = q.y;
-                r[4 * c + 2] = q.z;
-                r[4 * c + 3] = q.w;
-            }
+            const uint32_t frame = *opt.frame;
             VmfMixture mx;
             float rawLen[kMlpLobes], lobeLog[kMlpLobes];
             mixture_from_raw(r, mx, rawLen);
@@ -136,8 +132,6 @@ __global__ void __launch_bounds__(256) k_learned_sample(SceneDev sc, GuideWave w
                                                  opt.seedLo, opt.seedHi);
                 dir = mat_sample(sc, batch, id, wi, sf, aux.medium, r1.u[0], r1.u[1], r1.u[2]).dir;
             }
-            // the direction as the shading kernel will decode it, and the
-            // one-sample MIS pdf there
             float s, t;
             dir_yup_to_octa(dir, s, t);
             const uint16_t sh = f2h(s), th = f2h(t);
@@ -151,7 +145,7 @@ __global__ void __launch_bounds__(256) k_learned_sample(SceneDev sc, GuideWave w
         }
         guide[i] = word;
     }
-}
+};
 
 // ---- training samples ---------------------------------------------------------
 struct ChainView {
@@ -169,7 +163,8 @@ __device__ __forceinline__ uint32_t chain_length(const PathChain& pc, uint32_t p
     return L;
 }
 
-// Vertex d of path p as a training sample: false if it is not one.
+// Vertex d of path p as a training sample: false if it is not one.  With
+// feat == nullptr only the validity is decided.
 __device__ __forceinline__ bool chain_sample(const ChainView& v, uint32_t p, uint32_t d,
                                              uint32_t lastD, uint32_t frame, float* feat,
                                              float4& target) {
@@ -193,6 +188,7 @@ __device__ __forceinline__ bool chain_sample(const ChainView& v, uint32_t p, uin
     if (v.product) wgt *= fabsf(nn.x * dd.x + nn.y * dd.y + nn.z * dd.z);
     if (!(wgt > 0.0f) || !(wgt < 3.0e38f)) return false;
     if (v.weightMax > 0.0f) wgt = fminf(wgt, v.weightMax);
+    if (!feat) return true;  // counting pass: validity only
     const float4 a = pc.nodeA[at], pa = pc.nodeA[at - P];
     const V3 pos = v3(a.x, a.y, a.z);
     const V3 wo = normalize(v3(pa.x, pa.y, pa.z) - pos);
@@ -204,7 +200,6 @@ __device__ __forceinline__ bool chain_sample(const ChainView& v, uint32_t p, uin
 
 __global__ void __launch_bounds__(256) k_learned_count(ChainView v, uint32_t* __restrict__ count) {
     const uint32_t frame = *v.frame;
-    float f[kMlpIn];
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < v.pc.paths;
          p += gridDim.x * blockDim.x) {
         const uint32_t L = chain_length(v.pc, p, frame);
@@ -212,7 +207,7 @@ __global__ void __launch_bounds__(256) k_learned_count(ChainView v, uint32_t* __
         uint32_t c = 0;
         for (uint32_t d = 1; d <= L; d++) {
             float4 t;
-            if (chain_sample(v, p, d, lastD, frame, f, t)) c++;
+            if (chain_sample(v, p, d, lastD, frame, nullptr, t)) c++;
         }
         count[p] = c;
     }
@@ -262,18 +257,44 @@ __global__ void k_learned_steps(const uint32_t* __restrict__ total, LearnedScrat
     s.stepCount[k] = c < perStep ? c : perStep;
 }
 
+__global__ void __launch_bounds__(256) k_learned_ema(const float* __restrict__ params,
+                                                     float* __restrict__ ema, float beta,
+                                                     float* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < uint32_t(kMlpParams);
+         i += gridDim.x * blockDim.x) {
+        const float e = beta * ema[i] + (1.0f - beta) * params[i];
+        ema[i] = e;
+        out[i] = e;
+    }
+}
+
 }  // namespace
+
+int learned_ema(const float* params, float* ema, float beta, float* out, cudaStream_t st) {
+    k_learned_ema<<<(kMlpParams + 255) / 256, 256, 0, st>>>(params, ema, beta, out);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
 
 int learned_guide_wavefront(const SceneDev& sc, const GuideDev& g, const GuideWave& w,
                             const MlpDev& net, const LearnedScratch& s, float misRatio,
                             const PathOptions& opt, uint32_t depthTag, uint2* guide,
                             cudaStream_t st) {
-    const uint32_t grid = grid_for(w.maxRays, 256, 148 * 8);
-    k_learned_features<<<grid, 256, 0, st>>>(sc, g, w, s.features);
-    MRB_CUDA(cudaGetLastError());
-    int r = mlp_forward(net, s.features, w.maxRays, s.outputs, st, w.count);
-    if (r) return r;
-    k_learned_sample<<<grid, 256, 0, st>>>(sc, w, s.outputs, misRatio, opt, depthTag, guide);
+    (void)s;
+    static bool attr[64] = {};
+    int dev = 0;
+    MRB_CUDA(cudaGetDevice(&dev));
+    if (!attr[dev & 63]) {
+        MRB_CUDA(cudaFuncSetAttribute(k_mlp_forward_io<GuideIO>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(sizeof(MlpFwdSmem))));
+        attr[dev & 63] = true;
+    }
+    const uint32_t tiles = (w.maxRays + kMlpTile - 1) / kMlpTile;
+    const uint32_t cap = 148u * kMlpFwdCtasPerSm;
+    const uint32_t grid = tiles < cap ? (tiles ? tiles : 1u) : cap;
+    k_mlp_forward_io<<<grid, kMlpTile, sizeof(MlpFwdSmem), st>>>(
+        net, GuideIO{sc, g, w, misRatio, opt, depthTag, guide});
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

@@ -12,8 +12,6 @@
 namespace mrb {
 
 struct LearnedScratch {
-    float* features;      // maxRays x 80 (per wavefront); reused for training samples
-    float* outputs;       // maxRays x 40
     float* trainX;        // capacity x 80
     float* trainT;        // capacity x 4
     uint32_t* pathCount;  // paths + 1
@@ -27,12 +25,12 @@ struct LearnedScratch {
     uint32_t product;     // 1: weights carry |cos| at the vertex (target L_in |cos|)
 };
 
-// Guide words for one wavefront from the network: features of every ray's
-// hit, a forward pass, then per ray a draw from the vMF mixture (with
-// probability misRatio) or from the BxDF, the one-sample MIS pdf of the
-// drawn direction, and its octahedral coordinates (half precision, as the
-// octree sampler writes them).  Rays at specular surfaces, lights or none
-// get no guide word.
+// Guide words for one wavefront from the network, in one kernel: features
+// of every ray's hit, the forward pass, then per ray a draw from the vMF
+// mixture (with probability misRatio) or from the BxDF, the one-sample MIS
+// pdf of the drawn direction, and its octahedral coordinates (half
+// precision, as the octree sampler writes them).  Rays at specular
+// surfaces, lights or none get no guide word.
 int learned_guide_wavefront(const SceneDev& sc, const GuideDev& g, const GuideWave& w,
                             const MlpDev& net, const LearnedScratch& s, float misRatio,
                             const PathOptions& opt, uint32_t depthTag, uint2* guide,
@@ -48,6 +46,9 @@ int learned_collect(const GuideDev& g, const PathChain& pc, const uint32_t* fram
 // `steps` Adam steps on the collected samples, step k on its share; the
 // frame loss sums the batches' losses, each scored before its step.
 int learned_train(mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t st);
+// Exponential moving average of the parameters for inference:
+// ema = beta ema + (1 - beta) params, then out = ema (fp32).
+int learned_ema(const float* params, float* ema, float beta, float* out, cudaStream_t st);
 size_t learned_scan_temp_bytes(uint32_t paths);
 uint32_t learned_launches(uint32_t steps);
 

@@ -202,8 +202,12 @@ struct mrb_tracer {
     uint32_t learnedWarmupOctree = 1;  // 0: the BxDF alone samples the warm-up frames
     uint64_t learnedSeed = 1;
     float learnedRate = 1.0e-2f, learnedWeightMax = 0.0f;
+    // inference weights: an exponential moving average of the trained ones
+    // with this decay per frame (0: the trained weights themselves)
+    float learnedEma = 0.0f;
+    DBuf lEma, lEmaBackup;
     mrb_mlp* net = nullptr;
-    DBuf chainN, chainD, chainT, lFeat, lOut, lTrainX, lTrainT, lCount, lOffset, lScan, lSteps,
+    DBuf chainN, chainD, chainT, lTrainX, lTrainT, lCount, lOffset, lScan, lSteps,
         lLoss, netBackup;
     // The network trains on a side stream while the frame renders: frame f
     // trains on frame f-1's samples and renders with the weights as they
@@ -373,8 +377,6 @@ std::vector<float> learned_init(uint64_t seed) {
 
 LearnedScratch learned_scratch(const mrb_tracer* t) {
     LearnedScratch s{};
-    s.features = t->lFeat.as<float>();
-    s.outputs = t->lOut.as<float>();
     s.trainX = t->lTrainX.as<float>();
     s.trainT = t->lTrainT.as<float>();
     s.pathCount = t->lCount.as<uint32_t>();
@@ -389,14 +391,28 @@ LearnedScratch learned_scratch(const mrb_tracer* t) {
     return s;
 }
 
-// The forward passes' copy of the network (parameters and weight image).
-int learned_refresh_forward(mrb_tracer* t) {
+// The forward passes' copy of the network (parameters and weight image):
+// the trained weights, or their moving average (advanced by one step when
+// `step`, else taken as it stands).
+int learned_refresh_forward(mrb_tracer* t, bool step = true) {
     const MlpDev m = mlp_dev(t->net);
     char* f = t->lFwd.as<char>();
+    uint16_t* image = reinterpret_cast<uint16_t*>(f + size_t(kMlpParams) * 4);
+    if (t->learnedEma > 0.0f) {
+        if (step) {
+            if (learned_ema(m.params, t->lEma.as<float>(), t->learnedEma,
+                            reinterpret_cast<float*>(f), t->stream))
+                return MRB_E_CUDA;
+        } else {
+            MRB_CUDA(cudaMemcpyAsync(f, t->lEma.p, size_t(kMlpParams) * 4,
+                                     cudaMemcpyDeviceToDevice, t->stream));
+        }
+        return mlp_build_image(reinterpret_cast<const float*>(f), image, t->stream);
+    }
     MRB_CUDA(cudaMemcpyAsync(f, m.params, size_t(kMlpParams) * 4, cudaMemcpyDeviceToDevice,
                              t->stream));
-    MRB_CUDA(cudaMemcpyAsync(f + size_t(kMlpParams) * 4, m.wImage, kMlpImageBytes,
-                             cudaMemcpyDeviceToDevice, t->stream));
+    MRB_CUDA(cudaMemcpyAsync(image, m.wImage, kMlpImageBytes, cudaMemcpyDeviceToDevice,
+                             t->stream));
     return 0;
 }
 
@@ -407,15 +423,16 @@ int ensure_learned(mrb_tracer* t) {
     const uint32_t cap = t->learnedSamples / t->learnedSteps * t->learnedSteps;
     int r;
     if ((r = t->chainN.alloc(chain)) || (r = t->chainD.alloc(chain)) ||
-        (r = t->chainT.alloc(chain)) || (r = t->lFeat.alloc(size_t(t->maxRays) * kMlpIn * 4)) ||
-        (r = t->lOut.alloc(size_t(t->maxRays) * kMlpOut * 4)) ||
+        (r = t->chainT.alloc(chain)) ||
         (r = t->lTrainX.alloc(size_t(cap) * kMlpIn * 4)) ||
         (r = t->lTrainT.alloc(size_t(cap) * 16)) ||
         (r = t->lCount.alloc((size_t(t->chainPaths) + 1) * 4)) ||
         (r = t->lOffset.alloc((size_t(t->chainPaths) + 1) * 4)) ||
         (r = t->lScan.alloc(learned_scan_temp_bytes(t->chainPaths))) ||
         (r = t->lSteps.alloc(size_t(t->learnedSteps) * 4)) || (r = t->lLoss.alloc(16)) ||
-        (r = t->netBackup.alloc(mlp_state_bytes())) || (r = t->lFwd.alloc(size_t(kMlpParams) * 4 + kMlpImageBytes)))
+        (r = t->netBackup.alloc(mlp_state_bytes())) || (r = t->lFwd.alloc(size_t(kMlpParams) * 4 + kMlpImageBytes)) ||
+        (r = t->lEma.alloc(size_t(kMlpParams) * 4)) ||
+        (r = t->lEmaBackup.alloc(size_t(kMlpParams) * 4)))
         return r;
     if (!t->trainStream) {
         MRB_CUDA(cudaStreamCreateWithFlags(&t->trainStream, cudaStreamNonBlocking));
@@ -432,7 +449,9 @@ int ensure_learned(mrb_tracer* t) {
         // no samples collected yet: the first frame's steps train on nothing
         MRB_CUDA(cudaMemsetAsync(t->lSteps.p, 0, t->lSteps.bytes, t->stream));
         MRB_CUDA(cudaMemsetAsync(t->lLoss.p, 0, t->lLoss.bytes, t->stream));
-        if ((r = learned_refresh_forward(t))) return r;
+        MRB_CUDA(cudaMemcpyAsync(t->lEma.p, mlp_dev(t->net).params, size_t(kMlpParams) * 4,
+                                 cudaMemcpyDeviceToDevice, t->stream));
+        if ((r = learned_refresh_forward(t, false))) return r;
         t->learnedReset = false;
     }
     return 0;
@@ -701,12 +720,13 @@ uint32_t launches_per_frame(const mrb_tracer* t) {
         uint32_t guided = t->skipPG ? 0u : std::min(t->maxDepth, t->guideBounce);
         if (learned_active(t) && guided == t->maxDepth) guided--;
         if (!learned_active(t) && !octree_guides(t)) guided = 0;
-        // learned guiding: features, forward pass and sampler per guided
-        // depth, and the frame's training
-        const uint32_t perDepth = learned_active(t) ? 3u
+        // learned guiding: one fused encode / forward / sample kernel per
+        // guided depth, and the frame's training
+        const uint32_t perDepth = learned_active(t) ? 1u
                                                     : guide_launches(t->svo, guide_options(t), t->maxRays);
         n += guided * perDepth + (octree_guides(t) ? 2 + 2 * t->svoP.depth : 0u);
-        if (t->learned && t->net) n += learned_launches(t->learnedSteps);
+        if (t->learned && t->net)
+            n += learned_launches(t->learnedSteps) + (t->learnedEma > 0.0f ? 2u : 0u);
     }
     return n;
 }
@@ -1251,6 +1271,12 @@ int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double v) {
             return MRB_E_ARG;
         }
         t->learnedRate = static_cast<float>(v);
+    } else if (t->wfpg && k == "LearnedEMA") {
+        if (!(v >= 0.0 && v < 1.0)) {
+            set_error("LearnedEMA must be in [0, 1)");
+            return MRB_E_ARG;
+        }
+        t->learnedEma = static_cast<float>(v);
     } else if (t->wfpg && k == "LearnedWeightMax") {
         if (!(v >= 0.0)) {
             set_error("LearnedWeightMax must be >= 0");
@@ -1512,9 +1538,18 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             MRB_CUDA(cudaMemcpyAsync(b + U * 28, t->svo.nodeAvg, N * 4, cudaMemcpyDeviceToDevice, t->stream));
         }
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, true, t->stream)) return MRB_E_CUDA;
+        if (t->net)
+            MRB_CUDA(cudaMemcpyAsync(t->lEmaBackup.p, t->lEma.p, size_t(kMlpParams) * 4,
+                                     cudaMemcpyDeviceToDevice, t->stream));
         if ((r = record_frame(t))) return r;
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, false, t->stream)) return MRB_E_CUDA;
-        if (t->net && (r = learned_refresh_forward(t))) return r;
+        if (t->net) {
+            MRB_CUDA(cudaMemcpyAsync(t->lEma.p, t->lEmaBackup.p, size_t(kMlpParams) * 4,
+                                     cudaMemcpyDeviceToDevice, t->stream));
+            // the forward copy as it was: the restored state, without a new
+            // average step
+            if ((r = learned_refresh_forward(t, false))) return r;
+        }
         MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &f0, 4, cudaMemcpyHostToDevice, t->stream));
         if (pb) {
             const char* b = t->payloadBackup.as<char>();

@@ -357,7 +357,8 @@ class WFPGTracer(PathTracer):
         "PGDataStructDumpIntervalExp", "LearnedGuiding", "LearnedWarmupFrames",
         "LearnedTrainSteps", "LearnedSamples", "LearnedSeed", "LearnedProductTarget",
         "LearnedWarmupOctree")
-    FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha", "LearnedRate", "LearnedWeightMax")
+    FLOAT_KEYS = ("BXDF-GuideMISRatio", "RFieldFilterAlpha", "LearnedRate", "LearnedWeightMax",
+                  "LearnedEMA")
     STRING_KEYS = ("InitialSVO", "PGDataStructDumpName")
 
     def __init__(self, system: TracerSystem, scene: GPUScene):
