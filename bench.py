@@ -313,6 +313,20 @@ def _budget_image(t, budget_ms: float, est_ms: float, torch):
     return np.where(w > 0, img[..., :3] / np.where(w > 0, w, 1.0), 0.0), frames, used
 
 
+def _reference(make, frames: int):
+    """A converged render as two independent halves: (their average, the
+    variance of that average per pixel and channel, estimated as
+    mean((R1 - R2)^2) / 4).  The variance is the floor every MSE against the
+    reference carries; subtracting it leaves the run's own error."""
+    halves = []
+    for seed in (0, 1):
+        t = make(seed)
+        halves.append(_frames_image(t, max(1, frames // 2)))
+        t.close()
+    r1, r2 = halves
+    return 0.5 * (r1 + r2), float(np.mean((r1 - r2) ** 2)) / 4.0
+
+
 def run_guided(args, g, m, torch, dev: int) -> dict:
     """The same frame with SVO path guiding, and the equal-time MSE of the
     guided and plain tracers against a converged plain render
@@ -362,11 +376,12 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     q1.record(pstream)
     q1.synchronize()
     plain_ms = q0.elapsed_time(q1) / 20
-    ref = m.PathTracer(g.system, g)
-    ref.set_options(dict(OPTS, Seed=99))
-    _attach_filter(g.system, ref)
-    ref_img = _frames_image(ref, args.mse_reference_spp)
-    ref.close()
+    def make_ref(half):
+        r = m.PathTracer(g.system, g)
+        r.set_options(dict(OPTS, Seed=99 + 1000 * half))
+        _attach_filter(g.system, r)
+        return r
+    ref_img, ref_var = _reference(make_ref, args.mse_reference_spp)
     budget = float(args.mse_budget_ms)
     plain_img, plain_frames, plain_used = _budget_image(p, budget, plain_ms, torch)
     gt = m.WFPGTracer(g.system, g)   # a cold cache: learning is part of the budget
@@ -374,19 +389,22 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     gt.set_options(GUIDED_FLOATS)
     _attach_filter(g.system, gt)
     guided_img, guided_frames, guided_used = _budget_image(gt, budget, guided_ms, torch)
-    mse_p = float(np.mean((plain_img - ref_img) ** 2))
-    mse_g = float(np.mean((guided_img - ref_img) ** 2))
+    raw_p = float(np.mean((plain_img - ref_img) ** 2))
+    raw_g = float(np.mean((guided_img - ref_img) ** 2))
+    mse_p, mse_g = raw_p - ref_var, raw_g - ref_var
     out["equal_time_mse"] = {
         "budget_ms": budget, "reference_spp": args.mse_reference_spp,
+        "reference_variance": ref_var,
         "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "device_ms": plain_used,
-                  "mse": mse_p},
+                  "mse": mse_p, "mse_raw": raw_p},
         "guided": {"frames": guided_frames, "ms_per_frame": guided_ms,
-                   "device_ms": guided_used, "mse": mse_g},
+                   "device_ms": guided_used, "mse": mse_g, "mse_raw": raw_g},
         "guided_over_plain": mse_g / mse_p if mse_p > 0 else None,
         "mse_x_frames": {"plain": mse_p * plain_frames, "guided": mse_g * guided_frames},
-        "note": "1 spp per frame at 1920x1080; the reference is a separate plain render "
-                "(different seed); the guided tracer starts with a cold octree, and its "
-                "build and every frame count against the budget (device time)"}
+        "note": "1 spp per frame at 1920x1080; the reference is two separate plain renders "
+                "(other seeds), whose own variance is subtracted from every MSE (mse_raw keeps "
+                "it); the guided tracer starts with a cold octree, and its build and every "
+                "frame count against the budget (device time)"}
     return out
 
 
@@ -545,13 +563,23 @@ def _frame_ms(t, torch, frames=20):
 
 
 def run_learned(args, m, system, torch) -> dict:
+    """The learned-guiding comparison on the config Cornell scene and on its
+    shielded-light variant (light reaching the room only by way of the
+    ceiling), where guiding has indirect light to find."""
+    out = _run_learned_scene(args, m, system, torch, shielded=False)
+    out["shielded_light"] = _run_learned_scene(args, m, system, torch, shielded=True)
+    return out
+
+
+def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
     """Learned guiding on the 8k-triangle Cornell scene (128x128, 4 spp per
     frame, depth 5): plain path tracing, SVO path guiding and learned guiding
     (MLP vMF mixture trained online on the tensor cores; its first 16 frames
     sampled by the BxDF alone, or by the octree guider for "_octree") get
     the same device-time budget from a cold start and are scored by mean
-    squared error against a 4096-spp plain render."""
-    scene = m.scenes.cornell(seed=1)
+    squared error against a 16384-spp plain render, less that render's own
+    variance."""
+    scene = m.scenes.cornell(seed=1, shielded=shielded)
     g = m.GPUScene(system, scene)
     g.construct_accelerators()
 
@@ -571,10 +599,10 @@ def run_learned(args, m, system, torch) -> dict:
                            if learned or not k.startswith("Learned")})
         return t
 
-    ref = make("plain", 4242)
-    ref_img = _frames_image(ref, args.learned_reference_spp // 4)
-    ref.close()
-    out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp}
+    ref_img, ref_var = _reference(lambda half: make("plain", 4242 + half),
+                                  args.learned_reference_spp // 4)
+    out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp,
+           "reference_variance": ref_var}
     kinds = (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
              ("learned_1_octree", 15))
     if args.learned_kinds:
@@ -587,8 +615,9 @@ def run_learned(args, m, system, torch) -> dict:
         probe.close()
         t = make(kind, seed)
         img, frames, used = _budget_image(t, args.learned_budget_ms, ms, torch)
+        raw = float(np.mean((img - ref_img) ** 2))
         entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames, "device_ms": used,
-                 "mse": float(np.mean((img - ref_img) ** 2))}
+                 "mse": raw - ref_var, "mse_raw": raw}
         if kind.startswith("learned"):
             entry["held_out_loss_last_frame"] = t.learned_loss()
             entry["train_steps_per_frame"] = int(kind.split("_")[1])
@@ -605,7 +634,9 @@ def run_learned(args, m, system, torch) -> dict:
         out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
                             for k in ("plain", "svo", "learned_1", "learned_4",
                                       "learned_1_octree")}
-    out["config"] = {"scene": "config-1 Cornell box (seed 1), 128x128, 4 spp per frame, depth 5",
+    out["config"] = {"scene": ("Cornell box (seed 1) with the light facing the ceiling over an "
+                               "opaque panel" if shielded else "config-1 Cornell box (seed 1)")
+                     + ", 128x128, 4 spp per frame, depth 5",
                      **LEARNED, **LEARNED_FLOATS,
                      "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
                                 "activations, FP32 accumulation on tcgen05 tensor cores"}
@@ -715,8 +746,8 @@ def main():
     ap.add_argument("--pool-stack", type=int, default=128)
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the learned-guiding equal-time MSE comparison")
-    ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
-    ap.add_argument("--learned-reference-spp", type=int, default=4096)
+    ap.add_argument("--learned-budget-ms", type=float, default=250.0)
+    ap.add_argument("--learned-reference-spp", type=int, default=16384)
     ap.add_argument("--learned-kinds", default="",
                     help="comma list of plain,svo,learned_1,learned_4,learned_1_octree "
                          "(default all)")

@@ -101,11 +101,15 @@ class _Builder:
 
 
 def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = False,
-            triangles: int | None = None) -> Scene:
+            triangles: int | None = None, shielded: bool = False) -> Scene:
     """mixed=True gives the spheres, in turn, Lambert, LambertC, Metal (GGX
     conductor), Unreal and Refract materials (a test input for every BxDF).
     triangles: scale the spheres' tessellation (segments = 2 x rings) so the
-    scene has about that many triangles (default 32 x 16 per sphere)."""
+    scene has about that many triangles (default 32 x 16 per sphere).
+    shielded=True replaces the ceiling-wide light by a 0.2 x 0.2 light 0.1
+    below the ceiling's centre, facing it, over an opaque 0.3 x 0.3 panel:
+    the room sees the light only by way of the lit ceiling, the
+    indirect-lighting case path guiding is for."""
     rng = np.random.default_rng(seed)
     segments, rings = 32, 16
     if triangles is not None:
@@ -127,12 +131,23 @@ def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = Fa
         ((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0), (1, 0, 0)),    # left
         ((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1), (-1, 0, 0)),   # right
     ]
-    for w in walls:
-        b.add(*_quad(*w), lambert())
+    for p0, p1, p2, p3, n in walls:
+        # counter-clockwise seen from inside: the winding agrees with n
+        b.add(*_quad(p0, p3, p2, p1, n), lambert())
     mats.append({"type": LIGHT, "radiance": np.array([17, 12, 4], np.float32)})
     light = len(mats) - 1
     y = 0.999
-    b.add(*_quad((0, y, 0), (0, y, 1), (1, y, 1), (1, y, 0), (0, -1, 0)), light)
+    if not shielded:
+        b.add(*_quad((0, y, 0), (1, y, 0), (1, y, 1), (0, y, 1), (0, -1, 0)), light)
+    else:
+        # the light faces the ceiling from 0.1 below it; an opaque panel
+        # just under the light hides it from the room
+        ly, lo, hi = 0.9, 0.4, 0.6
+        b.add(*_quad((lo, ly, lo), (lo, ly, hi), (hi, ly, hi), (hi, ly, lo), (0, 1, 0)), light)
+        py, plo, phi = 0.895, 0.35, 0.65
+        # one quad: triangles are two-sided, the panel shades from both
+        b.add(*_quad((plo, py, plo), (phi, py, plo), (phi, py, phi), (plo, py, phi), (0, -1, 0)),
+              lambert())
     kinds = [LAMBERT, LAMBERTC, METAL, UNREAL, REFRACT]
     for k in range(8):
         r = float(rng.uniform(0.1, 0.25))
@@ -160,7 +175,7 @@ def cornell(seed: int = 1, width: int = 128, height: int = 128, mixed: bool = Fa
     cam = {"position": [0.5, 0.5, -1.0], "gaze": [0.5, 0.5, 0.5], "up": [0.0, 1.0, 0.0],
            "near_far": [0.1, 100.0], "fov": [fov, fov]}
     return Scene("cornell", pos, nrm, uv, idx, mat, mats, np.array([1.0, 1.5], np.float32), 0,
-                 cam, width, height, meta={"seed": seed, "mixed": mixed,
+                 cam, width, height, meta={"seed": seed, "mixed": mixed, "shielded": shielded,
                                            "sphere_tessellation": (segments, rings)})
 
 
@@ -210,8 +225,8 @@ def clusters(seed: int = 1, width: int = 1920, height: int = 1080, n_clusters: i
     light = len(mats) - 1
     L = [((0, 30, 30), (0, 70, 30), (0, 70, 70), (0, 30, 70), (1, 0, 0)),
          ((100, 30, 30), (100, 30, 70), (100, 70, 70), (100, 70, 30), (-1, 0, 0)),
-         ((30, 100, 30), (30, 100, 70), (70, 100, 70), (70, 100, 30), (0, -1, 0)),
-         ((30, 30, 100), (70, 30, 100), (70, 70, 100), (30, 70, 100), (0, 0, -1))]
+         ((30, 100, 30), (70, 100, 30), (70, 100, 70), (30, 100, 70), (0, -1, 0)),
+         ((30, 30, 100), (30, 70, 100), (70, 70, 100), (70, 30, 100), (0, 0, -1))]
     b = _Builder()
     b.add(positions, normals, uvs, indices, 0)
     b.mat[0] = tri_mat
