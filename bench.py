@@ -586,6 +586,13 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
     def make(kind, seed):
         t = m.PathTracer(system, g) if kind == "plain" else m.WFPGTracer(system, g)
         opts = dict(C1, Seed=seed)
+        if kind == "wfpg_bxdf":
+            # the same tracer with its network never taking over: the BxDF
+            # samples every frame (the method without the network)
+            opts.update(LEARNED, LearnedWarmupFrames=1 << 30)
+            t.set_options(opts)
+            t.set_options(LEARNED_FLOATS)
+            return t
         learned = kind.startswith("learned")
         if kind != "plain":
             opts.update({k: v for k, v in LEARNED.items()
@@ -603,7 +610,7 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
                                   args.learned_reference_spp // 4)
     out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp,
            "reference_variance": ref_var}
-    kinds = (("plain", 11), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
+    kinds = (("plain", 11), ("wfpg_bxdf", 16), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
              ("learned_1_octree", 15))
     if args.learned_kinds:
         kinds = tuple(k for k in kinds if k[0] in args.learned_kinds.split(","))
@@ -624,15 +631,16 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
             entry["warm_up_sampler"] = "octree" if kind.endswith("_octree") else "BxDF"
         t.close()
         out[kind] = entry
-    if len(kinds) == 5:
+    if len(kinds) == 6:
         best = min(("learned_1", "learned_4", "learned_1_octree"), key=lambda k: out[k]["mse"])
         out["learned"] = dict(out[best], variant=best)
         out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
+        out["learned_over_wfpg_bxdf"] = out["learned"]["mse"] / out["wfpg_bxdf"]["mse"]
         out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
         # per-sample efficiency (MSE x spp; lower is better), which the frame
         # cost then trades against
         out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
-                            for k in ("plain", "svo", "learned_1", "learned_4",
+                            for k in ("plain", "wfpg_bxdf", "svo", "learned_1", "learned_4",
                                       "learned_1_octree")}
     out["config"] = {"scene": ("Cornell box (seed 1) with the light facing the ceiling over an "
                                "opaque panel" if shielded else "config-1 Cornell box (seed 1)")
@@ -749,8 +757,8 @@ def main():
     ap.add_argument("--learned-budget-ms", type=float, default=250.0)
     ap.add_argument("--learned-reference-spp", type=int, default=16384)
     ap.add_argument("--learned-kinds", default="",
-                    help="comma list of plain,svo,learned_1,learned_4,learned_1_octree "
-                         "(default all)")
+                    help="comma list of plain,wfpg_bxdf,svo,learned_1,learned_4,"
+                         "learned_1_octree (default all)")
     ap.add_argument("--only", choices=["all", "guided", "learned"], default="all",
                     help="guided: only the WFPG timing (for profiling a small case); "
                          "learned: only the learned-guiding comparison")

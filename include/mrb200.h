@@ -273,15 +273,21 @@ void mrb_tracer_destroy(mrb_tracer* t);
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
 /* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha",
  * "LearnedRate" (Adam step size of the learned guide, default 1e-2),
- * "LearnedWeightMax" (cap on a training sample's weight, 0 = none).
+ * "LearnedWeightMax" (cap on a training sample's weight, 0 = none),
+ * "LearnedEMA" (inference weights = moving average of the trained ones with
+ * this decay per frame, [0, 1), default 0 = the trained weights).
  * Learned guiding (no counterpart in the reference), integer options of the
  * WFPG tracer: "LearnedGuiding" (0/1): a guiding network (mrb_mlp_*) trains
- * every frame from the path chains and, after "LearnedWarmupFrames" frames
- * (default 16) of octree guiding, its vMF mixture replaces the octree product
- * sampler (one-sample MIS with the BxDF, ratio BXDF-GuideMISRatio);
- * "LearnedTrainSteps" (Adam steps per frame, default 4), "LearnedSamples"
- * (training samples per frame, default 65,536), "LearnedSeed" (weights'
- * initial draw). */
+ * every frame from the path chains (on a side stream, overlapped with the
+ * next frame) and, after "LearnedWarmupFrames" frames (default 16), its vMF
+ * mixture replaces the octree product sampler (one-sample MIS with the BxDF,
+ * ratio BXDF-GuideMISRatio; the last depth is not guided);
+ * "LearnedWarmupOctree" (1, default: the octree guides the warm-up frames;
+ * 0: the BxDF alone samples them), "LearnedTrainSteps" (Adam steps per
+ * frame, default 4), "LearnedSamples" (training samples per frame, default
+ * 65,536), "LearnedProductTarget" (1, default: training weights carry the
+ * |cos| at the vertex, so the mixture learns L_in |cos|; 0: L_in),
+ * "LearnedSeed" (weights' initial draw). */
 int mrb_tracer_set_option_float(mrb_tracer* t, const char* name, double value);
 /* The learned guiding network's parameters (mrb_mlp_param_count floats). */
 int mrb_tracer_learned_params(mrb_tracer* t, float* host_params);
