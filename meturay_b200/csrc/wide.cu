@@ -361,8 +361,12 @@ __device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut&
     }
 }
 
+// Nine 128-thread blocks per SM (56 registers, a few bytes spilled): the
+// traversal's dependent loads and ALU chains want resident warps more than
+// registers (measured on clusters-1M: 8 blocks 4.77 ms, 9 blocks 4.57 ms,
+// 10 blocks 5.27 ms per frame of traversal; 7 blocks at 68 registers 5.05 ms).
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_trace_wide(WideAccelDev acc,
+__global__ void __launch_bounds__(128, 9) k_trace_wide(WideAccelDev acc,
                                                     const float4* __restrict__ rayO,
                                                     const float4* __restrict__ rayD,
                                                     const uint32_t* __restrict__ dCount,
