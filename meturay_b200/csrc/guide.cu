@@ -252,7 +252,7 @@ __device__ __forceinline__ float product_pdf(const GuideSmem<X>& S, int warp, fl
 }
 
 template <int X>
-__global__ void __launch_bounds__(kGuideTPB, 3) k_guide(GuideArgs A) {
+__global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
     __shared__ GuideSmem<X> S;
     constexpr int DPP = X / 8;
     const float dppF = static_cast<float>(DPP);
@@ -797,7 +797,7 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
     const uint32_t kernelIndex = iteration < 4 ? iteration : 4;
     switch (kernelIndex) {
         case 0:
-        case 1: k_guide<64><<<148 * 3, kGuideTPB, 0, st>>>(ga); break;
+        case 1: k_guide<64><<<148 * 4, kGuideTPB, 0, st>>>(ga); break;
         case 2: k_guide<32><<<148 * 4, kGuideTPB, 0, st>>>(ga); break;
         case 3: k_guide<16><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;
         default: k_guide<8><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;
