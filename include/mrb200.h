@@ -344,6 +344,14 @@ int mrb_tracer_set_filter(mrb_tracer* t, const mrb_recon_filter* f);
  * sum of per-frame per-pixel means with the frame count in .w.  Either way
  * rgb / w is the pixel's estimate. */
 int mrb_tracer_get_image(mrb_tracer* t, float* host_rgba);
+/* Asynchronous read-back for pipelined hosts: the image as it stands after
+ * the work queued so far is snapshotted on the device, and copied into
+ * `host_rgba` (pinned memory; width x height x 4 floats) on a separate copy
+ * stream while later frames render.  The host buffer is valid after
+ * mrb_tracer_wait_image.  A new call first waits for the previous copy to
+ * leave the snapshot buffer. */
+int mrb_tracer_get_image_async(mrb_tracer* t, float* host_rgba);
+int mrb_tracer_wait_image(mrb_tracer* t);
 int mrb_tracer_get_samples(mrb_tracer* t, float* host_rgba);
 int mrb_tracer_reset_image(mrb_tracer* t);
 /* The image's per-pixel estimate (rgb / w) as a .exr (FLOAT RGB) or .pfm file. */

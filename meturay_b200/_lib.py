@@ -91,6 +91,8 @@ def _load() -> C.CDLL:
         "mrb_tracer_finalize": (i32, [vp]),
         "mrb_tracer_render_frame": (i32, [vp]),
         "mrb_tracer_get_image": (i32, [vp, vp]),
+        "mrb_tracer_get_image_async": (i32, [vp, vp]),
+        "mrb_tracer_wait_image": (i32, [vp]),
         "mrb_tracer_get_samples": (i32, [vp, vp]),
         "mrb_tracer_reset_image": (i32, [vp]),
         "mrb_tracer_stats": (i32, [vp, C.POINTER(u64), C.POINTER(u32)]),

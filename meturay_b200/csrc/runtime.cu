@@ -225,6 +225,11 @@ struct mrb_tracer {
     DBuf chainA, chainB, chainNee, chainPath, binKey, binRid, heads, headScan, binBegin, binEnd,
         guideSort, guideScan, guideBuf, payloadBackup;
     DBuf imageBackup;  // image and ray counters around the eager frame of a capture
+    // asynchronous image read-back: device snapshot, copied on copyStream
+    DBuf imageStage;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t snapDone = nullptr, copyDone = nullptr;
+    bool copyPending = false;
     size_t guideSortBytes = 0;
     uint32_t chainPaths = 0, chainLevels = 0;
     // reconstruction filter (AttachReconFilter); image coordinates per sample
@@ -236,6 +241,7 @@ struct mrb_tracer {
     bool graphDirty = true;
     ~mrb_tracer() {
         if (trainStream) cudaStreamSynchronize(trainStream);
+        if (copyStream) cudaStreamSynchronize(copyStream);
         if (net) mrb_mlp_destroy(net);
         if (svoReady) svo_free(svo);
         if (graph) cudaGraphExecDestroy(graph);
@@ -244,6 +250,9 @@ struct mrb_tracer {
         if (trainFork) cudaEventDestroy(trainFork);
         if (trainJoin) cudaEventDestroy(trainJoin);
         if (trainStream) cudaStreamDestroy(trainStream);
+        if (snapDone) cudaEventDestroy(snapDone);
+        if (copyDone) cudaEventDestroy(copyDone);
+        if (copyStream) cudaStreamDestroy(copyStream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1593,6 +1602,37 @@ int mrb_tracer_get_image(mrb_tracer* t, float* host) {
     MRB_CUDA(cudaMemcpyAsync(host, t->image.p, size_t(t->width) * t->height * 16,
                              cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaStreamSynchronize(t->stream));
+    return check_device_errors(t);
+}
+
+int mrb_tracer_get_image_async(mrb_tracer* t, float* host) {
+    if (!t || !host || !t->image.p) return MRB_E_ARG;
+    const size_t bytes = size_t(t->width) * t->height * 16;
+    if (!t->copyStream) {
+        MRB_CUDA(cudaStreamCreateWithFlags(&t->copyStream, cudaStreamNonBlocking));
+        MRB_CUDA(cudaEventCreateWithFlags(&t->snapDone, cudaEventDisableTiming));
+        MRB_CUDA(cudaEventCreateWithFlags(&t->copyDone, cudaEventDisableTiming));
+    }
+    if (int r = t->imageStage.alloc(bytes)) return r;
+    // the previous copy must have left the snapshot buffer
+    if (t->copyPending) MRB_CUDA(cudaStreamWaitEvent(t->stream, t->copyDone, 0));
+    MRB_CUDA(cudaMemcpyAsync(t->imageStage.p, t->image.p, bytes, cudaMemcpyDeviceToDevice,
+                             t->stream));
+    MRB_CUDA(cudaEventRecord(t->snapDone, t->stream));
+    MRB_CUDA(cudaStreamWaitEvent(t->copyStream, t->snapDone, 0));
+    MRB_CUDA(cudaMemcpyAsync(host, t->imageStage.p, bytes, cudaMemcpyDeviceToHost,
+                             t->copyStream));
+    MRB_CUDA(cudaEventRecord(t->copyDone, t->copyStream));
+    t->copyPending = true;
+    return 0;
+}
+
+int mrb_tracer_wait_image(mrb_tracer* t) {
+    if (!t) return MRB_E_ARG;
+    if (t->copyPending) {
+        MRB_CUDA(cudaEventSynchronize(t->copyDone));
+        t->copyPending = false;
+    }
     return check_device_errors(t);
 }
 

@@ -313,6 +313,14 @@ class PathTracer:
     def image_into(self, host_ptr: int):
         check(lib.mrb_tracer_get_image(self._h, host_ptr))
 
+    def image_into_async(self, host_ptr: int):
+        """Snapshot the image and copy it into pinned host memory while later
+        frames render; valid after wait_image()."""
+        check(lib.mrb_tracer_get_image_async(self._h, host_ptr))
+
+    def wait_image(self):
+        check(lib.mrb_tracer_wait_image(self._h))
+
     def sample_radiance(self) -> np.ndarray:
         s = self.samples
         out = np.zeros((self.height * s, self.width * s, 4), np.float32)

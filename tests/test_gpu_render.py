@@ -178,3 +178,23 @@ def test_recapture_keeps_the_accumulated_image(system):
     assert float(a[..., 3].mean()) == float(b[..., 3].mean()) == 4.0
     assert t.stats() == u.stats()
     assert _rel_mean_err(a[..., :3], b[..., :3]) < 1e-6
+
+
+def test_async_image_readback_matches(system):
+    """The pipelined read-back delivers the image as it stood when it was
+    queued, while later frames keep rendering."""
+    import torch
+    from meturay_b200 import scenes
+    scene = scenes.cornell(seed=1, width=32, height=32)
+    _, t = _setup(system, scene, dict(CORNELL_OPTS, Seed=5))
+    host = [torch.empty(32 * 32 * 4, dtype=torch.float32).pin_memory() for _ in range(2)]
+    t.render_frame()
+    t.image_into_async(host[0].data_ptr())
+    first_weight = None
+    t.render_frame()
+    t.wait_image()
+    first_weight = float(host[0].view(32, 32, 4)[..., 3].mean())
+    t.image_into_async(host[1].data_ptr())
+    t.wait_image()
+    assert first_weight == 1.0
+    np.testing.assert_array_equal(host[1].numpy().reshape(32, 32, 4), t.image())
