@@ -319,15 +319,24 @@ def _budget_image(t, budget_ms: float, est_ms: float, torch):
 def _reference(make, frames: int):
     """A converged render as two independent halves: (their average, the
     variance of that average per pixel and channel, estimated as
-    mean((R1 - R2)^2) / 4).  The variance is the floor every MSE against the
-    reference carries; subtracting it leaves the run's own error."""
+    mean((R1 - R2)^2) / 4, and the same for the relative error).  The
+    variance is the floor every error against the reference carries;
+    subtracting it leaves the run's own error."""
     halves = []
     for seed in (0, 1):
         t = make(seed)
         halves.append(_frames_image(t, max(1, frames // 2)))
         t.close()
     r1, r2 = halves
-    return 0.5 * (r1 + r2), float(np.mean((r1 - r2) ** 2)) / 4.0
+    ref = 0.5 * (r1 + r2)
+    d2 = (r1 - r2) ** 2
+    return ref, float(np.mean(d2)) / 4.0, float(np.mean(d2 / (ref * ref + 0.01))) / 4.0
+
+
+def _rel_mse(img, ref) -> float:
+    """Relative MSE, mean((x - r)^2 / (r^2 + 0.01)): bright outliers weigh
+    less than in the MSE, so it moves less with rare high-energy paths."""
+    return float(np.mean((img - ref) ** 2 / (ref * ref + 0.01)))
 
 
 def run_guided(args, g, m, torch, dev: int) -> dict:
@@ -384,7 +393,7 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
         r.set_options(dict(OPTS, Seed=99 + 1000 * half))
         _attach_filter(g.system, r)
         return r
-    ref_img, ref_var = _reference(make_ref, args.mse_reference_spp)
+    ref_img, ref_var, ref_rvar = _reference(make_ref, args.mse_reference_spp)
     budget = float(args.mse_budget_ms)
     plain_img, plain_frames, plain_used = _budget_image(p, budget, plain_ms, torch)
     gt = m.WFPGTracer(g.system, g)   # a cold cache: learning is part of the budget
@@ -399,9 +408,11 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
         "budget_ms": budget, "reference_spp": args.mse_reference_spp,
         "reference_variance": ref_var,
         "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "device_ms": plain_used,
-                  "mse": mse_p, "mse_raw": raw_p},
+                  "mse": mse_p, "mse_raw": raw_p,
+                  "rel_mse": _rel_mse(plain_img, ref_img) - ref_rvar},
         "guided": {"frames": guided_frames, "ms_per_frame": guided_ms,
-                   "device_ms": guided_used, "mse": mse_g, "mse_raw": raw_g},
+                   "device_ms": guided_used, "mse": mse_g, "mse_raw": raw_g,
+                   "rel_mse": _rel_mse(guided_img, ref_img) - ref_rvar},
         "guided_over_plain": mse_g / mse_p if mse_p > 0 else None,
         "mse_x_frames": {"plain": mse_p * plain_frames, "guided": mse_g * guided_frames},
         "note": "1 spp per frame at 1920x1080; the reference is two separate plain renders "
@@ -609,8 +620,8 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
                            if learned or not k.startswith("Learned")})
         return t
 
-    ref_img, ref_var = _reference(lambda half: make("plain", 4242 + half),
-                                  args.learned_reference_spp // 4)
+    ref_img, ref_var, ref_rvar = _reference(lambda half: make("plain", 4242 + half),
+                                            args.learned_reference_spp // 4)
     out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp,
            "reference_variance": ref_var}
     kinds = (("plain", 11), ("wfpg_bxdf", 16), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
@@ -627,7 +638,8 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
         img, frames, used = _budget_image(t, args.learned_budget_ms, ms, torch)
         raw = float(np.mean((img - ref_img) ** 2))
         entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames, "device_ms": used,
-                 "mse": raw - ref_var, "mse_raw": raw}
+                 "mse": raw - ref_var, "mse_raw": raw,
+                 "rel_mse": _rel_mse(img, ref_img) - ref_rvar}
         if kind.startswith("learned"):
             entry["held_out_loss_last_frame"] = t.learned_loss()
             entry["train_steps_per_frame"] = int(kind.split("_")[1])
