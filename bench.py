@@ -128,6 +128,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def aggregate_ranks(dist, torch, ms: float, e2e_ms: float, rays: int, e2e_rays: int,
+                    device: str):
+    """Whole-job figures of the replicas: the slowest rank's times (the job
+    ends when its last replica does) and the sum of every rank's rays."""
+    tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=device)
+    rr = torch.tensor([rays, e2e_rays], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    dist.all_reduce(rr, op=dist.ReduceOp.SUM)
+    return float(tt[0]), float(tt[1]), int(rr[0]), int(rr[1])
+
+
 def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import torch
     import meturay_b200 as m
@@ -213,12 +224,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         if (args.learned and args.only == "all" and rank == 0 and world == 1) else None
 
     if dist:
-        tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-        rr = torch.tensor([rays, e2e_rays], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dist.all_reduce(rr, op=dist.ReduceOp.SUM)
-        ms, e2e_ms = float(tt[0]), float(tt[1])
-        rays, e2e_rays = int(rr[0]), int(rr[1])
+        ms, e2e_ms, rays, e2e_rays = aggregate_ranks(dist, torch, ms, e2e_ms, rays, e2e_rays,
+                                                     "cuda")
     if rank != 0:
         return None
 
