@@ -268,7 +268,8 @@ void mrb_tracer_destroy(mrb_tracer* t);
  * "NextEventEstimation", "RussianRouletteStart", "DirectLightMIS",
  * plus "Seed" (RNG key) and "Frame" (RNG iteration counter).  WFPGTracer
  * also takes (WFPGTracer.h:25-56) "OctreeLevel", "MinRayBinLevel",
- * "BinRayCount", "DoProductPathGuiding" (true only), "PurePG", "SkipPG",
+ * "BinRayCount", "DoProductPathGuiding" (true: product sampler; false: 2D
+ * piecewise-constant sampler over the field), "PurePG", "SkipPG",
  * "GuideBounceAmount", "OmitDirectRadiance". */
 int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t value);
 /* Floating-point WFPG options: "BXDF-GuideMISRatio", "RFieldFilterAlpha",

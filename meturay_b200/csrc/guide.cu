@@ -10,7 +10,8 @@
 //   k_bin_resolve     KCCheckReducedSVOBins / FindMarkedBin
 //   radix sort, k_bin_heads/k_bin_ranges
 //                     PartitionRaysWRTCustomData: rays grouped by bin
-//   k_guide<X>        KCGenAndSampleDistributionProduct
+//   k_guide<X, kProduct>  KCGenAndSampleDistributionProduct (kProduct) or
+//                     KCGenAndSampleDistribution (2D PWC over the field)
 //                     (WFPGTracerKC.cuh:1560-1766), one block per bin:
 //                     representative surface -> X*X cone traces through
 //                     the octree -> radiance read -> 11-tap Gaussian filter
@@ -202,6 +203,7 @@ struct GuideSmem {
     uint32_t repRid[kGuideWarps];
     float origin[4];
     float jitter[2];
+    float marg[X];      // non-product sampler: row marginal prefix sums
     ConePrefix prefix;  // the descent every cone of the bin shares
     uint32_t begin, end, key, bin;
     int nextTile;
@@ -251,7 +253,131 @@ __device__ __forceinline__ float product_pdf(const GuideSmem<X>& S, int warp, fl
     return S.pdfX[warp][cell] * S.pdfY[warp][ocy] * inner;
 }
 
+// KCGenAndSampleDistribution (WFPGTracerKC.cuh:1356-1559), the non-product
+// sampler of one bin: a 2D piecewise-constant distribution over the
+// filtered X x X field (S.field).  Row prefix sums run left to right, one
+// thread per row, into S.tmp; the marginal over rows bottom to top, by one
+// thread, into S.marg (both in float, in this order on both sides of the
+// oracle comparison).  Then one thread per ray: a draw from the
+// distribution (probability misRatio) or from the BxDF.  A draw takes the
+// first row whose prefix exceeds xi0 * total and the first cell of that row
+// whose prefix exceeds xi1 * rowTotal, with the offset inside the cell from
+// the remainder.  The density over the unit square is f * X^2 / total, over
+// the sphere (equal-area map) that / (4 pi).  The guide word carries the
+// one-sample MIS pdf as the product sampler's does.
 template <int X>
+__device__ __forceinline__ void pwc_sample_bin(const GuideArgs& A, GuideSmem<X>& S, uint32_t begin,
+                                               uint32_t end, uint32_t frame) {
+    const uint32_t tid = threadIdx.x;
+    const SceneDev& sc = A.sc;
+    if (tid < static_cast<uint32_t>(X)) {
+        float acc = 0.0f;
+        for (int x = 0; x < X; x++) {
+            acc += S.field[tid * X + x];
+            S.tmp[tid * X + x] = acc;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float acc = 0.0f;
+        for (int y = 0; y < X; y++) {
+            acc += S.tmp[y * X + X - 1];
+            S.marg[y] = acc;
+        }
+    }
+    __syncthreads();
+    const float total = S.marg[X - 1];
+    const float scale = static_cast<float>(X * X) / total;
+    const float below1 = 0x1.fffffep-1f;
+    auto pdf_at = [&](float u, float v) {
+        int ix = f2i_sat(floorf(u * static_cast<float>(X)));
+        int iy = f2i_sat(floorf(v * static_cast<float>(X)));
+        ix = ix < 0 ? 0 : (ix > X - 1 ? X - 1 : ix);
+        iy = iy < 0 ? 0 : (iy > X - 1 ? X - 1 : iy);
+        return S.field[iy * X + ix] * scale * kInv4Pi;
+    };
+    for (uint32_t r = tid; begin + r < end; r += kGuideTPB) {
+        const uint32_t rid = A.binRid[begin + r];
+        const uint32_t key = A.w.hit.key[rid];
+        const uint32_t batch = key >> kIdBits, id = key & kIdMask;
+        const float4 rd = A.w.rayD[rid];
+        const V3 d = v3(rd.x, rd.y, rd.z);
+        const RayAux aux = A.w.aux[rid];
+        const bool isLight = batch == kBatchLight;
+        const bool spec = !isLight && mat_specular(sc, batch, id);
+        const float2 hb = A.w.hit.bary[rid];
+        const Surface sf = gen_surface(sc, A.w.hit.prim[rid], hb.x, hb.y, d);
+        const V3 wi = -d;
+        const Rand4 r0 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 0u,
+                                         A.opt.seedLo, A.opt.seedHi);
+        const bool purePG = A.go.purePG != 0;
+        float s = 0.0f, t = 0.0f, pdf = 1.0f;
+        bool bxdfSel = true;
+        if (!purePG && (isLight || spec)) {
+            // SampleMIS early out: light or specular surface
+        } else if (!purePG && r0.u[0] >= A.go.misRatio) {
+            const Rand4 r1 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 1u,
+                                             A.opt.seedLo, A.opt.seedHi);
+            const BSample bs = mat_sample(sc, batch, id, wi, sf, aux.medium, r1.u[0], r1.u[1],
+                                          r1.u[2]);
+            dir_yup_to_octa(bs.dir, s, t);
+            const float pdfSampled = bs.pdf;
+            const float pdfOther = pdf_at(s, t);
+            const float ratio = 1.0f - A.go.misRatio;
+            const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+            pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+            pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            bxdfSel = true;
+        } else {
+            const float tY = r0.u[1] * total;
+            int lo = 0, hi = X - 1;  // first row whose prefix exceeds tY, else the last
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (S.marg[mid] > tY) hi = mid;
+                else lo = mid + 1;
+            }
+            const int y = lo;
+            const float rowTot = S.tmp[y * X + X - 1];
+            const float prevY = (y > 0) ? S.marg[y - 1] : 0.0f;
+            const float dv = fminf(fmaxf((tY - prevY) / rowTot, 0.0f), below1);
+            const float tX = r0.u[2] * rowTot;
+            lo = 0;
+            hi = X - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (S.tmp[y * X + mid] > tX) hi = mid;
+                else lo = mid + 1;
+            }
+            const int x = lo;
+            const float prevX = (x > 0) ? S.tmp[y * X + x - 1] : 0.0f;
+            const float du = fminf(fmaxf((tX - prevX) / S.field[y * X + x], 0.0f), below1);
+            const float rcpX = 1.0f / static_cast<float>(X);
+            s = (static_cast<float>(x) + du) * rcpX;
+            t = (static_cast<float>(y) + dv) * rcpX;
+            const float pdfSampled = S.field[y * X + x] * scale * kInv4Pi;
+            if (purePG) {
+                pdf = pdfSampled;
+            } else {
+                const V3 wo = octa_to_dir_yup(s, t);
+                const float pdfOther = mat_pdf(sc, batch, id, wo, wi, sf);
+                const float ratio = A.go.misRatio;
+                const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+                pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+                pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            }
+            bxdfSel = false;
+        }
+        if (pdf != pdf || s != s || t != t) {
+            s = 0.5f;
+            t = 0.5f;
+            pdf = 1.0f;
+        }
+        A.guide[rid] = make_uint2(uint32_t(f2h(s)) | (uint32_t(f2h(t)) << 16),
+                                  uint32_t(f2h(pdf)) | (bxdfSel ? kGuideBxdf : 0u) | kGuideValid);
+    }
+}
+
+template <int X, bool kProduct>
 __global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
     __shared__ GuideSmem<X> S;
     constexpr int DPP = X / 8;
@@ -387,150 +513,154 @@ __global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
             S.field[p] = acc;
         }
         __syncthreads();
-        // 8x8 outer field: mean and max of each DPP x DPP block
-        if (tid < 64) {
-            const int cx = static_cast<int>(tid) & 7, cy = static_cast<int>(tid) >> 3;
-            float sum = 0.0f, mx = 0.0f;
-            for (int iy = 0; iy < DPP; iy++)
-                for (int ix = 0; ix < DPP; ix++) {
-                    const float v = S.field[(cy * DPP + iy) * X + cx * DPP + ix];
-                    sum += v;
-                    mx = fmaxf(mx, v);
-                }
-            S.small[tid] = sum / static_cast<float>(DPP * DPP);
-            S.norm[tid] = mx;
-        }
-        __syncthreads();
-        // one warp per ray of the bin
-        for (uint32_t r = static_cast<uint32_t>(warp); begin + r < end; r += kGuideWarps) {
-            const uint32_t rid = A.binRid[begin + r];
-            const uint32_t key = A.w.hit.key[rid];
-            const uint32_t batch = key >> kIdBits, id = key & kIdMask;
-            const float4 rd = A.w.rayD[rid];
-            const V3 d = v3(rd.x, rd.y, rd.z);
-            const RayAux aux = A.w.aux[rid];
-            const bool isLight = batch == kBatchLight;
-            const bool spec = !isLight && mat_specular(sc, batch, id);
-            const float2 hb = A.w.hit.bary[rid];
-            const Surface sf = gen_surface(sc, A.w.hit.prim[rid], hb.x, hb.y, d);
-            const V3 wi = -d;
-            const V3 nrm = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
-            // MultiplyWithBXDF + GeneratePDFAndCDF
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                const int c = static_cast<int>(lane) + 32 * j;
-                const int cx = c & 7, cy = c >> 3;
-                float gray = 1.0f;
-                if (!isLight && !spec) {
-                    const V3 wo = bxdf_proj(cx, cy, nrm);
-                    gray = lum3(mat_eval(sc, batch, id, wo, wi, sf));
-                }
-                const float prod = fmaxf(kVeryLargeEpsilon, gray * S.small[c]);
-                const float incl = scan8(prod, lane);
-                const float rowTotal = __shfl_sync(0xFFFFFFFFu, incl, 7, 8);
-                const float rcp = 1.0f / rowTotal;
-                S.cdfX[warp][c] = incl * rcp;
-                S.pdfX[warp][c] = prod * 8.0f * rcp;
-                if ((lane & 7u) == 0) S.rowTot[warp][cy] = rowTotal;
+        if constexpr (!kProduct) {
+            pwc_sample_bin<X>(A, S, begin, end, frame);
+        } else {
+            // 8x8 outer field: mean and max of each DPP x DPP block
+            if (tid < 64) {
+                const int cx = static_cast<int>(tid) & 7, cy = static_cast<int>(tid) >> 3;
+                float sum = 0.0f, mx = 0.0f;
+                for (int iy = 0; iy < DPP; iy++)
+                    for (int ix = 0; ix < DPP; ix++) {
+                        const float v = S.field[(cy * DPP + iy) * X + cx * DPP + ix];
+                        sum += v;
+                        mx = fmaxf(mx, v);
+                    }
+                S.small[tid] = sum / static_cast<float>(DPP * DPP);
+                S.norm[tid] = mx;
             }
-            __syncwarp();
-            {
-                const float py = (lane < 8) ? S.rowTot[warp][lane] : 0.0f;
-                const float incl = scan8(py, lane);
-                const float colTotal = __shfl_sync(0xFFFFFFFFu, incl, 7, 8);
-                const float rcp = 1.0f / colTotal;
-                if (lane < 8) {
-                    S.cdfY[warp][lane] = incl * rcp;
-                    S.pdfY[warp][lane] = py * (8.0f * rcp);
+            __syncthreads();
+            // one warp per ray of the bin
+            for (uint32_t r = static_cast<uint32_t>(warp); begin + r < end; r += kGuideWarps) {
+                const uint32_t rid = A.binRid[begin + r];
+                const uint32_t key = A.w.hit.key[rid];
+                const uint32_t batch = key >> kIdBits, id = key & kIdMask;
+                const float4 rd = A.w.rayD[rid];
+                const V3 d = v3(rd.x, rd.y, rd.z);
+                const RayAux aux = A.w.aux[rid];
+                const bool isLight = batch == kBatchLight;
+                const bool spec = !isLight && mat_specular(sc, batch, id);
+                const float2 hb = A.w.hit.bary[rid];
+                const Surface sf = gen_surface(sc, A.w.hit.prim[rid], hb.x, hb.y, d);
+                const V3 wi = -d;
+                const V3 nrm = to_space(v3(0.0f, 0.0f, 1.0f), sf.w2t);
+                // MultiplyWithBXDF + GeneratePDFAndCDF
+    #pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int c = static_cast<int>(lane) + 32 * j;
+                    const int cx = c & 7, cy = c >> 3;
+                    float gray = 1.0f;
+                    if (!isLight && !spec) {
+                        const V3 wo = bxdf_proj(cx, cy, nrm);
+                        gray = lum3(mat_eval(sc, batch, id, wo, wi, sf));
+                    }
+                    const float prod = fmaxf(kVeryLargeEpsilon, gray * S.small[c]);
+                    const float incl = scan8(prod, lane);
+                    const float rowTotal = __shfl_sync(0xFFFFFFFFu, incl, 7, 8);
+                    const float rcp = 1.0f / rowTotal;
+                    S.cdfX[warp][c] = incl * rcp;
+                    S.pdfX[warp][c] = prod * 8.0f * rcp;
+                    if ((lane & 7u) == 0) S.rowTot[warp][cy] = rowTotal;
                 }
-            }
-            __syncwarp();
-            const Rand4 r0 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 0u,
-                                             A.opt.seedLo, A.opt.seedHi);
-            const bool purePG = A.go.purePG != 0;
-            float s = 0.0f, t = 0.0f, pdf = 1.0f;
-            bool bxdfSel = true;
-            if (!purePG && (isLight || spec)) {
-                // SampleMIS early out: light or specular surface
-            } else if (!purePG && r0.u[0] >= A.go.misRatio) {
-                // BxDF sample, guide pdf of its direction
-                const Rand4 r1 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 1u,
-                                                 A.opt.seedLo, A.opt.seedHi);
-                const BSample bs = mat_sample(sc, batch, id, wi, sf, aux.medium, r1.u[0], r1.u[1],
-                                              r1.u[2]);
-                dir_yup_to_octa(bs.dir, s, t);
-                const float pdfSampled = bs.pdf;
-                const float pdfOther = product_pdf<X>(S, warp, s, t) * kInv4Pi;
-                const float ratio = 1.0f - A.go.misRatio;
-                const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
-                pdf = pdfSampled * ratio / (w0 / (w0 + w1));
-                pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
-                bxdfSel = true;
-            } else {
-                // ProductSampler::Sample (ProductSampler.cuh:337-470)
-                const float xi0 = r0.u[1], xi1 = r0.u[2];
-                const float cY = (lane < 8) ? S.cdfY[warp][lane] : 0.0f;
-                uint32_t mask = __ballot_sync(0xFFFFFFFFu, lane < 8 && xi0 > cY);
-                int rowId = __ffs(~mask) - 1;
-                rowId = rowId > 7 ? 7 : rowId;
-                const float cX = (lane < 8) ? S.cdfX[warp][rowId * 8 + static_cast<int>(lane)] : 0.0f;
-                mask = __ballot_sync(0xFFFFFFFFu, lane < 8 && xi1 > cX);
-                int colId = __ffs(~mask) - 1;
-                colId = colId > 7 ? 7 : colId;
-                const int cell = rowId * 8 + colId;
-                const float normC = S.norm[cell];
-                float u = 0.0f, v = 0.0f, tex = 0.0f;
-                int lucky = -1;
-                for (int round = 0; round < 24; round++) {
-                    const Rand4 rl = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag,
-                                                     2u + static_cast<uint32_t>(round) * 32u + lane,
-                                                     A.opt.seedLo, A.opt.seedHi);
-                    u = rl.u[0];
-                    v = rl.u[1];
-                    const int ix = f2i_sat(u * dppF), iy = f2i_sat(v * dppF);
-                    tex = S.field[(rowId * DPP + iy) * X + colId * DPP + ix];
-                    const float nv = tex / normC;
-                    const uint32_t acc = __ballot_sync(0xFFFFFFFFu, rl.u[2] <= nv);
-                    lucky = __ffs(acc) - 1;
-                    if (lucky >= 0) {
-                        u = __shfl_sync(0xFFFFFFFFu, u, lucky);
-                        v = __shfl_sync(0xFFFFFFFFu, v, lucky);
-                        tex = __shfl_sync(0xFFFFFFFFu, tex, lucky);
-                        break;
+                __syncwarp();
+                {
+                    const float py = (lane < 8) ? S.rowTot[warp][lane] : 0.0f;
+                    const float incl = scan8(py, lane);
+                    const float colTotal = __shfl_sync(0xFFFFFFFFu, incl, 7, 8);
+                    const float rcp = 1.0f / colTotal;
+                    if (lane < 8) {
+                        S.cdfY[warp][lane] = incl * rcp;
+                        S.pdfY[warp][lane] = py * (8.0f * rcp);
                     }
                 }
-                u = __shfl_sync(0xFFFFFFFFu, u, 0);
-                v = __shfl_sync(0xFFFFFFFFu, v, 0);
-                tex = __shfl_sync(0xFFFFFFFFu, tex, 0);
-                const float pdfInner = (lucky >= 0) ? tex / S.small[cell] : 1.0f;
-                const float pdfS = S.pdfY[warp][rowId] * S.pdfX[warp][cell] * pdfInner;
-                const float rcpX = 1.0f / static_cast<float>(X);
-                s = (static_cast<float>(colId) * dppF + u * dppF) * rcpX;
-                t = (static_cast<float>(rowId) * dppF + v * dppF) * rcpX;
-                if (purePG) {
-                    pdf = pdfS * kInv4Pi;
-                } else {
-                    const float pdfSampled = pdfS * kInv4Pi;
-                    const V3 wo = octa_to_dir_yup(s, t);
-                    const float pdfOther = mat_pdf(sc, batch, id, wo, wi, sf);
-                    const float ratio = A.go.misRatio;
+                __syncwarp();
+                const Rand4 r0 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 0u,
+                                                 A.opt.seedLo, A.opt.seedHi);
+                const bool purePG = A.go.purePG != 0;
+                float s = 0.0f, t = 0.0f, pdf = 1.0f;
+                bool bxdfSel = true;
+                if (!purePG && (isLight || spec)) {
+                    // SampleMIS early out: light or specular surface
+                } else if (!purePG && r0.u[0] >= A.go.misRatio) {
+                    // BxDF sample, guide pdf of its direction
+                    const Rand4 r1 = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag, 1u,
+                                                     A.opt.seedLo, A.opt.seedHi);
+                    const BSample bs = mat_sample(sc, batch, id, wi, sf, aux.medium, r1.u[0], r1.u[1],
+                                                  r1.u[2]);
+                    dir_yup_to_octa(bs.dir, s, t);
+                    const float pdfSampled = bs.pdf;
+                    const float pdfOther = product_pdf<X>(S, warp, s, t) * kInv4Pi;
+                    const float ratio = 1.0f - A.go.misRatio;
                     const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
                     pdf = pdfSampled * ratio / (w0 / (w0 + w1));
                     pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+                    bxdfSel = true;
+                } else {
+                    // ProductSampler::Sample (ProductSampler.cuh:337-470)
+                    const float xi0 = r0.u[1], xi1 = r0.u[2];
+                    const float cY = (lane < 8) ? S.cdfY[warp][lane] : 0.0f;
+                    uint32_t mask = __ballot_sync(0xFFFFFFFFu, lane < 8 && xi0 > cY);
+                    int rowId = __ffs(~mask) - 1;
+                    rowId = rowId > 7 ? 7 : rowId;
+                    const float cX = (lane < 8) ? S.cdfX[warp][rowId * 8 + static_cast<int>(lane)] : 0.0f;
+                    mask = __ballot_sync(0xFFFFFFFFu, lane < 8 && xi1 > cX);
+                    int colId = __ffs(~mask) - 1;
+                    colId = colId > 7 ? 7 : colId;
+                    const int cell = rowId * 8 + colId;
+                    const float normC = S.norm[cell];
+                    float u = 0.0f, v = 0.0f, tex = 0.0f;
+                    int lucky = -1;
+                    for (int round = 0; round < 24; round++) {
+                        const Rand4 rl = philox_uniform4(aux.sample, frame, kTagGuide | A.depthTag,
+                                                         2u + static_cast<uint32_t>(round) * 32u + lane,
+                                                         A.opt.seedLo, A.opt.seedHi);
+                        u = rl.u[0];
+                        v = rl.u[1];
+                        const int ix = f2i_sat(u * dppF), iy = f2i_sat(v * dppF);
+                        tex = S.field[(rowId * DPP + iy) * X + colId * DPP + ix];
+                        const float nv = tex / normC;
+                        const uint32_t acc = __ballot_sync(0xFFFFFFFFu, rl.u[2] <= nv);
+                        lucky = __ffs(acc) - 1;
+                        if (lucky >= 0) {
+                            u = __shfl_sync(0xFFFFFFFFu, u, lucky);
+                            v = __shfl_sync(0xFFFFFFFFu, v, lucky);
+                            tex = __shfl_sync(0xFFFFFFFFu, tex, lucky);
+                            break;
+                        }
+                    }
+                    u = __shfl_sync(0xFFFFFFFFu, u, 0);
+                    v = __shfl_sync(0xFFFFFFFFu, v, 0);
+                    tex = __shfl_sync(0xFFFFFFFFu, tex, 0);
+                    const float pdfInner = (lucky >= 0) ? tex / S.small[cell] : 1.0f;
+                    const float pdfS = S.pdfY[warp][rowId] * S.pdfX[warp][cell] * pdfInner;
+                    const float rcpX = 1.0f / static_cast<float>(X);
+                    s = (static_cast<float>(colId) * dppF + u * dppF) * rcpX;
+                    t = (static_cast<float>(rowId) * dppF + v * dppF) * rcpX;
+                    if (purePG) {
+                        pdf = pdfS * kInv4Pi;
+                    } else {
+                        const float pdfSampled = pdfS * kInv4Pi;
+                        const V3 wo = octa_to_dir_yup(s, t);
+                        const float pdfOther = mat_pdf(sc, batch, id, wo, wi, sf);
+                        const float ratio = A.go.misRatio;
+                        const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+                        pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+                        pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+                    }
+                    bxdfSel = false;
                 }
-                bxdfSel = false;
-            }
-            if (lane == 0) {
-                if (pdf != pdf || s != s || t != t) {
-                    s = 0.5f;
-                    t = 0.5f;
-                    pdf = 1.0f;
+                if (lane == 0) {
+                    if (pdf != pdf || s != s || t != t) {
+                        s = 0.5f;
+                        t = 0.5f;
+                        pdf = 1.0f;
+                    }
+                    A.guide[rid] = make_uint2(uint32_t(f2h(s)) | (uint32_t(f2h(t)) << 16),
+                                              uint32_t(f2h(pdf)) | (bxdfSel ? kGuideBxdf : 0u) |
+                                                  kGuideValid);
                 }
-                A.guide[rid] = make_uint2(uint32_t(f2h(s)) | (uint32_t(f2h(t)) << 16),
-                                          uint32_t(f2h(pdf)) | (bxdfSel ? kGuideBxdf : 0u) |
-                                              kGuideValid);
+                __syncwarp();
             }
-            __syncwarp();
         }
         __syncthreads();
     }
@@ -797,10 +927,22 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
     const uint32_t kernelIndex = iteration < 4 ? iteration : 4;
     switch (kernelIndex) {
         case 0:
-        case 1: k_guide<64><<<148 * 4, kGuideTPB, 0, st>>>(ga); break;
-        case 2: k_guide<32><<<148 * 4, kGuideTPB, 0, st>>>(ga); break;
-        case 3: k_guide<16><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;
-        default: k_guide<8><<<148 * 6, kGuideTPB, 0, st>>>(ga); break;
+        case 1:
+            if (go.product) k_guide<64, true><<<148 * 4, kGuideTPB, 0, st>>>(ga);
+            else k_guide<64, false><<<148 * 4, kGuideTPB, 0, st>>>(ga);
+            break;
+        case 2:
+            if (go.product) k_guide<32, true><<<148 * 4, kGuideTPB, 0, st>>>(ga);
+            else k_guide<32, false><<<148 * 4, kGuideTPB, 0, st>>>(ga);
+            break;
+        case 3:
+            if (go.product) k_guide<16, true><<<148 * 6, kGuideTPB, 0, st>>>(ga);
+            else k_guide<16, false><<<148 * 6, kGuideTPB, 0, st>>>(ga);
+            break;
+        default:
+            if (go.product) k_guide<8, true><<<148 * 6, kGuideTPB, 0, st>>>(ga);
+            else k_guide<8, false><<<148 * 6, kGuideTPB, 0, st>>>(ga);
+            break;
     }
     MRB_CUDA(cudaGetLastError());
     return 0;

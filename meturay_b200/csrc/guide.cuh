@@ -22,7 +22,8 @@ int svo_normalize_filter(const GuideDev& g, const SvoResult& v, cudaStream_t st)
 struct GuideOptions {
     uint32_t minBinLevel;   // MinRayBinLevel clamped to the leaf depth
     uint32_t binRayCount;   // BinRayCount
-    uint32_t purePG;        // PurePG: product sample only, no BxDF MIS
+    uint32_t purePG;        // PurePG: guide sample only, no BxDF MIS
+    uint32_t product;       // DoProductPathGuiding: product sampler, else 2D PWC over the field
     float misRatio;         // BXDF-GuideMISRatio (probability of the guide)
     float filter[11];       // normalised Gaussian taps, RFieldFilterAlpha
 };

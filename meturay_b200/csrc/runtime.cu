@@ -511,6 +511,7 @@ GuideOptions guide_options(const mrb_tracer* t) {
     g.minBinLevel = std::min(t->octreeLevel, t->minRayBinLevel);
     g.binRayCount = t->binRayCount;
     g.purePG = t->purePG;
+    g.product = t->productPG;
     g.misRatio = t->misRatio;
     // StaticGaussianFilter1D<11> (BlockTextureFilter.cuh:72-110): taps
     // exp(-t^2 / (2 alpha)) normalised to sum 1, evaluated in double
@@ -1344,11 +1345,7 @@ int mrb_tracer_set_option(mrb_tracer* t, const char* name, uint64_t v) {
         }
         t->binRayCount = uint32_t(v);
     } else if (t->wfpg && k == "DoProductPathGuiding") {
-        if (!v) {
-            set_error("DoProductPathGuiding=false (non-product 2D PWC guiding) is not built");
-            return MRB_E_UNSUPPORTED;
-        }
-        t->productPG = 1;
+        t->productPG = v ? 1 : 0;
     } else if (t->wfpg && k == "PurePG") {
         t->purePG = v ? 1 : 0;
     } else if (t->wfpg && k == "SkipPG") {

@@ -2308,6 +2308,110 @@ struct WRay {
     float t = 0.0f, b0 = 0.0f, b1 = 0.0f;
 };
 
+// The non-product sampler of one bin (KCGenAndSampleDistribution,
+// WFPGTracerKC.cuh:1356-1559): a 2D piecewise-constant distribution over
+// the filtered X x X field, one ray at a time.  Row prefix sums run left to
+// right, the marginal over rows bottom to top, both in float; a sample
+// takes the first row whose prefix exceeds xi0 * total, then the first cell
+// of that row whose prefix exceeds xi1 * rowTotal, with the offset inside
+// the cell from the remainder.  Density over the unit square: f * X^2 /
+// total; over the sphere (equal-area map): that / (4 pi).
+template <int X>
+void guide_bin_pwc(const oracle_scene* s, const oracle_options* opt,
+                   const oracle_wfpg_options* w, uint32_t depthTag, const std::vector<float>& field,
+                   const std::vector<uint32_t>& rays, std::vector<WRay>& wave) {
+    const uint32_t frame = opt->frame;
+    std::vector<float> rowPre(X * X);
+    float marg[X];
+    for (int y = 0; y < X; y++) {
+        float acc = 0.0f;
+        for (int x = 0; x < X; x++) {
+            acc += field[y * X + x];
+            rowPre[y * X + x] = acc;
+        }
+    }
+    {
+        float acc = 0.0f;
+        for (int y = 0; y < X; y++) {
+            acc += rowPre[y * X + X - 1];
+            marg[y] = acc;
+        }
+    }
+    const float total = marg[X - 1];
+    const float scale = static_cast<float>(X * X) / total;
+    const float kInv4Pi = 0.25f * kInvPiF;
+    const float below1 = 0x1.fffffep-1f;
+    auto pdf_at = [&](float u, float v) {
+        int ix = f2i_sat(std::floor(u * static_cast<float>(X)));
+        int iy = f2i_sat(std::floor(v * static_cast<float>(X)));
+        ix = std::min(std::max(ix, 0), X - 1);
+        iy = std::min(std::max(iy, 0), X - 1);
+        return field[iy * X + ix] * scale * kInv4Pi;
+    };
+    for (uint32_t i : rays) {
+        WRay& wr = wave[i];
+        const uint32_t batch = wr.key >> 24, id = wr.key & 0xFFFFFFu;
+        const bool isLight = batch == kBatchLight;
+        const bool spec = !isLight && mat_specular(s, batch, id);
+        const Surface<float> sf = gen_surface(s, wr.prim, wr.b0, wr.b1, wr.r.d);
+        const F3 wi = -wr.r.d;
+        const uint32_t smp = wr.r.aux.sample;
+        const Rng4 r0 = rng_block(smp, frame, kTagGuide | depthTag, 0u, opt->seed_lo, opt->seed_hi);
+        const bool purePG = w->pure_pg != 0;
+        float ss = 0.0f, tt = 0.0f, pdf = 1.0f;
+        bool bxdfSel = true;
+        if (!purePG && (isLight || spec)) {
+        } else if (!purePG && r0.u[0] >= w->mis_ratio) {
+            const Rng4 r1 = rng_block(smp, frame, kTagGuide | depthTag, 1u, opt->seed_lo, opt->seed_hi);
+            const BSample<float> bs = mat_sample(s, batch, id, wi, sf, wr.r.aux.medium, r1.u[0], r1.u[1], r1.u[2]);
+            dir_yup_to_octa(bs.dir, ss, tt);
+            const float pdfSampled = bs.pdf;
+            const float pdfOther = pdf_at(ss, tt);
+            const float ratio = 1.0f - w->mis_ratio;
+            const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+            pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+            pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            bxdfSel = true;
+        } else {
+            const float tY = r0.u[1] * total;
+            int y = X - 1;
+            for (int k = 0; k < X; k++)
+                if (marg[k] > tY) { y = k; break; }
+            const float rowTot = rowPre[y * X + X - 1];
+            const float prevY = (y > 0) ? marg[y - 1] : 0.0f;
+            const float dv = std::min(std::max((tY - prevY) / rowTot, 0.0f), below1);
+            const float tX = r0.u[2] * rowTot;
+            int x = X - 1;
+            for (int k = 0; k < X; k++)
+                if (rowPre[y * X + k] > tX) { x = k; break; }
+            const float prevX = (x > 0) ? rowPre[y * X + x - 1] : 0.0f;
+            const float du = std::min(std::max((tX - prevX) / field[y * X + x], 0.0f), below1);
+            const float rcpX = 1.0f / static_cast<float>(X);
+            ss = (static_cast<float>(x) + du) * rcpX;
+            tt = (static_cast<float>(y) + dv) * rcpX;
+            const float pdfSampled = field[y * X + x] * scale * kInv4Pi;
+            if (purePG) {
+                pdf = pdfSampled;
+            } else {
+                const F3 wo = octa_to_dir_yup(ss, tt);
+                const float pdfOther = mat_pdf(s, batch, id, wo, wi, sf);
+                const float ratio = w->mis_ratio;
+                const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+                pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+                pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            }
+            bxdfSel = false;
+        }
+        if (pdf != pdf || ss != ss || tt != tt) {
+            ss = 0.5f;
+            tt = 0.5f;
+            pdf = 1.0f;
+        }
+        wr.g0 = uint32_t(f2h(ss)) | (uint32_t(f2h(tt)) << 16);
+        wr.g1 = uint32_t(f2h(pdf)) | (bxdfSel ? kGuideBxdf : 0u) | kGuideValid;
+    }
+}
+
 // One bin of KCGenAndSampleDistributionProduct, X x X field
 template <int X>
 void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* opt,
@@ -2368,6 +2472,10 @@ void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* op
             acc += tmp[ny * X + nx] * w->filter[j + 5];
         }
         field[p] = acc;
+    }
+    if (!w->product) {
+        guide_bin_pwc<X>(s, opt, w, depthTag, field, rays, wave);
+        return;
     }
     float small[64], normc[64];
     for (int c = 0; c < 64; c++) {

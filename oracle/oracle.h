@@ -177,6 +177,7 @@ typedef struct oracle_wfpg_options {
     float mis_ratio;
     float filter[11];
     uint32_t dump_iteration;
+    uint32_t product;  /* 1: KCGenAndSampleDistributionProduct, 0: KCGenAndSampleDistribution */
 } oracle_wfpg_options;
 uint64_t oracle_render_wfpg(const oracle_scene* scene, const oracle_bvh* bvh,
                             const oracle_camera* cam, const oracle_options* opt,

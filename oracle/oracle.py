@@ -225,7 +225,7 @@ class OracleScene:
                     frame: int = 0, mis: bool = False, min_bin_level: int = 5,
                     bin_ray_count: int = 512, pure_pg: bool = False, skip_pg: bool = False,
                     guide_bounce: int = 512, mis_ratio: float = 0.5, filter_alpha: float = 1.0,
-                    dump_iteration: int | None = None, threads: int = 0):
+                    dump_iteration: int | None = None, threads: int = 0, product: bool = True):
         """One WFPG frame; returns per-sample radiance, rays traced and the
         guide words / bin ids (per path) of step dump_iteration."""
         cam = Camera()
@@ -246,6 +246,7 @@ class OracleScene:
         w.guide_bounce = guide_bounce
         w.mis_ratio = float(mis_ratio)
         w.filter[:] = [float(v) for v in gauss_taps(filter_alpha)]
+        w.product = 1 if product else 0
         w.dump_iteration = 0xFFFFFFFF if dump_iteration is None else int(dump_iteration)
         paths = width * samples * height * samples
         out = np.zeros((height * samples, width * samples, 3), np.float32)
@@ -322,7 +323,7 @@ class WfpgOptions(C.Structure):
     _fields_ = [("min_bin_level", C.c_uint32), ("bin_ray_count", C.c_uint32),
                 ("pure_pg", C.c_uint32), ("skip_pg", C.c_uint32), ("guide_bounce", C.c_uint32),
                 ("mis_ratio", C.c_float), ("filter", C.c_float * 11),
-                ("dump_iteration", C.c_uint32)]
+                ("dump_iteration", C.c_uint32), ("product", C.c_uint32)]
 
 
 def gauss_taps(alpha: float) -> np.ndarray:

@@ -74,7 +74,8 @@ def _oracle_kwargs(opts):
                 guide_bounce=opts.get("GuideBounceAmount", 512),
                 mis_ratio=opts.get("BXDF-GuideMISRatio", 0.5),
                 filter_alpha=opts.get("RFieldFilterAlpha", 1.0),
-                mis=bool(opts.get("DirectLightMIS", 0)))
+                mis=bool(opts.get("DirectLightMIS", 0)),
+                product=bool(opts.get("DoProductPathGuiding", 1)))
 
 
 def _cam(scene):
@@ -82,10 +83,14 @@ def _cam(scene):
     return np.concatenate([camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
 
 
-def test_guide_words_and_bins_match_oracle(system, oracle):
+@pytest.mark.parametrize("product", [1, 0])
+def test_guide_words_and_bins_match_oracle(system, oracle, product):
+    """Per-ray bins and guide words of the first wavefront, for the product
+    sampler and for the 2D piecewise-constant sampler over the field
+    (DoProductPathGuiding false)."""
     from meturay_b200 import scenes
     scene = scenes.cornell(seed=6, width=32, height=32, mixed=True)
-    opts = dict(WFPG_OPTS)
+    opts = dict(WFPG_OPTS, DoProductPathGuiding=product)
     g, t = _wfpg(system, scene, opts)
     t.generate_work()
     t.render()
@@ -108,15 +113,18 @@ def test_guide_words_and_bins_match_oracle(system, oracle):
     assert np.array_equal(valid, (dg[smp][:, 1] >> 17) & 1)
 
 
-@pytest.mark.parametrize("variant", ["mis", "pure", "mis_nee_mis"])
+@pytest.mark.parametrize("variant", ["mis", "pure", "mis_nee_mis", "nonproduct",
+                                     "nonproduct_pure"])
 def test_wfpg_frames_match_oracle(system, oracle, variant):
     """Two stepwise frames: per-sample radiance and the octree payload after
     each frame's deposit."""
     from meturay_b200 import scenes
     scene = scenes.cornell(seed=6, width=32, height=32, mixed=True)
     opts = dict(WFPG_OPTS)
-    if variant == "pure":
+    if variant in ("pure", "nonproduct_pure"):
         opts["PurePG"] = 1
+    if variant.startswith("nonproduct"):
+        opts["DoProductPathGuiding"] = 0
     if variant == "mis_nee_mis":
         opts["DirectLightMIS"] = 1
         opts["BXDF-GuideMISRatio"] = 0.7
