@@ -565,9 +565,12 @@ def run_serving(args, m, system) -> dict:
 # ---- learned guiding (C5) ------------------------------------------------
 C1 = {"Samples": 2, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
       "DirectLightMIS": 0}
+# GuideBounceAmount 2: both guiders guide the first two bounces, where the
+# indirect light they learn is; later bounces carry little of the image and
+# their guiding costs more than it returns (shielded scene, four seeds)
 LEARNED = {"LearnedGuiding": 1, "LearnedWarmupFrames": 16, "LearnedTrainSteps": 1,
            "LearnedSamples": 65536, "LearnedWarmupOctree": 0, "OctreeLevel": 10,
-           "MinRayBinLevel": 5, "BinRayCount": 512}
+           "MinRayBinLevel": 5, "BinRayCount": 512, "GuideBounceAmount": 2}
 LEARNED_FLOATS = {"LearnedRate": 1e-2, "LearnedWeightMax": 5.0, "BXDF-GuideMISRatio": 0.5,
                   "RFieldFilterAlpha": 0.6}
 
@@ -659,6 +662,14 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
         out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
         out["learned_over_wfpg_bxdf"] = out["learned"]["mse"] / out["wfpg_bxdf"]["mse"]
         out["learned_over_svo"] = out["learned"]["mse"] / out["svo"]["mse"]
+        # the same ratios on the relative MSE (the learned variant with the
+        # lowest one), which rare high-energy paths move less
+        best_rel = min(("learned_1", "learned_4", "learned_1_octree"),
+                       key=lambda k: out[k]["rel_mse"])
+        out["rel_mse_learned_variant"] = best_rel
+        out["learned_over_plain_rel"] = out[best_rel]["rel_mse"] / out["plain"]["rel_mse"]
+        out["learned_over_wfpg_bxdf_rel"] = (out[best_rel]["rel_mse"]
+                                             / out["wfpg_bxdf"]["rel_mse"])
         # per-sample efficiency (MSE x spp; lower is better), which the frame
         # cost then trades against
         out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
