@@ -340,6 +340,14 @@ def _reference(make, frames: int):
     return ref, float(np.mean(d2)) / 4.0, float(np.mean(d2 / (ref * ref + 0.01))) / 4.0
 
 
+def _clamped_mse(img, ref) -> float:
+    """MSE after clamping both images at the reference's 99.9th percentile:
+    a score that a single firefly pixel cannot dominate (it is biased, so
+    it only ranks samplers; it is not an error estimate)."""
+    c = float(np.percentile(ref, 99.9))
+    return float(np.mean((np.minimum(img, c) - np.minimum(ref, c)) ** 2))
+
+
 def _rel_mse(img, ref) -> float:
     """Relative MSE, mean((x - r)^2 / (r^2 + 0.01)): bright outliers weigh
     less than in the MSE, so it moves less with rare high-energy paths."""
@@ -408,6 +416,24 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     gt.set_options(GUIDED_FLOATS)
     _attach_filter(g.system, gt)
     guided_img, guided_frames, guided_used = _budget_image(gt, budget, guided_ms, torch)
+    # the same guider with coarser ray bins (MinRayBinLevel 3, BinRayCount
+    # 4096): fewer radiance fields per wavefront, each shared by more rays
+    coarse = dict(GUIDED_OPTS, MinRayBinLevel=3, BinRayCount=4096)
+    gc = m.WFPGTracer(g.system, g)
+    gc.set_options(dict(coarse, Seed=101))
+    gc.set_options(GUIDED_FLOATS)
+    _attach_filter(g.system, gc)
+    for _ in range(3):
+        gc.render_frame()
+    gc_ms = _frame_ms(gc, torch, frames=10)
+    gc.close()
+    gc = m.WFPGTracer(g.system, g)
+    gc.set_options(dict(coarse, Seed=202))
+    gc.set_options(GUIDED_FLOATS)
+    _attach_filter(g.system, gc)
+    coarse_img, coarse_frames, coarse_used = _budget_image(gc, budget, gc_ms, torch)
+    gc.close()
+    raw_c = float(np.mean((coarse_img - ref_img) ** 2))
     raw_p = float(np.mean((plain_img - ref_img) ** 2))
     raw_g = float(np.mean((guided_img - ref_img) ** 2))
     mse_p, mse_g = raw_p - ref_var, raw_g - ref_var
@@ -416,10 +442,18 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
         "reference_variance": ref_var,
         "plain": {"frames": plain_frames, "ms_per_frame": plain_ms, "device_ms": plain_used,
                   "mse": mse_p, "mse_raw": raw_p,
-                  "rel_mse": _rel_mse(plain_img, ref_img) - ref_rvar},
+                  "rel_mse": _rel_mse(plain_img, ref_img) - ref_rvar,
+                  "clamped_mse": _clamped_mse(plain_img, ref_img)},
         "guided": {"frames": guided_frames, "ms_per_frame": guided_ms,
                    "device_ms": guided_used, "mse": mse_g, "mse_raw": raw_g,
-                   "rel_mse": _rel_mse(guided_img, ref_img) - ref_rvar},
+                   "rel_mse": _rel_mse(guided_img, ref_img) - ref_rvar,
+                   "clamped_mse": _clamped_mse(guided_img, ref_img)},
+        "guided_coarse_bins": {"MinRayBinLevel": 3, "BinRayCount": 4096,
+                               "frames": coarse_frames, "ms_per_frame": gc_ms,
+                               "device_ms": coarse_used, "mse": raw_c - ref_var,
+                               "mse_raw": raw_c,
+                               "rel_mse": _rel_mse(coarse_img, ref_img) - ref_rvar,
+                               "clamped_mse": _clamped_mse(coarse_img, ref_img)},
         "guided_over_plain": mse_g / mse_p if mse_p > 0 else None,
         "mse_x_frames": {"plain": mse_p * plain_frames, "guided": mse_g * guided_frames},
         "note": "1 spp per frame at 1920x1080; the reference is two separate plain renders "
@@ -649,7 +683,8 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
         raw = float(np.mean((img - ref_img) ** 2))
         entry = {"ms_per_frame": ms, "frames": frames, "spp": 4 * frames, "device_ms": used,
                  "mse": raw - ref_var, "mse_raw": raw,
-                 "rel_mse": _rel_mse(img, ref_img) - ref_rvar}
+                 "rel_mse": _rel_mse(img, ref_img) - ref_rvar,
+                 "clamped_mse": _clamped_mse(img, ref_img)}
         if kind.startswith("learned"):
             entry["held_out_loss_last_frame"] = t.learned_loss()
             entry["train_steps_per_frame"] = int(kind.split("_")[1])
