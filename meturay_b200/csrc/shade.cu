@@ -58,11 +58,27 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
     const uint32_t frame = *opt.frame;
     const CameraDev cam = *camPtr;
     if (blockIdx.x == 0 && threadIdx.x == 0) *count = total;
-    for (uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x; sid < total;
-         sid += gridDim.x * blockDim.x) {
-        const uint32_t sx = sid % SW, sy = sid / SW;
+    // wavefront slot i -> sample: 8 x 4 sample tiles, so that the 32 camera
+    // rays of a warp cover a compact patch of the image (more shared node
+    // visits in the first traversal).  Every ray carries its sample id,
+    // which keys its random numbers and its outputs, so the order of the
+    // wavefront changes no result.
+    const bool tiled = (SW % 8u == 0u) && (SH % 4u == 0u);
+    const uint32_t tilesX = SW / 8u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += gridDim.x * blockDim.x) {
+        uint32_t sx, sy;
+        if (tiled) {
+            const uint32_t tile = i >> 5, w = i & 31u;
+            sx = (tile % tilesX) * 8u + (w & 7u);
+            sy = (tile / tilesX) * 4u + (w >> 3);
+        } else {
+            sx = i % SW;
+            sy = i / SW;
+        }
+        const uint32_t sid = sy * SW + sx;
         Rand4 rc = philox_uniform4(sid, frame, kTagCamera, 0u, opt.seedLo, opt.seedHi);
-        camera_ray(cam, sx, sy, SW, SH, rc, rayO[sid], rayD[sid]);
+        camera_ray(cam, sx, sy, SW, SH, rc, rayO[i], rayD[i]);
         RayAux a;
         a.rf[0] = a.rf[1] = a.rf[2] = 1.0f;
         a.sample = sid;
@@ -74,7 +90,7 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
         a.type = kCameraRay;
         a.prevPDF = __int_as_float(0x7fc00000);
         a.pad = 0;
-        aux[sid] = a;
+        aux[i] = a;
         samples[sid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         // image-space coordinates for the reconstruction filter
         // (GPUCameraPinhole::GenerateRay localCoords * resolution,
