@@ -2,7 +2,7 @@
 
 The oracle restates PathTracerKC.cuh (NEE, Russian roulette, Lambert /
 Metal / Refract BxDFs, primitive lights) with the same counter-based RNG and
-the same FP32 operation order.  Tolerance: relative mean
+the same FP32 operation order.  Tolerance (the drop-in's bar): relative mean
 error of the per-pixel radiance below 1e-4; in practice the images agree to
 float atomic-addition order.  The FP64 oracle's error is reported, not bounded.
 """
