@@ -475,7 +475,7 @@ def _log_uniform(rng, lo, hi):
 
 
 def _pool_scenes(m, system, rng, n, tris):
-    """n seeded Cornell-style scenes (config-1 generator), triangle counts
+    """n seeded Cornell-style scenes (the 8k-triangle Cornell generator), triangle counts
     log-uniform in `tris` through the spheres' tessellation."""
     out = []
     for i in range(n):
@@ -488,7 +488,7 @@ def _pool_scenes(m, system, rng, n, tris):
 
 
 def run_batching(args, m, system, torch) -> dict:
-    """C3: one frame of 16 spp for each of 256 seeded scenes, all jobs in one
+    """Batching: one frame of 16 spp for each of 256 seeded scenes, all jobs in one
     wavefront pool (every traversal launch covers every scene in flight);
     wavefront size and traversal launch shape picked by the autotuner."""
     from meturay_b200.pool import autotune
@@ -551,7 +551,7 @@ def _sphere_camera(rng, center, radius):
 
 
 def run_serving(args, m, system) -> dict:
-    """C4: Poisson arrivals of render jobs against one wavefront pool with
+    """Serving: Poisson arrivals of render jobs against one wavefront pool with
     32 resident scenes; jobs are admitted by free HBM and join the running
     iterations as they arrive.  Latency = arrival to the end of the
     iteration that finished the job (host clock)."""
@@ -596,7 +596,7 @@ def run_serving(args, m, system) -> dict:
                     "load exceeds the device's throughput, so latency includes queueing"}
 
 
-# ---- learned guiding (C5) ------------------------------------------------
+# ---- learned guiding --------------------------------------------------------
 C1 = {"Samples": 2, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
       "DirectLightMIS": 0}
 # GuideBounceAmount 2: both guiders guide the first two bounces, where the
@@ -711,7 +711,8 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
                             for k in ("plain", "wfpg_bxdf", "svo", "learned_1", "learned_4",
                                       "learned_1_octree")}
     out["config"] = {"scene": ("Cornell box (seed 1) with the light facing the ceiling over an "
-                               "opaque panel" if shielded else "config-1 Cornell box (seed 1)")
+                               "opaque panel" if shielded else
+                               "Cornell box with a ceiling-wide light (seed 1)")
                      + ", 128x128, 4 spp per frame, depth 5",
                      **LEARNED, **LEARNED_FLOATS,
                      "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
