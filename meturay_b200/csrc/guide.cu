@@ -204,6 +204,8 @@ struct GuideSmem {
     float origin[4];
     float jitter[2];
     float marg[X];      // non-product sampler: row marginal prefix sums
+    float span[12];     // cone loop constants per level (ConeTables)
+    float vs2[11];
     ConePrefix prefix;  // the descent every cone of the bin shares
     uint32_t begin, end, key, bin;
     int nextTile;
@@ -389,6 +391,9 @@ __global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
     const SceneDev& sc = A.sc;
     const float aperture = (4.0f * kPiF) / (static_cast<float>(X) * static_cast<float>(X));
     const uint32_t mix = hash32(frame ^ hash32(A.depthTag ^ 0xA511E9B3u ^ A.opt.seedLo));
+    if (tid < 12) S.span[tid] = neg_exp2i(tid);
+    if (tid < 11) S.vs2[tid] = level_voxel_size_sqr(A.g, tid);
+    const ConeTables tables{S.span, S.vs2};  // read after the first bin's barrier
     // bins differ widely in cost (rays, cone lengths): blocks take them in
     // turn from a counter rather than in a fixed stride
     for (;;) {
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
                 const V3 dir = octa_to_dir_yup(s, t);
                 bool isLeaf;
                 uint32_t id;
-                cone_trace(A.g, org, dir, tMin, aperture, 0u, isLeaf, id, &S.prefix);
+                cone_trace(A.g, org, dir, tMin, aperture, 0u, isLeaf, id, &S.prefix, &tables);
                 float r = read_radiance(A.g, dir, id, isLeaf);
                 if (r == 0.0f) r = kLargeEpsilon;
                 S.field[p] = r;

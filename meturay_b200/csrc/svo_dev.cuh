@@ -536,6 +536,14 @@ __device__ __forceinline__ bool cone_begin(const GuideDev& g, V3 pos, V3 dir, fl
     return false;
 }
 
+// Per-level constants of the cone loop, computed once per block: span[L] =
+// 2^-L (neg_exp2i) and vs2[L] = the squared voxel size of level L
+// (level_voxel_size_sqr).  Same values as computing them in the loop.
+struct ConeTables {
+    const float* span;  // 12 entries (levels 0..11)
+    const float* vs2;   // 11 entries (levels 0..10)
+};
+
 // One iteration of the reference's loop.  The empty-child skip takes the
 // child's exit crossings from values the iteration already has: per axis
 // the child's far plane is the node's far plane (child bit set: corner +
@@ -544,15 +552,16 @@ __device__ __forceinline__ bool cone_begin(const GuideDev& g, V3 pos, V3 dir, fl
 // the trace has ended.
 __device__ __forceinline__ bool cone_step(const GuideDev& g, float aperture,
                                           uint32_t maxQueryLevelOffset, ConeState& s,
-                                          bool& isLeaf, uint32_t& leafId) {
+                                          bool& isLeaf, uint32_t& leafId,
+                                          const ConeTables* tab = nullptr) {
     if (s.step == kConeTraceMaxSteps) {
         leafId = kInvalid;
         isLeaf = false;
         return true;
     }
     s.step++;
-    const float childSpan = neg_exp2i(s.depth + 1);
-    const float curSpan = neg_exp2i(s.depth);
+    const float childSpan = tab ? tab->span[s.depth + 1] : neg_exp2i(s.depth + 1);
+    const float curSpan = tab ? tab->span[s.depth] : neg_exp2i(s.depth);
     const V3 topRight = s.corner + v3(curSpan, curSpan, curSpan);
     const V3 tm = topRight * s.dc - s.pb;
     const float tMax = fminf(fminf(tm.x, tm.y), tm.z);
@@ -585,7 +594,7 @@ __device__ __forceinline__ bool cone_step(const GuideDev& g, float aperture,
     const uint32_t level = s.depth + 1;
     const float area = s.tMin * s.tMin * aperture;
     const float diam2 = 4.0f * (area * kInvPiF);
-    bool term = diam2 > level_voxel_size_sqr(g, level);
+    bool term = diam2 > (tab ? tab->vs2[level] : level_voxel_size_sqr(g, level));
     const bool childLeaf = svo_children_leaf(node);
     term |= (g.leafDepth - level) <= maxQueryLevelOffset;
     if (childLeaf || term) {
@@ -604,10 +613,11 @@ __device__ __forceinline__ bool cone_step(const GuideDev& g, float aperture,
 __device__ __forceinline__ float cone_trace(const GuideDev& g, V3 pos, V3 dir, float tMin,
                                             float aperture, uint32_t maxQueryLevelOffset,
                                             bool& isLeaf, uint32_t& leafId,
-                                            const ConePrefix* pre = nullptr) {
+                                            const ConePrefix* pre = nullptr,
+                                            const ConeTables* tab = nullptr) {
     ConeState s;
     if (cone_begin(g, pos, dir, tMin, pre, s, isLeaf, leafId)) return s.tMin;
-    while (!cone_step(g, aperture, maxQueryLevelOffset, s, isLeaf, leafId)) {
+    while (!cone_step(g, aperture, maxQueryLevelOffset, s, isLeaf, leafId, tab)) {
     }
     return s.tMin;
 }
