@@ -514,14 +514,25 @@ __global__ void __launch_bounds__(256) k_pool_camera(const PoolHeader* __restric
          g += gridDim.x * blockDim.x) {
         const uint32_t j = job_of(sBase, nj, g);
         const JobDev& J = jobs[j];
-        const uint32_t sid = g - J.sampleBase;
+        const uint32_t li = g - J.sampleBase;
         const uint32_t SW = J.width * J.samples, SH = J.height * J.samples;
-        const uint32_t sx = sid % SW, sy = sid / SW;
+        // slot -> sample of the job in 4 x 8 tiles, as k_camera lays them out
+        uint32_t sx, sy;
+        if ((SW % 4u == 0u) && (SH % 8u == 0u)) {
+            const uint32_t tile = li >> 5, w = li & 31u, tilesX = SW / 4u;
+            sx = (tile % tilesX) * 4u + (w & 3u);
+            sy = (tile / tilesX) * 8u + (w >> 2);
+        } else {
+            sx = li % SW;
+            sy = li / SW;
+        }
+        const uint32_t sid = sy * SW + sx;
+        const uint32_t gs = J.sampleBase + sid;  // the sample this slot renders
         const Rand4 rc = philox_uniform4(sid, J.frame, kTagCamera, 0u, J.seedLo, J.seedHi);
         camera_ray(J.cam, sx, sy, SW, SH, rc, rayO[g], rayD[g]);
         RayAux a;
         a.rf[0] = a.rf[1] = a.rf[2] = 1.0f;
-        a.sample = g;
+        a.sample = gs;
         a.endpoint = kInvalid;
         a.medium = static_cast<uint16_t>(J.sc.baseMedium);
         a.depth = 0;
@@ -529,7 +540,7 @@ __global__ void __launch_bounds__(256) k_pool_camera(const PoolHeader* __restric
         a.prevPDF = __int_as_float(0x7fc00000);
         a.pad = j;
         aux[g] = a;
-        samples[g] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        samples[gs] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
