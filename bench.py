@@ -823,7 +823,7 @@ def main():
     ap.add_argument("--pool-stack", type=int, default=128)
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the learned-guiding equal-time MSE comparison")
-    ap.add_argument("--learned-budget-ms", type=float, default=250.0)
+    ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
     ap.add_argument("--learned-reference-spp", type=int, default=16384)
     ap.add_argument("--learned-kinds", default="",
                     help="comma list of plain,wfpg_bxdf,svo,learned_1,learned_4,"
