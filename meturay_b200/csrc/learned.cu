@@ -323,9 +323,11 @@ int learned_train(mrb_mlp* net, const LearnedScratch& s, float lr, cudaStream_t 
     MRB_CUDA(cudaMemsetAsync(s.frameLoss, 0, 8, st));
     const uint32_t perStep = s.capacity / s.steps;
     for (uint32_t k = 0; k < s.steps; k++) {
+        // at most half the SMs: the training overlaps the frame, whose
+        // kernels need the rest (a training CTA holds 140 KB of shared memory)
         int r = mlp_train_step_dev(net, s.trainX + size_t(k) * perStep * kMlpIn,
                                    s.trainT + size_t(k) * perStep * 4, perStep, s.stepCount + k, lr,
-                                   st);
+                                   st, 74);
         if (r) return r;
         k_learned_loss<<<1, 32, 0, st>>>(mlp_loss(net), s.frameLoss);
     }

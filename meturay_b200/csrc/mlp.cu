@@ -372,11 +372,12 @@ int mlp_forward(const MlpDev& m, const float* in, uint32_t n, float* out, cudaSt
 }
 
 int mlp_gradients(const MlpDev& m, const float* in, const float* targets, uint32_t n, float* grad,
-                  float* loss, cudaStream_t st, const uint32_t* dCount) {
+                  float* loss, cudaStream_t st, const uint32_t* dCount, uint32_t maxCtas) {
     if (n == 0) return 0;
     if (mlp_smem_setup()) return MRB_E_CUDA;
-    k_mlp_train<<<mlp_grid(n), kMlpTile, sizeof(MlpSmem), st>>>(m, in, targets, n, dCount, grad,
-                                                               loss);
+    uint32_t grid = mlp_grid(n);
+    if (maxCtas && grid > maxCtas) grid = maxCtas;
+    k_mlp_train<<<grid, kMlpTile, sizeof(MlpSmem), st>>>(m, in, targets, n, dCount, grad, loss);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -437,10 +438,10 @@ namespace mrb {
 MlpDev mlp_dev(const mrb_mlp* m) { return m->dev(); }
 float* mlp_params(mrb_mlp* m) { return m->params.as<float>(); }
 int mlp_train_step_dev(mrb_mlp* m, const float* in, const float* targets, uint32_t maxN,
-                       const uint32_t* dCount, float lr, cudaStream_t st) {
+                       const uint32_t* dCount, float lr, cudaStream_t st, uint32_t maxCtas) {
     MRB_CUDA(cudaMemsetAsync(m->loss.p, 0, 8, st));
     int r = mlp_gradients(m->dev(), in, targets, maxN, m->grad.as<float>(), m->loss.as<float>(),
-                          st, dCount);
+                          st, dCount, maxCtas);
     if (r) return r;
     return mlp_adam(m->params.as<float>(), m->m1.as<float>(), m->m2.as<float>(),
                     m->step.as<uint32_t>(), m->grad.as<float>(), m->loss.as<float>(), lr,

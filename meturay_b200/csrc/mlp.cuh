@@ -51,8 +51,10 @@ int mlp_forward(const MlpDev& m, const float* in, uint32_t n, float* out, cudaSt
 // loss is sum_s w_s * -log q(dir_s | x_s) / sum_s w_s.  grad (kMlpParams)
 // and loss (2 floats: weighted loss sum, weight sum) are accumulated into.
 int mlp_gradients(const MlpDev& m, const float* in, const float* targets, uint32_t n,
-                  float* grad, float* loss, cudaStream_t st, const uint32_t* dCount = nullptr);
-// (dCount, when given, holds the sample count on the device; n bounds it.)
+                  float* grad, float* loss, cudaStream_t st, const uint32_t* dCount = nullptr,
+                  uint32_t maxCtas = 0);
+// (dCount, when given, holds the sample count on the device; n bounds it.
+// maxCtas > 0 caps the grid, each CTA then taking more tiles.)
 // Adam (lr, 0.9, 0.999, 1e-8) on params with state m1/m2 and step count on
 // the device; grad is divided by loss[1] (the weight sum) first, then
 // cleared; the bf16 image is rewritten.  A batch of weight sum 0 takes no
@@ -74,7 +76,7 @@ MlpDev mlp_dev(const mrb_mlp* m);
 float* mlp_params(mrb_mlp* m);
 // One Adam step of a network handle on a batch whose count is on the device.
 int mlp_train_step_dev(mrb_mlp* m, const float* in, const float* targets, uint32_t maxN,
-                       const uint32_t* dCount, float lr, cudaStream_t st);
+                       const uint32_t* dCount, float lr, cudaStream_t st, uint32_t maxCtas = 0);
 uint32_t* mlp_error_flag(mrb_mlp* m);
 // (weighted loss sum, weight sum) of the last training step's batch.
 float* mlp_loss(mrb_mlp* m);
