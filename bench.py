@@ -253,8 +253,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded clusters-1M scene)",
-        "config": dict(WORKLOAD, parallelism=f"replicas{world}",
-                       traversal="8-wide quantised BVH" if args.traversal else "binary LBVH"),
+        "config": run_config(world),
+        "traversal": "8-wide quantised BVH" if args.traversal else "binary LBVH",
         "rays_per_step": rays / args.steps / world,
         "mpaths_per_s": scene.width * scene.height * world * args.steps / ms / 1e3,
         "e2e": {"value": e2e_rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
@@ -759,46 +759,73 @@ def _camera16(scene):
                            np.array(c["near_far"], f)]).astype(f)
 
 
-def cpu_leg(scene, os_, rows: int, threads: int) -> dict:
+# The CPU legs (cpu_baseline of the GPU arm and the --impl reference arm)
+# time the same row-stratified sample of the full 1920x1080 frame: step i
+# renders every CPU_ROW_STRIDE-th image row starting at row i mod
+# CPU_ROW_STRIDE, so CPU_ROW_STRIDE consecutive steps cover the whole frame
+# once and every step sees the top, middle and bottom of the image alike.
+CPU_ROW_STRIDE = 4
+
+
+def _load_scenes():
+    """The seeded scene generator, loaded from its file on its own: the CPU
+    legs must not import the package (which maps libmrb200.so)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mrb_scenes_standalone",
+                                                  ROOT / "meturay_b200" / "scenes.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses resolve their module by name
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cpu_leg(scene, os_, step: int, threads: int) -> dict:
+    """One CPU step: the rows r = step mod CPU_ROW_STRIDE (mod CPU_ROW_STRIDE)
+    of the frame, at the frame index of the step (1 spp, depth 8, NEE)."""
     cf = _camera16(scene)
     t0 = time.perf_counter()
-    _, rays = os_.render(cf, scene.width, scene.height, 1, 8, 3, True, 1,
-                         threads=threads, rows=(0, rows))
+    _, rays = os_.render(cf, scene.width, scene.height, 1, 8, 3, True, 1, frame=step,
+                         threads=threads, rows=(step % CPU_ROW_STRIDE, scene.height),
+                         row_step=CPU_ROW_STRIDE)
     dt = time.perf_counter() - t0
-    return {"rays": rays, "seconds": dt, "rows": rows}
+    return {"rays": rays, "seconds": dt}
+
+
+def cpu_sample_text(scene, steps: int, cores: int) -> str:
+    return (f"{steps} steps; step i renders every {CPU_ROW_STRIDE}th row of the "
+            f"{scene.width}x{scene.height} clusters-1M frame from row i mod {CPU_ROW_STRIDE} "
+            f"({scene.height // CPU_ROW_STRIDE} rows, 1 spp, depth 8), {cores} threads")
 
 
 def run_reference(args) -> dict:
-    import meturay_b200.scenes as scenes
+    scenes = _load_scenes()
     cores = os.cpu_count() or 1
     scene = scenes.clusters(seed=1)
     os_ = _oracle_setup(scene)
-    # size each step to about 1.5 s of work on this host
-    probe = cpu_leg(scene, os_, 16, cores)
-    rate = probe["rays"] / max(probe["seconds"], 1e-6)
-    rows = int(min(scene.height, max(16, 16 * 1.5 / max(probe["seconds"], 1e-3))))
-    for _ in range(args.warmup):
-        cpu_leg(scene, os_, min(rows, 64), cores)
+    for w in range(args.warmup):
+        cpu_leg(scene, os_, w, cores)
     total_rays, total_s = 0, 0.0
-    for _ in range(args.steps):
-        r = cpu_leg(scene, os_, rows, cores)
+    for i in range(args.steps):
+        r = cpu_leg(scene, os_, i, cores)
         total_rays += r["rays"]
         total_s += r["seconds"]
     value = total_rays / total_s / 1e6
-    sample = (f"first {rows} of {scene.height} image rows (1920 px wide) of the clusters-1M frame "
-              f"per step, {cores} threads")
     return {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded clusters-1M scene)",
-        "config": dict(WORKLOAD, parallelism="cpu"),
+        "config": run_config(args.gpus),
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": cpu_sample_text(scene, args.steps, cores)},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "probe_rate_mrays": rate / 1e6,
     }
+
+
+def run_config(world: int) -> dict:
+    """The workload of the line; both arms report the same one."""
+    return dict(WORKLOAD, parallelism=f"replicas{world}")
 
 
 def main():
@@ -854,18 +881,22 @@ def main():
         dist = tdist
     out = run_ours(args, rank, world, dist)
     if out is not None and not args.no_cpu_baseline and args.only == "all":
-        import meturay_b200.scenes as scenes
-        scene = scenes.clusters(seed=1)
+        # the reference arm's sample: 2 x CPU_ROW_STRIDE steps = the whole
+        # frame twice (about 5-10 s on the host's cores)
+        scene = _load_scenes().clusters(seed=1)
         os_ = _oracle_setup(scene)
         cores = os.cpu_count() or 1
-        probe = cpu_leg(scene, os_, 16, cores)
-        rows = int(min(scene.height, max(16, 16 * 12.0 / max(probe["seconds"], 1e-3))))
-        r = cpu_leg(scene, os_, rows, cores)
-        out["cpu_baseline"] = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s",
+        cpu_leg(scene, os_, 0, cores)  # warm-up
+        steps = 2 * CPU_ROW_STRIDE
+        tot_r, tot_s = 0, 0.0
+        for i in range(steps):
+            r = cpu_leg(scene, os_, i, cores)
+            tot_r += r["rays"]
+            tot_s += r["seconds"]
+        out["cpu_baseline"] = {"value": tot_r / tot_s / 1e6, "unit": "Mrays/s",
                                "cores": cores, "kind": "port",
-                               "sample": f"first {rows} of 1080 rows of the clusters-1M frame "
-                                         f"(1 spp, depth 8), {cores} threads, "
-                                         f"{r['seconds']:.1f} s"}
+                               "sample": cpu_sample_text(scene, steps, cores)
+                               + f", {tot_s:.1f} s"}
     if out is not None:
         print(json.dumps(out))
     if dist:

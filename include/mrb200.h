@@ -467,12 +467,16 @@ int mrb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, int
  * the reference).  For callers that cannot call cudaMalloc -- a host that
  * manages all device memory itself and forbids libraries to allocate, or a
  * latency-critical path that cannot afford cudaMalloc's implicit device
- * synchronisation.  Scratch is a file-scope device array of about 8.4 MB,
- * resident on every device that loads the library until exit; n is limited
- * to 1,048,576 pairs (larger n returns MRB_E_ARG).  All calls share the
- * array: calls that overlap on the GPU race, so serialise them on one
- * stream.  The first call on a device looks up the array's address with that
- * device current; make it before any stream capture.  Allocates nothing. */
+ * synchronisation.  Scratch is a file-scope device array of 8.5 MiB
+ * (8,912,896 bytes), resident on every device that loads the library until
+ * exit; n is limited to 1,048,576 pairs (larger n returns MRB_E_ARG).  All
+ * calls share the array: calls that overlap on the GPU race, so serialise
+ * them on one stream.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture, and
+ * do not call this entry point on a device after cudaDeviceReset (the
+ * cached address is then stale).  A look-back wait of the sort that gives up
+ * (bounded; not expected in practice) leaves the output unordered and is not
+ * reported by this entry point.  Allocates nothing. */
 int mrb_radix_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n,
                                      int begin_bit, int end_bit, int descending, void* stream);
 /* LBVH hierarchy + AABBs from sorted codes (LinearBVH.hpp:30-100,181-396).

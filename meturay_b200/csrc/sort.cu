@@ -13,6 +13,8 @@
 // The element count may live on the device (rays whose count a previous
 // kernel produced); tiles past the count exit at once, so the sort needs no
 // host synchronisation and can be captured in a CUDA graph.
+#include <mutex>
+
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -268,15 +270,26 @@ int radix_sort_pairs(K* keys, uint32_t* vals, const uint32_t* dCount, uint32_t m
     uint32_t* valsAlt = reinterpret_cast<uint32_t*>(p);
 
     const size_t smem = sizeof(SortSmem<K>);
-    // the attribute is set once per device, before any stream capture
-    static bool configured[2][64] = {};
+    // the attribute is set once per device, before any stream capture; the
+    // lock keeps two host threads' first sorts on a device from racing
+    constexpr int kMaxDevices = 64;
+    static bool configured[2][kMaxDevices] = {};
+    static std::mutex configuredMutex;
     int dev = 0;
     MRB_CUDA(cudaGetDevice(&dev));
-    bool& done = configured[sizeof(K) == 8 ? 1 : 0][dev & 63];
-    if (!done) {
-        MRB_CUDA(cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(smem)));
-        done = true;
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("radix sort: device %d out of the supported range [0, %d)", dev, kMaxDevices);
+        return -1;
+    }
+    {
+        std::lock_guard<std::mutex> lock(configuredMutex);
+        bool& done = configured[sizeof(K) == 8 ? 1 : 0][dev];
+        if (!done) {
+            MRB_CUDA(cudaFuncSetAttribute(k_onesweep<K>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+            done = true;
+        }
     }
     MRB_CUDA(cudaMemsetAsync(hist, 0, size_t(8) * 256 * 4, stream));
     MRB_CUDA(cudaMemsetAsync(tickets, 0, size_t(8) * 4, stream));

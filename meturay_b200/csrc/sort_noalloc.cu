@@ -9,8 +9,8 @@
 //
 // Limits and sharing rules:
 //   - at most kNoAllocMaxPairs (1,048,576) key/value pairs per call; the
-//     array costs about 8.4 MB on every device that loads the library and
-//     stays resident until the process exits;
+//     array costs 8.5 MiB (8,912,896 bytes) on every device that loads the
+//     library and stays resident until the process exits;
 //   - every call uses the same array: calls that overlap on the GPU (on
 //     different streams, or from different host threads) race and corrupt
 //     each other; serialise them on one stream;
@@ -19,7 +19,15 @@
 //     error word) itself before using them;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The cached address is
+//     kept for the life of the process, so do not call this entry point on
+//     a device after cudaDeviceReset (or any other teardown of its primary
+//     context): the module, and with it the array, is loaded anew there;
+//   - a look-back wait of the sort that gives up (bounded, and not expected
+//     in practice: it takes a tile stalled for millions of polls) sets an
+//     error word inside the array, which this entry point cannot return
+//     without a device synchronisation; the order of that call's output is
+//     then undefined and nothing reports it.
 #include <mutex>
 
 #include "../../include/mrb200.h"

@@ -1480,8 +1480,9 @@ uint64_t render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera*
     uint32_t rowB = opt->row_begin, rowE = opt->row_end;
     if (rowE == 0 || rowE > SH) rowE = SH;
     if (rowB > rowE) rowB = rowE;
-    const uint32_t first = rowB * SW;
-    const uint32_t count = (rowE - rowB) * SW;
+    const uint32_t rowStep = opt->row_step ? opt->row_step : 1;
+    const uint32_t rowCount = (rowE - rowB + rowStep - 1) / rowStep;
+    const uint32_t count = rowCount * SW;
     std::atomic<uint64_t> rays{0};
     const float* P = cam->position;
     parallel_for(count, opt->threads, [&](uint32_t b0, uint32_t b1) {
@@ -1489,7 +1490,7 @@ uint64_t render(const oracle_scene* s, const oracle_bvh* b, const oracle_camera*
         uint64_t local = 0;
         std::vector<PRay<T>> cur, next;
         for (uint32_t k = b0; k < b1; k++) {
-            uint32_t sid = first + k;
+            uint32_t sid = (rowB + (k / SW) * rowStep) * SW + k % SW;
             out[3 * sid] = out[3 * sid + 1] = out[3 * sid + 2] = T(0);
             // Camera ray (GPUCameraPinhole.cuh:209-243; GenerationKernels.cuh:48-75)
             uint32_t sx = sid % SW, sy = sid / SW;

@@ -100,6 +100,7 @@ typedef struct oracle_options {
     uint32_t frame;
     uint32_t threads;        /* 0 = all hardware threads */
     uint32_t row_begin, row_end;  /* sample rows to render (0,0 = all) */
+    uint32_t row_step;       /* render every row_step-th row from row_begin (0 = 1) */
 } oracle_options;
 
 /* Build the LBVH of the scene (a1..a7) and keep it inside a handle. */

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import subprocess
 from pathlib import Path
 
@@ -19,11 +20,16 @@ REF_LIB = HERE / "_ref" / "libmrayref.so"
 
 
 def build(ref_root: str | None = None) -> None:
-    """Compile the oracle (and the reference shim when the sources exist)."""
+    """Compile the oracle; with ``ref_root`` (or the REF_ROOT environment
+    variable) naming an MRay source tree, also the reference shim."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    root = Path(ref_root or "/root/reference")
-    if (root / "Source" / "RayLib" / "Ray.hpp").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
+    ref_root = ref_root or os.environ.get("REF_ROOT")
+    if not ref_root:
+        return
+    root = Path(ref_root)
+    if not (root / "Source" / "RayLib" / "Ray.hpp").exists():
+        raise FileNotFoundError(f"REF_ROOT={root} is not an MRay source tree")
+    subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
 
 
 class Scene(C.Structure):
@@ -51,7 +57,7 @@ class Camera(C.Structure):
 class Options(C.Structure):
     _fields_ = [(k, C.c_uint32) for k in ("width", "height", "samples", "max_depth", "rr_start",
                                           "nee", "mis", "seed_lo", "seed_hi", "frame", "threads",
-                                          "row_begin", "row_end")]
+                                          "row_begin", "row_end", "row_step")]
 
 
 def _load():
@@ -203,8 +209,10 @@ class OracleScene:
     def render(self, camera_frame: np.ndarray, width: int, height: int, samples: int,
                max_depth: int, rr_start: int, nee: bool, seed: int, frame: int = 0,
                threads: int = 0, rows: tuple[int, int] = (0, 0), fp64: bool = False,
-               mis: bool = False):
-        """Per-sample radiance ((h*s), (w*s), 3) and the rays traced."""
+               mis: bool = False, row_step: int = 1):
+        """Per-sample radiance ((h*s), (w*s), 3) and the rays traced.  ``rows``
+        (begin, end) and ``row_step`` select the sample rows rendered (every
+        row_step-th row from begin); the others stay zero."""
         cam = Camera()
         f = camera_frame
         cam.position[:] = [float(v) for v in f[0:3]]
@@ -214,7 +222,8 @@ class OracleScene:
         cam.plane_size[:] = [float(v) for v in f[12:14]]
         cam.near_far[:] = [float(v) for v in f[14:16]]
         o = Options(width, height, samples, max_depth, rr_start, 1 if nee else 0, 1 if mis else 0,
-                    seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, frame, threads, rows[0], rows[1])
+                    seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, frame, threads, rows[0], rows[1],
+                    row_step)
         out = np.zeros((height * samples, width * samples, 3), np.float64 if fp64 else np.float32)
         fn = lib.oracle_render_f64 if fp64 else lib.oracle_render
         rays = fn(C.byref(self.c), self.bvh, C.byref(cam), C.byref(o), _p(out))

@@ -8,11 +8,12 @@ The CPU oracle is then checked against these vectors by
 ``tests/test_oracle_golden.py``; the reference tree is not needed at test
 time.
 
-    python tests/golden/make_golden.py [REF_ROOT]
+    python tests/golden/make_golden.py REF_ROOT     (or REF_ROOT=... in the environment)
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -28,7 +29,10 @@ def _p(a):
     return C.c_void_p(a.ctypes.data)
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    ref_root = ref_root or os.environ.get("REF_ROOT")
+    if not ref_root:
+        sys.exit("make_golden: pass the MRay source tree as REF_ROOT (argument or environment)")
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REF_ROOT={ref_root}"],
                    check=True)
     R = C.CDLL(str(ROOT / "oracle" / "_ref" / "libmrayref.so"))
