@@ -368,6 +368,13 @@ int mrb_tracer_launches_per_frame(mrb_tracer* t);
  * depths).  work[4]: rays traced, inner nodes visited, triangles tested,
  * depths.  The frame counts like any other. */
 int mrb_tracer_profile_frame(mrb_tracer* t, float* stage_ms, uint64_t* work);
+/* The same with the guided stages apart.  stage_ms[n_stages] (up to 12):
+ * camera, traversal, partition, shading, reconstruction, then the octree
+ * guider's clear of the bin words, binning and collapse, bin sort and
+ * ranges, guide kernel (the learned guider's fused kernel counts here too),
+ * and per frame the radiance deposit, the normalize-and-filter passes and
+ * the learned guider's join and sample collection. */
+int mrb_tracer_profile_stages(mrb_tracer* t, float* stage_ms, uint32_t n_stages, uint64_t* work);
 
 /* ---- wavefront pool: continuous batching of render jobs ----------------
  * (no counterpart in the reference: MRay renders one scene per tracer.)

@@ -99,6 +99,7 @@ def _load() -> C.CDLL:
         "mrb_tracer_stream": (vp, [vp]),
         "mrb_tracer_launches_per_frame": (i32, [vp]),
         "mrb_tracer_profile_frame": (i32, [vp, vp, vp]),
+        "mrb_tracer_profile_stages": (i32, [vp, vp, u32, vp]),
         "mrb_morton_codes": (i32, [vp, vp, u32, vp, vp, vp, vp]),
         "mrb_radix_sort_temp_bytes": (sz, [u32, i32, i32, i32]),
         "mrb_radix_sort_pairs_u64": (i32, [vp, vp, u32, i32, i32, i32, vp, sz, vp]),

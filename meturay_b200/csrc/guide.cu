@@ -904,10 +904,15 @@ uint32_t guide_launches(const SvoResult& v, const GuideOptions& go, uint32_t max
 
 int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, const GuideWave& w,
                     const GuideScratch& s, const GuideOptions& go, const PathOptions& opt,
-                    uint32_t iteration, uint32_t depthTag, cudaStream_t st) {
+                    uint32_t iteration, uint32_t depthTag, cudaStream_t st, cudaEvent_t* marks) {
+    auto mark = [&](int i) -> cudaError_t {
+        return marks ? cudaEventRecord(marks[i], st) : cudaSuccess;
+    };
     const uint32_t grid = grid_for(w.maxRays, 256, 148 * 8);
+    MRB_CUDA(mark(0));
     MRB_CUDA(cudaMemsetAsync(g.leafBin, 0, size_t(g.leafCount) * 4, st));
     MRB_CUDA(cudaMemsetAsync(g.nodeBin, 0, size_t(g.nodeCount) * 4, st));
+    MRB_CUDA(mark(1));
     BinArgs ba{g, w, s.binKey, s.guide};
     k_bin_init<<<grid, 256, 0, st>>>(ba);
     k_collapse_leaf<<<grid_for(g.leafCount, 256, 148 * 8), 256, 0, st>>>(g, go.minBinLevel,
@@ -919,6 +924,7 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
                                                                        go.binRayCount);
     }
     k_bin_resolve<<<grid, 256, 0, st>>>(g, w.count, s.binKey);
+    MRB_CUDA(mark(2));
     int r = radix_sort_pairs<uint32_t>(s.binKey, s.binRid, w.count, w.maxRays, 0, 32, false,
                                        s.sortTemp, s.sortTempBytes, st, true);
     if (r) return r;
@@ -927,6 +933,7 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
     k_bin_ranges<<<grid, 256, 0, st>>>(s.binKey, w.count, s.heads, s.headScan, s.binBegin,
                                        s.binEnd);
     MRB_CUDA(cudaMemsetAsync(s.binNext, 0, 4, st));
+    MRB_CUDA(mark(3));
     GuideArgs ga{sc, g, w, s.binKey, s.binRid, s.binBegin, s.binEnd, s.headScan + w.maxRays,
                  s.binNext, s.guide, go, opt, depthTag};
     const uint32_t kernelIndex = iteration < 4 ? iteration : 4;
@@ -950,6 +957,7 @@ int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v, c
             break;
     }
     MRB_CUDA(cudaGetLastError());
+    MRB_CUDA(mark(4));
     return 0;
 }
 

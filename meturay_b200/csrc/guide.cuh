@@ -59,10 +59,12 @@ struct GuideWave {
 // partition by bin and run the per-bin radiance field + product sampler.
 // `iteration` (0-based depth step) picks the field resolution: 64^2 for
 // the first two, then 32^2, 16^2, 8^2 (WFPGTracer.cu:224-230).
+// With `marks` (5 events) the sub-stages are bracketed for profiling: clear
+// the bin words | bin and collapse | sort and range the bins | guide kernel.
 int guide_wavefront(const SceneDev& sc, const GuideDev& g, const SvoResult& v,
                     const GuideWave& w, const GuideScratch& s, const GuideOptions& go,
                     const PathOptions& opt, uint32_t iteration, uint32_t depthTag,
-                    cudaStream_t st);
+                    cudaStream_t st, cudaEvent_t* marks = nullptr);
 uint32_t guide_launches(const SvoResult& v, const GuideOptions& go, uint32_t maxRays);
 
 // KCAccumulateRadianceToLeaf with the chain sums (PathNode.cuh

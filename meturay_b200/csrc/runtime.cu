@@ -590,9 +590,16 @@ int step_camera(mrb_tracer* t) {
                            t->hasFilter ? t->imgCoords.as<float2>() : nullptr, t->stream);
 }
 
+// Stage slots of a profiled frame (stage_ms of mrb_tracer_profile_stages).
+enum Stage : int {
+    kStCamera = 0, kStTrace, kStPartition, kStShade, kStResolve,
+    kStGuideClear, kStGuideBin, kStGuideSort, kStGuideKernel,
+    kStDeposit, kStNormalize, kStLearned, kStageCount
+};
+
 struct StageTimer {
-    cudaEvent_t ev[2 * 8] = {};
-    float ms[8] = {};
+    cudaEvent_t ev[24] = {};
+    float ms[kStageCount] = {};
 };
 
 // One Render() step: HitRays -> PartitionRaysWRTWork -> WorkRays
@@ -642,15 +649,28 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
                         t->headScan.as<uint32_t>(), t->binBegin.as<uint32_t>(),
                         t->binEnd.as<uint32_t>(), t->guideSort.p, t->guideSortBytes,
                         t->guideScan.p, t->guideBuf.as<uint2>(), t->binEnd.as<uint32_t>() + t->maxRays};
-        if (learned_active(t))
+        cudaEvent_t* gm = tm ? &tm->ev[16] : nullptr;
+        if (learned_active(t)) {
+            if (mark(16)) return MRB_E_CUDA;
             r = learned_guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), gw,
                                         learned_forward_net(t),
                                         learned_scratch(t), t->misRatio, path_options(t), d,
                                         t->guideBuf.as<uint2>(), t->stream);
-        else
+            if (r || mark(17) || lap(kStGuideKernel, 16)) return r ? r : MRB_E_CUDA;
+        } else {
             r = guide_wavefront(sc->dev(), guide_dev(t->svo, t->svoP), t->svo, gw, gs,
-                                guide_options(t), path_options(t), d, d, t->stream);
-        if (r) return r;
+                                guide_options(t), path_options(t), d, d, t->stream, gm);
+            if (r) return r;
+            if (tm) {
+                const int st[4] = {kStGuideClear, kStGuideBin, kStGuideSort, kStGuideKernel};
+                MRB_CUDA(cudaEventSynchronize(gm[4]));
+                for (int i = 0; i < 4; i++) {
+                    float ms = 0.f;
+                    MRB_CUDA(cudaEventElapsedTime(&ms, gm[i], gm[i + 1]));
+                    tm->ms[st[i]] += ms;
+                }
+            }
+        }
     }
     if (mark(2)) return MRB_E_CUDA;
     PortionTable pt = portion_table(t);
@@ -679,8 +699,15 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
     return 0;
 }
 
-int step_finalize(mrb_tracer* t) {
+int step_finalize(mrb_tracer* t, StageTimer* tm = nullptr) {
     int r;
+    // with a timer: deposit | normalize and filter | learned join and
+    // collect | reconstruction, bracketed by events 8..12
+    auto mark = [&](int i) -> int {
+        if (tm) MRB_CUDA(cudaEventRecord(tm->ev[8 + i], t->stream));
+        return 0;
+    };
+    if (mark(0)) return MRB_E_CUDA;
     if (t->wfpg) {
         // WFPGTracer::Finalize: AccumulateRaidances + NormalizeAndFilterRadiance
         const GuideDev g = guide_dev(t->svo, t->svoP);
@@ -689,14 +716,21 @@ int step_finalize(mrb_tracer* t) {
         if (octree_guides(t)) {
             if ((r = path_deposit(g, path_chain(t), t->frameWord.as<uint32_t>(), t->stream)))
                 return r;
+            if (mark(1)) return MRB_E_CUDA;
             if ((r = svo_normalize_filter(g, t->svo, t->stream))) return r;
+        } else if (mark(1)) {
+            return MRB_E_CUDA;
         }
+        if (mark(2)) return MRB_E_CUDA;
         if ((r = learned_join(t))) return r;
         if (t->learned && t->net &&
             (r = learned_collect(g, path_chain(t), t->frameWord.as<uint32_t>(),
                                  learned_scratch(t), t->stream)))
             return r;
+    } else if (mark(1) || mark(2)) {
+        return MRB_E_CUDA;
     }
+    if (mark(3)) return MRB_E_CUDA;
     if (t->hasFilter)
         r = recon_filter_grid(t->filter, t->samplesBuf.as<float4>(), t->imgCoords.as<float2>(),
                               t->width, t->height, t->samples, 1.0f, t->image.as<float4>(),
@@ -705,7 +739,18 @@ int step_finalize(mrb_tracer* t) {
         r = resolve(t->samplesBuf.as<float4>(), t->width, t->height, t->samples,
                     t->image.as<float4>(), t->stream);
     if (r) return r;
-    return frame_advance(t->frameWord.as<uint32_t>(), t->stream);
+    if ((r = frame_advance(t->frameWord.as<uint32_t>(), t->stream))) return r;
+    if (tm) {
+        if (mark(4)) return MRB_E_CUDA;
+        MRB_CUDA(cudaEventSynchronize(tm->ev[12]));
+        const int st[4] = {kStDeposit, kStNormalize, kStLearned, kStResolve};
+        for (int i = 0; i < 4; i++) {
+            float ms = 0.f;
+            MRB_CUDA(cudaEventElapsedTime(&ms, tm->ev[8 + i], tm->ev[9 + i]));
+            tm->ms[st[i]] += ms;
+        }
+    }
+    return 0;
 }
 
 int record_frame(mrb_tracer* t) {
@@ -1823,6 +1868,16 @@ int mrb_tracer_launches_per_frame(mrb_tracer* t) {
 }
 
 int mrb_tracer_profile_frame(mrb_tracer* t, float* stageMs, uint64_t* work) {
+    float all[kStageCount] = {};
+    int r = mrb_tracer_profile_stages(t, all, kStageCount, work);
+    if (r) return r;
+    // the five-stage form folds the finalize stages into "resolve"
+    for (int i = 0; i < 4; i++) stageMs[i] = all[i];
+    stageMs[kStResolve] = all[kStResolve] + all[kStDeposit] + all[kStNormalize] + all[kStLearned];
+    return 0;
+}
+
+int mrb_tracer_profile_stages(mrb_tracer* t, float* stageMs, uint32_t nStages, uint64_t* work) {
     if (!t || !stageMs || !work) return MRB_E_ARG;
     if (!t->camSet) {
         set_error("tracer: camera not set");
@@ -1843,20 +1898,16 @@ int mrb_tracer_profile_frame(mrb_tracer* t, float* stageMs, uint64_t* work) {
     if ((r = step_camera(t))) return r;
     MRB_CUDA(cudaEventRecord(tm.ev[7], t->stream));
     MRB_CUDA(cudaEventSynchronize(tm.ev[7]));
-    MRB_CUDA(cudaEventElapsedTime(&tm.ms[0], tm.ev[6], tm.ev[7]));
+    MRB_CUDA(cudaEventElapsedTime(&tm.ms[kStCamera], tm.ev[6], tm.ev[7]));
     for (uint32_t d = 0; d < t->maxDepth; d++)
         if ((r = step_depth(t, d, &tm, wc.as<unsigned long long>()))) return r;
-    MRB_CUDA(cudaEventRecord(tm.ev[6], t->stream));
-    if ((r = step_finalize(t))) return r;
-    MRB_CUDA(cudaEventRecord(tm.ev[7], t->stream));
-    MRB_CUDA(cudaEventSynchronize(tm.ev[7]));
-    MRB_CUDA(cudaEventElapsedTime(&tm.ms[4], tm.ev[6], tm.ev[7]));
+    if ((r = step_finalize(t, &tm))) return r;
     unsigned long long w[2] = {0, 0};
     MRB_CUDA(cudaMemcpyAsync(w, wc.p, 16, cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaMemcpyAsync(&rays1, t->counters.p, 8, cudaMemcpyDeviceToHost, t->stream));
     MRB_CUDA(cudaStreamSynchronize(t->stream));
     for (auto& e : tm.ev) cudaEventDestroy(e);
-    for (int i = 0; i < 5; i++) stageMs[i] = tm.ms[i];
+    for (uint32_t i = 0; i < nStages && i < uint32_t(kStageCount); i++) stageMs[i] = tm.ms[i];
     work[0] = rays1 - rays0;
     work[1] = w[0];
     work[2] = w[1];

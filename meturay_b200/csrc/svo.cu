@@ -75,12 +75,15 @@ __device__ TriRaster tri_setup(const SvoParams& P, V3 p0, V3 p1, V3 p2) {
     u = u < 0 ? 0 : (u > 65535 ? 65535 : u);
     v = v < 0 ? 0 : (v > 65535 ? 65535 : v);
     const uint32_t packedNormal = uint32_t(u) | (uint32_t(v) << 16);
-    // rotation that looks down the dominant axis: QuatF(angle, axis)
+    // rotation that looks down the dominant axis: QuatF(angle, axis).  The
+    // half angle is float(pi)/4 or float(pi)/2, whose sin and cos are taken
+    // correctly rounded (the portable polynomials are an ulp off at pi/4,
+    // which moves the conservative edges and with them whole voxel rows)
     Q4 rot = {1.0f, 0.0f, 0.0f, 0.0f};
     if (dom != 2 || neg) {
-        const float angle = ((dom == 2) ? kPiF : (kPiF * 0.5f)) * 0.5f;
-        float sn, cs;
-        pm_sincos(angle, sn, cs);
+        const bool halfPi = (dom == 2);
+        const float sn = halfPi ? 1.0f : 0x1.6a09e6p-1f;
+        const float cs = halfPi ? -0x1.777a5cp-25f : 0x1.6a09e6p-1f;
         V3 axis;
         if (dom == 0) axis = v3(-domSign * 0.0f, -domSign * 1.0f, -domSign * 0.0f);
         else if (dom == 1) axis = v3(domSign * 1.0f, domSign * 0.0f, domSign * 0.0f);

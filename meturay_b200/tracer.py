@@ -350,6 +350,20 @@ class PathTracer:
                 "node_visits": int(work[1]), "tri_tests": int(work[2]),
                 "trace_launches": int(work[3])}
 
+    STAGES = ("camera", "trace", "partition", "shade", "reconstruct", "guide_clear",
+              "guide_bin", "guide_sort", "guide_kernel", "deposit", "normalize_filter",
+              "learned_collect")
+
+    def profile_stages(self) -> dict:
+        """One stepwise frame timed stage by stage, the guided stages apart
+        (milliseconds per stage, summed over depths) and its work counts."""
+        ms = np.zeros(len(self.STAGES), np.float32)
+        work = np.zeros(4, np.uint64)
+        check(lib.mrb_tracer_profile_stages(self._h, _ptr(ms), len(self.STAGES), _ptr(work)))
+        out = {f"{k}_ms": float(v) for k, v in zip(self.STAGES, ms)}
+        out.update(rays=int(work[0]), node_visits=int(work[1]), tri_tests=int(work[2]))
+        return out
+
     @property
     def stream(self) -> int:
         return lib.mrb_tracer_stream(self._h) or 0

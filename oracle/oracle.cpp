@@ -1593,12 +1593,15 @@ uint32_t voxelize_tri(const SvoP& P, V3<float> p0, V3<float> p1, V3<float> p2,
     u = std::min(std::max(u, 0), 65535);
     v = std::min(std::max(v, 0), 65535);
     const uint32_t packed = uint32_t(u) | (uint32_t(v) << 16);
-    // Quaternion(angle, axis) (Quaternion.hpp:15-24)
+    // Quaternion(angle, axis) (Quaternion.hpp:15-24).  The half angle is
+    // float(pi)/4 or float(pi)/2; their sin and cos are taken correctly
+    // rounded (the values the C library returns for these two arguments),
+    // not from the portable polynomials, which are an ulp off at pi/4.
     Q4<float> rot{1.0f, 0.0f, 0.0f, 0.0f};
     if (dom != 2 || neg) {
-        const float angle = ((dom == 2) ? kPiF : (kPiF * 0.5f)) * 0.5f;
-        float sn, cs;
-        pm_sincos(angle, sn, cs);
+        const bool halfPi = (dom == 2);
+        const float sn = halfPi ? 1.0f : 0x1.6a09e6p-1f;
+        const float cs = halfPi ? -0x1.777a5cp-25f : 0x1.6a09e6p-1f;
         F3 axis = (dom == 0) ? F3(-domSign * 0.0f, -domSign * 1.0f, -domSign * 0.0f)
                  : (dom == 1) ? F3(domSign * 1.0f, domSign * 0.0f, domSign * 0.0f)
                               : F3(0.0f, 1.0f, 0.0f);
@@ -2045,6 +2048,53 @@ struct Tree {
     }
 };
 
+// Ray binning of one wavefront (WFPGTracer.cu:488-628): KCInitializeSVOBins
+// (WFPGTracerKC.cuh:965-1018; the leaf of each hit, neighbours searched),
+// leaf ray counts (sort + RLE + KCWriteLeafRayAmounts), KCCollapseRayCountsLeaf
+// / KCCollapseRayCounts bottom-up to minLevel (AnisoSVO.cu:265-350,
+// 1485-1528) and KCCheckReducedSVOBins (WFPGTracerKC.cuh:1045-1066).  hit(i, p)
+// gives ray i's hit position or false for a ray the binning skips.  binKey[i]:
+// kBinInvalid, leaf | kBinLeaf, or the node index of the marked bin.
+template <class HitPos>
+void bin_rays(oracle_svo* svo, uint32_t n, uint32_t minLevel, uint32_t binRayCount, HitPos hit,
+              uint32_t* binKey) {
+    Tree tree{svo};
+    const uint32_t D = svo->P.depth;
+    std::fill(svo->leafBin.begin(), svo->leafBin.end(), 0u);
+    std::fill(svo->nodeBin.begin(), svo->nodeBin.end(), 0u);
+    for (uint32_t i = 0; i < n; i++) {
+        binKey[i] = kBinInvalid;
+        F3 p;
+        if (!hit(i, p)) continue;
+        uint32_t leaf;
+        if (tree.nearest(leaf, p, D)) {
+            binKey[i] = leaf | kBinLeaf;
+            svo->leafBin[leaf] += 1u;
+        }
+    }
+    for (size_t l = 0; l < svo->leafBin.size(); l++) {
+        if (D == minLevel) { svo->leafBin[l] |= kBinMark; continue; }
+        const uint32_t cnt = svo->leafBin[l] & ~kBinMark;
+        if (cnt == 0) continue;
+        if (cnt < binRayCount) svo->nodeBin[svo->leafParents[l]] += cnt;
+        else svo->leafBin[l] |= kBinMark;
+    }
+    for (int L = int(D) - 1; L >= int(minLevel); L--) {
+        for (uint32_t k = svo->levelOffsets[L]; k < svo->levelOffsets[L + 1]; k++) {
+            if (uint32_t(L) == minLevel) { svo->nodeBin[k] |= kBinMark; continue; }
+            const uint32_t cnt = svo->nodeBin[k] & ~kBinMark;
+            if (cnt < binRayCount) svo->nodeBin[node_parent(svo->nodes[k])] += cnt;
+            else svo->nodeBin[k] |= kBinMark;
+        }
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        if (binKey[i] == kBinInvalid) continue;
+        bool isLeaf;
+        const uint32_t node = tree.marked_bin(binKey[i] & ~kBinLeaf, isLeaf);
+        if (!isLeaf) binKey[i] = node;
+    }
+}
+
 // KCReduceVoxelPayload (AnisoSVOKC.cuh:8-320), one voxel at a time with
 // sequential sums, then KCAverageNormals bottom-up (AnisoSVO.cu:428-528)
 void payload_init(oracle_svo* o, const float* lightRad, uint32_t omit) {
@@ -2282,6 +2332,57 @@ void scan8(const float in[8], float out[8]) {
 extern "C" void oracle_svo_payload_init(oracle_svo* o, const float* light_rad, uint32_t omit) {
     payload_init(o, light_rad, omit);
     normalize_filter(o);
+}
+
+extern "C" int64_t oracle_voxelize(const float* pos, const uint32_t* idx, uint32_t T,
+                                   const float* extent, uint32_t res, uint64_t* counts,
+                                   uint64_t* codes, uint32_t* normals, uint64_t capacity) {
+    const SvoP P = svo_params_of(extent, res);
+    std::vector<uint64_t> c;
+    std::vector<uint32_t> nr;
+    for (uint32_t t = 0; t < T; t++) {
+        V3<float> a(pos[3 * idx[3 * t]], pos[3 * idx[3 * t] + 1], pos[3 * idx[3 * t] + 2]);
+        V3<float> b(pos[3 * idx[3 * t + 1]], pos[3 * idx[3 * t + 1] + 1], pos[3 * idx[3 * t + 1] + 2]);
+        V3<float> d(pos[3 * idx[3 * t + 2]], pos[3 * idx[3 * t + 2] + 1], pos[3 * idx[3 * t + 2] + 2]);
+        counts[t] = voxelize_tri(P, a, b, d, codes ? &c : nullptr, codes ? &nr : nullptr);
+    }
+    uint64_t total = 0;
+    for (uint32_t t = 0; t < T; t++) total += counts[t];
+    if (!codes) return int64_t(total);
+    if (total > capacity) return -1;
+    std::copy(c.begin(), c.end(), codes);
+    std::copy(nr.begin(), nr.end(), normals);
+    return int64_t(total);
+}
+
+extern "C" void oracle_svo_bin_rays(oracle_svo* o, const float* org, const float* dir,
+                                    const float* t, const uint8_t* valid, uint32_t n,
+                                    uint32_t minLevel, uint32_t binRayCount, uint32_t* binOut) {
+    bin_rays(o, n, std::min(minLevel, o->P.depth), binRayCount,
+             [&](uint32_t i, F3& p) {
+                 if (!valid[i]) return false;
+                 p = F3(org[3 * i] + t[i] * dir[3 * i], org[3 * i + 1] + t[i] * dir[3 * i + 1],
+                        org[3 * i + 2] + t[i] * dir[3 * i + 2]);
+                 return true;
+             },
+             binOut);
+}
+
+extern "C" void oracle_svo_cone_trace(const oracle_svo* o, const float* org, const float* dir,
+                                      const float* tmin, const float* aperture,
+                                      uint32_t maxQueryOffset, uint32_t n, float* tOut,
+                                      uint32_t* idOut, uint8_t* leafOut, float* radOut) {
+    Tree tree{o};
+    for (uint32_t i = 0; i < n; i++) {
+        bool isLeaf = false;
+        uint32_t id = kInvalid;
+        const F3 d(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        tOut[i] = tree.cone_trace(F3(org[3 * i], org[3 * i + 1], org[3 * i + 2]), d, tmin[i],
+                                  aperture[i], maxQueryOffset, isLeaf, id);
+        idOut[i] = id;
+        leafOut[i] = isLeaf ? 1 : 0;
+        radOut[i] = tree.read_radiance(d, id, isLeaf);
+    }
 }
 
 extern "C" void oracle_svo_payload_get(const oracle_svo* o, uint32_t* leafNormSpec,
@@ -2689,43 +2790,19 @@ extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* 
         rays += cur.size();
         const bool guideNow = !w->skip_pg && it < w->guide_bounce;
         if (guideNow) {
-            std::fill(svo->leafBin.begin(), svo->leafBin.end(), 0u);
-            std::fill(svo->nodeBin.begin(), svo->nodeBin.end(), 0u);
             std::vector<uint32_t> binKey(cur.size(), kBinInvalid);
-            for (size_t i = 0; i < cur.size(); i++) {
-                const WRay& wr = cur[i];
-                if (wr.r.aux.type == NEE_RAY || (wr.key >> 24) == kBatchNull) continue;
-                const F3 p(wr.r.o.x + wr.t * wr.r.d.x, wr.r.o.y + wr.t * wr.r.d.y, wr.r.o.z + wr.t * wr.r.d.z);
-                uint32_t leaf;
-                if (tree.nearest(leaf, p, D)) {
-                    binKey[i] = leaf | kBinLeaf;
-                    svo->leafBin[leaf] += 1u;
-                }
-            }
-            // KCCollapseRayCountsLeaf / KCCollapseRayCounts
-            for (size_t l = 0; l < svo->leafBin.size(); l++) {
-                if (D == minLevel) { svo->leafBin[l] |= kBinMark; continue; }
-                const uint32_t cnt = svo->leafBin[l] & ~kBinMark;
-                if (cnt == 0) continue;
-                if (cnt < w->bin_ray_count) svo->nodeBin[svo->leafParents[l]] += cnt;
-                else svo->leafBin[l] |= kBinMark;
-            }
-            for (int L = int(D) - 1; L >= int(minLevel); L--) {
-                for (uint32_t k = svo->levelOffsets[L]; k < svo->levelOffsets[L + 1]; k++) {
-                    if (uint32_t(L) == minLevel) { svo->nodeBin[k] |= kBinMark; continue; }
-                    const uint32_t cnt = svo->nodeBin[k] & ~kBinMark;
-                    if (cnt < w->bin_ray_count) svo->nodeBin[node_parent(svo->nodes[k])] += cnt;
-                    else svo->nodeBin[k] |= kBinMark;
-                }
-            }
+            bin_rays(svo, uint32_t(cur.size()), minLevel, w->bin_ray_count,
+                     [&](uint32_t i, F3& p) {
+                         const WRay& wr = cur[i];
+                         if (wr.r.aux.type == NEE_RAY || (wr.key >> 24) == kBatchNull) return false;
+                         p = F3(wr.r.o.x + wr.t * wr.r.d.x, wr.r.o.y + wr.t * wr.r.d.y,
+                                wr.r.o.z + wr.t * wr.r.d.z);
+                         return true;
+                     },
+                     binKey.data());
             std::map<uint32_t, std::vector<uint32_t>> bins;
-            for (size_t i = 0; i < cur.size(); i++) {
-                if (binKey[i] == kBinInvalid) continue;
-                bool isLeaf;
-                const uint32_t node = tree.marked_bin(binKey[i] & ~kBinLeaf, isLeaf);
-                if (!isLeaf) binKey[i] = node;
-                bins[binKey[i]].push_back(uint32_t(i));
-            }
+            for (size_t i = 0; i < cur.size(); i++)
+                if (binKey[i] != kBinInvalid) bins[binKey[i]].push_back(uint32_t(i));
             std::vector<std::pair<uint32_t, const std::vector<uint32_t>*>> list;
             for (auto& kv : bins) list.push_back({kv.first, &kv.second});
             const uint32_t ki = it < 4 ? it : 4;

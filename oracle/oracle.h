@@ -164,6 +164,24 @@ void oracle_svo_payload_get(const oracle_svo*, uint32_t* leaf_norm_spec, uint32_
                             uint64_t* leaf_irr, uint32_t* leaf_cnt, uint32_t* leaf_avg,
                             uint32_t* node_avg);
 
+/* TriFunctions::Voxelize over every triangle (counting pass, then codes and
+ * packed spherical normals u16 | u16 << 16 in triangle order, at most
+ * capacity); codes == NULL counts only.  Returns the voxel count, -1 when
+ * capacity is too small. */
+int64_t oracle_voxelize(const float* pos, const uint32_t* idx, uint32_t tri_count,
+                        const float* extent6, uint32_t resolution, uint64_t* counts,
+                        uint64_t* codes, uint32_t* normals, uint64_t capacity);
+/* Ray bins of one wavefront over the octree: rays i with valid[i] hit at
+ * org + t * dir; bin_out: 0xFFFFFFFF, leaf | 1 << 31, or a node index. */
+void oracle_svo_bin_rays(oracle_svo*, const float* org, const float* dir, const float* t,
+                         const uint8_t* valid, uint32_t n, uint32_t min_level,
+                         uint32_t bin_ray_count, uint32_t* bin_out);
+/* ConeTraceRay + ReadRadiance for n cones. */
+void oracle_svo_cone_trace(const oracle_svo*, const float* org, const float* dir,
+                           const float* tmin, const float* aperture, uint32_t max_query_offset,
+                           uint32_t n, float* t_out, uint32_t* id_out, uint8_t* leaf_out,
+                           float* rad_out);
+
 /* One WFPG frame (WFPGTracer.cu:1480-1833) over the octree, which it
  * updates (deposit + normalise/filter).  Per-sample radiance to out (3 per
  * sample); guide words and bin ids of step dump_iteration per path to

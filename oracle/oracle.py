@@ -371,6 +371,35 @@ class OracleSvo:
             lib.oracle_svo_destroy(self.h)
             self.h = None
 
+    def bin_rays(self, org: np.ndarray, dirs: np.ndarray, t: np.ndarray, valid: np.ndarray,
+                 min_level: int, bin_ray_count: int) -> np.ndarray:
+        """Bin ids of rays hitting at org + t * dirs (valid: rays the binning
+        takes): 0xFFFFFFFF, leaf | 1 << 31 or the node index of the bin."""
+        org = np.ascontiguousarray(org, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        valid = np.ascontiguousarray(valid, np.uint8)
+        out = np.zeros(t.shape[0], np.uint32)
+        lib.oracle_svo_bin_rays(self.h, _p(org), _p(dirs), _p(t), _p(valid),
+                                C.c_uint32(t.shape[0]), C.c_uint32(min_level),
+                                C.c_uint32(bin_ray_count), _p(out))
+        return out
+
+    def cone_trace(self, org: np.ndarray, dirs: np.ndarray, tmin: np.ndarray,
+                   aperture: np.ndarray, max_query_offset: int = 0) -> dict:
+        """ConeTraceRay + ReadRadiance per cone: t, id, is_leaf, radiance."""
+        org = np.ascontiguousarray(org, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        tmin = np.ascontiguousarray(tmin, np.float32)
+        aperture = np.ascontiguousarray(aperture, np.float32)
+        n = tmin.shape[0]
+        out = {"t": np.zeros(n, np.float32), "id": np.zeros(n, np.uint32),
+               "leaf": np.zeros(n, np.uint8), "radiance": np.zeros(n, np.float32)}
+        lib.oracle_svo_cone_trace(self.h, _p(org), _p(dirs), _p(tmin), _p(aperture),
+                                  C.c_uint32(max_query_offset), C.c_uint32(n), _p(out["t"]),
+                                  _p(out["id"]), _p(out["leaf"]), _p(out["radiance"]))
+        return out
+
     def export(self) -> dict:
         sz = np.zeros(6, np.uint32)
         lib.oracle_svo_sizes(self.h, _p(sz))
@@ -391,6 +420,24 @@ class OracleSvo:
                                        _p(out["leaf_irr"]), _p(out["leaf_cnt"]),
                                        _p(out["leaf_avg"]), _p(out["node_avg"]))
         return out
+
+
+def voxelize(positions: np.ndarray, indices: np.ndarray, extent: np.ndarray, resolution: int):
+    """TriFunctions::Voxelize over every triangle: (per-triangle voxel counts,
+    Morton codes, packed spherical normals u16 | u16 << 16), triangle order."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    ext = np.ascontiguousarray(extent[:6], np.float32)
+    T = idx.shape[0]
+    counts = np.zeros(T, np.uint64)
+    lib.oracle_voxelize.restype = C.c_int64
+    n = lib.oracle_voxelize(_p(pos), _p(idx), C.c_uint32(T), _p(ext), C.c_uint32(resolution),
+                            _p(counts), None, None, C.c_uint64(0))
+    codes = np.zeros(n, np.uint64)
+    normals = np.zeros(n, np.uint32)
+    lib.oracle_voxelize(_p(pos), _p(idx), C.c_uint32(T), _p(ext), C.c_uint32(resolution),
+                        _p(counts), _p(codes), _p(normals), C.c_uint64(n))
+    return counts, codes, normals
 
 
 def svo_build(scene, tri_key: np.ndarray, extent: np.ndarray, resolution: int) -> dict:

@@ -2,8 +2,10 @@
 
 Runs the reference routines compiled by ``make -C oracle ref`` into
 ``oracle/_ref/libmrayref.so`` (MRay headers #included from the reference
-tree; LBVH kernels cut from LinearBVH.hpp at build time) on seeded random
-inputs and stores inputs + outputs in ``tests/golden/reference_vectors.npz``.
+tree; LBVH kernels cut from LinearBVH.hpp and the octree kernels cut from
+AnisoSVO.cu at build time) on seeded random inputs and stores inputs +
+outputs in ``tests/golden/reference_vectors.npz`` and (octree: voxelizer,
+level build, ray bins, cone traces) ``tests/golden/svo_reference_vectors.npz``.
 The CPU oracle is then checked against these vectors by
 ``tests/test_oracle_golden.py``; the reference tree is not needed at test
 time.
@@ -259,6 +261,122 @@ def main(ref_root: str | None = None) -> None:
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1024:.0f} KiB, {len(g)} arrays)")
+    svo_golden(R)
+
+
+def _scenes():
+    """The seeded scene generator, loaded from its file alone."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mrb_scenes_standalone",
+                                                  ROOT / "meturay_b200" / "scenes.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def svo_golden(R) -> None:
+    """Octree vectors from the reference's own code (oracle/ref_svo.cpp):
+    TriFunctions::Voxelize, the Constrcut level kernels, ray binning with
+    collapse, and ConeTraceRay + ReadRadiance, on two seeded scenes.  The
+    cones read the oracle's payload (normal words and half2 averages after
+    KCReduceVoxelPayload and the filters), stored beside them as input."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as o
+    scenes = _scenes()
+    R.ref_svo_voxelize.restype = C.c_int64
+    R.ref_svo_build.restype = C.c_void_p
+    g: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(20261204)
+    cases = (("cornell64", scenes.cornell(seed=1), 64),
+             ("clusters128", scenes.clusters(seed=3, n_clusters=8, tris_per_cluster=300), 128))
+    for tag, scene, res in cases:
+        pos = np.ascontiguousarray(scene.positions, np.float32)
+        idx = np.ascontiguousarray(scene.indices, np.uint32)
+        ext = np.concatenate([pos.min(0), pos.max(0)]).astype(np.float32)
+        tabs = o.scene_tables(scene)
+        light_rad = np.array([m["radiance"] for m in scene.materials if int(m["type"]) == 4],
+                             np.float32).reshape(-1, 3)
+        T = idx.shape[0]
+        counts = np.zeros(T, np.uint64)
+        box = np.zeros(6, np.float32)
+        n = R.ref_svo_voxelize(_p(pos), _p(idx), C.c_uint32(T), _p(ext), C.c_uint32(res),
+                               _p(box), _p(counts), None, None, C.c_uint64(0))
+        codes = np.zeros(n, np.uint64)
+        normals = np.zeros(n, np.uint32)
+        assert R.ref_svo_voxelize(_p(pos), _p(idx), C.c_uint32(T), _p(ext), C.c_uint32(res),
+                                  _p(box), _p(counts), _p(codes), _p(normals),
+                                  C.c_uint64(n)) == n
+        st = C.c_int(0)
+        h = C.c_void_p(R.ref_svo_build(_p(codes), C.c_uint64(n), _p(ext), C.c_uint32(res),
+                                       C.byref(st)))
+        assert st.value == 0
+        sz = np.zeros(3, np.uint32)
+        R.ref_svo_sizes(h, _p(sz))
+        nodes = np.zeros(sz[0], np.uint64)
+        parents = np.zeros(sz[1], np.uint32)
+        leaf_codes = np.zeros(sz[1], np.uint64)
+        offsets = np.zeros(sz[2], np.uint32)
+        R.ref_svo_get(h, _p(nodes), _p(parents), _p(leaf_codes), _p(offsets))
+        g.update({f"{tag}_pos": pos, f"{tag}_idx": idx, f"{tag}_ext": ext,
+                  f"{tag}_res": np.array([res], np.uint32), f"{tag}_tri_key": tabs["tri_key"],
+                  f"{tag}_light_rad": light_rad, f"{tag}_svo_box": box,
+                  f"{tag}_tri_counts": counts, f"{tag}_codes": codes, f"{tag}_normals": normals,
+                  f"{tag}_nodes": nodes, f"{tag}_leaf_parents": parents,
+                  f"{tag}_leaf_codes": leaf_codes, f"{tag}_level_offsets": offsets})
+        # rays hitting points inside random leaves, from random origins
+        m = 4000
+        lo, hi = box[:3].astype(np.float64), box[3:].astype(np.float64)
+        vs = (hi - lo) / res
+        c = leaf_codes[rng.integers(0, leaf_codes.shape[0], m)]
+        cell = np.zeros((m, 3))
+        for b in range(21):
+            for k in range(3):
+                cell[:, k] += ((c >> np.uint64(3 * b + k)) & np.uint64(1)).astype(np.float64) * (1 << b)
+        hitp = lo + (cell + rng.uniform(0.05, 0.95, (m, 3))) * vs
+        org = (hitp + rng.normal(size=(m, 3)) * 0.3 * (hi - lo)).astype(np.float32)
+        d = hitp - org
+        tt = np.linalg.norm(d, axis=1)
+        d = (d / tt[:, None]).astype(np.float32)
+        tt = tt.astype(np.float32)
+        valid = (rng.uniform(size=m) > 0.1).astype(np.uint8)
+        g.update({f"{tag}_bin_org": org, f"{tag}_bin_dir": d, f"{tag}_bin_t": tt,
+                  f"{tag}_bin_valid": valid})
+        for ml, brc in ((5, 512), (3, 64), (1, 4096)):
+            out = np.zeros(m, np.uint32)
+            R.ref_svo_bin_rays(h, _p(org), _p(d), _p(tt), _p(valid), C.c_uint32(m),
+                               C.c_uint32(ml), C.c_uint32(brc), _p(out))
+            g[f"{tag}_bins_{ml}_{brc}"] = out
+        # cones over the oracle's payload
+        svo = o.OracleSvo(scene, tabs["tri_key"], ext, res, light_rad)
+        ex = svo.export()
+        assert np.array_equal(ex["nodes"], nodes), "oracle octree differs from the reference"
+        R.ref_svo_set_payload(h, _p(ex["leaf_normals"]), _p(ex["node_normals"]),
+                              _p(ex["leaf_avg"]), _p(ex["node_avg"]))
+        for k in ("leaf_normals", "node_normals", "leaf_avg", "node_avg"):
+            g[f"{tag}_payload_{k}"] = ex[k]
+        org = (lo + rng.uniform(0.02, 0.98, (m, 3)) * (hi - lo)).astype(np.float32)
+        d = rng.normal(size=(m, 3))
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        tmin = (rng.uniform(0, 0.05, m) * (hi - lo).max()).astype(np.float32)
+        tmin[: m // 4] = 0.0
+        tmax = np.full(m, 3.0e38, np.float32)
+        ap = (4.0 * np.pi / rng.choice([64.0 ** 2, 32.0 ** 2, 8.0 ** 2], m)).astype(np.float32)
+        g.update({f"{tag}_cone_org": org, f"{tag}_cone_dir": d, f"{tag}_cone_tmin": tmin,
+                  f"{tag}_cone_aperture": ap})
+        for mq in (0, 2):
+            t = np.zeros(m, np.float32)
+            nid = np.zeros(m, np.uint32)
+            leaf = np.zeros(m, np.uint8)
+            rad = np.zeros(m, np.float32)
+            R.ref_svo_cone_trace(h, _p(org), _p(d), _p(tmin), _p(tmax), _p(ap), C.c_uint32(mq),
+                                 C.c_uint32(m), _p(t), _p(nid), _p(leaf), _p(rad))
+            g.update({f"{tag}_cone{mq}_t": t, f"{tag}_cone{mq}_id": nid,
+                      f"{tag}_cone{mq}_leaf": leaf, f"{tag}_cone{mq}_radiance": rad})
+        R.ref_svo_destroy(h)
+    out = HERE / "svo_reference_vectors.npz"
+    np.savez_compressed(out, **g)
+    print(f"wrote {out} ({out.stat().st_size / 1024:.0f} KiB, {len(g)} arrays)")
 
 
 if __name__ == "__main__":

@@ -161,3 +161,81 @@ def test_vndf_sample_within_tolerance(oracle):
     assert np.abs(out[:, :3] - G["vndf_h"]).max() < VNDF_ATOL
     rel = np.abs(out[:, 3] - G["vndf_pdf"]) / np.maximum(np.abs(G["vndf_pdf"]), 1e-6)
     assert np.median(rel) < 1e-5 and rel.max() < 1e-2
+
+
+# ---- octree (guided path): vectors from the reference's own voxelizer, level
+# kernels, ray binning and cone tracer (tests/golden/make_golden.py svo_golden)
+S = dict(np.load(Path(__file__).resolve().parent / "golden" / "svo_reference_vectors.npz"))
+SVO_CASES = ("cornell64", "clusters128")
+
+
+class _Mesh:
+    def __init__(self, tag):
+        self.positions = S[f"{tag}_pos"]
+        self.indices = S[f"{tag}_idx"]
+
+
+def _svo(oracle, tag):
+    return oracle.OracleSvo(_Mesh(tag), S[f"{tag}_tri_key"], S[f"{tag}_ext"],
+                            int(S[f"{tag}_res"][0]), S[f"{tag}_light_rad"])
+
+
+@pytest.mark.parametrize("tag", SVO_CASES)
+def test_svo_voxelize_matches_reference(oracle, tag):
+    """TriFunctions::Voxelize: per-triangle voxel counts and Morton codes are
+    bit-exact.  The packed spherical normal (two 16-bit UNORMs of atan2 and
+    acos) may differ by one step where the oracle's portable atan2/acos and
+    the C library round to neighbouring floats."""
+    counts, codes, normals = oracle.voxelize(S[f"{tag}_pos"], S[f"{tag}_idx"], S[f"{tag}_ext"],
+                                             int(S[f"{tag}_res"][0]))
+    assert np.array_equal(counts, S[f"{tag}_tri_counts"])
+    assert np.array_equal(codes, S[f"{tag}_codes"])
+    ref = S[f"{tag}_normals"]
+    du = np.abs((normals & 0xFFFF).astype(np.int64) - (ref & 0xFFFF).astype(np.int64))
+    dv = np.abs((normals >> 16).astype(np.int64) - (ref >> 16).astype(np.int64))
+    assert du.max() <= 1 and dv.max() <= 1
+    assert np.count_nonzero(normals != ref) <= max(1, ref.shape[0] // 500)
+
+
+@pytest.mark.parametrize("tag", SVO_CASES)
+def test_svo_structure_matches_reference(oracle, tag):
+    """AnisoSVOctreeCPU::Constrcut's level kernels: packed nodes (children,
+    parent, child mask, leaf bit), leaf parents, leaf codes and level offsets
+    bit-exact."""
+    ex = _svo(oracle, tag).export()
+    for k in ("nodes", "leaf_parents", "leaf_codes", "level_offsets"):
+        assert np.array_equal(ex[k], S[f"{tag}_{k}"]), k
+
+
+@pytest.mark.parametrize("tag", SVO_CASES)
+@pytest.mark.parametrize("min_level,ray_count", [(5, 512), (3, 64), (1, 4096)])
+def test_svo_bins_match_reference(oracle, tag, min_level, ray_count):
+    """Ray binning: the leaf of each hit (NearestNodeIndex with the neighbour
+    search), leaf ray counts, the bottom-up collapse to MinRayBinLevel until
+    BinRayCount rays, and FindMarkedBin: every ray's bin id bit-exact."""
+    svo = _svo(oracle, tag)
+    got = svo.bin_rays(S[f"{tag}_bin_org"], S[f"{tag}_bin_dir"], S[f"{tag}_bin_t"],
+                       S[f"{tag}_bin_valid"], min_level, ray_count)
+    assert np.array_equal(got, S[f"{tag}_bins_{min_level}_{ray_count}"])
+
+
+@pytest.mark.parametrize("tag", SVO_CASES)
+@pytest.mark.parametrize("max_query_offset", [0, 2])
+def test_svo_cone_trace_matches_reference(oracle, tag, max_query_offset):
+    """ConeTraceRay + ReadRadiance: returned t, node or leaf index, leaf flag
+    and radiance bit-exact for cones of three apertures, half of them from
+    tMin 0 inside the octree.  The radiance is read from the oracle's payload,
+    stored with the vectors as the reference's input."""
+    svo = _svo(oracle, tag)
+    ex = svo.export()
+    for k in ("leaf_normals", "node_normals", "leaf_avg", "node_avg"):
+        assert np.array_equal(ex[k], S[f"{tag}_payload_{k}"]), k
+    got = svo.cone_trace(S[f"{tag}_cone_org"], S[f"{tag}_cone_dir"], S[f"{tag}_cone_tmin"],
+                         S[f"{tag}_cone_aperture"], max_query_offset)
+    p = f"{tag}_cone{max_query_offset}"
+    assert np.array_equal(got["t"].view(np.uint32), S[f"{p}_t"].view(np.uint32))
+    assert np.array_equal(got["id"], S[f"{p}_id"])
+    assert np.array_equal(got["leaf"], S[f"{p}_leaf"])
+    assert np.array_equal(got["radiance"].view(np.uint32), S[f"{p}_radiance"].view(np.uint32))
+    assert np.count_nonzero(S[f"{p}_id"] != 0xFFFFFFFF) > 1000
+    assert np.count_nonzero(S[f"{p}_radiance"]) > 50
