@@ -363,6 +363,10 @@ class OracleSvo:
                                                  C.c_uint32(resolution), C.byref(st)))
         self.status = st.value
         self._rad = np.ascontiguousarray(np.asarray(light_radiance, np.float32).reshape(-1, 3))
+        lights = self._key[(self._key >> 24) == 4] & 0xFFFFFF
+        if lights.size and int(lights.max()) >= self._rad.shape[0]:
+            raise ValueError(f"light radiance has {self._rad.shape[0]} entries; the triangle "
+                             f"keys index light {int(lights.max())}")
         if self.status == 0:
             lib.oracle_svo_payload_init(self.h, _p(self._rad), C.c_uint32(1 if omit_direct else 0))
 

@@ -295,8 +295,7 @@ def svo_golden(R) -> None:
         idx = np.ascontiguousarray(scene.indices, np.uint32)
         ext = np.concatenate([pos.min(0), pos.max(0)]).astype(np.float32)
         tabs = o.scene_tables(scene)
-        light_rad = np.array([m["radiance"] for m in scene.materials if int(m["type"]) == 4],
-                             np.float32).reshape(-1, 3)
+        light_rad = tabs["light_radiance"]  # one per light triangle, as the keys index them
         T = idx.shape[0]
         counts = np.zeros(T, np.uint64)
         box = np.zeros(6, np.float32)
