@@ -2095,6 +2095,25 @@ void bin_rays(oracle_svo* svo, uint32_t n, uint32_t minLevel, uint32_t binRayCou
     }
 }
 
+// AnisoSVOctreeGPU::DepositRadiance (AnisoSVO.cuh:1080-1098) with
+// VoxelPayload::WriteLeafRadiance (:490-537): the leaf of the vertex (with the
+// neighbour search), the side its normal puts wo on, one sample of the
+// luminance there (2^-24 fixed point).  False when no leaf is found.
+bool deposit_leaf(oracle_svo* svo, const Tree& tree, F3 pos, F3 wo, float luminance) {
+    uint32_t leaf;
+    if (!tree.nearest(leaf, pos, svo->P.depth)) return false;
+    float sd, spc;
+    const F3 n = read_normal_spec(svo->leafNormSpec[leaf], sd, spc);
+    const float NdL = dot(n, wo);
+    int side;
+    if (NdL >= 0.0f) side = 0;
+    else if (NdL < 0.0f) side = 1;
+    else return true;
+    svo->leafIrr[2 * leaf + side] += to_fixed(luminance);
+    svo->leafCnt[2 * leaf + side] += 1u;
+    return true;
+}
+
 // KCReduceVoxelPayload (AnisoSVOKC.cuh:8-320), one voxel at a time with
 // sequential sums, then KCAverageNormals bottom-up (AnisoSVO.cu:428-528)
 void payload_init(oracle_svo* o, const float* lightRad, uint32_t omit) {
@@ -2366,6 +2385,24 @@ extern "C" void oracle_svo_bin_rays(oracle_svo* o, const float* org, const float
                  return true;
              },
              binOut);
+}
+
+extern "C" void oracle_svo_set_radiance(oracle_svo* o, const uint64_t* leafIrr,
+                                        const uint32_t* leafCnt) {
+    std::copy(leafIrr, leafIrr + o->leafIrr.size(), o->leafIrr.begin());
+    std::copy(leafCnt, leafCnt + o->leafCnt.size(), o->leafCnt.begin());
+}
+
+extern "C" void oracle_svo_normalize(oracle_svo* o) { normalize_filter(o); }
+
+extern "C" void oracle_svo_deposit(oracle_svo* o, const float* pos, const float* wo,
+                                   const float* lum, uint32_t n) {
+    std::fill(o->leafIrr.begin(), o->leafIrr.end(), 0ull);
+    std::fill(o->leafCnt.begin(), o->leafCnt.end(), 0u);
+    Tree tree{o};
+    for (uint32_t i = 0; i < n; i++)
+        deposit_leaf(o, tree, F3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]),
+                     F3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), lum[i]);
 }
 
 extern "C" void oracle_svo_cone_trace(const oracle_svo* o, const float* org, const float* dir,
@@ -2875,17 +2912,7 @@ extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* 
             const F3 pos(chain.pos[3 * at], chain.pos[3 * at + 1], chain.pos[3 * at + 2]);
             const size_t pa = chain.at(d - 1, p);
             const F3 wo = normalize(F3(chain.pos[3 * pa], chain.pos[3 * pa + 1], chain.pos[3 * pa + 2]) - pos);
-            uint32_t leaf;
-            if (!tree.nearest(leaf, pos, D)) continue;
-            float sd, spc;
-            const F3 n = read_normal_spec(svo->leafNormSpec[leaf], sd, spc);
-            const float NdL = dot(n, wo);
-            int side;
-            if (NdL >= 0.0f) side = 0;
-            else if (NdL < 0.0f) side = 1;
-            else continue;
-            svo->leafIrr[2 * leaf + side] += to_fixed(lum3(tot));
-            svo->leafCnt[2 * leaf + side] += 1u;
+            deposit_leaf(svo, tree, pos, wo, lum3(tot));
         }
     }
     normalize_filter(svo);

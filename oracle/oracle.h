@@ -176,6 +176,13 @@ int64_t oracle_voxelize(const float* pos, const uint32_t* idx, uint32_t tri_coun
 void oracle_svo_bin_rays(oracle_svo*, const float* org, const float* dir, const float* t,
                          const uint8_t* valid, uint32_t n, uint32_t min_level,
                          uint32_t bin_ray_count, uint32_t* bin_out);
+/* Leaf radiance sums (2 per leaf, 2^-24 fixed point) and sample counts (2
+ * per leaf) set directly; NormalizeAndFilterRadiance over them. */
+void oracle_svo_set_radiance(oracle_svo*, const uint64_t* leaf_irr, const uint32_t* leaf_cnt);
+void oracle_svo_normalize(oracle_svo*);
+/* DepositRadiance of n vertices (position, wo, luminance) over zeroed sums. */
+void oracle_svo_deposit(oracle_svo*, const float* pos, const float* wo, const float* lum,
+                        uint32_t n);
 /* ConeTraceRay + ReadRadiance for n cones. */
 void oracle_svo_cone_trace(const oracle_svo*, const float* org, const float* dir,
                            const float* tmin, const float* aperture, uint32_t max_query_offset,

@@ -389,6 +389,22 @@ class OracleSvo:
                                 C.c_uint32(bin_ray_count), _p(out))
         return out
 
+    def set_radiance(self, leaf_irr: np.ndarray, leaf_cnt: np.ndarray, normalize: bool = True):
+        """Set the leaf radiance sums (2^-24 fixed point) and counts, then
+        NormalizeAndFilterRadiance."""
+        irr = np.ascontiguousarray(leaf_irr, np.uint64)
+        cnt = np.ascontiguousarray(leaf_cnt, np.uint32)
+        lib.oracle_svo_set_radiance(self.h, _p(irr), _p(cnt))
+        if normalize:
+            lib.oracle_svo_normalize(self.h)
+
+    def deposit(self, pos: np.ndarray, wo: np.ndarray, lum: np.ndarray):
+        """DepositRadiance of path vertices over zeroed leaf sums."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        wo = np.ascontiguousarray(wo, np.float32)
+        lum = np.ascontiguousarray(lum, np.float32)
+        lib.oracle_svo_deposit(self.h, _p(pos), _p(wo), _p(lum), C.c_uint32(lum.shape[0]))
+
     def cone_trace(self, org: np.ndarray, dirs: np.ndarray, tmin: np.ndarray,
                    aperture: np.ndarray, max_query_offset: int = 0) -> dict:
         """ConeTraceRay + ReadRadiance per cone: t, id, is_leaf, radiance."""

@@ -14,7 +14,10 @@
 //     (AnisoSVO.cu:1485-1528) and FindMarkedBin (KCCheckReducedSVOBins,
 //     WFPGTracerKC.cuh:1045-1066);
 //   - AnisoSVOctreeGPU::ConeTraceRay and ReadRadiance (AnisoSVO.cuh:767-1033,
-//     1035-1055, VoxelPayload::ReadRadiance :433-470).
+//     1035-1055, VoxelPayload::ReadRadiance :433-470);
+//   - the payload passes: KCAverageNormals (AnisoSVO.cu:418-517),
+//     NormalizeAndFilterRadiance with its three kernels (AnisoSVO.cu:352-380,
+//     519-654, 1415-1483) and DepositRadiance (AnisoSVO.cuh:1080-1098).
 //
 // TEST INFRASTRUCTURE ONLY (tests/golden/make_golden.py).  The reference
 // headers are #included from REF_ROOT and the kernel bodies are cut out of
@@ -112,10 +115,16 @@ static inline float __uint_as_float(unsigned int x) {
 #undef protected
 
 #define CUDA_LAUNCH_BOUNDS_1D
-// KCMarkMortonChanges .. KCSetParentOfLeafChildren (AnisoSVO.cu:58-222) and
-// KCCollapseRayCounts / KCCollapseRayCountsLeaf (AnisoSVO.cu:265-350)
+// KCMarkMortonChanges .. KCSetParentOfLeafChildren (AnisoSVO.cu:58-222),
+// KCCollapseRayCounts / KCCollapseRayCountsLeaf (AnisoSVO.cu:265-350),
+// KCCCopyRadianceToHalfBufferLeaf (:352-380) and KCAverageNormals,
+// KCBottomUpFilterIrradiance, KCTopDownFilterIrradiance (:418-654).  This
+// file is compiled with -ftrivial-auto-var-init=zero: KCAverageNormals adds
+// into its second k-means buffer before anything is written there, and
+// zero is the start that clustering intends.
 #include "svo_level_kernels.inc"
 #include "svo_collapse_kernels.inc"
+#include "svo_payload_kernels.inc"
 
 namespace {
 
@@ -178,6 +187,10 @@ struct RefSvo {
     std::vector<uint32_t> binInfo, leafBinInfo;
     std::vector<uint32_t> nodeNormSpec, leafNormSpec;
     std::vector<Vector2h> nodeAvg, leafAvg;
+    std::vector<Vector2f> leafIrr;
+    std::vector<Vector2ui> leafCnt;
+    std::vector<uint32_t> shadowHit, shadowMiss;
+    std::vector<half> nodeFactor;
 };
 
 }  // namespace
@@ -313,6 +326,11 @@ void* ref_svo_build(const uint64_t* voxels, uint64_t nvox, const float* scene_aa
     h->leafNormSpec.assign(U, 0);
     h->nodeAvg.assign(nodeCount, Vector2h(0.0f, 0.0f));
     h->leafAvg.assign(U, Vector2h(0.0f, 0.0f));
+    h->leafIrr.assign(U, Vector2f(0.0f, 0.0f));
+    h->leafCnt.assign(U, Vector2ui(0u, 0u));
+    h->shadowHit.assign(U, 0u);
+    h->shadowMiss.assign(U, 0u);
+    h->nodeFactor.assign(nodeCount, half(0.0f));
     T.dNodes = h->nodes.data();
     T.dLeafParents = h->leafParents.data();
     T.dLevelNodeOffsets = h->levelOffsets.data();
@@ -322,6 +340,11 @@ void* ref_svo_build(const uint64_t* voxels, uint64_t nvox, const float* scene_aa
     T.payload.dNormalAndSpecLeaf = h->leafNormSpec.data();
     T.payload.dAvgIrradianceNode = h->nodeAvg.data();
     T.payload.dAvgIrradianceLeaf = h->leafAvg.data();
+    T.payload.dTotalIrradianceLeaf = h->leafIrr.data();
+    T.payload.dSampleCountLeaf = h->leafCnt.data();
+    T.payload.dShadowRayHitLeaf = h->shadowHit.data();
+    T.payload.dShadowRayMissLeaf = h->shadowMiss.data();
+    T.payload.dGuidingFactorNode = h->nodeFactor.data();
     T.dBoundaryLight = nullptr;
     return h.release();
 }
@@ -428,6 +451,87 @@ void ref_svo_cone_trace(const void* p, const float* o, const float* d, const flo
         id_out[i] = id;
         leaf_out[i] = isLeaf ? 1 : 0;
         rad_out[i] = T.ReadRadiance(ray.getDirection(), aperture[i], id, isLeaf);
+    }
+}
+
+// KCAverageNormals bottom-up over the node levels (AnisoSVO.cu:1066-1088)
+// from the given leaf normal words; node words out.
+void ref_svo_average_normals(void* p, const uint32_t* leaf_norm_spec, uint32_t* node_norm_spec) {
+    RefSvo* h = static_cast<RefSvo*>(p);
+    AnisoSVOctreeGPU& T = h->tree;
+    std::copy(leaf_norm_spec, leaf_norm_spec + h->leafNormSpec.size(), h->leafNormSpec.begin());
+    const uint32_t levelCount = T.leafDepth;
+    for (uint32_t i = 0; i < levelCount; i++) {
+        const uint32_t levelIndex = levelCount - i - 1;
+        const bool lastNonLeafLevel = (levelIndex == (levelCount - 1));
+        const uint32_t count = h->levelCounts[levelIndex];
+        launch(count, [&] {
+            KCAverageNormals(T.payload, T.dNodes, T.dLevelNodeOffsets, levelIndex, count,
+                             lastNonLeafLevel);
+        });
+    }
+    std::copy(h->nodeNormSpec.begin(), h->nodeNormSpec.end(), node_norm_spec);
+}
+
+// AnisoSVOctreeCPU::NormalizeAndFilterRadiance (AnisoSVO.cu:1415-1483): leaf
+// averages from the FP32 sums and counts, bottom-up node averages, top-down
+// fill of the empty ones.  Uses the normal words set by ref_svo_set_payload;
+// leaf / node half2 averages out (u16 | u16 << 16).
+void ref_svo_normalize_filter(void* p, const float* leaf_irr2, const uint32_t* leaf_cnt2,
+                              uint32_t* leaf_avg, uint32_t* node_avg) {
+    RefSvo* h = static_cast<RefSvo*>(p);
+    AnisoSVOctreeGPU& T = h->tree;
+    for (size_t l = 0; l < h->leafIrr.size(); l++) {
+        h->leafIrr[l] = Vector2f(leaf_irr2[2 * l], leaf_irr2[2 * l + 1]);
+        h->leafCnt[l] = Vector2ui(leaf_cnt2[2 * l], leaf_cnt2[2 * l + 1]);
+    }
+    launch(T.leafCount, [&] {
+        KCCCopyRadianceToHalfBufferLeaf(T.payload.dAvgIrradianceLeaf,
+                                        T.payload.dTotalIrradianceLeaf,
+                                        T.payload.dSampleCountLeaf, T.leafCount, 1.0f);
+    });
+    const uint32_t levelCount = T.leafDepth;
+    const std::vector<uint32_t>& offs = h->levelOffsets;
+    for (uint32_t i = 0; i < levelCount; i++) {
+        const uint32_t levelIndex = levelCount - i - 1;
+        const bool lastNonLeafLevel = (levelIndex == (levelCount - 1));
+        const uint32_t count = offs[levelIndex + 1] - offs[levelIndex];
+        launch(count, [&] {
+            KCBottomUpFilterIrradiance(T.payload, T.dNodes, T.dLevelNodeOffsets, levelIndex,
+                                       count, lastNonLeafLevel);
+        });
+    }
+    for (uint32_t i = 1; i <= levelCount; i++) {
+        const bool isLeafLevel = (i == levelCount);
+        const uint32_t count = offs[i + 1] - offs[i];
+        launch(count, [&] {
+            KCTopDownFilterIrradiance(T.payload, T.dNodes, T.dLeafParents, T.dLevelNodeOffsets,
+                                      i, count, isLeafLevel);
+        });
+    }
+    std::memcpy(leaf_avg, h->leafAvg.data(), 4 * h->leafAvg.size());
+    std::memcpy(node_avg, h->nodeAvg.data(), 4 * h->nodeAvg.size());
+}
+
+// AnisoSVOctreeGPU::DepositRadiance (AnisoSVO.cuh:1080-1098 with
+// VoxelPayload::WriteLeafRadiance :490-537) for n path vertices, in order,
+// over zeroed accumulators; leaf sums (2 floats) and counts (2) out.  The
+// surface normal and wi the reference passes are not read by it.
+void ref_svo_deposit(void* p, const float* pos, const float* wo, const float* lum, uint32_t n,
+                     float* leaf_irr2, uint32_t* leaf_cnt2) {
+    RefSvo* h = static_cast<RefSvo*>(p);
+    AnisoSVOctreeGPU& T = h->tree;
+    std::fill(h->leafIrr.begin(), h->leafIrr.end(), Vector2f(0.0f, 0.0f));
+    std::fill(h->leafCnt.begin(), h->leafCnt.end(), Vector2ui(0u, 0u));
+    for (uint32_t i = 0; i < n; i++) {
+        const Vector3f w(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+        T.DepositRadiance(Vector3f(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), w, w, w, lum[i]);
+    }
+    for (size_t l = 0; l < h->leafIrr.size(); l++) {
+        leaf_irr2[2 * l] = h->leafIrr[l][0];
+        leaf_irr2[2 * l + 1] = h->leafIrr[l][1];
+        leaf_cnt2[2 * l] = h->leafCnt[l][0];
+        leaf_cnt2[2 * l + 1] = h->leafCnt[l][1];
     }
 }
 

@@ -278,9 +278,11 @@ def _scenes():
 def svo_golden(R) -> None:
     """Octree vectors from the reference's own code (oracle/ref_svo.cpp):
     TriFunctions::Voxelize, the Constrcut level kernels, ray binning with
-    collapse, and ConeTraceRay + ReadRadiance, on two seeded scenes.  The
-    cones read the oracle's payload (normal words and half2 averages after
-    KCReduceVoxelPayload and the filters), stored beside them as input."""
+    collapse, ConeTraceRay + ReadRadiance, KCAverageNormals,
+    NormalizeAndFilterRadiance and DepositRadiance, on two seeded scenes.
+    The cones and the normal averaging read the oracle's payload (leaf normal
+    words from KCReduceVoxelPayload, half2 averages after the filters), stored
+    beside them as input."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as o
     scenes = _scenes()
@@ -372,6 +374,38 @@ def svo_golden(R) -> None:
                                  C.c_uint32(m), _p(t), _p(nid), _p(leaf), _p(rad))
             g.update({f"{tag}_cone{mq}_t": t, f"{tag}_cone{mq}_id": nid,
                       f"{tag}_cone{mq}_leaf": leaf, f"{tag}_cone{mq}_radiance": rad})
+        # KCAverageNormals over the oracle's leaf normal words
+        nn = np.zeros(nodes.shape[0], np.uint32)
+        R.ref_svo_average_normals(h, _p(ex["leaf_normals"]), _p(nn))
+        g[f"{tag}_node_normals"] = nn
+        if tag == "clusters128":
+            U = leaf_codes.shape[0]
+            # NormalizeAndFilterRadiance over seeded sums (2^-24 fixed point;
+            # the reference gets them as FP32) and counts, 60 % of them empty
+            cnt = (rng.integers(1, 40, (U, 2)) * (rng.uniform(size=(U, 2)) < 0.4)).astype(np.uint32)
+            fx = (rng.uniform(0, 2.0, (U, 2)) * cnt * (1 << 24)).astype(np.uint64)
+            ffl = (fx.astype(np.float64) / (1 << 24)).astype(np.float32)
+            la = np.zeros(U, np.uint32)
+            na = np.zeros(nodes.shape[0], np.uint32)
+            R.ref_svo_normalize_filter(h, _p(ffl), _p(cnt), _p(la), _p(na))
+            g.update({f"{tag}_norm_irr": fx, f"{tag}_norm_cnt": cnt, f"{tag}_norm_leaf_avg": la,
+                      f"{tag}_norm_node_avg": na})
+            # DepositRadiance of vertices in and around random leaves
+            m = 8000
+            c = leaf_codes[rng.integers(0, U, m)]
+            cell = np.zeros((m, 3))
+            for b in range(21):
+                for k in range(3):
+                    cell[:, k] += ((c >> np.uint64(3 * b + k)) & np.uint64(1)).astype(np.float64) * (1 << b)
+            pos = (lo + (cell + rng.uniform(-0.1, 1.1, (m, 3))) * vs).astype(np.float32)
+            wo = rng.normal(size=(m, 3))
+            wo = (wo / np.linalg.norm(wo, axis=1, keepdims=True)).astype(np.float32)
+            lum = rng.uniform(0, 3, m).astype(np.float32)
+            ri = np.zeros((U, 2), np.float32)
+            rc = np.zeros((U, 2), np.uint32)
+            R.ref_svo_deposit(h, _p(pos), _p(wo), _p(lum), C.c_uint32(m), _p(ri), _p(rc))
+            g.update({f"{tag}_dep_pos": pos, f"{tag}_dep_wo": wo, f"{tag}_dep_lum": lum,
+                      f"{tag}_dep_irr": ri, f"{tag}_dep_cnt": rc})
         R.ref_svo_destroy(h)
     out = HERE / "svo_reference_vectors.npz"
     np.savez_compressed(out, **g)

@@ -239,3 +239,59 @@ def test_svo_cone_trace_matches_reference(oracle, tag, max_query_offset):
     assert np.array_equal(got["radiance"].view(np.uint32), S[f"{p}_radiance"].view(np.uint32))
     assert np.count_nonzero(S[f"{p}_id"] != 0xFFFFFFFF) > 1000
     assert np.count_nonzero(S[f"{p}_radiance"]) > 50
+
+
+@pytest.mark.parametrize("tag", SVO_CASES)
+def test_svo_node_normals_match_reference(oracle, tag):
+    """KCAverageNormals (k-means with K = 2 over the children's Toksvig-scaled
+    normals, bottom-up): every node's normal/specular word bit-exact from the
+    same leaf words."""
+    ex = _svo(oracle, tag).export()
+    assert np.array_equal(ex["leaf_normals"], S[f"{tag}_payload_leaf_normals"])
+    assert np.array_equal(ex["node_normals"], S[f"{tag}_node_normals"])
+
+
+def _half_steps(a, b):
+    """Largest distance in binary16 steps between two arrays of half2 words."""
+    ua = np.concatenate([a & 0xFFFF, a >> 16]).astype(np.int64)
+    ub = np.concatenate([b & 0xFFFF, b >> 16]).astype(np.int64)
+    return int(np.abs(ua - ub).max())
+
+
+def test_svo_normalize_filter_matches_reference(oracle):
+    """NormalizeAndFilterRadiance: leaf averages (sum / count, clamped, to
+    half), bottom-up node averages over the children with the normal-side
+    swap and the empty-marker rules, then the top-down fill.  The oracle
+    divides the 2^-24 fixed-point sums in double and averages the children in
+    FP32 with one rounding to half; the reference divides FP32 sums and adds
+    the children in half precision.  Tolerances: leaf averages within one
+    binary16 step, node averages within four, and the empty markers (which
+    decide the top-down fill) identical."""
+    tag = "clusters128"
+    svo = _svo(oracle, tag)
+    svo.set_radiance(S[f"{tag}_norm_irr"], S[f"{tag}_norm_cnt"])
+    ex = svo.export()
+    leaf_ref, node_ref = S[f"{tag}_norm_leaf_avg"], S[f"{tag}_norm_node_avg"]
+    assert _half_steps(ex["leaf_avg"], leaf_ref) <= 1
+    assert np.count_nonzero(ex["leaf_avg"] != leaf_ref) <= leaf_ref.shape[0] // 1000
+    assert _half_steps(ex["node_avg"], node_ref) <= 4
+    assert np.count_nonzero(ex["node_avg"] != node_ref) <= node_ref.shape[0] // 4
+    for a, r in ((ex["leaf_avg"], leaf_ref), (ex["node_avg"], node_ref)):
+        for sh in (0, 16):
+            assert np.array_equal(((a >> sh) & 0xFFFF) == 0x7BFF, ((r >> sh) & 0xFFFF) == 0x7BFF)
+
+
+def test_svo_deposit_matches_reference(oracle):
+    """DepositRadiance: the leaf of each vertex (neighbour search), the side
+    its normal puts wo on, and the per-leaf, per-side sample counts are
+    bit-exact; the radiance sums agree within 1e-4 relative (the reference
+    adds FP32 values, the oracle 2^-24 fixed-point ones)."""
+    tag = "clusters128"
+    svo = _svo(oracle, tag)
+    svo.deposit(S[f"{tag}_dep_pos"], S[f"{tag}_dep_wo"], S[f"{tag}_dep_lum"])
+    ex = svo.export()
+    assert np.array_equal(ex["leaf_cnt"], S[f"{tag}_dep_cnt"])
+    assert S[f"{tag}_dep_cnt"].sum() > 7000
+    got = ex["leaf_irr"].astype(np.float64) / (1 << 24)
+    ref = S[f"{tag}_dep_irr"].astype(np.float64)
+    assert np.all(np.abs(got - ref) <= 1e-4 * np.maximum(ref, 1e-3))
