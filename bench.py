@@ -38,7 +38,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Mrays/s"
-WORKLOAD = {"workload": "clusters-1M plain path tracing", "triangles": 1000004,
+WORKLOAD = {"workload": "clusters-1M plain path tracing", "triangles": 1000008,
             "resolution": "1920x1080", "spp_per_step": 1, "max_depth": 8,
             "nee": True, "rr_start": 3, "scene_seed": 1,
             "recon_filter": "Tent, radius 1 pixel (the reference's tConf filter)",
@@ -723,17 +723,7 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
 def _oracle_setup(scene):
     """Scene arrays as the hot path consumes them, built by the oracle alone."""
     from oracle import oracle as o
-    import ctypes as C
-    tbn = np.zeros((scene.positions.shape[0], 4), np.float32)
-    pos = np.ascontiguousarray(scene.positions, np.float32)
-    nrm = np.ascontiguousarray(scene.normals, np.float32)
-    uvs = np.ascontiguousarray(scene.uvs, np.float32)
-    idx = np.ascontiguousarray(scene.indices, np.uint32)
-    o.lib.oracle_build_tbn(o._p(pos), o._p(nrm), o._p(uvs), o._p(idx),
-                           C.c_uint32(pos.shape[0]), C.c_uint32(idx.shape[0]), o._p(tbn))
-    ex = o.scene_tables(scene)
-    ex["tbn"] = tbn
-    return o.OracleScene(scene, ex)
+    return o.OracleScene.from_scene(scene)
 
 
 def _camera16(scene):

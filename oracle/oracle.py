@@ -185,6 +185,15 @@ class OracleScene:
         self.bvh = lib.oracle_bvh_create(C.byref(s), C.byref(st))
         self.bvh_status = st.value
 
+    @classmethod
+    def from_scene(cls, scene) -> "OracleScene":
+        """The scene with every table (HitKeys, material and light tables,
+        tangent-space rotations) built by the oracle itself, so that nothing
+        the checker uses comes from the device it checks."""
+        ex = scene_tables(scene)
+        ex["tbn"] = build_tbn(scene)
+        return cls(scene, ex)
+
     def __del__(self):
         if getattr(self, "bvh", None):
             lib.oracle_bvh_destroy(self.bvh)
@@ -440,6 +449,13 @@ class OracleSvo:
                                        _p(out["leaf_irr"]), _p(out["leaf_cnt"]),
                                        _p(out["leaf_avg"]), _p(out["node_avg"]))
         return out
+
+
+def scene_extent(scene) -> np.ndarray:
+    """Scene AABB (min xyz, max xyz) as the LBVH build reduces it: over the
+    per-triangle boxes of KCGenerateAABBs."""
+    aabbs, ext, _, _ = morton_codes(scene.positions, scene.indices)
+    return ext
 
 
 def voxelize(positions: np.ndarray, indices: np.ndarray, extent: np.ndarray, resolution: int):

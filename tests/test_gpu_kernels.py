@@ -177,8 +177,7 @@ def test_trace_closest_hit(system, cuda, oracle, name, make, mode):
     info = g.accel_info()
     if scene.triangle_count > 1:
         assert 0 < info["wide_nodes"] <= scene.triangle_count - 1
-    ex = g.export()
-    os_ = oracle.OracleScene(scene, ex)
+    os_ = oracle.OracleScene.from_scene(scene)
     n = 20000
     rays = _rays_for(scene, n, seed=11)
     key, prim, t, bary = os_.trace(rays)

@@ -29,7 +29,7 @@ def _setup(system, scene, opts):
 
 def _oracle_render(oracle, g, scene, opts, frame=0, fp64=False):
     from meturay_b200 import camera_frame
-    os_ = oracle.OracleScene(scene, g.export())
+    os_ = oracle.OracleScene.from_scene(scene)
     cf = np.concatenate([camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
     img, rays = os_.render(cf, scene.width, scene.height, opts["Samples"], opts["MaxDepth"],
                            opts["RussianRouletteStart"], bool(opts["NextEventEstimation"]),
@@ -125,7 +125,7 @@ def test_every_bxdf_with_and_without_mis(system, oracle, mis):
         pass
     t.finalize()
     gpu = t.sample_radiance()[..., :3]
-    os_ = oracle.OracleScene(scene, g.export())
+    os_ = oracle.OracleScene.from_scene(scene)
     cf = np.concatenate([camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
     ref, ref_rays = os_.render(cf, scene.width, scene.height, opts["Samples"], opts["MaxDepth"],
                                opts["RussianRouletteStart"], True, opts["Seed"], mis=bool(mis))
@@ -149,7 +149,7 @@ def test_scene_file_renders_like_the_oracle(system, oracle):
         pass
     t.finalize()
     gpu = t.sample_radiance()[..., :3]
-    os_ = oracle.OracleScene(scene, g.export())
+    os_ = oracle.OracleScene.from_scene(scene)
     cf = np.concatenate([m.camera_frame(scene.camera), np.float32(scene.camera["near_far"])])
     ref, ref_rays = os_.render(cf, scene.width, scene.height, opts["Samples"], opts["MaxDepth"],
                                opts["RussianRouletteStart"], True, opts["Seed"], mis=True)

@@ -30,8 +30,8 @@ def test_svo_bit_exact(system, oracle, name, make, res):
     g.construct_accelerators()
     g.build_svo(res)
     gpu = g.export_svo()
-    acc = g.export_accel()
-    ref = oracle.svo_build(scene, g.export()["tri_key"], acc["extent"], res)
+    ref = oracle.svo_build(scene, oracle.scene_tables(scene)["tri_key"],
+                           oracle.scene_extent(scene), res)
     assert ref["status"] == 0
     assert gpu["voxels"] == ref["voxels"]
     assert np.array_equal(gpu["level_offsets"], ref["level_offsets"])

@@ -24,10 +24,10 @@ def _rel_mean_err(a, b):
 
 
 def _oracle_svo(oracle, g, scene, res, omit=False):
-    ex = g.export()
-    acc = g.export_accel()
-    return oracle.OracleSvo(scene, ex["tri_key"], acc["extent"], res, ex["light_radiance"],
-                            omit_direct=omit)
+    """The oracle's octree from its own tables and scene extent."""
+    ex = oracle.scene_tables(scene)
+    return oracle.OracleSvo(scene, ex["tri_key"], oracle.scene_extent(scene), res,
+                            ex["light_radiance"], omit_direct=omit)
 
 
 def _assert_payload(gpu, ref, keys=PAYLOAD):
@@ -95,7 +95,7 @@ def test_guide_words_and_bins_match_oracle(system, oracle, product):
     t.generate_work()
     t.render()
     st = t.guide_state()
-    o = oracle.OracleScene(scene, g.export())
+    o = oracle.OracleScene.from_scene(scene)
     svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
     _, _, dg, db = o.render_wfpg(_cam(scene), scene.width, scene.height, 1, opts["MaxDepth"],
                                  opts["RussianRouletteStart"], True, opts["Seed"], svo,
@@ -130,7 +130,7 @@ def test_wfpg_frames_match_oracle(system, oracle, variant):
         opts["BXDF-GuideMISRatio"] = 0.7
         opts["RFieldFilterAlpha"] = 0.6
     g, t = _wfpg(system, scene, opts)
-    o = oracle.OracleScene(scene, g.export())
+    o = oracle.OracleScene.from_scene(scene)
     svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
     for frame in range(2):
         t.generate_work()
@@ -154,7 +154,7 @@ def test_wfpg_graph_frames_match_stepwise(system, oracle):
     scene = scenes.cornell(seed=7, width=32, height=32, mixed=True)
     opts = dict(WFPG_OPTS, Seed=11)
     g, t = _wfpg(system, scene, opts)
-    o = oracle.OracleScene(scene, g.export())
+    o = oracle.OracleScene.from_scene(scene)
     svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
     acc = np.zeros((scene.height, scene.width, 3), np.float64)
     for frame in range(3):
@@ -176,7 +176,7 @@ def test_wfpg_skip_pg_is_unguided(system, oracle):
     scene = scenes.cornell(seed=6, width=32, height=32, mixed=True)
     opts = dict(WFPG_OPTS, SkipPG=1)
     g, t = _wfpg(system, scene, opts)
-    o = oracle.OracleScene(scene, g.export())
+    o = oracle.OracleScene.from_scene(scene)
     svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
     t.generate_work()
     while t.render():
@@ -197,7 +197,7 @@ def test_wfpg_on_a_scene_file(system, oracle):
     scene = m.load_scene(Path(__file__).resolve().parent / "scenes" / "box_mixed.json", 32, 24)
     opts = dict(WFPG_OPTS, OctreeLevel=5, MinRayBinLevel=2, BinRayCount=32)
     g, t = _wfpg(system, scene, opts)
-    o = oracle.OracleScene(scene, g.export())
+    o = oracle.OracleScene.from_scene(scene)
     svo = _oracle_svo(oracle, g, scene, 1 << opts["OctreeLevel"])
     for frame in range(2):
         t.generate_work()
