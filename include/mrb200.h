@@ -376,6 +376,95 @@ int mrb_tracer_profile_frame(mrb_tracer* t, float* stage_ms, uint64_t* work);
  * the learned guider's join and sample collection. */
 int mrb_tracer_profile_stages(mrb_tracer* t, float* stage_ms, uint32_t n_stages, uint64_t* work);
 
+/* ---- accelerator group and base accelerator (the ray caster's interface)
+ * GPUAcceleratorGroupI / GPUBaseAcceleratorI (GPUAcceleratorI.h:46-173) as
+ * RayCasterCUDA::HitRays drives them (RayCasterCUDA.cu:35-166): the base
+ * accelerator hands each ray the key of the next surface whose box it
+ * crosses, the group's Hit traverses that surface's local-space LBVH.
+ * Transforms are row-major 3x4 local-to-world matrices (the fourth row of
+ * the reference's Matrix4x4 is 0 0 0 1).  Rays are RayGMem (32 B:
+ * position, tMin, direction, tMax) in device memory. */
+typedef struct mrb_accel_group mrb_accel_group;
+typedef struct mrb_base_accel mrb_base_accel;
+/* One surface of a group: triangles [tri_begin, tri_end) of the group's
+ * primitives under global transform transform_id (SurfaceDefinition,
+ * GPUAcceleratorI.h:34-39).  Ranges ascend and do not overlap. */
+typedef struct mrb_surface {
+    uint32_t tri_begin, tri_end;
+    uint32_t transform_id;
+} mrb_surface;
+/* InitializeGroup: host arrays of the group's triangles; tbn (w,x,y,z per
+ * vertex, as the triangle loader builds them), tri_cull and primitive_ids
+ * may be NULL.  Keys are the triangles' material HitKeys; primitive_ids are
+ * the ids Hit reports for each triangle (the primitive group's own indices
+ * when the caller packed several batches into one surface range; NULL: the
+ * triangle's index here).  Transform 0 is the identity until transforms are
+ * attached. */
+int mrb_accel_group_create(mrb_system* sys, const float* positions, uint32_t vertex_count,
+                           const float* tbn, const uint32_t* indices, const uint32_t* tri_keys,
+                           const uint8_t* tri_cull, const uint64_t* primitive_ids,
+                           uint32_t tri_count, const mrb_surface* surfaces,
+                           uint32_t surface_count, mrb_accel_group** out);
+void mrb_accel_group_destroy(mrb_accel_group* g);
+/* AttachGlobalTransformArray: count local-to-world matrices (12 floats
+ * each, host); their inverses are computed in double and rounded once. */
+int mrb_accel_group_attach_transforms(mrb_accel_group* g, const float* local_to_world,
+                                      uint32_t count, uint32_t identity_index);
+/* ConstructAccelerators: one LBVH per surface in its local space. */
+int mrb_accel_group_construct(mrb_accel_group* g, void* stream);
+/* Hit (GPUAcceleratorI.h:83-94; KCIntersectBVH, GPUAcceleratorBVHKC.cuh:
+ * 229-346): for i < ray_count, ray d_ray_ids[i] against surface
+ * (d_accel_keys[i] & 0xFFFFFF); a hit closer than the ray's tMax writes tMax
+ * back into d_rays and material key, transform id, 64-bit primitive id and
+ * the barycentrics (2 floats, TriangleHit) at index d_ray_ids[i]; hit
+ * structs are hit_stride bytes apart (HitStructPtr's combined size, a
+ * multiple of 4, at least 8).  Keys of surfaces the group does not have
+ * leave the ray untouched. */
+int mrb_accel_group_hit(const mrb_accel_group* g, uint32_t* d_material_keys,
+                        uint32_t* d_transform_ids, uint64_t* d_primitive_ids, void* d_hit_structs,
+                        uint32_t hit_stride, void* d_rays, const uint32_t* d_ray_ids,
+                        const uint32_t* d_accel_keys, uint32_t ray_count, void* stream);
+/* AcceleratorAABBs: world AABB of each surface (6 floats, min then max),
+ * up to capacity; returns the surface count. */
+int mrb_accel_group_aabbs(const mrb_accel_group* g, float* aabbs, uint32_t capacity);
+/* TotalPrimitiveCount, AcceleratorCount. */
+uint64_t mrb_accel_group_primitive_count(const mrb_accel_group* g);
+uint32_t mrb_accel_group_accelerator_count(const mrb_accel_group* g);
+/* TotalApproximateArea: sum of the triangles' world-space areas. */
+int mrb_accel_group_total_area(const mrb_accel_group* g, float* area, void* stream);
+/* SampleAreaWeightedPoints: count world positions and normals (3 floats
+ * each, device) on the surfaces, triangles drawn by area.  Philox with the
+ * seed replaces the reference's Sobol generator. */
+int mrb_accel_group_sample_points(const mrb_accel_group* g, float* d_positions, float* d_normals,
+                                  uint32_t count, uint64_t seed, void* stream);
+/* EachPrimVoxelCount / VoxelizeSurfaces (GPUAcceleratorI.h:113-133) over
+ * the octree box (6 floats, host) at resolution^3: per-primitive voxel
+ * counts, then codes, packed spherical normals (u16 | u16 << 16, the
+ * reference's Vector2us) and light keys at d_voxel_offsets[t] (exclusive
+ * scan of the counts, tri_count + 1 entries). */
+int mrb_accel_group_voxel_counts(const mrb_accel_group* g, uint64_t* d_counts, uint32_t resolution,
+                                 const float* octree_aabb, void* stream);
+int mrb_accel_group_voxelize(const mrb_accel_group* g, uint64_t* d_voxels,
+                             uint32_t* d_voxel_normals, uint32_t* d_voxel_light_keys,
+                             const uint64_t* d_voxel_offsets, const uint32_t* d_sorted_light_keys,
+                             uint32_t light_count, uint32_t resolution, const float* octree_aabb,
+                             void* stream);
+/* Base accelerator (GPUBaseAcceleratorBVH, GPUAcceleratorBVH.cu:35-260):
+ * Construct from the surfaces' world AABBs and accelerator keys (host);
+ * GetReady puts every ray id below ray_count at the root; Hit writes the
+ * next surface's key for each d_ray_ids[i] at d_accel_keys[i], 0 once the
+ * ray has no surface left (KCIntersectBaseBVH, GPUAcceleratorBVHKC.cuh:
+ * 513-652). */
+int mrb_base_accel_create(mrb_system* sys, mrb_base_accel** out);
+void mrb_base_accel_destroy(mrb_base_accel* b);
+int mrb_base_accel_construct(mrb_base_accel* b, const float* aabbs, const uint32_t* accel_keys,
+                             uint32_t count);
+int mrb_base_accel_get_ready(mrb_base_accel* b, uint32_t ray_count, void* stream);
+int mrb_base_accel_hit(const mrb_base_accel* b, uint32_t* d_accel_keys, const void* d_rays,
+                       const uint32_t* d_ray_ids, uint32_t ray_count, void* stream);
+/* SceneExtents. */
+int mrb_base_accel_extents(const mrb_base_accel* b, float* aabb);
+
 /* ---- wavefront pool: continuous batching of render jobs ----------------
  * (no counterpart in the reference: MRay renders one scene per tracer.)
  * Jobs of different scenes, resolutions and sample counts share one

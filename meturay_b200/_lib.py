@@ -156,6 +156,25 @@ def _load() -> C.CDLL:
         "mrb_write_pfm": (i32, [C.c_char_p, vp, u32, u32, u32]),
         "mrb_read_image": (i32, [C.c_char_p, vp, sz, C.POINTER(u32), C.POINTER(u32),
                                  C.POINTER(u32)]),
+        "mrb_accel_group_create": (i32, [vp, vp, u32, vp, vp, vp, vp, vp, u32, vp, u32,
+                                         C.POINTER(vp)]),
+        "mrb_accel_group_destroy": (None, [vp]),
+        "mrb_accel_group_attach_transforms": (i32, [vp, vp, u32, u32]),
+        "mrb_accel_group_construct": (i32, [vp, vp]),
+        "mrb_accel_group_hit": (i32, [vp, vp, vp, vp, vp, u32, vp, vp, vp, u32, vp]),
+        "mrb_accel_group_aabbs": (i32, [vp, vp, u32]),
+        "mrb_accel_group_primitive_count": (u64, [vp]),
+        "mrb_accel_group_accelerator_count": (u32, [vp]),
+        "mrb_accel_group_total_area": (i32, [vp, C.POINTER(C.c_float), vp]),
+        "mrb_accel_group_sample_points": (i32, [vp, vp, vp, u32, u64, vp]),
+        "mrb_accel_group_voxel_counts": (i32, [vp, vp, u32, vp, vp]),
+        "mrb_accel_group_voxelize": (i32, [vp, vp, vp, vp, vp, vp, u32, u32, vp, vp]),
+        "mrb_base_accel_create": (i32, [vp, C.POINTER(vp)]),
+        "mrb_base_accel_destroy": (None, [vp]),
+        "mrb_base_accel_construct": (i32, [vp, vp, vp, u32]),
+        "mrb_base_accel_get_ready": (i32, [vp, u32, vp]),
+        "mrb_base_accel_hit": (i32, [vp, vp, vp, vp, u32, vp]),
+        "mrb_base_accel_extents": (i32, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -134,6 +134,18 @@ __device__ __forceinline__ V3 vmax0(V3 v) { return {fmaxf(v.x, 0.0f), fmaxf(v.y,
 __device__ __forceinline__ V3 vsqrt(V3 v) { return {sqrtf(v.x), sqrtf(v.y), sqrtf(v.z)}; }
 __device__ __forceinline__ V3 vdiv(V3 a, V3 b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
 __device__ __forceinline__ V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+// Row-major 3x4 affine matrix m applied to a point (w = 1) and a direction
+// (w = 0), each row summed left to right: Matrix4x4 * Vector4 of
+// Ray::Transform (RayLib/Ray.hpp:459-465) without the constant fourth row.
+__device__ __forceinline__ V3 xform_point(const float* m, V3 p) {
+    return {((m[0] * p.x + m[1] * p.y) + m[2] * p.z) + m[3],
+            ((m[4] * p.x + m[5] * p.y) + m[6] * p.z) + m[7],
+            ((m[8] * p.x + m[9] * p.y) + m[10] * p.z) + m[11]};
+}
+__device__ __forceinline__ V3 xform_dir(const float* m, V3 d) {
+    return {(m[0] * d.x + m[1] * d.y) + m[2] * d.z, (m[4] * d.x + m[5] * d.y) + m[6] * d.z,
+            (m[8] * d.x + m[9] * d.y) + m[10] * d.z};
+}
 
 __device__ __forceinline__ Q4 qmul(Q4 a, Q4 b) {  // Quaternion.hpp:76-89
     return {a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z,

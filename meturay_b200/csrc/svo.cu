@@ -256,6 +256,68 @@ __global__ void __launch_bounds__(128) k_row_voxelize(SvoBuildIn in, SvoParams P
     }
 }
 
+// EachPrimVoxelCount / VoxelizeSurfaces of an accelerator group
+// (GPUAcceleratorI.h:113-133; KCGetVoxelCount / KCVoxelizePrims,
+// GPUAcceleratorCommonKC.cuh:439-542): one thread per primitive, its
+// vertices taken to world space by its surface's local-to-world matrix.
+__device__ __forceinline__ void prim_world_pos(const PrimVoxIn& in, uint32_t t, V3& a, V3& b,
+                                               V3& c) {
+    const uint32_t i0 = in.idx[3 * size_t(t)], i1 = in.idx[3 * size_t(t) + 1],
+                   i2 = in.idx[3 * size_t(t) + 2];
+    a = ld3(in.pos + 3 * size_t(i0));
+    b = ld3(in.pos + 3 * size_t(i1));
+    c = ld3(in.pos + 3 * size_t(i2));
+    if (in.triTransform) {
+        const float* m = in.transforms + 12 * size_t(in.triTransform[t]);
+        a = xform_point(m, a);
+        b = xform_point(m, b);
+        c = xform_point(m, c);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_prim_voxel_count(PrimVoxIn in, SvoParams P,
+                                                          unsigned long long* counts) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < in.triCount;
+         t += gridDim.x * blockDim.x) {
+        V3 a, b, c;
+        prim_world_pos(in, t, a, b, c);
+        const TriRaster R = tri_setup(P, a, b, c);
+        unsigned long long n = 0;
+        if (tri_rows(R))
+            for (int y = R.y0; y < R.y1; y++) n += tri_row(P, R, y, nullptr, nullptr, 0);
+        counts[t] = n;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_prim_voxelize(PrimVoxIn in, SvoParams P,
+                                                       const unsigned long long* __restrict__ offs,
+                                                       uint64_t* codes, uint32_t* normals,
+                                                       uint32_t* lightKeys,
+                                                       const uint32_t* __restrict__ sortedLights,
+                                                       uint32_t lightCount) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < in.triCount;
+         t += gridDim.x * blockDim.x) {
+        V3 a, b, c;
+        prim_world_pos(in, t, a, b, c);
+        const TriRaster R = tri_setup(P, a, b, c);
+        const unsigned long long o = offs[t], cnt = offs[t + 1] - o;
+        unsigned long long w = 0;
+        if (tri_rows(R))
+            for (int y = R.y0; y < R.y1 && w < cnt; y++)
+                w += tri_row(P, R, y, codes + o + w, normals + o + w, uint32_t(cnt - w));
+        // the primitive's work key if it is one of the (sorted) light keys
+        const uint32_t key = in.key[t];
+        uint32_t lo = 0, hi = lightCount;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sortedLights[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        const uint32_t lk = (lo < lightCount && sortedLights[lo] == key) ? key : 0u;
+        for (unsigned long long i = 0; i < cnt; i++) lightKeys[o + i] = lk;
+    }
+}
+
 __global__ void k_iota(uint32_t* v, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         v[i] = i;
@@ -599,6 +661,26 @@ void svo_free(SvoResult& r) {
     cudaFree(r.nodeBin);
     cudaFree(r.dLevelOffsets);
     r = SvoResult{};
+}
+
+int prim_voxel_count(const PrimVoxIn& in, const SvoParams& P, unsigned long long* counts,
+                     cudaStream_t st) {
+    if (in.triCount == 0) return 0;
+    const uint32_t blocks = std::min((in.triCount + 127) / 128, 148u * 16u);
+    k_prim_voxel_count<<<blocks, 128, 0, st>>>(in, P, counts);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int prim_voxelize(const PrimVoxIn& in, const SvoParams& P, const unsigned long long* offsets,
+                  uint64_t* codes, uint32_t* normals, uint32_t* lightKeys,
+                  const uint32_t* sortedLights, uint32_t lightCount, cudaStream_t st) {
+    if (in.triCount == 0) return 0;
+    const uint32_t blocks = std::min((in.triCount + 127) / 128, 148u * 16u);
+    k_prim_voxelize<<<blocks, 128, 0, st>>>(in, P, offsets, codes, normals, lightKeys,
+                                            sortedLights, lightCount);
+    MRB_CUDA(cudaGetLastError());
+    return 0;
 }
 
 }  // namespace mrb

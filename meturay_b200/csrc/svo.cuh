@@ -45,6 +45,30 @@ struct SvoResult {
     uint32_t* dLevelOffsets = nullptr;     // device copy of levelOffsets
 };
 
+// Primitives of an accelerator group for EachPrimVoxelCount /
+// VoxelizeSurfaces: triangle t's vertices go to world space through
+// transforms + 12 * triTransform[t] (row-major 3x4 local-to-world; no
+// transform when triTransform is null).
+struct PrimVoxIn {
+    uint32_t triCount;
+    const float* pos;
+    const uint32_t* idx;
+    const uint32_t* key;
+    const uint32_t* triTransform;
+    const float* transforms;
+};
+// Per-primitive voxel counts of the conservative raster (the octree box and
+// leaf resolution in P).
+int prim_voxel_count(const PrimVoxIn& in, const SvoParams& P, unsigned long long* counts,
+                     cudaStream_t st);
+// Voxel Morton codes and packed spherical normals of each primitive at
+// offsets[t] .. offsets[t + 1] (exclusive scan of the counts, triCount + 1
+// entries); light keys: the primitive's work key when it is one of the
+// sorted light keys, else 0.
+int prim_voxelize(const PrimVoxIn& in, const SvoParams& P, const unsigned long long* offsets,
+                  uint64_t* codes, uint32_t* normals, uint32_t* lightKeys,
+                  const uint32_t* sortedLights, uint32_t lightCount, cudaStream_t st);
+
 SvoParams svo_params(const float extent[6], uint32_t res);
 int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStream_t st);
 void svo_free(SvoResult& r);

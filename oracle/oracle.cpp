@@ -3187,6 +3187,179 @@ void oracle_camera_img_coords(const oracle_options* opt, float* out) {
         out[2 * sid + 1] = ly * static_cast<float>(opt->height);
     }
 }
+// ---- accelerator group of transformed surfaces (GPUAccBVHGroup::Hit,
+// GPUAcceleratorBVHKC.cuh:229-346: the ray moved to the surface's local
+// space by the inverse of its Matrix4x4 (Ray::Transform, RayLib/Ray.hpp:
+// 459-465), traversed there; t is shared because the direction is not
+// renormalised)
+struct oracle_group {
+    std::vector<float> pos;
+    std::vector<uint32_t> idx, key;
+    std::vector<uint8_t> cull;
+    std::vector<uint32_t> begin, end, xf;
+    std::vector<float> l2w, w2l;
+    std::vector<oracle_scene> sub;
+    std::vector<oracle_bvh*> bvh;
+    ~oracle_group() {
+        for (oracle_bvh* b : bvh) oracle_bvh_destroy(b);
+    }
+};
+
+namespace {
+// Inverse of a row-major 3x4 affine matrix in double, each entry rounded
+// once (the same steps as the device library's host side).
+bool affine_inverse_f(const float* m, float* out) {
+    double a[3][3], t[3];
+    for (int r = 0; r < 3; r++) {
+        for (int c = 0; c < 3; c++) a[r][c] = m[4 * r + c];
+        t[r] = m[4 * r + 3];
+    }
+    const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+    const double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+    const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+    const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+    double inv[3][3];
+    inv[0][0] = c00 / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = c01 / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = c02 / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    for (int r = 0; r < 3; r++) {
+        double tr = 0.0;
+        for (int c = 0; c < 3; c++) {
+            out[4 * r + c] = static_cast<float>(inv[r][c]);
+            tr -= inv[r][c] * t[c];
+        }
+        out[4 * r + 3] = static_cast<float>(tr);
+    }
+    return true;
+}
+inline V3<float> xf_point(const float* m, V3<float> p) {
+    return {((m[0] * p.x + m[1] * p.y) + m[2] * p.z) + m[3],
+            ((m[4] * p.x + m[5] * p.y) + m[6] * p.z) + m[7],
+            ((m[8] * p.x + m[9] * p.y) + m[10] * p.z) + m[11]};
+}
+inline V3<float> xf_dir(const float* m, V3<float> d) {
+    return {(m[0] * d.x + m[1] * d.y) + m[2] * d.z, (m[4] * d.x + m[5] * d.y) + m[6] * d.z,
+            (m[8] * d.x + m[9] * d.y) + m[10] * d.z};
+}
+}  // namespace
+
+extern "C" oracle_group* oracle_group_create(const float* pos, uint32_t V, const uint32_t* idx,
+                                             const uint32_t* key, const uint8_t* cull, uint32_t T,
+                                             const uint32_t* surfaces, uint32_t S,
+                                             const float* l2w, uint32_t nT, int* status) {
+    *status = 0;
+    oracle_group* g = new oracle_group();
+    g->pos.assign(pos, pos + 3 * size_t(V));
+    g->idx.assign(idx, idx + 3 * size_t(T));
+    g->key.assign(key, key + T);
+    g->cull.assign(T, 0);
+    if (cull) g->cull.assign(cull, cull + T);
+    g->l2w.assign(l2w, l2w + 12 * size_t(nT));
+    g->w2l.assign(12 * size_t(nT), 0.0f);
+    for (uint32_t i = 0; i < nT; i++)
+        if (!affine_inverse_f(&g->l2w[12 * size_t(i)], &g->w2l[12 * size_t(i)])) *status = 1;
+    g->sub.resize(S);
+    for (uint32_t si = 0; si < S; si++) {
+        const uint32_t b = surfaces[3 * si], e = surfaces[3 * si + 1];
+        g->begin.push_back(b);
+        g->end.push_back(e);
+        g->xf.push_back(surfaces[3 * si + 2]);
+        oracle_scene sc{};
+        sc.vertex_count = V;
+        sc.tri_count = e - b;
+        sc.pos = g->pos.data();
+        sc.idx = g->idx.data() + 3 * size_t(b);
+        sc.tri_key = g->key.data() + b;
+        sc.tri_cull = g->cull.data() + b;
+        g->sub[si] = sc;
+        int st = 0;
+        g->bvh.push_back(oracle_bvh_create(&g->sub[si], &st));
+        if (st > 1) *status = 2;
+    }
+    return g;
+}
+
+extern "C" void oracle_group_destroy(oracle_group* g) { delete g; }
+
+// Closest hit over every surface (surfaces in index order; a later surface
+// replaces the hit only when strictly closer).  rays: origin, tMin,
+// direction, tMax (8 floats).  Outputs per ray: material key, transform id,
+// primitive id (group index, ~0 on a miss), t (tMax when missed), bary.
+extern "C" void oracle_group_trace(const oracle_group* g, const float* rays, uint32_t n,
+                                   uint32_t* key, uint32_t* tid, uint64_t* prim, float* tOut,
+                                   float* bary) {
+    parallel_for(n, 0, [&](uint32_t b0, uint32_t b1) {
+        for (uint32_t i = b0; i < b1; i++) {
+            const float* r = rays + 8 * size_t(i);
+            float closest = r[7];
+            key[i] = 0;
+            tid[i] = 0;
+            prim[i] = ~0ull;
+            bary[2 * i] = bary[2 * i + 1] = 0.0f;
+            for (size_t si = 0; si < g->sub.size(); si++) {
+                const float* m = &g->w2l[12 * size_t(g->xf[si])];
+                const V3<float> o = xf_point(m, V3<float>(r[0], r[1], r[2]));
+                const V3<float> d = xf_dir(m, V3<float>(r[4], r[5], r[6]));
+                const Hit<float> h = trace_one<float>(&g->sub[si], g->bvh[si], o, d, r[3], closest);
+                if (h.prim != kInvalid && h.t < closest) {
+                    closest = h.t;
+                    key[i] = h.key;
+                    tid[i] = g->xf[si];
+                    prim[i] = uint64_t(g->begin[si]) + h.prim;
+                    bary[2 * i] = h.b0;
+                    bary[2 * i + 1] = h.b1;
+                }
+            }
+            tOut[i] = closest;
+        }
+    });
+}
+
+// World AABB of each surface: the local box of its triangles (the LBVH's
+// extent) with the eight corners transformed.
+extern "C" void oracle_group_aabbs(const oracle_group* g, float* out) {
+    for (size_t si = 0; si < g->sub.size(); si++) {
+        float lo[3] = {M<float>::Max, M<float>::Max, M<float>::Max};
+        float hi[3] = {-M<float>::Max, -M<float>::Max, -M<float>::Max};
+        for (uint32_t t = g->begin[si]; t < g->end[si]; t++)
+            for (int k = 0; k < 3; k++)
+                for (int c = 0; c < 3; c++) {
+                    const float v = g->pos[3 * size_t(g->idx[3 * size_t(t) + k]) + c];
+                    lo[c] = std::fmin(lo[c], v);
+                    hi[c] = std::fmax(hi[c], v);
+                }
+        const float* m = &g->l2w[12 * size_t(g->xf[si])];
+        float wl[3] = {M<float>::Max, M<float>::Max, M<float>::Max};
+        float wh[3] = {-M<float>::Max, -M<float>::Max, -M<float>::Max};
+        for (int k = 0; k < 8; k++) {
+            const V3<float> w = xf_point(m, V3<float>((k & 1) ? hi[0] : lo[0],
+                                                      (k & 2) ? hi[1] : lo[1],
+                                                      (k & 4) ? hi[2] : lo[2]));
+            const float wc[3] = {w.x, w.y, w.z};
+            for (int c = 0; c < 3; c++) {
+                wl[c] = std::fmin(wl[c], wc[c]);
+                wh[c] = std::fmax(wh[c], wc[c]);
+            }
+        }
+        for (int c = 0; c < 3; c++) {
+            out[6 * si + c] = wl[c];
+            out[6 * si + 3 + c] = wh[c];
+        }
+    }
+}
+
+// Row-major 3x4 inverse used by the group (for the tests' own checks).
+extern "C" int oracle_affine_inverse(const float* m, float* out) {
+    return affine_inverse_f(m, out) ? 0 : -1;
+}
+
 uint64_t oracle_render_f64(const oracle_scene* s, const oracle_bvh* b, const oracle_camera* cam,
                            const oracle_options* opt, double* out) {
     return render<double>(s, b, cam, opt, out);

@@ -631,3 +631,46 @@ def svo_dump_bytes(ex: dict, node_bin16=None, leaf_bin16=None) -> bytes:
              irr.astype(np.float32), ex["leaf_cnt"].astype(np.uint32), halves(ex["leaf_avg"]),
              ex["leaf_normals"].astype(np.uint32), np.zeros(U, np.uint8)]
     return b"".join(np.ascontiguousarray(p).tobytes() for p in parts)
+
+
+class OracleGroup:
+    """The oracle's accelerator group: one LBVH per surface in local space
+    under a local-to-world 3x4 matrix, closest hit over the surfaces."""
+
+    def __init__(self, positions, indices, keys, surfaces, local_to_world, cull=None):
+        self._pos = np.ascontiguousarray(positions, np.float32)
+        self._idx = np.ascontiguousarray(indices, np.uint32)
+        self._key = np.ascontiguousarray(keys, np.uint32)
+        self._cull = None if cull is None else np.ascontiguousarray(cull, np.uint8)
+        self._surf = np.ascontiguousarray(surfaces, np.uint32).reshape(-1, 3)
+        self._l2w = np.ascontiguousarray(local_to_world, np.float32).reshape(-1, 12)
+        lib.oracle_group_create.restype = C.c_void_p
+        st = C.c_int(0)
+        self.h = C.c_void_p(lib.oracle_group_create(
+            _p(self._pos), C.c_uint32(self._pos.shape[0]), _p(self._idx), _p(self._key),
+            _p(self._cull), C.c_uint32(self._idx.shape[0]), _p(self._surf),
+            C.c_uint32(self._surf.shape[0]), _p(self._l2w), C.c_uint32(self._l2w.shape[0]),
+            C.byref(st)))
+        self.status = st.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.oracle_group_destroy(self.h)
+            self.h = None
+
+    def trace(self, rays: np.ndarray) -> dict:
+        """rays: (n, 8) origin, tMin, direction, tMax."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        out = {"key": np.zeros(n, np.uint32), "transform": np.zeros(n, np.uint32),
+               "prim": np.zeros(n, np.uint64), "t": np.zeros(n, np.float32),
+               "bary": np.zeros((n, 2), np.float32)}
+        lib.oracle_group_trace(self.h, _p(rays), C.c_uint32(n), _p(out["key"]),
+                               _p(out["transform"]), _p(out["prim"]), _p(out["t"]),
+                               _p(out["bary"]))
+        return out
+
+    def aabbs(self) -> np.ndarray:
+        out = np.zeros((self._surf.shape[0], 6), np.float32)
+        lib.oracle_group_aabbs(self.h, _p(out))
+        return out

@@ -77,3 +77,34 @@ def test_scene_generators_deterministic():
     kinds = {m["type"] for m in k.materials}
     assert kinds == {1, 2, 3, 4}
     assert (k.positions.min(0) > -20).all() and (k.positions.max(0) < 120).all()
+
+
+def test_mray_binding_compiles_against_the_reference_headers(tmp_path):
+    """include/mray/GPUAccLBVHGroup.cuh implements MRay's GPUAcceleratorGroupI
+    and GPUBaseAcceleratorI over the C ABI.  Compiled here with nvcc against
+    the MRay sources the checker was built from (oracle/_ref/ref_root.txt,
+    written by `make -C oracle ref`), with the flags MRay's TracerCUDA
+    sources build with; both classes are instantiated so that every virtual
+    member is compiled.  Compile only: nothing is linked into the library."""
+    import subprocess
+    from pathlib import Path
+    root_file = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "ref_root.txt"
+    if not root_file.exists():
+        pytest.skip("the MRay sources are not present (checker built without them)")
+    ref = Path(root_file.read_text().strip())
+    if not (ref / "Source" / "TracerCUDA" / "GPUAcceleratorI.h").exists():
+        pytest.skip("the MRay sources are not present here")
+    inc = Path(__file__).resolve().parent.parent / "include"
+    tu = tmp_path / "binding.cu"
+    tu.write_text('#include "mray/GPUAccLBVHGroup.cuh"\n'
+                  "GPUAcceleratorGroupI* make_group(const GPUPrimitiveGroupI& p) {\n"
+                  "    return new mrb_mray::GPUAccLBVHGroup(p);\n}\n"
+                  "GPUBaseAcceleratorI* make_base() { return new mrb_mray::GPUBaseAccLBVH(); }\n")
+    cmd = ["/usr/local/cuda/bin/nvcc", "-std=c++17", "-DMETU_CUDA", "-DFMT_HEADER_ONLY",
+           "--expt-relaxed-constexpr", "--extended-lambda", "-rdc=true",
+           "-gencode", "arch=compute_100a,code=sm_100a", "-I", str(ref / "Source"),
+           "-I", str(ref / "Lib" / "Include"), "-I", str(inc), "-c", str(tu),
+           "-o", str(tmp_path / "binding.o")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert (tmp_path / "binding.o").stat().st_size > 0
