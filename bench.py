@@ -504,7 +504,7 @@ def run_batching(args, m, system, torch) -> dict:
     # of 2^16 .. 2^22 rays (two rays per camera sample)
     caps = [1 << k for k in (15, 17, 19, 21)]
     tune = autotune(system, [dataclasses.replace(j, frames=1) for j in jobs[::4]],
-                    capacities=caps, blocks=(64, 128, 256), stacks=(64, 128),
+                    capacities=caps, blocks=(64, 128, 256), stacks=(64, 128, 0),
                     max_depth=BATCH["max_depth"], iterations=3)
     feasible = [r for r in tune["table"] if r["capacity"] >= largest]
     best = max(feasible, key=lambda r: r["mrays_s"])
@@ -837,7 +837,8 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=64,
                     help="jobs in the serving run (Poisson arrivals at 200/s)")
     ap.add_argument("--pool-block", type=int, default=0)
-    ap.add_argument("--pool-stack", type=int, default=128)
+    ap.add_argument("--pool-stack", type=int, default=128,
+                    help="traversal stack of the pool: 64 or 128 (sorted order) or 0 (octant order)")
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the learned-guiding equal-time MSE comparison")
     ap.add_argument("--learned-budget-ms", type=float, default=1000.0)

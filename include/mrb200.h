@@ -142,6 +142,30 @@ int mrb_accel_hit(const mrb_scene* scene, const float* d_ray_o, const float* d_r
 int mrb_accel_set_traversal(mrb_scene* scene, int mode);
 /* info[4]: triangles, binary inner nodes, wide nodes, traversal mode. */
 int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
+/* Child order of the 8-wide traversal: 0 exact front-to-back (entry
+ * distances sorted, one stack entry per pushed child), 1 octant order (the
+ * collapse places children by the octant of their centroid; one stack entry
+ * per node group), 2 (default) the faster of the two: first on 65,536
+ * seeded rays over the scene box, timed at mrb_accel_construct (or at once
+ * when the accelerator is built), then on a tracer's own rays: the frame
+ * that mrb_tracer_render_frame runs before it captures its graph traces
+ * every depth's rays in both orders and keeps the faster sum (once per
+ * tracer).  Closest hits are the same either way, up to the choice among
+ * triangles at the same distance. */
+int mrb_accel_set_wide_order(mrb_scene* s, int order);
+/* The order in use (0 or 1) and the last measured times per order (ms:
+ * the probe's, or the summed per-depth traces of a tracer's frame; 0 when
+ * the order was set rather than measured). */
+int mrb_accel_wide_order(const mrb_scene* s, int* order, float* probe_ms2);
+/* The tree the 8-wide traversal layout is collapsed from (before
+ * mrb_accel_construct): 0 the LBVH, 1 a PLOC tree (parallel locally-ordered
+ * clustering by merged-box area) over the LBVH's Morton-sorted leaves, 2
+ * (default) whichever of the two has the smaller sum of inner-box surface
+ * areas.  The LBVH arrays and the binary traversal are the same either way. */
+int mrb_accel_set_wide_tree(mrb_scene* s, int tree);
+/* info[2]: the source used (0 LBVH, 1 PLOC), PLOC clustering steps;
+ * areas[2] (may be NULL): inner half-area sums of the LBVH and PLOC trees. */
+int mrb_accel_info_ext(const mrb_scene* s, uint32_t* info, double* areas);
 
 /* ---- sparse voxel octree of the scene (the WFPG radiance cache):
  * AnisoSVOctreeCPU::Constrcut (AnisoSVO.cu:657-1188) with the accelerator
@@ -496,6 +520,8 @@ int mrb_pool_create(mrb_system* sys, uint32_t capacity, uint32_t max_depth, size
 void mrb_pool_destroy(mrb_pool* pool);
 /* Traversal launch shape: block 64/128/256 threads, stack 64/128 entries. */
 int mrb_pool_set_launch(mrb_pool* pool, int trace_block, int trace_stack);
+/* trace_stack 0 selects the 8-wide traversal's octant child order (node
+ * groups on the stack) instead of the sorted order's 64 or 128 entries. */
 /* Queue a job (the scene's accelerator must be built; the scene must stay
  * alive until the job is done).  One frame must fit the capacity. */
 int mrb_pool_submit(mrb_pool* pool, mrb_scene* scene, const mrb_pool_job* job, uint64_t* job_id);

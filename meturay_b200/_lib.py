@@ -67,6 +67,10 @@ def _load() -> C.CDLL:
         "mrb_accel_hit": (i32, [vp, vp, vp, u32, vp, vp, vp, vp, vp]),
         "mrb_accel_set_traversal": (i32, [vp, i32]),
         "mrb_accel_info": (i32, [vp, vp]),
+        "mrb_accel_set_wide_tree": (i32, [vp, i32]),
+        "mrb_accel_set_wide_order": (i32, [vp, i32]),
+        "mrb_accel_wide_order": (i32, [vp, C.POINTER(C.c_int), vp]),
+        "mrb_accel_info_ext": (i32, [vp, vp, vp]),
         "mrb_svo_build": (i32, [vp, u32, vp]),
         "mrb_svo_info": (i32, [vp, vp, vp]),
         "mrb_svo_export": (i32, [vp, vp, vp, vp, vp, vp, vp]),

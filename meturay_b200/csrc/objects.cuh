@@ -97,10 +97,18 @@ struct mrb_scene {
     ~mrb_scene() {
         if (svoBuilt) svo_free(svo);
     }
-    // 8-wide quantised traversal layout derived from the LBVH
+    // 8-wide quantised traversal layout, collapsed from the PLOC tree built
+    // over the LBVH's sorted leaves (wideTree 1) or from the LBVH itself (0)
     DBuf wNodes, wTv0, wTe0, wTe1, wScratch;
     uint32_t wNodeCount = 0;
     int traversal = 1;  // 0: binary LBVH nodes, 1: 8-wide nodes
+    int wideTree = 2;        // 0 LBVH, 1 PLOC, 2 the one with less inner-box area
+    int wideOrderMode = 2;   // 0 sorted, 1 octant, 2 the faster as timed
+    int wideOrder = 0;       // in use
+    float wideOrderMs[2] = {0.0f, 0.0f};
+    int wideTreeUsed = 0;
+    uint32_t plocSteps = 0;
+    double areaLbvh = 0.0, areaPloc = 0.0;  // sums of inner half areas
     WideAccelDev wide() const {
         WideAccelDev a{};
         a.nodes = wNodes.as<WideNode>();

@@ -257,8 +257,8 @@ void mrb_pool_destroy(mrb_pool* p) { delete p; }
 
 int mrb_pool_set_launch(mrb_pool* p, int trace_block, int trace_stack) {
     if (!p || (trace_block != 64 && trace_block != 128 && trace_block != 256) ||
-        (trace_stack != 64 && trace_stack != 128)) {
-        mrb::set_error("pool: traversal block 64/128/256 and stack 64/128");
+        (trace_stack != 0 && trace_stack != 64 && trace_stack != 128)) {
+        mrb::set_error("pool: traversal block 64/128/256 and stack 64/128 (or 0: octant order)");
         return MRB_E_ARG;
     }
     p->block = trace_block;

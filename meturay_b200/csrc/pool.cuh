@@ -48,7 +48,8 @@ int shade_jobs(const JobDev* jobs, const float4* rayO, const float4* rayD, const
                uint32_t maxCount, float4* samples, float4* outO, float4* outD, RayAux* outAux,
                uint32_t* outCount, cudaStream_t stream);
 // Closest hit of rays of many scenes: the accelerator of each ray is its
-// job's.  block: 64, 128 or 256 threads; stack: 64 or 128 entries.
+// job's.  block: 64, 128 or 256 threads; stack: 64 or 128 entries of the
+// sorted child order, or 0 for the octant order's node groups.
 int trace_closest_wide_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
                             const float4* rayD, const uint32_t* dCount, uint32_t maxCount,
                             const HitOut& out, uint32_t* errorFlag, int block, int stack,

@@ -31,6 +31,7 @@
 #include "io.cuh"
 #include "learned.cuh"
 #include "objects.cuh"
+#include "ploc.cuh"
 
 namespace mrb {
 
@@ -239,6 +240,10 @@ struct mrb_tracer {
     // graph
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
+    // 8-wide child order chosen on this tracer's own rays: the eager frame
+    // before a capture times both orders at every depth
+    bool orderTune = false, orderTuned = false;
+    float orderMs[2] = {0.0f, 0.0f};
     ~mrb_tracer() {
         if (trainStream) cudaStreamSynchronize(trainStream);
         if (copyStream) cudaStreamSynchronize(copyStream);
@@ -575,7 +580,8 @@ int trace_dispatch(const mrb_scene* sc, const float4* rayO, const float4* rayD,
                    const uint32_t* dCount, uint32_t maxCount, const HitOut& ho, uint32_t* err,
                    cudaStream_t st, unsigned long long* counters = nullptr) {
     if (sc->traversal == 1 && sc->T > 1)
-        return trace_closest_wide(sc->wide(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
+        return trace_closest_wide(sc->wide(), rayO, rayD, dCount, maxCount, ho, err, st, counters,
+                                  sc->wideOrder);
     return trace_closest(sc->accel(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
 }
 
@@ -602,6 +608,39 @@ struct StageTimer {
     float ms[kStageCount] = {};
 };
 
+// Both 8-wide child orders traced over the rays of buffer `cur` (twice
+// each, the faster pass kept: the first launch of a kernel may load its
+// module), added to t->orderMs.  Every pass writes the same closest hits but
+// for ties; the frame's own trace follows and overwrites them.
+int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho) {
+    const mrb_scene* sc = t->scene;
+    cudaEvent_t e[2];
+    MRB_CUDA(cudaEventCreate(&e[0]));
+    MRB_CUDA(cudaEventCreate(&e[1]));
+    float best[2] = {1e30f, 1e30f};
+    int r = 0;
+    for (int rep = 0; rep < 2 && !r; rep++)
+        for (int o = 0; o < 2 && !r; o++) {
+            cudaEventRecord(e[0], t->stream);
+            r = trace_closest_wide(sc->wide(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+                                   t->count.as<uint32_t>() + cur, t->maxRays, ho,
+                                   t->errorFlags.as<uint32_t>(), t->stream, nullptr, o);
+            cudaEventRecord(e[1], t->stream);
+            if (!r && cudaEventSynchronize(e[1]) == cudaSuccess) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e[0], e[1]);
+                best[o] = std::min(best[o], ms);
+            }
+        }
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    if (r) return r;
+    MRB_CUDA(cudaGetLastError());
+    t->orderMs[0] += best[0];
+    t->orderMs[1] += best[1];
+    return 0;
+}
+
 // One Render() step: HitRays -> PartitionRaysWRTWork -> WorkRays
 // (PathTracer.cu:144-291) for the rays of buffer `cur`.  With a timer the
 // stages are bracketed by events and the traversal is repeated once in its
@@ -626,6 +665,7 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
         tm->ms[stage] += ms;
         return 0;
     };
+    if (t->orderTune && (r = time_wide_orders(t, cur, ho))) return r;
     if (mark(0)) return MRB_E_CUDA;
     if ((r = trace_dispatch(sc, t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(), cnt + cur,
                             t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
@@ -1134,10 +1174,44 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
                        s->aInner.as<float>(), s->aTriAabb.as<float>(), s->aSorted.as<uint32_t>(),
                        s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>(),
                        s->dCull.as<uint8_t>()};
+        // the PLOC tree over the same sorted leaves: tighter upper boxes than
+        // the Morton splits give the collapse better nodes to start from
+        DBuf pLeft, pRight, pInner, pRoot, pScratch;
+        s->wideTreeUsed = 0;
+        if (s->wideTree != 0) {
+            if ((r = pLeft.alloc((n - 1) * 4)) || (r = pRight.alloc((n - 1) * 4)) ||
+                (r = pInner.alloc((n - 1) * 24)) || (r = pRoot.alloc(4)) ||
+                (r = pScratch.alloc(ploc_scratch_bytes(n))))
+                return r;
+            PlocIn pi{n, s->aTriAabb.as<float>(), s->aSorted.as<uint32_t>()};
+            PlocOut po{pLeft.as<uint32_t>(), pRight.as<uint32_t>(), pInner.as<float>(),
+                       pRoot.as<uint32_t>()};
+            if ((r = ploc_build(pi, po, pScratch.p, &s->plocSteps, st))) return r;
+            double* d8 = static_cast<double*>(pScratch.p);
+            if ((r = inner_area_sum(s->aInner.as<float>(), n - 1, d8, &s->areaLbvh, st)) ||
+                (r = inner_area_sum(pInner.as<float>(), n - 1, d8, &s->areaPloc, st)))
+                return r;
+            pScratch.release();
+            if (s->wideTree == 1 || s->areaPloc < s->areaLbvh) {
+                s->wideTreeUsed = 1;
+                wi.root = pRoot.as<uint32_t>();
+                wi.left = pLeft.as<uint32_t>();
+                wi.right = pRight.as<uint32_t>();
+                wi.inner = pInner.as<float>();
+            }
+        }
         if ((r = wide_build(wi, s->wNodes.as<WideNode>(), s->wTv0.as<float4>(), s->wTe0.as<float4>(),
                             s->wTe1.as<float4>(), s->wScratch.p, &s->wNodeCount, st)))
             return r;
         s->wScratch.release();
+        s->wideOrderMs[0] = s->wideOrderMs[1] = 0.0f;
+        if (s->wideOrderMode == 2) {
+            if ((r = wide_order_autotune(s->wide(), s->aExtent.as<float>(), st, &s->wideOrder,
+                                         s->wideOrderMs)))
+                return r;
+        } else {
+            s->wideOrder = s->wideOrderMode;
+        }
     }
     uint32_t root = 0, err = 0;
     MRB_CUDA(cudaMemcpyAsync(&root, s->aRoot.p, 4, cudaMemcpyDeviceToHost, st));
@@ -1261,12 +1335,62 @@ int mrb_accel_set_traversal(mrb_scene* s, int mode) {
     return 0;
 }
 
+int mrb_accel_set_wide_order(mrb_scene* s, int order) {
+    if (!s || order < 0 || order > 2) {
+        set_error("wide order must be 0 (sorted), 1 (octant) or 2 (the faster on probe rays)");
+        return MRB_E_ARG;
+    }
+    s->wideOrderMode = order;
+    if (!s->built || s->T < 2) return 0;
+    if (set_device(s->sys)) return MRB_E_CUDA;
+    s->wideOrderMs[0] = s->wideOrderMs[1] = 0.0f;
+    if (order == 2)
+        return wide_order_autotune(s->wide(), s->aExtent.as<float>(), nullptr, &s->wideOrder,
+                                   s->wideOrderMs);
+    s->wideOrder = order;
+    return 0;
+}
+
+int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms2) {
+    if (!s || !order) return MRB_E_ARG;
+    *order = s->wideOrder;
+    if (ms2) {
+        ms2[0] = s->wideOrderMs[0];
+        ms2[1] = s->wideOrderMs[1];
+    }
+    return 0;
+}
+
+int mrb_accel_set_wide_tree(mrb_scene* s, int tree) {
+    if (!s || tree < 0 || tree > 2) {
+        set_error("wide tree must be 0 (LBVH), 1 (PLOC) or 2 (the one with less box area)");
+        return MRB_E_ARG;
+    }
+    if (s->built) {
+        set_error("wide tree: set it before mrb_accel_construct");
+        return MRB_E_STATE;
+    }
+    s->wideTree = tree;
+    return 0;
+}
+
 int mrb_accel_info(const mrb_scene* s, uint32_t* info) {
     if (!s || !info) return MRB_E_ARG;
     info[0] = s->T;
     info[1] = s->T > 1 ? s->T - 1 : 0;
     info[2] = s->wNodeCount;
     info[3] = static_cast<uint32_t>(s->traversal);
+    return 0;
+}
+
+int mrb_accel_info_ext(const mrb_scene* s, uint32_t* info, double* areas) {
+    if (!s || !info) return MRB_E_ARG;
+    info[0] = static_cast<uint32_t>(s->wideTreeUsed);
+    info[1] = s->plocSteps;
+    if (areas) {
+        areas[0] = s->areaLbvh;
+        areas[1] = s->areaPloc;
+    }
     return 0;
 }
 
@@ -1577,6 +1701,11 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
                                  cudaMemcpyDeviceToDevice, t->stream));
         MRB_CUDA(cudaMemcpyAsync(&f0, t->frameWord.p, 4, cudaMemcpyDeviceToHost, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
+        // the scene's automatic child order is settled on this frame's rays
+        // (once per tracer; the captured frame bakes the choice in)
+        mrb_scene* sc = t->scene;
+        t->orderTune = !t->orderTuned && sc->traversal == 1 && sc->T > 1 && sc->wideOrderMode == 2;
+        t->orderMs[0] = t->orderMs[1] = 0.0f;
         // the octree's radiance state of a WFPG tracer is put back too
         const size_t U = t->svo.leafCount, N = t->svo.nodeCount;
         const size_t pb = t->wfpg ? U * 16 + U * 8 + U * 4 + N * 4 : 0;
@@ -1592,7 +1721,17 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         if (t->net)
             MRB_CUDA(cudaMemcpyAsync(t->lEmaBackup.p, t->lEma.p, size_t(kMlpParams) * 4,
                                      cudaMemcpyDeviceToDevice, t->stream));
-        if ((r = record_frame(t))) return r;
+        r = record_frame(t);
+        if (t->orderTune) {
+            t->orderTune = false;
+            if (!r) {
+                t->orderTuned = true;
+                sc->wideOrder = t->orderMs[1] < t->orderMs[0] ? 1 : 0;
+                sc->wideOrderMs[0] = t->orderMs[0];
+                sc->wideOrderMs[1] = t->orderMs[1];
+            }
+        }
+        if (r) return r;
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, false, t->stream)) return MRB_E_CUDA;
         if (t->net) {
             MRB_CUDA(cudaMemcpyAsync(t->lEma.p, t->lEmaBackup.p, size_t(kMlpParams) * 4,

@@ -105,8 +105,52 @@ __global__ void __launch_bounds__(128) k_collapse(
             area[nc] = (c1 >= n) ? half_area(lo, hi) : -1.0f;
             nc++;
         }
+        // slot of each child: the octant of its centroid around the node's
+        // centre, matched greedily by the largest projection on the
+        // octant's diagonal, so that slot ^ (ray octant) orders the
+        // children roughly front to back for any ray direction
+        {
+            float nlo[3], nhi[3];
+            child_box(it.bnode, n, inner, triAabb, sortedIdx, nlo, nhi);
+            float cost[8][8];
+            for (int k = 0; k < nc; k++) {
+                float lo[3], hi[3];
+                child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
+                float dc[3];
+                for (int c = 0; c < 3; c++) dc[c] = (lo[c] + hi[c]) - (nlo[c] + nhi[c]);
+                for (int sl = 0; sl < 8; sl++)
+                    cost[k][sl] = -(((sl & 1) ? dc[0] : -dc[0]) + ((sl & 2) ? dc[1] : -dc[1]) +
+                                    ((sl & 4) ? dc[2] : -dc[2]));
+            }
+            uint32_t slotOf[8];
+            uint32_t usedChild = 0, usedSlot = 0;
+            for (int round = 0; round < nc; round++) {
+                int bk = -1, bs = -1;
+                float bc = 0.0f;
+                for (int k = 0; k < nc; k++) {
+                    if (usedChild & (1u << k)) continue;
+                    for (int sl = 0; sl < 8; sl++) {
+                        if (usedSlot & (1u << sl)) continue;
+                        if (bk < 0 || cost[k][sl] < bc) {
+                            bk = k;
+                            bs = sl;
+                            bc = cost[k][sl];
+                        }
+                    }
+                }
+                slotOf[bk] = uint32_t(bs);
+                usedChild |= 1u << bk;
+                usedSlot |= 1u << bs;
+            }
+            uint32_t bySlot[8];
+            for (int sl = 0; sl < 8; sl++) bySlot[sl] = kInvalid;
+            for (int k = 0; k < nc; k++) bySlot[slotOf[k]] = ch[k];
+            nc = 8;
+            for (int sl = 0; sl < 8; sl++) ch[sl] = bySlot[sl];
+        }
         int nInner = 0, nLeaf = 0;
-        for (int k = 0; k < nc; k++) (ch[k] >= n) ? nInner++ : nLeaf++;
+        for (int k = 0; k < nc; k++)
+            if (ch[k] != kInvalid) (ch[k] >= n) ? nInner++ : nLeaf++;
         const uint32_t childBase = nInner ? atomicAdd(nodeCounter, uint32_t(nInner)) : 0u;
         const uint32_t triBase = nLeaf ? atomicAdd(triCounter, uint32_t(nLeaf)) : 0u;
         const uint32_t qbase = nInner ? atomicAdd(qoutCount, uint32_t(nInner)) : 0u;
@@ -127,6 +171,7 @@ __global__ void __launch_bounds__(128) k_collapse(
         uint32_t imask = 0;
         int ri = 0, rl = 0;
         for (int k = 0; k < nc; k++) {
+            if (ch[k] == kInvalid) continue;  // empty slot
             float lo[3], hi[3];
             child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
             for (int c = 0; c < 3; c++) {
@@ -196,7 +241,8 @@ __global__ void k_reset_count(uint32_t* c) {
 // Traversal
 // ---------------------------------------------------------------------------
 constexpr int kCachedNodes = 73;  // 1 + 8 + 64: the top three levels
-constexpr int kWideStack = 128;
+constexpr int kWideStack = 128;  // sorted order: one entry per pushed child
+constexpr int kWideGroups = 48;  // octant order: at most one group per level
 
 __device__ __forceinline__ float safe_dir(float d) {
     return (fabsf(d) > 1e-20f) ? d : copysignf(1e-20f, d);
@@ -247,8 +293,15 @@ __device__ __forceinline__ void tri_test(const WideAccelDev& acc, uint32_t s, V3
 
 // Closest hit of one ray in one 8-wide tree.  The top `cached` nodes are
 // read from shared memory (sNodes), the rest through the read-only cache.
+//
+// Closest hit of one ray in one 8-wide tree, children in exact
+// front-to-back order: the hit internal children are sorted by entry
+// distance, the nearest entered and the others pushed one by one with their
+// distance (entries beyond the closest hit are dropped when popped).  The
+// top `cached` nodes are read from shared memory (sNodes), the rest through
+// the read-only cache.
 template <bool kCount, int kStack>
-__device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const WideNode* sNodes,
+__device__ __forceinline__ void trace_wide_sorted(const WideAccelDev& acc, const WideNode* sNodes,
                                                int cached, V3 o, V3 d, float tmin,
                                                float& closest, int& hitTri, float& hb0,
                                                float& hb1, uint32_t& nodeVisits,
@@ -346,6 +399,117 @@ __device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const Wi
     }
 }
 
+// Closest hit of one ray in one 8-wide tree, children in octant order:
+// the collapse put every child in the slot of its centroid's octant around
+// the node's centre, so the order slot ^ octant (octant: the sign bits of
+// the ray direction) runs roughly front to back without sorting.  The stack
+// holds node groups: the child base of a visited node, its internal-child
+// mask and the bits of its hit internal children still to visit, one entry
+// per node however many children were hit.  A child's node index is the
+// child base plus the number of internal children in lower slots.
+// Triangles of leaf children are tested as soon as their box is hit.
+template <bool kCount, int kStack>
+__device__ __forceinline__ void trace_wide_octant(const WideAccelDev& acc, const WideNode* sNodes,
+                                                  int cached, V3 o, V3 d, float tmin,
+                                                  float& closest, int& hitTri, float& hb0,
+                                                  float& hb1, uint32_t& nodeVisits,
+                                                  uint32_t& triTests, uint32_t* errorFlag) {
+    if (acc.triCount == 1) {
+        if (kCount) triTests++;
+        tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
+    } else if (acc.triCount > 1) {
+        const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
+        const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) |
+                             (inv.z < 0.0f ? 4u : 0u);
+        uint2 stack[kStack];  // (child base, internal mask << 8 | pending hit bits)
+        int sp = 0;
+        int node = 0;
+        while (node >= 0) {
+            if (kCount) nodeVisits++;
+            uint4 w0, w1, w2, w3, w4;
+            if (node < cached) {
+                const uint4* sm = reinterpret_cast<const uint4*>(sNodes + node);
+                w0 = sm[0]; w1 = sm[1]; w2 = sm[2]; w3 = sm[3]; w4 = sm[4];
+            } else {
+                const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
+                w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
+                w4 = __ldg(g + 4);
+            }
+            const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
+                        lz = __uint_as_float(w0.z);
+            const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+            const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+            const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+            const uint32_t imask = w0.w >> 24;
+            const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
+            const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
+                        bz = (lz - o.z) * inv.z;
+            const uint32_t childBase = w1.x, triBase = w1.y;
+            const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
+            const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
+            const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
+            const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
+            const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
+            const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
+            uint32_t hits = 0;  // bit (slot ^ oct) for each hit internal child
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
+                if (meta == 0u) continue;
+                const int kk = k & 3;
+                const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
+                const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
+                const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
+                const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
+                const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
+                const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
+                if (!(tn <= tf)) continue;
+                if (meta & 0x40u) {  // leaf: test the triangle right away
+                    if (kCount) triTests++;
+                    tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
+                             hb0, hb1);
+                } else {
+                    hits |= 1u << (uint32_t(k) ^ oct);
+                }
+            }
+            uint32_t base = childBase, im = imask;
+            if (hits == 0) {  // resume the most recent group with pending children
+                if (sp == 0) break;
+                const uint2 e = stack[--sp];
+                base = e.x;
+                im = e.y >> 8;
+                hits = e.y & 0xFFu;
+            }
+            const uint32_t b = uint32_t(__ffs(int(hits)) - 1);
+            const uint32_t slot = b ^ oct;
+            hits &= hits - 1u;
+            if (hits) {
+                if (sp < kStack) stack[sp++] = make_uint2(base, (im << 8) | hits);
+                else atomicExch(errorFlag, 3u);
+            }
+            node = int(base + uint32_t(__popc(im & ((1u << slot) - 1u))));
+        }
+    }
+}
+
+// Either order; kStack for the sorted order's per-child entries, kGroups
+// for the octant order's per-node groups.
+template <bool kCount, bool kOctant, int kStack, int kGroups>
+__device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const WideNode* sNodes,
+                                               int cached, V3 o, V3 d, float tmin,
+                                               float& closest, int& hitTri, float& hb0,
+                                               float& hb1, uint32_t& nodeVisits,
+                                               uint32_t& triTests, uint32_t* errorFlag) {
+    if (kOctant)
+        trace_wide_octant<kCount, kGroups>(acc, sNodes, cached, o, d, tmin, closest, hitTri, hb0,
+                                           hb1, nodeVisits, triTests, errorFlag);
+    else
+        trace_wide_sorted<kCount, kStack>(acc, sNodes, cached, o, d, tmin, closest, hitTri, hb0,
+                                          hb1, nodeVisits, triTests, errorFlag);
+}
+
 __device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut& out, uint32_t i,
                                           int hitTri, float closest, float hb0, float hb1) {
     if (hitTri >= 0) {
@@ -365,7 +529,7 @@ __device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut&
 // traversal's dependent loads and ALU chains want resident warps more than
 // registers (measured on clusters-1M: 8 blocks 4.77 ms, 9 blocks 4.57 ms,
 // 10 blocks 5.27 ms per frame of traversal; 7 blocks at 68 registers 5.05 ms).
-template <bool kCount>
+template <bool kCount, bool kOctant>
 __global__ void __launch_bounds__(128, 9) k_trace_wide(WideAccelDev acc,
                                                     const float4* __restrict__ rayO,
                                                     const float4* __restrict__ rayD,
@@ -385,7 +549,7 @@ __global__ void __launch_bounds__(128, 9) k_trace_wide(WideAccelDev acc,
         float closest = rd.w;
         int hitTri = -1;
         float hb0 = 0.0f, hb1 = 0.0f;
-        trace_wide_ray<kCount, kWideStack>(acc, sNodes, cached, V3{ro.x, ro.y, ro.z},
+        trace_wide_ray<kCount, kOctant, kWideStack, kWideGroups>(acc, sNodes, cached, V3{ro.x, ro.y, ro.z},
                                            V3{rd.x, rd.y, rd.z}, ro.w, closest, hitTri, hb0, hb1,
                                            nodeVisits, triTests, errorFlag);
         write_hit(acc, out, i, hitTri, closest, hb0, hb1);
@@ -406,7 +570,7 @@ __global__ void __launch_bounds__(128, 9) k_trace_wide(WideAccelDev acc,
 // Rays of many scenes: each ray's tree is its job's (RayAux::pad is the job
 // slot).  No shared-memory top levels: neighbouring rays may use different
 // trees.
-template <int kBlock, int kStack>
+template <int kBlock, int kStack, bool kOctant>
 __global__ void __launch_bounds__(kBlock) k_trace_wide_jobs(const JobDev* __restrict__ jobs,
                                                             const RayAux* __restrict__ aux,
                                                             const float4* __restrict__ rayO,
@@ -422,7 +586,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_wide_jobs(const JobDev* __rest
         float closest = rd.w;
         int hitTri = -1;
         float hb0 = 0.0f, hb1 = 0.0f;
-        trace_wide_ray<false, kStack>(acc, nullptr, 0, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z},
+        trace_wide_ray<false, kOctant, kStack, kWideGroups>(acc, nullptr, 0, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z},
                                       ro.w, closest, hitTri, hb0, hb1, nodeVisits, triTests,
                                       errorFlag);
         write_hit(acc, out, i, hitTri, closest, hb0, hb1);
@@ -479,31 +643,119 @@ int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0,
 
 int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
                        const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
-                       uint32_t* errorFlag, cudaStream_t stream, unsigned long long* counters) {
+                       uint32_t* errorFlag, cudaStream_t stream, unsigned long long* counters,
+                       int order) {
     if (maxCount == 0) return 0;
     uint32_t blocks = (maxCount + 127) / 128;
     blocks = blocks < 148u * 16u ? blocks : 148u * 16u;
-    if (counters)
-        k_trace_wide<true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
-                                                       errorFlag, counters);
-    else
-        k_trace_wide<false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out,
-                                                        errorFlag, nullptr);
+    if (order == 1) {
+        if (counters)
+            k_trace_wide<true, true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
+                                                                 out, errorFlag, counters);
+        else
+            k_trace_wide<false, true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
+                                                                  out, errorFlag, nullptr);
+    } else {
+        if (counters)
+            k_trace_wide<true, false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
+                                                                  out, errorFlag, counters);
+        else
+            k_trace_wide<false, false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount,
+                                                                   maxCount, out, errorFlag, nullptr);
+    }
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
 
-template <int kBlock, int kStack>
+namespace {
+// Seeded probe rays over the scene's box: origins uniform in it, directions
+// uniform on the sphere (Philox counter (i, 0, 0x60000, 0)).
+__global__ void k_probe_rays(const float* __restrict__ ext, uint32_t n, float4* rayO,
+                             float4* rayD) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Rand4 r = philox_uniform4(i, 0u, 0x60000u, 0u, 0x5eedu, 0u);
+        const Rand4 q = philox_uniform4(i, 1u, 0x60000u, 0u, 0x5eedu, 0u);
+        float o[3];
+        for (int c = 0; c < 3; c++) o[c] = ext[c] + r.u[c] * (ext[3 + c] - ext[c]);
+        const float z = 1.0f - 2.0f * q.u[0];
+        const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        float sn, cs;
+        pm_sincos(6.2831853f * q.u[1], sn, cs);
+        rayO[i] = make_float4(o[0], o[1], o[2], 0.0f);
+        rayD[i] = make_float4(rr * cs, rr * sn, z, 3.0e38f);
+    }
+}
+}  // namespace
+
+int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStream_t st,
+                        int* orderOut, float* msOut) {
+    constexpr uint32_t kProbe = 1u << 16;
+    void* buf = nullptr;
+    const size_t bytes = size_t(kProbe) * (16 + 16 + 4 + 4 + 4 + 8) + 16;
+    MRB_CUDA(cudaMalloc(&buf, bytes));
+    char* b = static_cast<char*>(buf);
+    float4* ro = reinterpret_cast<float4*>(b);
+    float4* rd = ro + kProbe;
+    HitOut ho{reinterpret_cast<uint32_t*>(rd + kProbe), nullptr, nullptr, nullptr};
+    ho.prim = ho.key + kProbe;
+    ho.t = reinterpret_cast<float*>(ho.prim + kProbe);
+    ho.bary = reinterpret_cast<float2*>(ho.t + kProbe);
+    uint32_t* err = reinterpret_cast<uint32_t*>(ho.bary + kProbe);
+    cudaEvent_t e[2];
+    cudaEventCreate(&e[0]);
+    cudaEventCreate(&e[1]);
+    float best[2] = {1e30f, 1e30f};
+    int rc = 0;
+    k_probe_rays<<<(kProbe + 255) / 256, 256, 0, st>>>(dExtent, kProbe, ro, rd);
+    for (int rep = 0; rep < 4 && rc == 0; rep++)
+        for (int order = 0; order < 2 && rc == 0; order++) {
+            cudaEventRecord(e[0], st);
+            rc = trace_closest_wide(acc, ro, rd, nullptr, kProbe, ho, err, st, nullptr, order);
+            cudaEventRecord(e[1], st);
+            cudaEventSynchronize(e[1]);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e[0], e[1]);
+            if (rep > 0) best[order] = std::min(best[order], ms);  // the first pass warms up
+        }
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    cudaFree(buf);
+    if (rc) return rc;
+    MRB_CUDA(cudaGetLastError());
+    *orderOut = best[1] < best[0] ? 1 : 0;
+    if (msOut) {
+        msOut[0] = best[0];
+        msOut[1] = best[1];
+    }
+    return 0;
+}
+
+template <int kBlock, int kStack, bool kOctant>
 static int launch_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
                        const float4* rayD, const uint32_t* dCount, uint32_t maxCount,
                        const HitOut& out, uint32_t* errorFlag, cudaStream_t stream) {
     uint32_t blocks = (maxCount + kBlock - 1) / kBlock;
     const uint32_t cap = 148u * (2048u / kBlock);
     blocks = blocks < cap ? blocks : cap;
-    k_trace_wide_jobs<kBlock, kStack><<<blocks, kBlock, 0, stream>>>(jobs, aux, rayO, rayD, dCount,
-                                                                     maxCount, out, errorFlag);
+    k_trace_wide_jobs<kBlock, kStack, kOctant><<<blocks, kBlock, 0, stream>>>(
+        jobs, aux, rayO, rayD, dCount, maxCount, out, errorFlag);
     MRB_CUDA(cudaGetLastError());
     return 0;
+}
+
+template <int kBlock>
+static int launch_jobs_stack(const JobDev* jobs, const RayAux* aux, const float4* rayO,
+                             const float4* rayD, const uint32_t* dCount, uint32_t maxCount,
+                             const HitOut& out, uint32_t* errorFlag, int stack,
+                             cudaStream_t stream) {
+    if (stack == 0)
+        return launch_jobs<kBlock, kWideStack, true>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                                     errorFlag, stream);
+    if (stack > 64)
+        return launch_jobs<kBlock, 128, false>(jobs, aux, rayO, rayD, dCount, maxCount, out,
+                                               errorFlag, stream);
+    return launch_jobs<kBlock, 64, false>(jobs, aux, rayO, rayD, dCount, maxCount, out, errorFlag,
+                                          stream);
 }
 
 int trace_closest_wide_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
@@ -511,23 +763,16 @@ int trace_closest_wide_jobs(const JobDev* jobs, const RayAux* aux, const float4*
                             const HitOut& out, uint32_t* errorFlag, int block, int stack,
                             cudaStream_t stream) {
     if (maxCount == 0) return 0;
-    const bool big = stack > 64;
     switch (block) {
         case 64:
-            return big ? launch_jobs<64, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                              errorFlag, stream)
-                       : launch_jobs<64, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                             errorFlag, stream);
+            return launch_jobs_stack<64>(jobs, aux, rayO, rayD, dCount, maxCount, out, errorFlag,
+                                         stack, stream);
         case 256:
-            return big ? launch_jobs<256, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                               errorFlag, stream)
-                       : launch_jobs<256, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                              errorFlag, stream);
+            return launch_jobs_stack<256>(jobs, aux, rayO, rayD, dCount, maxCount, out, errorFlag,
+                                          stack, stream);
         default:
-            return big ? launch_jobs<128, 128>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                               errorFlag, stream)
-                       : launch_jobs<128, 64>(jobs, aux, rayO, rayD, dCount, maxCount, out,
-                                              errorFlag, stream);
+            return launch_jobs_stack<128>(jobs, aux, rayO, rayD, dCount, maxCount, out, errorFlag,
+                                          stack, stream);
     }
 }
 

@@ -41,9 +41,16 @@ size_t wide_scratch_bytes(uint32_t n);
 // into tv0/te0/te1 (n each).  Synchronises the stream every 8 levels.
 int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0, float4* te1,
                void* scratch, uint32_t* nodeCountOut, cudaStream_t stream);
+// order 0: children in exact front-to-back order (sorted entry distances,
+// per-child stack entries); 1: octant order with per-node group entries.
 int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
                        const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
                        uint32_t* errorFlag, cudaStream_t stream,
-                       unsigned long long* counters = nullptr);
+                       unsigned long long* counters = nullptr, int order = 0);
+// Times both orders on 65,536 seeded rays over the scene box (device
+// extent: min xyz, max xyz) and returns the faster; msOut[2] (may be null)
+// the best times.
+int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStream_t stream,
+                        int* orderOut, float* msOut);
 
 }  // namespace mrb

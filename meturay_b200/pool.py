@@ -182,13 +182,14 @@ def _finish(pool: WavefrontPool, ids: list[int]):
 
 
 def autotune(system: TracerSystem, jobs: list[Job], capacities=(1 << 16, 1 << 18, 1 << 20, 1 << 22),
-             blocks=(64, 128, 256), stacks=(64, 128), max_depth: int = 8,
+             blocks=(64, 128, 256), stacks=(64, 128, 0), max_depth: int = 8,
              iterations: int = 3) -> dict:
     """Measure rays/s of `iterations` pool iterations over the given jobs for
     each wavefront size (camera samples per iteration; 2 rays each) and
-    traversal launch shape, and return the fastest configuration with the
-    table of all measured ones.  The jobs' frame counts are replaced so that
-    every timed iteration has work."""
+    traversal launch shape (block size; stack of 64 or 128 entries for the
+    sorted child order, 0 for the octant order), and return the fastest
+    configuration with the table of all measured ones.  The jobs' frame
+    counts are replaced so that every timed iteration has work."""
     from dataclasses import replace
     table = []
     best = None

@@ -158,8 +158,31 @@ class GPUScene:
     def accel_info(self) -> dict:
         info = np.zeros(4, np.uint32)
         check(lib.mrb_accel_info(self._h, _ptr(info)))
+        ext = np.zeros(2, np.uint32)
+        areas = np.zeros(2, np.float64)
+        check(lib.mrb_accel_info_ext(self._h, _ptr(ext), _ptr(areas)))
         return {"triangles": int(info[0]), "binary_nodes": int(info[1]),
-                "wide_nodes": int(info[2]), "traversal": int(info[3])}
+                "wide_nodes": int(info[2]), "traversal": int(info[3]),
+                "wide_tree": "ploc" if ext[0] == 1 else "lbvh", "ploc_steps": int(ext[1]),
+                "inner_area_lbvh": float(areas[0]), "inner_area_ploc": float(areas[1])}
+
+    def set_wide_order(self, order: int):
+        """Child order of the 8-wide traversal: 0 sorted, 1 octant, 2 (default)
+        the faster one, timed on seeded probe rays at construction and then
+        on a tracer's own rays in the frame before it captures its graph."""
+        check(lib.mrb_accel_set_wide_order(self._h, int(order)))
+
+    def wide_order(self) -> dict:
+        o = C.c_int(0)
+        ms = np.zeros(2, np.float32)
+        check(lib.mrb_accel_wide_order(self._h, C.byref(o), _ptr(ms)))
+        return {"order": "octant" if o.value == 1 else "sorted",
+                "ms_sorted": float(ms[0]), "ms_octant": float(ms[1])}
+
+    def set_wide_tree(self, tree: int):
+        """Before construct_accelerators: the tree collapsed into the 8-wide
+        layout: 0 the LBVH, 1 PLOC, 2 (default) the one with less box area."""
+        check(lib.mrb_accel_set_wide_tree(self._h, int(tree)))
 
     def build_svo(self, resolution: int):
         """Sparse voxel octree of the scene at `resolution` leaf voxels per axis."""

@@ -164,16 +164,19 @@ def _rays_for(scene, n, seed):
     return rays
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("name,make", _scenes())
 def test_trace_closest_hit(system, cuda, oracle, name, make, mode):
     """mode 0: binary LBVH nodes, bit-exact against the oracle's traversal of
-    the same tree.  mode 1: 8-wide quantised nodes; same hit/miss and the
-    same closest distance bit for bit, same primitive except at ties."""
+    the same tree.  modes 1 and 2: 8-wide quantised nodes in sorted and in
+    octant child order; same hit/miss and the same closest distance bit for
+    bit, same primitive except at ties."""
     torch = cuda
     scene = make()
     g = _build(system, scene)
-    g.set_traversal(mode)
+    g.set_traversal(min(mode, 1))
+    if mode >= 1:
+        g.set_wide_order(mode - 1)
     info = g.accel_info()
     if scene.triangle_count > 1:
         assert 0 < info["wide_nodes"] <= scene.triangle_count - 1

@@ -112,7 +112,7 @@ def test_launch_shapes_agree(system):
     job = Job(g, 40, 40, samples=2, frames=2, max_depth=5, seed=2)
     ref = None
     for block in (64, 128, 256):
-        for stack in (64, 128):
+        for stack in (64, 128, 0):  # 0: the octant child order
             pool = WavefrontPool(system, capacity=1 << 15, max_depth=5)
             pool.set_launch(block, stack)
             img = _run(pool, [job])[0]
