@@ -142,21 +142,31 @@ int mrb_accel_hit(const mrb_scene* scene, const float* d_ray_o, const float* d_r
 int mrb_accel_set_traversal(mrb_scene* scene, int mode);
 /* info[4]: triangles, binary inner nodes, wide nodes, traversal mode. */
 int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
-/* Child order of the 8-wide traversal: 0 exact front-to-back (entry
- * distances sorted, one stack entry per pushed child), 1 octant order (the
- * collapse places children by the octant of their centroid; one stack entry
- * per node group), 2 (default) the faster of the two: first on 65,536
- * seeded rays over the scene box, timed at mrb_accel_construct (or at once
- * when the accelerator is built), then on a tracer's own rays: the frame
- * that mrb_tracer_render_frame runs before it captures its graph traces
- * every depth's rays in both orders and keeps the faster sum (once per
- * tracer).  Closest hits are the same either way, up to the choice among
- * triangles at the same distance. */
+/* Traversal kernel of the 8-wide layout.  Child order: sorted (exact
+ * front to back: entry distances sorted, one stack entry per pushed child)
+ * or octant (the collapse places children by the octant of their centroid,
+ * visited in the order slot ^ ray octant; one stack entry per node group,
+ * leaf triangles tested after the node's box tests).  Refill: a warp's idle
+ * lanes take its next rays once eight of them are idle (a gain where path
+ * lengths differ, a loss for coherent camera rays).  MRB_WIDE_AUTO
+ * (default): the fastest kernel, timed first on 65,536 seeded rays over the
+ * scene box at mrb_accel_construct (or at once when the accelerator is
+ * built), then per depth on a tracer's own rays: the frame that
+ * mrb_tracer_render_frame runs before it captures its graph traces every
+ * depth's rays with every kernel and keeps the fastest per depth (once per
+ * tracer and traversal setting).  Closest hits are the same with every
+ * kernel, up to the choice among triangles at the same distance. */
+#define MRB_WIDE_SORTED 0
+#define MRB_WIDE_OCTANT 1
+#define MRB_WIDE_SORTED_REFILL 2
+#define MRB_WIDE_OCTANT_REFILL 3
+#define MRB_WIDE_AUTO 4
 int mrb_accel_set_wide_order(mrb_scene* s, int order);
-/* The order in use (0 or 1) and the last measured times per order (ms:
- * the probe's, or the summed per-depth traces of a tracer's frame; 0 when
- * the order was set rather than measured). */
-int mrb_accel_wide_order(const mrb_scene* s, int* order, float* probe_ms2);
+/* The kernel in use where no tracer tuned its own (MRB_WIDE_SORTED ..
+ * MRB_WIDE_OCTANT_REFILL) and, in ms4 (may be NULL), the last measured
+ * times per kernel (the probe's, or the per-depth sums of a tracer's
+ * frame; 0 when the kernel was set rather than measured). */
+int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms4);
 /* The tree the 8-wide traversal layout is collapsed from (before
  * mrb_accel_construct): 0 the LBVH, 1 a PLOC tree (parallel locally-ordered
  * clustering by merged-box area) over the LBVH's Morton-sorted leaves, 2
@@ -387,6 +397,10 @@ int mrb_tracer_stats(mrb_tracer* t, uint64_t* rays_traced, uint32_t* frames);
 void* mrb_tracer_stream(mrb_tracer* t);
 /* Number of kernels one frame launches (>= 0), or a negative status. */
 int mrb_tracer_launches_per_frame(mrb_tracer* t);
+/* The 8-wide traversal kernel of each depth (MRB_WIDE_SORTED ..
+ * MRB_WIDE_OCTANT_REFILL; -1 with the binary traversal) for the first n
+ * depths; returns how many were written. */
+int mrb_tracer_wide_orders(const mrb_tracer* t, int* orders, uint32_t n);
 /* Render one frame stage by stage with CUDA events around each stage.
  * stage_ms[5]: camera, traversal, partition, shading, resolve (summed over
  * depths).  work[4]: rays traced, inner nodes visited, triangles tested,

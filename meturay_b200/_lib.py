@@ -102,6 +102,7 @@ def _load() -> C.CDLL:
         "mrb_tracer_stats": (i32, [vp, C.POINTER(u64), C.POINTER(u32)]),
         "mrb_tracer_stream": (vp, [vp]),
         "mrb_tracer_launches_per_frame": (i32, [vp]),
+        "mrb_tracer_wide_orders": (i32, [vp, C.POINTER(C.c_int), u32]),
         "mrb_tracer_profile_frame": (i32, [vp, vp, vp]),
         "mrb_tracer_profile_stages": (i32, [vp, vp, u32, vp]),
         "mrb_morton_codes": (i32, [vp, vp, u32, vp, vp, vp, vp]),

@@ -103,9 +103,13 @@ struct mrb_scene {
     uint32_t wNodeCount = 0;
     int traversal = 1;  // 0: binary LBVH nodes, 1: 8-wide nodes
     int wideTree = 2;        // 0 LBVH, 1 PLOC, 2 the one with less inner-box area
-    int wideOrderMode = 2;   // 0 sorted, 1 octant, 2 the faster as timed
-    int wideOrder = 0;       // in use
-    float wideOrderMs[2] = {0.0f, 0.0f};
+    // traversal kernel (WideOrder), or MRB_WIDE_AUTO: the fastest as timed
+    int wideOrderMode = MRB_WIDE_AUTO;
+    int wideOrder = 0;  // in use where no tracer has tuned its own
+    float wideOrderMs[kWideOrders] = {};
+    // bumped whenever the traversal choice changes, so that captured frames
+    // and tuned per-depth kernels are redone
+    uint32_t traceEpoch = 0;
     int wideTreeUsed = 0;
     uint32_t plocSteps = 0;
     double areaLbvh = 0.0, areaPloc = 0.0;  // sums of inner half areas

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <cmath>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/mrb200.h"
@@ -240,10 +241,13 @@ struct mrb_tracer {
     // graph
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
-    // 8-wide child order chosen on this tracer's own rays: the eager frame
-    // before a capture times both orders at every depth
-    bool orderTune = false, orderTuned = false;
-    float orderMs[2] = {0.0f, 0.0f};
+    uint32_t graphEpoch = 0;  // scene traceEpoch the graph was captured for
+    // 8-wide traversal kernel per depth, chosen on this tracer's own rays:
+    // the eager frame before a capture times every kernel at every depth
+    bool orderTune = false;
+    uint32_t orderEpoch = ~0u;  // scene traceEpoch depthOrder was tuned for
+    std::vector<int> depthOrder;
+    std::vector<std::array<float, kWideOrders>> depthMs;
     ~mrb_tracer() {
         if (trainStream) cudaStreamSynchronize(trainStream);
         if (copyStream) cudaStreamSynchronize(copyStream);
@@ -576,12 +580,13 @@ PortionTable portion_table(const mrb_tracer* t) {
     return PortionTable{p, p + 8, p + 16};
 }
 
+// order: the 8-wide kernel, or -1 for the scene's.
 int trace_dispatch(const mrb_scene* sc, const float4* rayO, const float4* rayD,
                    const uint32_t* dCount, uint32_t maxCount, const HitOut& ho, uint32_t* err,
-                   cudaStream_t st, unsigned long long* counters = nullptr) {
+                   cudaStream_t st, unsigned long long* counters = nullptr, int order = -1) {
     if (sc->traversal == 1 && sc->T > 1)
         return trace_closest_wide(sc->wide(), rayO, rayD, dCount, maxCount, ho, err, st, counters,
-                                  sc->wideOrder);
+                                  order >= 0 ? order : sc->wideOrder);
     return trace_closest(sc->accel(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
 }
 
@@ -608,19 +613,21 @@ struct StageTimer {
     float ms[kStageCount] = {};
 };
 
-// Both 8-wide child orders traced over the rays of buffer `cur` (twice
-// each, the faster pass kept: the first launch of a kernel may load its
-// module), added to t->orderMs.  Every pass writes the same closest hits but
-// for ties; the frame's own trace follows and overwrites them.
-int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho) {
+// Every 8-wide traversal kernel run over the rays of buffer `cur` of depth
+// d (twice each, the faster pass kept: the first launch of a kernel may load
+// its module), into t->depthMs[d].  Every pass writes the same closest hits
+// but for ties; the frame's own trace follows and overwrites them.
+int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho, uint32_t d) {
     const mrb_scene* sc = t->scene;
+    if (d >= t->depthMs.size()) return 0;
     cudaEvent_t e[2];
     MRB_CUDA(cudaEventCreate(&e[0]));
     MRB_CUDA(cudaEventCreate(&e[1]));
-    float best[2] = {1e30f, 1e30f};
+    std::array<float, kWideOrders> best;
+    best.fill(1e30f);
     int r = 0;
     for (int rep = 0; rep < 2 && !r; rep++)
-        for (int o = 0; o < 2 && !r; o++) {
+        for (int o = 0; o < kWideOrders && !r; o++) {
             cudaEventRecord(e[0], t->stream);
             r = trace_closest_wide(sc->wide(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
                                    t->count.as<uint32_t>() + cur, t->maxRays, ho,
@@ -636,9 +643,16 @@ int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho) {
     cudaEventDestroy(e[1]);
     if (r) return r;
     MRB_CUDA(cudaGetLastError());
-    t->orderMs[0] += best[0];
-    t->orderMs[1] += best[1];
+    t->depthMs[d] = best;
     return 0;
+}
+
+// The traversal kernel of depth d: the tracer's own choice where it tuned
+// one for the scene's current traversal, else the scene's.
+int depth_order(const mrb_tracer* t, uint32_t d) {
+    if (!t->orderTune && t->orderEpoch == t->scene->traceEpoch && d < t->depthOrder.size())
+        return t->depthOrder[d];
+    return -1;
 }
 
 // One Render() step: HitRays -> PartitionRaysWRTWork -> WorkRays
@@ -665,16 +679,18 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
         tm->ms[stage] += ms;
         return 0;
     };
-    if (t->orderTune && (r = time_wide_orders(t, cur, ho))) return r;
+    if (t->orderTune && (r = time_wide_orders(t, cur, ho, d))) return r;
+    const int order = depth_order(t, d);
     if (mark(0)) return MRB_E_CUDA;
     if ((r = trace_dispatch(sc, t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(), cnt + cur,
-                            t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream)))
+                            t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream, nullptr,
+                            order)))
         return r;
     if (mark(1) || lap(1, 0)) return MRB_E_CUDA;
     if (workCounters) {
         if ((r = trace_dispatch(sc, t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
                                 cnt + cur, t->maxRays, ho, t->errorFlags.as<uint32_t>(), t->stream,
-                                workCounters)))
+                                workCounters, order)))
             return r;
     }
     if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
@@ -1204,8 +1220,8 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
                             s->wTe1.as<float4>(), s->wScratch.p, &s->wNodeCount, st)))
             return r;
         s->wScratch.release();
-        s->wideOrderMs[0] = s->wideOrderMs[1] = 0.0f;
-        if (s->wideOrderMode == 2) {
+        for (float& m : s->wideOrderMs) m = 0.0f;
+        if (s->wideOrderMode == MRB_WIDE_AUTO) {
             if ((r = wide_order_autotune(s->wide(), s->aExtent.as<float>(), st, &s->wideOrder,
                                          s->wideOrderMs)))
                 return r;
@@ -1224,6 +1240,7 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
     }
     s->rootInner = (n == 1) ? ~0 : static_cast<int>(root - n);
     s->built = true;
+    s->traceEpoch++;
     return 0;
 }
 
@@ -1332,33 +1349,45 @@ int mrb_accel_set_traversal(mrb_scene* s, int mode) {
         return MRB_E_ARG;
     }
     s->traversal = mode;
+    s->traceEpoch++;
     return 0;
 }
 
 int mrb_accel_set_wide_order(mrb_scene* s, int order) {
-    if (!s || order < 0 || order > 2) {
-        set_error("wide order must be 0 (sorted), 1 (octant) or 2 (the faster on probe rays)");
+    if (!s || order < 0 || order > MRB_WIDE_AUTO) {
+        set_error("wide order must be 0 (sorted), 1 (octant), 2 (sorted, refilled lanes), "
+                  "3 (octant, refilled lanes) or 4 (the fastest as timed)");
         return MRB_E_ARG;
     }
     s->wideOrderMode = order;
+    s->traceEpoch++;
+    for (float& m : s->wideOrderMs) m = 0.0f;
+    if (order != MRB_WIDE_AUTO) {
+        s->wideOrder = order;
+        return 0;
+    }
     if (!s->built || s->T < 2) return 0;
     if (set_device(s->sys)) return MRB_E_CUDA;
-    s->wideOrderMs[0] = s->wideOrderMs[1] = 0.0f;
-    if (order == 2)
-        return wide_order_autotune(s->wide(), s->aExtent.as<float>(), nullptr, &s->wideOrder,
-                                   s->wideOrderMs);
-    s->wideOrder = order;
+    return wide_order_autotune(s->wide(), s->aExtent.as<float>(), nullptr, &s->wideOrder,
+                               s->wideOrderMs);
+}
+
+int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms4) {
+    if (!s || !order) return MRB_E_ARG;
+    *order = s->wideOrder;
+    if (ms4)
+        for (int o = 0; o < kWideOrders; o++) ms4[o] = s->wideOrderMs[o];
     return 0;
 }
 
-int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms2) {
-    if (!s || !order) return MRB_E_ARG;
-    *order = s->wideOrder;
-    if (ms2) {
-        ms2[0] = s->wideOrderMs[0];
-        ms2[1] = s->wideOrderMs[1];
+int mrb_tracer_wide_orders(const mrb_tracer* t, int* orders, uint32_t n) {
+    if (!t || (n && !orders)) return MRB_E_ARG;
+    uint32_t k = 0;
+    for (; k < n && k < t->maxDepth; k++) {
+        const int o = depth_order(t, k);
+        orders[k] = o >= 0 ? o : (t->scene->traversal == 1 ? t->scene->wideOrder : -1);
     }
-    return 0;
+    return int(k);
 }
 
 int mrb_accel_set_wide_tree(mrb_scene* s, int tree) {
@@ -1684,6 +1713,8 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
     // the captured frame bakes in which sampler guides: capture again when
     // the network takes over
     if (t->wfpg && t->learned && t->frames == t->learnedWarmup) t->graphDirty = true;
+    // the scene's traversal changed since the capture
+    if (t->graphEpoch != t->scene->traceEpoch) t->graphDirty = true;
     if (t->graphDirty || !t->graph) {
         if (t->graph) {
             cudaGraphExecDestroy(t->graph);
@@ -1701,11 +1732,18 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
                                  cudaMemcpyDeviceToDevice, t->stream));
         MRB_CUDA(cudaMemcpyAsync(&f0, t->frameWord.p, 4, cudaMemcpyDeviceToHost, t->stream));
         MRB_CUDA(cudaStreamSynchronize(t->stream));
-        // the scene's automatic child order is settled on this frame's rays
-        // (once per tracer; the captured frame bakes the choice in)
+        // with the automatic traversal kernel, each depth's kernel is settled
+        // on this frame's rays (once per tracer and scene traversal; the
+        // captured frame bakes the choice in)
         mrb_scene* sc = t->scene;
-        t->orderTune = !t->orderTuned && sc->traversal == 1 && sc->T > 1 && sc->wideOrderMode == 2;
-        t->orderMs[0] = t->orderMs[1] = 0.0f;
+        t->orderTune = sc->traversal == 1 && sc->T > 1 && sc->wideOrderMode == MRB_WIDE_AUTO &&
+                       t->orderEpoch != sc->traceEpoch;
+        if (t->orderTune) {
+            std::array<float, kWideOrders> z;
+            z.fill(0.0f);
+            t->depthMs.assign(t->maxDepth, z);
+            t->depthOrder.assign(t->maxDepth, 0);
+        }
         // the octree's radiance state of a WFPG tracer is put back too
         const size_t U = t->svo.leafCount, N = t->svo.nodeCount;
         const size_t pb = t->wfpg ? U * 16 + U * 8 + U * 4 + N * 4 : 0;
@@ -1725,10 +1763,25 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         if (t->orderTune) {
             t->orderTune = false;
             if (!r) {
-                t->orderTuned = true;
-                sc->wideOrder = t->orderMs[1] < t->orderMs[0] ? 1 : 0;
-                sc->wideOrderMs[0] = t->orderMs[0];
-                sc->wideOrderMs[1] = t->orderMs[1];
+                // per depth the fastest kernel; for the scene's other callers
+                // the fastest over the whole frame
+                std::array<float, kWideOrders> sum;
+                sum.fill(0.0f);
+                for (size_t d = 0; d < t->depthMs.size(); d++) {
+                    int best = 0;
+                    for (int o = 0; o < kWideOrders; o++) {
+                        sum[o] += t->depthMs[d][o];
+                        if (t->depthMs[d][o] < t->depthMs[d][best]) best = o;
+                    }
+                    t->depthOrder[d] = best;
+                }
+                int best = 0;
+                for (int o = 0; o < kWideOrders; o++) {
+                    sc->wideOrderMs[o] = sum[o];
+                    if (sum[o] < sum[best]) best = o;
+                }
+                sc->wideOrder = best;
+                t->orderEpoch = sc->traceEpoch;
             }
         }
         if (r) return r;
@@ -1772,6 +1825,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             return MRB_E_CUDA;
         }
         t->graphDirty = false;
+        t->graphEpoch = t->scene->traceEpoch;
     }
     MRB_CUDA(cudaGraphLaunch(t->graph, t->stream));
     t->frames++;

@@ -24,6 +24,8 @@
 // meta per slot: 0 empty, 0x80|rank internal child, 0x40|rank leaf child.
 // A child plane decodes as lo + q * 2^(e-127); quantisation rounds outward,
 // so decoded boxes contain the exact child boxes.
+#include <type_traits>
+
 #include "../../include/mrb200.h"
 #include "common.cuh"
 #include "wide.cuh"
@@ -291,223 +293,257 @@ __device__ __forceinline__ void tri_test(const WideAccelDev& acc, uint32_t s, V3
     }
 }
 
-// Closest hit of one ray in one 8-wide tree.  The top `cached` nodes are
-// read from shared memory (sNodes), the rest through the read-only cache.
-//
-// Closest hit of one ray in one 8-wide tree, children in exact
-// front-to-back order: the hit internal children are sorted by entry
-// distance, the nearest entered and the others pushed one by one with their
-// distance (entries beyond the closest hit are dropped when popped).  The
-// top `cached` nodes are read from shared memory (sNodes), the rest through
-// the read-only cache.
-template <bool kCount, int kStack>
-__device__ __forceinline__ void trace_wide_sorted(const WideAccelDev& acc, const WideNode* sNodes,
-                                               int cached, V3 o, V3 d, float tmin,
-                                               float& closest, int& hitTri, float& hb0,
-                                               float& hb1, uint32_t& nodeVisits,
-                                               uint32_t& triTests, uint32_t* errorFlag) {
-    if (acc.triCount == 1) {
-        if (kCount) triTests++;
-        tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
-    } else if (acc.triCount > 1) {
-        const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
-        uint2 stack[kStack];  // (node, entry distance bits)
-        int sp = 0;
-        int node = 0;
-        while (node >= 0) {
-            if (kCount) nodeVisits++;
-            uint4 w0, w1, w2, w3, w4;
-            if (node < cached) {
-                const uint4* s = reinterpret_cast<const uint4*>(sNodes + node);
-                w0 = s[0]; w1 = s[1]; w2 = s[2]; w3 = s[3]; w4 = s[4];
-            } else {
-                const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
-                w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
-                w4 = __ldg(g + 4);
-            }
-            const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
-                        lz = __uint_as_float(w0.z);
-            const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
-            const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
-            const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-            // t = (lo + q*s - o) * inv = q * (s*inv) + (lo - o) * inv
-            const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
-            const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
-                        bz = (lz - o.z) * inv.z;
-            const uint32_t childBase = w1.x, triBase = w1.y;
-            // near/far plane choice per axis from the ray direction
-            const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
-            const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
-            const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
-            const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
-            const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
-            const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
-            // internal children that are hit, keyed by entry distance:
-            // (distance bits with the low three cleared) | slot
-            uint32_t key[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                key[k] = 0xFFFFFFFFu;
-                const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
-                if (meta == 0u) continue;
-                const int kk = k & 3;
-                const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
-                const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
-                const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
-                const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
-                const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
-                const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
-                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
-                if (!(tn <= tf)) continue;
-                if (meta & 0x40u) {  // leaf: test the triangle right away
-                    if (kCount) triTests++;
-                    tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
-                             hb0, hb1);
-                } else {
-                    key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
-                }
-            }
-            sort8(key);
-            // push the farther hits (farthest first), enter the nearest
-            node = -1;
-#pragma unroll
-            for (int j = 7; j >= 0; j--) {
-                if (key[j] == 0xFFFFFFFFu) continue;
-                const float tn = __uint_as_float(key[j] & ~7u);
-                if (tn > closest) continue;
-                const uint32_t slot = key[j] & 7u;
-                const uint32_t meta = byte_of(slot < 4 ? w1.z : w1.w, int(slot & 3u));
-                const uint32_t child = childBase + (meta & 0x3Fu);
-                if (j == 0) {
-                    node = int(child);
-                } else if (sp < kStack) {
-                    stack[sp++] = make_uint2(child, key[j] & ~7u);
-                } else {
-                    atomicExch(errorFlag, 3u);
-                }
-            }
-            if (node < 0) {
-                // the nearest hit was beyond the closest triangle: fall
-                // through to the stack
-            }
-            while (node < 0 && sp > 0) {
-                const uint2 e = stack[--sp];
-                if (__uint_as_float(e.y) <= closest) node = int(e.x);
-            }
-        }
-    }
+template <int k>
+using IntC = std::integral_constant<int, k>;
+
+// Per-ray state of a traversal: the ray, its closest hit so far and the
+// node to visit next (-1: done).  The stack lives beside it.
+struct WideRay {
+    V3 o, d, inv;
+    float tmin, closest, hb0, hb1;
+    int hitTri, node, sp;
+    uint32_t oct;  // sign bits of the direction: x | y << 1 | z << 2
+};
+
+__device__ __forceinline__ void wide_ray_begin(WideRay& r, float4 ro, float4 rd) {
+    r.o = V3{ro.x, ro.y, ro.z};
+    r.d = V3{rd.x, rd.y, rd.z};
+    r.tmin = ro.w;
+    r.closest = rd.w;
+    r.hb0 = r.hb1 = 0.0f;
+    r.hitTri = -1;
+    r.inv = V3{1.0f / safe_dir(rd.x), 1.0f / safe_dir(rd.y), 1.0f / safe_dir(rd.z)};
+    r.oct = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
+    r.node = 0;
+    r.sp = 0;
 }
 
-// Closest hit of one ray in one 8-wide tree, children in octant order:
-// the collapse put every child in the slot of its centroid's octant around
-// the node's centre, so the order slot ^ octant (octant: the sign bits of
-// the ray direction) runs roughly front to back without sorting.  The stack
+// A node's words and its child slabs in the ray's frame: child plane q
+// lies at t = q * a + b per axis; the near and far plane words are chosen
+// per axis from the direction's sign.  The top `cached` nodes are read from
+// shared memory (sNodes), the rest through the read-only cache.
+struct NodeSlabs {
+    uint32_t childBase, triBase, meta0, meta1, imask;
+    float ax, ay, az, bx, by, bz;
+    uint32_t qn[6], qf[6];  // x0 x1 y0 y1 z0 z1: bytes of slots 0-3 and 4-7
+};
+
+__device__ __forceinline__ void node_slabs(const WideAccelDev& acc, const WideNode* sNodes,
+                                           int cached, int node, const WideRay& r,
+                                           NodeSlabs& s) {
+    uint4 w0, w1, w2, w3, w4;
+    if (node < cached) {
+        const uint4* sm = reinterpret_cast<const uint4*>(sNodes + node);
+        w0 = sm[0]; w1 = sm[1]; w2 = sm[2]; w3 = sm[3]; w4 = sm[4];
+    } else {
+        const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
+        w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
+        w4 = __ldg(g + 4);
+    }
+    const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+    const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    s.imask = w0.w >> 24;
+    // t = (lo + q*s - o) * inv = q * (s*inv) + (lo - o) * inv
+    s.ax = sx * r.inv.x;
+    s.ay = sy * r.inv.y;
+    s.az = sz * r.inv.z;
+    s.bx = (__uint_as_float(w0.x) - r.o.x) * r.inv.x;
+    s.by = (__uint_as_float(w0.y) - r.o.y) * r.inv.y;
+    s.bz = (__uint_as_float(w0.z) - r.o.z) * r.inv.z;
+    s.childBase = w1.x;
+    s.triBase = w1.y;
+    s.meta0 = w1.z;
+    s.meta1 = w1.w;
+    const bool px = r.inv.x >= 0.0f, py = r.inv.y >= 0.0f, pz = r.inv.z >= 0.0f;
+    s.qn[0] = px ? w2.x : w3.z; s.qn[1] = px ? w2.y : w3.w;
+    s.qf[0] = px ? w3.z : w2.x; s.qf[1] = px ? w3.w : w2.y;
+    s.qn[2] = py ? w2.z : w4.x; s.qn[3] = py ? w2.w : w4.y;
+    s.qf[2] = py ? w4.x : w2.z; s.qf[3] = py ? w4.y : w2.w;
+    s.qn[4] = pz ? w3.x : w4.z; s.qn[5] = pz ? w3.y : w4.w;
+    s.qf[4] = pz ? w4.z : w3.x; s.qf[5] = pz ? w4.w : w3.y;
+}
+
+// Entry and exit distance of child slot k (compile-time k).
+template <int k>
+__device__ __forceinline__ void child_span(const NodeSlabs& s, float tmin, float closest,
+                                           float& tn, float& tf) {
+    constexpr int h = k < 4 ? 0 : 1, kk = k & 3;
+    const float tnx = __fmaf_rn(float(byte_of(s.qn[0 + h], kk)), s.ax, s.bx);
+    const float tfx = __fmaf_rn(float(byte_of(s.qf[0 + h], kk)), s.ax, s.bx);
+    const float tny = __fmaf_rn(float(byte_of(s.qn[2 + h], kk)), s.ay, s.by);
+    const float tfy = __fmaf_rn(float(byte_of(s.qf[2 + h], kk)), s.ay, s.by);
+    const float tnz = __fmaf_rn(float(byte_of(s.qn[4 + h], kk)), s.az, s.bz);
+    const float tfz = __fmaf_rn(float(byte_of(s.qf[4 + h], kk)), s.az, s.bz);
+    tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+    tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
+}
+
+template <int k>
+__device__ __forceinline__ uint32_t meta_of(const NodeSlabs& s) {
+    return byte_of(k < 4 ? s.meta0 : s.meta1, k & 3);
+}
+
+// One node of the traversal in exact front-to-back order: the hit internal
+// children are sorted by entry distance, the nearest entered and the others
+// pushed one by one with their distance (entries beyond the closest hit are
+// dropped when popped); leaf children are tested as soon as their box is
+// hit.  False when the ray is done.
+template <bool kCount, int kStack>
+__device__ __forceinline__ bool visit_sorted(const WideAccelDev& acc, const WideNode* sNodes,
+                                             int cached, WideRay& r, uint2* stack,
+                                             uint32_t& nodeVisits, uint32_t& triTests,
+                                             uint32_t* errorFlag) {
+    if (kCount) nodeVisits++;
+    NodeSlabs s;
+    node_slabs(acc, sNodes, cached, r.node, r, s);
+    // internal children that are hit, keyed by entry distance:
+    // (distance bits with the low three cleared) | slot
+    uint32_t key[8];
+    auto child = [&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        key[k] = 0xFFFFFFFFu;
+        const uint32_t meta = meta_of<k>(s);
+        if (meta == 0u) return;
+        float tn, tf;
+        child_span<k>(s, r.tmin, r.closest, tn, tf);
+        if (!(tn <= tf)) return;
+        if (meta & 0x40u) {
+            if (kCount) triTests++;
+            tri_test(acc, s.triBase + (meta & 0x3Fu), r.o, r.d, r.tmin, r.closest, r.hitTri,
+                     r.hb0, r.hb1);
+        } else {
+            key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
+        }
+    };
+    child(IntC<0>{}); child(IntC<1>{}); child(IntC<2>{}); child(IntC<3>{});
+    child(IntC<4>{}); child(IntC<5>{}); child(IntC<6>{}); child(IntC<7>{});
+    sort8(key);
+    // push the farther hits (farthest first), enter the nearest
+    int next = -1;
+#pragma unroll
+    for (int j = 7; j >= 0; j--) {
+        if (key[j] == 0xFFFFFFFFu) continue;
+        const float tn = __uint_as_float(key[j] & ~7u);
+        if (tn > r.closest) continue;
+        const uint32_t slot = key[j] & 7u;
+        const uint32_t meta = byte_of(slot < 4 ? s.meta0 : s.meta1, int(slot & 3u));
+        const uint32_t c = s.childBase + (meta & 0x3Fu);
+        if (j == 0) {
+            next = int(c);
+        } else if (r.sp < kStack) {
+            stack[r.sp++] = make_uint2(c, key[j] & ~7u);
+        } else {
+            atomicExch(errorFlag, 3u);
+        }
+    }
+    // the nearest hit may lie beyond the closest triangle: fall through to
+    // the stack
+    while (next < 0 && r.sp > 0) {
+        const uint2 e = stack[--r.sp];
+        if (__uint_as_float(e.y) <= r.closest) next = int(e.x);
+    }
+    r.node = next;
+    return next >= 0;
+}
+
+// One node of the traversal in octant order: the collapse put every child
+// in the slot of its centroid's octant around the node's centre, so the
+// order slot ^ oct runs roughly front to back without sorting.  The stack
 // holds node groups: the child base of a visited node, its internal-child
 // mask and the bits of its hit internal children still to visit, one entry
 // per node however many children were hit.  A child's node index is the
-// child base plus the number of internal children in lower slots.
-// Triangles of leaf children are tested as soon as their box is hit.
+// child base plus the number of internal children in lower slots.  The
+// triangles of hit leaf children are tested after the eight box tests, so
+// the box tests carry no triangle test between them.  False when the ray
+// is done.
 template <bool kCount, int kStack>
-__device__ __forceinline__ void trace_wide_octant(const WideAccelDev& acc, const WideNode* sNodes,
-                                                  int cached, V3 o, V3 d, float tmin,
-                                                  float& closest, int& hitTri, float& hb0,
-                                                  float& hb1, uint32_t& nodeVisits,
-                                                  uint32_t& triTests, uint32_t* errorFlag) {
-    if (acc.triCount == 1) {
+__device__ __forceinline__ bool visit_octant(const WideAccelDev& acc, const WideNode* sNodes,
+                                             int cached, WideRay& r, uint2* stack,
+                                             uint32_t& nodeVisits, uint32_t& triTests,
+                                             uint32_t* errorFlag) {
+    if (kCount) nodeVisits++;
+    NodeSlabs s;
+    node_slabs(acc, sNodes, cached, r.node, r, s);
+    uint32_t hits = 0;      // bit (slot ^ oct) for each hit internal child
+    uint32_t leafHits = 0;  // bit slot for each hit leaf child
+    auto child = [&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const uint32_t meta = meta_of<k>(s);
+        if (meta == 0u) return;
+        float tn, tf;
+        child_span<k>(s, r.tmin, r.closest, tn, tf);
+        const bool hit = tn <= tf;
+        if (hit && (meta & 0x40u)) leafHits |= 1u << k;
+        if (hit && !(meta & 0x40u)) hits |= 1u << (uint32_t(k) ^ r.oct);
+    };
+    child(IntC<0>{}); child(IntC<1>{}); child(IntC<2>{}); child(IntC<3>{});
+    child(IntC<4>{}); child(IntC<5>{}); child(IntC<6>{}); child(IntC<7>{});
+    while (leafHits) {
+        const uint32_t k = uint32_t(__ffs(int(leafHits)) - 1);
+        leafHits &= leafHits - 1u;
+        const uint32_t meta = ((k < 4 ? s.meta0 : s.meta1) >> (8u * (k & 3u))) & 0xFFu;
         if (kCount) triTests++;
-        tri_test(acc, 0, o, d, tmin, closest, hitTri, hb0, hb1);
-    } else if (acc.triCount > 1) {
-        const V3 inv = {1.0f / safe_dir(d.x), 1.0f / safe_dir(d.y), 1.0f / safe_dir(d.z)};
-        const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) |
-                             (inv.z < 0.0f ? 4u : 0u);
-        uint2 stack[kStack];  // (child base, internal mask << 8 | pending hit bits)
-        int sp = 0;
-        int node = 0;
-        while (node >= 0) {
-            if (kCount) nodeVisits++;
-            uint4 w0, w1, w2, w3, w4;
-            if (node < cached) {
-                const uint4* sm = reinterpret_cast<const uint4*>(sNodes + node);
-                w0 = sm[0]; w1 = sm[1]; w2 = sm[2]; w3 = sm[3]; w4 = sm[4];
-            } else {
-                const uint4* g = reinterpret_cast<const uint4*>(acc.nodes + node);
-                w0 = __ldg(g); w1 = __ldg(g + 1); w2 = __ldg(g + 2); w3 = __ldg(g + 3);
-                w4 = __ldg(g + 4);
-            }
-            const float lx = __uint_as_float(w0.x), ly = __uint_as_float(w0.y),
-                        lz = __uint_as_float(w0.z);
-            const float sx = __uint_as_float((w0.w & 0xFFu) << 23);
-            const float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
-            const float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-            const uint32_t imask = w0.w >> 24;
-            const float ax = sx * inv.x, ay = sy * inv.y, az = sz * inv.z;
-            const float bx = (lx - o.x) * inv.x, by = (ly - o.y) * inv.y,
-                        bz = (lz - o.z) * inv.z;
-            const uint32_t childBase = w1.x, triBase = w1.y;
-            const uint32_t qnx0 = inv.x >= 0.0f ? w2.x : w3.z, qnx1 = inv.x >= 0.0f ? w2.y : w3.w;
-            const uint32_t qfx0 = inv.x >= 0.0f ? w3.z : w2.x, qfx1 = inv.x >= 0.0f ? w3.w : w2.y;
-            const uint32_t qny0 = inv.y >= 0.0f ? w2.z : w4.x, qny1 = inv.y >= 0.0f ? w2.w : w4.y;
-            const uint32_t qfy0 = inv.y >= 0.0f ? w4.x : w2.z, qfy1 = inv.y >= 0.0f ? w4.y : w2.w;
-            const uint32_t qnz0 = inv.z >= 0.0f ? w3.x : w4.z, qnz1 = inv.z >= 0.0f ? w3.y : w4.w;
-            const uint32_t qfz0 = inv.z >= 0.0f ? w4.z : w3.x, qfz1 = inv.z >= 0.0f ? w4.w : w3.y;
-            uint32_t hits = 0;  // bit (slot ^ oct) for each hit internal child
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const uint32_t meta = byte_of(k < 4 ? w1.z : w1.w, k & 3);
-                if (meta == 0u) continue;
-                const int kk = k & 3;
-                const float tnx = __fmaf_rn(float(byte_of(k < 4 ? qnx0 : qnx1, kk)), ax, bx);
-                const float tfx = __fmaf_rn(float(byte_of(k < 4 ? qfx0 : qfx1, kk)), ax, bx);
-                const float tny = __fmaf_rn(float(byte_of(k < 4 ? qny0 : qny1, kk)), ay, by);
-                const float tfy = __fmaf_rn(float(byte_of(k < 4 ? qfy0 : qfy1, kk)), ay, by);
-                const float tnz = __fmaf_rn(float(byte_of(k < 4 ? qnz0 : qnz1, kk)), az, bz);
-                const float tfz = __fmaf_rn(float(byte_of(k < 4 ? qfz0 : qfz1, kk)), az, bz);
-                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
-                if (!(tn <= tf)) continue;
-                if (meta & 0x40u) {  // leaf: test the triangle right away
-                    if (kCount) triTests++;
-                    tri_test(acc, triBase + (meta & 0x3Fu), o, d, tmin, closest, hitTri,
-                             hb0, hb1);
-                } else {
-                    hits |= 1u << (uint32_t(k) ^ oct);
-                }
-            }
-            uint32_t base = childBase, im = imask;
-            if (hits == 0) {  // resume the most recent group with pending children
-                if (sp == 0) break;
-                const uint2 e = stack[--sp];
-                base = e.x;
-                im = e.y >> 8;
-                hits = e.y & 0xFFu;
-            }
-            const uint32_t b = uint32_t(__ffs(int(hits)) - 1);
-            const uint32_t slot = b ^ oct;
-            hits &= hits - 1u;
-            if (hits) {
-                if (sp < kStack) stack[sp++] = make_uint2(base, (im << 8) | hits);
-                else atomicExch(errorFlag, 3u);
-            }
-            node = int(base + uint32_t(__popc(im & ((1u << slot) - 1u))));
-        }
+        tri_test(acc, s.triBase + (meta & 0x3Fu), r.o, r.d, r.tmin, r.closest, r.hitTri, r.hb0,
+                 r.hb1);
     }
+    uint32_t base = s.childBase, im = s.imask;
+    if (hits == 0) {  // resume the most recent group with pending children
+        if (r.sp == 0) {
+            r.node = -1;
+            return false;
+        }
+        const uint2 e = stack[--r.sp];
+        base = e.x;
+        im = e.y >> 8;
+        hits = e.y & 0xFFu;
+    }
+    const uint32_t b = uint32_t(__ffs(int(hits)) - 1);
+    const uint32_t slot = b ^ r.oct;
+    hits &= hits - 1u;
+    if (hits) {
+        if (r.sp < kStack) stack[r.sp++] = make_uint2(base, (im << 8) | hits);
+        else atomicExch(errorFlag, 3u);
+    }
+    r.node = int(base + uint32_t(__popc(im & ((1u << slot) - 1u))));
+    return true;
 }
 
-// Either order; kStack for the sorted order's per-child entries, kGroups
-// for the octant order's per-node groups.
-template <bool kCount, bool kOctant, int kStack, int kGroups>
-__device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const WideNode* sNodes,
-                                               int cached, V3 o, V3 d, float tmin,
-                                               float& closest, int& hitTri, float& hb0,
-                                               float& hb1, uint32_t& nodeVisits,
-                                               uint32_t& triTests, uint32_t* errorFlag) {
+template <bool kCount, bool kOctant, int kStack>
+__device__ __forceinline__ bool wide_visit(const WideAccelDev& acc, const WideNode* sNodes,
+                                           int cached, WideRay& r, uint2* stack,
+                                           uint32_t& nodeVisits, uint32_t& triTests,
+                                           uint32_t* errorFlag) {
     if (kOctant)
-        trace_wide_octant<kCount, kGroups>(acc, sNodes, cached, o, d, tmin, closest, hitTri, hb0,
-                                           hb1, nodeVisits, triTests, errorFlag);
-    else
-        trace_wide_sorted<kCount, kStack>(acc, sNodes, cached, o, d, tmin, closest, hitTri, hb0,
-                                          hb1, nodeVisits, triTests, errorFlag);
+        return visit_octant<kCount, kStack>(acc, sNodes, cached, r, stack, nodeVisits, triTests,
+                                            errorFlag);
+    return visit_sorted<kCount, kStack>(acc, sNodes, cached, r, stack, nodeVisits, triTests,
+                                        errorFlag);
+}
+
+// Stack entries per ray: the sorted order pushes one entry per child, the
+// octant order one per node group (at most one per level).
+template <bool kOctant>
+struct WideStack {
+    static constexpr int value = kOctant ? kWideGroups : kWideStack;
+};
+
+// Closest hit of one ray in one 8-wide tree, in either child order.
+template <bool kCount, bool kOctant, int kStack>
+__device__ __forceinline__ void trace_wide_ray(const WideAccelDev& acc, const WideNode* sNodes,
+                                               int cached, float4 ro, float4 rd, WideRay& r,
+                                               uint32_t& nodeVisits, uint32_t& triTests,
+                                               uint32_t* errorFlag) {
+    wide_ray_begin(r, ro, rd);
+    if (acc.triCount == 1) {
+        if (kCount) triTests++;
+        tri_test(acc, 0, r.o, r.d, r.tmin, r.closest, r.hitTri, r.hb0, r.hb1);
+    } else if (acc.triCount > 1) {
+        uint2 stack[kStack];
+        while (wide_visit<kCount, kOctant, kStack>(acc, sNodes, cached, r, stack, nodeVisits,
+                                                   triTests, errorFlag)) {
+        }
+    }
 }
 
 __device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut& out, uint32_t i,
@@ -525,6 +561,26 @@ __device__ __forceinline__ void write_hit(const WideAccelDev& acc, const HitOut&
     }
 }
 
+__device__ __forceinline__ void load_top_nodes(const WideAccelDev& acc, WideNode* sNodes,
+                                               int cached) {
+    for (int i = threadIdx.x; i < cached * 5; i += blockDim.x)
+        reinterpret_cast<uint4*>(sNodes)[i] = __ldg(reinterpret_cast<const uint4*>(acc.nodes) + i);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void add_work(unsigned long long* counters, uint32_t nodeVisits,
+                                         uint32_t triTests) {
+    unsigned long long a = nodeVisits, b = triTests;
+    for (int s = 16; s > 0; s >>= 1) {
+        a += __shfl_xor_sync(0xFFFFFFFFu, a, s);
+        b += __shfl_xor_sync(0xFFFFFFFFu, b, s);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters + 0, a);
+        atomicAdd(counters + 1, b);
+    }
+}
+
 // Nine 128-thread blocks per SM (56 registers, a few bytes spilled): the
 // traversal's dependent loads and ALU chains want resident warps more than
 // registers (measured on clusters-1M: 8 blocks 4.77 ms, 9 blocks 4.57 ms,
@@ -539,32 +595,88 @@ __global__ void __launch_bounds__(128, 9) k_trace_wide(WideAccelDev acc,
                                                     unsigned long long* counters) {
     __shared__ WideNode sNodes[kCachedNodes];
     const int cached = acc.nodeCount < uint32_t(kCachedNodes) ? int(acc.nodeCount) : kCachedNodes;
-    for (int i = threadIdx.x; i < cached * 5; i += blockDim.x)
-        reinterpret_cast<uint4*>(sNodes)[i] = __ldg(reinterpret_cast<const uint4*>(acc.nodes) + i);
-    __syncthreads();
+    load_top_nodes(acc, sNodes, cached);
     const uint32_t n = dCount ? *dCount : hCount;
     uint32_t nodeVisits = 0, triTests = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 ro = rayO[i], rd = rayD[i];
-        float closest = rd.w;
-        int hitTri = -1;
-        float hb0 = 0.0f, hb1 = 0.0f;
-        trace_wide_ray<kCount, kOctant, kWideStack, kWideGroups>(acc, sNodes, cached, V3{ro.x, ro.y, ro.z},
-                                           V3{rd.x, rd.y, rd.z}, ro.w, closest, hitTri, hb0, hb1,
-                                           nodeVisits, triTests, errorFlag);
-        write_hit(acc, out, i, hitTri, closest, hb0, hb1);
+        WideRay r;
+        trace_wide_ray<kCount, kOctant, WideStack<kOctant>::value>(
+            acc, sNodes, cached, rayO[i], rayD[i], r, nodeVisits, triTests, errorFlag);
+        write_hit(acc, out, i, r.hitTri, r.closest, r.hb0, r.hb1);
     }
-    if (kCount) {
-        unsigned long long a = nodeVisits, b = triTests;
-        for (int s = 16; s > 0; s >>= 1) {
-            a += __shfl_xor_sync(0xFFFFFFFFu, a, s);
-            b += __shfl_xor_sync(0xFFFFFFFFu, b, s);
+    if (kCount) add_work(counters, nodeVisits, triTests);
+}
+
+// Lanes refilled: a lane whose ray is done takes its warp's next ray once
+// kRefillLanes lanes (or all) are idle, so a warp of rays with uneven path
+// lengths keeps its lanes busy until its rays run out.  Warp w owns the
+// 32-ray chunks w, w + W, w + 2W, ... (W warps in the grid) and hands their
+// rays out in order; the set of rays a warp traces is the same as without
+// refilling, only the lanes they run on differ.  Refilling mixes rays of
+// neighbouring chunks in one warp: a gain for the scattered rays of later
+// bounces, a loss for coherent camera rays (measured per depth by the
+// tracer's order tuning).
+constexpr int kRefillLanes = 8;
+
+template <bool kCount, bool kOctant>
+__global__ void __launch_bounds__(128, 9) k_trace_wide_refill(WideAccelDev acc,
+                                                           const float4* __restrict__ rayO,
+                                                           const float4* __restrict__ rayD,
+                                                           const uint32_t* __restrict__ dCount,
+                                                           uint32_t hCount, HitOut out,
+                                                           uint32_t* errorFlag,
+                                                           unsigned long long* counters) {
+    constexpr int kStack = WideStack<kOctant>::value;
+    __shared__ WideNode sNodes[kCachedNodes];
+    const int cached = acc.nodeCount < uint32_t(kCachedNodes) ? int(acc.nodeCount) : kCachedNodes;
+    load_top_nodes(acc, sNodes, cached);
+    const uint32_t n = dCount ? *dCount : hCount;
+    uint32_t nodeVisits = 0, triTests = 0;
+    if (acc.triCount < 2) {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += gridDim.x * blockDim.x) {
+            WideRay r;
+            trace_wide_ray<kCount, kOctant, kStack>(acc, sNodes, cached, rayO[i], rayD[i], r,
+                                                    nodeVisits, triTests, errorFlag);
+            write_hit(acc, out, i, r.hitTri, r.closest, r.hb0, r.hb1);
         }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(counters + 0, a);
-            atomicAdd(counters + 1, b);
+    } else {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint64_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint64_t nWarps = (gridDim.x * blockDim.x) >> 5;
+        uint32_t next = 0;  // rays of the warp's sequence handed out (warp-uniform)
+        bool more = warp * 32u < n, active = false;
+        uint32_t ri = 0;
+        WideRay r;
+        r.node = -1;
+        uint2 stack[kStack];
+        while (true) {
+            if (more) {
+                const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
+                if (__popc(need) >= kRefillLanes || need == 0xFFFFFFFFu) {
+                    if (!active) {
+                        const uint32_t j = next + uint32_t(__popc(need & ((1u << lane) - 1u)));
+                        const uint64_t idx = (warp + uint64_t(j >> 5) * nWarps) * 32u + (j & 31u);
+                        if (idx < n) {
+                            ri = uint32_t(idx);
+                            wide_ray_begin(r, rayO[ri], rayD[ri]);
+                            active = true;
+                        }
+                    }
+                    next += uint32_t(__popc(need));
+                    more = (warp + uint64_t(next >> 5) * nWarps) * 32u + (next & 31u) < n;
+                }
+            }
+            if (!__any_sync(0xFFFFFFFFu, active)) break;
+            if (!active) continue;
+            if (!wide_visit<kCount, kOctant, kStack>(acc, sNodes, cached, r, stack, nodeVisits,
+                                                     triTests, errorFlag)) {
+                write_hit(acc, out, ri, r.hitTri, r.closest, r.hb0, r.hb1);
+                active = false;
+            }
         }
     }
+    if (kCount) add_work(counters, nodeVisits, triTests);
 }
 
 // Rays of many scenes: each ray's tree is its job's (RayAux::pad is the job
@@ -582,14 +694,10 @@ __global__ void __launch_bounds__(kBlock) k_trace_wide_jobs(const JobDev* __rest
     uint32_t nodeVisits = 0, triTests = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const WideAccelDev acc = jobs[aux[i].pad].wide;
-        const float4 ro = rayO[i], rd = rayD[i];
-        float closest = rd.w;
-        int hitTri = -1;
-        float hb0 = 0.0f, hb1 = 0.0f;
-        trace_wide_ray<false, kOctant, kStack, kWideGroups>(acc, nullptr, 0, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z},
-                                      ro.w, closest, hitTri, hb0, hb1, nodeVisits, triTests,
-                                      errorFlag);
-        write_hit(acc, out, i, hitTri, closest, hb0, hb1);
+        WideRay r;
+        trace_wide_ray<false, kOctant, kOctant ? kWideGroups : kStack>(
+            acc, nullptr, 0, rayO[i], rayD[i], r, nodeVisits, triTests, errorFlag);
+        write_hit(acc, out, i, r.hitTri, r.closest, r.hb0, r.hb1);
     }
 }
 
@@ -648,20 +756,23 @@ int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4
     if (maxCount == 0) return 0;
     uint32_t blocks = (maxCount + 127) / 128;
     blocks = blocks < 148u * 16u ? blocks : 148u * 16u;
-    if (order == 1) {
-        if (counters)
-            k_trace_wide<true, true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
-                                                                 out, errorFlag, counters);
-        else
-            k_trace_wide<false, true><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
-                                                                  out, errorFlag, nullptr);
-    } else {
-        if (counters)
-            k_trace_wide<true, false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount,
-                                                                  out, errorFlag, counters);
-        else
-            k_trace_wide<false, false><<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount,
-                                                                   maxCount, out, errorFlag, nullptr);
+    auto go = [&](auto kernel) {
+        kernel<<<blocks, 128, 0, stream>>>(acc, rayO, rayD, dCount, maxCount, out, errorFlag,
+                                           counters);
+    };
+    const bool c = counters != nullptr;
+    switch (order) {
+        case kWideSorted: c ? go(k_trace_wide<true, false>) : go(k_trace_wide<false, false>); break;
+        case kWideOctant: c ? go(k_trace_wide<true, true>) : go(k_trace_wide<false, true>); break;
+        case kWideSortedRefill:
+            c ? go(k_trace_wide_refill<true, false>) : go(k_trace_wide_refill<false, false>);
+            break;
+        case kWideOctantRefill:
+            c ? go(k_trace_wide_refill<true, true>) : go(k_trace_wide_refill<false, true>);
+            break;
+        default:
+            set_error("wide traversal: order %d unknown", order);
+            return MRB_E_ARG;
     }
     MRB_CUDA(cudaGetLastError());
     return 0;
@@ -704,11 +815,12 @@ int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStrea
     cudaEvent_t e[2];
     cudaEventCreate(&e[0]);
     cudaEventCreate(&e[1]);
-    float best[2] = {1e30f, 1e30f};
+    float best[kWideOrders];
+    for (float& b : best) b = 1e30f;
     int rc = 0;
     k_probe_rays<<<(kProbe + 255) / 256, 256, 0, st>>>(dExtent, kProbe, ro, rd);
     for (int rep = 0; rep < 4 && rc == 0; rep++)
-        for (int order = 0; order < 2 && rc == 0; order++) {
+        for (int order = 0; order < kWideOrders && rc == 0; order++) {
             cudaEventRecord(e[0], st);
             rc = trace_closest_wide(acc, ro, rd, nullptr, kProbe, ho, err, st, nullptr, order);
             cudaEventRecord(e[1], st);
@@ -722,11 +834,12 @@ int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStrea
     cudaFree(buf);
     if (rc) return rc;
     MRB_CUDA(cudaGetLastError());
-    *orderOut = best[1] < best[0] ? 1 : 0;
-    if (msOut) {
-        msOut[0] = best[0];
-        msOut[1] = best[1];
-    }
+    int pick = 0;
+    for (int o = 1; o < kWideOrders; o++)
+        if (best[o] < best[pick]) pick = o;
+    *orderOut = pick;
+    if (msOut)
+        for (int o = 0; o < kWideOrders; o++) msOut[o] = best[o];
     return 0;
 }
 

@@ -41,15 +41,25 @@ size_t wide_scratch_bytes(uint32_t n);
 // into tv0/te0/te1 (n each).  Synchronises the stream every 8 levels.
 int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0, float4* te1,
                void* scratch, uint32_t* nodeCountOut, cudaStream_t stream);
-// order 0: children in exact front-to-back order (sorted entry distances,
-// per-child stack entries); 1: octant order with per-node group entries.
+// Traversal kernels of the 8-wide layout.  Sorted: children in exact
+// front-to-back order (sorted entry distances, per-child stack entries).
+// Octant: children in the order slot ^ (ray octant), per-node group stack
+// entries.  Refill: the same orders with a warp's idle lanes taking its next
+// rays.
+enum WideOrder : int {
+    kWideSorted = 0,
+    kWideOctant = 1,
+    kWideSortedRefill = 2,
+    kWideOctantRefill = 3,
+    kWideOrders = 4
+};
 int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
                        const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
                        uint32_t* errorFlag, cudaStream_t stream,
                        unsigned long long* counters = nullptr, int order = 0);
-// Times both orders on 65,536 seeded rays over the scene box (device
-// extent: min xyz, max xyz) and returns the faster; msOut[2] (may be null)
-// the best times.
+// Times every traversal kernel on 65,536 seeded rays over the scene box
+// (device extent: min xyz, max xyz) and returns the fastest; msOut
+// (kWideOrders entries, may be null) the best times.
 int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStream_t stream,
                         int* orderOut, float* msOut);
 

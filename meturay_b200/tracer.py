@@ -22,6 +22,11 @@ import numpy as np
 from ._lib import Camera, Material, MrbError, SceneDesc, check, lib
 from .scenes import Scene
 
+# traversal kernels of the 8-wide layout (MRB_WIDE_SORTED ..
+# MRB_WIDE_OCTANT_REFILL), and the automatic choice (MRB_WIDE_AUTO)
+WIDE_ORDERS = ("sorted", "octant", "sorted_refill", "octant_refill")
+WIDE_AUTO = 4
+
 __all__ = ["TracerSystem", "GPUScene", "PathTracer", "WFPGTracer", "MrbError"]
 
 
@@ -166,18 +171,24 @@ class GPUScene:
                 "wide_tree": "ploc" if ext[0] == 1 else "lbvh", "ploc_steps": int(ext[1]),
                 "inner_area_lbvh": float(areas[0]), "inner_area_ploc": float(areas[1])}
 
-    def set_wide_order(self, order: int):
-        """Child order of the 8-wide traversal: 0 sorted, 1 octant, 2 (default)
-        the faster one, timed on seeded probe rays at construction and then
-        on a tracer's own rays in the frame before it captures its graph."""
+    def set_wide_order(self, order):
+        """Traversal kernel of the 8-wide layout: "sorted", "octant",
+        "sorted_refill", "octant_refill" (or 0-3), or "auto" (4, default):
+        the fastest, timed on seeded probe rays at construction and then per
+        depth on a tracer's own rays in the frame before it captures its
+        graph."""
+        if isinstance(order, str):
+            order = WIDE_AUTO if order == "auto" else WIDE_ORDERS.index(order)
         check(lib.mrb_accel_set_wide_order(self._h, int(order)))
 
     def wide_order(self) -> dict:
+        """The kernel in use where no tracer tuned its own, and the last
+        measured ms per kernel."""
         o = C.c_int(0)
-        ms = np.zeros(2, np.float32)
+        ms = np.zeros(len(WIDE_ORDERS), np.float32)
         check(lib.mrb_accel_wide_order(self._h, C.byref(o), _ptr(ms)))
-        return {"order": "octant" if o.value == 1 else "sorted",
-                "ms_sorted": float(ms[0]), "ms_octant": float(ms[1])}
+        return {"order": WIDE_ORDERS[o.value],
+                "ms": {k: float(v) for k, v in zip(WIDE_ORDERS, ms)}}
 
     def set_wide_tree(self, tree: int):
         """Before construct_accelerators: the tree collapsed into the 8-wide
@@ -361,6 +372,15 @@ class PathTracer:
 
     def launches_per_frame(self) -> int:
         return check(lib.mrb_tracer_launches_per_frame(self._h))
+
+    def wide_orders(self) -> list:
+        """The 8-wide traversal kernel of each depth (names; None with the
+        binary traversal)."""
+        buf = (C.c_int * 256)()
+        n = lib.mrb_tracer_wide_orders(self._h, buf, 256)
+        if n < 0:
+            check(n)
+        return [WIDE_ORDERS[buf[i]] if buf[i] >= 0 else None for i in range(n)]
 
     def profile_frame(self) -> dict:
         """One stepwise frame with per-stage CUDA-event timings and work counts."""

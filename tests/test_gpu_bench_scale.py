@@ -6,9 +6,9 @@ that the bench renders at 1920x1080, 1 sample per pixel, depth 8.
   parent, inner AABBs, root) bit-exact against the oracle;
 * closest hits of the frame's camera rays (every 4th column of every 4th
   row: 129,600 rays): the binary layout bit-exact against the oracle's
-  traversal of the same tree; the 8-wide layout, in sorted and in octant
-  child order, with the same hit/miss and the same closest distance bit for
-  bit, primitives differing only at ties (at most 0.1 % of rays);
+  traversal of the same tree; the 8-wide layout, with every traversal
+  kernel, with the same hit/miss and the same closest distance bit for bit,
+  primitives differing only at ties (at most 0.1 % of rays);
 * per-sample radiance of a band of 32 rows of the bench frame within the
   drop-in's 1e-4 relative mean error.
 
@@ -73,13 +73,14 @@ def _camera_rays(scene, step=4):
     return rays
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", ["binary", "sorted", "octant", "sorted_refill",
+                                  "octant_refill"])
 def test_camera_closest_hits_at_full_size(big, cuda, mode):
     torch = cuda
     scene, g, os_ = big
-    g.set_traversal(min(mode, 1))
-    if mode >= 1:
-        g.set_wide_order(mode - 1)  # 1: sorted child order, 2: octant order
+    g.set_traversal(0 if mode == "binary" else 1)
+    if mode != "binary":
+        g.set_wide_order(mode)
     rays = _camera_rays(scene)
     n = rays.shape[0]
     assert n >= 100_000
@@ -94,7 +95,7 @@ def test_camera_closest_hits_at_full_size(big, cuda, mode):
           db.data_ptr())
     torch.cuda.synchronize()
     g.set_traversal(1)
-    g.set_wide_order(2)
+    g.set_wide_order("auto")
     gk = dk.cpu().numpy().view(np.uint32)
     gp = dp.cpu().numpy().view(np.uint32)
     gt = dt.cpu().numpy()
@@ -104,7 +105,7 @@ def test_camera_closest_hits_at_full_size(big, cuda, mode):
     assert np.array_equal(gp != 0xFFFFFFFF, hit)
     assert np.array_equal(gt[hit].view(np.uint32), t[hit].view(np.uint32))
     same = gp == prim
-    if mode == 0:
+    if mode == "binary":
         assert same.all()
     else:
         assert (~same).sum() <= n // 1000, f"{(~same).sum()} ties"

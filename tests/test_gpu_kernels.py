@@ -110,9 +110,11 @@ def test_radix_sort_u32(cuda, oracle, n, bits, desc):
     assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev)
 
 
-def _build(system, scene):
+def _build(system, scene, tree=None):
     from meturay_b200 import GPUScene
     g = GPUScene(system, scene)
+    if tree is not None:
+        g.set_wide_tree(tree)
     g.construct_accelerators()
     return g
 
@@ -164,22 +166,30 @@ def _rays_for(scene, n, seed):
     return rays
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+KERNELS = ("sorted", "octant", "sorted_refill", "octant_refill")
+WIDE = {f"{tree}-{k}": (t, k) for t, tree in enumerate(("lbvh", "ploc")) for k in KERNELS}
+
+
+@pytest.mark.parametrize("mode", ["binary"] + list(WIDE))
 @pytest.mark.parametrize("name,make", _scenes())
 def test_trace_closest_hit(system, cuda, oracle, name, make, mode):
-    """mode 0: binary LBVH nodes, bit-exact against the oracle's traversal of
-    the same tree.  modes 1 and 2: 8-wide quantised nodes in sorted and in
-    octant child order; same hit/miss and the same closest distance bit for
-    bit, same primitive except at ties."""
+    """binary: the LBVH nodes, bit-exact against the oracle's traversal of
+    the same tree.  The 8-wide quantised nodes, collapsed from the LBVH or
+    from the PLOC tree, with every traversal kernel (sorted and octant
+    child order, with and without refilled lanes): same hit/miss and the
+    same closest distance bit for bit, same primitive except at ties."""
     torch = cuda
     scene = make()
-    g = _build(system, scene)
-    g.set_traversal(min(mode, 1))
-    if mode >= 1:
-        g.set_wide_order(mode - 1)
+    tree, order = WIDE.get(mode, (None, None))
+    g = _build(system, scene, tree)
+    g.set_traversal(0 if tree is None else 1)
+    if order is not None:
+        g.set_wide_order(order)
     info = g.accel_info()
     if scene.triangle_count > 1:
         assert 0 < info["wide_nodes"] <= scene.triangle_count - 1
+        if tree is not None:
+            assert info["wide_tree"] == ("ploc" if tree == 1 else "lbvh")
     os_ = oracle.OracleScene.from_scene(scene)
     n = 20000
     rays = _rays_for(scene, n, seed=11)
@@ -202,7 +212,7 @@ def test_trace_closest_hit(system, cuda, oracle, name, make, mode):
     assert np.array_equal(gp != 0xFFFFFFFF, hit)
     assert np.array_equal(gt[hit].view(np.uint32), t[hit].view(np.uint32))
     same = gp == prim
-    if mode == 0:
+    if mode == "binary":
         assert same.all()
     else:
         assert (~same).sum() <= max(2, n // 1000), f"{(~same).sum()} ties"
