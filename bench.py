@@ -65,6 +65,39 @@ def _traffic_per_launch(traversal):
     return int(m.group(1)) if m else None
 
 
+# Algorithmic bytes of the traversal (per unit): per ray 72 B (ray 32 + id 4
+# + key 4 in; tMax 4 + key 4 + transform 4 + primitive 8 + barycentrics 8 +
+# status 4 out), per node visited its node bytes (8-wide quantised 80 B,
+# binary LBVH 64 B), per triangle tested 36 B (three vertices).
+RAY_BYTES, TRI_BYTES = 72, 36
+NODE_BYTES = {0: 64, 1: 80}
+
+
+def trace_bytes(rays: float, visits: float, tris: float, traversal: int) -> float:
+    return RAY_BYTES * rays + NODE_BYTES[traversal] * visits + TRI_BYTES * tris
+
+
+def _trace_roofline(t, prof: dict, traversal: int, traffic, peak: float,
+                    peak_kind: str) -> dict:
+    """Roofline of the traversal kernels over one profiled frame: the
+    algorithmic bytes of the frame's rays, node visits and triangle tests
+    (counted by the counting form of the kernels the frame runs) over the
+    frame's traversal time."""
+    tb = trace_bytes(prof["rays"], prof["node_visits"], prof["tri_tests"], traversal)
+    ts = prof["trace_ms"] / 1e3
+    achieved = tb / ts / 1e9 if ts > 0 else 0.0
+    return {"bound": "hbm",
+            "kernel": "k_trace_wide / k_trace_wide_refill" if traversal == 1 else "k_trace",
+            "kernel_per_depth": t.wide_orders() if traversal == 1 else None,
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_frame": tb, "rays_per_frame": prof["rays"],
+            "trace_ms_per_frame": prof["trace_ms"],
+            "launches_per_frame": prof.get("trace_launches"),
+            "node_visits_per_ray": prof["node_visits"] / max(prof["rays"], 1),
+            "tri_tests_per_ray": prof["tri_tests"] / max(prof["rays"], 1)}
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -222,6 +255,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         serving = run_serving(args, m, system)
     learned = run_learned(args, m, system, torch) \
         if (args.learned and args.only == "all" and rank == 0 and world == 1) else None
+    closed = run_closed(args, m, system, torch) \
+        if (args.closed and args.only == "all" and rank == 0 and world == 1) else None
 
     if dist:
         ms, e2e_ms, rays, e2e_rays = aggregate_ranks(dist, torch, ms, e2e_ms, rays, e2e_rays,
@@ -230,16 +265,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         return None
 
     peak, peak_kind = _peaks()
-    # algorithmic bytes of the traversal: per ray 32 B in (origin/tMin,
-    # direction/tMax) + 20 B out (key, prim, t, barycentrics); per node
-    # visited 80 B (8-wide quantised) or 64 B (binary); per triangle tested
-    # 48 B (v0, e0, e1)
-    node_bytes = 80 if args.traversal == 1 else 64
-    trace_bytes = (52 * prof["rays"] + node_bytes * prof["node_visits"]
-                   + 48 * prof["tri_tests"])
-    trace_s = prof["trace_ms"] / 1e3
-    achieved = trace_bytes / trace_s / 1e9 if trace_s > 0 else 0.0
-    traffic = _traffic_per_launch(args.traversal)
+    roof = _trace_roofline(t, prof, args.traversal, _traffic_per_launch(args.traversal), peak,
+                           peak_kind)
+    roof["stage_ms"] = {k: prof[k] for k in ("camera_ms", "trace_ms", "partition_ms", "shade_ms",
+                                             "resolve_ms")}
     return {
         "metric": METRIC,
         "value": rays / (ms / 1e3) / 1e6,
@@ -259,21 +288,11 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "mpaths_per_s": scene.width * scene.height * world * args.steps / ms / 1e3,
         "e2e": {"value": e2e_rays / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
                 "h2d_bytes_per_step": cam_bytes, "d2h_bytes_per_step": img_bytes},
-        "roofline": {"bound": "hbm",
-                     "kernel": "k_trace_wide" if args.traversal == 1 else "k_trace",
-                     "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_frame": trace_bytes,
-                     "trace_ms_per_frame": prof["trace_ms"],
-                     "launches_per_frame": prof["trace_launches"],
-                     "stage_ms": {k: prof[k] for k in ("camera_ms", "trace_ms", "partition_ms",
-                                                       "shade_ms", "resolve_ms")},
-                     "node_visits_per_ray": prof["node_visits"] / max(prof["rays"], 1),
-                     "tri_tests_per_ray": prof["tri_tests"] / max(prof["rays"], 1)},
+        "roofline": roof,
         "gpu_launches": launches,
         "clocks": clk,
         "guided": guided,
+        "closed_scene": closed,
         "batching": batching,
         "serving": serving,
         "learned": learned,
@@ -378,10 +397,13 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
     ms = e0.elapsed_time(e1)
     r1, _ = t.stats()
     guided_ms = ms / steps
+    stages = [t.profile_stages() for _ in range(3)]
     out = {"metric": METRIC, "value": (r1 - r0) / (ms / 1e3) / 1e6, "unit": "Mrays/s",
            "steps": steps, "ms_per_step": guided_ms,
            "rays_per_step": (r1 - r0) / steps,
            "launches_per_frame": t.launches_per_frame(),
+           "stage_ms": {k: float(np.mean([x[k] for x in stages]))
+                        for k in stages[0] if k.endswith("_ms")},
            "config": {"tracer": "WFPGTracer", **{k: v for k, v in GUIDED_OPTS.items()},
                       **GUIDED_FLOATS,
                       "field": "64x64 at depths 0-1, then 32x32, 16x16, 8x8",
@@ -460,6 +482,56 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
                 "(other seeds), whose own variance is subtracted from every MSE (mse_raw keeps "
                 "it); the guided tracer starts with a cold octree, and its build and every "
                 "frame count against the budget (device time)"}
+    return out
+
+
+# ---- bounce-heavy closed scene -------------------------------------------
+CLOSED = {"Samples": 4, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
+          "DirectLightMIS": 0}
+STAGES5 = ("camera_ms", "trace_ms", "partition_ms", "shade_ms", "resolve_ms")
+
+
+def run_closed(args, m, system, torch) -> dict:
+    """The plain tracer on a closed scene at a resolution that fills the GPU:
+    the Cornell box (seed 1, 7,692 triangles) at 1920x1080, 4 spp per frame,
+    depth 5, NEE, Tent filter.  Every camera ray hits and most paths bounce
+    to the last depth, so partition, shading and incoherent secondary rays
+    carry the frame; reported with its stage split and traversal roofline."""
+    scene = m.scenes.cornell(seed=1, width=1920, height=1080)
+    g = m.GPUScene(system, scene)
+    g.construct_accelerators()
+    g.set_traversal(args.traversal)
+    t = m.PathTracer(system, g)
+    t.set_options(dict(CLOSED, Seed=5))
+    _attach_filter(system, t)
+    stream = torch.cuda.ExternalStream(t.stream)
+    for _ in range(max(3, args.warmup)):
+        t.render_frame()
+    torch.cuda.synchronize()
+    steps = max(5, min(args.steps, 20))
+    r0, _ = t.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        t.render_frame()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    r1, _ = t.stats()
+    profs = [t.profile_frame() for _ in range(3)]
+    prof = {k: float(np.mean([x[k] for x in profs])) for k in profs[0]}
+    peak, peak_kind = _peaks()
+    roof = _trace_roofline(t, prof, args.traversal, None, peak, peak_kind)
+    total = sum(prof[k] for k in STAGES5)
+    out = {"metric": METRIC, "value": (r1 - r0) / (ms / 1e3) / 1e6, "unit": "Mrays/s",
+           "steps": steps, "ms_per_step": ms / steps, "rays_per_step": (r1 - r0) / steps,
+           "camera_rays_per_step": scene.width * scene.height * CLOSED["Samples"],
+           "stage_ms": {k: prof[k] for k in STAGES5},
+           "stage_share": {k: prof[k] / total for k in STAGES5},
+           "roofline": roof,
+           "config": {"scene": "Cornell box (seed 1), 7,692 triangles", "resolution": "1920x1080",
+                      **CLOSED, "recon_filter": "Tent, radius 1 pixel"}}
+    t.close()
     return out
 
 
@@ -839,6 +911,8 @@ def main():
     ap.add_argument("--pool-block", type=int, default=0)
     ap.add_argument("--pool-stack", type=int, default=128,
                     help="traversal stack of the pool: 64 or 128 (sorted order) or 0 (octant order)")
+    ap.add_argument("--no-closed", dest="closed", action="store_false",
+                    help="skip the bounce-heavy Cornell 1080p 4 spp entry")
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the learned-guiding equal-time MSE comparison")
     ap.add_argument("--learned-budget-ms", type=float, default=1000.0)
@@ -878,16 +952,35 @@ def main():
         os_ = _oracle_setup(scene)
         cores = os.cpu_count() or 1
         cpu_leg(scene, os_, 0, cores)  # warm-up
+        from oracle import oracle as o
+        o.trace_counters(reset=True)
         steps = 2 * CPU_ROW_STRIDE
         tot_r, tot_s = 0, 0.0
         for i in range(steps):
             r = cpu_leg(scene, os_, i, cores)
             tot_r += r["rays"]
             tot_s += r["seconds"]
+        visits, tris = o.trace_counters()
         out["cpu_baseline"] = {"value": tot_r / tot_s / 1e6, "unit": "Mrays/s",
                                "cores": cores, "kind": "port",
                                "sample": cpu_sample_text(scene, steps, cores)
                                + f", {tot_s:.1f} s"}
+        # the same frame's work counted independently of the GPU kernels: the
+        # oracle's traversal of the reference's binary LBVH over the CPU
+        # sample's rays, scaled to the GPU frame's ray count
+        roof = out["roofline"]
+        vpr, tpr = visits / max(tot_r, 1), tris / max(tot_r, 1)
+        nr = roof["rays_per_frame"]
+        tb = trace_bytes(nr, vpr * nr, tpr * nr, 0)
+        ach = tb / (roof["trace_ms_per_frame"] / 1e3) / 1e9
+        roof["reference_tree"] = {
+            "source": "oracle traversal of the binary LBVH (the reference's tree and "
+                      "traversal order) over the cpu_baseline sample's rays",
+            "node_visits_per_ray": vpr, "tri_tests_per_ray": tpr,
+            "algorithmic_bytes_per_frame": tb, "achieved": ach, "frac": ach / roof["peak"],
+            "note": "the reference tree's work done in the 8-wide kernels' time; above 1.0 "
+                    "where the 8-wide layout visits fewer, smaller nodes than the binary "
+                    "tree would stream"}
     if out is not None:
         print(json.dumps(out))
     if dist:

@@ -145,8 +145,9 @@ int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
 /* Traversal kernel of the 8-wide layout.  Child order: sorted (exact
  * front to back: entry distances sorted, one stack entry per pushed child)
  * or octant (the collapse places children by the octant of their centroid,
- * visited in the order slot ^ ray octant; one stack entry per node group,
- * leaf triangles tested after the node's box tests).  Refill: a warp's idle
+ * visited in the order slot ^ ray octant; one stack entry per node group).
+ * Either tests the triangles of a node's hit leaves after its eight box
+ * tests.  Refill: a warp's idle
  * lanes take its next rays once eight of them are idle (a gain where path
  * lengths differ, a loss for coherent camera rays).  MRB_WIDE_AUTO
  * (default): the fastest kernel, timed first on 65,536 seeded rays over the

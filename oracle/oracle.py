@@ -76,6 +76,7 @@ def _load():
     lib.oracle_bvh_root.argtypes = [vp]
     lib.oracle_trace.argtypes = [C.POINTER(Scene), vp, vp, u32, vp, vp, vp, vp, u32]
     lib.oracle_trace_linear.argtypes = [C.POINTER(Scene), vp, u32, vp, vp, vp, vp, u32]
+    lib.oracle_trace_counters.argtypes = [vp, C.c_int]
     lib.oracle_render.restype = C.c_uint64
     lib.oracle_render.argtypes = [C.POINTER(Scene), vp, C.POINTER(Camera), C.POINTER(Options), vp]
     lib.oracle_render_f64.restype = C.c_uint64
@@ -127,6 +128,15 @@ def lbvh(sorted_codes: np.ndarray, sorted_idx: np.ndarray, leaf_aabbs: np.ndarra
                                _p(out["inner"]), _p(out["root"]))
     out["status"] = st
     return out
+
+
+def trace_counters(reset: bool = False) -> tuple[int, int]:
+    """Inner LBVH nodes entered and triangles tested by the oracle's
+    traversal (OracleScene.trace / render, all threads) since the last reset;
+    reset=True zeroes them after reading."""
+    out = np.zeros(2, np.uint64)
+    lib.oracle_trace_counters(_p(out), 1 if reset else 0)
+    return int(out[0]), int(out[1])
 
 
 def partition(keys: np.ndarray, batch_bits: int, id_bits: int):
