@@ -181,6 +181,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     scene = m.scenes.clusters(seed=1, width=args.res[0], height=args.res[1])
     system = m.TracerSystem(dev)
     g = m.GPUScene(system, scene)
+    g.set_wide_order(args.wide_order)
     g.construct_accelerators()
     g.set_traversal(args.traversal)
     if args.only == "guided":
@@ -410,6 +411,77 @@ def run_guided(args, g, m, torch, dev: int) -> dict:
                       "leaf_radiance": "64-bit fixed-point sums (2^-24), FP16 averages"}}
     if args.mse_budget_ms <= 0:
         return out
+    # ---- equal-time MSE ----
+    # The converged render is the plain tracer with NEE and MIS (the same
+    # expectation as every estimator below, at far lower variance: NEE
+    # without MIS throws fireflies off glossy lobes and next to the lights,
+    # which would make a reference of that estimator noisier than the runs
+    # it scores).
+    def make_ref(half):
+        r = m.PathTracer(g.system, g)
+        r.set_options(dict(OPTS, DirectLightMIS=1, Seed=99 + 1000 * half))
+        _attach_filter(g.system, r)
+        return r
+    ref_img, ref_var, ref_rvar = _reference(make_ref, args.mse_reference_spp)
+    budget = float(args.mse_budget_ms)
+
+    def run(kind, opts, floats, seed):
+        def make(sd):
+            t = (m.PathTracer if kind == "plain" else m.WFPGTracer)(g.system, g)
+            t.set_options(dict(opts, Seed=sd))
+            if floats:
+                t.set_options(floats)
+            _attach_filter(g.system, t)
+            return t
+        probe = make(seed + 500)
+        for _ in range(5):
+            probe.render_frame()
+        est = _frame_ms(probe, torch, frames=10)
+        probe.close()
+        t = make(seed)   # a cold start: the octree build counts against the budget
+        img, frames, used = _budget_image(t, budget, est, torch)
+        t.close()
+        raw = float(np.mean((img - ref_img) ** 2))
+        return {"frames": frames, "ms_per_frame": est, "device_ms": used,
+                "mse": raw - ref_var, "mse_raw": raw, "mse_x_frames": (raw - ref_var) * frames,
+                "rel_mse": _rel_mse(img, ref_img) - ref_rvar,
+                "clamped_mse": _clamped_mse(img, ref_img)}
+
+    mis = {"DirectLightMIS": 1}
+    nonee = {"NextEventEstimation": 0}
+    runs = {
+        # the configured options (the reference's defaults: NEE, no MIS)
+        "plain": ("plain", OPTS, None),
+        "guided": ("wfpg", GUIDED_OPTS, GUIDED_FLOATS),
+        "wfpg_unguided": ("wfpg", dict(GUIDED_OPTS, SkipPG=1), GUIDED_FLOATS),
+        # NEE with MIS (the plain tracer only: with MIS the guided tracers
+        # are biased, the NEE weight using the BxDF pdf and the guided path
+        # ray the mixture pdf, WFPGTracerKC.cuh:338-347)
+        "plain_mis": ("plain", dict(OPTS, **mis), None),
+        # NEE off, as the reference's own WFPG configurations run
+        # (WorkingDir/tConf_veach_product.json)
+        "plain_nonee": ("plain", dict(OPTS, **nonee), None),
+        "guided_nonee": ("wfpg", dict(GUIDED_OPTS, **nonee), GUIDED_FLOATS),
+        "guided_nonee_bounce1": ("wfpg", dict(GUIDED_OPTS, GuideBounceAmount=1, **nonee),
+                                 GUIDED_FLOATS),
+    }
+    res = {k: run(kind, o, f, 7 + i) for i, (k, (kind, o, f)) in enumerate(runs.items())}
+
+    def ratio(a, b):
+        return res[a]["mse"] / res[b]["mse"] if res[b]["mse"] > 0 else None
+
+    out["equal_time_mse"] = {
+        "budget_ms": budget, "reference_spp": args.mse_reference_spp,
+        "reference": "plain tracer, NEE with MIS, two halves of other seeds",
+        "reference_variance": ref_var, **res,
+        "guided_over_plain": ratio("guided", "plain"),
+        "guided_over_wfpg_unguided": ratio("guided", "wfpg_unguided"),
+        "guided_nonee_over_plain_nonee": ratio("guided_nonee", "plain_nonee"),
+        "note": "1 spp per frame at 1920x1080; every MSE less the reference's own variance "
+                "(mse_raw keeps it); mse_x_frames is the error per frame of samples; guided "
+                "tracers start with a cold octree, whose build counts against the budget "
+                "(device time)"}
+    return out
     # ---- equal-time MSE ----
     p = m.PathTracer(g.system, g)
     p.set_options(dict(OPTS, Seed=7))
@@ -714,8 +786,18 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
     g.construct_accelerators()
 
     def make(kind, seed):
-        t = m.PathTracer(system, g) if kind == "plain" else m.WFPGTracer(system, g)
-        opts = dict(C1, Seed=seed)
+        plain = kind in ("plain", "plain_nee")
+        t = m.PathTracer(system, g) if plain else m.WFPGTracer(system, g)
+        # NEE off for every estimator, as the reference's own WFPG
+        # configurations run (WorkingDir/tConf_veach_product.json): with
+        # NEE, next to the ceiling light NEE throws fireflies that dominate
+        # every MSE (plain_nee: NEE as configured), and with NEE and MIS the
+        # guided estimators are biased (the NEE weight uses the BxDF pdf,
+        # the guided path ray the mixture pdf, WFPGTracerKC.cuh:338-347)
+        opts = dict(C1, Seed=seed, NextEventEstimation=1 if kind == "plain_nee" else 0)
+        if plain:
+            t.set_options(opts)
+            return t
         if kind == "wfpg_bxdf":
             # the same tracer with its network never taking over: the BxDF
             # samples every frame (the method without the network)
@@ -736,12 +818,18 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
                            if learned or not k.startswith("Learned")})
         return t
 
-    ref_img, ref_var, ref_rvar = _reference(lambda half: make("plain", 4242 + half),
+    # the converged render: NEE with MIS (the same expectation as every
+    # estimator here, without the fireflies NEE alone throws next to the light)
+    def make_ref(seed):
+        t = m.PathTracer(system, g)
+        t.set_options(dict(C1, Seed=seed, DirectLightMIS=1))
+        return t
+    ref_img, ref_var, ref_rvar = _reference(lambda half: make_ref(4242 + half),
                                             args.learned_reference_spp // 4)
     out = {"budget_ms": args.learned_budget_ms, "reference_spp": args.learned_reference_spp,
            "reference_variance": ref_var}
     kinds = (("plain", 11), ("wfpg_bxdf", 16), ("svo", 12), ("learned_1", 13), ("learned_4", 14),
-             ("learned_1_octree", 15))
+             ("learned_1_octree", 15), ("plain_nee", 17))
     if args.learned_kinds:
         kinds = tuple(k for k in kinds if k[0] in args.learned_kinds.split(","))
     for kind, seed in kinds:
@@ -763,7 +851,8 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
             entry["warm_up_sampler"] = "octree" if kind.endswith("_octree") else "BxDF"
         t.close()
         out[kind] = entry
-    if len(kinds) == 6:
+    if all(k in out for k in ("plain", "wfpg_bxdf", "svo", "learned_1", "learned_4",
+                              "learned_1_octree")):
         best = min(("learned_1", "learned_4", "learned_1_octree"), key=lambda k: out[k]["mse"])
         out["learned"] = dict(out[best], variant=best)
         out["learned_over_plain"] = out["learned"]["mse"] / out["plain"]["mse"]
@@ -781,11 +870,12 @@ def _run_learned_scene(args, m, system, torch, shielded: bool) -> dict:
         # cost then trades against
         out["mse_x_spp"] = {k: out[k]["mse"] * out[k]["spp"]
                             for k in ("plain", "wfpg_bxdf", "svo", "learned_1", "learned_4",
-                                      "learned_1_octree")}
+                                      "learned_1_octree", "plain_nee") if k in out}
     out["config"] = {"scene": ("Cornell box (seed 1) with the light facing the ceiling over an "
                                "opaque panel" if shielded else
                                "Cornell box with a ceiling-wide light (seed 1)")
-                     + ", 128x128, 4 spp per frame, depth 5",
+                     + ", 128x128, 4 spp per frame, depth 5, NEE off (plain_nee: the plain "
+                       "tracer with NEE); reference: plain, NEE with MIS",
                      **LEARNED, **LEARNED_FLOATS,
                      "network": "80-64-64-64-40 ReLU MLP, 8 vMF lobes, BF16 weights and "
                                 "activations, FP32 accumulation on tcgen05 tensor cores"}
@@ -903,7 +993,7 @@ def main():
                     help="skip the WFPG (SVO path guiding) run")
     ap.add_argument("--mse-budget-ms", type=float, default=2000.0,
                     help="equal-time MSE budget per tracer (0 skips the comparison)")
-    ap.add_argument("--mse-reference-spp", type=int, default=1024)
+    ap.add_argument("--mse-reference-spp", type=int, default=2048)
     ap.add_argument("--no-pool", dest="pool", action="store_false",
                     help="skip the wavefront-pool batching and serving runs")
     ap.add_argument("--serve-jobs", type=int, default=64,
@@ -911,6 +1001,9 @@ def main():
     ap.add_argument("--pool-block", type=int, default=0)
     ap.add_argument("--pool-stack", type=int, default=128,
                     help="traversal stack of the pool: 64 or 128 (sorted order) or 0 (octant order)")
+    ap.add_argument("--wide-order", default="auto",
+                    choices=["auto", "sorted", "octant", "sorted_refill", "octant_refill"],
+                    help="8-wide traversal kernel of the headline frame (auto: timed per depth)")
     ap.add_argument("--no-closed", dest="closed", action="store_false",
                     help="skip the bounce-heavy Cornell 1080p 4 spp entry")
     ap.add_argument("--no-learned", dest="learned", action="store_false",
