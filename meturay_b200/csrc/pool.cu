@@ -64,11 +64,60 @@ struct mrb_pool {
     uint64_t iterations = 0;
     cudaGraphExec_t graph = nullptr;
     bool graphDirty = true;
+    // Image buffers of released jobs, kept for the next admissions: a
+    // cudaMalloc per admission and a cudaFree (which waits for the whole
+    // device) per release cost milliseconds each inside the serving loop.
+    // Bounded by kSpareBytes, and freed (oldest first) before a new buffer
+    // would take the admitted and kept images past the HBM budget.
+    std::vector<std::pair<void*, size_t>> spare;
+    size_t spareBytes = 0;
+    // pinned staging for image read-back
+    void* stage = nullptr;
+    size_t stageBytes = 0;
     ~mrb_pool() {
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
         if (hostTable) cudaFreeHost(hostTable);
+        if (stage) cudaFreeHost(stage);
+        for (auto& b : spare) cudaFree(b.first);
         if (stream) cudaStreamDestroy(stream);
+    }
+    static constexpr size_t kSpareBytes = size_t(1) << 30;
+    // a kept buffer of at least `bytes` and at most 4x that, else a new one
+    int take_image(DBuf& img, size_t bytes) {
+        int best = -1;
+        for (size_t i = 0; i < spare.size(); i++)
+            if (spare[i].second >= bytes && spare[i].second <= 4 * bytes &&
+                (best < 0 || spare[i].second < spare[size_t(best)].second))
+                best = int(i);
+        if (best < 0) {
+            // a new buffer: kept ones go first where they would take the
+            // images past the budget
+            while (!spare.empty() && used + spareBytes + bytes > budget) {
+                cudaFree(spare.front().first);
+                spareBytes -= spare.front().second;
+                spare.erase(spare.begin());
+            }
+            return img.alloc(bytes);
+        }
+        img.release();
+        img.p = spare[size_t(best)].first;
+        img.bytes = spare[size_t(best)].second;
+        spareBytes -= img.bytes;
+        spare.erase(spare.begin() + best);
+        return 0;
+    }
+    void keep_image(DBuf& img) {
+        if (!img.p) return;
+        spare.emplace_back(img.p, img.bytes);
+        spareBytes += img.bytes;
+        img.p = nullptr;
+        img.bytes = 0;
+        while (spareBytes > kSpareBytes && !spare.empty()) {
+            cudaFree(spare.front().first);
+            spareBytes -= spare.front().second;
+            spare.erase(spare.begin());
+        }
     }
     PoolHeader* header() { return reinterpret_cast<PoolHeader*>(hostTable); }
     JobDev* hostJobs() { return reinterpret_cast<JobDev*>(hostTable + sizeof(PoolHeader)); }
@@ -333,7 +382,7 @@ int mrb_pool_step(mrb_pool* p, uint32_t* finished, uint32_t* active, uint32_t* q
     while (!p->queue.empty() && p->used + p->queue.front()->bytes <= p->budget &&
            p->active.size() < kPoolMaxJobs) {
         PoolJob* j = p->queue.front();
-        int r = j->image.alloc(j->bytes);
+        int r = p->take_image(j->image, j->bytes);
         if (r) {
             // the budget was optimistic: wait until memory frees up
             if (p->active.empty()) return r;
@@ -420,10 +469,20 @@ int mrb_pool_job_image(mrb_pool* p, uint64_t id, float* host_rgba, int release) 
             mrb::set_error("pool: job %llu's image was released", static_cast<unsigned long long>(id));
             return MRB_E_STATE;
         }
-        MRB_CUDA(cudaMemcpy(host_rgba, j->image.p, j->bytes, cudaMemcpyDeviceToHost));
+        // through pinned staging on the pool's stream
+        if (p->stageBytes < j->bytes) {
+            if (p->stage) cudaFreeHost(p->stage);
+            p->stage = nullptr;
+            p->stageBytes = 0;
+            MRB_CUDA(cudaHostAlloc(&p->stage, j->bytes, cudaHostAllocDefault));
+            p->stageBytes = j->bytes;
+        }
+        MRB_CUDA(cudaMemcpyAsync(p->stage, j->image.p, j->bytes, cudaMemcpyDeviceToHost, p->stream));
+        MRB_CUDA(cudaStreamSynchronize(p->stream));
+        std::memcpy(host_rgba, p->stage, j->bytes);
     }
     if (release && j->image.p) {
-        j->image.release();
+        p->keep_image(j->image);
         p->used -= j->bytes;
         for (auto& u : p->jobs)
             if (u.get() == j) u.reset();
