@@ -522,16 +522,33 @@ __global__ void __launch_bounds__(kGuideTPB, 4) k_guide(GuideArgs A) {
             pwc_sample_bin<X>(A, S, begin, end, frame);
         } else {
             // 8x8 outer field: mean and max of each DPP x DPP block
+            // (ProductSampler.cuh:160-215).  The mean adds the block's texels
+            // as the reference's cub warp reduction does: row-major, in chunks
+            // of at most 32 (a logical warp of min(32, max(2, DPP^2)) lanes,
+            // lanes past DPP^2 holding 0), each chunk as a pairwise tree
+            // (pairs at distance 1, 2, 4, ...), the chunk sums added in order
             if (tid < 64) {
+                constexpr int N = DPP * DPP;
+                constexpr int W = N >= 32 ? 32 : (N < 2 ? 2 : N);
+                constexpr int IT = N >= 32 ? N / 32 : 1;
                 const int cx = static_cast<int>(tid) & 7, cy = static_cast<int>(tid) >> 3;
-                float sum = 0.0f, mx = 0.0f;
-                for (int iy = 0; iy < DPP; iy++)
-                    for (int ix = 0; ix < DPP; ix++) {
-                        const float v = S.field[(cy * DPP + iy) * X + cx * DPP + ix];
-                        sum += v;
-                        mx = fmaxf(mx, v);
+                float total = 0.0f, mx = 0.0f;
+                for (int it = 0; it < IT; it++) {
+                    float v[W];
+#pragma unroll
+                    for (int l = 0; l < W; l++) {
+                        const int li = l + it * 32;
+                        v[l] = (li < N) ? S.field[(cy * DPP + li / DPP) * X + cx * DPP + li % DPP]
+                                        : 0.0f;
+                        mx = fmaxf(mx, v[l]);
                     }
-                S.small[tid] = sum / static_cast<float>(DPP * DPP);
+#pragma unroll
+                    for (int off = 1; off < W; off <<= 1)
+#pragma unroll
+                        for (int l = 0; l + off < W; l += 2 * off) v[l] = v[l] + v[l + off];
+                    total += v[0];
+                }
+                S.small[tid] = total / static_cast<float>(N);
                 S.norm[tid] = mx;
             }
             __syncthreads();

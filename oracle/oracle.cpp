@@ -2346,6 +2346,159 @@ void scan8(const float in[8], float out[8]) {
     for (int i = 0; i < 8; i++) out[i] = x[i];
 }
 
+// ProductSampler's constructor (ProductSampler.cuh:160-215): the mean and
+// the maximum of each of the 8x8 product cells' DPP x DPP texels.  The mean
+// adds the texels as the sampler's cub warp reduction does: the cell's
+// texels in row-major order, in chunks of at most 32 (a logical warp of
+// min(32, max(2, DPP^2)) lanes, lanes past DPP^2 holding 0), each chunk
+// summed as a pairwise tree (lane pairs at distance 1, 2, 4, ...), the chunk
+// sums added in order to 0.
+template <int X>
+void product_cells(const float* field, float small[64], float normc[64]) {
+    constexpr int DPP = X / 8, N = DPP * DPP;
+    constexpr int W = N >= 32 ? 32 : (N < 2 ? 2 : N);
+    constexpr int IT = N >= 32 ? N / 32 : 1;
+    for (int c = 0; c < 64; c++) {
+        const int cx = c & 7, cy = c >> 3;
+        float total = 0.0f, mx = 0.0f;
+        for (int it = 0; it < IT; it++) {
+            float v[W];
+            for (int l = 0; l < W; l++) {
+                const int li = l + it * 32;
+                v[l] = (li < N) ? field[(cy * DPP + li / DPP) * X + cx * DPP + li % DPP] : 0.0f;
+                mx = std::fmax(mx, v[l]);
+            }
+            for (int off = 1; off < W; off <<= 1)
+                for (int l = 0; l + off < W; l += 2 * off) v[l] = v[l] + v[l + off];
+            total += v[0];
+        }
+        small[c] = total / static_cast<float>(N);
+        normc[c] = mx;
+    }
+}
+
+// GeneratePDFAndCDF (ProductSampler.cuh:217-368): rows of the product of
+// the cell means and the BxDF's gray values (floored at VeryLargeEpsilon),
+// row and marginal CDFs by 8-wide inclusive scans.
+struct ProductCdf {
+    float pdfX[64], cdfX[64], pdfY[8], cdfY[8];
+};
+
+void product_build(const float gray[64], const float small[64], ProductCdf& P) {
+    float rowTot[8];
+    for (int row = 0; row < 8; row++) {
+        float prod[8], incl[8];
+        for (int cx = 0; cx < 8; cx++)
+            prod[cx] = std::fmax(1.0e-3f, gray[row * 8 + cx] * small[row * 8 + cx]);
+        scan8(prod, incl);
+        const float rowTotal = incl[7];
+        const float rcp = 1.0f / rowTotal;
+        for (int cx = 0; cx < 8; cx++) {
+            P.cdfX[row * 8 + cx] = incl[cx] * rcp;
+            P.pdfX[row * 8 + cx] = prod[cx] * 8.0f * rcp;
+        }
+        rowTot[row] = rowTotal;
+    }
+    float incl[8];
+    scan8(rowTot, incl);
+    const float rcp = 1.0f / incl[7];
+    for (int l = 0; l < 8; l++) {
+        P.cdfY[l] = incl[l] * rcp;
+        P.pdfY[l] = rowTot[l] * (8.0f * rcp);
+    }
+}
+
+// ProductSampler::Pdf (ProductSampler.cuh:508-540), indices clamped to the
+// map (the reference reads past it for uv = 1).
+template <int X>
+float product_pdf(const float* field, const float small[64], const ProductCdf& P, float u,
+                  float v) {
+    constexpr int DPP = X / 8;
+    const float dppF = static_cast<float>(DPP);
+    const float ex = u * 8.0f, ey = v * 8.0f;
+    const float ox = std::floor(ex), oy = std::floor(ey);
+    const float ix = (ex - ox) * dppF, iy = (ey - oy) * dppF;
+    const int ocx = std::min(std::max(f2i_sat(ox), 0), 7), ocy = std::min(std::max(f2i_sat(oy), 0), 7);
+    int gx = ocx * DPP + f2i_sat(std::floor(ix)), gy = ocy * DPP + f2i_sat(std::floor(iy));
+    gx = std::min(std::max(gx, 0), X - 1);
+    gy = std::min(std::max(gy, 0), X - 1);
+    const int cell = ocy * 8 + ocx;
+    const float inner = field[gy * X + gx] / small[cell];
+    return P.pdfX[cell] * P.pdfY[ocy] * inner;
+}
+
+// ProductSampler::Sample (ProductSampler.cuh:370-470): the row and the
+// column by CDF search (first entry not below the draw, clamped to the last
+// cell), then rejection sampling inside the cell: in each of 24 rounds
+// every lane draws (u, v, acceptance) and the lowest accepting lane wins;
+// if none does, lane 0's last draw is taken with an inner pdf of 1.
+// draw(round, lane, u, v, a) supplies the numbers.  Returns the map
+// coordinates and the product pdf (before the sphere's 1/(4 pi)).
+template <int X, class Draw>
+void product_sample(const float* field, const float small[64], const float normc[64],
+                    const ProductCdf& P, float xi0, float xi1, Draw&& draw, float& ss, float& tt,
+                    float& pdfS, int* rowOut = nullptr, int* colOut = nullptr) {
+    constexpr int DPP = X / 8;
+    const float dppF = static_cast<float>(DPP);
+    int rowId = 8;
+    for (int l = 0; l < 8; l++)
+        if (!(xi0 > P.cdfY[l])) {
+            rowId = l;
+            break;
+        }
+    rowId = std::min(rowId, 7);
+    int colId = 8;
+    for (int l = 0; l < 8; l++)
+        if (!(xi1 > P.cdfX[rowId * 8 + l])) {
+            colId = l;
+            break;
+        }
+    colId = std::min(colId, 7);
+    if (rowOut) *rowOut = rowId;
+    if (colOut) *colOut = colId;
+    const int cell = rowId * 8 + colId;
+    float u = 0.0f, v = 0.0f, tex = 0.0f, u0 = 0.0f, v0 = 0.0f, tex0 = 0.0f;
+    bool lucky = false;
+    for (int round = 0; round < 24 && !lucky; round++) {
+        for (uint32_t lane = 0; lane < 32; lane++) {
+            float du, dv, da;
+            draw(round, lane, du, dv, da);
+            const int ix = f2i_sat(du * dppF), iy = f2i_sat(dv * dppF);
+            const float tx = field[(rowId * DPP + iy) * X + colId * DPP + ix];
+            if (lane == 0) {
+                u0 = du;
+                v0 = dv;
+                tex0 = tx;
+            }
+            if (da <= tx / normc[cell]) {
+                u = du;
+                v = dv;
+                tex = tx;
+                lucky = true;
+                break;
+            }
+        }
+    }
+    if (!lucky) {
+        u = u0;
+        v = v0;
+        tex = tex0;
+    }
+    const float pdfInner = lucky ? tex / small[cell] : 1.0f;
+    pdfS = P.pdfY[rowId] * P.pdfX[cell] * pdfInner;
+    const float rcpX = 1.0f / static_cast<float>(X);
+    ss = (static_cast<float>(colId) * dppF + u * dppF) * rcpX;
+    tt = (static_cast<float>(rowId) * dppF + v * dppF) * rcpX;
+}
+
+// One-sample MIS of the drawn direction (SampleMIS, ProductSampler.cuh:
+// 640-650): pdfSampled * ratio / BalanceHeuristic.
+inline float mis_pdf(float pdfSampled, float ratio, float pdfOther) {
+    const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
+    const float pdf = pdfSampled * ratio / (w0 / (w0 + w1));
+    return (pdfSampled == 0.0f) ? 0.0f : pdf;
+}
+
 }  // namespace
 
 extern "C" void oracle_svo_payload_init(oracle_svo* o, const float* light_rad, uint32_t omit) {
@@ -2617,18 +2770,7 @@ void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* op
         return;
     }
     float small[64], normc[64];
-    for (int c = 0; c < 64; c++) {
-        const int cx = c & 7, cy = c >> 3;
-        float sum = 0.0f, mx = 0.0f;
-        for (int iy = 0; iy < DPP; iy++)
-            for (int ix = 0; ix < DPP; ix++) {
-                const float v = field[(cy * DPP + iy) * X + cx * DPP + ix];
-                sum += v;
-                mx = std::fmax(mx, v);
-            }
-        small[c] = sum / static_cast<float>(DPP * DPP);
-        normc[c] = mx;
-    }
+    product_cells<X>(field.data(), small, normc);
     const float kInv4Pi = 0.25f * kInvPiF;
     for (uint32_t i : rays) {
         WRay& wr = wave[i];
@@ -2638,116 +2780,41 @@ void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* op
         const Surface<float> sf = gen_surface(s, wr.prim, wr.b0, wr.b1, wr.r.d);
         const F3 wi = -wr.r.d;
         const F3 nrm = to_space(F3(0.0f, 0.0f, 1.0f), sf.w2t);
-        float pdfX[64], cdfX[64], rowTot[8], pdfY[8], cdfY[8];
-        for (int row = 0; row < 8; row++) {
-            float prod[8], incl[8];
-            for (int cx = 0; cx < 8; cx++) {
-                const int c = row * 8 + cx;
-                float gray = 1.0f;
-                if (!isLight && !spec) gray = lum3(mat_eval(s, batch, id, bxdf_proj(cx, row, nrm), wi, sf));
-                prod[cx] = std::fmax(1.0e-3f, gray * small[c]);
-            }
-            scan8(prod, incl);
-            const float rowTotal = incl[7];
-            const float rcp = 1.0f / rowTotal;
-            for (int cx = 0; cx < 8; cx++) {
-                cdfX[row * 8 + cx] = incl[cx] * rcp;
-                pdfX[row * 8 + cx] = prod[cx] * 8.0f * rcp;
-            }
-            rowTot[row] = rowTotal;
+        float gray[64];
+        for (int c = 0; c < 64; c++) {
+            gray[c] = 1.0f;
+            if (!isLight && !spec) gray[c] = lum3(mat_eval(s, batch, id, bxdf_proj(c & 7, c >> 3, nrm), wi, sf));
         }
-        {
-            float incl[8];
-            scan8(rowTot, incl);
-            const float rcp = 1.0f / incl[7];
-            for (int l = 0; l < 8; l++) {
-                cdfY[l] = incl[l] * rcp;
-                pdfY[l] = rowTot[l] * (8.0f * rcp);
-            }
-        }
+        ProductCdf P;
+        product_build(gray, small, P);
         const uint32_t smp = wr.r.aux.sample;
         const Rng4 r0 = rng_block(smp, frame, kTagGuide | depthTag, 0u, opt->seed_lo, opt->seed_hi);
         const bool purePG = w->pure_pg != 0;
         float ss = 0.0f, tt = 0.0f, pdf = 1.0f;
         bool bxdfSel = true;
-        auto product_pdf = [&](float u, float v) {
-            const float ex = u * 8.0f, ey = v * 8.0f;
-            const float ox = std::floor(ex), oy = std::floor(ey);
-            const float ix = (ex - ox) * dppF, iy = (ey - oy) * dppF;
-            int ocx = std::min(std::max(f2i_sat(ox), 0), 7), ocy = std::min(std::max(f2i_sat(oy), 0), 7);
-            int gx = ocx * DPP + f2i_sat(std::floor(ix)), gy = ocy * DPP + f2i_sat(std::floor(iy));
-            gx = std::min(std::max(gx, 0), X - 1);
-            gy = std::min(std::max(gy, 0), X - 1);
-            const int cell = ocy * 8 + ocx;
-            const float inner = field[gy * X + gx] / small[cell];
-            return pdfX[cell] * pdfY[ocy] * inner;
-        };
         if (!purePG && (isLight || spec)) {
         } else if (!purePG && r0.u[0] >= w->mis_ratio) {
             const Rng4 r1 = rng_block(smp, frame, kTagGuide | depthTag, 1u, opt->seed_lo, opt->seed_hi);
             const BSample<float> bs = mat_sample(s, batch, id, wi, sf, wr.r.aux.medium, r1.u[0], r1.u[1], r1.u[2]);
             dir_yup_to_octa(bs.dir, ss, tt);
-            const float pdfSampled = bs.pdf;
-            const float pdfOther = product_pdf(ss, tt) * kInv4Pi;
-            const float ratio = 1.0f - w->mis_ratio;
-            const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
-            pdf = pdfSampled * ratio / (w0 / (w0 + w1));
-            pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+            const float pdfOther = product_pdf<X>(field.data(), small, P, ss, tt) * kInv4Pi;
+            pdf = mis_pdf(bs.pdf, 1.0f - w->mis_ratio, pdfOther);
             bxdfSel = true;
         } else {
-            const float xi0 = r0.u[1], xi1 = r0.u[2];
-            int rowId = 8;
-            for (int l = 0; l < 8; l++)
-                if (!(xi0 > cdfY[l])) { rowId = l; break; }
-            rowId = std::min(rowId, 7);
-            int colId = 8;
-            for (int l = 0; l < 8; l++)
-                if (!(xi1 > cdfX[rowId * 8 + l])) { colId = l; break; }
-            colId = std::min(colId, 7);
-            const int cell = rowId * 8 + colId;
-            float u = 0.0f, v = 0.0f, tex = 0.0f;
-            bool lucky = false;
-            float u0 = 0.0f, v0 = 0.0f, tex0 = 0.0f;
-            for (int round = 0; round < 24 && !lucky; round++) {
-                for (uint32_t lane = 0; lane < 32; lane++) {
-                    const Rng4 rl = rng_block(smp, frame, kTagGuide | depthTag, 2u + uint32_t(round) * 32u + lane,
-                                              opt->seed_lo, opt->seed_hi);
-                    const int ix = f2i_sat(rl.u[0] * dppF), iy = f2i_sat(rl.u[1] * dppF);
-                    const float tx = field[(rowId * DPP + iy) * X + colId * DPP + ix];
-                    if (lane == 0) {
-                        u0 = rl.u[0];
-                        v0 = rl.u[1];
-                        tex0 = tx;
-                    }
-                    if (rl.u[2] <= tx / normc[cell]) {
-                        u = rl.u[0];
-                        v = rl.u[1];
-                        tex = tx;
-                        lucky = true;
-                        break;
-                    }
-                }
-            }
-            if (!lucky) {
-                u = u0;
-                v = v0;
-                tex = tex0;
-            }
-            const float pdfInner = lucky ? tex / small[cell] : 1.0f;
-            const float pdfS = pdfY[rowId] * pdfX[cell] * pdfInner;
-            const float rcpX = 1.0f / static_cast<float>(X);
-            ss = (static_cast<float>(colId) * dppF + u * dppF) * rcpX;
-            tt = (static_cast<float>(rowId) * dppF + v * dppF) * rcpX;
+            auto draw = [&](int round, uint32_t lane, float& du, float& dv, float& da) {
+                const Rng4 rl = rng_block(smp, frame, kTagGuide | depthTag, 2u + uint32_t(round) * 32u + lane,
+                                          opt->seed_lo, opt->seed_hi);
+                du = rl.u[0];
+                dv = rl.u[1];
+                da = rl.u[2];
+            };
+            float pdfS;
+            product_sample<X>(field.data(), small, normc, P, r0.u[1], r0.u[2], draw, ss, tt, pdfS);
             if (purePG) {
                 pdf = pdfS * kInv4Pi;
             } else {
-                const float pdfSampled = pdfS * kInv4Pi;
                 const F3 wo = octa_to_dir_yup(ss, tt);
-                const float pdfOther = mat_pdf(s, batch, id, wo, wi, sf);
-                const float ratio = w->mis_ratio;
-                const float w0 = ratio * pdfSampled, w1 = (1.0f - ratio) * pdfOther;
-                pdf = pdfSampled * ratio / (w0 / (w0 + w1));
-                pdf = (pdfSampled == 0.0f) ? 0.0f : pdf;
+                pdf = mis_pdf(pdfS * kInv4Pi, w->mis_ratio, mat_pdf(s, batch, id, wo, wi, sf));
             }
             bxdfSel = false;
         }
@@ -2762,6 +2829,85 @@ void guide_bin(const oracle_scene* s, const Tree& tree, const oracle_options* op
 }
 
 }  // namespace
+
+// The product sampler on table inputs (test infrastructure: the pin of the
+// restatement against the reference's own ProductSampler run by
+// oracle/psamp/psamp_harness.cu).  Per bin a 64x64 field; per ray a table
+// surface (kPinSurface floats: RGB per product cell, a BxDF sample's uv and
+// pdf, Pdf(wo) = a + b wo.x + c wo.y) and 32 lanes x streamLen uniforms,
+// consumed as SampleMIS and Sample draw them (ProductSampler.cuh:370-470,
+// 556-660): lane 0 draws the MIS choice, then (guide branch) the row; the
+// leader lane of the chosen row within its group of four rows (lane
+// 8 * (row % 4)) draws the column; then every lane draws (u, v) and the
+// acceptance per rejection round.
+namespace {
+constexpr int kPinSurface = 198;
+}
+
+extern "C" void oracle_product_pin(const float* fields, uint32_t bins, uint32_t raysPerBin,
+                                   const float* surfaces, const float* streams,
+                                   uint32_t streamLen, float misRatio, float mult, float* uv,
+                                   float* pdfOut, uint32_t* selOut, float* smallOut,
+                                   float* normOut) {
+    constexpr int X = 64;
+    for (uint32_t b = 0; b < bins; b++) {
+        const float* field = fields + size_t(b) * X * X;
+        float small[64], normc[64];
+        product_cells<X>(field, small, normc);
+        for (int c = 0; c < 64; c++) {
+            smallOut[b * 64 + c] = small[c];
+            normOut[b * 64 + c] = normc[c];
+        }
+        for (uint32_t r = 0; r < raysPerBin; r++) {
+            const uint32_t ray = b * raysPerBin + r;
+            const float* t = surfaces + size_t(ray) * kPinSurface;
+            const float* st = streams + size_t(ray) * 32 * streamLen;
+            uint32_t next[32] = {};
+            auto take = [&](uint32_t lane) {
+                const uint32_t k = next[lane]++;
+                return k < streamLen ? st[size_t(lane) * streamLen + k] : 0.5f;
+            };
+            float gray[64];
+            for (int c = 0; c < 64; c++) gray[c] = lum3(F3(t[3 * c], t[3 * c + 1], t[3 * c + 2]));
+            ProductCdf P;
+            product_build(gray, small, P);
+            float ss = 0.0f, tt = 0.0f, pdf = 0.0f;
+            bool sel;
+            const float xi = take(0);
+            if (xi >= misRatio) {
+                ss = t[192];
+                tt = t[193];
+                const float pdfOther = product_pdf<X>(field, small, P, ss, tt) * mult;
+                pdf = mis_pdf(t[194], 1.0f - misRatio, pdfOther);
+                sel = true;
+            } else {
+                const float xi0 = take(0);
+                int row = 8;
+                for (int l = 0; l < 8; l++)
+                    if (!(xi0 > P.cdfY[l])) {
+                        row = l;
+                        break;
+                    }
+                row = std::min(row, 7);
+                const float xi1 = take(uint32_t(8 * (row % 4)));
+                auto draw = [&](int, uint32_t lane, float& du, float& dv, float& da) {
+                    du = take(lane);
+                    dv = take(lane);
+                    da = take(lane);
+                };
+                float pdfS;
+                product_sample<X>(field, small, normc, P, xi0, xi1, draw, ss, tt, pdfS);
+                const float pdfOther = t[195] + t[196] * ss + t[197] * tt;
+                pdf = mis_pdf(pdfS * mult, misRatio, pdfOther);
+                sel = false;
+            }
+            uv[2 * size_t(ray)] = ss;
+            uv[2 * size_t(ray) + 1] = tt;
+            pdfOut[ray] = pdf;
+            selOut[ray] = sel ? 1u : 0u;
+        }
+    }
+}
 
 extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* b,
                                        const oracle_camera* cam, const oracle_options* opt,

@@ -205,6 +205,12 @@ typedef struct oracle_wfpg_options {
     uint32_t dump_iteration;
     uint32_t product;  /* 1: KCGenAndSampleDistributionProduct, 0: KCGenAndSampleDistribution */
 } oracle_wfpg_options;
+/* The product sampler on table inputs, for its pin against the reference's
+ * own sampler (test infrastructure; see oracle.cpp). */
+void oracle_product_pin(const float* fields, uint32_t bins, uint32_t rays_per_bin,
+                        const float* surfaces, const float* streams, uint32_t stream_len,
+                        float mis_ratio, float mult, float* uv, float* pdf, uint32_t* sel,
+                        float* small, float* norm);
 uint64_t oracle_render_wfpg(const oracle_scene* scene, const oracle_bvh* bvh,
                             const oracle_camera* cam, const oracle_options* opt,
                             const oracle_wfpg_options* wopt, oracle_svo* svo, float* out_rgb,

@@ -77,6 +77,8 @@ def _load():
     lib.oracle_trace.argtypes = [C.POINTER(Scene), vp, vp, u32, vp, vp, vp, vp, u32]
     lib.oracle_trace_linear.argtypes = [C.POINTER(Scene), vp, u32, vp, vp, vp, vp, u32]
     lib.oracle_trace_counters.argtypes = [vp, C.c_int]
+    lib.oracle_product_pin.argtypes = [vp, u32, u32, vp, vp, u32, C.c_float, C.c_float, vp, vp,
+                                       vp, vp, vp]
     lib.oracle_render.restype = C.c_uint64
     lib.oracle_render.argtypes = [C.POINTER(Scene), vp, C.POINTER(Camera), C.POINTER(Options), vp]
     lib.oracle_render_f64.restype = C.c_uint64
@@ -137,6 +139,24 @@ def trace_counters(reset: bool = False) -> tuple[int, int]:
     out = np.zeros(2, np.uint64)
     lib.oracle_trace_counters(_p(out), 1 if reset else 0)
     return int(out[0]), int(out[1])
+
+
+def product_pin(fields: np.ndarray, rays_per_bin: int, surfaces: np.ndarray,
+                streams: np.ndarray, mis_ratio: float, mult: float) -> dict:
+    """The oracle's product sampler on table inputs (fields (bins, 64, 64);
+    surfaces (rays, 198); streams (rays, 32, n) uniforms per lane), as the
+    reference sampler's harness runs it."""
+    fields = np.ascontiguousarray(fields, np.float32)
+    surfaces = np.ascontiguousarray(surfaces, np.float32)
+    streams = np.ascontiguousarray(streams, np.float32)
+    bins, rays = fields.shape[0], surfaces.shape[0]
+    out = {"uv": np.zeros((rays, 2), np.float32), "pdf": np.zeros(rays, np.float32),
+           "sel": np.zeros(rays, np.uint32), "small": np.zeros((bins, 64), np.float32),
+           "norm": np.zeros((bins, 64), np.float32)}
+    lib.oracle_product_pin(_p(fields), bins, rays_per_bin, _p(surfaces), _p(streams),
+                           streams.shape[2], float(mis_ratio), float(mult), _p(out["uv"]),
+                           _p(out["pdf"]), _p(out["sel"]), _p(out["small"]), _p(out["norm"]))
+    return out
 
 
 def partition(keys: np.ndarray, batch_bits: int, id_bits: int):
