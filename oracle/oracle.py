@@ -21,7 +21,8 @@ REF_LIB = HERE / "_ref" / "libmrayref.so"
 
 def build(ref_root: str | None = None) -> None:
     """Compile the oracle; with ``ref_root`` (or the REF_ROOT environment
-    variable) naming an MRay source tree, also the reference shim."""
+    variable) naming an MRay source tree, also the reference shim and the
+    product-sampler harness (the latter needs nvcc)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     ref_root = ref_root or os.environ.get("REF_ROOT")
     if not ref_root:
@@ -29,7 +30,7 @@ def build(ref_root: str | None = None) -> None:
     root = Path(ref_root)
     if not (root / "Source" / "RayLib" / "Ray.hpp").exists():
         raise FileNotFoundError(f"REF_ROOT={root} is not an MRay source tree")
-    subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), "ref", "psamp", f"REF_ROOT={root}"], check=True)
 
 
 class Scene(C.Structure):
