@@ -18,10 +18,12 @@
 //
 // Node (80 B = five 16-byte loads):
 //   n0 = (box.lo.xyz, exps): exps = ex | ey << 8 | ez << 16 | imask << 24
-//   n1 = (childBase, triBase, meta[0..3], meta[4..7])
+//   n1 = (childBase, triBase, leafMask, 0)
 //   n2 = (qlo.x[0..7], qlo.y[0..7]), n3 = (qlo.z[0..7], qhi.x[0..7]),
 //   n4 = (qhi.y[0..7], qhi.z[0..7])
-// meta per slot: 0 empty, 0x80|rank internal child, 0x40|rank leaf child.
+// Slot k holds an internal child (imask bit k: node childBase + the number
+// of internal children in lower slots), a leaf (leafMask bit k: triangle
+// triBase + the number of leaves in lower slots) or nothing.
 // A child plane decodes as lo + q * 2^(e-127); quantisation rounds outward,
 // so decoded boxes contain the exact child boxes.
 #include <type_traits>
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(128) k_collapse(
             e[c] = quant_exponent(bhi[c] - blo[c]);
             scale[c] = __uint_as_float(e[c] << 23);
         }
-        uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint32_t leafMask = 0;
         uint8_t q[6][8];
         for (int c = 0; c < 6; c++)
             for (int k = 0; k < 8; k++) q[c][k] = (c < 3) ? 255 : 0;  // empty slot never hits
@@ -187,12 +189,11 @@ __global__ void __launch_bounds__(128) k_collapse(
                 q[3 + c][k] = static_cast<uint8_t>(qh);
             }
             if (ch[k] >= n) {
-                meta[k] = uint8_t(0x80u | ri);
                 imask |= 1u << k;
                 qout[qbase + ri] = WorkItem{ch[k], childBase + uint32_t(ri)};
                 ri++;
             } else {
-                meta[k] = uint8_t(0x40u | rl);
+                leafMask |= 1u << k;
                 // leaf: the triangle, reordered into this node's leaf block
                 const uint32_t t = sortedIdx[ch[k]];
                 const uint32_t s = triBase + uint32_t(rl);
@@ -211,9 +212,7 @@ __global__ void __launch_bounds__(128) k_collapse(
         WideNode nd;
         nd.n0 = make_float4(blo[0], blo[1], blo[2],
                             __uint_as_float(e[0] | (e[1] << 8) | (e[2] << 16) | (imask << 24)));
-        uint32_t m0 = meta[0] | (meta[1] << 8) | (meta[2] << 16) | (uint32_t(meta[3]) << 24);
-        uint32_t m1 = meta[4] | (meta[5] << 8) | (meta[6] << 16) | (uint32_t(meta[7]) << 24);
-        nd.n1 = make_uint4(childBase, triBase, m0, m1);
+        nd.n1 = make_uint4(childBase, triBase, leafMask, 0u);
         auto pack = [&](int c, int k0) {
             return q[c][k0] | (q[c][k0 + 1] << 8) | (q[c][k0 + 2] << 16) |
                    (uint32_t(q[c][k0 + 3]) << 24);
@@ -323,7 +322,7 @@ __device__ __forceinline__ void wide_ray_begin(WideRay& r, float4 ro, float4 rd)
 // per axis from the direction's sign.  The top `cached` nodes are read from
 // shared memory (sNodes), the rest through the read-only cache.
 struct NodeSlabs {
-    uint32_t childBase, triBase, meta0, meta1, imask;
+    uint32_t childBase, triBase, leafMask, imask;
     float ax, ay, az, bx, by, bz;
     uint32_t qn[6], qf[6];  // x0 x1 y0 y1 z0 z1: bytes of slots 0-3 and 4-7
 };
@@ -353,8 +352,7 @@ __device__ __forceinline__ void node_slabs(const WideAccelDev& acc, const WideNo
     s.bz = (__uint_as_float(w0.z) - r.o.z) * r.inv.z;
     s.childBase = w1.x;
     s.triBase = w1.y;
-    s.meta0 = w1.z;
-    s.meta1 = w1.w;
+    s.leafMask = w1.z;
     const bool px = r.inv.x >= 0.0f, py = r.inv.y >= 0.0f, pz = r.inv.z >= 0.0f;
     s.qn[0] = px ? w2.x : w3.z; s.qn[1] = px ? w2.y : w3.w;
     s.qf[0] = px ? w3.z : w2.x; s.qf[1] = px ? w3.w : w2.y;
@@ -379,10 +377,6 @@ __device__ __forceinline__ void child_span(const NodeSlabs& s, float tmin, float
     tf = fminf(fminf(tfx, tfy), fminf(tfz, closest));
 }
 
-template <int k>
-__device__ __forceinline__ uint32_t meta_of(const NodeSlabs& s) {
-    return byte_of(k < 4 ? s.meta0 : s.meta1, k & 3);
-}
 
 // One node of the traversal in exact front-to-back order: the hit internal
 // children are sorted by entry distance, the nearest entered and the others
@@ -402,27 +396,25 @@ __device__ __forceinline__ bool visit_sorted(const WideAccelDev& acc, const Wide
     // internal children that are hit, keyed by entry distance:
     // (distance bits with the low three cleared) | slot
     uint32_t key[8];
-    uint32_t leafHits = 0;  // bit slot for each hit leaf child
+    uint32_t m = 0;  // bit slot for each hit slot
     auto child = [&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        key[k] = 0xFFFFFFFFu;
-        const uint32_t meta = meta_of<k>(s);
-        if (meta == 0u) return;
         float tn, tf;
         child_span<k>(s, r.tmin, r.closest, tn, tf);
         const bool hit = tn <= tf;
-        if (hit && (meta & 0x40u)) leafHits |= 1u << k;
-        if (hit && !(meta & 0x40u)) key[k] = (__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k);
+        key[k] = (hit && ((s.imask >> k) & 1u)) ? ((__float_as_uint(tn) & 0x7FFFFFF8u) | uint32_t(k))
+                                                : 0xFFFFFFFFu;
+        if (hit) m |= 1u << k;
     };
     child(IntC<0>{}); child(IntC<1>{}); child(IntC<2>{}); child(IntC<3>{});
     child(IntC<4>{}); child(IntC<5>{}); child(IntC<6>{}); child(IntC<7>{});
+    uint32_t leafHits = m & s.leafMask;
     while (leafHits) {
         const uint32_t k = uint32_t(__ffs(int(leafHits)) - 1);
         leafHits &= leafHits - 1u;
-        const uint32_t meta = ((k < 4 ? s.meta0 : s.meta1) >> (8u * (k & 3u))) & 0xFFu;
         if (kCount) triTests++;
-        tri_test(acc, s.triBase + (meta & 0x3Fu), r.o, r.d, r.tmin, r.closest, r.hitTri, r.hb0,
-                 r.hb1);
+        tri_test(acc, s.triBase + uint32_t(__popc(s.leafMask & ((1u << k) - 1u))), r.o, r.d,
+                 r.tmin, r.closest, r.hitTri, r.hb0, r.hb1);
     }
     sort8(key);
     // push the farther hits (farthest first), enter the nearest
@@ -433,8 +425,7 @@ __device__ __forceinline__ bool visit_sorted(const WideAccelDev& acc, const Wide
         const float tn = __uint_as_float(key[j] & ~7u);
         if (tn > r.closest) continue;
         const uint32_t slot = key[j] & 7u;
-        const uint32_t meta = byte_of(slot < 4 ? s.meta0 : s.meta1, int(slot & 3u));
-        const uint32_t c = s.childBase + (meta & 0x3Fu);
+        const uint32_t c = s.childBase + uint32_t(__popc(s.imask & ((1u << slot) - 1u)));
         if (j == 0) {
             next = int(c);
         } else if (r.sp < kStack) {
@@ -471,28 +462,29 @@ __device__ __forceinline__ bool visit_octant(const WideAccelDev& acc, const Wide
     if (kCount) nodeVisits++;
     NodeSlabs s;
     node_slabs(acc, sNodes, cached, r.node, r, s);
-    uint32_t hits = 0;      // bit (slot ^ oct) for each hit internal child
-    uint32_t leafHits = 0;  // bit slot for each hit leaf child
+    uint32_t m = 0;  // bit slot for each hit slot
     auto child = [&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        const uint32_t meta = meta_of<k>(s);
-        if (meta == 0u) return;
         float tn, tf;
         child_span<k>(s, r.tmin, r.closest, tn, tf);
-        const bool hit = tn <= tf;
-        if (hit && (meta & 0x40u)) leafHits |= 1u << k;
-        if (hit && !(meta & 0x40u)) hits |= 1u << (uint32_t(k) ^ r.oct);
+        if (tn <= tf) m |= 1u << k;
     };
     child(IntC<0>{}); child(IntC<1>{}); child(IntC<2>{}); child(IntC<3>{});
     child(IntC<4>{}); child(IntC<5>{}); child(IntC<6>{}); child(IntC<7>{});
+    uint32_t leafHits = m & s.leafMask;
     while (leafHits) {
         const uint32_t k = uint32_t(__ffs(int(leafHits)) - 1);
         leafHits &= leafHits - 1u;
-        const uint32_t meta = ((k < 4 ? s.meta0 : s.meta1) >> (8u * (k & 3u))) & 0xFFu;
         if (kCount) triTests++;
-        tri_test(acc, s.triBase + (meta & 0x3Fu), r.o, r.d, r.tmin, r.closest, r.hitTri, r.hb0,
-                 r.hb1);
+        tri_test(acc, s.triBase + uint32_t(__popc(s.leafMask & ((1u << k) - 1u))), r.o, r.d,
+                 r.tmin, r.closest, r.hitTri, r.hb0, r.hb1);
     }
+    // hit internal children, bit k moved to k ^ oct (swapping bit pairs,
+    // then pairs of pairs, then nibbles, as the octant's bits say)
+    uint32_t hits = m & s.imask;
+    hits = (r.oct & 1u) ? (((hits & 0x55u) << 1) | ((hits >> 1) & 0x55u)) : hits;
+    hits = (r.oct & 2u) ? (((hits & 0x33u) << 2) | ((hits >> 2) & 0x33u)) : hits;
+    hits = (r.oct & 4u) ? (((hits & 0x0Fu) << 4) | ((hits >> 4) & 0x0Fu)) : hits;
     uint32_t base = s.childBase, im = s.imask;
     if (hits == 0) {  // resume the most recent group with pending children
         if (r.sp == 0) {
