@@ -188,6 +188,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         return run_guided(args, g, m, torch, dev)
     if args.only == "learned":
         return {"learned": run_learned(args, m, system, torch)}
+    if args.only == "closed":
+        return {"closed_scene": run_closed(args, m, system, torch)}
     t = m.PathTracer(system, g)
     t.set_options(dict(OPTS, Seed=1 + rank))
     _attach_filter(system, t)
@@ -1013,9 +1015,10 @@ def main():
     ap.add_argument("--learned-kinds", default="",
                     help="comma list of plain,wfpg_bxdf,svo,learned_1,learned_4,"
                          "learned_1_octree (default all)")
-    ap.add_argument("--only", choices=["all", "guided", "learned"], default="all",
+    ap.add_argument("--only", choices=["all", "guided", "learned", "closed"], default="all",
                     help="guided: only the WFPG timing (for profiling a small case); "
-                         "learned: only the learned-guiding comparison")
+                         "learned: only the learned-guiding comparison; closed: only the "
+                         "closed-scene entry")
     ap.add_argument("--res", default="1920x1080",
                     help="image size WxH (the workload is 1920x1080; smaller for profiling)")
     args = ap.parse_args()
