@@ -241,7 +241,12 @@ __global__ void k_reset_count(uint32_t* c) {
 // ---------------------------------------------------------------------------
 // Traversal
 // ---------------------------------------------------------------------------
-constexpr int kCachedNodes = 73;  // 1 + 8 + 64: the top three levels
+// The top two levels (1 + 8 nodes) are read from shared memory.  Three
+// levels (73 nodes, 5.8 KB per block) measured 2 % slower on both
+// clusters-1M and Cornell: the smaller carve-out leaves more of the SM's
+// on-chip memory to L1, which serves the lower levels.  None at all was
+// faster on clusters-1M but 13 % slower on Cornell.
+constexpr int kCachedNodes = 9;
 constexpr int kWideStack = 128;  // sorted order: one entry per pushed child
 constexpr int kWideGroups = 48;  // octant order: at most one group per level
 
