@@ -600,14 +600,14 @@ __device__ __forceinline__ void add_work(unsigned long long* counters, uint32_t 
     }
 }
 
-// Resident blocks per SM: the traversal's dependent loads and ALU chains
-// want resident warps more than registers.  Sorted order: nine 128-thread
-// blocks (56 registers; on clusters-1M 8 blocks 4.77 ms, 9 blocks 4.57 ms,
-// 10 blocks 5.27 ms per frame of traversal).  Octant order, whose node loop
-// is leaner: eight (64 registers, no spill; 2.66 ms against 2.70 at nine and
-// 2.84 at ten, which spills).
+// Eight 128-thread blocks per SM (64 registers, no spill): the traversal's
+// dependent loads and ALU chains want resident warps more than registers,
+// but not at the price of spills.  Octant order on clusters-1M: 2.66 ms of
+// traversal per frame at eight blocks, 2.70 at nine (56 registers), 2.84 at
+// ten (48, spilling); sorted order on the closed Cornell frame: 34.5 ms at
+// eight, 34.9 at nine.
 template <bool kCount, bool kOctant>
-__global__ void __launch_bounds__(128, kOctant ? 8 : 9) k_trace_wide(WideAccelDev acc,
+__global__ void __launch_bounds__(128, 8) k_trace_wide(WideAccelDev acc,
                                                     const float4* __restrict__ rayO,
                                                     const float4* __restrict__ rayD,
                                                     const uint32_t* __restrict__ dCount,
@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(128, kOctant ? 8 : 9) k_trace_wide(WideAccelDe
 constexpr int kRefillLanes = 8;
 
 template <bool kCount, bool kOctant>
-__global__ void __launch_bounds__(128, kOctant ? 8 : 9) k_trace_wide_refill(WideAccelDev acc,
+__global__ void __launch_bounds__(128, 8) k_trace_wide_refill(WideAccelDev acc,
                                                            const float4* __restrict__ rayO,
                                                            const float4* __restrict__ rayD,
                                                            const uint32_t* __restrict__ dCount,
