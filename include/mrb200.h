@@ -354,6 +354,17 @@ int mrb_tracer_svo_export(mrb_tracer* t, uint64_t* nodes, uint32_t* leaf_parents
                           uint64_t* leaf_codes, uint32_t* leaf_norm_spec, uint32_t* leaf_lights,
                           uint32_t* level_offsets, uint32_t* node_norm_spec, uint64_t* leaf_irr,
                           uint32_t* leaf_cnt, uint32_t* leaf_avg, uint32_t* node_avg);
+/* The octree's shadow-ray statistics (VoxelPayload dShadowRayHitLeaf /
+ * dShadowRayMissLeaf and dGuidingFactorNode, AnisoSVO.cuh:75-85):
+ * leaf_shadow[2 * leaf] counts the rays launched from a path vertex in the
+ * leaf whose light contribution was taken (a NEE ray reaching its light, or
+ * a path ray reaching a light or the boundary where the boundary work
+ * accepts it), leaf_shadow[2 * leaf + 1] the NEE rays stopped by a surface
+ * (DepositNEEHitMiss, WFPGTracerKC.cuh:194, 258), summed since the octree
+ * was built or loaded; node_factor[node] is the binary16 guiding factor, the
+ * mean of the children's miss ratios (NaN: none of the leaves below has a
+ * shadow ray), as of the last NormalizeAndFilterRadiance.  NULL skips. */
+int mrb_tracer_svo_guiding(mrb_tracer* t, uint32_t* leaf_shadow, uint16_t* node_factor);
 /* Guide state of the wavefront shaded by the last Render() step of a WFPG
  * frame: ray count, per ray its path (sample) index and guide words (uv
  * half2 | pdf half + flags bit16 BxDF-selected, bit17 valid), and the

@@ -83,6 +83,7 @@ def _load() -> C.CDLL:
         "mrb_tracer_set_option_float": (i32, [vp, C.c_char_p, C.c_double]),
         "mrb_tracer_svo_info": (i32, [vp, vp, vp]),
         "mrb_tracer_svo_export": (i32, [vp] + [vp] * 11),
+        "mrb_tracer_svo_guiding": (i32, [vp, vp, vp]),
         "mrb_tracer_guide_export": (i32, [vp, C.POINTER(u32), vp, vp, vp, vp]),
         "mrb_tracer_create": (i32, [vp, vp, C.c_char_p, C.POINTER(vp)]),
         "mrb_tracer_destroy": (None, [vp]),

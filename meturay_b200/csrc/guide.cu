@@ -719,6 +719,15 @@ __global__ void __launch_bounds__(256) k_path_deposit(GuideDev g, PathChain pc,
             const V3 wo = normalize(v3(pa.x, pa.y, pa.z) - pos);
             uint32_t leaf;
             if (!svo_nearest(g, leaf, pos, g.leafDepth)) continue;
+            if (d + 1 <= lastD) {
+                // DepositNEEHitMiss (AnisoSVO.cuh:1101-1115) of the rays this
+                // vertex launched, at its own leaf
+                const float en = pc.contribNee[size_t(d + 1) * P + p].w;
+                const float ep = pc.contribPath[size_t(d + 1) * P + p].w;
+                const uint32_t hits = (en == kChainHit ? 1u : 0u) + (ep == kChainHit ? 1u : 0u);
+                if (hits) atomicAdd(g.leafShadow + 2 * leaf, hits);
+                if (en == kChainMiss) atomicAdd(g.leafShadow + 2 * leaf + 1, 1u);
+            }
             float sd, sp;
             const V3 n = read_normal_spec(g.leafNormSpec[leaf], sd, sp);
             const float NdL = dot(n, wo);
@@ -753,7 +762,11 @@ __global__ void __launch_bounds__(256) k_leaf_normalize(GuideDev g) {
 // KCBottomUpFilterIrradiance: per node, the children's averages on the
 // side that matches the node normal (swapped where the child's normal
 // faces away); children at HALF_MAX carry no data.  The sum runs in FP32
-// and is rounded to FP16 once.
+// and is rounded to FP16 once.  The guiding factor is the FP32 mean of the
+// children's factors that are not NaN, rounded to FP16 (AnisoSVO.cu:
+// 586-613); a leaf's factor is misses / (hits + misses) of its shadow rays
+// (VoxelPayload::ReadGuidingFactor, AnisoSVO.cuh:477-488), NaN without any.
+// A node whose children are all NaN gets the binary16 NaN 0x7FFF (0 / 0).
 __global__ void __launch_bounds__(256) k_bottom_up(GuideDev g, uint32_t begin, uint32_t end,
                                                    int childrenAreLeaf) {
     for (uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x; k < end;
@@ -764,8 +777,22 @@ __global__ void __launch_bounds__(256) k_bottom_up(GuideDev g, uint32_t begin, u
         const V3 n = read_normal_spec(g.nodeNormSpec[k], sd, sp);
         float sum[2] = {0.0f, 0.0f};
         uint32_t valid[2] = {0u, 0u};
+        float factorSum = 0.0f;
+        uint32_t factorValid = 0;
         for (uint32_t i = 0; i < cnt; i++) {
             const uint32_t c = ci + i;
+            float factor;
+            if (childrenAreLeaf) {
+                const uint2 hm = reinterpret_cast<const uint2*>(g.leafShadow)[c];
+                const float hit = static_cast<float>(hm.x), miss = static_cast<float>(hm.y);
+                factor = miss / (hit + miss);
+            } else {
+                factor = h2f(g.nodeFactor[c]);
+            }
+            if (!isnan(factor)) {
+                factorValid++;
+                factorSum += factor;
+            }
             const uint32_t irr = childrenAreLeaf ? g.leafAvg[c] : g.nodeAvg[c];
             const V3 cn = read_normal_spec(childrenAreLeaf ? g.leafNormSpec[c] : g.nodeNormSpec[c],
                                            sd, sp);
@@ -786,6 +813,8 @@ __global__ void __launch_bounds__(256) k_bottom_up(GuideDev g, uint32_t begin, u
             w |= uint32_t(h) << (16 * j);
         }
         g.nodeAvg[k] = w;
+        g.nodeFactor[k] =
+            factorValid ? f2h(factorSum / static_cast<float>(factorValid)) : kFactorNone;
     }
 }
 
@@ -873,6 +902,8 @@ GuideDev guide_dev(const SvoResult& v, const SvoParams& p) {
     g.leafCnt = v.leafCnt;
     g.leafAvg = v.leafAvg;
     g.nodeAvg = v.nodeAvg;
+    g.leafShadow = v.leafShadow;
+    g.nodeFactor = v.nodeFactor;
     g.leafBin = v.leafBin;
     g.nodeBin = v.nodeBin;
     return g;

@@ -14,9 +14,13 @@
 // This core keeps bin words as 32-bit (mark bit 31, 31-bit count), leaf sums
 // in 2^-24 fixed point and averages as half pairs; the dump converts each to
 // the reference's field (16-bit bin info with mark bit 15 and a 15-bit
-// count, FP32 sums, FP32 averages) and the load converts back.  Guiding
-// factors are not kept by this core: they are written as 0 and skipped on
-// load (the reference's loader skips the leaf array as well).
+// count, FP32 sums, FP32 averages) and the load converts back.  The node
+// guiding factor field holds N bytes of the binary16 node factors as they
+// lie in memory (the first N / 2 factors: the reference copies N bytes of
+// its half array); the leaf factor field stays 0 (the reference writes
+// nothing there).  The load puts the N bytes back at the start of the half
+// array, marks the rest NaN (no data) and starts the shadow-ray counters at
+// zero; the next NormalizeAndFilterRadiance recomputes every factor.
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -88,13 +92,15 @@ int svo_dump(const SvoResult& v, const SvoParams& P, std::vector<uint8_t>& out, 
     std::vector<uint32_t> nodeBin(N), nodeAvg(N), nodeNs(N), leafParents(U), leafBin(U),
         leafCnt(2 * U), leafAvg(U), leafNs(U);
     std::vector<unsigned long long> leafIrr(2 * U);
+    std::vector<uint16_t> nodeFactor(N);
     if (d2h(nodes.data(), v.nodes, N * 8, st) || d2h(nodeBin.data(), v.nodeBin, N * 4, st) ||
         d2h(nodeAvg.data(), v.nodeAvg, N * 4, st) || d2h(nodeNs.data(), v.nodeNormSpec, N * 4, st) ||
         d2h(leafParents.data(), v.leafParents, U * 4, st) ||
         d2h(leafBin.data(), v.leafBin, U * 4, st) || d2h(leafCnt.data(), v.leafCnt, U * 8, st) ||
         d2h(leafAvg.data(), v.leafAvg, U * 4, st) ||
         d2h(leafNs.data(), v.leafNormSpec, U * 4, st) ||
-        d2h(leafIrr.data(), v.leafIrr, U * 16, st))
+        d2h(leafIrr.data(), v.leafIrr, U * 16, st) ||
+        d2h(nodeFactor.data(), v.nodeFactor, N * 2, st))
         return MRB_E_CUDA;
     MRB_CUDA(cudaStreamSynchronize(st));
     size_t off = 0;
@@ -120,7 +126,8 @@ int svo_dump(const SvoResult& v, const SvoParams& P, std::vector<uint8_t>& out, 
     }
     put(out, off, f2.data(), 2 * N);
     put(out, off, nodeNs.data(), N);
-    off += N;  // node guiding factors: 0
+    std::memcpy(out.data() + off, nodeFactor.data(), N);  // N bytes of the half array
+    off += N;
     for (size_t i = 0; i < 2 * U; i++) f2[i] = fixed_to_float(leafIrr[i]);
     put(out, off, f2.data(), 2 * U);
     put(out, off, leafCnt.data(), 2 * U);
@@ -221,7 +228,9 @@ int svo_load(const uint8_t* data, size_t size, SvoParams& P, SvoResult& out, cud
     for (uint32_t i = 0; i < N; i++)
         nodeAvg[i] = uint32_t(f2h(f2[2 * i])) | (uint32_t(f2h(f2[2 * i + 1])) << 16);
     get(data, off, nodeNs.data(), N);
-    off += N;  // node guiding factors
+    std::vector<uint16_t> nodeFactor(N, kFactorNone);
+    std::memcpy(nodeFactor.data(), data + off, N);
+    off += N;
     get(data, off, f2.data(), 2 * size_t(U));
     for (size_t i = 0; i < 2 * size_t(U); i++) leafIrr[i] = float_to_fixed(f2[i]);
     get(data, off, leafCnt.data(), 2 * size_t(U));
@@ -256,6 +265,8 @@ int svo_load(const uint8_t* data, size_t size, SvoParams& P, SvoResult& out, cud
         (r = alloc(reinterpret_cast<void**>(&v.leafCnt), size_t(U) * 8)) ||
         (r = alloc(reinterpret_cast<void**>(&v.leafAvg), size_t(U) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&v.nodeAvg), size_t(N) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&v.leafShadow), size_t(U) * 8)) ||
+        (r = alloc(reinterpret_cast<void**>(&v.nodeFactor), size_t(N) * 2)) ||
         (r = alloc(reinterpret_cast<void**>(&v.leafBin), size_t(U) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&v.nodeBin), size_t(N) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&v.dLevelOffsets), size_t(L) * 4))) {
@@ -272,6 +283,8 @@ int svo_load(const uint8_t* data, size_t size, SvoParams& P, SvoResult& out, cud
         h2d(v.nodeAvg, nodeAvg.data(), size_t(N) * 4, st) ||
         h2d(v.leafBin, leafBin.data(), size_t(U) * 4, st) ||
         h2d(v.nodeBin, nodeBin.data(), size_t(N) * 4, st) ||
+        h2d(v.nodeFactor, nodeFactor.data(), size_t(N) * 2, st) ||
+        cudaMemsetAsync(v.leafShadow, 0, size_t(U) * 8, st) != cudaSuccess ||
         h2d(v.dLevelOffsets, levelOffsets.data(), size_t(L) * 4, st)) {
         svo_free(v);
         return MRB_E_CUDA;

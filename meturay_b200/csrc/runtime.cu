@@ -746,7 +746,8 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
     const bool gen = (d + 1) < t->maxDepth;
     if (mark(4)) return MRB_E_CUDA;
     r = shade(sc->dev(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
-              t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull, t->maxRays,
+              t->aux[cur].as<RayAux>(), hi, t->sortedIds.as<uint32_t>(), pt.nonNull, cnt + cur,
+              t->maxRays,
               t->samplesBuf.as<float4>(), path_options(t), gen, t->rayO[nxt].as<float4>(),
               t->rayD[nxt].as<float4>(), t->aux[nxt].as<RayAux>(), cnt + nxt, path_chain(t),
               guideNow ? t->guideBuf.as<uint2>() : nullptr, t->stream);
@@ -1746,7 +1747,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         }
         // the octree's radiance state of a WFPG tracer is put back too
         const size_t U = t->svo.leafCount, N = t->svo.nodeCount;
-        const size_t pb = t->wfpg ? U * 16 + U * 8 + U * 4 + N * 4 : 0;
+        const size_t pb = t->wfpg ? U * 16 + U * 8 + U * 4 + N * 4 + U * 8 + N * 2 : 0;
         if (pb) {
             if ((r = t->payloadBackup.alloc(pb))) return r;
             char* b = t->payloadBackup.as<char>();
@@ -1754,6 +1755,10 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             MRB_CUDA(cudaMemcpyAsync(b + U * 16, t->svo.leafCnt, U * 8, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(b + U * 24, t->svo.leafAvg, U * 4, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(b + U * 28, t->svo.nodeAvg, N * 4, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(b + U * 28 + N * 4, t->svo.leafShadow, U * 8,
+                                     cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(b + U * 36 + N * 4, t->svo.nodeFactor, N * 2,
+                                     cudaMemcpyDeviceToDevice, t->stream));
         }
         if (t->net && mlp_state_copy(t->net, t->netBackup.p, true, t->stream)) return MRB_E_CUDA;
         if (t->net)
@@ -1800,6 +1805,10 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
             MRB_CUDA(cudaMemcpyAsync(t->svo.leafCnt, b + U * 16, U * 8, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(t->svo.leafAvg, b + U * 24, U * 4, cudaMemcpyDeviceToDevice, t->stream));
             MRB_CUDA(cudaMemcpyAsync(t->svo.nodeAvg, b + U * 28, N * 4, cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->svo.leafShadow, b + U * 28 + N * 4, U * 8,
+                                     cudaMemcpyDeviceToDevice, t->stream));
+            MRB_CUDA(cudaMemcpyAsync(t->svo.nodeFactor, b + U * 36 + N * 4, N * 2,
+                                     cudaMemcpyDeviceToDevice, t->stream));
         }
         MRB_CUDA(cudaMemcpyAsync(t->image.p, t->imageBackup.p, t->image.bytes,
                                  cudaMemcpyDeviceToDevice, t->stream));
@@ -2015,6 +2024,18 @@ int mrb_tracer_svo_export(mrb_tracer* t, uint64_t* nodes, uint32_t* leafParents,
                         levelOffsets)))
         return r;
     return export_payload(t->svo, nodeNormSpec, leafIrr, leafCnt, leafAvg, nodeAvg);
+}
+
+int mrb_tracer_svo_guiding(mrb_tracer* t, uint32_t* leafShadow, uint16_t* nodeFactor) {
+    if (!t || !t->wfpg) return MRB_E_ARG;
+    if (set_device(t->sys)) return MRB_E_CUDA;
+    int r = ensure_svo(t);
+    if (r) return r;
+    MRB_CUDA(cudaStreamSynchronize(t->stream));
+    if (svo_copy(leafShadow, t->svo.leafShadow, size_t(t->svo.leafCount) * 8) ||
+        svo_copy(nodeFactor, t->svo.nodeFactor, size_t(t->svo.nodeCount) * 2))
+        return MRB_E_CUDA;
+    return 0;
 }
 
 int mrb_tracer_guide_export(mrb_tracer* t, uint32_t* count, uint32_t* samples, uint32_t* guide2,

@@ -160,6 +160,7 @@ struct ShadeArgs {
     HitIn hit;
     const uint32_t* sortedIds;
     const uint32_t* nonNull;
+    const uint32_t* count;  // all rays of the wavefront
     float4* samples;
     PathOptions opt;
     int gen;
@@ -186,7 +187,9 @@ template <bool kMulti>
 // kernel's gathers want resident warps (closed Cornell 1080p frame: 11.9 ->
 // 11.2 ms of shading at 112 -> 80 registers).
 __global__ void __launch_bounds__(128, 6) k_shade(ShadeArgs A) {
-    const uint32_t n = *A.nonNull;
+    // the WFPG tracer also visits the rays that left the scene (sorted
+    // last), for the shadow-ray events of the boundary work
+    const uint32_t n = (!kMulti && A.opt.wfpg) ? *A.count : *A.nonNull;
     const uint32_t tracerFrame = kMulti ? 0u : *A.opt.frame;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t ltMask = (1u << lane) - 1u;
@@ -254,10 +257,23 @@ __global__ void __launch_bounds__(128, 6) k_shade(ShadeArgs A) {
                     if (A.opt.wfpg && !camera) {
                         float4* c = (aux.type == kNeeRay) ? A.chain.contribNee : A.chain.contribPath;
                         c[size_t(aux.depth) * A.chain.paths + aux.sample] =
-                            make_float4(total.x, total.y, total.z, 0.0f);
+                            make_float4(total.x, total.y, total.z, kChainHit);
                     }
                 }
-            } else if (aux.type != kNeeRay && (gen || A.opt.wfpg)) {
+            } else if (batch == kBatchNull) {
+                // WFPGTracerBoundaryWork of the Null boundary light (emits
+                // zero): the rays it accepts still count as reaching a light
+                // for the vertex that launched them (WFPGTracerKC.cuh:163-195)
+                const bool accepted = aux.type == kSpecPathRay ||
+                                      (aux.type == kPathRay && (oMis || !oNee));
+                if (accepted)
+                    A.chain.contribPath[size_t(aux.depth) * A.chain.paths + aux.sample].w = kChainHit;
+            } else if (aux.type == kNeeRay) {
+                // a NEE ray stopped by a surface (WFPGTracerPathWork,
+                // WFPGTracerKC.cuh:250-260)
+                if (A.opt.wfpg)
+                    A.chain.contribNee[size_t(aux.depth) * A.chain.paths + aux.sample].w = kChainMiss;
+            } else if (gen || A.opt.wfpg) {
                 // PathTracerPathWork (PathTracerKC.cuh:428-649)
                 const uint32_t prim = A.hit.prim[rid];
                 const float2 hb = A.hit.bary[rid];
@@ -607,11 +623,11 @@ int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t 
 }
 
 int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayAux* aux,
-          const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull, uint32_t maxCount,
-          float4* samples, const PathOptions& opt, bool gen, float4* outO, float4* outD,
-          RayAux* outAux, uint32_t* outCount, const PathChain& chain, const uint2* guide,
-          cudaStream_t stream) {
-    ShadeArgs a{sc,   rayO,    rayD, aux,  hit,  sortedIds, nonNull, samples,
+          const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull,
+          const uint32_t* count, uint32_t maxCount, float4* samples, const PathOptions& opt,
+          bool gen, float4* outO, float4* outD, RayAux* outAux, uint32_t* outCount,
+          const PathChain& chain, const uint2* guide, cudaStream_t stream) {
+    ShadeArgs a{sc,   rayO,    rayD, aux,  hit,  sortedIds, nonNull, count, samples,
                 opt,  gen ? 1 : 0, outO, outD, outAux, outCount, chain, guide, nullptr};
     k_shade<false><<<grid_for(maxCount, 128, 148 * 16), 128, 0, stream>>>(a);
     MRB_CUDA(cudaGetLastError());
@@ -658,7 +674,7 @@ int shade_jobs(const JobDev* jobs, const float4* rayO, const float4* rayD, const
                uint32_t maxCount, float4* samples, float4* outO, float4* outD, RayAux* outAux,
                uint32_t* outCount, cudaStream_t stream) {
     PathOptions opt{};
-    ShadeArgs a{SceneDev{}, rayO, rayD, aux, hit, sortedIds, nonNull, samples, opt, 1,
+    ShadeArgs a{SceneDev{}, rayO, rayD, aux, hit, sortedIds, nonNull, nonNull, samples, opt, 1,
                 outO, outD, outAux, outCount, PathChain{}, nullptr, jobs};
     k_shade<true><<<grid_for(maxCount, 128, 148 * 16), 128, 0, stream>>>(a);
     MRB_CUDA(cudaGetLastError());

@@ -24,7 +24,13 @@ struct HitIn {
 //   nodeA = (vertex position, frame stamp bits); depth 0 is the camera
 //   nodeB = (path throughput arriving at the vertex, -)
 //   contribNee / contribPath = endpoint radiance reaching the chain from
-//   the NEE / path ray of that depth (AccumRadianceDownChain input)
+//   the NEE / path ray of that depth (AccumRadianceDownChain input); .w
+//   marks the shadow-ray event of that ray for the vertex that launched
+//   it (WFPGTracerKC.cuh:194, 258): kChainHit when its light contribution
+//   was taken (a light or the boundary reached by any non-camera ray the
+//   boundary work accepts), kChainMiss when a NEE ray hit a surface
+constexpr float kChainHit = 1.0f;
+constexpr float kChainMiss = 2.0f;
 struct PathChain {
     float4* nodeA;
     float4* nodeB;
@@ -48,10 +54,10 @@ int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount
 int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t maxCount,
                   uint32_t idBits, const PortionTable& table, cudaStream_t stream);
 int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayAux* aux,
-          const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull, uint32_t maxCount,
-          float4* samples, const PathOptions& opt, bool gen, float4* outO, float4* outD,
-          RayAux* outAux, uint32_t* outCount, const PathChain& chain, const uint2* guide,
-          cudaStream_t stream);
+          const HitIn& hit, const uint32_t* sortedIds, const uint32_t* nonNull,
+          const uint32_t* count, uint32_t maxCount, float4* samples, const PathOptions& opt,
+          bool gen, float4* outO, float4* outD, RayAux* outAux, uint32_t* outCount,
+          const PathChain& chain, const uint2* guide, cudaStream_t stream);
 int resolve(const float4* samples, uint32_t width, uint32_t height, uint32_t sp, float4* image,
             cudaStream_t stream);
 int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream);

@@ -611,6 +611,8 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
         (r = alloc(reinterpret_cast<void**>(&out.leafCnt), size_t(U) * 8)) ||
         (r = alloc(reinterpret_cast<void**>(&out.leafAvg), size_t(U) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&out.nodeAvg), size_t(out.nodeCount) * 4)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.leafShadow), size_t(U) * 8)) ||
+        (r = alloc(reinterpret_cast<void**>(&out.nodeFactor), size_t(out.nodeCount) * 2)) ||
         (r = alloc(reinterpret_cast<void**>(&out.leafBin), size_t(U) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&out.nodeBin), size_t(out.nodeCount) * 4)) ||
         (r = alloc(reinterpret_cast<void**>(&out.dLevelOffsets), out.levelOffsets.size() * 4))) {
@@ -637,6 +639,8 @@ int svo_build(const SvoBuildIn& in, const SvoParams& P, SvoResult& out, cudaStre
     k_leaf_payload<<<grid_of(U), 256, 0, st>>>(out.leafRunStart, vidx, vnorm, vlight, in.lightRad,
                                               in.omitDirect, U, out.leafNormSpec, out.leafIrr,
                                               out.leafCnt, out.leafLight);
+    // shadow-ray counters start at zero (AnisoSVO.cu:1029-1030)
+    MRB_CUDA(cudaMemsetAsync(out.leafShadow, 0, size_t(U) * 8, st));
     MRB_CUDA(cudaMemcpyAsync(out.dLevelOffsets, out.levelOffsets.data(),
                              out.levelOffsets.size() * 4, cudaMemcpyHostToDevice, st));
     MRB_CUDA(cudaGetLastError());
@@ -657,6 +661,8 @@ void svo_free(SvoResult& r) {
     cudaFree(r.leafCnt);
     cudaFree(r.leafAvg);
     cudaFree(r.nodeAvg);
+    cudaFree(r.leafShadow);
+    cudaFree(r.nodeFactor);
     cudaFree(r.leafBin);
     cudaFree(r.nodeBin);
     cudaFree(r.dLevelOffsets);

@@ -40,6 +40,9 @@ struct SvoResult {
     uint32_t* leafCnt = nullptr;           // 2 per leaf, sample counts
     uint32_t* leafAvg = nullptr;           // half2 averages (front | back << 16)
     uint32_t* nodeAvg = nullptr;
+    uint32_t* leafShadow = nullptr;        // 2 per leaf: NEE shadow rays that reached / missed
+                                           // their light from a vertex in the leaf
+    uint16_t* nodeFactor = nullptr;        // half: guiding factor (mean miss ratio of the children)
     uint32_t* leafBin = nullptr;           // ray bins: mark bit 31 | ray count
     uint32_t* nodeBin = nullptr;
     uint32_t* dLevelOffsets = nullptr;     // device copy of levelOffsets

@@ -220,6 +220,8 @@ constexpr uint32_t kBinMark = 0x80000000u;          // bin word: mark bit | ray 
 constexpr uint32_t kBinLeaf = 0x80000000u;          // bin id: leaf flag | index
 constexpr uint32_t kBinInvalid = 0xFFFFFFFFu;
 constexpr uint16_t kHalfMax = 0x7BFFu;              // 65504
+constexpr uint16_t kFactorNone = 0x7FFFu;           // guiding factor without data: the binary16
+                                                    // NaN the reference's conversion of NaN gives
 constexpr double kFixScale = 16777216.0;            // radiance sums: 2^24 fixed point
 
 struct GuideDev {
@@ -236,6 +238,8 @@ struct GuideDev {
     uint32_t* leafCnt;             // 2 per leaf: sample counts
     uint32_t* leafAvg;             // half2: averaged radiance (front | back << 16)
     uint32_t* nodeAvg;
+    uint32_t* leafShadow;          // 2 per leaf: NEE shadow rays that reached / missed their light
+    uint16_t* nodeFactor;          // half: mean miss ratio of the children (kFactorNone: no data)
     // ray bins
     uint32_t* leafBin;
     uint32_t* nodeBin;

@@ -470,6 +470,9 @@ class WFPGTracer(PathTracer):
         check(lib.mrb_tracer_svo_info(self._h, _ptr(info), _ptr(params)))
         out = _svo_arrays(info, params)
         check(lib.mrb_tracer_svo_export(self._h, *[_ptr(out[k]) for k in _SVO_KEYS + _PAYLOAD_KEYS]))
+        out["leaf_shadow"] = np.zeros((out["leaves"], 2), np.uint32)
+        out["node_factor"] = np.zeros(out["nodes_count"], np.uint16)
+        check(lib.mrb_tracer_svo_guiding(self._h, _ptr(out["leaf_shadow"]), _ptr(out["node_factor"])))
         return out
 
     def guide_state(self) -> dict:

@@ -1237,9 +1237,14 @@ struct Chain {
     std::vector<float> rf;       // levels * paths * 3
     std::vector<uint8_t> valid;  // levels * paths
     std::vector<float> nee, path;
+    // shadow-ray event of the NEE / path ray of each slot for the vertex
+    // that launched it: 1 its light contribution was taken, 2 (NEE only)
+    // it was stopped by a surface
+    std::vector<uint8_t> eventNee, eventPath;
     Chain(uint32_t L, uint32_t P)
         : levels(L), paths(P), pos(size_t(L) * P * 3, 0.0f), rf(size_t(L) * P * 3, 0.0f),
-          valid(size_t(L) * P, 0), nee(size_t(L) * P * 3, 0.0f), path(size_t(L) * P * 3, 0.0f) {}
+          valid(size_t(L) * P, 0), nee(size_t(L) * P * 3, 0.0f), path(size_t(L) * P * 3, 0.0f),
+          eventNee(size_t(L) * P, 0), eventPath(size_t(L) * P, 0) {}
     size_t at(uint32_t d, uint32_t p) const { return size_t(d) * paths + p; }
 };
 
@@ -1276,6 +1281,7 @@ void path_work(Ctx<T>& c, const PRay<T>& r, uint32_t prim, T ha, T hb, uint32_t 
             if (aux.depth + 1 < chain->levels) {
                 const size_t nx = chain->at(aux.depth + 1, aux.sample);
                 for (int k = 0; k < 3; k++) chain->nee[3 * nx + k] = chain->path[3 * nx + k] = 0.0f;
+                chain->eventNee[nx] = chain->eventPath[nx] = 0;
             }
         }
     }
@@ -1467,6 +1473,8 @@ void boundary_work(Ctx<T>& c, const PRay<T>& r, uint32_t lightIdx, uint32_t prim
                 dst[0] = total.x;
                 dst[1] = total.y;
                 dst[2] = total.z;
+                // DepositNEEHitMiss(prev vertex, hit) (WFPGTracerKC.cuh:192-194)
+                ((aux.type == NEE_RAY) ? chain->eventNee : chain->eventPath)[at] = 1;
             }
         }
     }
@@ -1701,6 +1709,10 @@ struct oracle_svo {
     // radiance-cache payload (VoxelPayload, AnisoSVO.cuh:22-114)
     std::vector<uint32_t> leafNormSpec, nodeNormSpec, leafAvg, nodeAvg, leafBin, nodeBin, leafCnt;
     std::vector<uint64_t> leafIrr;
+    // shadow-ray counters (hits, misses per leaf) and binary16 node guiding
+    // factors (dShadowRayHitLeaf / dShadowRayMissLeaf / dGuidingFactorNode)
+    std::vector<uint32_t> leafShadow;
+    std::vector<uint16_t> nodeFactor;
 };
 
 namespace {
@@ -2099,9 +2111,14 @@ void bin_rays(oracle_svo* svo, uint32_t n, uint32_t minLevel, uint32_t binRayCou
 // VoxelPayload::WriteLeafRadiance (:490-537): the leaf of the vertex (with the
 // neighbour search), the side its normal puts wo on, one sample of the
 // luminance there (2^-24 fixed point).  False when no leaf is found.
-bool deposit_leaf(oracle_svo* svo, const Tree& tree, F3 pos, F3 wo, float luminance) {
+// With hits / misses it is also DepositNEEHitMiss (AnisoSVO.cuh:1101-1115)
+// at the same leaf.
+bool deposit_leaf(oracle_svo* svo, const Tree& tree, F3 pos, F3 wo, float luminance,
+                  uint32_t hits = 0, uint32_t misses = 0) {
     uint32_t leaf;
     if (!tree.nearest(leaf, pos, svo->P.depth)) return false;
+    svo->leafShadow[2 * leaf] += hits;
+    svo->leafShadow[2 * leaf + 1] += misses;
     float sd, spc;
     const F3 n = read_normal_spec(svo->leafNormSpec[leaf], sd, spc);
     const float NdL = dot(n, wo);
@@ -2127,6 +2144,8 @@ void payload_init(oracle_svo* o, const float* lightRad, uint32_t omit) {
     o->nodeNormSpec.assign(N, 0);
     o->leafBin.assign(U, 0);
     o->nodeBin.assign(N, 0);
+    o->leafShadow.assign(2 * size_t(U), 0);
+    o->nodeFactor.assign(N, 0x7FFFu);
     for (uint32_t j = 0; j < U; j++) {
         const uint32_t b = o->runStart[j], e = o->runStart[j + 1], dup = e - b;
         const F3 n0 = unpack_normal16(o->voxNormal[o->runVoxel[b]]);
@@ -2237,8 +2256,22 @@ void normalize_filter(oracle_svo* o) {
             const F3 n = read_normal_spec(o->nodeNormSpec[k], sd, sp);
             float sum[2] = {0.0f, 0.0f};
             uint32_t valid[2] = {0, 0};
+            // guiding factor (AnisoSVO.cu:586-613): mean of the children's
+            // factors that are not NaN; a leaf's is misses / (hits + misses)
+            // (VoxelPayload::ReadGuidingFactor, AnisoSVO.cuh:477-488)
+            float factorSum = 0.0f;
+            uint32_t factorValid = 0;
             for (uint32_t i = 0; i < cnt; i++) {
                 const uint32_t c = ci + i;
+                const float factor =
+                    childLeaf ? static_cast<float>(o->leafShadow[2 * c + 1]) /
+                                    (static_cast<float>(o->leafShadow[2 * c]) +
+                                     static_cast<float>(o->leafShadow[2 * c + 1]))
+                              : h2f(o->nodeFactor[c]);
+                if (!std::isnan(factor)) {
+                    factorValid++;
+                    factorSum += factor;
+                }
                 const uint32_t irr = childLeaf ? o->leafAvg[c] : o->nodeAvg[c];
                 const F3 cn = read_normal_spec(childLeaf ? o->leafNormSpec[c] : o->nodeNormSpec[c], sd, sp);
                 const bool swap = dot(cn, n) < 0.0f;
@@ -2258,6 +2291,8 @@ void normalize_filter(oracle_svo* o) {
                 w |= uint32_t(h) << (16 * j);
             }
             o->nodeAvg[k] = w;
+            // no child with data: 0 / 0, the binary16 NaN 0x7FFF
+            o->nodeFactor[k] = factorValid ? f2h(factorSum / static_cast<float>(factorValid)) : 0x7FFFu;
         }
     }
     for (uint32_t L = 1; L <= D; L++) {
@@ -2547,6 +2582,31 @@ extern "C" void oracle_svo_set_radiance(oracle_svo* o, const uint64_t* leafIrr,
 }
 
 extern "C" void oracle_svo_normalize(oracle_svo* o) { normalize_filter(o); }
+
+// DepositNEEHitMiss of n vertices over zeroed counters: is_hit[i] picks the
+// hit or the miss counter of the vertex's leaf.
+extern "C" void oracle_svo_deposit_nee(oracle_svo* o, const float* pos, const uint8_t* isHit,
+                                       uint32_t n) {
+    std::fill(o->leafShadow.begin(), o->leafShadow.end(), 0u);
+    Tree tree{o};
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t leaf;
+        if (!tree.nearest(leaf, F3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), o->P.depth)) continue;
+        o->leafShadow[2 * leaf + (isHit[i] ? 0 : 1)] += 1u;
+    }
+}
+
+// Shadow-ray counters (2 per leaf: hits, misses) in; NULL leaves them.
+extern "C" void oracle_svo_set_shadow(oracle_svo* o, const uint32_t* leafShadow) {
+    if (leafShadow) std::copy(leafShadow, leafShadow + o->leafShadow.size(), o->leafShadow.begin());
+}
+
+// Shadow-ray counters and binary16 node guiding factors out; NULL skips.
+extern "C" void oracle_svo_guiding_get(const oracle_svo* o, uint32_t* leafShadow,
+                                       uint16_t* nodeFactor) {
+    if (leafShadow) std::memcpy(leafShadow, o->leafShadow.data(), o->leafShadow.size() * 4);
+    if (nodeFactor) std::memcpy(nodeFactor, o->nodeFactor.data(), o->nodeFactor.size() * 2);
+}
 
 extern "C" void oracle_svo_deposit(oracle_svo* o, const float* pos, const float* wo,
                                    const float* lum, uint32_t n) {
@@ -3016,11 +3076,21 @@ extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* 
         const bool gen = (it + 1) < opt->max_depth;
         std::vector<PRay<float>> outs;
         for (WRay& wr : cur) {
-            if (wr.prim == kInvalid) continue;
             const uint32_t batch = wr.key >> 24, id = wr.key & 0xFFFFFFu;
-            if (batch == kBatchNull) continue;
+            const Aux<float>& ax = wr.r.aux;
+            if (wr.prim == kInvalid || batch == kBatchNull) {
+                // the Null boundary light's work: zero emission, but the rays
+                // it accepts count as reaching a light (WFPGTracerKC.cuh:163-195)
+                const bool accepted = ax.type == SPECULAR_PATH_RAY ||
+                                      (ax.type == PATH_RAY && (opt->mis || !opt->nee));
+                if (accepted) chain.eventPath[chain.at(ax.depth, ax.sample)] = 1;
+                continue;
+            }
             if (batch == kBatchLight) {
                 boundary_work(c, wr.r, id, wr.prim, wr.b0, wr.b1, wr.t, &chain);
+            } else if (ax.type == NEE_RAY) {
+                // DepositNEEHitMiss(prev vertex, miss) (WFPGTracerKC.cuh:250-260)
+                chain.eventNee[chain.at(ax.depth, ax.sample)] = 2;
             } else {
                 outs.clear();
                 const uint32_t gw[2] = {wr.g0, wr.g1};
@@ -3058,7 +3128,13 @@ extern "C" uint64_t oracle_render_wfpg(const oracle_scene* s, const oracle_bvh* 
             const F3 pos(chain.pos[3 * at], chain.pos[3 * at + 1], chain.pos[3 * at + 2]);
             const size_t pa = chain.at(d - 1, p);
             const F3 wo = normalize(F3(chain.pos[3 * pa], chain.pos[3 * pa + 1], chain.pos[3 * pa + 2]) - pos);
-            deposit_leaf(svo, tree, pos, wo, lum3(tot));
+            uint32_t hits = 0, misses = 0;
+            if (d + 1 <= lastD) {
+                const size_t q = chain.at(d + 1, p);
+                hits = (chain.eventNee[q] == 1 ? 1u : 0u) + (chain.eventPath[q] == 1 ? 1u : 0u);
+                misses = chain.eventNee[q] == 2 ? 1u : 0u;
+            }
+            deposit_leaf(svo, tree, pos, wo, lum3(tot), hits, misses);
         }
     }
     normalize_filter(svo);

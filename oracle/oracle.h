@@ -163,6 +163,13 @@ void oracle_svo_payload_init(oracle_svo*, const float* light_rad, uint32_t omit)
 void oracle_svo_payload_get(const oracle_svo*, uint32_t* leaf_norm_spec, uint32_t* node_norm_spec,
                             uint64_t* leaf_irr, uint32_t* leaf_cnt, uint32_t* leaf_avg,
                             uint32_t* node_avg);
+/* Shadow-ray counters (hits, misses per leaf: DepositNEEHitMiss) and the
+ * binary16 node guiding factors of the last NormalizeAndFilterRadiance.
+ * Set replaces the counters (the factors follow at the next normalise). */
+void oracle_svo_set_shadow(oracle_svo*, const uint32_t* leaf_shadow);
+/* DepositNEEHitMiss of n vertices over zeroed counters (is_hit: 1 hit, 0 miss). */
+void oracle_svo_deposit_nee(oracle_svo*, const float* pos, const uint8_t* is_hit, uint32_t n);
+void oracle_svo_guiding_get(const oracle_svo*, uint32_t* leaf_shadow, uint16_t* node_factor);
 
 /* TriFunctions::Voxelize over every triangle (counting pass, then codes and
  * packed spherical normals u16 | u16 << 16 in triangle order, at most

@@ -438,6 +438,20 @@ class OracleSvo:
         if normalize:
             lib.oracle_svo_normalize(self.h)
 
+    def set_shadow(self, leaf_shadow: np.ndarray, normalize: bool = True):
+        """Set the per-leaf shadow-ray counters (hits, misses), then
+        NormalizeAndFilterRadiance (which derives the node guiding factors)."""
+        sh = np.ascontiguousarray(leaf_shadow, np.uint32)
+        lib.oracle_svo_set_shadow(self.h, _p(sh))
+        if normalize:
+            lib.oracle_svo_normalize(self.h)
+
+    def deposit_nee(self, pos: np.ndarray, is_hit: np.ndarray):
+        """DepositNEEHitMiss of vertices over zeroed shadow-ray counters."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        hit = np.ascontiguousarray(is_hit, np.uint8)
+        lib.oracle_svo_deposit_nee(self.h, _p(pos), _p(hit), C.c_uint32(hit.shape[0]))
+
     def deposit(self, pos: np.ndarray, wo: np.ndarray, lum: np.ndarray):
         """DepositRadiance of path vertices over zeroed leaf sums."""
         pos = np.ascontiguousarray(pos, np.float32)
@@ -479,6 +493,9 @@ class OracleSvo:
             lib.oracle_svo_payload_get(self.h, _p(out["leaf_normals"]), _p(out["node_normals"]),
                                        _p(out["leaf_irr"]), _p(out["leaf_cnt"]),
                                        _p(out["leaf_avg"]), _p(out["node_avg"]))
+            out["leaf_shadow"] = np.zeros((U, 2), np.uint32)
+            out["node_factor"] = np.zeros(N, np.uint16)
+            lib.oracle_svo_guiding_get(self.h, _p(out["leaf_shadow"]), _p(out["node_factor"]))
         return out
 
 
@@ -640,8 +657,9 @@ def _u64_to_f32_rne(v: int) -> np.float32:
 def svo_dump_bytes(ex: dict, node_bin16=None, leaf_bin16=None) -> bytes:
     """The dump of an exported octree (tracer.export_svo()), restated from
     the reference's layout: 48-byte header, tree arrays, then the payload
-    with FP32 sums (2^-24 fixed point here), FP32 averages (half pairs here)
-    and zero guiding factors."""
+    with FP32 sums (2^-24 fixed point here), FP32 averages (half pairs here),
+    the first N bytes of the binary16 node guiding factors (the reference
+    copies N bytes of its half array) and zero leaf guiding factors."""
     N, U = ex["nodes_count"], ex["leaves"]
     lv = ex["level_offsets"].astype(np.uint32)
     nb = np.zeros(N, np.uint16) if node_bin16 is None else np.asarray(node_bin16, np.uint16)
@@ -652,13 +670,16 @@ def svo_dump_bytes(ex: dict, node_bin16=None, leaf_bin16=None) -> bytes:
         pairs = np.stack([w & 0xFFFF, w >> 16], 1).astype(np.uint16)
         return pairs.view(np.float16).astype(np.float32)
 
+    nf = ex.get("node_factor")
+    factor_bytes = (np.zeros(N, np.uint8) if nf is None else
+                    np.frombuffer(np.ascontiguousarray(nf, np.uint16).tobytes()[:N], np.uint8))
     irr = np.array([_u64_to_f32_rne(int(v)) for v in ex["leaf_irr"].ravel()],
                    np.float32) * np.float32(2.0 ** -24)
     parts = [np.asarray(ex["lo"], np.float32), np.asarray(ex["hi"], np.float32),
              np.array([ex["resolution"], ex["depth"], N, U], np.uint32),
              np.array([ex["leaf_size"]], np.float32), np.array([lv.size], np.uint32),
              ex["nodes"].astype(np.uint64), nb, ex["leaf_parents"].astype(np.uint32), lb, lv,
-             halves(ex["node_avg"]), ex["node_normals"].astype(np.uint32), np.zeros(N, np.uint8),
+             halves(ex["node_avg"]), ex["node_normals"].astype(np.uint32), factor_bytes,
              irr.astype(np.float32), ex["leaf_cnt"].astype(np.uint32), halves(ex["leaf_avg"]),
              ex["leaf_normals"].astype(np.uint32), np.zeros(U, np.uint8)]
     return b"".join(np.ascontiguousarray(p).tobytes() for p in parts)

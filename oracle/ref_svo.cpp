@@ -535,4 +535,46 @@ void ref_svo_deposit(void* p, const float* pos, const float* wo, const float* lu
     }
 }
 
+// AnisoSVOctreeGPU::DepositNEEHitMiss (AnisoSVO.cuh:1101-1115 with
+// VoxelPayload::WriteLeafNEEHitMiss :540-545) for n vertices, in order, over
+// zeroed counters: is_hit[i] picks the hit or the miss counter; per-leaf
+// hits and misses out.
+void ref_svo_deposit_nee(void* p, const float* pos, const uint8_t* is_hit, uint32_t n,
+                         uint32_t* hit_out, uint32_t* miss_out) {
+    RefSvo* h = static_cast<RefSvo*>(p);
+    AnisoSVOctreeGPU& T = h->tree;
+    std::fill(h->shadowHit.begin(), h->shadowHit.end(), 0u);
+    std::fill(h->shadowMiss.begin(), h->shadowMiss.end(), 0u);
+    for (uint32_t i = 0; i < n; i++)
+        T.DepositNEEHitMiss(Vector3f(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), 1.0f,
+                            is_hit[i] != 0);
+    std::copy(h->shadowHit.begin(), h->shadowHit.end(), hit_out);
+    std::copy(h->shadowMiss.begin(), h->shadowMiss.end(), miss_out);
+}
+
+// The guiding factors of KCBottomUpFilterIrradiance (AnisoSVO.cu:520-615)
+// over the given per-leaf shadow-ray counters, level by level from the
+// deepest; binary16 node factors out.  Uses the normal and radiance payload
+// already set (the factors do not depend on it).
+void ref_svo_guiding_factors(void* p, const uint32_t* hit, const uint32_t* miss,
+                             uint16_t* node_factor) {
+    RefSvo* h = static_cast<RefSvo*>(p);
+    AnisoSVOctreeGPU& T = h->tree;
+    std::copy(hit, hit + h->shadowHit.size(), h->shadowHit.begin());
+    std::copy(miss, miss + h->shadowMiss.size(), h->shadowMiss.begin());
+    const uint32_t levelCount = T.leafDepth;
+    const std::vector<uint32_t>& offs = h->levelOffsets;
+    for (uint32_t i = 0; i < levelCount; i++) {
+        const uint32_t levelIndex = levelCount - i - 1;
+        const bool lastNonLeafLevel = (levelIndex == (levelCount - 1));
+        const uint32_t count = offs[levelIndex + 1] - offs[levelIndex];
+        launch(count, [&] {
+            KCBottomUpFilterIrradiance(T.payload, T.dNodes, T.dLevelNodeOffsets, levelIndex,
+                                       count, lastNonLeafLevel);
+        });
+    }
+    static_assert(sizeof(half) == 2, "half");
+    std::memcpy(node_factor, h->nodeFactor.data(), 2 * h->nodeFactor.size());
+}
+
 }  // extern "C"

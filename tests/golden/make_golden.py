@@ -406,6 +406,22 @@ def svo_golden(R) -> None:
             R.ref_svo_deposit(h, _p(pos), _p(wo), _p(lum), C.c_uint32(m), _p(ri), _p(rc))
             g.update({f"{tag}_dep_pos": pos, f"{tag}_dep_wo": wo, f"{tag}_dep_lum": lum,
                       f"{tag}_dep_irr": ri, f"{tag}_dep_cnt": rc})
+            # DepositNEEHitMiss at the same vertices (a stream of its own, so
+            # the arrays above keep their values), then the guiding factors
+            # of KCBottomUpFilterIrradiance over seeded counters, 70 % of
+            # the leaves without a shadow ray
+            rs = np.random.default_rng(20261205)
+            is_hit = (rs.uniform(size=m) < 0.6).astype(np.uint8)
+            nh = np.zeros(U, np.uint32)
+            nm = np.zeros(U, np.uint32)
+            R.ref_svo_deposit_nee(h, _p(pos), _p(is_hit), C.c_uint32(m), _p(nh), _p(nm))
+            sh = (rs.integers(0, 50, (U, 2)) * (rs.uniform(size=(U, 1)) < 0.3)).astype(np.uint32)
+            sh[rs.uniform(size=U) < 0.05, 0] = 0  # some leaves with misses only
+            nf = np.zeros(nodes.shape[0], np.uint16)
+            sh_hit, sh_miss = np.ascontiguousarray(sh[:, 0]), np.ascontiguousarray(sh[:, 1])
+            R.ref_svo_guiding_factors(h, _p(sh_hit), _p(sh_miss), _p(nf))
+            g.update({f"{tag}_nee_hit": is_hit, f"{tag}_nee_hits": nh, f"{tag}_nee_misses": nm,
+                      f"{tag}_shadow": sh, f"{tag}_node_factor": nf})
         R.ref_svo_destroy(h)
     out = HERE / "svo_reference_vectors.npz"
     np.savez_compressed(out, **g)

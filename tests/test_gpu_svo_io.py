@@ -70,6 +70,11 @@ def test_load_round_trip_and_next_frame(system):
               "leaf_cnt", "leaf_avg", "node_avg"):
         assert np.array_equal(ex_a[k], ex_b[k]), k
     assert ex_b["resolution"] == ex_a["resolution"] and not ex_b["leaf_codes"].any()
+    # the dump carries N bytes of the node guiding factors; the shadow-ray
+    # counters start again at zero
+    N = ex_a["nodes_count"]
+    assert ex_b["node_factor"].tobytes()[:N] == ex_a["node_factor"].tobytes()[:N]
+    assert ex_a["leaf_shadow"].any() and not ex_b["leaf_shadow"].any()
     # the next frame reads only the averages, which load back exactly
     a.render_frame()
     b.set_options({"Frame": 3})

@@ -17,6 +17,9 @@ pytestmark = pytest.mark.gpu
 
 REL_MEAN_TOL = 1e-4
 PAYLOAD = ("leaf_normals", "node_normals", "leaf_irr", "leaf_cnt", "leaf_avg", "node_avg")
+# what a frame changes: the radiance state, the shadow-ray counters
+# (DepositNEEHitMiss) and the node guiding factors
+FRAME_STATE = PAYLOAD[2:] + ("leaf_shadow", "node_factor")
 
 
 def _rel_mean_err(a, b):
@@ -114,7 +117,7 @@ def test_guide_words_and_bins_match_oracle(system, oracle, product):
 
 
 @pytest.mark.parametrize("variant", ["mis", "pure", "mis_nee_mis", "nonproduct",
-                                     "nonproduct_pure"])
+                                     "nonproduct_pure", "nee_off"])
 def test_wfpg_frames_match_oracle(system, oracle, variant):
     """Two stepwise frames: per-sample radiance and the octree payload after
     each frame's deposit."""
@@ -125,6 +128,9 @@ def test_wfpg_frames_match_oracle(system, oracle, variant):
         opts["PurePG"] = 1
     if variant.startswith("nonproduct"):
         opts["DoProductPathGuiding"] = 0
+    if variant == "nee_off":
+        # path rays reaching a light or leaving the box count as hits
+        opts["NextEventEstimation"] = 0
     if variant == "mis_nee_mis":
         opts["DirectLightMIS"] = 1
         opts["BXDF-GuideMISRatio"] = 0.7
@@ -144,7 +150,14 @@ def test_wfpg_frames_match_oracle(system, oracle, variant):
         rays, frames = t.stats()
         assert gpu.sum() > 0
         assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
-        _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
+        ex = t.export_svo()
+        _assert_payload(ex, svo.export(), FRAME_STATE)
+        # NEE rays reach their light from some vertices and are stopped
+        # from others; nodes over leaves with shadow rays carry a factor
+        sh = ex["leaf_shadow"]
+        assert sh[:, 0].sum() > 0
+        assert (sh[:, 1].sum() > 0) == (variant != "nee_off")
+        assert np.count_nonzero(ex["node_factor"] != 0x7FFF) > 0
 
 
 def test_wfpg_graph_frames_match_stepwise(system, oracle):
@@ -166,7 +179,7 @@ def test_wfpg_graph_frames_match_stepwise(system, oracle):
     img = t.image()
     assert img[..., 3].min() == 3.0
     assert _rel_mean_err(img[..., :3].astype(np.float64), acc) < REL_MEAN_TOL
-    _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
+    _assert_payload(t.export_svo(), svo.export(), FRAME_STATE)
 
 
 def test_wfpg_skip_pg_is_unguided(system, oracle):
@@ -186,7 +199,7 @@ def test_wfpg_skip_pg_is_unguided(system, oracle):
                                  opts["RussianRouletteStart"], True, opts["Seed"], svo,
                                  **_oracle_kwargs(opts))
     assert _rel_mean_err(t.sample_radiance()[..., :3], ref) < REL_MEAN_TOL
-    _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
+    _assert_payload(t.export_svo(), svo.export(), FRAME_STATE)
 
 
 def test_wfpg_on_a_scene_file(system, oracle):
@@ -210,4 +223,4 @@ def test_wfpg_on_a_scene_file(system, oracle):
         gpu = t.sample_radiance()[..., :3]
         assert gpu.sum() > 0
         assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
-        _assert_payload(t.export_svo(), svo.export(), PAYLOAD[2:])
+        _assert_payload(t.export_svo(), svo.export(), FRAME_STATE)

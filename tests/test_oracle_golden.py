@@ -297,6 +297,37 @@ def test_svo_deposit_matches_reference(oracle):
     assert np.all(np.abs(got - ref) <= 1e-4 * np.maximum(ref, 1e-3))
 
 
+def test_svo_nee_deposit_matches_reference(oracle):
+    """DepositNEEHitMiss: the leaf of each vertex (the same neighbour search
+    as DepositRadiance) takes one hit or one miss; per-leaf counters
+    bit-exact."""
+    tag = "clusters128"
+    svo = _svo(oracle, tag)
+    svo.deposit_nee(S[f"{tag}_dep_pos"], S[f"{tag}_nee_hit"])
+    ex = svo.export()
+    assert np.array_equal(ex["leaf_shadow"][:, 0], S[f"{tag}_nee_hits"])
+    assert np.array_equal(ex["leaf_shadow"][:, 1], S[f"{tag}_nee_misses"])
+    assert S[f"{tag}_nee_hits"].sum() > 4000 and S[f"{tag}_nee_misses"].sum() > 2500
+
+
+def test_svo_guiding_factors_match_reference(oracle):
+    """KCBottomUpFilterIrradiance's guiding factors: a leaf's miss ratio
+    misses / (hits + misses), NaN without shadow rays; a node's the FP32 mean
+    of its children's factors that are not NaN, rounded to binary16, and the
+    NaN 0x7FFF when none has data.  Bit-exact over seeded counters (70 % of
+    the leaves without any, some with misses only)."""
+    tag = "clusters128"
+    svo = _svo(oracle, tag)
+    svo.set_shadow(S[f"{tag}_shadow"])
+    ref = S[f"{tag}_node_factor"]
+    got = svo.export()["node_factor"]
+    assert np.array_equal(got, ref)
+    nan = (ref & 0x7C00) == 0x7C00
+    assert 0 < np.count_nonzero(nan) < ref.shape[0] // 2
+    sh = S[f"{tag}_shadow"]
+    assert np.count_nonzero((sh[:, 0] == 0) & (sh[:, 1] > 0)) > 100  # leaves with misses only
+
+
 def test_product_sampler_matches_reference(oracle):
     """ProductSampler (ProductSampler.cuh:160-660): the reference's own
     sampler, run once on a B200 by the harness of oracle/psamp/ with table
