@@ -182,6 +182,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     system = m.TracerSystem(dev)
     g = m.GPUScene(system, scene)
     g.set_wide_order(args.wide_order)
+    g.set_wide_collapse(args.wide_collapse)
     g.construct_accelerators()
     g.set_traversal(args.traversal)
     if args.only == "guided":
@@ -573,6 +574,7 @@ def run_closed(args, m, system, torch) -> dict:
     carry the frame; reported with its stage split and traversal roofline."""
     scene = m.scenes.cornell(seed=1, width=1920, height=1080)
     g = m.GPUScene(system, scene)
+    g.set_wide_collapse(args.wide_collapse)
     g.construct_accelerators()
     g.set_traversal(args.traversal)
     t = m.PathTracer(system, g)
@@ -1006,6 +1008,8 @@ def main():
     ap.add_argument("--wide-order", default="auto",
                     choices=["auto", "sorted", "octant", "sorted_refill", "octant_refill"],
                     help="8-wide traversal kernel of the headline frame (auto: timed per depth)")
+    ap.add_argument("--wide-collapse", type=int, default=1, choices=[0, 1],
+                    help="8-wide node children: 1 the surface-area plan, 0 largest area first")
     ap.add_argument("--no-closed", dest="closed", action="store_false",
                     help="skip the bounce-heavy Cornell 1080p 4 spp entry")
     ap.add_argument("--no-learned", dest="learned", action="store_false",

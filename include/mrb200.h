@@ -174,6 +174,13 @@ int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms4);
  * (default) whichever of the two has the smaller sum of inner-box surface
  * areas.  The LBVH arrays and the binary traversal are the same either way. */
 int mrb_accel_set_wide_tree(mrb_scene* s, int tree);
+/* How each 8-wide node picks its children among the binary tree's
+ * descendants (before mrb_accel_construct): 0 opens the internal child with
+ * the largest surface area until eight children; 1 (default) follows a
+ * bottom-up dynamic program that minimises the sum of the wide nodes'
+ * surface areas (Ylitie, Karras and Laine, HPG 2017, one triangle per
+ * leaf).  The traversal layout only; the LBVH arrays do not change. */
+int mrb_accel_set_wide_collapse(mrb_scene* s, int collapse);
 /* info[2]: the source used (0 LBVH, 1 PLOC), PLOC clustering steps;
  * areas[2] (may be NULL): inner half-area sums of the LBVH and PLOC trees. */
 int mrb_accel_info_ext(const mrb_scene* s, uint32_t* info, double* areas);

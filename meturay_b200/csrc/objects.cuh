@@ -103,6 +103,7 @@ struct mrb_scene {
     uint32_t wNodeCount = 0;
     int traversal = 1;  // 0: binary LBVH nodes, 1: 8-wide nodes
     int wideTree = 2;        // 0 LBVH, 1 PLOC, 2 the one with less inner-box area
+    int wideCollapse = 1;    // kWideCollapseGreedy / kWideCollapseSah
     // traversal kernel (WideOrder), or MRB_WIDE_AUTO: the fastest as timed
     int wideOrderMode = MRB_WIDE_AUTO;
     int wideOrder = 0;  // in use where no tracer has tuned its own

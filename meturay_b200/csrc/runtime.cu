@@ -1190,7 +1190,7 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
         WideBuildIn wi{n, s->aRoot.as<uint32_t>(), s->aLeft.as<uint32_t>(), s->aRight.as<uint32_t>(),
                        s->aInner.as<float>(), s->aTriAabb.as<float>(), s->aSorted.as<uint32_t>(),
                        s->dPos.as<float>(), s->dIdx.as<uint32_t>(), s->dKey.as<uint32_t>(),
-                       s->dCull.as<uint8_t>()};
+                       s->dCull.as<uint8_t>(), s->wideCollapse};
         // the PLOC tree over the same sorted leaves: tighter upper boxes than
         // the Morton splits give the collapse better nodes to start from
         DBuf pLeft, pRight, pInner, pRoot, pScratch;
@@ -1401,6 +1401,19 @@ int mrb_accel_set_wide_tree(mrb_scene* s, int tree) {
         return MRB_E_STATE;
     }
     s->wideTree = tree;
+    return 0;
+}
+
+int mrb_accel_set_wide_collapse(mrb_scene* s, int collapse) {
+    if (!s || (collapse != kWideCollapseGreedy && collapse != kWideCollapseSah)) {
+        set_error("wide collapse must be 0 (largest area first) or 1 (surface-area plan)");
+        return MRB_E_ARG;
+    }
+    if (s->built) {
+        set_error("wide collapse: set it before mrb_accel_construct");
+        return MRB_E_STATE;
+    }
+    s->wideCollapse = collapse;
     return 0;
 }
 

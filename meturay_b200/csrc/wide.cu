@@ -8,8 +8,15 @@
 // replaces about three binary levels.
 //
 // Collapse (top-down, one launch per level of the wide tree): a wide node is
-// formed from a binary node by repeatedly opening the internal child with
-// the largest surface area until it has eight children or only leaves.
+// formed from a binary node by choosing which binary descendants become its
+// (at most eight) children.  Default: the surface-area dynamic program of
+// Ylitie, Karras and Laine ("Efficient Incoherent Ray Traversal on GPUs
+// Through Compressed Wide BVHs", HPG 2017), with one-triangle leaves: a
+// bottom-up pass gives every binary node g the least sum of wide-node
+// surface areas that represents its subtree as at most i children,
+// cost(g, i) for i = 1..8, and the collapse follows its choices.  Without
+// it, the internal child with the largest surface area is opened until the
+// node has eight children or only leaves.
 // Internal children get consecutive wide-node slots and leaf children
 // consecutive triangle slots; slots are handed out by atomic counters per
 // level, so the first 1 + 8 + 64 slots are the top three levels.  The
@@ -70,6 +77,128 @@ __device__ __forceinline__ uint32_t quant_exponent(float extent) {
     return e < 1u ? 1u : e;
 }
 
+// ---------------------------------------------------------------------------
+// Surface-area collapse plan
+//   cost(leaf, i) = 0 (every triangle is a leaf child exactly once)
+//   D(g, i)       = min over k in 1..i-1 of cost(left, k) + cost(right, i - k)
+//   E(g, 2) = D(g, 2), E(g, i) = min(E(g, i - 1), D(g, i))
+//   cost(g, 1)    = area(g) + E(g, 8)          (g becomes a wide node)
+//   cost(g, i)    = min(cost(g, 1), E(g, i))   (i >= 2)
+// Plan per inner node (8 bytes): byte 0 bit i - 1 set where cost(g, i) takes
+// cost(g, 1) (g stays one child), byte i - 1 (i = 2..8) the k of D(g, i), 0
+// where E(g, i) = E(g, i - 1).  D(g, 2) always has k = 1.
+// ---------------------------------------------------------------------------
+__global__ void k_plan_parents(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                               uint32_t n, uint32_t* parent, uint32_t* flags) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j + 1 < n;
+         j += gridDim.x * blockDim.x) {
+        parent[left[j]] = n + j;
+        parent[right[j]] = n + j;
+        flags[j] = 0u;
+    }
+}
+
+// One thread per leaf walks up; the second arrival at a node evaluates it
+// (the pattern of the LBVH's bottom-up box pass).  The walk ends at the root.
+__global__ void k_plan_up(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                          const float* __restrict__ inner, const uint32_t* __restrict__ parent,
+                          const uint32_t* __restrict__ root, uint32_t n, uint32_t* flags,
+                          float* cost, uint2* plan) {
+    const uint32_t top = *root;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t g = parent[i];
+        while (true) {
+            __threadfence();
+            if (atomicAdd(flags + (g - n), 1u) == 0u) break;  // the sibling is not done yet
+            __threadfence();
+            const uint32_t j = g - n;
+            const uint32_t l = left[j], r = right[j];
+            float cl[9], cr[9];
+            for (int k = 1; k <= 8; k++) {
+                cl[k] = (l >= n) ? __ldcg(cost + 8 * size_t(l - n) + (k - 1)) : 0.0f;
+                cr[k] = (r >= n) ? __ldcg(cost + 8 * size_t(r - n) + (k - 1)) : 0.0f;
+            }
+            float E[9];
+            uint32_t ks[9];
+            for (int c = 2; c <= 8; c++) {
+                float best = 0.0f;
+                uint32_t bk = 0;
+                for (int k = 1; k < c; k++) {
+                    const float v = cl[k] + cr[c - k];
+                    if (bk == 0 || v < best) {
+                        best = v;
+                        bk = uint32_t(k);
+                    }
+                }
+                if (c > 2 && E[c - 1] <= best) {
+                    best = E[c - 1];
+                    bk = 0;
+                }
+                E[c] = best;
+                ks[c] = bk;
+            }
+            const float* b = inner + 6 * size_t(j);
+            const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+            const float c1 = (dx * dy + dy * dz + dz * dx) + E[8];
+            float* cj = cost + 8 * size_t(j);
+            uint32_t single = 0;
+            cj[0] = c1;
+            for (int c = 2; c <= 8; c++) {
+                if (c1 <= E[c]) single |= 1u << (c - 1);
+                cj[c - 1] = fminf(c1, E[c]);
+            }
+            plan[j] = make_uint2(single | (ks[2] << 8) | (ks[3] << 16) | (ks[4] << 24),
+                                 ks[5] | (ks[6] << 8) | (ks[7] << 16) | (ks[8] << 24));
+            if (g == top) break;
+            g = parent[g];
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t plan_byte(uint2 p, int b) {
+    return ((b < 4 ? p.x : p.y) >> (8 * (b & 3))) & 0xFFu;
+}
+
+// The children of the wide node made from binary node g under the plan: at
+// most eight, at least two.  Each pending entry holds at least one slot, so
+// at most eight entries are ever pending.
+__device__ __forceinline__ int plan_children(uint32_t g, uint32_t n, const uint32_t* __restrict__ left,
+                                             const uint32_t* __restrict__ right,
+                                             const uint2* __restrict__ plan, uint32_t ch[8]) {
+    uint32_t sg[16];
+    uint8_t si[16], sown[16];
+    int sp = 1, nc = 0;
+    sg[0] = g;
+    si[0] = 8;
+    sown[0] = 1;
+    while (sp > 0) {
+        sp--;
+        const uint32_t x = sg[sp];
+        int i = si[sp];
+        const bool own = sown[sp] != 0;
+        if (!own && (x < n || i == 1)) {
+            ch[nc++] = x;
+            continue;
+        }
+        const uint2 pl = plan[x - n];
+        if (!own && ((pl.x >> (i - 1)) & 1u)) {
+            ch[nc++] = x;
+            continue;
+        }
+        uint32_t k;
+        while ((k = plan_byte(pl, i - 1)) == 0u) i--;
+        // left takes k slots, right i - k (each >= 1)
+        sg[sp] = right[x - n];
+        si[sp] = uint8_t(i - int(k));
+        sown[sp] = 0;
+        sg[sp + 1] = left[x - n];
+        si[sp + 1] = uint8_t(k);
+        sown[sp + 1] = 0;
+        sp += 2;
+    }
+    return nc;
+}
+
 __global__ void __launch_bounds__(128) k_collapse(
     const WorkItem* __restrict__ qin, const uint32_t* __restrict__ qinCount, WorkItem* qout,
     uint32_t* qoutCount, uint32_t* nodeCounter, uint32_t* triCounter, uint32_t n,
@@ -77,7 +206,8 @@ __global__ void __launch_bounds__(128) k_collapse(
     const float* __restrict__ inner, const float* __restrict__ triAabb,
     const uint32_t* __restrict__ sortedIdx, const float* __restrict__ pos,
     const uint32_t* __restrict__ idx, const uint32_t* __restrict__ key,
-    const uint8_t* __restrict__ cull, WideNode* nodes, float4* tv0, float4* te0, float4* te1) {
+    const uint8_t* __restrict__ cull, const uint2* __restrict__ plan, WideNode* nodes, float4* tv0,
+    float4* te0, float4* te1) {
     const uint32_t count = *qinCount;
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
          w += gridDim.x * blockDim.x) {
@@ -87,27 +217,31 @@ __global__ void __launch_bounds__(128) k_collapse(
         int nc = 2;
         ch[0] = left[it.bnode - n];
         ch[1] = right[it.bnode - n];
-        for (int k = 0; k < 2; k++) {
-            float lo[3], hi[3];
-            child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
-            area[k] = (ch[k] >= n) ? half_area(lo, hi) : -1.0f;
-        }
-        // open the largest internal child until eight children
-        while (nc < 8) {
-            int best = -1;
-            for (int k = 0; k < nc; k++)
-                if (ch[k] >= n && (best < 0 || area[k] > area[best])) best = k;
-            if (best < 0) break;
-            const uint32_t b = ch[best];
-            const uint32_t c0 = left[b - n], c1 = right[b - n];
-            ch[best] = c0;
-            ch[nc] = c1;
-            float lo[3], hi[3];
-            child_box(c0, n, inner, triAabb, sortedIdx, lo, hi);
-            area[best] = (c0 >= n) ? half_area(lo, hi) : -1.0f;
-            child_box(c1, n, inner, triAabb, sortedIdx, lo, hi);
-            area[nc] = (c1 >= n) ? half_area(lo, hi) : -1.0f;
-            nc++;
+        if (plan) {
+            nc = plan_children(it.bnode, n, left, right, plan, ch);
+        } else {
+            for (int k = 0; k < 2; k++) {
+                float lo[3], hi[3];
+                child_box(ch[k], n, inner, triAabb, sortedIdx, lo, hi);
+                area[k] = (ch[k] >= n) ? half_area(lo, hi) : -1.0f;
+            }
+            // open the largest internal child until eight children
+            while (nc < 8) {
+                int best = -1;
+                for (int k = 0; k < nc; k++)
+                    if (ch[k] >= n && (best < 0 || area[k] > area[best])) best = k;
+                if (best < 0) break;
+                const uint32_t b = ch[best];
+                const uint32_t c0 = left[b - n], c1 = right[b - n];
+                ch[best] = c0;
+                ch[nc] = c1;
+                float lo[3], hi[3];
+                child_box(c0, n, inner, triAabb, sortedIdx, lo, hi);
+                area[best] = (c0 >= n) ? half_area(lo, hi) : -1.0f;
+                child_box(c1, n, inner, triAabb, sortedIdx, lo, hi);
+                area[nc] = (c1 >= n) ? half_area(lo, hi) : -1.0f;
+                nc++;
+            }
         }
         // slot of each child: the octant of its centroid around the node's
         // centre, matched greedily by the largest projection on the
@@ -724,9 +858,16 @@ __global__ void __launch_bounds__(kBlock) k_trace_wide_jobs(const JobDev* __rest
 
 }  // namespace
 
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+size_t queue_bytes(uint32_t n) { return align256(size_t(n + 1) * sizeof(WorkItem) * 2 + 64); }
+}  // namespace
+
 size_t wide_scratch_bytes(uint32_t n) {
-    // two work queues of n items + 4 counters
-    return size_t(n + 1) * sizeof(WorkItem) * 2 + 64;
+    // two work queues of n items + 4 counters; the collapse plan: parents
+    // (2n), arrival flags (n), costs (8n) and plans (n)
+    return queue_bytes(n) + align256(size_t(2) * n * 4) + align256(size_t(n) * 4) +
+           align256(size_t(8) * n * 4) + align256(size_t(n) * 8);
 }
 
 int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0, float4* te1,
@@ -740,6 +881,23 @@ int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0,
     q[0] = static_cast<WorkItem*>(scratch);
     q[1] = q[0] + (n + 1);
     uint32_t* counters = reinterpret_cast<uint32_t*>(q[1] + (n + 1));
+    const uint2* plan = nullptr;
+    if (in.collapse == kWideCollapseSah) {
+        char* b = static_cast<char*>(scratch) + queue_bytes(n);
+        uint32_t* parent = reinterpret_cast<uint32_t*>(b);
+        b += align256(size_t(2) * n * 4);
+        uint32_t* flags = reinterpret_cast<uint32_t*>(b);
+        b += align256(size_t(n) * 4);
+        float* cost = reinterpret_cast<float*>(b);
+        b += align256(size_t(8) * n * 4);
+        uint2* pl = reinterpret_cast<uint2*>(b);
+        const uint32_t g = std::min<uint32_t>((n + 255) / 256, 148u * 8u);
+        k_plan_parents<<<g, 256, 0, stream>>>(in.left, in.right, n, parent, flags);
+        k_plan_up<<<g, 256, 0, stream>>>(in.left, in.right, in.inner, parent, in.root, n, flags,
+                                         cost, pl);
+        MRB_CUDA(cudaGetLastError());
+        plan = pl;
+    }
     k_collapse_init<<<1, 32, 0, stream>>>(q[0], counters, in.root);
     MRB_CUDA(cudaGetLastError());
     // one launch per level; the host checks for an empty queue every 8 levels
@@ -750,7 +908,7 @@ int wide_build(const WideBuildIn& in, WideNode* nodes, float4* tv0, float4* te0,
         k_collapse<<<grid, 128, 0, stream>>>(q[cur], counters + cur, q[cur ^ 1], counters + (cur ^ 1),
                                              counters + 2, counters + 3, n, in.left, in.right,
                                              in.inner, in.triAabb, in.sortedIdx, in.pos, in.idx,
-                                             in.key, in.cull, nodes, tv0, te0, te1);
+                                             in.key, in.cull, plan, nodes, tv0, te0, te1);
         MRB_CUDA(cudaGetLastError());
         if ((level & 7) == 7) {
             uint32_t h[4];

@@ -34,7 +34,14 @@ struct WideBuildIn {
     const uint32_t* idx;
     const uint32_t* key;
     const uint8_t* cull;
+    int collapse;                // kWideCollapseGreedy or kWideCollapseSah
 };
+
+// How a wide node chooses its children among the binary node's descendants:
+// opening the largest-area internal child first, or the surface-area
+// dynamic program (least sum of wide-node areas).
+constexpr int kWideCollapseGreedy = 0;
+constexpr int kWideCollapseSah = 1;
 
 size_t wide_scratch_bytes(uint32_t n);
 // Collapses the LBVH into wide nodes (at most n-1) and reorders triangles

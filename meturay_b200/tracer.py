@@ -195,6 +195,12 @@ class GPUScene:
         layout: 0 the LBVH, 1 PLOC, 2 (default) the one with less box area."""
         check(lib.mrb_accel_set_wide_tree(self._h, int(tree)))
 
+    def set_wide_collapse(self, collapse: int):
+        """Before construct_accelerators: how each 8-wide node picks its
+        children: 0 the largest-area internal child first, 1 (default) the
+        surface-area dynamic program."""
+        check(lib.mrb_accel_set_wide_collapse(self._h, int(collapse)))
+
     def build_svo(self, resolution: int):
         """Sparse voxel octree of the scene at `resolution` leaf voxels per axis."""
         check(lib.mrb_svo_build(self._h, int(resolution), None))

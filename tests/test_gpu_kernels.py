@@ -110,11 +110,13 @@ def test_radix_sort_u32(cuda, oracle, n, bits, desc):
     assert np.array_equal(dv.cpu().numpy().view(np.uint32), ev)
 
 
-def _build(system, scene, tree=None):
+def _build(system, scene, tree=None, collapse=None):
     from meturay_b200 import GPUScene
     g = GPUScene(system, scene)
     if tree is not None:
         g.set_wide_tree(tree)
+    if collapse is not None:
+        g.set_wide_collapse(collapse)
     g.construct_accelerators()
     return g
 
@@ -167,7 +169,11 @@ def _rays_for(scene, n, seed):
 
 
 KERNELS = ("sorted", "octant", "sorted_refill", "octant_refill")
-WIDE = {f"{tree}-{k}": (t, k) for t, tree in enumerate(("lbvh", "ploc")) for k in KERNELS}
+# the surface-area collapse (default) with every kernel; the largest-area
+# collapse with two
+WIDE = {f"{tree}-{k}": (t, k, None) for t, tree in enumerate(("lbvh", "ploc")) for k in KERNELS}
+WIDE.update({f"{tree}-greedy-{k}": (t, k, 0) for t, tree in enumerate(("lbvh", "ploc"))
+             for k in ("sorted", "octant")})
 
 
 @pytest.mark.parametrize("mode", ["binary"] + list(WIDE))
@@ -175,13 +181,14 @@ WIDE = {f"{tree}-{k}": (t, k) for t, tree in enumerate(("lbvh", "ploc")) for k i
 def test_trace_closest_hit(system, cuda, oracle, name, make, mode):
     """binary: the LBVH nodes, bit-exact against the oracle's traversal of
     the same tree.  The 8-wide quantised nodes, collapsed from the LBVH or
-    from the PLOC tree, with every traversal kernel (sorted and octant
-    child order, with and without refilled lanes): same hit/miss and the
-    same closest distance bit for bit, same primitive except at ties."""
+    from the PLOC tree by either collapse, with every traversal kernel
+    (sorted and octant child order, with and without refilled lanes): same
+    hit/miss and the same closest distance bit for bit, same primitive except
+    at ties."""
     torch = cuda
     scene = make()
-    tree, order = WIDE.get(mode, (None, None))
-    g = _build(system, scene, tree)
+    tree, order, collapse = WIDE.get(mode, (None, None, None))
+    g = _build(system, scene, tree, collapse)
     g.set_traversal(0 if tree is None else 1)
     if order is not None:
         g.set_wide_order(order)

@@ -145,8 +145,9 @@ def test_wfpg_frames_match_oracle(system, oracle, variant):
         t.finalize()
         gpu = t.sample_radiance()[..., :3]
         ref, ref_rays, _, _ = o.render_wfpg(_cam(scene), scene.width, scene.height, 1,
-                                            opts["MaxDepth"], opts["RussianRouletteStart"], True,
-                                            opts["Seed"], svo, frame=frame, **_oracle_kwargs(opts))
+                                            opts["MaxDepth"], opts["RussianRouletteStart"],
+                                            bool(opts["NextEventEstimation"]), opts["Seed"], svo,
+                                            frame=frame, **_oracle_kwargs(opts))
         rays, frames = t.stats()
         assert gpu.sum() > 0
         assert _rel_mean_err(gpu, ref) < REL_MEAN_TOL
