@@ -271,6 +271,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     peak, peak_kind = _peaks()
     roof = _trace_roofline(t, prof, args.traversal, _traffic_per_launch(args.traversal), peak,
                            peak_kind)
+    roof["wide_collapse"] = g.wide_collapse()
     roof["stage_ms"] = {k: prof[k] for k in ("camera_ms", "trace_ms", "partition_ms", "shade_ms",
                                              "resolve_ms")}
     return {
@@ -598,6 +599,7 @@ def run_closed(args, m, system, torch) -> dict:
     prof = {k: float(np.mean([x[k] for x in profs])) for k in profs[0]}
     peak, peak_kind = _peaks()
     roof = _trace_roofline(t, prof, args.traversal, None, peak, peak_kind)
+    roof["wide_collapse"] = g.wide_collapse()
     total = sum(prof[k] for k in STAGES5)
     out = {"metric": METRIC, "value": (r1 - r0) / (ms / 1e3) / 1e6, "unit": "Mrays/s",
            "steps": steps, "ms_per_step": ms / steps, "rays_per_step": (r1 - r0) / steps,
@@ -1008,8 +1010,9 @@ def main():
     ap.add_argument("--wide-order", default="auto",
                     choices=["auto", "sorted", "octant", "sorted_refill", "octant_refill"],
                     help="8-wide traversal kernel of the headline frame (auto: timed per depth)")
-    ap.add_argument("--wide-collapse", type=int, default=1, choices=[0, 1],
-                    help="8-wide node children: 1 the surface-area plan, 0 largest area first")
+    ap.add_argument("--wide-collapse", type=int, default=2, choices=[0, 1, 2],
+                    help="8-wide node children: 0 largest area first, 1 the surface-area plan, "
+                         "2 the one the probe rays read less of")
     ap.add_argument("--no-closed", dest="closed", action="store_false",
                     help="skip the bounce-heavy Cornell 1080p 4 spp entry")
     ap.add_argument("--no-learned", dest="learned", action="store_false",

@@ -176,11 +176,25 @@ int mrb_accel_wide_order(const mrb_scene* s, int* order, float* ms4);
 int mrb_accel_set_wide_tree(mrb_scene* s, int tree);
 /* How each 8-wide node picks its children among the binary tree's
  * descendants (before mrb_accel_construct): 0 opens the internal child with
- * the largest surface area until eight children; 1 (default) follows a
- * bottom-up dynamic program that minimises the sum of the wide nodes'
- * surface areas (Ylitie, Karras and Laine, HPG 2017, one triangle per
- * leaf).  The traversal layout only; the LBVH arrays do not change. */
+ * the largest surface area until eight children; 1 follows a bottom-up
+ * dynamic program that minimises the sum of the wide nodes' surface areas
+ * (Ylitie, Karras and Laine, HPG 2017, one triangle per leaf); 2 (default)
+ * builds both and keeps the layout of which 65,536 seeded probe rays (origins
+ * uniform in the scene box, directions uniform) read fewer bytes (node
+ * visits x 80 B + triangle tests x 48 B, counted on the device, so the
+ * choice is deterministic).  The traversal layout only; the LBVH arrays do
+ * not change. */
 int mrb_accel_set_wide_collapse(mrb_scene* s, int collapse);
+/* The collapse of the scene's layout (0 or 1) and, after an automatic
+ * choice, the probe bytes of each (probe_bytes2[0] largest-area-first, [1]
+ * surface-area plan; zeros otherwise; may be NULL).  The automatic choice
+ * keeps the other layout as the scene's alternate: a tracer whose traversal
+ * kernel is automatic times every kernel over both layouts on the rays of
+ * each depth of its first frame, keeps for the whole frame the layout whose
+ * fastest kernels sum to less (one tree in L2 at a time) and per depth the
+ * fastest kernel on it (the probe rays, spread through the scene box, need
+ * not look like a camera's); every other caller traces the scene's layout. */
+int mrb_accel_wide_collapse(const mrb_scene* s, int* used, double* probe_bytes2);
 /* info[2]: the source used (0 LBVH, 1 PLOC), PLOC clustering steps;
  * areas[2] (may be NULL): inner half-area sums of the LBVH and PLOC trees. */
 int mrb_accel_info_ext(const mrb_scene* s, uint32_t* info, double* areas);
@@ -417,8 +431,10 @@ void* mrb_tracer_stream(mrb_tracer* t);
 /* Number of kernels one frame launches (>= 0), or a negative status. */
 int mrb_tracer_launches_per_frame(mrb_tracer* t);
 /* The 8-wide traversal kernel of each depth (MRB_WIDE_SORTED ..
- * MRB_WIDE_OCTANT_REFILL; -1 with the binary traversal) for the first n
- * depths; returns how many were written. */
+ * MRB_WIDE_OCTANT_REFILL over the scene's layout; 4 + the kernel over the
+ * scene's alternate layout, the other collapse, which the automatic
+ * collapse keeps for tracers to time; -1 with the binary traversal) for the
+ * first n depths; returns how many were written. */
 int mrb_tracer_wide_orders(const mrb_tracer* t, int* orders, uint32_t n);
 /* Render one frame stage by stage with CUDA events around each stage.
  * stage_ms[5]: camera, traversal, partition, shading, resolve (summed over

@@ -69,6 +69,7 @@ def _load() -> C.CDLL:
         "mrb_accel_info": (i32, [vp, vp]),
         "mrb_accel_set_wide_tree": (i32, [vp, i32]),
         "mrb_accel_set_wide_collapse": (i32, [vp, i32]),
+        "mrb_accel_wide_collapse": (i32, [vp, C.POINTER(i32), vp]),
         "mrb_accel_set_wide_order": (i32, [vp, i32]),
         "mrb_accel_wide_order": (i32, [vp, C.POINTER(C.c_int), vp]),
         "mrb_accel_info_ext": (i32, [vp, vp, vp]),

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
 #include <vector>
 
 #include "../../include/mrb200.h"
@@ -45,6 +46,10 @@ struct DBuf {
         return 0;
     }
     template <class T> T* as() const { return static_cast<T*>(p); }
+    void swap(DBuf& o) {
+        std::swap(p, o.p);
+        std::swap(bytes, o.bytes);
+    }
 };
 
 template <class T>
@@ -103,7 +108,9 @@ struct mrb_scene {
     uint32_t wNodeCount = 0;
     int traversal = 1;  // 0: binary LBVH nodes, 1: 8-wide nodes
     int wideTree = 2;        // 0 LBVH, 1 PLOC, 2 the one with less inner-box area
-    int wideCollapse = 1;    // kWideCollapseGreedy / kWideCollapseSah
+    int wideCollapse = 2;    // kWideCollapseGreedy / kWideCollapseSah / 2: the one the probe reads less of
+    int wideCollapseUsed = 1;
+    double collapseProbeBytes[2] = {0.0, 0.0};  // per collapse (automatic choice only)
     // traversal kernel (WideOrder), or MRB_WIDE_AUTO: the fastest as timed
     int wideOrderMode = MRB_WIDE_AUTO;
     int wideOrder = 0;  // in use where no tracer has tuned its own
@@ -114,6 +121,19 @@ struct mrb_scene {
     int wideTreeUsed = 0;
     uint32_t plocSteps = 0;
     double areaLbvh = 0.0, areaPloc = 0.0;  // sums of inner half areas
+    // the alternate 8-wide layout (the other collapse; automatic choice only)
+    DBuf aNodes2, aTv02, aTe02, aTe12;
+    uint32_t wAltNodeCount = 0;
+    WideAccelDev wideAlt() const {
+        WideAccelDev a{};
+        a.nodes = aNodes2.as<WideNode>();
+        a.tv0 = aTv02.as<float4>();
+        a.te0 = aTe02.as<float4>();
+        a.te1 = aTe12.as<float4>();
+        a.nodeCount = wAltNodeCount;
+        a.triCount = T;
+        return a;
+    }
     WideAccelDev wide() const {
         WideAccelDev a{};
         a.nodes = wNodes.as<WideNode>();

@@ -247,7 +247,7 @@ struct mrb_tracer {
     bool orderTune = false;
     uint32_t orderEpoch = ~0u;  // scene traceEpoch depthOrder was tuned for
     std::vector<int> depthOrder;
-    std::vector<std::array<float, kWideOrders>> depthMs;
+    std::vector<std::array<float, kTunedOrders>> depthMs;
     ~mrb_tracer() {
         if (trainStream) cudaStreamSynchronize(trainStream);
         if (copyStream) cudaStreamSynchronize(copyStream);
@@ -326,6 +326,12 @@ int ensure_buffers(mrb_tracer* t) {
     MRB_CUDA(cudaMemsetAsync(t->image.p, 0, t->image.bytes, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->counters.p, 0, 16, t->stream));
     MRB_CUDA(cudaMemsetAsync(t->errorFlags.p, 0, 16, t->stream));
+    // the sorts' give-up flags are read after every frame, also where a sort
+    // has not run yet (the guide sort under SkipPG)
+    MRB_CUDA(cudaMemsetAsync(radix_sort_error_flag(t->sortTemp.p, t->maxRays), 0, 4, t->stream));
+    if (t->wfpg)
+        MRB_CUDA(cudaMemsetAsync(radix_sort_error_flag(t->guideSort.p, t->maxRays), 0, 4,
+                                 t->stream));
     MRB_CUDA(cudaMemcpyAsync(t->frameWord.p, &t->frameStart, 4, cudaMemcpyHostToDevice,
                              t->stream));
     MRB_CUDA(cudaStreamSynchronize(t->stream));
@@ -584,9 +590,14 @@ PortionTable portion_table(const mrb_tracer* t) {
 int trace_dispatch(const mrb_scene* sc, const float4* rayO, const float4* rayD,
                    const uint32_t* dCount, uint32_t maxCount, const HitOut& ho, uint32_t* err,
                    cudaStream_t st, unsigned long long* counters = nullptr, int order = -1) {
-    if (sc->traversal == 1 && sc->T > 1)
+    if (sc->traversal == 1 && sc->T > 1) {
+        // orders kWideOrders.. run the same kernels over the alternate layout
+        if (order >= kWideOrders && sc->wAltNodeCount)
+            return trace_closest_wide(sc->wideAlt(), rayO, rayD, dCount, maxCount, ho, err, st,
+                                      counters, order - kWideOrders);
         return trace_closest_wide(sc->wide(), rayO, rayD, dCount, maxCount, ho, err, st, counters,
-                                  order >= 0 ? order : sc->wideOrder);
+                                  order >= 0 ? order % kWideOrders : sc->wideOrder);
+    }
     return trace_closest(sc->accel(), rayO, rayD, dCount, maxCount, ho, err, st, counters);
 }
 
@@ -614,8 +625,10 @@ struct StageTimer {
 };
 
 // Every 8-wide traversal kernel run over the rays of buffer `cur` of depth
-// d (twice each, the faster pass kept: the first launch of a kernel may load
-// its module), into t->depthMs[d].  Every pass writes the same closest hits
+// d, over the scene's layout and, where the scene keeps one, its alternate
+// layout (twice each, the faster pass kept: the first launch of a kernel may
+// load its module), into t->depthMs[d] (entries kWideOrders.. for the
+// alternate; 1e30 where there is none).  Every pass writes the same closest hits
 // but for ties; the frame's own trace follows and overwrites them.
 int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho, uint32_t d) {
     const mrb_scene* sc = t->scene;
@@ -623,15 +636,18 @@ int time_wide_orders(mrb_tracer* t, int cur, const HitOut& ho, uint32_t d) {
     cudaEvent_t e[2];
     MRB_CUDA(cudaEventCreate(&e[0]));
     MRB_CUDA(cudaEventCreate(&e[1]));
-    std::array<float, kWideOrders> best;
+    std::array<float, kTunedOrders> best;
     best.fill(1e30f);
+    const int orders = sc->wAltNodeCount ? kTunedOrders : kWideOrders;
     int r = 0;
     for (int rep = 0; rep < 2 && !r; rep++)
-        for (int o = 0; o < kWideOrders && !r; o++) {
+        for (int o = 0; o < orders && !r; o++) {
             cudaEventRecord(e[0], t->stream);
-            r = trace_closest_wide(sc->wide(), t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
+            r = trace_closest_wide(o < kWideOrders ? sc->wide() : sc->wideAlt(),
+                                   t->rayO[cur].as<float4>(), t->rayD[cur].as<float4>(),
                                    t->count.as<uint32_t>() + cur, t->maxRays, ho,
-                                   t->errorFlags.as<uint32_t>(), t->stream, nullptr, o);
+                                   t->errorFlags.as<uint32_t>(), t->stream, nullptr,
+                                   o % kWideOrders);
             cudaEventRecord(e[1], t->stream);
             if (!r && cudaEventSynchronize(e[1]) == cudaSuccess) {
                 float ms = 0.0f;
@@ -1217,9 +1233,44 @@ int mrb_accel_construct(mrb_scene* s, void* stream) {
                 wi.inner = pInner.as<float>();
             }
         }
+        wi.collapse = (s->wideCollapse == kWideCollapseGreedy) ? kWideCollapseGreedy : kWideCollapseSah;
         if ((r = wide_build(wi, s->wNodes.as<WideNode>(), s->wTv0.as<float4>(), s->wTe0.as<float4>(),
                             s->wTe1.as<float4>(), s->wScratch.p, &s->wNodeCount, st)))
             return r;
+        s->wideCollapseUsed = wi.collapse;
+        s->collapseProbeBytes[0] = s->collapseProbeBytes[1] = 0.0;
+        s->aNodes2.release();
+        s->aTv02.release();
+        s->aTe02.release();
+        s->aTe12.release();
+        s->wAltNodeCount = 0;
+        if (s->wideCollapse == 2) {
+            // both collapses: the layout the probe rays read fewer bytes of is
+            // the scene's; the other stays as the alternate that tracers time
+            // per depth on their own rays
+            if ((r = s->aNodes2.alloc((n - 1) * sizeof(WideNode))) ||
+                (r = s->aTv02.alloc(size_t(n) * 16)) || (r = s->aTe02.alloc(size_t(n) * 16)) ||
+                (r = s->aTe12.alloc(size_t(n) * 16)))
+                return r;
+            wi.collapse = kWideCollapseGreedy;
+            if ((r = wide_build(wi, s->aNodes2.as<WideNode>(), s->aTv02.as<float4>(),
+                                s->aTe02.as<float4>(), s->aTe12.as<float4>(), s->wScratch.p,
+                                &s->wAltNodeCount, st)))
+                return r;
+            double pb[2];
+            if ((r = wide_probe_compare(s->wide(), s->wideAlt(), s->aExtent.as<float>(), st, pb)))
+                return r;
+            s->collapseProbeBytes[kWideCollapseSah] = pb[0];
+            s->collapseProbeBytes[kWideCollapseGreedy] = pb[1];
+            if (pb[1] < pb[0]) {
+                s->wNodes.swap(s->aNodes2);
+                s->wTv0.swap(s->aTv02);
+                s->wTe0.swap(s->aTe02);
+                s->wTe1.swap(s->aTe12);
+                std::swap(s->wNodeCount, s->wAltNodeCount);
+                s->wideCollapseUsed = kWideCollapseGreedy;
+            }
+        }
         s->wScratch.release();
         for (float& m : s->wideOrderMs) m = 0.0f;
         if (s->wideOrderMode == MRB_WIDE_AUTO) {
@@ -1405,8 +1456,9 @@ int mrb_accel_set_wide_tree(mrb_scene* s, int tree) {
 }
 
 int mrb_accel_set_wide_collapse(mrb_scene* s, int collapse) {
-    if (!s || (collapse != kWideCollapseGreedy && collapse != kWideCollapseSah)) {
-        set_error("wide collapse must be 0 (largest area first) or 1 (surface-area plan)");
+    if (!s || collapse < 0 || collapse > 2) {
+        set_error("wide collapse must be 0 (largest area first), 1 (surface-area plan) or 2 "
+                  "(the one the probe rays read less of)");
         return MRB_E_ARG;
     }
     if (s->built) {
@@ -1414,6 +1466,16 @@ int mrb_accel_set_wide_collapse(mrb_scene* s, int collapse) {
         return MRB_E_STATE;
     }
     s->wideCollapse = collapse;
+    return 0;
+}
+
+int mrb_accel_wide_collapse(const mrb_scene* s, int* used, double* probeBytes2) {
+    if (!s || !used) return MRB_E_ARG;
+    *used = s->wideCollapseUsed;
+    if (probeBytes2) {
+        probeBytes2[0] = s->collapseProbeBytes[0];
+        probeBytes2[1] = s->collapseProbeBytes[1];
+    }
     return 0;
 }
 
@@ -1753,7 +1815,7 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         t->orderTune = sc->traversal == 1 && sc->T > 1 && sc->wideOrderMode == MRB_WIDE_AUTO &&
                        t->orderEpoch != sc->traceEpoch;
         if (t->orderTune) {
-            std::array<float, kWideOrders> z;
+            std::array<float, kTunedOrders> z;
             z.fill(0.0f);
             t->depthMs.assign(t->maxDepth, z);
             t->depthOrder.assign(t->maxDepth, 0);
@@ -1781,17 +1843,30 @@ int mrb_tracer_render_frame(mrb_tracer* t) {
         if (t->orderTune) {
             t->orderTune = false;
             if (!r) {
-                // per depth the fastest kernel; for the scene's other callers
-                // the fastest over the whole frame
+                // one layout for the whole frame (mixing them per depth would
+                // keep both trees in L2 and slow the next frame's first depth):
+                // the one whose fastest kernels sum to less; then per depth the
+                // fastest kernel on it.  For the scene's other callers the
+                // fastest kernel over the whole frame on the scene's layout.
                 std::array<float, kWideOrders> sum;
                 sum.fill(0.0f);
+                float layoutMs[2] = {0.0f, 0.0f};
+                for (size_t d = 0; d < t->depthMs.size(); d++) {
+                    for (int L = 0; L < 2; L++) {
+                        float m = t->depthMs[d][L * kWideOrders];
+                        for (int o = 1; o < kWideOrders; o++)
+                            m = std::min(m, t->depthMs[d][L * kWideOrders + o]);
+                        layoutMs[L] += m;
+                    }
+                    for (int o = 0; o < kWideOrders; o++) sum[o] += t->depthMs[d][o];
+                }
+                const int L = layoutMs[1] < layoutMs[0] ? 1 : 0;
                 for (size_t d = 0; d < t->depthMs.size(); d++) {
                     int best = 0;
-                    for (int o = 0; o < kWideOrders; o++) {
-                        sum[o] += t->depthMs[d][o];
-                        if (t->depthMs[d][o] < t->depthMs[d][best]) best = o;
-                    }
-                    t->depthOrder[d] = best;
+                    for (int o = 1; o < kWideOrders; o++)
+                        if (t->depthMs[d][L * kWideOrders + o] < t->depthMs[d][L * kWideOrders + best])
+                            best = o;
+                    t->depthOrder[d] = L * kWideOrders + best;
                 }
                 int best = 0;
                 for (int o = 0; o < kWideOrders; o++) {

@@ -1022,6 +1022,42 @@ int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStrea
     return 0;
 }
 
+int wide_probe_compare(const WideAccelDev& a, const WideAccelDev& b, const float* dExtent,
+                       cudaStream_t st, double bytesOut[2]) {
+    constexpr uint32_t kProbe = 1u << 16;
+    void* buf = nullptr;
+    const size_t bytes = size_t(kProbe) * (16 + 16 + 4 + 4 + 4 + 8) + 64;
+    MRB_CUDA(cudaMalloc(&buf, bytes));
+    char* base = static_cast<char*>(buf);
+    float4* ro = reinterpret_cast<float4*>(base);
+    float4* rd = ro + kProbe;
+    HitOut ho{reinterpret_cast<uint32_t*>(rd + kProbe), nullptr, nullptr, nullptr};
+    ho.prim = ho.key + kProbe;
+    ho.t = reinterpret_cast<float*>(ho.prim + kProbe);
+    ho.bary = reinterpret_cast<float2*>(ho.t + kProbe);
+    unsigned long long* work = reinterpret_cast<unsigned long long*>(ho.bary + kProbe);
+    uint32_t* err = reinterpret_cast<uint32_t*>(work + 2);
+    int rc = 0;
+    k_probe_rays<<<(kProbe + 255) / 256, 256, 0, st>>>(dExtent, kProbe, ro, rd);
+    for (int which = 0; which < 2 && !rc; which++) {
+        unsigned long long h[2] = {0ull, 0ull};
+        if (cudaMemsetAsync(work, 0, 16 + 4, st) != cudaSuccess) rc = MRB_E_CUDA;
+        if (!rc)
+            rc = trace_closest_wide(which ? b : a, ro, rd, nullptr, kProbe, ho, err, st, work,
+                                    kWideOctant);
+        if (!rc && (cudaMemcpyAsync(h, work, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess))
+            rc = MRB_E_CUDA;
+        bytesOut[which] = double(h[0]) * double(sizeof(WideNode)) + double(h[1]) * 48.0;
+    }
+    cudaFree(buf);
+    if (rc) {
+        set_error("wide BVH: probe trace failed");
+        return rc;
+    }
+    return 0;
+}
+
 template <int kBlock, int kStack, bool kOctant>
 static int launch_jobs(const JobDev* jobs, const RayAux* aux, const float4* rayO,
                        const float4* rayD, const uint32_t* dCount, uint32_t maxCount,

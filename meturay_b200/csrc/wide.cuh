@@ -60,6 +60,9 @@ enum WideOrder : int {
     kWideOctantRefill = 3,
     kWideOrders = 4
 };
+// A tracer's per-depth choice: kernel o over the scene's layout (o <
+// kWideOrders) or kernel o - kWideOrders over its alternate layout.
+constexpr int kTunedOrders = 2 * kWideOrders;
 int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4* rayD,
                        const uint32_t* dCount, uint32_t maxCount, const HitOut& out,
                        uint32_t* errorFlag, cudaStream_t stream,
@@ -67,6 +70,12 @@ int trace_closest_wide(const WideAccelDev& acc, const float4* rayO, const float4
 // Times every traversal kernel on 65,536 seeded rays over the scene box
 // (device extent: min xyz, max xyz) and returns the fastest; msOut
 // (kWideOrders entries, may be null) the best times.
+// Bytes the octant kernel reads (node visits x 80 B + triangle tests x
+// 48 B, counted on the device) tracing the 65,536 seeded probe rays of
+// wide_order_autotune through two layouts of the same scene: out[0] for a,
+// out[1] for b.
+int wide_probe_compare(const WideAccelDev& a, const WideAccelDev& b, const float* dExtent,
+                       cudaStream_t stream, double out[2]);
 int wide_order_autotune(const WideAccelDev& acc, const float* dExtent, cudaStream_t stream,
                         int* orderOut, float* msOut);
 

@@ -197,9 +197,19 @@ class GPUScene:
 
     def set_wide_collapse(self, collapse: int):
         """Before construct_accelerators: how each 8-wide node picks its
-        children: 0 the largest-area internal child first, 1 (default) the
-        surface-area dynamic program."""
+        children: 0 the largest-area internal child first, 1 the surface-area
+        dynamic program, 2 (default) both, keeping the layout the seeded
+        probe rays read fewer bytes of."""
         check(lib.mrb_accel_set_wide_collapse(self._h, int(collapse)))
+
+    def wide_collapse(self) -> dict:
+        """The collapse in use and, after an automatic choice, the probe
+        bytes of each."""
+        used = C.c_int32()
+        b = np.zeros(2, np.float64)
+        check(lib.mrb_accel_wide_collapse(self._h, C.byref(used), _ptr(b)))
+        names = ("largest_area", "surface_area")
+        return {"used": names[used.value], "probe_bytes": {k: float(v) for k, v in zip(names, b)}}
 
     def build_svo(self, resolution: int):
         """Sparse voxel octree of the scene at `resolution` leaf voxels per axis."""
@@ -380,13 +390,16 @@ class PathTracer:
         return check(lib.mrb_tracer_launches_per_frame(self._h))
 
     def wide_orders(self) -> list:
-        """The 8-wide traversal kernel of each depth (names; None with the
-        binary traversal)."""
+        """The 8-wide traversal kernel of each depth (names, with "+alt" where
+        it runs over the scene's alternate layout; None with the binary
+        traversal)."""
         buf = (C.c_int * 256)()
         n = lib.mrb_tracer_wide_orders(self._h, buf, 256)
         if n < 0:
             check(n)
-        return [WIDE_ORDERS[buf[i]] if buf[i] >= 0 else None for i in range(n)]
+        k = len(WIDE_ORDERS)
+        return [None if buf[i] < 0 else
+                WIDE_ORDERS[buf[i] % k] + ("+alt" if buf[i] >= k else "") for i in range(n)]
 
     def profile_frame(self) -> dict:
         """One stepwise frame with per-stage CUDA-event timings and work counts."""

@@ -169,11 +169,27 @@ def _rays_for(scene, n, seed):
 
 
 KERNELS = ("sorted", "octant", "sorted_refill", "octant_refill")
-# the surface-area collapse (default) with every kernel; the largest-area
-# collapse with two
+# the automatic collapse (default) with every kernel; each explicit one
+# with two
 WIDE = {f"{tree}-{k}": (t, k, None) for t, tree in enumerate(("lbvh", "ploc")) for k in KERNELS}
-WIDE.update({f"{tree}-greedy-{k}": (t, k, 0) for t, tree in enumerate(("lbvh", "ploc"))
-             for k in ("sorted", "octant")})
+WIDE.update({f"{tree}-{c}-{k}": (t, k, ci) for t, tree in enumerate(("lbvh", "ploc"))
+             for ci, c in enumerate(("greedy", "sah")) for k in ("sorted", "octant")})
+
+
+@pytest.mark.parametrize("name,make", _scenes()[::2])
+def test_wide_collapse_choice(system, name, make):
+    """The automatic collapse keeps the layout of which the seeded probe
+    rays read fewer bytes, and reports both measures; the explicit choices
+    are kept as set."""
+    scene = make()
+    g = _build(system, scene)
+    info = g.wide_collapse()
+    b = info["probe_bytes"]
+    assert b["largest_area"] > 0 and b["surface_area"] > 0
+    assert info["used"] == ("largest_area" if b["largest_area"] < b["surface_area"]
+                            else "surface_area")
+    for c, name_ in ((0, "largest_area"), (1, "surface_area")):
+        assert _build(system, scene, collapse=c).wide_collapse()["used"] == name_
 
 
 @pytest.mark.parametrize("mode", ["binary"] + list(WIDE))

@@ -1,9 +1,11 @@
 """Choice of the 8-wide traversal kernel inside a tracer.
 
 * The automatic choice times every kernel per depth on the tracer's own
-  rays (the frame run before the graph capture) and renders what a fixed
-  kernel renders: relative mean error of the image below 1e-4 (the kernels
-  differ only in which of two triangles at the same distance is reported).
+  rays (the frame run before the graph capture), over the scene's layout
+  and its alternate (the other collapse), and renders what a fixed kernel
+  renders: relative mean error of the image below 1e-4 (the kernels and
+  layouts differ only in which of two triangles at the same distance is
+  reported).
 * Every kernel renders the oracle's frame within the drop-in's 1e-4.
 * A traversal setting changed after the capture is picked up by the next
   frame: the graph is captured again and the per-depth choice redone.
@@ -17,6 +19,7 @@ REL_TOL = 1e-4
 OPTS = {"Samples": 2, "MaxDepth": 5, "NextEventEstimation": 1, "RussianRouletteStart": 3,
         "DirectLightMIS": 0, "Seed": 3}
 KERNELS = ("sorted", "octant", "sorted_refill", "octant_refill")
+TUNED = KERNELS + tuple(k + "+alt" for k in KERNELS)   # "+alt": the alternate layout
 
 
 def _rel(a, b):
@@ -49,7 +52,8 @@ def test_auto_choice_renders_what_a_fixed_kernel_renders(system, cornell):
     g.set_traversal(1)
     g.set_wide_order("auto")
     auto, orders = _frames(system, g)
-    assert len(orders) == OPTS["MaxDepth"] and all(o in KERNELS for o in orders)
+    assert len(orders) == OPTS["MaxDepth"] and all(o in TUNED for o in orders)
+    assert all(v > 0 for v in g.wide_collapse()["probe_bytes"].values())  # both layouts built
     ms = g.wide_order()["ms"]
     assert all(v > 0 for v in ms.values())   # every kernel was timed
     for k in KERNELS:
@@ -91,7 +95,7 @@ def test_traversal_change_after_capture(system, cornell):
     t = PathTracer(system, g)
     t.set_options(OPTS)
     t.render_frame()
-    assert all(o in KERNELS for o in t.wide_orders())
+    assert all(o in TUNED for o in t.wide_orders())
     g.set_traversal(0)          # binary nodes from the next frame on
     t.render_frame()
     assert t.wide_orders() == [None] * OPTS["MaxDepth"]
