@@ -393,6 +393,10 @@ int mrb_tracer_svo_guiding(mrb_tracer* t, uint32_t* leaf_shadow, uint16_t* node_
 int mrb_tracer_guide_export(mrb_tracer* t, uint32_t* count, uint32_t* samples, uint32_t* guide2,
                             uint32_t* sorted_bin_key, uint32_t* sorted_rid);
 int mrb_tracer_set_resolution(mrb_tracer* t, uint32_t width, uint32_t height);
+/* The camera of the next frames.  The frame is copied to the device in
+ * stream order (after the frames already enqueued) from one of four pinned
+ * staging slots; the call waits only when the upload that last used its
+ * slot, four calls back, is still queued. */
 int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* cam);
 /* The camera frame as the device sees it (14 floats: position, bottom-left,
  * right, up, plane size, near/far); GPUCameraPinhole.cuh:135-162. */

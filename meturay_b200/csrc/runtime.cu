@@ -173,7 +173,13 @@ struct mrb_tracer {
     uint32_t samples = 1, maxDepth = 5, nee = 1, rrStart = 3, mis = 0;
     uint64_t seed = 1;
     uint32_t width = 0, height = 0;
-    CameraDev* hostCam = nullptr;  // pinned staging copy of the camera frame
+    // pinned staging copies of the camera frame, used in turn; camEv[i] marks
+    // the upload that last read slot i
+    static constexpr int kCamSlots = 4;
+    CameraDev* hostCam = nullptr;
+    cudaEvent_t camEv[kCamSlots] = {};
+    bool camEvUsed[kCamSlots] = {};
+    int camSlot = 0;
     DBuf devCam;                   // the frame the camera kernel reads
     bool camSet = false;
     uint32_t launchesPerFrame = 0;
@@ -256,6 +262,8 @@ struct mrb_tracer {
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
         if (hostCam) cudaFreeHost(hostCam);
+        for (cudaEvent_t ev : camEv)
+            if (ev) cudaEventDestroy(ev);
         if (trainFork) cudaEventDestroy(trainFork);
         if (trainJoin) cudaEventDestroy(trainJoin);
         if (trainStream) cudaStreamDestroy(trainStream);
@@ -1518,7 +1526,11 @@ int mrb_tracer_create(mrb_system* sys, mrb_scene* scene, const char* type, mrb_t
     t->wfpg = wfpg;
     if (wfpg) t->maxDepth = 10;  // WFPGTracer::Options::maximumDepth
     cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&t->hostCam), sizeof(CameraDev));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(reinterpret_cast<void**>(&t->hostCam),
+                           sizeof(CameraDev) * mrb_tracer::kCamSlots);
+    for (int i = 0; i < mrb_tracer::kCamSlots && e == cudaSuccess; i++)
+        e = cudaEventCreateWithFlags(&t->camEv[i], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete t;
         set_error("tracer setup: %s", cudaGetErrorString(e));
@@ -1713,9 +1725,12 @@ int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* c) {
     if (!t || !c) return MRB_E_ARG;
     float f[14];
     mrb_camera_frame(c, f);
-    // the previous upload may still be reading the staging copy
-    MRB_CUDA(cudaStreamSynchronize(t->stream));
-    CameraDev& cam = *t->hostCam;
+    // the next staging slot; the upload that last read it may still be queued
+    // (no wait on the frames in flight: the stream orders each upload after
+    // the frames before it)
+    const int slot = (t->camSlot + 1) % mrb_tracer::kCamSlots;
+    if (t->camEvUsed[slot]) MRB_CUDA(cudaEventSynchronize(t->camEv[slot]));
+    CameraDev& cam = t->hostCam[slot];
     for (int i = 0; i < 3; i++) {
         cam.position[i] = f[i];
         cam.bottomLeft[i] = f[3 + i];
@@ -1727,8 +1742,11 @@ int mrb_tracer_set_camera(mrb_tracer* t, const mrb_camera* c) {
     cam.nearFar[0] = c->near_far[0];
     cam.nearFar[1] = c->near_far[1];
     // host -> device copy of the frame; graphs read it from device memory
-    MRB_CUDA(cudaMemcpyAsync(t->devCam.p, t->hostCam, sizeof(CameraDev), cudaMemcpyHostToDevice,
+    MRB_CUDA(cudaMemcpyAsync(t->devCam.p, &cam, sizeof(CameraDev), cudaMemcpyHostToDevice,
                              t->stream));
+    MRB_CUDA(cudaEventRecord(t->camEv[slot], t->stream));
+    t->camEvUsed[slot] = true;
+    t->camSlot = slot;
     t->camSet = true;
     return 0;
 }
