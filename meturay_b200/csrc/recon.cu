@@ -232,6 +232,72 @@ __global__ void __launch_bounds__(256) k_filter_grid(const float4* __restrict__ 
     }
 }
 
+// The same splat for a 16x16 pixel tile per block: the tile's samples with
+// their halo (coordinates and values) are staged once in shared memory by
+// coalesced row loads, then each thread sums its pixel's window from there in
+// the order of k_filter_grid (rows, then columns, ascending), so the image is
+// the same bit for bit; only the reads change (each sample was read by up to
+// win^2 pixels through L1/L2).
+constexpr int32_t kFilterTile = 16;
+__global__ void __launch_bounds__(256) k_filter_grid_tiled(const float4* __restrict__ samples,
+                                                           const float2* __restrict__ coords,
+                                                           uint32_t width, uint32_t height,
+                                                           uint32_t sp, ReconFilterDev f,
+                                                           float multiplier,
+                                                           float4* __restrict__ image) {
+    extern __shared__ float4 smem[];
+    const int32_t range = static_cast<int32_t>(f.wh);
+    const int32_t hi = (range + 2) / 2;
+    const int32_t loMin = -(range - 1) / 2 - ((range % 2 == 0) ? 1 : 0);
+    const float r2 = f.radius * f.radius;
+    const int32_t S = static_cast<int32_t>(sp);
+    const int32_t SW = static_cast<int32_t>(width) * S, SH = static_cast<int32_t>(height) * S;
+    // staged sample rectangle: pixels [t0 - hi, t0 + tile - 1 - loMin + 1], times S
+    const int32_t span = (kFilterTile + hi - loMin + 1) * S;
+    float4* sv = smem;                                           // span * span values
+    float2* sc = reinterpret_cast<float2*>(smem + span * span);  // span * span coordinates
+    const int32_t tilesX = (static_cast<int32_t>(width) + kFilterTile - 1) / kFilterTile;
+    const int32_t tx0 = (static_cast<int32_t>(blockIdx.x) % tilesX) * kFilterTile;
+    const int32_t ty0 = (static_cast<int32_t>(blockIdx.x) / tilesX) * kFilterTile;
+    const int32_t ox = (tx0 - hi) * S, oy = (ty0 - hi) * S;      // staged origin (samples)
+    for (int32_t i = threadIdx.x; i < span * span; i += blockDim.x) {
+        const int32_t ly = i / span, lx = i - ly * span;
+        const int32_t sy = oy + ly, sx = ox + lx;
+        if (sy >= 0 && sy < SH && sx >= 0 && sx < SW) {
+            const size_t sid = size_t(sy) * size_t(SW) + size_t(sx);
+            sc[i] = coords[sid];
+            sv[i] = samples[sid];
+        }
+    }
+    __syncthreads();
+    const int32_t px = tx0 + static_cast<int32_t>(threadIdx.x) % kFilterTile;
+    const int32_t py = ty0 + static_cast<int32_t>(threadIdx.x) / kFilterTile;
+    if (px >= static_cast<int32_t>(width) || py >= static_cast<int32_t>(height)) return;
+    const float pcx = static_cast<float>(px) + 0.5f, pcy = static_cast<float>(py) + 0.5f;
+    const int32_t sy0 = max(0, (py - hi) * S), sy1 = min(SH, (py - loMin + 2) * S);
+    const int32_t sx0 = max(0, (px - hi) * S), sx1 = min(SW, (px - loMin + 2) * S);
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, wsum = 0.0f;
+    for (int32_t sy = sy0; sy < sy1; sy++)
+        for (int32_t sx = sx0; sx < sx1; sx++) {
+            const int32_t li = (sy - oy) * span + (sx - ox);
+            const float2 c = sc[li];
+            const SamplePix s = sample_pix(c.x, c.y, f.wh);
+            if (!s.ok) continue;
+            const int32_t x = px - s.ix, y = py - s.iy;
+            if (x < s.x0 || x >= s.x1 || y < s.y0 || y >= s.y1) continue;
+            if (!sample_reaches(s, c.x, c.y, x, y, f.wh, r2)) continue;
+            const float w = recon_weight(f, pcx, pcy, c.x, c.y) * multiplier;
+            const float4 v = sv[li];
+            wsum += w;
+            ax += w * v.x;
+            ay += w * v.y;
+            az += w * v.z;
+        }
+    const size_t p = size_t(py) * width + size_t(px);
+    float4 acc = image[p];
+    image[p] = make_float4(acc.x + ax, acc.y + ay, acc.z + az, acc.w + wsum);
+}
+
 // KCCheckPixels (ImageMemory.cu:34-60)
 __global__ void __launch_bounds__(256) k_check_pixels(float* __restrict__ pixels, uint32_t channels,
                                                       size_t count) {
@@ -411,8 +477,22 @@ int recon_filter_grid(const ReconFilterDev& f, const float4* samples, const floa
                       uint32_t width, uint32_t height, uint32_t sp, float multiplier,
                       float4* image, cudaStream_t stream) {
     const size_t pix = size_t(width) * height;
-    k_filter_grid<<<grid_of(pix, 148 * 16), 256, 0, stream>>>(samples, coords, width, height, sp, f,
-                                                             multiplier, image);
+    // the tiled form where its staged rectangle fits the default 48 KB of
+    // shared memory (1 and 2 samples per pixel axis with small filters)
+    const int32_t range = static_cast<int32_t>(f.wh);
+    const int32_t hi = (range + 2) / 2;
+    const int32_t loMin = -(range - 1) / 2 - ((range % 2 == 0) ? 1 : 0);
+    const size_t span = size_t(kFilterTile + hi - loMin + 1) * sp;
+    const size_t smemBytes = span * span * (sizeof(float4) + sizeof(float2));
+    if (smemBytes <= 48 * 1024) {
+        const size_t tiles = size_t((width + kFilterTile - 1) / kFilterTile) *
+                             ((height + kFilterTile - 1) / kFilterTile);
+        k_filter_grid_tiled<<<static_cast<uint32_t>(tiles), 256, smemBytes, stream>>>(
+            samples, coords, width, height, sp, f, multiplier, image);
+    } else {
+        k_filter_grid<<<grid_of(pix, 148 * 16), 256, 0, stream>>>(samples, coords, width, height,
+                                                                 sp, f, multiplier, image);
+    }
     MRB_CUDA(cudaGetLastError());
     return 0;
 }

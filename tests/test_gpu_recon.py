@@ -148,6 +148,26 @@ def test_tracer_filter_matches_oracle_splat(system, cuda, oracle, flt):
     assert _bits_equal(px[..., :3], img[..., :3]) and _bits_equal(cnt, img[..., 3])
 
 
+@pytest.mark.parametrize("samples", [1, 3])
+def test_tracer_filter_tile_and_fallback(system, oracle, samples):
+    """The filter stages a 16x16 pixel tile's samples in shared memory where
+    they fit (1 or 2 samples per pixel axis with these filters) and reads
+    them from global memory otherwise (3 and more); either way the image is
+    the oracle's splat bit for bit, on an image whose sides are not tile
+    multiples."""
+    from meturay_b200 import scenes
+    scene = scenes.cornell(seed=2, width=37, height=21)
+    opts = dict(OPTS, Samples=samples)
+    flt = ("Tent", 1.0, {})
+    g, t = _tracer(system, scene, opts, flt=flt)
+    t.render_frame()
+    img = t.image()
+    s = t.sample_radiance().reshape(-1, 4)
+    coords = oracle.camera_img_coords(scene.width, scene.height, samples, opts["Seed"], 0)
+    ref_p, ref_c = oracle.filter_to_img("Tent", 1.0, s, coords, (scene.width, scene.height))
+    assert _bits_equal(img[..., :3], ref_p[..., :3]) and _bits_equal(img[..., 3], ref_c)
+
+
 def test_tracer_filter_frames_accumulate_and_graph_matches_eager(system, oracle):
     from meturay_b200 import scenes
     scene = scenes.cornell(seed=4, width=40, height=32)
