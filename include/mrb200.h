@@ -162,6 +162,9 @@ int mrb_accel_info(const mrb_scene* scene, uint32_t* info4);
 #define MRB_WIDE_SORTED_REFILL 2
 #define MRB_WIDE_OCTANT_REFILL 3
 #define MRB_WIDE_AUTO 4
+/* Flag in mrb_tracer_wide_orders: the kernel runs over the scene's
+ * alternate 8-wide layout (mrb_accel_wide_collapse). */
+#define MRB_WIDE_ALT_LAYOUT 16
 int mrb_accel_set_wide_order(mrb_scene* s, int order);
 /* The kernel in use where no tracer tuned its own (MRB_WIDE_SORTED ..
  * MRB_WIDE_OCTANT_REFILL) and, in ms4 (may be NULL), the last measured
@@ -435,8 +438,8 @@ void* mrb_tracer_stream(mrb_tracer* t);
 /* Number of kernels one frame launches (>= 0), or a negative status. */
 int mrb_tracer_launches_per_frame(mrb_tracer* t);
 /* The 8-wide traversal kernel of each depth (MRB_WIDE_SORTED ..
- * MRB_WIDE_OCTANT_REFILL over the scene's layout; 4 + the kernel over the
- * scene's alternate layout, the other collapse, which the automatic
+ * MRB_WIDE_OCTANT_REFILL, with MRB_WIDE_ALT_LAYOUT set where it runs over
+ * the scene's alternate layout, the other collapse, which the automatic
  * collapse keeps for tracers to time; -1 with the binary traversal) for the
  * first n depths; returns how many were written. */
 int mrb_tracer_wide_orders(const mrb_tracer* t, int* orders, uint32_t n);

@@ -1445,7 +1445,9 @@ int mrb_tracer_wide_orders(const mrb_tracer* t, int* orders, uint32_t n) {
     uint32_t k = 0;
     for (; k < n && k < t->maxDepth; k++) {
         const int o = depth_order(t, k);
-        orders[k] = o >= 0 ? o : (t->scene->traversal == 1 ? t->scene->wideOrder : -1);
+        orders[k] = o >= kWideOrders ? (o - kWideOrders) | MRB_WIDE_ALT_LAYOUT
+                  : o >= 0           ? o
+                  : (t->scene->traversal == 1 ? t->scene->wideOrder : -1);
     }
     return int(k);
 }

@@ -397,9 +397,9 @@ class PathTracer:
         n = lib.mrb_tracer_wide_orders(self._h, buf, 256)
         if n < 0:
             check(n)
-        k = len(WIDE_ORDERS)
+        alt = 16  # MRB_WIDE_ALT_LAYOUT
         return [None if buf[i] < 0 else
-                WIDE_ORDERS[buf[i] % k] + ("+alt" if buf[i] >= k else "") for i in range(n)]
+                WIDE_ORDERS[buf[i] & ~alt] + ("+alt" if buf[i] & alt else "") for i in range(n)]
 
     def profile_frame(self) -> dict:
         """One stepwise frame with per-stage CUDA-event timings and work counts."""
