@@ -228,16 +228,19 @@ __global__ void k_copy_back(const K* __restrict__ ks, K* __restrict__ kd,
 
 inline size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Head of the scratch, cleared by one memset per sort: eight 256-bin
+// histograms, eight pass tickets, the give-up flag.
+constexpr size_t kHistBytes = size_t(8) * 256 * 4;
+constexpr size_t kHeadBytes = kHistBytes + size_t(8) * 4 + 4;
+
 }  // namespace
 
 size_t radix_sort_temp_bytes(uint32_t maxCount, int keyBytes, int beginBit, int endBit) {
     const int passes = (endBit - beginBit + 7) / 8;
     const size_t tiles = (size_t(maxCount) + kTile - 1) / kTile;
     size_t bytes = 0;
-    bytes += align_up(size_t(8) * 256 * 4);                 // histograms
+    bytes += align_up(kHeadBytes);                          // histograms, tickets, error flag
     bytes += align_up((tiles + 1) * 256 * 4);               // tile status
-    bytes += align_up(size_t(8) * 4);                       // tickets
-    bytes += align_up(4);                                   // error flag
     bytes += align_up(size_t(maxCount) * keyBytes);         // key ping-pong
     bytes += align_up(size_t(maxCount) * 4);                // value ping-pong
     (void)passes;
@@ -258,13 +261,11 @@ int radix_sort_pairs(K* keys, uint32_t* vals, const uint32_t* dCount, uint32_t m
     const uint32_t tiles = (maxCount + kTile - 1) / kTile;
     unsigned char* p = static_cast<unsigned char*>(temp);
     uint32_t* hist = reinterpret_cast<uint32_t*>(p);
-    p += align_up(size_t(8) * 256 * 4);
+    uint32_t* tickets = hist + 8 * 256;
+    uint32_t* err = tickets + 8;
+    p += align_up(kHeadBytes);
     uint32_t* status = reinterpret_cast<uint32_t*>(p);
     p += align_up((size_t(tiles) + 1) * 256 * 4);
-    uint32_t* tickets = reinterpret_cast<uint32_t*>(p);
-    p += align_up(size_t(8) * 4);
-    uint32_t* err = reinterpret_cast<uint32_t*>(p);
-    p += align_up(4);
     K* keysAlt = reinterpret_cast<K*>(p);
     p += align_up(size_t(maxCount) * sizeof(K));
     uint32_t* valsAlt = reinterpret_cast<uint32_t*>(p);
@@ -291,9 +292,7 @@ int radix_sort_pairs(K* keys, uint32_t* vals, const uint32_t* dCount, uint32_t m
             done = true;
         }
     }
-    MRB_CUDA(cudaMemsetAsync(hist, 0, size_t(8) * 256 * 4, stream));
-    MRB_CUDA(cudaMemsetAsync(tickets, 0, size_t(8) * 4, stream));
-    MRB_CUDA(cudaMemsetAsync(err, 0, 4, stream));
+    MRB_CUDA(cudaMemsetAsync(hist, 0, kHeadBytes, stream));  // histograms, tickets, flag
     k_histogram<K><<<148 * 4, kThreads, 0, stream>>>(keys, dCount, maxCount, beginBit, endBit,
                                                     desc ? 1 : 0, hist);
     k_hist_scan<<<passes, 256, 0, stream>>>(hist);
@@ -319,13 +318,8 @@ int radix_sort_pairs(K* keys, uint32_t* vals, const uint32_t* dCount, uint32_t m
     return 0;
 }
 
-uint32_t* radix_sort_error_flag(void* temp, uint32_t maxCount) {
-    const size_t tiles = (size_t(maxCount) + kTile - 1) / kTile;
-    unsigned char* p = static_cast<unsigned char*>(temp);
-    p += align_up(size_t(8) * 256 * 4);
-    p += align_up((tiles + 1) * 256 * 4);
-    p += align_up(size_t(8) * 4);
-    return reinterpret_cast<uint32_t*>(p);
+uint32_t* radix_sort_error_flag(void* temp, uint32_t) {
+    return reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(temp) + kHistBytes) + 8;
 }
 
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, const uint32_t*, uint32_t, int, int,
