@@ -187,9 +187,10 @@ int record_iteration(mrb_pool* p) {
                                          cnt + cur, p->maxRays, ho,
                                          p->errorFlags.as<uint32_t>(), p->block, p->stack, st)))
             return r;
-        if ((r = add_count(p->counters.as<unsigned long long>(), cnt + cur, st))) return r;
+        // also adds this wavefront to the traced-ray total and clears the
+        // next wavefront's counter
         if ((r = dense_keys(ho.key, cnt + cur, p->maxRays, p->idBits, p->dense.as<uint32_t>(), pt,
-                            st)))
+                            st, p->counters.as<unsigned long long>(), cnt + nxt)))
             return r;
         if ((r = radix_sort_pairs<uint32_t>(p->dense.as<uint32_t>(), p->sortedIds.as<uint32_t>(),
                                             cnt + cur, p->maxRays, 0, 3 + int(p->idBits), true,
@@ -197,7 +198,6 @@ int record_iteration(mrb_pool* p) {
             return r;
         if ((r = find_portions(p->dense.as<uint32_t>(), cnt + cur, p->maxRays, p->idBits, pt, st)))
             return r;
-        MRB_CUDA(cudaMemsetAsync(cnt + nxt, 0, 4, st));
         const HitIn hi{ho.key, ho.prim, ho.t, ho.bary};
         if ((r = shade_jobs(p->devJobs(), p->rayO[cur].as<float4>(), p->rayD[cur].as<float4>(),
                             p->aux[cur].as<RayAux>(), hi, p->sortedIds.as<uint32_t>(), pt.nonNull,

@@ -717,7 +717,6 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
                                 workCounters, order)))
             return r;
     }
-    if ((r = add_count(t->counters.as<unsigned long long>(), cnt + cur, t->stream))) return r;
     // the learned sampler skips the last depth, whose guide words no ray
     // reads (the octree guider keeps the reference's schedule)
     const bool guideNow = t->wfpg && !t->skipPG && d < t->guideBounce &&
@@ -754,8 +753,10 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
     }
     if (mark(2)) return MRB_E_CUDA;
     PortionTable pt = portion_table(t);
+    // also adds this wavefront to the traced-ray total and clears the next
+    // wavefront's counter
     if ((r = dense_keys(ho.key, cnt + cur, t->maxRays, sc->idBits, t->dense.as<uint32_t>(), pt,
-                        t->stream)))
+                        t->stream, t->counters.as<unsigned long long>(), cnt + nxt)))
         return r;
     if ((r = radix_sort_pairs<uint32_t>(t->dense.as<uint32_t>(), t->sortedIds.as<uint32_t>(),
                                         cnt + cur, t->maxRays, 0, 3 + int(sc->idBits), true,
@@ -765,7 +766,6 @@ int step_depth(mrb_tracer* t, uint32_t d, StageTimer* tm = nullptr,
                            t->stream)))
         return r;
     if (mark(3) || lap(2, 2)) return MRB_E_CUDA;
-    MRB_CUDA(cudaMemsetAsync(cnt + nxt, 0, 4, t->stream));
     HitIn hi{ho.key, ho.prim, ho.t, ho.bary};
     const bool gen = (d + 1) < t->maxDepth;
     if (mark(4)) return MRB_E_CUDA;
@@ -842,14 +842,14 @@ int record_frame(mrb_tracer* t) {
     return step_finalize(t);
 }
 
-// Kernel launches recorded per frame (camera, per depth: trace, add_count,
-// dense keys, histogram, histogram scan, onesweep passes (+copy-back),
-// portions, shade; then resolve and frame advance).
+// Kernel launches recorded per frame (camera, per depth: trace, dense keys
+// (with the ray count), histogram, histogram scan, onesweep passes
+// (+copy-back), portions, shade; then resolve and frame advance).
 uint32_t launches_per_frame(const mrb_tracer* t) {
     const uint32_t bits = 3 + t->scene->idBits;
     const uint32_t passes = (bits + 7) / 8;
     const uint32_t sort = 2 + passes + (passes & 1);
-    uint32_t n = 1 + t->maxDepth * (3 + sort + 2) + 2;
+    uint32_t n = 1 + t->maxDepth * (2 + sort + 2) + 2;
     if (t->wfpg && t->svoReady) {
         // guiding per guided depth; deposit, leaf averages and the two
         // level filters per frame

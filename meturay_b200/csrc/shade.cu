@@ -110,15 +110,24 @@ __global__ void __launch_bounds__(256) k_camera(const CameraDev* __restrict__ ca
     }
 }
 
+// Block 0 also adds the wavefront's ray count to the traced-ray total and
+// clears the next wavefront's counter (where given): two tiny launches less
+// per depth.
 __global__ void __launch_bounds__(256) k_dense_keys(const uint32_t* __restrict__ hitKey,
                                                     const uint32_t* __restrict__ dCount,
                                                     uint32_t idBits, uint32_t* __restrict__ dense,
-                                                    PortionTable table) {
+                                                    PortionTable table,
+                                                    unsigned long long* rayTotal,
+                                                    uint32_t* nextCount) {
     const uint32_t n = *dCount;
     if (blockIdx.x == 0 && threadIdx.x < 8) {
         table.offset[threadIdx.x] = 0;
         table.end[threadIdx.x] = 0;
-        if (threadIdx.x == 0) *table.nonNull = n;
+        if (threadIdx.x == 0) {
+            *table.nonNull = n;
+            if (rayTotal) *rayTotal += n;
+            if (nextCount) *nextCount = 0u;
+        }
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t k = hitKey[i];
@@ -491,9 +500,6 @@ __global__ void __launch_bounds__(256) k_resolve(const float4* __restrict__ samp
     }
 }
 
-__global__ void k_add_u64(unsigned long long* acc, const uint32_t* v) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *acc += *v;
-}
 __global__ void k_frame_advance(uint32_t* frame) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *frame += 1u;
 }
@@ -607,9 +613,10 @@ int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseM
 }
 
 int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount, uint32_t idBits,
-               uint32_t* dense, const PortionTable& table, cudaStream_t stream) {
+               uint32_t* dense, const PortionTable& table, cudaStream_t stream,
+               unsigned long long* rayTotal, uint32_t* nextCount) {
     k_dense_keys<<<grid_for(maxCount, 256, 148 * 8), 256, 0, stream>>>(hitKey, dCount, idBits, dense,
-                                                                      table);
+                                                                      table, rayTotal, nextCount);
     MRB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -642,11 +649,6 @@ int resolve(const float4* samples, uint32_t width, uint32_t height, uint32_t sp,
     return 0;
 }
 
-int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream) {
-    k_add_u64<<<1, 32, 0, stream>>>(acc, v);
-    MRB_CUDA(cudaGetLastError());
-    return 0;
-}
 
 int frame_advance(uint32_t* frame, cudaStream_t stream) {
     k_frame_advance<<<1, 32, 0, stream>>>(frame);

@@ -49,8 +49,12 @@ struct PathChain {
 int camera_generate(const CameraDev* cam, const PathOptions& opt, uint32_t baseMedium,
                     float4* rayO, float4* rayD, RayAux* aux, float4* samples, uint32_t* count,
                     const PathChain& chain, float2* imgCoords, cudaStream_t stream);
+// Dense sort keys (batch | material index in idBits) and the portion table
+// cleared; with rayTotal, *dCount is added to it; with nextCount, that
+// counter is set to 0 (both by one thread, in stream order).
 int dense_keys(const uint32_t* hitKey, const uint32_t* dCount, uint32_t maxCount, uint32_t idBits,
-               uint32_t* dense, const PortionTable& table, cudaStream_t stream);
+               uint32_t* dense, const PortionTable& table, cudaStream_t stream,
+               unsigned long long* rayTotal = nullptr, uint32_t* nextCount = nullptr);
 int find_portions(const uint32_t* sortedDense, const uint32_t* dCount, uint32_t maxCount,
                   uint32_t idBits, const PortionTable& table, cudaStream_t stream);
 int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayAux* aux,
@@ -60,7 +64,6 @@ int shade(const SceneDev& sc, const float4* rayO, const float4* rayD, const RayA
           const PathChain& chain, const uint2* guide, cudaStream_t stream);
 int resolve(const float4* samples, uint32_t width, uint32_t height, uint32_t sp, float4* image,
             cudaStream_t stream);
-int add_count(unsigned long long* acc, const uint32_t* v, cudaStream_t stream);
 int frame_advance(uint32_t* frame, cudaStream_t stream);
 
 }  // namespace mrb
